@@ -1,0 +1,221 @@
+"""Python binding of the B200 melt-pool solver's C ABI (include/amcfd.h).
+
+This is the host-side mirror of the reference's in-process interface
+(CFDSolverManager.h:96-104 driven by src/main.cpp:123-201): a deck is parsed,
+a solver context is created on one GPU, and each call to ``Solver.step()``
+performs one time step (timet += delt, updateLaser, iterativeLoopSolve,
+updateSolutions) on the device.  Fields are read back by the reference's
+registry keys ("temp", "uvel", ...).
+
+The binding loads ``libamcfd_b200.so`` built in this directory; there is no
+fallback: a missing library is an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libamcfd_b200.so")
+MAX_ZONES = 32
+
+SCHEME_UPWIND, SCHEME_POWER_LAW, SCHEME_EXPONENTIAL = 0, 1, 2
+ORDER_EXACT, ORDER_REDBLACK = 0, 1
+PREC_FP64, PREC_FP32 = 0, 1
+PHASES = {"laser": 1, "energy_assemble": 2, "energy_residual": 3, "props": 4,
+          "block_correct": 5, "energy_solve": 6, "h2t": 7, "meltpool": 8, "momentum": 9,
+          "fluxes": 10, "update": 11}
+ERRORS = {0: "AMCFD_OK", -1: "AMCFD_E_ARG", -2: "AMCFD_E_IO", -3: "AMCFD_E_PARSE",
+          -4: "AMCFD_E_CUDA", -5: "AMCFD_E_NONFINITE", -6: "AMCFD_E_TIMEOUT",
+          -7: "AMCFD_E_NOMEM", -8: "AMCFD_E_CAPACITY"}
+
+_D = C.c_double
+_I = C.c_int
+
+
+class AmcfdParams(C.Structure):
+    _fields_ = [("nzx", _I), ("nzy", _I), ("nzz", _I),
+                ("xzone", _D * MAX_ZONES), ("ncvx", _D * MAX_ZONES), ("powrx", _D * MAX_ZONES),
+                ("yzone", _D * MAX_ZONES), ("ncvy", _D * MAX_ZONES), ("powry", _D * MAX_ZONES),
+                ("zzone", _D * MAX_ZONES), ("ncvz", _D * MAX_ZONES), ("powrz", _D * MAX_ZONES)] + \
+        [(n, _D) for n in ("dens denl viscos tsolid tliquid hsmelt hlfriz acpa acpb acpl "
+                           "thconsa thconsb thconsc thconla thconlb urfu urfv urfw urfp urfh "
+                           "htci htcj htck1 htckn emiss tempwest tempeast tempnorth tempbottom "
+                           "temppreheat beta dgdtp darcyKo a_oxygen grav sigm tempamb pressamb "
+                           "gasconst alaspow alaseta alasrb alasfact lasertime xstart ystart "
+                           "scanvel avolpow apowseta heatthick heatrb avolfact").split()] + \
+        [("isevap", _I)] + [(n, _D) for n in "evaplatent evaptemp evapfact molarmass".split()] + \
+        [(n, _D) for n in "delt outtime finaltime nonlintol".split()] + \
+        [(n, _I) for n in "maxit scheme navierstokes steady udtoolpath ntool".split()] + \
+        [("tool_txyz", C.POINTER(_D)), ("tool_on", C.POINTER(_I)), ("tool_id", C.POINTER(_I)),
+         ("nheattable", _I), ("heattable", C.POINTER(_D)),
+         ("nvardt", _I), ("vardt", C.POINTER(_D))] + \
+        [(n, _I) for n in "powderbed movingmesh species freesurface".split()]
+
+
+class AmcfdReport(C.Structure):
+    _fields_ = [("timet", _D), ("niter", _I), ("itertot", _I)] + \
+        [(n, _D) for n in ("resorh resorm resoru resorv resorw tpeak alen depth width ratio "
+                           "heatinlaser ahtoploss accul heatout heatvol beamposx beamposy "
+                           "scanvel").split()] + \
+        [(n, _I) for n in ("istat iend jstat jend kstat jstart powerindicator momentum_cells "
+                           "fallback").split()]
+
+    def as_dict(self) -> Dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class AmcfdOptions(C.Structure):
+    _fields_ = [("device", _I), ("order", _I), ("precision", _I), ("use_graphs", _I),
+                ("check_finite", _I), ("reserved", _I * 8)]
+
+
+class AmcfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Load libamcfd_b200.so (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(
+                f"{LIB_PATH} is missing: build it with `python __graft_entry__.py build`")
+        L = C.CDLL(LIB_PATH)
+        P, VP = C.POINTER, C.c_void_p
+        L.amcfd_deck_load.argtypes = [C.c_char_p, P(VP)]
+        L.amcfd_deck_params.argtypes = [VP, P(AmcfdParams)]
+        L.amcfd_deck_error.restype = C.c_char_p
+        L.amcfd_deck_free.argtypes = [VP]
+        L.amcfd_deck_string.argtypes = [VP, C.c_char_p]
+        L.amcfd_deck_string.restype = C.c_char_p
+        L.amcfd_sizeof_params.restype = C.c_size_t
+        L.amcfd_sizeof_report.restype = C.c_size_t
+        if hasattr(L, "amcfd_create"):
+            L.amcfd_create.argtypes = [P(AmcfdParams), P(AmcfdOptions), P(VP)]
+            L.amcfd_destroy.argtypes = [VP]
+            L.amcfd_last_error.argtypes = [VP]
+            L.amcfd_last_error.restype = C.c_char_p
+            L.amcfd_step.argtypes = [VP, P(AmcfdReport)]
+            L.amcfd_get_field.argtypes = [VP, C.c_char_p, P(_D)]
+            L.amcfd_set_field.argtypes = [VP, C.c_char_p, P(_D)]
+            L.amcfd_get_grid.argtypes = [VP, C.c_char_p, P(_D)]
+            L.amcfd_dims.argtypes = [VP, P(_I), P(_I), P(_I)]
+            L.amcfd_run_phase.argtypes = [VP, _I, P(AmcfdReport)]
+            L.amcfd_phase_name.argtypes = [_I]
+            L.amcfd_phase_name.restype = C.c_char_p
+            L.amcfd_last_timing.argtypes = [VP, P(_D), _I]
+        _lib = L
+    return _lib
+
+
+class Deck:
+    """A parsed keyword deck (amcfd_deck_load)."""
+
+    def __init__(self, path: str):
+        L = lib()
+        self._h = C.c_void_p()
+        rc = L.amcfd_deck_load(path.encode(), C.byref(self._h))
+        if rc != 0:
+            raise AmcfdError(rc, L.amcfd_deck_error().decode())
+        self.path = path
+        self.params = AmcfdParams()
+        rc = L.amcfd_deck_params(self._h, C.byref(self.params))
+        if rc != 0:
+            raise AmcfdError(rc, L.amcfd_deck_error().decode())
+
+    def string(self, what: str) -> Optional[str]:
+        r = lib().amcfd_deck_string(self._h, what.encode())
+        return None if r is None else r.decode()
+
+    @property
+    def dims(self):
+        p = self.params
+        ni = int(sum(p.ncvx[q] for q in range(p.nzx))) + 2
+        nj = int(sum(p.ncvy[q] for q in range(p.nzy))) + 2
+        nk = int(sum(p.ncvz[q] for q in range(p.nzz))) + 2
+        return ni, nj, nk
+
+    def close(self):
+        if self._h:
+            lib().amcfd_deck_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Solver:
+    """One melt-pool instance on one GPU (amcfd_create ... amcfd_destroy)."""
+
+    def __init__(self, deck: Deck, order: int = ORDER_EXACT, precision: int = PREC_FP64,
+                 device: int = 0, use_graphs: int = 0, check_finite: int = 1):
+        L = lib()
+        self.deck = deck  # keeps toolpath storage alive
+        opts = AmcfdOptions(device=device, order=order, precision=precision,
+                            use_graphs=use_graphs, check_finite=check_finite)
+        self._h = C.c_void_p()
+        rc = L.amcfd_create(C.byref(deck.params), C.byref(opts), C.byref(self._h))
+        if rc != 0:
+            msg = L.amcfd_last_error(self._h).decode() if self._h else "create failed"
+            raise AmcfdError(rc, msg)
+        ni, nj, nk = C.c_int(), C.c_int(), C.c_int()
+        L.amcfd_dims(self._h, C.byref(ni), C.byref(nj), C.byref(nk))
+        self.shape = (nk.value, nj.value, ni.value)
+        self.report = AmcfdReport()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise AmcfdError(rc, lib().amcfd_last_error(self._h).decode())
+
+    def step(self) -> Dict:
+        self._check(lib().amcfd_step(self._h, C.byref(self.report)))
+        return self.report.as_dict()
+
+    def run_phase(self, phase) -> Dict:
+        ph = PHASES[phase] if isinstance(phase, str) else int(phase)
+        self._check(lib().amcfd_run_phase(self._h, ph, C.byref(self.report)))
+        return self.report.as_dict()
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        self._check(lib().amcfd_get_field(self._h, name.encode(),
+                                          out.ctypes.data_as(C.POINTER(_D))))
+        return out
+
+    def set(self, name: str, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64).reshape(self.shape)
+        self._check(lib().amcfd_set_field(self._h, name.encode(), a.ctypes.data_as(C.POINTER(_D))))
+
+    def grid(self, name: str) -> np.ndarray:
+        n = {"x": 2, "xu": 2, "y": 1, "yv": 1, "z": 0, "zw": 0}[name]
+        out = np.empty(self.shape[n], dtype=np.float64)
+        self._check(lib().amcfd_get_grid(self._h, name.encode(), out.ctypes.data_as(C.POINTER(_D))))
+        return out
+
+    def timing(self, n: int = 16) -> np.ndarray:
+        out = np.zeros(n, dtype=np.float64)
+        lib().amcfd_last_timing(self._h, out.ctypes.data_as(C.POINTER(_D)), n)
+        return out
+
+    def close(self):
+        if self._h:
+            lib().amcfd_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,187 @@
+/*
+ * amcfd.h -- C ABI of the B200 melt-pool solver (libamcfd_b200.so).
+ *
+ * The reference AM-CFD exposes no library API: its boundary is the
+ * `AM-CFD <deck.k>` process (src/main.cpp:25-52) and, in-process, the public
+ * methods of CFDSolverManager (src/headers/CFDSolverManager.h:96-104) that
+ * main() calls once per time step.  Each entry point below names the
+ * reference interface it replaces.  All functions return 0 on success and a
+ * negative AMCFD_E* code on failure; amcfd_last_error() gives the message.
+ * Host buffers belong to the caller, device memory to the context; a context
+ * is used from one host thread and owns one CUDA stream.
+ */
+#ifndef AMCFD_H
+#define AMCFD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMCFD_OK 0
+#define AMCFD_E_ARG -1        /* invalid argument or unsupported option */
+#define AMCFD_E_IO -2         /* deck, mesh or toolpath file missing/unreadable */
+#define AMCFD_E_PARSE -3      /* malformed deck row */
+#define AMCFD_E_CUDA -4       /* CUDA runtime error */
+#define AMCFD_E_NONFINITE -5  /* NaN/Inf detected in a residual or field reduction */
+#define AMCFD_E_TIMEOUT -6    /* a bounded device-side wait gave up */
+#define AMCFD_E_NOMEM -7      /* device allocation failed */
+#define AMCFD_E_CAPACITY -8   /* size beyond a fixed capacity */
+
+#define AMCFD_MAX_ZONES 32
+
+/* Discretisation scheme, *SELECT_DISCRETIZATION (Mesh.cpp:378-392). */
+#define AMCFD_SCHEME_UPWIND 0
+#define AMCFD_SCHEME_POWER_LAW 1
+#define AMCFD_SCHEME_EXPONENTIAL 2
+
+/*
+ * Solver parameters: the DomainManager / Mesh fields that the hot path reads
+ * (DomainManager.h:25-72, Mesh.h:22-71), already mapped from the deck by
+ * DomainManager::assignInputValues (DomainManager.cpp:29-263).
+ */
+typedef struct amcfd_params {
+    /* grid zones (DomainManager.cpp:33-46): length, control volumes, exponent */
+    int nzx, nzy, nzz;
+    double xzone[AMCFD_MAX_ZONES], ncvx[AMCFD_MAX_ZONES], powrx[AMCFD_MAX_ZONES];
+    double yzone[AMCFD_MAX_ZONES], ncvy[AMCFD_MAX_ZONES], powry[AMCFD_MAX_ZONES];
+    double zzone[AMCFD_MAX_ZONES], ncvz[AMCFD_MAX_ZONES], powrz[AMCFD_MAX_ZONES];
+    /* material (DomainManager.cpp:59-73) */
+    double dens, denl, viscos, tsolid, tliquid, hsmelt, hlfriz, acpa, acpb, acpl;
+    double thconsa, thconsb, thconsc, thconla, thconlb;
+    /* under-relaxation (:76-80) */
+    double urfu, urfv, urfw, urfp, urfh;
+    /* energy boundary conditions and boundary temperatures (:83-94) */
+    double htci, htcj, htck1, htckn, emiss;
+    double tempwest, tempeast, tempnorth, tempbottom, temppreheat;
+    /* momentum boundary conditions (:97-100) */
+    double beta, dgdtp, darcyKo, a_oxygen;
+    /* *PARAMETERS (Mesh.cpp:440-470) */
+    double grav, sigm, tempamb, pressamb, gasconst;
+    /* Gaussian surface source (:105-108) */
+    double alaspow, alaseta, alasrb, alasfact;
+    /* single track (:51-54): laser-on time, start point, scan speed */
+    double lasertime, xstart, ystart, scanvel;
+    /* scalar volumetric source (:169-173); heatthick = 0 disables it */
+    double avolpow, apowseta, heatthick, heatrb, avolfact;
+    /* *BOUNDARY_EVAPORATION (DomainManager.cpp:113-120); isevap = 0 when absent */
+    int isevap;
+    double evaplatent, evaptemp, evapfact, molarmass;
+    /* time control (Mesh.cpp:284-299) */
+    double delt, outtime, finaltime, nonlintol;
+    int maxit;
+    int scheme;          /* AMCFD_SCHEME_* */
+    int navierstokes;    /* 0 when *FLUID_FLOW_OFF */
+    int steady;          /* delt >= 100 (DomainManager.cpp:203-210) */
+    /* *TOOLPATH_FILE rows (DomainManager.cpp:276-286); udtoolpath = 0 for a single track */
+    int udtoolpath;
+    int ntool;
+    const double *tool_txyz; /* ntool x 4: t, x, y, z */
+    const int *tool_on;      /* ntool: laser-on flag of the segment ending at the row */
+    const int *tool_id;      /* ntool: track id */
+    /* *VOLUMETRIC_HEAT_SOURCE_TABLE rows (t, avolpow, apowseta, heatthick, heatrb, avolfact),
+     * read per outer iteration by calculateSource(5) (CFDSolverManager.cpp:1707-1717) */
+    int nheattable;
+    const double *heattable; /* nheattable x 6 */
+    /* *CONTROL_TIMESTEP_VARIABLE rows (t, delt, outtime), applied per step (main.cpp:125-134) */
+    int nvardt;
+    const double *vardt;     /* nvardt x 3 */
+    /* features the hot path does not implement; amcfd_create rejects them */
+    int powderbed, movingmesh, species, freesurface;
+} amcfd_params;
+
+/* Per-step results, the scalars main() and PrintManager read after
+ * iterativeLoopSolve (CFDSolverManager.h:81-90, BoundCondManager.h:331-342). */
+typedef struct amcfd_step_report {
+    double timet;
+    int niter, itertot;
+    double resorh, resorm, resoru, resorv, resorw;
+    double tpeak, alen, depth, width, ratio;
+    double heatinlaser, ahtoploss, accul, heatout, heatvol;
+    double beamposx, beamposy, scanvel;
+    int istat, iend, jstat, jend, kstat, jstart, powerindicator;
+    int momentum_cells;  /* cells of the momentum box solved in the last outer iteration */
+    int fallback;        /* reserved: 1 when a warm-start guess was rejected */
+} amcfd_step_report;
+
+/* Line-sweep ordering of the line-by-line solver. */
+#define AMCFD_ORDER_EXACT 0    /* the reference's lexicographic Gauss-Seidel order (parity mode) */
+#define AMCFD_ORDER_REDBLACK 1 /* red-black line ordering over (j,k): fully parallel sweeps */
+
+/* Arithmetic of the bulk fields and coefficients. */
+#define AMCFD_PREC_FP64 0
+#define AMCFD_PREC_FP32 1      /* FP32 bulk, FP64 reductions and H->T inversion */
+
+typedef struct amcfd_options {
+    int device;          /* CUDA device ordinal */
+    int order;           /* AMCFD_ORDER_* */
+    int precision;       /* AMCFD_PREC_* */
+    int use_graphs;      /* capture the fixed-shape part of an outer iteration */
+    int check_finite;    /* fail with AMCFD_E_NONFINITE when a reduction is not finite */
+    int reserved[8];
+} amcfd_options;
+
+typedef struct amcfd_deck amcfd_deck;
+typedef struct amcfd_ctx amcfd_ctx;
+
+/* Deck parsing: replaces Mesh::getDomainInfo / assignParameters / readMeshFile
+ * (Mesh.h:74-84) and DomainManager::assignInputValues / getToolpath
+ * (DomainManager.h:256-258).  The returned params point into the deck's own
+ * storage (toolpath rows) and stay valid until amcfd_deck_free. */
+int amcfd_deck_load(const char *path, amcfd_deck **out);
+int amcfd_deck_params(const amcfd_deck *deck, amcfd_params *out);
+const char *amcfd_deck_error(void);
+void amcfd_deck_free(amcfd_deck *deck);
+/* "keyword_id", "directory", "geometry_file" (NULL unless *OUTPUT_FINAL_GEOMETRY),
+ * "mesh_file": the names PrintManager derives its output files from. */
+const char *amcfd_deck_string(const amcfd_deck *deck, const char *what);
+/* sizeof(amcfd_params) / sizeof(amcfd_step_report), for bindings that mirror the structs */
+size_t amcfd_sizeof_params(void);
+size_t amcfd_sizeof_report(void);
+
+/* Context creation: replaces CFDSolverManager::generateGrid + initializeSolver
+ * and BoundCondManager::initializeBoundaries (CFDSolverManager.cpp:34-590,
+ * BoundCondManager.cpp:27-63).  opts may be NULL (FP64, exact order, device 0). */
+int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ctx **out);
+void amcfd_destroy(amcfd_ctx *ctx);
+const char *amcfd_last_error(const amcfd_ctx *ctx);
+
+/* One time step: main.cpp:136-162 -- timet += delt, BoundCondManager::updateLaser,
+ * CFDSolverManager::iterativeLoopSolve, CFDSolverManager::updateSolutions. */
+int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
+
+/* Field access by the reference's registry key (CFDSolverManager.cpp:528-541):
+ * "temp","uvel","vvel","wvel","pressure","pp","enthalpy","fracl","fraclnot",
+ * "hnot","diff","rho","vis","sourceinput"; grid arrays "x","y","z","xu","yv","zw".
+ * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
+int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out);
+int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in);
+int amcfd_get_grid(amcfd_ctx *ctx, const char *name, double *host_out);
+int amcfd_dims(const amcfd_ctx *ctx, int *ni, int *nj, int *nk);
+
+/* Kernel-level entry points for parity tests: run one phase of an outer
+ * iteration on the current device state (the reference function each phase
+ * replaces is listed in amcfd_phase_name). */
+#define AMCFD_PHASE_LASER 1          /* BoundCondManager::updateLaser */
+#define AMCFD_PHASE_ENERGY_ASSEMBLE 2 /* applyBCs(5)+discretizeEquations(5)+calculateSource(5) */
+#define AMCFD_PHASE_ENERGY_RESIDUAL 3 /* calculateResiduals(5) */
+#define AMCFD_PHASE_PROPS 4          /* bareplateMaterialProps */
+#define AMCFD_PHASE_BLOCK_CORRECT 5  /* enhanceConvergenceSpeed(5) */
+#define AMCFD_PHASE_ENERGY_SOLVE 6   /* solveEntireDomain(5) */
+#define AMCFD_PHASE_H2T 7            /* convertEnthalpyToTemp */
+#define AMCFD_PHASE_MELTPOOL 8       /* getMeltPoolShape */
+#define AMCFD_PHASE_MOMENTUM 9       /* cleanVelocities + ivar 1..4 chain */
+#define AMCFD_PHASE_FLUXES 10        /* calculateFluxes */
+#define AMCFD_PHASE_UPDATE 11        /* updateSolutions */
+int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report);
+const char *amcfd_phase_name(int phase);
+
+/* Device time of the last amcfd_step split by kernel family (ms); n entries. */
+int amcfd_last_timing(const amcfd_ctx *ctx, double *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMCFD_H */

@@ -1,0 +1,67 @@
+#!/bin/bash
+# Recipe that compiles the reference AM-CFD solver from its own sources into
+# oracle/_ref/ (git-ignored).  It is test infrastructure: the binaries it makes
+# pin the C restatement in oracle/amcfd_oracle.c and serve as the timed CPU
+# baseline.  Nothing of the reference tree is committed; the sources are copied
+# into oracle/_ref/src at build time and two recorded patches are applied there:
+#
+#   1. CFDSolverManager.cpp:1698 reads the volumetric heat-source table even for
+#      surface-Gaussian decks that have no table, which segfaults on the first
+#      outer iteration.  The branch is keyed on the table flag alone, so a deck
+#      without a volumetric source takes the scalar branch (heatthick = 0, no
+#      volumetric source), which is the intended behaviour.
+#   2. DomainManager.h:83-85 fixes the grid capacity at 400 x 500 x 210 nodes;
+#      the 402- and 602-node x axes of the larger decks overflow the 1-D member
+#      arrays.  The bounds become 610 x 310 x 130 (enough for the 602 x 302 x
+#      122-node deck, and a smaller footprint than the original 42 M cells).
+#
+# Usage: oracle/build_ref.sh [reference-root]   (default: $AMCFD_REFERENCE or
+#        /root/reference).  Exits 0 without building when the tree is absent.
+set -euo pipefail
+HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${1:-${AMCFD_REFERENCE:-/root/reference}}
+OUT="$HERE/_ref"
+if [ ! -f "$REF/src/main.cpp" ]; then
+    echo "build_ref: reference tree not found at $REF; nothing built"
+    exit 0
+fi
+mkdir -p "$OUT/obj"
+rm -rf "$OUT/src"
+mkdir -p "$OUT/src"
+cp -r "$REF/src/sources" "$REF/src/headers" "$REF/src/main.cpp" "$REF/src/version.h" "$OUT/src/"
+chmod -R u+w "$OUT/src"
+
+# patch 1: heat-source branch (CFDSolverManager.cpp:1698)
+sed -i 's/if (meshObj_->volheatsource_ == true \&\& meshObj_->volheatsourcetable_ == false)/if (meshObj_->volheatsourcetable_ == false)/' \
+    "$OUT/src/sources/CFDSolverManager.cpp"
+grep -q 'if (meshObj_->volheatsourcetable_ == false)' "$OUT/src/sources/CFDSolverManager.cpp" \
+    || { echo "build_ref: patch 1 did not apply"; exit 1; }
+# patch 2: grid capacity (DomainManager.h:83-85)
+sed -i -e 's/const int _nx_ = 400;/const int _nx_ = 610;/' \
+       -e 's/const int _ny_ = 500;/const int _ny_ = 310;/' \
+       -e 's/const int _nz_ = 210;/const int _nz_ = 130;/' "$OUT/src/headers/DomainManager.h"
+for b in "_nx_ = 610" "_ny_ = 310" "_nz_ = 130"; do
+    grep -q "const int $b;" "$OUT/src/headers/DomainManager.h" \
+        || { echo "build_ref: patch 2 did not apply ($b)"; exit 1; }
+done
+
+cat > "$OUT/src/version.cpp" <<'EOF'
+#include "version.h"
+const std::string gGIT_VERSION = "reference-oracle";
+const std::string gGIT_VERSION_SHORT = "ref";
+EOF
+
+CXX=${AMCFD_REF_CXX:-g++}   # the system g++ (it ships libgomp)
+FLAGS="-O3 -fopenmp -std=c++11 -I$OUT/src/headers -I$OUT/src -w"
+objs=()
+for f in "$OUT"/src/sources/*.cpp "$OUT/src/version.cpp"; do
+    o="$OUT/obj/$(basename "${f%.cpp}").o"
+    $CXX $FLAGS -c "$f" -o "$o" &
+    objs+=("$o")
+done
+wait
+# stock command-line solver (the reference's own main)
+$CXX $FLAGS "$OUT/src/main.cpp" "${objs[@]}" -o "$OUT/AM-CFD"
+# per-step field dump driver (our own main around the reference managers)
+$CXX $FLAGS "$HERE/ref_driver.cpp" "${objs[@]}" -o "$OUT/amcfd_ref_dump"
+echo "build_ref: built $OUT/AM-CFD and $OUT/amcfd_ref_dump"
