@@ -25,9 +25,8 @@ MAX_ZONES = 32
 SCHEME_UPWIND, SCHEME_POWER_LAW, SCHEME_EXPONENTIAL = 0, 1, 2
 ORDER_EXACT, ORDER_REDBLACK = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
-PHASES = {"laser": 1, "energy_assemble": 2, "energy_residual": 3, "props": 4,
-          "block_correct": 5, "energy_solve": 6, "h2t": 7, "meltpool": 8, "momentum": 9,
-          "fluxes": 10, "update": 11}
+PHASES = {"laser": 1, "energy_assemble": 2, "energy_solve": 3, "h2t": 4, "meltpool": 5,
+          "momentum": 6, "converge": 7, "update": 8}
 ERRORS = {0: "AMCFD_OK", -1: "AMCFD_E_ARG", -2: "AMCFD_E_IO", -3: "AMCFD_E_PARSE",
           -4: "AMCFD_E_CUDA", -5: "AMCFD_E_NONFINITE", -6: "AMCFD_E_TIMEOUT",
           -7: "AMCFD_E_NOMEM", -8: "AMCFD_E_CAPACITY"}

@@ -1,0 +1,737 @@
+// Host driver and C ABI of the solver (include/amcfd.h).
+//
+// A context owns one instance on one GPU: the device arrays, a CUDA stream and
+// the host copy of the grid and laser state.  amcfd_step() reproduces one pass
+// of the reference time loop (src/main.cpp:125-162): variable time step,
+// timet += delt, BoundCondManager::updateLaser (beam position on the host,
+// heat flux on the device), the SIMPLE outer loop of
+// CFDSolverManager::iterativeLoopSolve (CFDSolverManager.cpp:595-722) as a
+// chain of kernels per outer iteration, and updateSolutions.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "amcfd.h"
+#include "kernels.cuh"
+
+namespace amcfd {
+template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
+template <typename T> void set_sweep_smem_limit(size_t smem);
+}  // namespace amcfd
+
+using namespace amcfd;
+
+struct amcfd_ctx {
+    std::string err;
+    amcfd_params prm;
+    std::vector<double> tool, heattable, vardt;
+    std::vector<int> tool_on, tool_id;
+    int precision = AMCFD_PREC_FP64;
+    int order = AMCFD_ORDER_EXACT;
+    int device = 0;
+    int ni = 0, nj = 0, nk = 0, nip = 0;
+    double hlcal = 0, hlatnt = 0;
+    std::vector<double> x, y, z, xu, yv, zw, dxpwinv, dypsinv, dzpbinv, fracx, fracy, fracz;
+    // laser / time state (BoundCondManager.h:339-349, DomainManager::timet_)
+    double timet = 0, delt = 0, outtime = 0, scanvel = 0;
+    double beamposx = 0, beamposy = 0, beamposz = 0, oldbeamposx = 0, oldbeamposy = 0,
+           oldbeamposz = 0;
+    int powerindicator = 1, init = 1, trackindx = 1, istart = 0, jstart = 0, vardt_state = 0;
+    int itertot = 0, niter = 0;
+    Inst<double> I64;
+    Inst<float> I32;
+    std::vector<void *> allocs;
+    cudaStream_t stream = nullptr;
+    Status *st_dev = nullptr;
+    Status *st_host = nullptr;  // pinned
+    cudaEvent_t ev[16];
+    double last_ms[16] = {0};
+    bool events = false;
+};
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            return AMCFD_E_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+static int fail(amcfd_ctx *ctx, int code, const std::string &msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+// ---- grid: CFDSolverManager::generateGrid (CFDSolverManager.cpp:126-240) -------------
+static void zone_faces(int nz, const double *len, const double *ncv, const double *powr,
+                       std::vector<double> &face)
+{
+    face[0] = 0.0;
+    face[1] = 0.0;
+    int ist = 2;
+    double statloc = 0.0;
+    for (int zi = 0; zi < nz; zi++) {
+        for (int q = 0; q < ncv[zi]; q++) {
+            double term;
+            if (powr[zi] >= 0.0)
+                term = std::pow((double)(q + 1) / ncv[zi], powr[zi]);
+            else
+                term = 1.0 - std::pow(1.0 - (double)(q + 1) / ncv[zi], -powr[zi]);
+            face[q + ist] = statloc + len[zi] * term;
+        }
+        ist += (int)ncv[zi];
+        statloc += len[zi];
+    }
+}
+
+static void build_grid(amcfd_ctx *c)
+{
+    const amcfd_params &p = c->prm;
+    auto axis = [](int n, int nz, const double *len, const double *ncv, const double *powr,
+                   std::vector<double> &face, std::vector<double> &cen, std::vector<double> &inv,
+                   std::vector<double> &frac) {
+        face.assign(n + 1, 0.0);
+        cen.assign(n + 1, 0.0);
+        inv.assign(n + 1, 0.0);
+        frac.assign(n + 1, 0.0);
+        zone_faces(nz, len, ncv, powr, face);
+        for (int q = 0; q < n - 1; q++) cen[q] = (face[q + 1] + face[q]) * 0.5;
+        cen[n - 1] = face[n - 1];
+        for (int q = 1; q < n; q++) inv[q] = 1.0 / (cen[q] - cen[q - 1]);
+        for (int q = 0; q < n - 1; q++) frac[q] = (cen[q + 1] - face[q + 1]) / (cen[q + 1] - cen[q]);
+    };
+    axis(c->ni, p.nzx, p.xzone, p.ncvx, p.powrx, c->xu, c->x, c->dxpwinv, c->fracx);
+    axis(c->nj, p.nzy, p.yzone, p.ncvy, p.powry, c->yv, c->y, c->dypsinv, c->fracy);
+    axis(c->nk, p.nzz, p.zzone, p.ncvz, p.powrz, c->zw, c->z, c->dzpbinv, c->fracz);
+}
+
+// ---- laser position: BoundCondManager::getLaserCoords / updateLaser (:68-275) ----------
+static void laser_coords(amcfd_ctx *c)
+{
+    const amcfd_params &p = c->prm;
+    if (p.steady) {
+        c->beamposx = p.xstart;
+    } else if (!p.udtoolpath) {
+        c->oldbeamposx = c->beamposx;
+        if (c->timet <= p.lasertime) {
+            c->beamposx = p.xstart + c->timet * c->scanvel;
+            if (c->init) {
+                c->oldbeamposx = c->beamposx;
+                c->init = 0;
+            }
+        } else {
+            c->beamposx = p.xstart + p.lasertime * c->scanvel;
+            c->powerindicator = 0;
+        }
+        c->beamposy = p.ystart;
+    } else {
+        double tx = 0.0, ty = 0.0, tz = 0.0, deltaty = 0.0;
+        const double small = 1.0e-8;
+        c->oldbeamposx = c->beamposx;
+        c->oldbeamposy = c->beamposy;
+        c->oldbeamposz = c->beamposz;
+        int oldpower = c->powerindicator;
+        const int n = (int)c->tool_on.size();
+        for (int ii = 1; ii < n; ii++) {
+            const double *b = &c->tool[4 * ii];
+            if (c->timet <= b[0] + small) {
+                const double *a = &c->tool[4 * (ii - 1)];
+                double ratio = (c->timet - a[0]) / (b[0] - a[0]);
+                double dx = b[1] - a[1];
+                deltaty = b[2] - a[2];
+                double dz = b[3] - a[3];
+                tx = ratio * dx + a[1];
+                ty = ratio * deltaty + a[2];
+                tz = ratio * dz + a[3];
+                c->powerindicator = c->tool_on[ii];
+                if (c->init) {
+                    c->oldbeamposx = a[1];
+                    c->oldbeamposy = a[2];
+                    c->oldbeamposz = a[3];
+                    oldpower = c->tool_on[ii - 1];
+                    c->init = 0;
+                }
+                break;
+            }
+        }
+        c->beamposx = tx;
+        c->beamposy = ty;
+        c->beamposz = tz;
+        double dist = std::sqrt((c->beamposx - c->oldbeamposx) * (c->beamposx - c->oldbeamposx) +
+                                (c->beamposy - c->oldbeamposy) * (c->beamposy - c->oldbeamposy) +
+                                (c->beamposz - c->oldbeamposz) * (c->beamposz - c->oldbeamposz));
+        c->scanvel = dist / c->delt;
+        if (oldpower - c->powerindicator > 0 && deltaty > small) c->trackindx++;
+    }
+    // nearest node to the beam (:92-126)
+    int iout = 0, jout = 0;
+    for (int i = 1; i < c->ni - 1; i++) {
+        if (c->beamposx <= c->x[i]) break;
+        iout = i;
+    }
+    if (std::fabs(c->beamposx - c->x[iout + 1]) < std::fabs(c->beamposx - c->x[iout])) iout++;
+    c->istart = iout;
+    for (int j = 1; j < c->nj - 1; j++) {
+        if (c->beamposy <= c->y[j]) break;
+        jout = j;
+    }
+    if (std::fabs(c->beamposy - c->y[jout + 1]) < std::fabs(c->beamposy - c->y[jout])) jout++;
+    c->jstart = jout;
+}
+
+// ---- device setup ----------------------------------------------------------------------
+template <typename T>
+static int alloc3(amcfd_ctx *ctx, T **ptr, size_t n)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+        return AMCFD_E_NOMEM;
+    }
+    ctx->allocs.push_back(p);
+    cudaMemsetAsync(p, 0, n * sizeof(T), ctx->stream);
+    *ptr = (T *)p;
+    return 0;
+}
+
+template <typename T>
+static int upload(amcfd_ctx *ctx, T *dst, const std::vector<double> &src)
+{
+    std::vector<T> tmp(src.begin(), src.end());
+    CK(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+template <typename T>
+static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
+{
+    const amcfd_params &q = ctx->prm;
+    Params &p = I.p;
+    memset(&p, 0, sizeof(p));
+    p.ni = ctx->ni; p.nj = ctx->nj; p.nk = ctx->nk; p.nip = ctx->nip;
+    p.nim1 = p.ni - 1; p.njm1 = p.nj - 1; p.nkm1 = p.nk - 1;
+    p.nim2 = p.ni - 2; p.njm2 = p.nj - 2; p.nkm2 = p.nk - 2;
+    p.dens = q.dens; p.denl = q.denl; p.viscos = q.viscos; p.tsolid = q.tsolid;
+    p.tliquid = q.tliquid; p.hsmelt = q.hsmelt; p.hlcal = ctx->hlcal; p.hlatnt = ctx->hlatnt;
+    p.acpa = q.acpa; p.acpb = q.acpb; p.acpl = q.acpl;
+    p.thconsa = q.thconsa; p.thconsb = q.thconsb; p.thconsc = q.thconsc;
+    p.thconla = q.thconla; p.thconlb = q.thconlb;
+    p.urfu = q.urfu; p.urfv = q.urfv; p.urfw = q.urfw; p.urfp = q.urfp; p.urfh = q.urfh;
+    p.htci = q.htci; p.htcj = q.htcj; p.htckn = q.htckn; p.emiss = q.emiss; p.sigm = q.sigm;
+    p.tempamb = q.tempamb; p.beta = q.beta; p.grav = q.grav; p.dgdtp = q.dgdtp;
+    p.darcyKo = q.darcyKo; p.a_oxygen = q.a_oxygen;
+    p.alaspow = q.alaspow; p.alaseta = q.alaseta; p.alasrb = q.alasrb; p.alasfact = q.alasfact;
+    p.pressamb = q.pressamb; p.gasconst = q.gasconst; p.evaplatent = q.evaplatent;
+    p.evaptemp = q.evaptemp; p.evapfact = q.evapfact; p.molarmass = q.molarmass;
+    p.isevap = q.isevap; p.scheme = q.scheme; p.steady = q.steady; p.navierstokes = q.navierstokes;
+    p.nheattable = q.nheattable;
+    p.volsrc = (q.nheattable > 0 || q.heatthick > 0.0) ? 1 : 0;
+    p.avolpow = q.avolpow; p.apowseta = q.apowseta; p.heatthick = q.heatthick;
+    p.heatrb = q.heatrb; p.avolfact = q.avolfact;
+
+    const size_t n3 = (size_t)p.nk * p.nj * p.nip;
+    Fields<T> &g = I.g;
+    memset(&g, 0, sizeof(g));
+    int rc;
+    double *m1[12];
+    const std::vector<double> *src1[12] = {&ctx->x, &ctx->y, &ctx->z, &ctx->xu, &ctx->yv, &ctx->zw,
+                                           &ctx->dxpwinv, &ctx->dypsinv, &ctx->dzpbinv,
+                                           &ctx->fracx, &ctx->fracy, &ctx->fracz};
+    for (int a = 0; a < 12; a++) {
+        if ((rc = alloc3<double>(ctx, &m1[a], src1[a]->size()))) return rc;
+        if ((rc = upload<double>(ctx, m1[a], *src1[a]))) return rc;
+    }
+    g.x = m1[0]; g.y = m1[1]; g.z = m1[2]; g.xu = m1[3]; g.yv = m1[4]; g.zw = m1[5];
+    g.dxpwinv = m1[6]; g.dypsinv = m1[7]; g.dzpbinv = m1[8]; g.fracx = m1[9]; g.fracy = m1[10];
+    g.fracz = m1[11];
+    T **f3[] = {&g.uvel, &g.vvel, &g.wvel, &g.unot, &g.vnot, &g.wnot, &g.pressure, &g.pp,
+                &g.h, &g.hnot, &g.temp, &g.fracl, &g.fraclnot, &g.sourceinput,
+                &g.diff_cur, &g.rho_cur, &g.vis_cur, &g.diff_nxt, &g.rho_nxt, &g.vis_nxt,
+                &g.an, &g.as, &g.ae, &g.aw, &g.at, &g.ab, &g.ap, &g.su, &g.pr, &g.cf, &g.iden,
+                &g.dux, &g.dvy, &g.dwz};
+    for (auto f : f3)
+        if ((rc = alloc3<T>(ctx, f, n3))) return rc;
+    if ((rc = alloc3<double>(ctx, &g.heatin, (size_t)p.nj * p.nip))) return rc;
+    if (q.nheattable > 0) {
+        if ((rc = alloc3<double>(ctx, &g.heattable, ctx->heattable.size()))) return rc;
+        if ((rc = upload<double>(ctx, g.heattable, ctx->heattable))) return rc;
+    }
+    // reduction regions
+    I.sm_count = 148;
+    cudaDeviceGetAttribute(&I.sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+    I.stream = ctx->stream;
+    I.order = ctx->order;
+    I.nb_las = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 255) / 256));
+    I.nb_bc = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 2 * p.nk * (p.ni + p.nj) + 255) / 256));
+    I.asm_grid = dim3((p.ni + 31) / 32, (p.nj + 7) / 8, (p.nk + 3) / 4);
+    I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
+    I.nb_h2t = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
+    I.nb_mom = I.sm_count * 2;
+    I.grid_1d = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
+    double *red;
+    size_t nred = (size_t)(I.nb_las + I.nb_bc + I.nb_asm + I.nb_h2t + 5 * I.nb_mom) * R_NSLOTS;
+    if ((rc = alloc3<double>(ctx, &red, nred))) return rc;
+    I.red_las = red;
+    I.red_bc = I.red_las + (size_t)I.nb_las * R_NSLOTS;
+    I.red_asm = I.red_bc + (size_t)I.nb_bc * R_NSLOTS;
+    I.red_h2t = I.red_asm + (size_t)I.nb_asm * R_NSLOTS;
+    I.red_mom = I.red_h2t + (size_t)I.nb_h2t * R_NSLOTS;
+    g.red = red;
+    g.npart = I.asm_grid.y * I.asm_grid.z;
+    if ((rc = alloc3<double>(ctx, &g.bc, (size_t)g.npart * 4 * p.nip))) return rc;
+    if ((rc = alloc3<double>(ctx, &g.delphi, (size_t)p.nip))) return rc;
+    // exact-order scheduling
+    I.max_lines = (p.nj - 2) * (p.nk - 2);
+    if ((rc = alloc3<int>(ctx, &g.flags, (size_t)p.nk * p.nj))) return rc;
+    if ((rc = alloc3<int>(ctx, &I.flags_mom, (size_t)p.nk * p.nj))) return rc;
+    {
+        // (t, m, s) order of the visits (ks, k, s, j) of solveEntireDomain
+        const int M = p.nk - 2, J = p.nj - 2;
+        std::vector<int2> tk;
+        tk.reserve((size_t)4 * M * J);
+        const int Tw = 3 * (2 * M - 1) + (J - 1) + 2 + 1;
+        for (int t = 0; t < Tw; ++t)
+            for (int m = std::max(0, (t - 2 - (J - 1)) / 3 - 1); m <= std::min(2 * M - 1, t / 3); ++m)
+                for (int s = 0; s < 2; ++s) {
+                    int jj = t - 3 * m - 2 * s;
+                    if (jj >= 0 && jj < J) tk.push_back(make_int2(m, (s << 16) | jj));
+                }
+        if (tk.size() != (size_t)4 * M * J) return fail(ctx, AMCFD_E_ARG, "ticket enumeration mismatch");
+        int2 *d;
+        if ((rc = alloc3<int2>(ctx, &d, tk.size()))) return rc;
+        CK(cudaMemcpy(d, tk.data(), tk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+        g.tickets_energy = d;
+        g.ntickets_energy = (int)tk.size();
+        if ((rc = alloc3<int2>(ctx, &g.tickets_mom, tk.size()))) return rc;
+        if ((rc = alloc3<int>(ctx, &g.ntickets_mom, 1))) return rc;
+    }
+    g.st = ctx->st_dev;
+    I.check_finite = 0;
+    I.exact_warps = 4;
+    I.line_smem = (size_t)I.exact_warps * 3 * p.nip * sizeof(T);
+    set_sweep_smem_limit<T>(I.line_smem);
+    int bps = exact_sweep_blocks_per_sm<T>(I.exact_warps, I.line_smem);
+    I.exact_grid = std::max(1, I.sm_count * bps);
+
+    // initializeSolver (CFDSolverManager.cpp:402-525)
+    std::vector<double> hv(n3, 0.0);
+    auto enth = [&](double t) { return 0.5 * q.acpa * t * t + q.acpb * t; };
+    const double hpre = enth(q.temppreheat);
+    const double diff0 = (q.thconsa * q.temppreheat * q.temppreheat + q.thconsb * q.temppreheat +
+                          q.thconsc) / (q.acpa * q.temppreheat + q.acpb);
+    auto fill = [&](T *dst, double v) {
+        std::vector<double> a(n3, v);
+        return upload<T>(ctx, dst, a);
+    };
+    if ((rc = fill(g.vis_cur, q.viscos)) || (rc = fill(g.rho_cur, q.dens)) ||
+        (rc = fill(g.diff_cur, diff0)) || (rc = fill(g.hnot, hpre)) ||
+        (rc = fill(g.temp, q.temppreheat)))
+        return rc;
+    for (int k = 0; k < p.nk; k++)
+        for (int j = 0; j < p.nj; j++)
+            for (int i = 0; i < p.ni; i++) hv[cidx(i, j, k, p.nj, p.nip)] = hpre;
+    for (int k = 0; k < p.nk; k++)
+        for (int j = 0; j < p.nj; j++) {
+            hv[cidx(0, j, k, p.nj, p.nip)] = enth(q.tempwest);
+            hv[cidx(p.nim1, j, k, p.nj, p.nip)] = enth(q.tempeast);
+        }
+    for (int j = 0; j < p.nj; j++)
+        for (int i = 0; i < p.ni; i++) hv[cidx(i, j, 0, p.nj, p.nip)] = enth(q.tempbottom);
+    for (int k = 0; k < p.nk; k++)
+        for (int i = 0; i < p.ni; i++) hv[cidx(i, p.njm1, k, p.nj, p.nip)] = enth(q.tempnorth);
+    if ((rc = upload<T>(ctx, g.h, hv))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+static bool phase_ok(int phase) { return phase >= 1 && phase <= 8; }
+
+// ---- one outer iteration -----------------------------------------------------------------
+template <typename T>
+static void swap_props(Inst<T> &I)
+{
+    std::swap(I.g.diff_cur, I.g.diff_nxt);
+    std::swap(I.g.rho_cur, I.g.rho_nxt);
+    std::swap(I.g.vis_cur, I.g.vis_nxt);
+}
+
+template <typename T>
+static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
+{
+    switch (phase) {
+    case AMCFD_PHASE_ENERGY_ASSEMBLE:
+        launch_energy_bc<T>(I);
+        launch_energy_assemble<T>(I);
+        launch_block_correct<T>(I);
+        break;
+    case AMCFD_PHASE_ENERGY_SOLVE:
+        launch_energy_factor<T>(I);
+        launch_energy_sweeps<T>(I);
+        break;
+    case AMCFD_PHASE_H2T: launch_h2t<T>(I); break;
+    case AMCFD_PHASE_MELTPOOL: launch_meltpool<T>(I); break;
+    case AMCFD_PHASE_MOMENTUM: launch_momentum<T>(I); break;
+    case AMCFD_PHASE_CONVERGE:
+        launch_converge<T>(I, ctx->prm.nonlintol);
+        swap_props<T>(I);
+        break;
+    case AMCFD_PHASE_UPDATE: launch_update_solutions<T>(I); break;
+    default: break;
+    }
+}
+
+static int begin_step(amcfd_ctx *ctx)
+{
+    const amcfd_params &p = ctx->prm;
+    if (p.nvardt > 0) {
+        const int n = p.nvardt;
+        if (ctx->timet > ctx->vardt[3 * ctx->vardt_state] && ctx->vardt_state < n - 1)
+            ctx->vardt_state += 1;
+        ctx->delt = ctx->vardt[3 * ctx->vardt_state + 1];
+        ctx->outtime = ctx->vardt[3 * ctx->vardt_state + 2];
+    }
+    ctx->timet += ctx->delt;
+    if (!p.steady) laser_coords(ctx);
+    Status *h = ctx->st_host;
+    h->timet = ctx->timet;
+    h->delt = ctx->delt;
+    h->beamposx = ctx->beamposx;
+    h->beamposy = ctx->beamposy;
+    h->scanvel = ctx->scanvel;
+    h->powerindicator = ctx->powerindicator;
+    h->istart = ctx->istart;
+    h->jstart = ctx->jstart;
+    // the per-step block is the leading members of Status, up to heat_iter
+    CK(cudaMemcpyAsync(ctx->st_dev, h, offsetof(Status, heat_iter), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    if (ctx->precision == AMCFD_PREC_FP64)
+        launch_laser<double>(ctx->I64);
+    else
+        launch_laser<float>(ctx->I32);
+    ctx->niter = 0;
+    return 0;
+}
+
+static int read_status(amcfd_ctx *ctx)
+{
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st_dev, sizeof(Status), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    const Status *s = ctx->st_host;
+    if (s->error) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "device wait gave up (code %d, line %d)", s->error, s->error_where);
+        ctx->err = buf;
+        return s->error;
+    }
+    if (s->nonfinite) return fail(ctx, AMCFD_E_NONFINITE, "non-finite residual or temperature");
+    return 0;
+}
+
+template <typename T>
+static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
+{
+    const int maxit = ctx->prm.maxit;
+    int rc;
+    while (ctx->niter < maxit) {
+        ctx->niter++;
+        ctx->itertot++;
+        if (ctx->events) cudaEventRecord(ctx->ev[0], ctx->stream);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_ASSEMBLE);
+        if (ctx->events) cudaEventRecord(ctx->ev[1], ctx->stream);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_SOLVE);
+        if (ctx->events) cudaEventRecord(ctx->ev[2], ctx->stream);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
+        if (ctx->events) cudaEventRecord(ctx->ev[3], ctx->stream);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_MOMENTUM);
+        if (ctx->events) cudaEventRecord(ctx->ev[4], ctx->stream);
+        run_phase_impl<T>(ctx, I, AMCFD_PHASE_CONVERGE);
+        if (ctx->events) cudaEventRecord(ctx->ev[5], ctx->stream);
+        if ((rc = read_status(ctx))) return rc;
+        if (ctx->events) {
+            for (int q = 0; q < 5; q++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ctx->ev[q], ctx->ev[q + 1]);
+                ctx->last_ms[q] += ms;
+            }
+        }
+        if (ctx->st_host->converged) break;
+    }
+    return 0;
+}
+
+static void fill_report(amcfd_ctx *ctx, amcfd_step_report *r)
+{
+    if (!r) return;
+    const Status *s = ctx->st_host;
+    memset(r, 0, sizeof(*r));
+    r->timet = ctx->timet;
+    r->niter = ctx->niter;
+    r->itertot = ctx->itertot;
+    r->resorh = s->resorh; r->resorm = s->resorm; r->resoru = s->resoru;
+    r->resorv = s->resorv; r->resorw = s->resorw;
+    r->tpeak = s->tpeak; r->alen = s->alen; r->depth = s->depth; r->width = s->width;
+    r->ratio = s->ratio; r->heatinlaser = s->heatinlaser; r->ahtoploss = s->ahtoploss;
+    r->accul = s->accul; r->heatout = s->heatout; r->heatvol = s->heatvol;
+    r->beamposx = ctx->beamposx; r->beamposy = ctx->beamposy; r->scanvel = ctx->scanvel;
+    r->istat = s->istat; r->iend = s->iend; r->jstat = s->jstat; r->jend = s->jend;
+    r->kstat = s->kstat; r->jstart = ctx->jstart; r->powerindicator = ctx->powerindicator;
+    r->momentum_cells = s->box_cells;
+}
+
+// =========================================================================================
+extern "C" {
+
+int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ctx **out)
+{
+    if (!params || !out) return AMCFD_E_ARG;
+    *out = nullptr;
+    amcfd_ctx *ctx = new amcfd_ctx();
+    *out = ctx;
+    ctx->prm = *params;
+    amcfd_params &p = ctx->prm;
+    if (p.powderbed || p.movingmesh || p.species || p.freesurface)
+        return fail(ctx, AMCFD_E_ARG,
+                    "powder-bed mode, moving mesh, species and free surface are not implemented");
+    if (p.nzx < 1 || p.nzy < 1 || p.nzz < 1 || p.nzx > AMCFD_MAX_ZONES || p.nzy > AMCFD_MAX_ZONES ||
+        p.nzz > AMCFD_MAX_ZONES)
+        return fail(ctx, AMCFD_E_ARG, "bad zone counts");
+    if (p.acpa == 0.0) return fail(ctx, AMCFD_E_ARG, "acpa must be non-zero (H->T divides by it)");
+    if (opts) {
+        ctx->device = opts->device;
+        ctx->order = opts->order;
+        ctx->precision = opts->precision;
+    }
+    if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
+        return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");
+    if (ctx->precision != AMCFD_PREC_FP64 && ctx->precision != AMCFD_PREC_FP32)
+        return fail(ctx, AMCFD_E_ARG, "unknown precision");
+    if (p.udtoolpath) {
+        if (p.ntool < 2 || !p.tool_txyz || !p.tool_on || !p.tool_id)
+            return fail(ctx, AMCFD_E_ARG, "toolpath needs at least 2 rows");
+        ctx->tool.assign(p.tool_txyz, p.tool_txyz + 4 * p.ntool);
+        ctx->tool_on.assign(p.tool_on, p.tool_on + p.ntool);
+        ctx->tool_id.assign(p.tool_id, p.tool_id + p.ntool);
+    }
+    if (p.nheattable > 0) ctx->heattable.assign(p.heattable, p.heattable + 6 * p.nheattable);
+    if (p.nvardt > 0) ctx->vardt.assign(p.vardt, p.vardt + 3 * p.nvardt);
+    p.tool_txyz = nullptr; p.tool_on = nullptr; p.tool_id = nullptr;
+    p.heattable = nullptr; p.vardt = nullptr;
+    int sx = 0, sy = 0, sz = 0;
+    for (int q = 0; q < p.nzx; q++) sx += (int)p.ncvx[q];
+    for (int q = 0; q < p.nzy; q++) sy += (int)p.ncvy[q];
+    for (int q = 0; q < p.nzz; q++) sz += (int)p.ncvz[q];
+    ctx->ni = sx + 2; ctx->nj = sy + 2; ctx->nk = sz + 2;
+    if (sx < 1 || sy < 1 || sz < 1) return fail(ctx, AMCFD_E_ARG, "empty grid");
+    if (ctx->nj > 65535) return fail(ctx, AMCFD_E_CAPACITY, "nj above 65535");
+    ctx->nip = (ctx->ni + 31) / 32 * 32;
+    double cpavg = (p.acpa * p.tsolid + p.acpb + p.acpl) * 0.5;
+    ctx->hlcal = p.hsmelt + cpavg * (p.tliquid - p.tsolid);
+    ctx->hlatnt = p.hlfriz - ctx->hlcal;
+    ctx->delt = p.nvardt > 0 ? ctx->vardt[1] : p.delt;
+    ctx->outtime = p.nvardt > 0 ? ctx->vardt[2] : p.outtime;
+    ctx->scanvel = p.scanvel;
+    build_grid(ctx);
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaMalloc(&ctx->st_dev, sizeof(Status)));
+    CK(cudaMemset(ctx->st_dev, 0, sizeof(Status)));
+    CK(cudaMallocHost(&ctx->st_host, sizeof(Status)));
+    memset(ctx->st_host, 0, sizeof(Status));
+    {
+        // initial volumetric-source parameters and the status block defaults
+        Status s;
+        memset(&s, 0, sizeof(s));
+        s.avolpow = p.avolpow; s.apowseta = p.apowseta; s.heatthick = p.heatthick;
+        s.heatrb = p.heatrb; s.avolfact = p.avolfact;
+        s.delt = ctx->delt;
+        CK(cudaMemcpy(ctx->st_dev, &s, sizeof(s), cudaMemcpyHostToDevice));
+    }
+    for (int q = 0; q < 16; q++) CK(cudaEventCreate(&ctx->ev[q]));
+    int rc = ctx->precision == AMCFD_PREC_FP64 ? setup_instance<double>(ctx, ctx->I64)
+                                               : setup_instance<float>(ctx, ctx->I32);
+    if (rc) return rc;
+    int cf = opts ? opts->check_finite : 0;
+    ctx->I64.check_finite = cf;
+    ctx->I32.check_finite = cf;
+    if (p.steady) laser_coords(ctx);  // main.cpp:105-106
+    return 0;
+}
+
+void amcfd_destroy(amcfd_ctx *ctx)
+{
+    if (!ctx) return;
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (void *p : ctx->allocs) cudaFree(p);
+    if (ctx->st_dev) cudaFree(ctx->st_dev);
+    if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    for (int q = 0; q < 16; q++)
+        if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char *amcfd_last_error(const amcfd_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int amcfd_dims(const amcfd_ctx *ctx, int *ni, int *nj, int *nk)
+{
+    if (!ctx || !ni || !nj || !nk) return AMCFD_E_ARG;
+    *ni = ctx->ni; *nj = ctx->nj; *nk = ctx->nk;
+    return 0;
+}
+
+int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = begin_step(ctx);
+    if (rc) return rc;
+    rc = ctx->precision == AMCFD_PREC_FP64 ? outer_loop<double>(ctx, ctx->I64)
+                                           : outer_loop<float>(ctx, ctx->I32);
+    if (rc) return rc;
+    if (!ctx->prm.steady) {
+        if (ctx->precision == AMCFD_PREC_FP64)
+            launch_update_solutions<double>(ctx->I64);
+        else
+            launch_update_solutions<float>(ctx->I32);
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    fill_report(ctx, report);
+    return 0;
+}
+
+int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    if (phase == 0) return 0;
+    if (!phase_ok(phase)) return fail(ctx, AMCFD_E_ARG, "unknown phase");
+    CK(cudaSetDevice(ctx->device));
+    int rc;
+    if (phase == AMCFD_PHASE_LASER) {
+        if ((rc = begin_step(ctx))) return rc;
+    } else {
+        if (phase == AMCFD_PHASE_ENERGY_ASSEMBLE) {
+            ctx->niter++;
+            ctx->itertot++;
+        }
+        if (ctx->precision == AMCFD_PREC_FP64)
+            run_phase_impl<double>(ctx, ctx->I64, phase);
+        else
+            run_phase_impl<float>(ctx, ctx->I32, phase);
+    }
+    if ((rc = read_status(ctx))) return rc;
+    fill_report(ctx, report);
+    return 0;
+}
+
+const char *amcfd_phase_name(int phase)
+{
+    static const char *names[] = {"none", "laser", "energy_assemble", "energy_solve", "h2t",
+                                  "meltpool", "momentum", "converge", "update"};
+    return phase_ok(phase) ? names[phase] : "unknown";
+}
+
+static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
+{
+    struct E { const char *n; size_t off; };
+#define F(x) {#x, offsetof(Fields<double>, x)}
+    static const E tab[] = {
+        {"temp", offsetof(Fields<double>, temp)}, {"uvel", offsetof(Fields<double>, uvel)},
+        {"vvel", offsetof(Fields<double>, vvel)}, {"wvel", offsetof(Fields<double>, wvel)},
+        {"pressure", offsetof(Fields<double>, pressure)}, F(pp),
+        {"enthalpy", offsetof(Fields<double>, h)}, F(fracl), F(fraclnot), F(hnot),
+        {"diff", offsetof(Fields<double>, diff_cur)}, {"rho", offsetof(Fields<double>, rho_cur)},
+        {"vis", offsetof(Fields<double>, vis_cur)}, {"diff_next", offsetof(Fields<double>, diff_nxt)},
+        {"rho_next", offsetof(Fields<double>, rho_nxt)}, {"vis_next", offsetof(Fields<double>, vis_nxt)},
+        F(sourceinput), F(unot), F(vnot), F(wnot), F(an), F(as), F(ae), F(aw), F(at), F(ab),
+        F(ap), F(su), F(dux), F(dvy), F(dwz)};
+#undef F
+    // Fields<float> has the same member layout of pointers
+    const char *base = ctx->precision == AMCFD_PREC_FP64 ? (const char *)&ctx->I64.g
+                                                         : (const char *)&ctx->I32.g;
+    for (const E &e : tab)
+        if (!strcmp(e.n, name)) {
+            *ptr = *(void *const *)(base + e.off);
+            return 0;
+        }
+    return fail(ctx, AMCFD_E_ARG, std::string("unknown field ") + name);
+}
+
+int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
+{
+    if (!ctx || !name || !host_out) return AMCFD_E_ARG;
+    void *d;
+    int rc;
+    if ((rc = field_ptr(ctx, name, &d))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t rows = (size_t)ctx->nj * ctx->nk;
+    if (ctx->precision == AMCFD_PREC_FP64) {
+        CK(cudaMemcpy2D(host_out, ctx->ni * sizeof(double), d, ctx->nip * sizeof(double),
+                        ctx->ni * sizeof(double), rows, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp((size_t)ctx->ni * rows);
+        CK(cudaMemcpy2D(tmp.data(), ctx->ni * sizeof(float), d, ctx->nip * sizeof(float),
+                        ctx->ni * sizeof(float), rows, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < tmp.size(); q++) host_out[q] = tmp[q];
+    }
+    return 0;
+}
+
+int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in)
+{
+    if (!ctx || !name || !host_in) return AMCFD_E_ARG;
+    void *d;
+    int rc;
+    if ((rc = field_ptr(ctx, name, &d))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t rows = (size_t)ctx->nj * ctx->nk;
+    if (ctx->precision == AMCFD_PREC_FP64) {
+        CK(cudaMemcpy2D(d, ctx->nip * sizeof(double), host_in, ctx->ni * sizeof(double),
+                        ctx->ni * sizeof(double), rows, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> tmp(host_in, host_in + (size_t)ctx->ni * rows);
+        CK(cudaMemcpy2D(d, ctx->nip * sizeof(float), tmp.data(), ctx->ni * sizeof(float),
+                        ctx->ni * sizeof(float), rows, cudaMemcpyHostToDevice));
+    }
+    return 0;
+}
+
+int amcfd_get_grid(amcfd_ctx *ctx, const char *name, double *host_out)
+{
+    if (!ctx || !name || !host_out) return AMCFD_E_ARG;
+    const std::vector<double> *v = !strcmp(name, "x") ? &ctx->x : !strcmp(name, "y") ? &ctx->y
+                                 : !strcmp(name, "z") ? &ctx->z : !strcmp(name, "xu") ? &ctx->xu
+                                 : !strcmp(name, "yv") ? &ctx->yv : !strcmp(name, "zw") ? &ctx->zw
+                                 : nullptr;
+    if (!v) return fail(ctx, AMCFD_E_ARG, std::string("unknown grid array ") + name);
+    int n = name[0] == 'x' ? ctx->ni : name[0] == 'y' ? ctx->nj : ctx->nk;
+    memcpy(host_out, v->data(), n * sizeof(double));
+    return 0;
+}
+
+int amcfd_last_timing(const amcfd_ctx *ctx, double *ms, int n)
+{
+    if (!ctx || !ms) return AMCFD_E_ARG;
+    for (int q = 0; q < n && q < 16; q++) ms[q] = ctx->last_ms[q];
+    return 0;
+}
+
+// Per-phase device timing: enable (1) / disable (0) and clear the accumulators.
+int amcfd_profile(amcfd_ctx *ctx, int enable)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    ctx->events = enable != 0;
+    for (int q = 0; q < 16; q++) ctx->last_ms[q] = 0.0;
+    return 0;
+}
+
+}  // extern "C"

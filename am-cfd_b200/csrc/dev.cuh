@@ -1,0 +1,177 @@
+// Device-side data layout and helpers shared by the solver kernels.
+//
+// Layout: every 3-D field is a structure-of-arrays buffer indexed
+// (k*nj + j)*nip + i, i fastest, with the i-pitch nip padded to a multiple of
+// 32 elements so that every x-line starts on a 256-byte boundary (FP64).
+// The reference uses the same [k][j][i] order with an unpadded pitch
+// (CFDSolverManager.cpp:249).  Geometry is kept as 1-D FP64 metrics; volumes
+// and face areas are recomputed in the kernels with the reference's own
+// products (CFDSolverManager.cpp:243-286), so they are bit-identical to the
+// reference arrays.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace amcfd {
+
+constexpr double kSmall = 1.0e-6;  // CFDSolverManager.h:143
+constexpr double kLarge = 1.0e20;  // CFDSolverManager.h:144
+
+// std::max / std::min with the reference's NaN behaviour.
+__host__ __device__ __forceinline__ double maxd(double a, double b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ double mind(double a, double b) { return (b < a) ? b : a; }
+__host__ __device__ __forceinline__ float maxd(float a, float b) { return (a < b) ? b : a; }
+__host__ __device__ __forceinline__ float mind(float a, float b) { return (b < a) ? b : a; }
+
+// Scalar parameters of one instance (DomainManager/Mesh fields read by the hot path).
+struct Params {
+    int ni, nj, nk, nip;
+    int nim1, njm1, nkm1, nim2, njm2, nkm2;
+    double dens, denl, viscos, tsolid, tliquid, hsmelt, hlcal, hlatnt, acpa, acpb, acpl;
+    double thconsa, thconsb, thconsc, thconla, thconlb;
+    double urfu, urfv, urfw, urfp, urfh;
+    double htci, htcj, htckn, emiss, sigm, tempamb;
+    double beta, grav, dgdtp, darcyKo, a_oxygen;
+    double alaspow, alaseta, alasrb, alasfact;
+    double pressamb, gasconst, evaplatent, evaptemp, evapfact, molarmass;
+    int isevap, scheme, steady, navierstokes;
+    int nheattable;
+    int volsrc;  // a volumetric source is configured (scalar form with heatthick > 0, or a table)
+    double avolpow, apowseta, heatthick, heatrb, avolfact;  // scalar volumetric source
+};
+
+// Device status block: per-step inputs written by the host, per-iteration
+// results written by the kernels (reductions are FP64).
+struct Status {
+    // per step
+    double timet, delt, beamposx, beamposy, scanvel;
+    int powerindicator, istart, jstart, heat_iter;
+    double heatinlaser;
+    // current volumetric-source parameters (advanced per outer iteration)
+    double avolpow, apowseta, heatthick, heatrb, avolfact;
+    // per outer iteration
+    double ahtoploss, resorh, tpeak, alen, depth, width, ratio, accul, heatvol, heatout;
+    double fluxwest, fluxeast, fluxtop, fluxbottom, fluxnorth, fluxsouth;
+    double resoru, resorv, resorw, resorm, refmom, umaxt, mass_denom;
+    int istat, iend, jstat, jend, kstat, istatp1, iendm1;
+    int imin, imax, jmin, jmax, kmin, kmax;
+    int momentum_active, box_cells;
+    int niter, itertot, converged;
+    int error;         // 0, or an AMCFD_E_* code set by a kernel
+    int error_where;   // kernel-specific detail (e.g. the line that timed out)
+    int nonfinite;     // a reduction produced NaN/Inf
+    unsigned long long seq_energy, done_energy, ticket_energy;
+    unsigned long long seq_mom, done_mom, ticket_mom;
+};
+
+// Fixed-size reduction slots written per CTA and reduced in a fixed order.
+enum RedSlot {
+    R_SUMD = 0, R_SUMH, R_AHTOP, R_ACCUL, R_HEATVOL, R_FW, R_FE, R_FB, R_FT, R_FS, R_FN,
+    R_HEATIN, R_MSUMD, R_MDENOM, R_MRESORM, R_UMAX, R_TPEAK, R_NSLOTS
+};
+
+template <typename T>
+struct Fields {
+    // 1-D metrics (FP64)
+    const double *x, *y, *z, *xu, *yv, *zw, *dxpwinv, *dypsinv, *dzpbinv, *fracx, *fracy, *fracz;
+    // 3-D fields
+    T *uvel, *vvel, *wvel, *unot, *vnot, *wnot, *pressure, *pp;
+    T *h, *hnot, *temp, *fracl, *fraclnot, *sourceinput;
+    T *diff_cur, *rho_cur, *vis_cur, *diff_nxt, *rho_nxt, *vis_nxt;
+    // coefficients (shared by all equations, as in the reference)
+    T *an, *as, *ae, *aw, *at, *ab, *ap, *su, *apnot, *sp;
+    // pass-invariant line factorisation: pr = ae/den, cf = aw/den, iden = 1/den
+    T *pr, *cf, *iden;
+    T *dux, *dvy, *dwz;
+    double *heatin;     // nj*nip, Gaussian surface flux of the current step
+    double *heattable;  // nheattable x 6
+    // reductions
+    double *red;        // [nblocks][R_NSLOTS] per-CTA partials
+    double *bc;         // block correction: [npart][4][nip] per-CTA partial sums
+    double *delphi;     // nip
+    int npart;          // number of block-correction partial rows
+    // exact-order line sweep scheduling
+    int *flags;         // (nk*nj) per-line visit counters (monotone across calls)
+    int2 *tickets_energy;  // precomputed topological order of the energy visits
+    int ntickets_energy;
+    int2 *tickets_mom;     // regenerated on the device for each momentum box
+    int *ntickets_mom;
+    Status *st;
+};
+
+__host__ __device__ __forceinline__ size_t cidx(int i, int j, int k, int nj, int nip)
+{
+    return ((size_t)k * nj + j) * (size_t)nip + i;
+}
+
+// Discretisation scheme A(|Pe|) (CFDSolverManager.cpp:3071-3101).
+template <typename R>
+__device__ __forceinline__ R scheme_fn(int scheme, R pe)
+{
+    if (scheme == 1) {
+        R base = R(1) - R(0.1) * pe;
+        R out = base;
+#pragma unroll
+        for (int q = 1; q < 5; q++) out *= base;
+        return maxd(R(0), out);
+    }
+    if (scheme == 2) return pe / (exp(pe) - R(1));
+    return R(1);
+}
+
+// a_nb pair for one face: plus = D*A(|F|/D) + max(0,-F), minus = D*A(|F|/D) + max(0,F).
+template <typename R>
+__device__ __forceinline__ void face_coef(int scheme, R d, R f, R &plus, R &minus)
+{
+    R a = d * scheme_fn<R>(scheme, fabs(f) / d);
+    plus = a + maxd(R(0), -f);
+    minus = a + maxd(R(0), f);
+}
+
+// Warp sum / max of doubles with a fixed shuffle tree (deterministic).
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block reduction of up to 8 values into red[blk*R_NSLOTS + slot[q]] (sum or max).
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], const int (&slot)[NV],
+                                                   const bool (&is_max)[NV], double *red,
+                                                   int blk)
+{
+    __shared__ double sh[32][NV];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31;
+    const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+    const int warp = tid >> 5, nwarps = (nthreads + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; q++) v[q] = is_max[q] ? warp_max(v[q]) : warp_sum(v[q]);
+    if ((tid & 31) == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) sh[warp][q] = v[q];
+    }
+    __syncthreads();
+    if (tid < 32) {
+#pragma unroll
+        for (int q = 0; q < NV; q++) {
+            double x = (lane < nwarps) ? sh[lane][q] : (is_max[q] ? -INFINITY : 0.0);
+            x = is_max[q] ? warp_max(x) : warp_sum(x);
+            if (lane == 0) red[(size_t)blk * R_NSLOTS + slot[q]] = x;
+        }
+    }
+    (void)tid;
+}
+
+// Bounded spin budget for every device-side wait (about one second).
+constexpr long long kSpinLimit = 1ll << 24;
+
+}  // namespace amcfd

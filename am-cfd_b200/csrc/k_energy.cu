@@ -1,0 +1,758 @@
+// Energy-equation kernels of one SIMPLE outer iteration, plus the per-step
+// laser and push-back kernels.  Each kernel names the reference routine it
+// replaces; arithmetic follows the reference expression by expression so that
+// the FP64 build matches the CPU solve to rounding.
+#include "kernels.cuh"
+
+namespace amcfd {
+
+// ---------------------------------------------------------------------------
+// updateLaser heat flux (BoundCondManager.cpp:128-159): Gaussian surface flux
+// heatin[j][i] and the partial sums of areaij*heatin (heatinlaser).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void laser_kernel(Params p, Fields<T> g, double *red)
+{
+    const Status *st = g.st;
+    double acc = 0.0;
+    const double rb2 = p.alasrb * p.alasrb;
+    const double varlas = p.alaspow * p.alaseta;
+    const double peakhin = p.alasfact * varlas / (M_PI * rb2);
+    const double pw = (double)st->powerindicator;
+    const int n = p.ni * p.nj;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        int j = q / p.ni, i = q - j * p.ni;
+        double ydist = st->beamposy - g.y[j];
+        double xdist = st->beamposx - g.x[i];
+        double dist2 = (xdist * xdist) + (ydist * ydist);
+        double hin = peakhin * exp(-p.alasfact * dist2 / rb2) * pw;
+        if (p.alasfact < 1.0e-6 && dist2 < rb2) hin = varlas / (M_PI * rb2) * pw;
+        g.heatin[(size_t)j * p.nip + i] = hin;
+        acc += area_ij(p, g, i, j) * hin;
+    }
+    double v[1] = {acc};
+    const int s[1] = {R_HEATIN};
+    const bool m[1] = {false};
+    block_reduce_store<1>(v, s, m, red, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// applyBCs(5) (BoundCondManager.cpp:565-654): top-surface flux balance and
+// convective side planes.  Also advances the volumetric heat-source table the
+// way calculateSource(5) does at the start of each outer iteration
+// (CFDSolverManager.cpp:1707-1717).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void energy_bc_kernel(Params p, Fields<T> g, double *red)
+{
+    Status *st = g.st;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (p.nheattable > 0) {
+            int it = st->heat_iter;
+            if (st->timet > g.heattable[6 * it] && it < p.nheattable - 1) it += 1;
+            st->heat_iter = it;
+            const double *row = &g.heattable[6 * it];
+            st->avolpow = row[1];
+            st->apowseta = row[2];
+            st->heatthick = row[3];
+            st->heatrb = row[4];
+            st->avolfact = row[5];
+        }
+    }
+    const int ni = p.ni, nj = p.nj, nip = p.nip;
+    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
+              nkm2 = p.nkm2;
+    const int ntop = (nim1 - 1) * (njm1 - 1);
+    const int new_ = (nkm1 - 1) * (njm1 - 1);
+    const int nns = (nkm1 - 1) * (nim1 - 1);
+    double ahtop = 0.0;
+    double a4 = p.tempamb;
+    for (int q = 1; q < 4; q++) a4 *= p.tempamb;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ntop + new_ + nns;
+         q += gridDim.x * blockDim.x) {
+        if (q < ntop) {
+            int j = 1 + q / (nim1 - 1), i = 1 + q % (nim1 - 1);
+            double t = (double)g.temp[cidx(i, j, nkm1, nj, nip)];
+            double hlossevap = 0.0;
+            if (p.isevap) {
+                double psat = p.pressamb * exp(-p.evaplatent * p.molarmass / p.gasconst *
+                                               (1.0 / t - 1.0 / p.evaptemp));
+                double mdot = p.evapfact * psat * sqrt(p.molarmass / (2.0 * M_PI * p.gasconst * t));
+                hlossevap = mdot * p.evaplatent;
+            }
+            double t4 = t;
+            for (int r = 1; r < 4; r++) t4 *= t;
+            double hlossradia = p.emiss * p.sigm * (t4 - a4);
+            double ctmp1 = (double)g.diff_cur[cidx(i, j, nkm2, nj, nip)] * g.dzpbinv[nkm1];
+            double hb = (double)g.h[cidx(i, j, nkm2, nj, nip)];
+            g.h[cidx(i, j, nkm1, nj, nip)] =
+                (T)(hb + (g.heatin[(size_t)j * nip + i] - hlossradia - hlossradia - hlossevap) / ctmp1);
+            ahtop += (hlossradia + hlossradia + hlossevap) * area_ij(p, g, i, j);
+        } else if (q < ntop + new_) {
+            int r = q - ntop;
+            int k = 1 + r / (njm1 - 1), j = 1 + r % (njm1 - 1);
+            double hc = p.htci * ((double)g.temp[cidx(0, j, k, nj, nip)] - p.tempamb);
+            double ctmp1 = (double)g.diff_cur[cidx(1, j, k, nj, nip)] * g.dxpwinv[1];
+            g.h[cidx(0, j, k, nj, nip)] = (T)((double)g.h[cidx(1, j, k, nj, nip)] - hc / ctmp1);
+            hc = p.htci * ((double)g.temp[cidx(nim1, j, k, nj, nip)] - p.tempamb);
+            ctmp1 = (double)g.diff_cur[cidx(nim2, j, k, nj, nip)] * g.dxpwinv[nim2];
+            g.h[cidx(nim1, j, k, nj, nip)] = (T)((double)g.h[cidx(nim2, j, k, nj, nip)] - hc / ctmp1);
+        } else {
+            int r = q - ntop - new_;
+            int k = 1 + r / (nim1 - 1), i = 1 + r % (nim1 - 1);
+            double hc = p.htcj * ((double)g.temp[cidx(i, 0, k, nj, nip)] - p.tempamb);
+            double ctmp1 = (double)g.diff_cur[cidx(i, 1, k, nj, nip)] * g.dypsinv[1];
+            g.h[cidx(i, 0, k, nj, nip)] = (T)((double)g.h[cidx(i, 1, k, nj, nip)] - hc / ctmp1);
+            hc = p.htcj * ((double)g.temp[cidx(i, njm1, k, nj, nip)] - p.tempamb);
+            ctmp1 = (double)g.diff_cur[cidx(i, njm2, k, nj, nip)] * g.dypsinv[njm2];
+            g.h[cidx(i, njm1, k, nj, nip)] = (T)((double)g.h[cidx(i, njm2, k, nj, nip)] - hc / ctmp1);
+        }
+    }
+    (void)ni;
+    double v[1] = {ahtop};
+    const int s[1] = {R_AHTOP};
+    const bool m[1] = {false};
+    block_reduce_store<1>(v, s, m, red, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Fused energy assembly: discretizeEquations(5) (CFDSolverManager.cpp:1157-1264),
+// calculateSource(5) (:1677-1843), calculateResiduals(5) (:2073-2101), the
+// coefficient/residual sums of enhanceConvergenceSpeed(5) (:2310-2332) and
+// bareplateMaterialProps (:2137-2189, written to the *_nxt buffers so the
+// old properties stay readable by neighbouring cells).
+// Block (32, 8); each thread walks KB planes.  Grid covers boundary cells too
+// (they only update properties).
+// ---------------------------------------------------------------------------
+constexpr int kAsmKB = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(256) energy_assemble_kernel(Params p, Fields<T> g, double *red)
+{
+    using R = T;
+    const Status *st = g.st;
+    const int i = blockIdx.x * 32 + threadIdx.x;
+    const int j = blockIdx.y * 8 + threadIdx.y;
+    const int k0 = blockIdx.z * kAsmKB;
+    const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
+    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
+              nkm2 = p.nkm2;
+    const int sch = p.scheme;
+    const double delt = st->delt;
+    const bool volsrc = p.volsrc != 0;
+    double sumd = 0.0, sumh = 0.0;
+    double bl = 0.0, blp = 0.0, blm = 0.0, blc = 0.0;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    for (int k = k0; k < k0 + kAsmKB && k < nk; ++k) {
+        if (i >= ni || j >= nj) break;
+        const size_t c = cidx(i, j, k, nj, nip);
+        // ---- material properties (all nodes) ----
+        {
+            double t = (double)g.temp[c], fl = (double)g.fracl[c];
+            double diffl = (p.thconla * t + p.thconlb) / p.acpl;
+            double dn = diffl, rn = p.denl, vn = p.viscos;
+            if (!(t >= p.tliquid)) {
+                double diffs = (p.thconsa * (t * t) + p.thconsb * t + p.thconsc) / (p.acpa * t + p.acpb);
+                dn = diffs; rn = p.dens; vn = 1e10;
+                if (!(t <= p.tsolid)) {
+                    dn = fl * diffl + (1.0 - fl) * diffs;
+                    rn = fl * p.denl + (1.0 - fl) * p.dens;
+                    vn = p.viscos;
+                }
+            }
+            g.diff_nxt[c] = (T)dn;
+            g.rho_nxt[c] = (T)rn;
+            g.vis_nxt[c] = (T)vn;
+        }
+        if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
+        const R *df = g.diff_cur, *rh = g.rho_cur, *h = g.h, *fl = g.fracl;
+        const R dcc = df[c], rhc = rh[c];
+        const R aik = (R)area_ik(p, g, i, k), ajk = (R)area_jk(p, g, j, k), aij = (R)area_ij(p, g, i, j);
+        R an, as_, ae, aw, at, ab, tmp;
+        // north face
+        if (j == njm2) {
+            R vn = g.vvel[c + sj];
+            R fn = rh[c + sj] * vn * aik;
+            R dn = df[c] * aik * (R)g.dypsinv[njm1];
+            face_coef<R>(sch, dn, fn, an, tmp);
+        } else {
+            R vn = g.vvel[c + sj];
+            R fn = rh[c + sj] * vn * aik;
+            R difn = dcc * df[c + sj] / ((R(1) - (R)g.fracy[j]) * df[c + sj] + (R)g.fracy[j] * dcc);
+            R dn = difn * aik * (R)g.dypsinv[j + 1];
+            face_coef<R>(sch, dn, fn, an, tmp);
+        }
+        // south face
+        if (j == 1) {
+            R vs = g.vvel[c];
+            R fs = rhc * vs * aik;
+            R ds = dcc * aik * (R)g.dypsinv[1];
+            face_coef<R>(sch, ds, fs, tmp, as_);
+        } else {
+            R vn = g.vvel[c];
+            R fn = rhc * vn * aik;
+            R difn = df[c - sj] * dcc / ((R(1) - (R)g.fracy[j - 1]) * dcc + (R)g.fracy[j - 1] * df[c - sj]);
+            R dn = difn * aik * (R)g.dypsinv[j];
+            face_coef<R>(sch, dn, fn, tmp, as_);
+        }
+        // east face
+        if (i == nim2) {
+            R ue = g.uvel[c + 1];
+            R fe = rh[c + 1] * ue * ajk;
+            R de = df[c] * ajk * (R)g.dxpwinv[nim1];
+            face_coef<R>(sch, de, fe, ae, tmp);
+        } else {
+            R ue = g.uvel[c + 1];
+            R fe = rh[c + 1] * ue * ajk;
+            R dife = dcc * df[c + 1] / ((R(1) - (R)g.fracx[i]) * df[c + 1] + (R)g.fracx[i] * dcc);
+            R de = dife * ajk * (R)g.dxpwinv[i + 1];
+            face_coef<R>(sch, de, fe, ae, tmp);
+        }
+        // west face
+        if (i == 1) {
+            R uw = g.uvel[c];
+            R fw = rhc * uw * ajk;
+            R dw = dcc * ajk * (R)g.dxpwinv[1];
+            face_coef<R>(sch, dw, fw, tmp, aw);
+        } else {
+            R ue = g.uvel[c];
+            R fe = rhc * ue * ajk;
+            R dife = df[c - 1] * dcc / ((R(1) - (R)g.fracx[i - 1]) * dcc + (R)g.fracx[i - 1] * df[c - 1]);
+            R de = dife * ajk * (R)g.dxpwinv[i];
+            face_coef<R>(sch, de, fe, tmp, aw);
+        }
+        // top face
+        if (k == nkm2) {
+            R wt = g.wvel[c + sk];
+            R ft = rh[c + sk] * wt * aij;
+            R dt = df[c] * aij * (R)g.dzpbinv[nkm1];
+            face_coef<R>(sch, dt, ft, at, tmp);
+        } else {
+            R wt = g.wvel[c + sk];
+            R ft = rh[c + sk] * wt * aij;
+            R dift = dcc * df[c + sk] / ((R(1) - (R)g.fracz[k]) * df[c + sk] + (R)g.fracz[k] * dcc);
+            R dt = dift * aij * (R)g.dzpbinv[k + 1];
+            face_coef<R>(sch, dt, ft, at, tmp);
+        }
+        // bottom face
+        if (k == 1) {
+            R wb = g.wvel[c];
+            R fb = rhc * wb * aij;
+            R db = dcc * aij * (R)g.dzpbinv[1];
+            face_coef<R>(sch, db, fb, tmp, ab);
+        } else {
+            R wt = g.wvel[c];
+            R ft = rhc * wt * aij;
+            R dift = df[c - sk] * dcc / ((R(1) - (R)g.fracz[k - 1]) * dcc + (R)g.fracz[k - 1] * df[c - sk]);
+            R dt = dift * aij * (R)g.dzpbinv[k];
+            face_coef<R>(sch, dt, ft, tmp, ab);
+        }
+        const R vol = (R)volume_p(p, g, i, j, k);
+        const R densbydt = rhc / (R)delt;
+        const R apnot = densbydt * vol;
+        R sp = R(0);
+        R su = apnot * g.hnot[c];
+        // ---- calculateSource(5) ----
+        if (volsrc) {
+            R srcin = R(0);
+            if (g.z[nkm1] - g.z[k] <= st->heatthick) {
+                double hr2 = st->heatrb * st->heatrb;
+                double bx = st->beamposx - g.x[i], by = st->beamposy - g.y[j];
+                srcin = (R)(st->avolpow * st->avolfact / M_PI / hr2 / st->heatthick * st->apowseta *
+                            exp(-st->avolfact / hr2 * ((bx * bx) + (by * by))) *
+                            (double)st->powerindicator);
+                su += vol * srcin;
+            }
+            g.sourceinput[c] = srcin;
+        }
+        const R hlatnt = (R)p.hlatnt;
+        const R variable1 = hlatnt * rhc / (R)delt;
+        const R volht = vol * variable1;
+        const R flc = fl[c];
+        su -= volht * (flc - g.fraclnot[c]);
+        {
+            const R *u = g.uvel, *v = g.vvel, *w = g.wvel;
+            R uc = u[c], up = u[c + 1], vc = v[c], vp = v[c + sj], wc = w[c], wp = w[c + sk];
+            R flew = ajk * (maxd(uc, R(0)) * fl[c - 1] - maxd(-uc, R(0)) * flc +
+                            maxd(-up, R(0)) * fl[c + 1] - maxd(up, R(0)) * flc);
+            R flns = aik * (maxd(vc, R(0)) * fl[c - sj] - maxd(-vc, R(0)) * flc +
+                            maxd(-vp, R(0)) * fl[c + sj] - maxd(vp, R(0)) * flc);
+            R fltb = aij * (maxd(wc, R(0)) * fl[c - sk] - maxd(-wc, R(0)) * flc +
+                            maxd(-wp, R(0)) * fl[c + sk] - maxd(wp, R(0)) * flc);
+            su += rhc * hlatnt * (flew + flns + fltb);
+        }
+        const R hc = h[c];
+        const R hjp = h[c + sj], hjm = h[c - sj], hip = h[c + 1], him = h[c - 1], hkp = h[c + sk],
+                hkm = h[c - sk];
+        // boundary folds, in the reference's order: k, j, i
+        if (k == 1) { su += ab * hkm; sp -= ab; ab = R(0); }
+        if (k == nkm2) { su += at * hkp; sp -= at; at = R(0); }
+        if (j == 1) { su += as_ * hjm; sp -= as_; as_ = R(0); }
+        if (j == njm2) { su += an * hjp; sp -= an; an = R(0); }
+        if (i == 1) { su += aw * him; sp -= aw; aw = R(0); }
+        if (i == nim2) { su += ae * hip; sp -= ae; ae = R(0); }
+        R ap = an + as_ + ae + aw + at + ab + apnot - sp;
+        const R urfh = (R)p.urfh;
+        ap /= urfh;
+        su += (R(1) - urfh) * ap * hc;
+        g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw;
+        g.at[c] = at; g.ab[c] = ab; g.ap[c] = ap; g.su[c] = su;
+        // ---- residual (calculateResiduals(5)) ----
+        R r = (an * hjp + as_ * hjm + ae * hip + aw * him + at * hkp + ab * hkm + su) / ap - hc;
+        sumd += fabs((double)r);
+        sumh += fabs((double)hc);
+        // ---- block-correction sums (enhanceConvergenceSpeed(5)) ----
+        bl += (double)(ap - an - as_ - at - ab);
+        blp += (double)ae;
+        blm += (double)aw;
+        blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
+    }
+    // per-i partial sums over this block's j-rows and planes
+    __shared__ double sb[4][8][33];
+    sb[0][threadIdx.y][threadIdx.x] = bl;
+    sb[1][threadIdx.y][threadIdx.x] = blp;
+    sb[2][threadIdx.y][threadIdx.x] = blm;
+    sb[3][threadIdx.y][threadIdx.x] = blc;
+    __syncthreads();
+    if (threadIdx.y < 4 && i < nip) {
+        double s = 0.0;
+        for (int y = 0; y < 8; ++y) s += sb[threadIdx.y][y][threadIdx.x];
+        const int part = blockIdx.z * gridDim.y + blockIdx.y;
+        g.bc[((size_t)part * 4 + threadIdx.y) * nip + i] = s;
+    }
+    __syncthreads();
+    double v[2] = {sumd, sumh};
+    const int s[2] = {R_SUMD, R_SUMH};
+    const bool m[2] = {false, false};
+    const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    block_reduce_store<2>(v, s, m, red, blk);
+    (void)ni;
+}
+
+// ---------------------------------------------------------------------------
+// Block correction solve (enhanceConvergenceSpeed(5), CFDSolverManager.cpp:2334-2349)
+// and the energy residual resorh (:2099).  One CTA.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, int nblk_asm,
+                                     int check_finite)
+{
+    extern __shared__ double sm[];  // 4 * nip
+    const int nip = p.nip, nim1 = p.nim1, nim2 = p.nim2;
+    double *bl = sm, *blp = sm + nip, *blm = sm + 2 * nip, *blc = sm + 3 * nip;
+    for (int q = threadIdx.x; q < 4 * nip; q += blockDim.x) {
+        int w = q / nip, i = q - w * nip;
+        double s = 0.0;
+        for (int part = 0; part < gd.npart; ++part) s += gd.bc[((size_t)part * 4 + w) * nip + i];
+        sm[q] = s;
+    }
+    double sd = 0.0, sh = 0.0;
+    for (int b = threadIdx.x; b < nblk_asm; b += blockDim.x) {
+        sd += red_asm[(size_t)b * R_NSLOTS + R_SUMD];
+        sh += red_asm[(size_t)b * R_NSLOTS + R_SUMH];
+    }
+    __syncthreads();
+    double v[2] = {sd, sh};
+    const int sl[2] = {0, 1};
+    const bool mx[2] = {false, false};
+    __shared__ double tot[R_NSLOTS];
+    block_reduce_store<2>(v, sl, mx, tot, 0);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        Status *st = gd.st;
+        double resorh = tot[0] / (tot[1] + kSmall);
+        st->resorh = resorh;
+        if (check_finite && !isfinite(resorh)) st->nonfinite = 1;
+        // 1-D TDMA in i
+        double *delphi = gd.delphi;
+        double pib_prev = blp[1] / bl[1];
+        double qib_prev = blc[1] / bl[1];
+        // pib/qib stored in bl/blm scratch (bl[i] no longer needed after use)
+        blm[1] = pib_prev;
+        blp[1] = qib_prev;
+        for (int i = 2; i < nim1; i++) {
+            double denom = bl[i] - blm[i] * pib_prev;
+            double pib = blp[i] / denom;
+            double qib = (blc[i] + blm[i] * qib_prev) / denom;
+            blm[i] = pib;
+            blp[i] = qib;
+            pib_prev = pib;
+            qib_prev = qib;
+        }
+        double d = blp[nim2];
+        delphi[nim2] = d;
+        for (int i = nim2 - 1; i > 0; i--) {
+            d = blm[i] * d + blp[i];
+            delphi[i] = d;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// convertEnthalpyToTemp (CFDSolverManager.cpp:2531-2571), fused with the
+// peak-temperature maximum (BoundCondManager.cpp:301) and the reductions of
+// calculateFluxes (BoundCondManager.cpp:778-843): boundary conduction fluxes,
+// heat accumulation and volumetric heat input.  H->T is evaluated in FP64.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void h2t_kernel(Params p, Fields<T> g, double *red)
+{
+    const Status *st = g.st;
+    const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
+    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
+              nkm2 = p.nkm2;
+    const double deltemp = p.tliquid - p.tsolid;
+    const double delt = st->delt;
+    double tmax = -INFINITY, accul = 0.0, heatvol = 0.0;
+    double fw = 0.0, fe = 0.0, fb = 0.0, ft = 0.0, fs = 0.0, fn = 0.0;
+    const size_t total = (size_t)nk * nj * nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(c % nip);
+        if (i >= ni) continue;
+        const int j = (int)((c / nip) % nj), k = (int)(c / sk);
+        const double h = (double)g.h[c];
+        double fl, t;
+        if (h >= p.hlcal) {
+            fl = 1.0;
+            t = (h - p.hlcal) / p.acpl + p.tliquid;
+        } else if (h <= p.hsmelt) {
+            fl = 0.0;
+            t = (sqrt(p.acpb * p.acpb + 2 * p.acpa * h) - p.acpb) / p.acpa;
+        } else {
+            fl = (h - p.hsmelt) / (p.hlcal - p.hsmelt);
+            t = deltemp * fl + p.tsolid;
+        }
+        g.fracl[c] = (T)fl;
+        g.temp[c] = (T)t;
+        double tt = (double)(T)t;
+        if (tt > tmax) tmax = tt;
+        if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
+        if (!p.steady) {
+            double dh1 = h - (double)g.hnot[c] + ((double)(T)fl - (double)g.fraclnot[c]) * p.hlatnt;
+            double vol = volume_p(p, g, i, j, k);
+            accul += vol * (double)g.rho_nxt[c] * dh1 / delt;
+            heatvol += (double)g.sourceinput[c] * vol;
+        }
+        const double *dx = g.dxpwinv, *dy = g.dypsinv, *dz = g.dzpbinv;
+        if (i == 1)
+            fw += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - 1] - h) * dx[1]);
+        if (i == nim2)
+            fe += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + 1] - h) * dx[nim1]);
+        if (k == 1)
+            fb += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c - sk] - h) * dz[1]);
+        if (k == nkm2)
+            ft += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c + sk] - h) * dz[nkm1]);
+        if (j == 1)
+            fs += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - sj] - h) * dy[1]);
+        if (j == njm2)
+            fn += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + sj] - h) * dy[njm1]);
+    }
+    double v[8] = {tmax, accul, heatvol, fw, fe, fb, ft, fs};
+    const int s[8] = {R_TPEAK, R_ACCUL, R_HEATVOL, R_FW, R_FE, R_FB, R_FT, R_FS};
+    const bool m[8] = {true, false, false, false, false, false, false, false};
+    block_reduce_store<8>(v, s, m, red, blockIdx.x);
+    __syncthreads();
+    double v2[1] = {fn};
+    const int s2[1] = {R_FN};
+    const bool m2[1] = {false};
+    block_reduce_store<1>(v2, s2, m2, red, blockIdx.x);
+}
+
+// Fixed-order block reduction of one slot over `nb` per-CTA partials.
+__device__ double reduce_slot(const double *red, int nb, int slot, bool is_max, double *scratch)
+{
+    double acc = is_max ? -INFINITY : 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        double x = red[(size_t)b * R_NSLOTS + slot];
+        acc = is_max ? fmax(acc, x) : acc + x;
+    }
+    acc = is_max ? warp_max(acc) : warp_sum(acc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = acc;
+    __syncthreads();
+    double r = is_max ? -INFINITY : 0.0;
+    if (warp == 0) {
+        r = (lane < (int)(blockDim.x >> 5)) ? scratch[lane] : (is_max ? -INFINITY : 0.0);
+        r = is_max ? warp_max(r) : warp_sum(r);
+        if (lane == 0) scratch[32] = r;
+    }
+    __syncthreads();
+    r = scratch[32];
+    __syncthreads();
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// getMeltPoolShape (BoundCondManager.cpp:280-447), one CTA.  The scans along
+// i/j/k are evaluated per column in parallel; the folds whose result depends on
+// order (the NaN behaviour of std::max/min) run sequentially in thread 0.
+// Also activates the momentum box and builds its exact-order ticket list.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, const double *red_h2t,
+                                                        int nblk_h2t)
+{
+    Status *st = g.st;
+    __shared__ double scratch[40];
+    extern __shared__ double colv[];  // 3 * nip doubles + nip ints
+    const int nj = p.nj, nip = p.nip;
+    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
+              nkm2 = p.nkm2;
+    const double ts = p.tsolid;
+    double tp = reduce_slot(red_h2t, nblk_h2t, R_TPEAK, true, scratch);
+    double t0 = (double)g.temp[0];
+    if (isnan(t0)) tp = t0;  // std::max_element keeps a leading NaN
+    if (threadIdx.x == 0) st->tpeak = tp;
+    if (!(tp > ts)) {
+        if (threadIdx.x == 0) {
+            st->alen = 0.0;
+            st->depth = 0.0;
+            st->width = 0.0;
+            st->momentum_active = 0;
+        }
+        return;
+    }
+    const int js = st->jstart, is0 = st->istart;
+    // Reads outside the node range (the reference reads past its arrays when the
+    // pool touches the north/south boundary rows) return NaN instead.
+    auto TT = [&](int i, int j, int k) {
+        if (i < 0 || i >= p.ni || j < 0 || j >= nj || k < 0 || k >= p.nk) return (double)NAN;
+        return (double)g.temp[cidx(i, j, k, nj, nip)];
+    };
+    auto YY = [&](int j) { return (j < 0 || j >= nj) ? (double)NAN : g.y[j]; };
+    double *depv = colv, *wmax = colv + nip, *wmin = colv + 2 * nip;
+    int *imaxc = (int *)(colv + 3 * nip);
+    // length: first i >= istart on the top row with T <= Ts; last i <= istart with T < Ts
+    int cand_max = INT_MAX, cand_min = INT_MIN;
+    for (int i = is0 + (int)threadIdx.x; i < nim1; i += blockDim.x)
+        if (TT(i, js, nkm1) <= ts) cand_max = min(cand_max, i);
+    for (int i = 1 + (int)threadIdx.x; i <= is0; i += blockDim.x)
+        if (TT(i, js, nkm1) < ts) cand_min = max(cand_min, i);
+    // depth scan per column i: kb = first k (descending from nkm2) with T < Ts
+    // width scans per column i on the top plane
+    int kmin_c = INT_MAX, jmax_c = INT_MIN, jmin_c = INT_MAX;
+    for (int i = 1 + (int)threadIdx.x; i < nim1; i += blockDim.x) {
+        int k = nkm2;
+        for (; k > 0; k--)
+            if (TT(i, js, k) < ts) break;
+        if (k < nkm2) kmin_c = min(kmin_c, k + 1);
+        int j = js;
+        for (; j < njm1; j++)
+            if (TT(i, j, nkm1) < ts) break;
+        if (j > js) jmax_c = max(jmax_c, j - 1);
+        j = js;
+        for (; j > 0; j--)
+            if (TT(i, j, nkm1) < ts) break;
+        if (j < js) jmin_c = min(jmin_c, j + 1);
+    }
+    // block min/max of the integer candidates
+    __shared__ int red_i[6];
+    if (threadIdx.x == 0) {
+        red_i[0] = INT_MAX; red_i[1] = INT_MIN; red_i[2] = INT_MAX; red_i[3] = INT_MIN;
+        red_i[4] = INT_MAX;
+    }
+    __syncthreads();
+    atomicMin(&red_i[0], cand_max);
+    atomicMax(&red_i[1], cand_min);
+    atomicMin(&red_i[2], kmin_c);
+    atomicMax(&red_i[3], jmax_c);
+    atomicMin(&red_i[4], jmin_c);
+    __syncthreads();
+    int imax = (is0 < nim1) ? (red_i[0] == INT_MAX ? nim1 - 1 : red_i[0]) : is0;
+    int imin = (is0 > 0) ? (red_i[1] == INT_MIN ? 1 : red_i[1]) : is0;
+    int kmin = min(nkm2, red_i[2]) - 1;
+    int jmax = max(js, red_i[3]) + 1;
+    int jmin = min(js, red_i[4]) - 1;
+    // per-column interpolated values for the order-dependent folds
+    for (int i = 1 + (int)threadIdx.x; i < nim1; i += blockDim.x) {
+        imaxc[i] = 1;
+        if (kmin != 0) {
+            if (TT(i, js, kmin + 1) < ts) {
+                imaxc[i] = 0;
+            } else {
+                double dtdzzinv = (g.z[kmin] - g.z[kmin - 1]) / (TT(i, js, kmin) - TT(i, js, kmin - 1));
+                depv[i] = g.z[nkm1] - g.z[kmin] + (TT(i, js, kmin) - ts) * dtdzzinv;
+            }
+        }
+        wmax[i] = NAN;
+        if (jmax != js && !(TT(i, jmax - 1, nkm1) < ts)) {
+            double dtdyyinv = (YY(jmax) - YY(jmax + 1)) / (TT(i, jmax, nkm1) - TT(i, jmax + 1, nkm1));
+            wmax[i] = YY(jmax) + (ts - TT(i, jmax, nkm1)) * dtdyyinv;
+        }
+        wmin[i] = NAN;
+        if (jmin != js && !(TT(i, jmin + 1, nkm1) < ts)) {
+            double dtdyyinv = (YY(jmin) - YY(jmin - 1)) / (TT(i, jmin, nkm1) - TT(i, jmin - 1, nkm1));
+            wmin[i] = YY(jmin) + (ts - TT(i, jmin, nkm1)) * dtdyyinv;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        auto XX = [&](int i) { return (i < 0 || i >= p.ni) ? (double)NAN : g.x[i]; };
+        double dtdxxinv = (XX(imax) - XX(imax + 1)) / (TT(imax, js, nkm1) - TT(imax + 1, js, nkm1));
+        double xxmax = XX(imax) + (ts - TT(imax, js, nkm1)) * dtdxxinv;
+        dtdxxinv = (XX(imin) - XX(imin - 1)) / (TT(imin, js, nkm1) - TT(imin - 1, js, nkm1));
+        double xxmin = XX(imin) + (ts - TT(imin, js, nkm1)) * dtdxxinv;
+        st->alen = xxmax - xxmin;
+        double depth = 0.0;
+        if (kmin == 0) {
+            depth = g.z[nkm1] - g.z[0];
+        } else {
+            for (int i = 1; i < nim1; i++)
+                if (imaxc[i]) depth = maxd(depv[i], depth);
+        }
+        st->depth = depth;
+        double yymax = g.y[0];
+        if (jmax != js)
+            for (int i = 1; i < nim1; i++)
+                if (!(TT(i, jmax - 1, nkm1) < ts)) yymax = maxd(wmax[i], yymax);
+        double yymin = YY(js);
+        if (jmin != js)
+            for (int i = 1; i < nim1; i++)
+                if (!(TT(i, jmin + 1, nkm1) < ts)) yymin = mind(wmin[i], yymin);
+        st->width = yymax - yymin;
+        st->imax = imax; st->imin = imin; st->kmin = kmin; st->kmax = nkm2;
+        st->jmax = jmax; st->jmin = jmin;
+        st->istat = max(imin - 3, 1);
+        st->iend = min(imax + 3, nim2);
+        st->jstat = max(jmin - 3, 1);
+        st->jend = min(jmax + 2, njm2);
+        st->kstat = max(kmin - 2, 2);
+        st->istatp1 = st->istat + 1;
+        st->iendm1 = st->iend - 1;
+        st->momentum_active = p.navierstokes ? 1 : 0;
+        st->box_cells = st->momentum_active
+            ? max(0, st->iendm1 - st->istatp1 + 1) * max(0, st->jend - st->jstat + 1) * max(0, nkm1 - st->kstat)
+            : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// End of an outer iteration: calculateFluxes ratio (BoundCondManager.cpp:846-857),
+// amaxres and the convergence test (CFDSolverManager.cpp:689-716).  One CTA.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, int nb_h2t,
+                                const double *red_bc, int nb_bc, const double *red_las, int nb_las,
+                                const double *red_mom, int nb_mom, double tol, int check_finite)
+{
+    __shared__ double scratch[40];
+    Status *st = gd.st;
+    double accul = reduce_slot(red_h2t, nb_h2t, R_ACCUL, false, scratch);
+    double heatvol = reduce_slot(red_h2t, nb_h2t, R_HEATVOL, false, scratch);
+    double fw = reduce_slot(red_h2t, nb_h2t, R_FW, false, scratch);
+    double fe = reduce_slot(red_h2t, nb_h2t, R_FE, false, scratch);
+    double fb = reduce_slot(red_h2t, nb_h2t, R_FB, false, scratch);
+    double ft = reduce_slot(red_h2t, nb_h2t, R_FT, false, scratch);
+    double fs = reduce_slot(red_h2t, nb_h2t, R_FS, false, scratch);
+    double fn = reduce_slot(red_h2t, nb_h2t, R_FN, false, scratch);
+    double ahtop = reduce_slot(red_bc, nb_bc, R_AHTOP, false, scratch);
+    double heatin = reduce_slot(red_las, nb_las, R_HEATIN, false, scratch);
+    if (threadIdx.x == 0) {
+        st->accul = p.steady ? 0.0 : accul;
+        st->heatvol = p.steady ? 0.0 : heatvol;
+        st->fluxwest = fw; st->fluxeast = fe; st->fluxbottom = fb; st->fluxtop = ft;
+        st->fluxsouth = fs; st->fluxnorth = fn;
+        st->ahtoploss = ahtop;
+        st->heatinlaser = heatin;
+        st->heatout = (fn + fb + fw + fe + fs) - ahtop;
+        double ratio = p.steady ? -st->heatout / heatin : (st->heatvol + heatin) / (st->accul - st->heatout);
+        st->ratio = ratio;
+        double list[5] = {st->resorm, st->resoru, st->resorv, st->resorw, 0.0};
+        double amaxres = list[0];
+        for (int q = 1; q < 5; q++)
+            if (amaxres < list[q]) amaxres = list[q];
+        int conv;
+        if (p.steady)
+            conv = (ratio <= 1.001 && ratio >= 0.999 && amaxres < tol);
+        else if (st->powerindicator == 1)
+            conv = (ratio <= 1.01 && ratio >= 0.99 && amaxres < tol);
+        else
+            conv = (st->resorh < 1e-6 && amaxres < tol);
+        st->converged = conv;
+        if (check_finite && (!isfinite(st->tpeak) || !isfinite(ratio) || !isfinite(st->resorh)))
+            st->nonfinite = 1;
+    }
+    (void)red_mom; (void)nb_mom;
+}
+
+// ---------------------------------------------------------------------------
+// updateSolutions (CFDSolverManager.cpp:2625-2687): solid velocities to zero and
+// the previous-step copies.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void update_solutions_kernel(Params p, Fields<T> g)
+{
+    const size_t total = (size_t)p.nk * p.nj * p.nip;
+    const T ts = (T)p.tsolid;
+    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += (size_t)gridDim.x * blockDim.x) {
+        if (g.temp[c] <= ts) {
+            g.uvel[c] = T(0);
+            g.vvel[c] = T(0);
+            g.wvel[c] = T(0);
+        }
+        g.unot[c] = g.uvel[c];
+        g.vnot[c] = g.vvel[c];
+        g.wnot[c] = g.wvel[c];
+        g.hnot[c] = g.h[c];
+        g.fraclnot[c] = g.fracl[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T> void launch_laser(Inst<T> &I)
+{
+    laser_kernel<T><<<I.nb_las, 256, 0, I.stream>>>(I.p, I.g, I.red_las);
+}
+template <typename T> void launch_energy_bc(Inst<T> &I)
+{
+    energy_bc_kernel<T><<<I.nb_bc, 256, 0, I.stream>>>(I.p, I.g, I.red_bc);
+}
+template <typename T> void launch_energy_assemble(Inst<T> &I)
+{
+    energy_assemble_kernel<T><<<I.asm_grid, dim3(32, 8), 0, I.stream>>>(I.p, I.g, I.red_asm);
+}
+template <typename T> void launch_block_correct(Inst<T> &I)
+{
+    block_correct_kernel<T><<<1, 1024, 4 * I.p.nip * sizeof(double), I.stream>>>(
+        I.p, I.g, I.red_asm, I.nb_asm, I.check_finite);
+}
+template <typename T> void launch_h2t(Inst<T> &I)
+{
+    h2t_kernel<T><<<I.nb_h2t, 256, 0, I.stream>>>(I.p, I.g, I.red_h2t);
+}
+template <typename T> void launch_meltpool(Inst<T> &I)
+{
+    size_t smem = 3 * (size_t)I.p.nip * sizeof(double) + (size_t)I.p.nip * sizeof(int);
+    meltpool_kernel<T><<<1, 1024, smem, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t);
+}
+template <typename T> void launch_converge(Inst<T> &I, double tol)
+{
+    converge_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t, I.red_bc, I.nb_bc,
+                                                  I.red_las, I.nb_las, I.red_mom, I.nb_mom, tol,
+                                                  I.check_finite);
+}
+template <typename T> void launch_update_solutions(Inst<T> &I)
+{
+    update_solutions_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g);
+}
+
+#define AMCFD_INST(T)                                        \
+    template void launch_laser<T>(Inst<T> &);               \
+    template void launch_energy_bc<T>(Inst<T> &);           \
+    template void launch_energy_assemble<T>(Inst<T> &);     \
+    template void launch_block_correct<T>(Inst<T> &);       \
+    template void launch_h2t<T>(Inst<T> &);                 \
+    template void launch_meltpool<T>(Inst<T> &);            \
+    template void launch_converge<T>(Inst<T> &, double);    \
+    template void launch_update_solutions<T>(Inst<T> &);
+AMCFD_INST(double)
+AMCFD_INST(float)
+#undef AMCFD_INST
+
+}  // namespace amcfd

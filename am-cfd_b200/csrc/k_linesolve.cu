@@ -1,0 +1,437 @@
+// Line-by-line TDMA on x-lines (solveEntireDomain, CFDSolverManager.cpp:2459-2526;
+// solveLiquidDomain, :2367-2454).
+//
+// Each x-line system  ap_i phi_i = aw_i phi_{i-1} + ae_i phi_{i+1} + d_i  with
+// d_i = at phi(k+1) + ab phi(k-1) + an phi(j+1) + as phi(j-1) + su  is solved
+// by the Thomas recurrences
+//     den_i = ap_i - aw_i pr_{i-1},  pr_i = ae_i/den_i,
+//     qr_i  = (d_i + aw_i qr_{i-1})/den_i,   phi_i = pr_i phi_{i+1} + qr_i.
+// den/pr do not depend on phi, so they are factored once per call
+// (factor kernels below).  The two remaining recurrences are affine maps and
+// are evaluated by one warp per line: each lane composes the maps of a
+// contiguous chunk of cells, a 5-step shuffle scan combines the chunks, and
+// each lane then applies the combined map to its own chunk.
+//
+// Sweep order.  The reference visits lines in the order
+//   ksweep(2) x k = nkm2..1 x jsweep(2) x j = 1..njm2
+// (Gauss-Seidel in j and k).  Visit (ks,k,s,j) only depends on visits at
+// wave t' < t, where t = 3m + (j-j0) + 2s and m = ks*M + (k1-k): writes of
+// one wave never touch a row another visit of the same wave reads.  The exact
+// mode runs visits in (t, m, s) order with per-line counters, reproducing the
+// reference iterates; the red-black mode updates all lines of one (j+k)
+// colour at once.
+#include "kernels.cuh"
+#include "amcfd.h"
+
+namespace amcfd {
+
+// ---------------------------------------------------------------------------
+// Factorisation: pr, cf = aw/den, iden = 1/den for every line of a box.
+// 32 lines per CTA, 32-cell chunks staged through shared memory so global
+// accesses stay coalesced; one thread per line walks its chunk sequentially.
+// ENERGY also applies the block correction phi += delphi[i] (enhanceConvergenceSpeed,
+// CFDSolverManager.cpp:2351-2361); BOX applies the |den| <= 1e-12 guard of
+// solveLiquidDomain (:2438-2439) and reads the box from the status block.
+// ---------------------------------------------------------------------------
+template <typename T, bool BOX>
+__global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g)
+{
+    __shared__ T tap[32][33], taw[32][33], tae[32][33], tph[32][33];
+    const Status *st = g.st;
+    int i0, i1, j0, j1, k0, k1;
+    if (BOX) {
+        if (!st->momentum_active) return;
+        i0 = st->istatp1; i1 = st->iendm1; j0 = st->jstat; j1 = st->jend; k0 = st->kstat; k1 = p.nkm2;
+    } else {
+        i0 = 1; i1 = p.nim2; j0 = 1; j1 = p.njm2; k0 = 1; k1 = p.nkm2;
+    }
+    const int J = j1 - j0 + 1, nlines = J * (k1 - k0 + 1);
+    if (J <= 0 || k1 < k0 || i1 < i0) return;
+    const int nj = p.nj, nip = p.nip;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int l0 = blockIdx.x * 32; l0 < nlines; l0 += gridDim.x * 32) {
+        T prv = T(0);  // pr of the previous cell (pr[istat] = 0)
+        for (int ib = i0; ib <= i1; ib += 32) {
+            for (int r = warp; r < 32; r += 8) {
+                int l = l0 + r, i = ib + lane;
+                if (l < nlines && i <= i1) {
+                    int k = k0 + l / J, j = j0 + l % J;
+                    size_t c = cidx(i, j, k, nj, nip);
+                    tap[r][lane] = g.ap[c];
+                    taw[r][lane] = g.aw[c];
+                    tae[r][lane] = g.ae[c];
+                    if (!BOX) tph[r][lane] = g.h[c] + (T)g.delphi[i];
+                }
+            }
+            __syncthreads();
+            if (warp == 0 && l0 + lane < nlines) {
+                const int r = lane;
+                const int n = min(32, i1 - ib + 1);
+                for (int q = 0; q < n; ++q) {
+                    T den = tap[r][q] - taw[r][q] * prv;
+                    if (BOX && fabs(den) <= T(1e-12)) den += T(kSmall);
+                    T id = T(1) / den;
+                    T pr = tae[r][q] * id;
+                    tap[r][q] = pr;
+                    taw[r][q] = taw[r][q] * id;
+                    tae[r][q] = id;
+                    prv = pr;
+                }
+            }
+            __syncthreads();
+            for (int r = warp; r < 32; r += 8) {
+                int l = l0 + r, i = ib + lane;
+                if (l < nlines && i <= i1) {
+                    int k = k0 + l / J, j = j0 + l % J;
+                    size_t c = cidx(i, j, k, nj, nip);
+                    g.pr[c] = tap[r][lane];
+                    g.cf[c] = taw[r][lane];
+                    g.iden[c] = tae[r][lane];
+                    if (!BOX) g.h[c] = tph[r][lane];
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Load of a value another warp may have just written (bypasses L1).
+template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) { return __ldcg(ptr); }
+
+// ---------------------------------------------------------------------------
+// One x-line solved by one warp.  `row` is the offset of node (0, j, k);
+// cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] are the fixed ends.
+// sb: 3 * nmax values of per-warp shared scratch.
+// ---------------------------------------------------------------------------
+template <typename T, bool COHERENT>
+__device__ __forceinline__ void solve_line(const Fields<T> &g, T *phi, size_t row, int i0, int i1,
+                                           size_t sj, size_t sk, T *sb, int nmax)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = i1 - i0 + 1;
+    const int L = (n + 31) >> 5;
+    const int a = i0 + lane * L;
+    const int b = min(a + L, i1 + 1);
+    T *se = sb, *sc = sb + nmax, *sp = sb + 2 * nmax;
+    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
+    // forward: qr_i = cf_i qr_{i-1} + e_i,  e_i = d_i / den_i
+    T A = T(1), B = T(0);
+    for (int i = a; i < b; ++i) {
+        size_t c = row + i;
+        T d = g.at[c] * ldp(c + sk) + g.ab[c] * ldp(c - sk) + g.an[c] * ldp(c + sj) +
+              g.as[c] * ldp(c - sj) + g.su[c];
+        T e = d * g.iden[c];
+        T cfi = g.cf[c];
+        se[i - i0] = e;
+        sc[i - i0] = cfi;
+        sp[i - i0] = g.pr[c];
+        B = cfi * B + e;
+        A = cfi * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_up_sync(0xffffffffu, A, o);
+        T B2 = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    T Ae = __shfl_up_sync(0xffffffffu, A, 1);
+    T Be = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) { Ae = T(1); Be = T(0); }
+    T q = Ae * ldp(row + i0 - 1) + Be;
+    for (int i = a; i < b; ++i) {
+        q = sc[i - i0] * q + se[i - i0];
+        se[i - i0] = q;
+    }
+    // backward: phi_i = pr_i phi_{i+1} + qr_i
+    A = T(1);
+    B = T(0);
+    for (int i = b - 1; i >= a; --i) {
+        T pri = sp[i - i0];
+        B = pri * B + se[i - i0];
+        A = pri * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_down_sync(0xffffffffu, A, o);
+        T B2 = __shfl_down_sync(0xffffffffu, B, o);
+        if (lane + o < 32) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    Ae = __shfl_down_sync(0xffffffffu, A, 1);
+    Be = __shfl_down_sync(0xffffffffu, B, 1);
+    if (lane == 31) { Ae = T(1); Be = T(0); }
+    T x = Ae * ldp(row + i1 + 1) + Be;
+    for (int i = b - 1; i >= a; --i) {
+        x = sp[i - i0] * x + se[i - i0];
+        phi[row + i] = x;
+    }
+}
+
+// Bounded wait until *f >= target (wrap-safe); false on timeout or a raised error.
+__device__ bool wait_ge(const int *f, int target, Status *st, int where)
+{
+    long long it = 0;
+    while (true) {
+        int v = *(volatile const int *)f;
+        if (v - target >= 0) return true;
+        if ((it & 63) == 63 && *(volatile int *)&st->error) return false;
+        if (++it > kSpinLimit) {
+            if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <bool BOX>
+__device__ __forceinline__ void box_of(const Params &p, const Status *st, int &i0, int &i1,
+                                       int &j0, int &j1, int &k0, int &k1)
+{
+    if (BOX) {
+        i0 = st->istatp1; i1 = st->iendm1; j0 = st->jstat; j1 = st->jend; k0 = st->kstat; k1 = p.nkm2;
+    } else {
+        i0 = 1; i1 = p.nim2; j0 = 1; j1 = p.njm2; k0 = 1; k1 = p.nkm2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exact-order sweep: persistent warps take visits in topological order.
+// Per-line counters hold seq*4 + (visits done in the current call).
+// ---------------------------------------------------------------------------
+template <typename T, bool BOX>
+__global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, const int2 *tickets,
+                                   int nt_static, unsigned long long *seqp,
+                                   unsigned long long *donep, unsigned long long *ticketp)
+{
+    extern __shared__ unsigned char smraw[];
+    Status *st = g.st;
+    __shared__ unsigned long long seq_s;
+    __shared__ int active_s, nt_s;
+    if (threadIdx.x == 0) {
+        seq_s = *(volatile unsigned long long *)seqp;
+        active_s = BOX ? st->momentum_active : 1;
+        nt_s = BOX ? *g.ntickets_mom : nt_static;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nmax = p.nip;
+    T *sb = reinterpret_cast<T *>(smraw) + (size_t)warp * 3 * nmax;
+    const int base = (int)(seq_s * 4ull);
+    if (active_s) {
+        int i0, i1, j0, j1, k0, k1;
+        box_of<BOX>(p, st, i0, i1, j0, j1, k0, k1);
+        const int M = k1 - k0 + 1;
+        const int nj = p.nj, nip = p.nip;
+        const size_t sj = nip, sk = (size_t)nj * nip;
+        const int nt = nt_s;
+        while (true) {
+            unsigned long long tk = 0;
+            if (lane == 0) tk = atomicAdd(ticketp, 1ull);
+            tk = __shfl_sync(0xffffffffu, tk, 0);
+            if (tk >= (unsigned long long)nt) break;
+            int2 e = tickets[tk];
+            const int m = e.x, s = e.y >> 16, jj = e.y & 0xffff;
+            const int ks = m / M, k = k1 - (m - ks * M), j = j0 + jj, v = 2 * ks + s;
+            int ok = 1;
+            if (lane == 0) {
+                const int where = k * nj + j;
+                if (ok && j > j0) ok = wait_ge(&flags[k * nj + j - 1], base + v + 1, st, where);
+                if (ok && j < j1 && v > 0) ok = wait_ge(&flags[k * nj + j + 1], base + v, st, where);
+                if (ok && k < k1) ok = wait_ge(&flags[(k + 1) * nj + j], base + 2 * ks + 2, st, where);
+                if (ok && k > k0 && ks > 0) ok = wait_ge(&flags[(k - 1) * nj + j], base + 2 * ks, st, where);
+                __threadfence();
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (!ok) break;
+            __syncwarp();
+            solve_line<T, true>(g, phi, cidx(0, j, k, nj, nip), i0, i1, sj, sk, sb, nmax);
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) atomicExch(&flags[k * nj + j], base + v + 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long prev = atomicAdd(donep, 1ull);
+        if (prev == (unsigned long long)gridDim.x - 1) {
+            // last CTA of this call: reset the counters for the next call
+            atomicExch(donep, 0ull);
+            atomicExch(ticketp, 0ull);
+            __threadfence();
+            atomicAdd(seqp, 1ull);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Red-black sweep: every line of one (j+k) colour, one warp per line.
+// ---------------------------------------------------------------------------
+template <typename T, bool BOX>
+__global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
+{
+    extern __shared__ unsigned char smraw[];
+    const Status *st = g.st;
+    if (BOX && !st->momentum_active) return;
+    int i0, i1, j0, j1, k0, k1;
+    box_of<BOX>(p, st, i0, i1, j0, j1, k0, k1);
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5;
+    const int nmax = p.nip;
+    T *sb = reinterpret_cast<T *>(smraw) + (size_t)warp * 3 * nmax;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const int wpb = blockDim.x >> 5;
+    // lines of this colour: for each k, j runs over one parity
+    const int half = (J + 1) / 2;
+    const int nl = half * K;
+    for (int q = blockIdx.x * wpb + warp; q < nl; q += gridDim.x * wpb) {
+        int kk = q / half, r = q - kk * half;
+        int k = k0 + kk;
+        int jpar = ((color - k - j0) % 2 + 2) % 2;  // offset of the first j of this colour
+        int j = j0 + jpar + 2 * r;
+        if (j > j1) continue;
+        solve_line<T, false>(g, phi, cidx(0, j, k, nj, nip), i0, i1, sj, sk, sb, nmax);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Ticket list of the momentum box, in (t, m, s) order (one CTA).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *tickets, int *ntickets,
+                                                           Status *st)
+{
+    __shared__ int cnt[1024];
+    if (!st->momentum_active) return;
+    const int J = st->jend - st->jstat + 1, M = p.nkm2 - st->kstat + 1;
+    if (J <= 0 || M <= 0) {
+        if (threadIdx.x == 0) *ntickets = 0;
+        return;
+    }
+    const int T = 3 * (2 * M - 1) + (J - 1) + 2 + 1;
+    auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };  // floor
+    auto count_t = [&](int t) {
+        int c = 0;
+        for (int s = 0; s < 2; ++s) {
+            int lo = max(0, -fdiv(-(t - 2 * s - (J - 1)), 3));  // ceil((t-2s-(J-1))/3)
+            int hi = min(2 * M - 1, fdiv(t - 2 * s, 3));
+            if (hi >= lo) c += hi - lo + 1;
+        }
+        return c;
+    };
+    int running = 0;  // tickets written by earlier rounds of 1024 waves
+    for (int t0 = 0; t0 < T; t0 += 1024) {
+        const int t = t0 + threadIdx.x;
+        const int c = t < T ? count_t(t) : 0;
+        cnt[threadIdx.x] = c;
+        __syncthreads();
+        for (int o = 1; o < 1024; o <<= 1) {  // inclusive scan
+            int v = threadIdx.x >= o ? cnt[threadIdx.x - o] : 0;
+            __syncthreads();
+            cnt[threadIdx.x] += v;
+            __syncthreads();
+        }
+        int off = running + cnt[threadIdx.x] - c;
+        if (t < T) {
+            int mlo = max(0, -fdiv(-(t - 2 - (J - 1)), 3));
+            int mhi = min(2 * M - 1, fdiv(t, 3));
+            for (int m = mlo; m <= mhi; ++m) {
+                for (int s = 0; s < 2; ++s) {
+                    int jj = t - 3 * m - 2 * s;
+                    if (jj >= 0 && jj < J) tickets[off++] = make_int2(m, (s << 16) | jj);
+                }
+            }
+        }
+        int total = cnt[1023];
+        __syncthreads();
+        running += total;
+    }
+    if (threadIdx.x == 0) *ntickets = running;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename T> void launch_energy_factor(Inst<T> &I)
+{
+    int lines = (I.p.nj - 2) * (I.p.nk - 2);
+    int grid = (lines + 31) / 32;
+    factor_kernel<T, false><<<grid, 256, 0, I.stream>>>(I.p, I.g);
+}
+template <typename T> void launch_box_factor(Inst<T> &I)
+{
+    int grid = std::min((I.max_lines + 31) / 32, I.sm_count * 4);
+    factor_kernel<T, true><<<grid, 256, 0, I.stream>>>(I.p, I.g);
+}
+template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
+{
+    const int warps = I.exact_warps;
+    const size_t smem = (size_t)warps * 3 * I.p.nip * sizeof(T);
+    if (I.order == AMCFD_ORDER_EXACT) {
+        Status *st = I.g.st;
+        if (box)
+            sweep_exact_kernel<T, true><<<I.exact_grid, 32 * warps, smem, I.stream>>>(
+                I.p, I.g, phi, I.flags_mom, I.g.tickets_mom, 0, &st->seq_mom, &st->done_mom,
+                &st->ticket_mom);
+        else
+            sweep_exact_kernel<T, false><<<I.exact_grid, 32 * warps, smem, I.stream>>>(
+                I.p, I.g, phi, I.g.flags, I.g.tickets_energy, I.g.ntickets_energy,
+                &st->seq_energy, &st->done_energy, &st->ticket_energy);
+    } else {
+        int lines = box ? I.max_lines : (I.p.nj - 2) * (I.p.nk - 2);
+        int grid = std::max(1, std::min((lines / 2 + warps - 1) / warps + 1, I.sm_count * 16));
+        for (int sweep = 0; sweep < 4; ++sweep)
+            for (int color = 0; color < 2; ++color) {
+                if (box)
+                    sweep_rb_kernel<T, true><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
+                else
+                    sweep_rb_kernel<T, false><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
+            }
+    }
+}
+template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
+template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
+{
+    T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
+    sweeps<T>(I, phi, true);
+}
+template <typename T> void launch_box_tickets(Inst<T> &I)
+{
+    box_tickets_kernel<<<1, 1024, 0, I.stream>>>(I.p, I.g.tickets_mom, I.g.ntickets_mom, I.g.st);
+}
+
+// Occupancy of the persistent sweep (host helper used at context creation).
+template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem)
+{
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_exact_kernel<T, false>, 32 * warps, smem);
+    int nb2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, sweep_exact_kernel<T, true>, 32 * warps, smem);
+    return std::max(1, std::min(nb, nb2));
+}
+template <typename T> void set_sweep_smem_limit(size_t smem)
+{
+    cudaFuncSetAttribute(sweep_exact_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(sweep_exact_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(sweep_rb_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(sweep_rb_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+#define AMCFD_INST(T)                                                     \
+    template void launch_energy_factor<T>(Inst<T> &);                    \
+    template void launch_box_factor<T>(Inst<T> &);                       \
+    template void launch_energy_sweeps<T>(Inst<T> &);                    \
+    template void launch_box_sweeps<T>(Inst<T> &, int);                  \
+    template void launch_box_tickets<T>(Inst<T> &);                      \
+    template int exact_sweep_blocks_per_sm<T>(int, size_t);              \
+    template void set_sweep_smem_limit<T>(size_t);
+AMCFD_INST(double)
+AMCFD_INST(float)
+#undef AMCFD_INST
+
+}  // namespace amcfd

@@ -1,0 +1,512 @@
+// Momentum and pressure-correction chain over the melt-pool box
+// (iterativeLoopSolve, CFDSolverManager.cpp:660-675): cleanVelocities, then for
+// u, v, w, p': applyBCs, discretizeEquations + calculateSource +
+// calculateResiduals (fused per cell), the line solver, and correctPressure.
+// The box (istat..iend, jstat..jend, kstat..nkm1) lives in the device status
+// block, so every launch has a fixed grid and walks the box with a stride.
+#include "kernels.cuh"
+#include "amcfd.h"
+
+namespace amcfd {
+
+struct Box {
+    int i0, i1, j0, j1, k0, k1, ni_, nj_, n;
+};
+
+__device__ __forceinline__ bool get_box(const Status *st, const Params &p, Box &b)
+{
+    if (!st->momentum_active) return false;
+    b.i0 = st->istatp1; b.i1 = st->iendm1; b.j0 = st->jstat; b.j1 = st->jend;
+    b.k0 = st->kstat; b.k1 = p.nkm2;
+    b.ni_ = b.i1 - b.i0 + 1; b.nj_ = b.j1 - b.j0 + 1;
+    b.n = (b.ni_ > 0 && b.nj_ > 0 && b.k1 >= b.k0) ? b.ni_ * b.nj_ * (b.k1 - b.k0 + 1) : 0;
+    return b.n > 0;
+}
+
+__device__ __forceinline__ void box_cell(const Box &b, int q, int &i, int &j, int &k)
+{
+    i = b.i0 + q % b.ni_;
+    int r = q / b.ni_;
+    j = b.j0 + r % b.nj_;
+    k = b.k0 + r / b.nj_;
+}
+
+// cleanVelocities (CFDSolverManager.cpp:2577-2620)
+template <typename T>
+__global__ void clean_velocities_kernel(Params p, Fields<T> g)
+{
+    Box b;
+    if (!get_box(g.st, p, b)) return;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const T ts = (T)p.tsolid;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        size_t c = cidx(i, j, k, nj, nip);
+        T tc = g.temp[c];
+        if (mind(tc, g.temp[c + 1]) <= ts) g.uvel[c + 1] = T(0);
+        if (mind(tc, g.temp[c + sj]) <= ts) g.vvel[c + sj] = T(0);
+        if (mind(tc, g.temp[c + sk]) <= ts) g.wvel[c + sk] = T(0);
+    }
+}
+
+// Surface-tension gradient dsigma/dT (BoundCondManager.cpp:706-741).
+__device__ __forceinline__ double surface_tension_gradient(double t, double a0, double dgdtp)
+{
+    const double A = 4.3e-4, R = 8314, Ts = 2.03e-8, k1 = 1.38e-2, H0 = -1.46e8;
+    if (a0 < 0) return dgdtp;
+    double K = k1 * exp(-H0 / R / t);
+    double g = (-A - R * Ts * log(1 + K * a0) - (K * a0 / (1 + K * a0)) * (Ts * H0 / t)) * 1;
+    if (t >= 2500) g = 0;
+    return g;
+}
+
+// applyBCs(1..4) (BoundCondManager.cpp:472-564): Marangoni shear on the top
+// plane for u and v, zero values on the box's east/west faces.  For u it also
+// records max |u| on the top plane (the reference momentum of
+// calculateResiduals(1), CFDSolverManager.cpp:1983-1991).
+template <typename T>
+__global__ void mom_bc_kernel(Params p, Fields<T> g, int ivar, double *red_umax)
+{
+    Box b;
+    const Status *st = g.st;
+    double umax = 0.0;
+    if (get_box(st, p, b)) {
+        const int nj = p.nj, nip = p.nip, nkm1 = p.nkm1, nkm2 = p.nkm2;
+        const int istat = st->istat, iend = st->iend;
+        const int ntop = (ivar <= 2) ? b.ni_ * b.nj_ : 0;
+        const int nedge = b.nj_ * (nkm1 - b.k0);
+        T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ntop + nedge;
+             q += gridDim.x * blockDim.x) {
+            if (q < ntop) {
+                int i = b.i0 + q % b.ni_, j = b.j0 + q / b.ni_;
+                size_t ct = cidx(i, j, nkm1, nj, nip), cb = cidx(i, j, nkm2, nj, nip);
+                double tt = (double)g.temp[ct];
+                double grad, fl, vis1;
+                if (ivar == 1) {
+                    double fx = g.fracx[i - 1];
+                    grad = (tt - (double)g.temp[ct - 1]) * g.dxpwinv[i];
+                    fl = (double)g.fracl[ct] * (1.0 - fx) + (double)g.fracl[ct - 1] * fx;
+                    double vc = (double)g.vis_nxt[cb], vw = (double)g.vis_nxt[cb - 1];
+                    vis1 = vc * vw / (vc * (1.0 - fx) + vw * fx);
+                } else {
+                    double fy = g.fracy[j - 1];
+                    grad = (tt - (double)g.temp[ct - nip]) * g.dypsinv[j];
+                    fl = (double)g.fracl[ct] * (1.0 - fy) + (double)g.fracl[ct - nip] * fy;
+                    double vc = (double)g.vis_nxt[cb], vs = (double)g.vis_nxt[cb - nip];
+                    vis1 = vc * vs / (vc * (1.0 - fy) + vs * fy);
+                }
+                double term1 = fl * surface_tension_gradient(tt, p.a_oxygen, p.dgdtp) * grad /
+                               (vis1 * g.dzpbinv[nkm1]);
+                T val = (T)((double)phi[cb] + term1);
+                phi[ct] = val;
+                if (ivar == 1) umax = maxd(umax, fabs((double)val));
+            } else {
+                int r = q - ntop;
+                int j = b.j0 + r % b.nj_, k = b.k0 + r / b.nj_;
+                phi[cidx(istat, j, k, nj, nip)] = T(0);
+                phi[cidx(iend, j, k, nj, nip)] = T(0);
+            }
+        }
+    }
+    if (ivar == 1) {
+        double v[1] = {umax};
+        const int s[1] = {R_UMAX};
+        const bool m[1] = {true};
+        block_reduce_store<1>(v, s, m, red_umax, blockIdx.x);
+    }
+}
+
+// discretizeEquations(1..3) + calculateSource(1..3) + calculateResiduals(1..3)
+// (CFDSolverManager.cpp:771-1111, 1408-1644, 1960-2046), one box cell per thread.
+template <typename T>
+__global__ void __launch_bounds__(256) mom_assemble_kernel(Params p, Fields<T> g, int ivar, double *red)
+{
+    using R = T;
+    Box b;
+    const Status *st = g.st;
+    double sumd = 0.0;
+    if (get_box(st, p, b)) {
+        const int nj = p.nj, nip = p.nip, nkm1 = p.nkm1, nkm2 = p.nkm2, njm2 = p.njm2, nim2 = p.nim2;
+        const size_t sj = nip, sk = (size_t)nj * nip;
+        const int sch = p.scheme;
+        const R delt = (R)st->delt;
+        const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt, *vis = g.vis_nxt;
+        const double *fx = g.fracx, *fy = g.fracy, *fz = g.fracz, *xu = g.xu, *yv = g.yv, *zw = g.zw;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
+            int i, j, k;
+            box_cell(b, q, i, j, k);
+            const size_t c = cidx(i, j, k, nj, nip);
+            R an, as_, ae, aw, at, ab, apnot, su, sp, tmp, areaD, vol;
+            const R rc = rho[c];
+            R *phi;
+            const R *phinot;
+            size_t cn;  // upstream scalar node of the staggered cell
+            R urf, flv;
+            if (ivar == 1) {
+                const R fxm = (R)fx[i - 1];
+                R vn = v[c + sj] * (R(1) - fxm) + v[c + sj - 1] * fxm;
+                R vs = v[c] * (R(1) - fxm) + v[c - 1] * fxm;
+                R ue = (u[c + 1] + u[c]) * R(0.5);
+                R uw = (u[c - 1] + u[c]) * R(0.5);
+                R wt = w[c + sk] * (R(1) - fxm) + w[c + sk - 1] * fxm;
+                R wb = w[c] * (R(1) - fxm) + w[c - 1] * fxm;
+                const R auik = (R)area_uik(g, i, k), ajk = (R)area_jk(p, g, j, k), auij = (R)area_uij(g, i, j);
+                R fn = vn * rc * auik, fs = vs * rc * auik, fe = ue * rc * ajk, fw = uw * rc * ajk;
+                R ft = wt * rc * auij, fb = wb * rc * auij;
+                R visu = vis[c] * vis[c - 1] / (fxm * vis[c - 1] + (R(1) - fxm) * vis[c]);
+                R visun = vis[c + sj] * vis[c + sj - 1] / (fxm * vis[c + sj - 1] + (R(1) - fxm) * vis[c + sj]);
+                R visus = vis[c - sj] * vis[c - sj - 1] / (fxm * vis[c - sj - 1] + (R(1) - fxm) * vis[c - sj]);
+                R visn = (j == njm2) ? visu : visu * visun / ((R(1) - (R)fy[j]) * visun + (R)fy[j] * visu);
+                R viss = (j == 1) ? visu : visu * visus / ((R)fy[j - 1] * visus + (R(1) - (R)fy[j - 1]) * visu);
+                R vise = vis[c], visw = vis[c - 1];
+                R visut = vis[c + sk] * vis[c + sk - 1] / (fxm * vis[c + sk - 1] + (R(1) - fxm) * vis[c + sk]);
+                R visub = vis[c - sk] * vis[c - sk - 1] / (fxm * vis[c - sk - 1] + (R(1) - fxm) * vis[c - sk]);
+                R vist = (k == nkm2) ? visu : visut * visu / ((R)fz[k] * visu + (R(1) - (R)fz[k]) * visut);
+                R visb = (k == 1) ? visu : visub * visu / ((R(1) - (R)fz[k - 1]) * visu + (R)fz[k - 1] * visub);
+                R dn = visn * auik * (R)g.dypsinv[j + 1], ds = viss * auik * (R)g.dypsinv[j];
+                R de = vise * ajk / (R)(xu[i + 1] - xu[i]), dw = visw * ajk / (R)(xu[i] - xu[i - 1]);
+                R dt = vist * auij * (R)g.dzpbinv[k + 1], db = visb * auij * (R)g.dzpbinv[k];
+                face_coef<R>(sch, dn, fn, an, tmp);
+                face_coef<R>(sch, ds, fs, tmp, as_);
+                face_coef<R>(sch, de, fe, ae, tmp);
+                face_coef<R>(sch, dw, fw, tmp, aw);
+                face_coef<R>(sch, dt, ft, at, tmp);
+                face_coef<R>(sch, db, fb, tmp, ab);
+                vol = (R)volume_u(g, i, j, k);
+                apnot = rc * vol / delt;
+                R delf = fn - fs + fe - fw + ft - fb;
+                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+                su = -cp1 * u[c];
+                su += ajk * (g.pressure[c - 1] - g.pressure[c]);
+                sp = -cp0;
+                su += apnot * g.unot[c];
+                R dudxp = (u[c + 1] - u[c]) / (R)(xu[i + 1] - xu[i]);
+                R dudxm = (u[c] - u[c - 1]) / (R)(xu[i] - xu[i - 1]);
+                su += (vise * dudxp - visw * dudxm) * ajk;
+                R dvdxp = (v[c + sj] - v[c + sj - 1]) * (R)g.dxpwinv[i];
+                R dvdxm = (v[c] - v[c - 1]) * (R)g.dxpwinv[i];
+                su += (visn * dvdxp - viss * dvdxm) * auik;
+                R dwdxp = (w[c + sk] - w[c + sk - 1]) * (R)g.dxpwinv[i];
+                R dwdxm = (w[c] - w[c - 1]) * (R)g.dxpwinv[i];
+                su += (vist * dwdxp - visb * dwdxm) * auij;
+                phi = g.uvel; phinot = g.unot; cn = c - 1; urf = (R)p.urfu; areaD = ajk;
+                flv = g.fracl[c] * (R(1) - fxm) + g.fracl[c - 1] * fxm;
+            } else if (ivar == 2) {
+                const R fym = (R)fy[j - 1];
+                R vn = (v[c] + v[c + sj]) * R(0.5);
+                R vs = (v[c] + v[c - sj]) * R(0.5);
+                R ue = u[c + 1] * (R(1) - fym) + u[c + 1 - sj] * fym;
+                R uw = u[c] * (R(1) - fym) + u[c - sj] * fym;
+                R wt = w[c + sk] * (R(1) - fym) + w[c + sk - sj] * fym;
+                R wb = w[c] * (R(1) - fym) + w[c - sj] * fym;
+                const R aik = (R)area_ik(p, g, i, k), avjk = (R)area_vjk(g, j, k), avij = (R)area_vij(g, i, j);
+                R fn = vn * rc * aik, fs = vs * rc * aik, fe = ue * rc * avjk, fw = uw * rc * avjk;
+                R ft = wt * rc * avij, fb = wb * rc * avij;
+                R visn = vis[c], viss = vis[c - sj];
+                R visv = vis[c] * vis[c - sj] / (fym * vis[c - sj] + (R(1) - fym) * vis[c]);
+                R visve = vis[c + 1] * vis[c + 1 - sj] / (fym * vis[c + 1 - sj] + (R(1) - fym) * vis[c + 1]);
+                R visvw = vis[c - 1] * vis[c - 1 - sj] / (fym * vis[c - 1 - sj] + (R(1) - fym) * vis[c - 1]);
+                R vise = (i == nim2) ? visv : visv * visve / ((R(1) - (R)fx[i]) * visve + (R)fx[i] * visv);
+                R visw = (i == 1) ? visv : visv * visvw / ((R)fx[i - 1] * visvw + (R(1) - (R)fx[i - 1]) * visv);
+                R visvt = vis[c + sk] * vis[c + sk - sj] / (fym * vis[c + sk - sj] + (R(1) - fym) * vis[c + sk]);
+                R visvb = vis[c - sk] * vis[c - sk - sj] / (fym * vis[c - sk - sj] + (R(1) - fym) * vis[c - sk]);
+                R vist = (k == nkm2) ? visv : visv * visvt / ((R(1) - (R)fz[k]) * visvt + (R)fz[k] * visv);
+                R visb = (k == 1) ? visv : visv * visvb / ((R)fz[k - 1] * visvb + (R(1) - (R)fz[k - 1]) * visv);
+                R dn = visn * aik / (R)(yv[j + 1] - yv[j]), ds = viss * aik / (R)(yv[j] - yv[j - 1]);
+                R de = vise * avjk * (R)g.dxpwinv[i + 1], dw = visw * avjk * (R)g.dxpwinv[i];
+                R dt = vist * avij * (R)g.dzpbinv[k + 1], db = visb * avij * (R)g.dzpbinv[k];
+                face_coef<R>(sch, dn, fn, an, tmp);
+                face_coef<R>(sch, ds, fs, tmp, as_);
+                face_coef<R>(sch, de, fe, ae, tmp);
+                face_coef<R>(sch, dw, fw, tmp, aw);
+                face_coef<R>(sch, dt, ft, at, tmp);
+                face_coef<R>(sch, db, fb, tmp, ab);
+                vol = (R)volume_v(g, i, j, k);
+                apnot = rc * vol / delt;
+                R delf = fn - fs + fe - fw + ft - fb;
+                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+                su = -cp1 * v[c];
+                su += aik * (g.pressure[c - sj] - g.pressure[c]);
+                sp = -cp0;
+                su += apnot * g.vnot[c];
+                R dudyp = (u[c + 1] - u[c + 1 - sj]) * (R)g.dypsinv[j];
+                R dudym = (u[c] - u[c - sj]) * (R)g.dypsinv[j];
+                su += (vise * dudyp - visw * dudym) * avjk;
+                R dvdyp = (v[c + sj] - v[c]) / (R)(yv[j + 1] - yv[j]);
+                R dvdym = (v[c] - v[c - sj]) / (R)(yv[j] - yv[j - 1]);
+                su += (visn * dvdyp - viss * dvdym) * aik;
+                R dwdyp = (w[c + sk] - w[c + sk - sj]) * (R)g.dypsinv[j];
+                R dwdym = (w[c] - w[c - sj]) * (R)g.dypsinv[j];
+                su += (vist * dwdyp - visb * dwdym) * avij;
+                phi = g.vvel; phinot = g.vnot; cn = c - sj; urf = (R)p.urfv; areaD = aik;
+                flv = g.fracl[c] * (R(1) - fym) + g.fracl[c - sj] * fym;
+            } else {
+                const R fzm = (R)fz[k - 1];
+                R vn = v[c + sj] * (R(1) - fzm) + v[c + sj - sk] * fzm;
+                R vs = v[c] * (R(1) - fzm) + v[c - sk] * fzm;
+                R ue = u[c + 1] * (R(1) - fzm) + u[c + 1 - sk] * fzm;
+                R uw = u[c] * (R(1) - fzm) + u[c - sk] * fzm;
+                R wt = (w[c] + w[c + sk]) * R(0.5);
+                R wb = (w[c] + w[c - sk]) * R(0.5);
+                const R awik = (R)area_wik(g, i, k), awjk = (R)area_wjk(g, j, k), aij = (R)area_ij(p, g, i, j);
+                R fn = vn * rc * awik, fs = vs * rc * awik, fe = ue * rc * awjk, fw = uw * rc * awjk;
+                R ft = wt * rc * aij, fb = wb * rc * aij;
+                R vis_w = vis[c] * vis[c - sk] / (fzm * vis[c - sk] + (R(1) - fzm) * vis[c]);
+                R viswn = vis[c + sj] * vis[c + sj - sk] / (fzm * vis[c + sj - sk] + (R(1) - fzm) * vis[c + sj]);
+                R visws = vis[c - sj] * vis[c - sj - sk] / (fzm * vis[c - sj - sk] + (R(1) - fzm) * vis[c - sj]);
+                R visn = (j == njm2) ? vis_w : vis_w * viswn / ((R(1) - (R)fy[j]) * viswn + (R)fy[j] * vis_w);
+                R viss = (j == 1) ? vis_w : vis_w * visws / ((R)fy[j - 1] * visws + (R(1) - (R)fy[j - 1]) * vis_w);
+                R viswe = vis[c + 1] * vis[c + 1 - sk] / (fzm * vis[c + 1 - sk] + (R(1) - fzm) * vis[c + 1]);
+                R visww = vis[c - 1] * vis[c - 1 - sk] / (fzm * vis[c - 1 - sk] + (R(1) - fzm) * vis[c - 1]);
+                R vise = (i == nim2) ? vis_w : vis_w * viswe / ((R(1) - (R)fx[i]) * viswe + (R)fx[i] * vis_w);
+                R visw = (i == 1) ? vis_w : vis_w * visww / ((R)fx[i - 1] * visww + (R(1) - (R)fx[i - 1]) * vis_w);
+                R vist = vis[c], visb = vis[c - sk];
+                R dn = visn * awik * (R)g.dypsinv[j + 1], ds = viss * awik * (R)g.dypsinv[j];
+                R de = vise * awjk * (R)g.dxpwinv[i + 1], dw = visw * awjk * (R)g.dxpwinv[i];
+                R dt = vist * aij / (R)(zw[k + 1] - zw[k]), db = visb * aij / (R)(zw[k] - zw[k - 1]);
+                face_coef<R>(sch, dn, fn, an, tmp);
+                face_coef<R>(sch, ds, fs, tmp, as_);
+                face_coef<R>(sch, de, fe, ae, tmp);
+                face_coef<R>(sch, dw, fw, tmp, aw);
+                face_coef<R>(sch, dt, ft, at, tmp);
+                face_coef<R>(sch, db, fb, tmp, ab);
+                vol = (R)volume_w(g, i, j, k);
+                apnot = rc * vol / delt;
+                R delf = fn - fs + fe - fw + ft - fb;
+                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+                su = -cp1 * w[c];
+                su += aij * (g.pressure[c - sk] - g.pressure[c]);
+                sp = -cp0;
+                su += apnot * g.wnot[c];
+                R dudzp = (u[c + 1] - u[c + 1 - sk]) * (R)g.dzpbinv[k];
+                R dudzm = (u[c] - u[c - sk]) * (R)g.dzpbinv[k];
+                su += (vise * dudzp - visw * dudzm) * awjk;
+                R dvdzp = (v[c + sj] - v[c + sj - sk]) * (R)g.dzpbinv[k];
+                R dvdzm = (v[c] - v[c - sk]) * (R)g.dzpbinv[k];
+                su += (visn * dvdzp - viss * dvdzm) * awik;
+                R dwdzp = (w[c + sk] - w[c]) / (R)(zw[k + 1] - zw[k]);
+                R dwdzm = (w[c] - w[c - sk]) / (R)(zw[k] - zw[k - 1]);
+                su += (vist * dwdzp - visb * dwdzm) * aij;
+                phi = g.wvel; phinot = g.wnot; cn = c - sk; urf = (R)p.urfw; areaD = aij;
+                flv = g.fracl[c] * (R(1) - fzm) + g.fracl[c - sk] * fzm;
+            }
+            (void)phinot;
+            // ---- calculateSource ----
+            if (flv > R(0)) {
+                R term = (R)p.darcyKo * ((R(1) - flv) * (R(1) - flv)) / ((flv * flv * flv) + (R)kSmall);
+                sp -= term * vol;
+                if (p.steady) {
+                    R area = ivar == 1 ? (R)area_jk(p, g, j, k) : ivar == 2 ? (R)area_vjk(g, j, k)
+                                                                            : (R)area_wjk(g, j, k);
+                    su += rc * (R)st->scanvel * area * (phi[c - 1] - phi[c]);
+                }
+                if (ivar == 3) {
+                    R fzm = (R)fz[k - 1];
+                    R boufac = rc * (R)p.grav * (R)p.beta;
+                    R tw = g.temp[c] * (R(1) - fzm) + g.temp[c - sk] * fzm;
+                    su += boufac * vol * (tw - (R)p.tsolid);
+                }
+            }
+            if (ivar != 3 && k == nkm2) {
+                su += at * phi[c + sk];
+                sp -= at;
+                at = R(0);
+            }
+            R ap = an + as_ + ae + aw + at + ab + apnot - sp;
+            R dcoef = areaD / ap;
+            ap /= urf;
+            su += (R(1) - urf) * ap * phi[c];
+            dcoef *= urf;
+            if (mind(g.temp[c], g.temp[cn]) <= (R)p.tsolid) {
+                su = R(0);
+                an = as_ = ae = aw = at = ab = R(0);
+                ap = (R)kLarge;
+            }
+            g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
+            g.ap[c] = ap; g.su[c] = su;
+            (ivar == 1 ? g.dux : ivar == 2 ? g.dvy : g.dwz)[c] = dcoef;
+            R r = an * phi[c + sj] + as_ * phi[c - sj] + ae * phi[c + 1] + aw * phi[c - 1] +
+                  at * phi[c + sk] + ab * phi[c - sk] + su - ap * phi[c];
+            sumd += fabs((double)r);
+            (void)nkm1;
+        }
+    }
+    double v[1] = {sumd};
+    const int s[1] = {R_MSUMD};
+    const bool m[1] = {false};
+    block_reduce_store<1>(v, s, m, red, blockIdx.x);
+}
+
+// discretizeEquations(4) + calculateSource(4) + calculateResiduals(4)
+// (CFDSolverManager.cpp:1112-1156, 1645-1676, 2047-2071).
+template <typename T>
+__global__ void __launch_bounds__(256) pp_assemble_kernel(Params p, Fields<T> g, double *red)
+{
+    using R = T;
+    Box b;
+    const Status *st = g.st;
+    double resorm = 0.0, denom = 0.0;
+    if (get_box(st, p, b)) {
+        const int nj = p.nj, nip = p.nip;
+        const size_t sj = nip, sk = (size_t)nj * nip;
+        const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt;
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
+            int i, j, k;
+            box_cell(b, q, i, j, k);
+            const size_t c = cidx(i, j, k, nj, nip);
+            const R rc = rho[c];
+            const R aik = (R)area_ik(p, g, i, k), ajk = (R)area_jk(p, g, j, k), aij = (R)area_ij(p, g, i, j);
+            R an = aik * g.dvy[c + sj] * rc;
+            R as_ = aik * g.dvy[c] * rc;
+            R ae = ajk * g.dux[c + 1] * rc;
+            R aw = ajk * g.dux[c] * rc;
+            R at = aij * g.dwz[c + sk] * rc;
+            R ab = aij * g.dwz[c] * rc;
+            R fn = v[c + sj] * aik * rc, fs = v[c] * aik * rc;
+            R fe = u[c + 1] * ajk * rc, fw = u[c] * ajk * rc;
+            R ft = w[c + sk] * aij * rc, fb = w[c] * aij * rc;
+            R delf = fn - fs + fe - fw + ft - fb;
+            R sp = R(0), su = -delf;
+            resorm += fabs((double)delf);
+            R ap = an + as_ + ae + aw + at + ab - sp;
+            if (g.temp[c] <= (R)p.tsolid) {
+                su = R(0);
+                an = as_ = ae = aw = at = ab = R(0);
+                ap = (R)kLarge;
+            }
+            g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
+            g.ap[c] = ap; g.su[c] = su;
+            double dtp = (fabs((double)u[c]) + fabs((double)u[c + 1])) * (double)ajk +
+                         (fabs((double)v[c]) + fabs((double)v[c + sj])) * (double)aik +
+                         (fabs((double)w[c]) + fabs((double)w[c + sk])) * (double)aij;
+            denom += 0.5 * fabs(dtp);
+        }
+    }
+    double vv[2] = {resorm, denom};
+    const int s[2] = {R_MRESORM, R_MDENOM};
+    const bool m[2] = {false, false};
+    block_reduce_store<2>(vv, s, m, red, blockIdx.x);
+}
+
+// correctPressure (CFDSolverManager.cpp:2692-2758): velocity correction, then
+// pressure update (two launches: the second zeroes p' that the first reads).
+template <typename T>
+__global__ void correct_velocity_kernel(Params p, Fields<T> g)
+{
+    Box b;
+    if (!get_box(g.st, p, b)) return;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const T ts = (T)p.tsolid;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        size_t c = cidx(i, j, k, nj, nip);
+        T tc = g.temp[c], ppc = g.pp[c];
+        if (mind(tc, g.temp[c - 1]) > ts) g.uvel[c] += g.dux[c] * (g.pp[c - 1] - ppc);
+        if (mind(tc, g.temp[c - sj]) > ts) g.vvel[c] += g.dvy[c] * (g.pp[c - sj] - ppc);
+        if (mind(tc, g.temp[c - sk]) > ts) g.wvel[c] += g.dwz[c] * (g.pp[c - sk] - ppc);
+    }
+}
+template <typename T>
+__global__ void correct_pressure_kernel(Params p, Fields<T> g)
+{
+    Box b;
+    if (!get_box(g.st, p, b)) return;
+    const int nj = p.nj, nip = p.nip;
+    const T ts = (T)p.tsolid, urfp = (T)p.urfp;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        size_t c = cidx(i, j, k, nj, nip);
+        if (g.temp[c] > ts) {
+            g.pressure[c] += urfp * g.pp[c];
+            g.pp[c] = T(0);
+        }
+    }
+}
+
+// Momentum residual normalisation (CFDSolverManager.cpp:1983-1991, 2018, 2044,
+// 2069-2070), one CTA.
+__device__ double reduce_region(const double *red, int nb, int slot, bool is_max, double *scratch)
+{
+    double acc = is_max ? -INFINITY : 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        double x = red[(size_t)b * R_NSLOTS + slot];
+        acc = is_max ? fmax(acc, x) : acc + x;
+    }
+    acc = is_max ? warp_max(acc) : warp_sum(acc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        double r = (lane < (int)(blockDim.x >> 5)) ? scratch[lane] : (is_max ? -INFINITY : 0.0);
+        r = is_max ? warp_max(r) : warp_sum(r);
+        if (lane == 0) scratch[32] = r;
+    }
+    __syncthreads();
+    double r = scratch[32];
+    __syncthreads();
+    return r;
+}
+
+template <typename T>
+__global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, int nb)
+{
+    __shared__ double scratch[40];
+    Status *st = g.st;
+    if (!st->momentum_active) return;
+    const size_t region = (size_t)nb * R_NSLOTS;
+    double s1 = reduce_region(red + 0 * region, nb, R_MSUMD, false, scratch);
+    double s2 = reduce_region(red + 1 * region, nb, R_MSUMD, false, scratch);
+    double s3 = reduce_region(red + 2 * region, nb, R_MSUMD, false, scratch);
+    double rm = reduce_region(red + 3 * region, nb, R_MRESORM, false, scratch);
+    double dn = reduce_region(red + 3 * region, nb, R_MDENOM, false, scratch);
+    double umax = reduce_region(red + 4 * region, nb, R_UMAX, true, scratch);
+    if (threadIdx.x == 0) {
+        umax = fmax(umax, 0.0);
+        double refmom = 0.25 * M_PI * (st->width * st->width) * p.dens * (umax * umax);
+        st->umaxt = umax;
+        st->refmom = refmom;
+        st->resoru = s1 / refmom;
+        st->resorv = s2 / refmom;
+        st->resorw = s3 / refmom;
+        dn *= p.dens;
+        st->mass_denom = dn;
+        st->resorm = rm / (dn + kSmall);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launcher: the whole momentum chain of one outer iteration
+// ---------------------------------------------------------------------------
+template <typename T> void launch_momentum(Inst<T> &I)
+{
+    const int nb = I.nb_mom;
+    const size_t region = (size_t)nb * R_NSLOTS;
+    launch_box_tickets<T>(I);
+    clean_velocities_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
+    for (int ivar = 1; ivar <= 4; ++ivar) {
+        mom_bc_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + 4 * region);
+        if (ivar <= 3)
+            mom_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * region);
+        else
+            pp_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * region);
+        launch_box_factor<T>(I);
+        launch_box_sweeps<T>(I, ivar);
+        if (ivar == 4) {
+            correct_velocity_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
+            correct_pressure_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
+        }
+    }
+    mom_finalize_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_mom, nb);
+}
+
+template void launch_momentum<double>(Inst<double> &);
+template void launch_momentum<float>(Inst<float> &);
+
+}  // namespace amcfd

@@ -1,0 +1,103 @@
+// Geometry helpers, the host-side instance record and the kernel launchers.
+#pragma once
+#include <cstdio>
+#include "dev.cuh"
+
+namespace amcfd {
+
+// Face areas and control volumes (CFDSolverManager.cpp:243-286), recomputed
+// from the 1-D metrics with the reference's products.  The reference arrays
+// are only filled for interior indices and are zero elsewhere; so are these.
+template <typename T>
+__device__ __forceinline__ double area_ij(const Params &p, const Fields<T> &g, int i, int j)
+{
+    if (i < 1 || i > p.nim2 || j < 1 || j > p.njm2) return 0.0;
+    return (g.xu[i + 1] - g.xu[i]) * (g.yv[j + 1] - g.yv[j]);
+}
+template <typename T>
+__device__ __forceinline__ double area_ik(const Params &p, const Fields<T> &g, int i, int k)
+{
+    if (i < 1 || i > p.nim2 || k < 1 || k > p.nkm2) return 0.0;
+    return (g.xu[i + 1] - g.xu[i]) * (g.zw[k + 1] - g.zw[k]);
+}
+template <typename T>
+__device__ __forceinline__ double area_jk(const Params &p, const Fields<T> &g, int j, int k)
+{
+    if (j < 1 || j > p.njm2 || k < 1 || k > p.nkm2) return 0.0;
+    return (g.yv[j + 1] - g.yv[j]) * (g.zw[k + 1] - g.zw[k]);
+}
+template <typename T>
+__device__ __forceinline__ double volume_p(const Params &p, const Fields<T> &g, int i, int j, int k)
+{
+    return (g.xu[i + 1] - g.xu[i]) * (g.yv[j + 1] - g.yv[j]) * (g.zw[k + 1] - g.zw[k]);
+}
+// staggered-cell areas/volumes of the momentum equations
+template <typename T>
+__device__ __forceinline__ double area_uij(const Fields<T> &g, int i, int j)
+{ return (g.x[i] - g.x[i - 1]) * (g.yv[j + 1] - g.yv[j]); }
+template <typename T>
+__device__ __forceinline__ double area_vij(const Fields<T> &g, int i, int j)
+{ return (g.xu[i + 1] - g.xu[i]) * (g.y[j] - g.y[j - 1]); }
+template <typename T>
+__device__ __forceinline__ double area_uik(const Fields<T> &g, int i, int k)
+{ return (g.x[i] - g.x[i - 1]) * (g.zw[k + 1] - g.zw[k]); }
+template <typename T>
+__device__ __forceinline__ double area_wik(const Fields<T> &g, int i, int k)
+{ return (g.xu[i + 1] - g.xu[i]) * (g.z[k] - g.z[k - 1]); }
+template <typename T>
+__device__ __forceinline__ double area_vjk(const Fields<T> &g, int j, int k)
+{ return (g.y[j] - g.y[j - 1]) * (g.zw[k + 1] - g.zw[k]); }
+template <typename T>
+__device__ __forceinline__ double area_wjk(const Fields<T> &g, int j, int k)
+{ return (g.yv[j + 1] - g.yv[j]) * (g.z[k] - g.z[k - 1]); }
+template <typename T>
+__device__ __forceinline__ double volume_u(const Fields<T> &g, int i, int j, int k)
+{ return (g.x[i] - g.x[i - 1]) * (g.yv[j + 1] - g.yv[j]) * (g.zw[k + 1] - g.zw[k]); }
+template <typename T>
+__device__ __forceinline__ double volume_v(const Fields<T> &g, int i, int j, int k)
+{ return (g.xu[i + 1] - g.xu[i]) * (g.y[j] - g.y[j - 1]) * (g.zw[k + 1] - g.zw[k]); }
+template <typename T>
+__device__ __forceinline__ double volume_w(const Fields<T> &g, int i, int j, int k)
+{ return (g.xu[i + 1] - g.xu[i]) * (g.yv[j + 1] - g.yv[j]) * (g.z[k] - g.z[k - 1]); }
+
+// Host-side record of one instance on the device.
+template <typename T>
+struct Inst {
+    Params p;
+    Fields<T> g;
+    cudaStream_t stream = nullptr;
+    int sm_count = 148;
+    int order = 0;
+    int check_finite = 0;
+    // reduction regions (per-CTA partials)
+    double *red_las = nullptr, *red_bc = nullptr, *red_asm = nullptr, *red_h2t = nullptr,
+           *red_mom = nullptr;
+    int nb_las = 0, nb_bc = 0, nb_asm = 0, nb_h2t = 0, nb_mom = 0;
+    dim3 asm_grid;
+    int grid_1d = 0;          // grid of the pointwise kernels
+    int exact_grid = 0;       // CTAs of the persistent exact-order line sweep
+    int exact_warps = 4;      // warps per CTA in the line sweeps
+    size_t line_smem = 0;     // dynamic smem of a line-sweep CTA
+    int *flags_mom = nullptr;
+    int max_lines = 0;        // (nj-2)*(nk-2)
+};
+
+// launchers (k_energy.cu)
+template <typename T> void launch_laser(Inst<T> &I);
+template <typename T> void launch_energy_bc(Inst<T> &I);
+template <typename T> void launch_energy_assemble(Inst<T> &I);
+template <typename T> void launch_block_correct(Inst<T> &I);
+template <typename T> void launch_h2t(Inst<T> &I);
+template <typename T> void launch_meltpool(Inst<T> &I);
+template <typename T> void launch_converge(Inst<T> &I, double tol);
+template <typename T> void launch_update_solutions(Inst<T> &I);
+// line solvers (k_linesolve.cu)
+template <typename T> void launch_energy_factor(Inst<T> &I);
+template <typename T> void launch_energy_sweeps(Inst<T> &I);
+template <typename T> void launch_box_factor(Inst<T> &I);
+template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
+template <typename T> void launch_box_tickets(Inst<T> &I);
+// momentum (k_momentum.cu)
+template <typename T> void launch_momentum(Inst<T> &I);
+
+}  // namespace amcfd

@@ -164,22 +164,32 @@ int amcfd_dims(const amcfd_ctx *ctx, int *ni, int *nj, int *nk);
 /* Kernel-level entry points for parity tests: run one phase of an outer
  * iteration on the current device state (the reference function each phase
  * replaces is listed in amcfd_phase_name). */
-#define AMCFD_PHASE_LASER 1          /* BoundCondManager::updateLaser */
-#define AMCFD_PHASE_ENERGY_ASSEMBLE 2 /* applyBCs(5)+discretizeEquations(5)+calculateSource(5) */
-#define AMCFD_PHASE_ENERGY_RESIDUAL 3 /* calculateResiduals(5) */
-#define AMCFD_PHASE_PROPS 4          /* bareplateMaterialProps */
-#define AMCFD_PHASE_BLOCK_CORRECT 5  /* enhanceConvergenceSpeed(5) */
-#define AMCFD_PHASE_ENERGY_SOLVE 6   /* solveEntireDomain(5) */
-#define AMCFD_PHASE_H2T 7            /* convertEnthalpyToTemp */
-#define AMCFD_PHASE_MELTPOOL 8       /* getMeltPoolShape */
-#define AMCFD_PHASE_MOMENTUM 9       /* cleanVelocities + ivar 1..4 chain */
-#define AMCFD_PHASE_FLUXES 10        /* calculateFluxes */
-#define AMCFD_PHASE_UPDATE 11        /* updateSolutions */
+/* 1: main.cpp:136-141, timet += delt and BoundCondManager::updateLaser */
+#define AMCFD_PHASE_LASER 1
+/* 2: applyBCs(5), discretizeEquations(5), calculateSource(5), calculateResiduals(5),
+ *    bareplateMaterialProps (into "diff_next"/"rho_next"/"vis_next") and the
+ *    block-correction solve of enhanceConvergenceSpeed(5) (CFDSolverManager.cpp:619-626) */
+#define AMCFD_PHASE_ENERGY_ASSEMBLE 2
+/* 3: the block-correction update and solveEntireDomain(5) (:626-642) */
+#define AMCFD_PHASE_ENERGY_SOLVE 3
+/* 4: convertEnthalpyToTemp (:643) */
+#define AMCFD_PHASE_H2T 4
+/* 5: getMeltPoolShape (:657) */
+#define AMCFD_PHASE_MELTPOOL 5
+/* 6: cleanVelocities and the u, v, w, p' chain (:660-675) */
+#define AMCFD_PHASE_MOMENTUM 6
+/* 7: calculateFluxes and the convergence test (:689-716); the new properties become current */
+#define AMCFD_PHASE_CONVERGE 7
+/* 8: CFDSolverManager::updateSolutions */
+#define AMCFD_PHASE_UPDATE 8
 int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report);
 const char *amcfd_phase_name(int phase);
 
 /* Device time of the last amcfd_step split by kernel family (ms); n entries. */
 int amcfd_last_timing(const amcfd_ctx *ctx, double *ms, int n);
+/* Enable (1) or disable (0) the per-phase CUDA-event timing read by amcfd_last_timing;
+ * clears the accumulated times. */
+int amcfd_profile(amcfd_ctx *ctx, int enable);
 
 #ifdef __cplusplus
 }

@@ -1360,7 +1360,6 @@ int orc_outer_iteration(orc *o)
 void orc_outer_loop(orc *o)
 {
     double alenold = o->alen;
-    o->niter = 0;
     while (o->niter < o->p.maxit)
         if (orc_outer_iteration(o)) return;
     if (fabs(o->alen - alenold) < 1.0e-6) o->steadylength = 1;
@@ -1383,8 +1382,9 @@ void orc_report(const orc *o, amcfd_step_report *r)
     r->momentum_cells = o->last_box_cells;
 }
 
-/* One time step, main.cpp:125-162. */
-void orc_step(orc *o, amcfd_step_report *r)
+/* Start of a time step, main.cpp:125-141: variable time step, timet += delt,
+ * updateLaser; resets the outer-iteration counter. */
+void orc_begin_step(orc *o)
 {
     if (o->p.nvardt > 0) {
         if (o->timet > o->vardt[3 * o->vardt_state] && o->vardt_state < o->p.nvardt - 1)
@@ -1394,6 +1394,13 @@ void orc_step(orc *o, amcfd_step_report *r)
     }
     o->timet += o->p.delt;
     if (!o->p.steady) orc_update_laser(o);
+    o->niter = 0;
+}
+
+/* One time step, main.cpp:125-162. */
+void orc_step(orc *o, amcfd_step_report *r)
+{
+    orc_begin_step(o);
     orc_outer_loop(o);
     if (!o->p.steady) orc_update_solutions(o);
     if (r) orc_report(o, r);

@@ -1,0 +1,154 @@
+"""GPU parity: the CUDA path through the C ABI against the CPU oracle.
+
+FP64, exact sweep order: the GPU reproduces the reference iterates, so every
+step must take the same number of outer iterations and the fields must agree
+to 1e-8 relative L2 (the residual differences are rounding from the order of
+FP64 reductions and fused multiply-adds).  Melt-pool box indices must be
+identical and L/D/W agree to 1e-8 relative.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl")
+TOL = 1e-8
+
+
+def _pair(deck, deckdir, **kw):
+    import amcfd
+    import oracle_py
+    path = deck.write(deckdir)
+    d = amcfd.Deck(path)
+    return d, amcfd.Solver(d, **kw), oracle_py.Oracle(d.params)
+
+
+def _cmp_fields(gpu, orc, fields=FIELDS, tol=TOL, where=""):
+    for f in fields:
+        a, b = gpu.get(f), orc.field(f)
+        err = rel_l2(a, b)
+        if np.linalg.norm(b) == 0:
+            assert np.max(np.abs(a)) < 1e-12, (where, f)
+        else:
+            assert err < tol, (where, f, err)
+
+
+def _cmp_report(rg, ro, where=""):
+    assert rg["niter"] == ro["niter"], (where, rg["niter"], ro["niter"])
+    for k in ("istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator"):
+        assert rg[k] == ro[k], (where, k, rg[k], ro[k])
+    for k in ("tpeak", "alen", "depth", "width", "ratio", "heatinlaser"):
+        a, b = rg[k], ro[k]
+        assert abs(a - b) <= 1e-8 * max(abs(b), 1e-12) + 1e-14, (where, k, a, b)
+
+
+@pytest.mark.parametrize("variant", ["base", "noflow", "upwind", "toolpath", "cooling", "p150"])
+def test_exact_fp64_steps(variant, deckdir):
+    import amcfd
+    import amcfd_decks as D
+    kw = dict(name=variant, steps=4)
+    if variant == "noflow":
+        kw["fluid_flow"] = False
+    elif variant == "upwind":
+        kw["scheme"] = "upwind"
+    elif variant == "toolpath":
+        kw["toolpath"] = True
+    elif variant == "cooling":
+        kw.update(steps=6, laser_off_after=3)
+    elif variant == "p150":
+        kw["power"] = 150.0
+    deck, gpu, orc = _pair(D.small(**kw), deckdir, order=amcfd.ORDER_EXACT,
+                           precision=amcfd.PREC_FP64)
+    for s in range(kw["steps"]):
+        rg, ro = gpu.step(), orc.step()
+        _cmp_report(rg, ro, where=f"{variant} step {s + 1}")
+        _cmp_fields(gpu, orc, where=f"{variant} step {s + 1}")
+    gpu.close()
+
+
+def test_exact_fp64_phases(deckdir):
+    """Phase by phase through the first two outer iterations of steps 1 and 2."""
+    import amcfd
+    import amcfd_decks as D
+    deck, gpu, orc = _pair(D.small("phases", steps=2), deckdir)
+    for step in range(2):
+        gpu.run_phase("laser")
+        orc.call("begin_step")
+        for it in range(2):
+            gpu.run_phase("energy_assemble")
+            orc.call("energy_assemble")
+            orc.call("residual", 5)
+            orc.call("props")
+            where = f"step {step + 1} iter {it + 1}"
+            for f in ("an", "as", "ae", "aw", "at", "ab", "ap", "su"):
+                a, b = gpu.get(f)[1:-1, 1:-1, 1:-1], orc.field(f)[1:-1, 1:-1, 1:-1]
+                assert rel_l2(a, b) < 1e-12, (where, f, rel_l2(a, b))
+            _cmp_fields(gpu, orc, ("enthalpy",), 1e-13, where)
+            for f, g in (("diff_next", "diff"), ("rho_next", "rho"), ("vis_next", "vis")):
+                assert rel_l2(gpu.get(f), orc.field(g)) < 1e-13, (where, f)
+            gpu.run_phase("energy_solve")
+            orc.call("block_correct")
+            orc.call("solve_entire")
+            _cmp_fields(gpu, orc, ("enthalpy",), 1e-10, where + " solve")
+            gpu.run_phase("h2t")
+            orc.call("h2t")
+            _cmp_fields(gpu, orc, ("temp", "fracl"), 1e-10, where + " h2t")
+            r = gpu.run_phase("meltpool")
+            orc.call("meltpool")
+            ro = orc.report()
+            for k in ("istat", "iend", "jstat", "jend", "kstat"):
+                assert r[k] == ro[k], (where, k)
+            assert abs(r["tpeak"] - ro["tpeak"]) < 1e-9 * ro["tpeak"]
+            gpu.run_phase("momentum")
+            orc.call("momentum")
+            _cmp_fields(gpu, orc, ("uvel", "vvel", "wvel", "pressure", "pp"), 1e-9, where + " mom")
+            r = gpu.run_phase("converge")
+            orc.call("fluxes")
+            ro = orc.report()
+            for k in ("resorm", "resoru", "resorv", "resorw", "ratio"):
+                assert abs(r[k] - ro[k]) <= 1e-7 * abs(ro[k]) + 1e-300, (where, k, r[k], ro[k])
+        gpu.run_phase("update")
+        orc.call("update_solutions")
+        _cmp_fields(gpu, orc, where=f"step {step + 1} end")
+    gpu.close()
+
+
+@pytest.mark.parametrize("flow,tol", [(False, 1e-9), (True, 1e-4)])
+def test_redblack_converges_to_same_solution(flow, tol, deckdir):
+    """The parallel red-black ordering and the exact order are two iterations
+    for the same discrete equations: with the outer loop run to 60 iterations
+    (tolerance 1e-12 is never met, so both stop at maxit) the energy-only
+    solutions agree to rounding, and with fluid flow to the remaining
+    outer-iteration error."""
+    import amcfd
+    import amcfd_decks as D
+    dk = D.small("rb", steps=2, maxit=60, fluid_flow=flow)
+    dk.tol = 1e-12
+    path = dk.write(deckdir)
+    d = amcfd.Deck(path)
+    ex = amcfd.Solver(d, order=amcfd.ORDER_EXACT)
+    rb = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK)
+    for _ in range(2):
+        ex.step()
+        rb.step()
+    assert rel_l2(rb.get("temp"), ex.get("temp")) < tol
+    assert rel_l2(rb.get("enthalpy"), ex.get("enthalpy")) < tol
+    ex.close()
+    rb.close()
+
+
+def test_fp32_close_to_fp64(deckdir):
+    import amcfd
+    import amcfd_decks as D
+    path = D.small("fp32", steps=3).write(deckdir)
+    d = amcfd.Deck(path)
+    s64 = amcfd.Solver(d, precision=amcfd.PREC_FP64)
+    s32 = amcfd.Solver(d, precision=amcfd.PREC_FP32)
+    for _ in range(3):
+        s64.step()
+        s32.step()
+    assert rel_l2(s32.get("temp"), s64.get("temp")) < 1e-3
+    s64.close()
+    s32.close()
