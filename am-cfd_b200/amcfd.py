@@ -112,6 +112,10 @@ def lib() -> C.CDLL:
             L.amcfd_phase_name.argtypes = [_I]
             L.amcfd_phase_name.restype = C.c_char_p
             L.amcfd_last_timing.argtypes = [VP, P(_D), _I]
+            L.amcfd_profile.argtypes = [VP, _I]
+            L.amcfd_run_steps.argtypes = [VP, _I, P(AmcfdReport), P(_D)]
+            L.amcfd_kernel_launches.argtypes = [VP]
+            L.amcfd_kernel_launches.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -203,10 +207,30 @@ class Solver:
         self._check(lib().amcfd_get_grid(self._h, name.encode(), out.ctypes.data_as(C.POINTER(_D))))
         return out
 
-    def timing(self, n: int = 16) -> np.ndarray:
+    def run_steps(self, n: int):
+        """n time steps; returns (last report, device milliseconds of the n steps)."""
+        ms = C.c_double()
+        self._check(lib().amcfd_run_steps(self._h, n, C.byref(self.report), C.byref(ms)))
+        return self.report.as_dict(), ms.value
+
+    def profile(self, enable: bool = True):
+        self._check(lib().amcfd_profile(self._h, 1 if enable else 0))
+
+    @property
+    def launches(self) -> int:
+        return int(lib().amcfd_kernel_launches(self._h))
+
+    def get_into(self, name: str, ptr: int):
+        """Copy a field into caller memory at address `ptr` (ni*nj*nk doubles)."""
+        self._check(lib().amcfd_get_field(self._h, name.encode(), C.cast(ptr, C.POINTER(_D))))
+
+    TIMING_SLOTS = ("energy_assemble", "factor", "energy_sweeps", "h2t_meltpool", "momentum",
+                    "converge", "laser", "update", "outer_iters", "sweep_launches")
+
+    def timing(self, n: int = 16) -> Dict:
         out = np.zeros(n, dtype=np.float64)
         lib().amcfd_last_timing(self._h, out.ctypes.data_as(C.POINTER(_D)), n)
-        return out
+        return {k: float(out[q]) for q, k in enumerate(self.TIMING_SLOTS)}
 
     def close(self):
         if self._h:

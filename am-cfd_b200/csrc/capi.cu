@@ -50,6 +50,7 @@ struct amcfd_ctx {
     cudaEvent_t ev[16];
     double last_ms[16] = {0};
     bool events = false;
+    long long launches = 0;  // kernels launched since creation
 };
 
 #define CK(call)                                                                          \
@@ -410,10 +411,19 @@ static int begin_step(amcfd_ctx *ctx)
     // the per-step block is the leading members of Status, up to heat_iter
     CK(cudaMemcpyAsync(ctx->st_dev, h, offsetof(Status, heat_iter), cudaMemcpyHostToDevice,
                        ctx->stream));
+    if (ctx->events) cudaEventRecord(ctx->ev[10], ctx->stream);
     if (ctx->precision == AMCFD_PREC_FP64)
         launch_laser<double>(ctx->I64);
     else
         launch_laser<float>(ctx->I32);
+    if (ctx->events) {
+        cudaEventRecord(ctx->ev[11], ctx->stream);
+        cudaEventSynchronize(ctx->ev[11]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[10], ctx->ev[11]);
+        ctx->last_ms[6] += ms;
+    }
+    ctx->launches += 1;
     ctx->niter = 0;
     return 0;
 }
@@ -435,6 +445,27 @@ static int read_status(amcfd_ctx *ctx)
     return 0;
 }
 
+// Kernel launches issued by one phase (the launch counter of the bench).
+static long long phase_launches(const amcfd_ctx *ctx, int phase)
+{
+    const long long sweeps = ctx->order == AMCFD_ORDER_EXACT ? 1 : 8;
+    switch (phase) {
+    case AMCFD_PHASE_LASER: return 1;
+    case AMCFD_PHASE_ENERGY_ASSEMBLE: return 3;
+    case AMCFD_PHASE_ENERGY_SOLVE: return 1 + sweeps;
+    case AMCFD_PHASE_H2T: return 1;
+    case AMCFD_PHASE_MELTPOOL: return 1;
+    case AMCFD_PHASE_MOMENTUM: return 2 + 4 * (3 + sweeps) + 2 + 1;
+    case AMCFD_PHASE_CONVERGE: return 1;
+    case AMCFD_PHASE_UPDATE: return 1;
+    default: return 0;
+    }
+}
+
+// Timing slots of amcfd_last_timing (accumulated device ms while profiling):
+// 0 energy BC+assembly+block correction, 1 line factorisation, 2 energy line
+// sweeps, 3 H->T + melt pool, 4 momentum chain, 5 convergence, 6 laser,
+// 7 push-back, 8 outer iterations run, 9 energy-sweep launches.
 template <typename T>
 static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
 {
@@ -443,25 +474,32 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
     while (ctx->niter < maxit) {
         ctx->niter++;
         ctx->itertot++;
-        if (ctx->events) cudaEventRecord(ctx->ev[0], ctx->stream);
+        const bool ev = ctx->events;
+        if (ev) cudaEventRecord(ctx->ev[0], ctx->stream);
         run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_ASSEMBLE);
-        if (ctx->events) cudaEventRecord(ctx->ev[1], ctx->stream);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_SOLVE);
-        if (ctx->events) cudaEventRecord(ctx->ev[2], ctx->stream);
+        if (ev) cudaEventRecord(ctx->ev[1], ctx->stream);
+        launch_energy_factor<T>(I);
+        if (ev) cudaEventRecord(ctx->ev[2], ctx->stream);
+        launch_energy_sweeps<T>(I);
+        if (ev) cudaEventRecord(ctx->ev[3], ctx->stream);
         run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
         run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
-        if (ctx->events) cudaEventRecord(ctx->ev[3], ctx->stream);
+        if (ev) cudaEventRecord(ctx->ev[4], ctx->stream);
         run_phase_impl<T>(ctx, I, AMCFD_PHASE_MOMENTUM);
-        if (ctx->events) cudaEventRecord(ctx->ev[4], ctx->stream);
+        if (ev) cudaEventRecord(ctx->ev[5], ctx->stream);
         run_phase_impl<T>(ctx, I, AMCFD_PHASE_CONVERGE);
-        if (ctx->events) cudaEventRecord(ctx->ev[5], ctx->stream);
+        if (ev) cudaEventRecord(ctx->ev[6], ctx->stream);
+        for (int ph = AMCFD_PHASE_ENERGY_ASSEMBLE; ph <= AMCFD_PHASE_CONVERGE; ++ph)
+            ctx->launches += phase_launches(ctx, ph);
         if ((rc = read_status(ctx))) return rc;
-        if (ctx->events) {
-            for (int q = 0; q < 5; q++) {
+        if (ev) {
+            for (int q = 0; q < 6; q++) {
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, ctx->ev[q], ctx->ev[q + 1]);
                 ctx->last_ms[q] += ms;
             }
+            ctx->last_ms[8] += 1.0;
+            ctx->last_ms[9] += ctx->order == AMCFD_ORDER_EXACT ? 1.0 : 8.0;
         }
         if (ctx->st_host->converged) break;
     }
@@ -598,16 +636,44 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
                                            : outer_loop<float>(ctx, ctx->I32);
     if (rc) return rc;
     if (!ctx->prm.steady) {
+        if (ctx->events) cudaEventRecord(ctx->ev[12], ctx->stream);
         if (ctx->precision == AMCFD_PREC_FP64)
             launch_update_solutions<double>(ctx->I64);
         else
             launch_update_solutions<float>(ctx->I32);
+        ctx->launches += 1;
+        if (ctx->events) {
+            cudaEventRecord(ctx->ev[13], ctx->stream);
+            cudaEventSynchronize(ctx->ev[13]);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev[12], ctx->ev[13]);
+            ctx->last_ms[7] += ms;
+        }
     }
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
     fill_report(ctx, report);
     return 0;
 }
+
+int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, double *device_ms)
+{
+    if (!ctx || nsteps < 0) return AMCFD_E_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventRecord(ctx->ev[14], ctx->stream));
+    for (int s = 0; s < nsteps; ++s) {
+        int rc = amcfd_step(ctx, report);
+        if (rc) return rc;
+    }
+    CK(cudaEventRecord(ctx->ev[15], ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev[15]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev[14], ctx->ev[15]));
+    if (device_ms) *device_ms = ms;
+    return 0;
+}
+
+long long amcfd_kernel_launches(const amcfd_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
 int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report)
 {

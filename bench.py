@@ -1,0 +1,305 @@
+"""Benchmark: the AM-CFD transient melt-pool solve on B200.
+
+Workload (one line per run): the 45-degree diagonal scan on a 400 x 200 x 100
+non-uniform grid (8 M interior cells; P = 300 W, r = 60 um, v = 0.8 m/s,
+dt = 5e-6 s, <= 20 SIMPLE outer iterations per step), synthetic deck from
+am-cfd_b200/amcfd_decks.py.  A "step" is one time step of the solver
+(updateLaser + iterativeLoopSolve + updateSolutions).
+
+value  = simulated milliseconds per wall second over K timed steps (device time
+         between CUDA events on the solver stream, max over ranks, all ranks'
+         replicas counted); cell-iters/s alongside.
+e2e    = the same metric through the C ABI with, every step, the host->device
+         copy of the step's laser/time block and the device->host read of the
+         step report and of the temperature field into pinned host memory.
+Each rank (one per GPU) runs an independent replica of the single-domain case
+("replicas only": the case does not shard).
+
+--impl reference times the reference's own CPU solver (oracle/_ref, OpenMP,
+all host threads) on the same deck.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "am-cfd_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "sim-ms/wall-s"
+# Algorithmic words per interior cell per outer iteration, by kernel family
+# (energy path; the contract total is 92 words per cell per outer iteration).
+WORDS = {"energy_assemble": 40, "factor": 2, "energy_sweeps": 40, "h2t_meltpool": 10}
+# DRAM traffic per interior cell per launch measured with ncu on the 120x60x40
+# deck, scaled by cell count (profiles/*.md).
+TRAFFIC_PER_CELL = {}
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.f = open(self.path, "w")
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
+                                     stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx = max(mx, float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_deck(tmp: str, steps: int, config: str):
+    import amcfd_decks as D
+    deck = {"config1": D.config1, "config0": D.config0}[config](steps=steps)
+    return deck, deck.write(tmp)
+
+
+def reference_arm(args, steps: int, warmup: int, config: str, threads: int):
+    """The reference CPU solver (oracle/_ref/amcfd_ref_dump --time) on the same deck."""
+    import oracle_py
+    exe = oracle_py.REF_DUMP
+    if not os.path.exists(exe):
+        return None, "reference binary oracle/_ref/amcfd_ref_dump not built"
+    with tempfile.TemporaryDirectory() as tmp:
+        deck, path = make_deck(tmp, warmup + steps, config)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        out = subprocess.run([exe, path, "--time", "--steps", str(warmup + steps)], env=env,
+                             capture_output=True, text=True, timeout=1800)
+        if out.returncode != 0:
+            return None, f"reference run failed: {out.stderr[-300:]}"
+        js = json.loads(out.stdout.strip().splitlines()[-1])
+    st = js["step_seconds"][warmup:]
+    it = js["step_iters"][warmup:]
+    secs = sum(st)
+    ncell = js["interior_cells"]
+    sim_ms = 1e3 * deck.dt * len(st)
+    return {"value": sim_ms / secs, "cell_iters_per_s": ncell * sum(it) / secs, "seconds": secs,
+            "steps": len(st), "outer_iters": sum(it), "threads": js["threads"],
+            "ms_per_step": 1e3 * secs / max(len(st), 1)}, None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--order", default="redblack", choices=["redblack", "exact"])
+    ap.add_argument("--config", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 exact-order comparison run")
+    args = ap.parse_args()
+    warmup = max(3, args.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    threads = os.cpu_count() or 1
+    cfg_desc = {"workload": ("diagonal 45-degree single track, 400x200x100 non-uniform cells "
+                             "(8.0 M), P=300 W, r=60 um, v=0.8 m/s, dt=5e-6 s, <=20 outer "
+                             "iterations/step" if args.config == "config1" else
+                             "single track +x, 120x60x40 cells, P=200 W, dt=1e-5 s"),
+                "deck": args.config, "l2": "working set 1.2-2.5 GB > 126 MB L2 (no flush needed)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ksteps = min(args.steps, 8)
+        kwarm = min(warmup, 1)
+        r, why = reference_arm(args, ksteps, kwarm, args.config, threads)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": kwarm,
+                "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic deck",
+                "config": dict(cfg_desc, solver="reference OpenMP build (oracle/_ref)"),
+                "cell_iters_per_s": r["cell_iters_per_s"],
+                "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["threads"],
+                                 "kind": "reference",
+                                 "sample": f"{r['steps']} steps after {kwarm} warm-up of the same deck"},
+                "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np
+    import torch
+    import amcfd
+
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    prec = amcfd.PREC_FP32 if args.precision == "fp32" else amcfd.PREC_FP64
+    order = amcfd.ORDER_REDBLACK if args.order == "redblack" else amcfd.ORDER_EXACT
+    tmp = tempfile.mkdtemp(prefix=f"amcfd_bench{rank}_")
+    total_steps = warmup + 2 * args.steps + 2
+    deck, path = make_deck(tmp, total_steps, args.config)
+    d = amcfd.Deck(path)
+    ni, nj, nk = d.dims
+    ncell = (ni - 2) * (nj - 2) * (nk - 2)
+    s = amcfd.Solver(d, order=order, precision=prec, device=dev)
+    s.run_steps(warmup)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = Clocks(dev)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    s.profile(True)
+    l0 = s.launches
+    rep, ms = s.run_steps(args.steps)
+    launches = s.launches - l0
+    prof = s.timing()
+    s.profile(False)
+    torch.cuda.synchronize()
+    barrier()
+    ck = clocks.stop()
+    ms = allmax(ms)
+    iters = prof["outer_iters"]
+    value = world * 1e3 * deck.dt * args.steps / (ms / 1e3)
+    cips = world * ncell * iters / (ms / 1e3)
+
+    # end to end: per step, laser block in, report + temperature field out (pinned)
+    host = torch.empty(ni * nj * nk, dtype=torch.float64, pin_memory=True)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step()
+        s.get_into("temp", host.data_ptr())
+    t1 = time.perf_counter()
+    barrier()
+    e2e_s = allmax(t1 - t0)
+    e2e = {"value": world * 1e3 * deck.dt * args.steps / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": 52, "d2h_bytes_per_step": int(ni * nj * nk * 8 + 512)}
+
+    # roofline of the dominant kernel family
+    peak, peak_kind = _peaks()
+    w = 4 if prec == amcfd.PREC_FP32 else 8
+    fam = max(WORDS, key=lambda k: prof[k])
+    nlaunch = iters * (1 if fam != "energy_sweeps" else 1)
+    avg_ms = prof[fam] / max(nlaunch, 1)
+    alg_bytes = WORDS[fam] * ncell * w
+    achieved = alg_bytes / (avg_ms / 1e3) / 1e9
+    tr = TRAFFIC_PER_CELL.get(f"{fam}:{args.precision}:{args.order}")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "kernel": fam,
+                "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
+                "traffic": tr * ncell if tr else None,
+                "iteration_frac": (92 * ncell * w * iters / (ms / 1e3) / 1e9) / peak}
+
+    extra = {}
+    if not args.no_compare and rank == 0:
+        # the plain FP64 exact-order solve of the same steps, for the speed-up at equal iterations
+        s64 = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, device=dev)
+        s64.run_steps(1)
+        nref = min(args.steps, 3)
+        _, ms64 = s64.run_steps(nref)
+        extra["fp64_exact_sim_ms_per_wall_s"] = 1e3 * deck.dt * nref / (ms64 / 1e3)
+        extra["speedup_vs_fp64_exact"] = (value / world) / extra["fp64_exact_sim_ms_per_wall_s"]
+        s64.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r, why = reference_arm(args, 2, 0, args.config, threads)
+        if r is not None:
+            cpu = {"value": r["value"], "unit": METRIC, "cores": r["threads"], "kind": "reference",
+                   "sample": f"first {r['steps']} steps of the same deck, OpenMP build of the reference",
+                   "cell_iters_per_s": r["cell_iters_per_s"]}
+        else:
+            cpu = {"value": None, "unit": METRIC, "cores": threads, "kind": "reference",
+                   "sample": why}
+    s.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32" if prec == amcfd.PREC_FP32 else "f64", "data": "synthetic deck",
+                "config": dict(cfg_desc, precision=args.precision, order=args.order,
+                               parallelism=f"replicas{world}"),
+                "cell_iters_per_s": cips, "outer_iters": iters, "gpu_launches": launches,
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
+                "phase_ms": {k: v for k, v in prof.items() if k not in ("outer_iters", "sweep_launches")}}
+        line.update(extra)
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

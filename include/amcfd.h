@@ -191,6 +191,13 @@ int amcfd_last_timing(const amcfd_ctx *ctx, double *ms, int n);
  * clears the accumulated times. */
 int amcfd_profile(amcfd_ctx *ctx, int enable);
 
+/* nsteps calls of amcfd_step bracketed by CUDA events on the context stream;
+ * *device_ms receives the device time between the events.  (main.cpp:123-201) */
+int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, double *device_ms);
+
+/* Number of kernels the context has launched since creation. */
+long long amcfd_kernel_launches(const amcfd_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif
