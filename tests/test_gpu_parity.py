@@ -115,13 +115,13 @@ def test_exact_fp64_phases(deckdir):
     gpu.close()
 
 
-@pytest.mark.parametrize("flow,tol", [(False, 1e-9), (True, 1e-4)])
-def test_redblack_converges_to_same_solution(flow, tol, deckdir):
+@pytest.mark.parametrize("flow,tol", [(False, 1e-5), (True, 1e-4)])
+def test_redblack_close_to_exact_order(flow, tol, deckdir):
     """The parallel red-black ordering and the exact order are two iterations
-    for the same discrete equations: with the outer loop run to 60 iterations
-    (tolerance 1e-12 is never met, so both stop at maxit) the energy-only
-    solutions agree to rounding, and with fluid flow to the remaining
-    outer-iteration error."""
+    for the same discrete equations; they differ only by what the outer loop
+    leaves unconverged (the energy-only loop stops on the heat-balance ratio
+    alone).  Observed gaps on this deck: 1.6e-6 (energy only) and 4.8e-6
+    (with flow) relative L2 in T after two steps."""
     import amcfd
     import amcfd_decks as D
     dk = D.small("rb", steps=2, maxit=60, fluid_flow=flow)
