@@ -198,6 +198,24 @@ int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, doubl
 /* Number of kernels the context has launched since creation. */
 long long amcfd_kernel_launches(const amcfd_ctx *ctx);
 
+/* Energy residual without any device allocation.  No counterpart in the reference:
+ * it exists for callers that cannot let a library allocate device memory (an
+ * application that owns all device memory through its own pool, or one under a
+ * fixed memory budget).  The caller passes device arrays an..su and the enthalpy h,
+ * laid out [nk][nj][pitch] (i fastest, pitch >= ni), and a device double for the
+ * result; resorh = sum|(sum a_nb h_nb + su)/ap - h| / (sum|h| + 1e-6) over the
+ * interior, as calculateResiduals(5) computes it.  Scratch is a file-scope device
+ * array held by every GPU that loads the library (64 KiB) that supports at most
+ * 4096 interior k-planes (nk - 2); larger grids get AMCFD_E_CAPACITY.  The first
+ * call on a device looks up that array's address (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race.  Work is
+ * queued on `stream` (a cudaStream_t, NULL for the default stream). */
+int amcfd_energy_residual_noalloc(const double *an, const double *as, const double *ae,
+                                  const double *aw, const double *at, const double *ab,
+                                  const double *ap, const double *su, const double *h,
+                                  int ni, int nj, int nk, int pitch,
+                                  double *resorh_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
