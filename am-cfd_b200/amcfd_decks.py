@@ -83,6 +83,14 @@ class Deck:
     tol: float = 1e-5
     scheme: str = "power_law"  # power_law | exponential_law | upwind
     fluid_flow: bool = True
+    # *BOUNDARY_EVAPORATION: (latent heat, evaporation T, factor, molar mass)
+    evaporation: Optional[Tuple[float, float, float, float]] = None
+    # *VOLUMETRIC_HEAT_SOURCE: (power, efficiency, thickness, radius, factor)
+    volumetric: Optional[Tuple[float, float, float, float, float]] = None
+    # *VOLUMETRIC_HEAT_SOURCE_TABLE rows (t, power, efficiency, thickness, radius, factor)
+    heat_table: Optional[List[Tuple[float, float, float, float, float, float]]] = None
+    # *CONTROL_TIMESTEP_VARIABLE rows (t, dt, output interval)
+    vardt: Optional[List[Tuple[float, float, float]]] = None
 
     @property
     def cells(self) -> Tuple[int, int, int]:
@@ -93,11 +101,14 @@ class Deck:
     def steps(self) -> int:
         return int(math.ceil(self.finaltime / self.dt - 1e-9))
 
-    def write(self, directory: str) -> str:
-        """Write deck, mesh and toolpath files under `directory`; return the deck path."""
+    def write(self, directory: str, relative: bool = False) -> str:
+        """Write deck, mesh and toolpath files under `directory`; return the deck path.
+        With relative=True the deck names its mesh/toolpath files without a
+        directory (the reference opens them relative to the working directory)."""
         os.makedirs(directory, exist_ok=True)
         directory = os.path.abspath(directory)
         mesh = os.path.join(directory, f"{self.name}_mesh.k")
+        ref = (lambda p: os.path.basename(p)) if relative else (lambda p: p)
         with open(mesh, "w") as f:
             for tag, zones in (("X", self.x_zones), ("Y", self.y_zones), ("Z", self.z_zones)):
                 f.write(f"*{tag}_GRID_PARAMETERS\n$ zones / lengths / control volumes / exponents\n")
@@ -109,7 +120,7 @@ class Deck:
         hsmelt, hlfriz = m.enthalpies()
         lines = [
             "*KEYWORD_ID", self.name,
-            "*DIRECTORY", os.path.join(directory, "out"),
+            "*DIRECTORY", ref(os.path.join(directory, "out")),
             "*PARAMETERS",
             f"accelGravity {self.gravity!r}", f"radBoltzmann {self.sigma!r}",
             f"ambientTemp {self.t_amb!r}", f"ambientPres {self.p_amb!r}",
@@ -139,13 +150,29 @@ class Deck:
             lines += ["*SELECT_DISCRETIZATION", self.scheme]
         if not self.fluid_flow:
             lines += ["*FLUID_FLOW_OFF"]
-        lines += ["*MESH_FILE", mesh]
+        if self.evaporation is not None:
+            lines += ["*BOUNDARY_EVAPORATION", "  " + " ".join(repr(float(v)) for v in self.evaporation)]
+        if self.volumetric is not None:
+            lines += ["*VOLUMETRIC_HEAT_SOURCE", "  " + " ".join(repr(float(v)) for v in self.volumetric)]
+        if self.heat_table is not None:
+            tab = os.path.join(directory, f"{self.name}_heat.txt")
+            with open(tab, "w") as f:
+                for row in self.heat_table:
+                    f.write(" ".join(repr(float(v)) for v in row) + "\n")
+            lines += ["*VOLUMETRIC_HEAT_SOURCE_TABLE", ref(tab)]
+        if self.vardt is not None:
+            tab = os.path.join(directory, f"{self.name}_dt.txt")
+            with open(tab, "w") as f:
+                for row in self.vardt:
+                    f.write(" ".join(repr(float(v)) for v in row) + "\n")
+            lines += ["*CONTROL_TIMESTEP_VARIABLE", ref(tab)]
+        lines += ["*MESH_FILE", ref(mesh)]
         if self.toolpath is not None:
             crs = os.path.join(directory, f"{self.name}.crs")
             with open(crs, "w") as f:
                 for t, x, y, z, on, tid in self.toolpath:
                     f.write(f"{t:.10e} {x:.10e} {y:.10e} {z:.10e} {int(on)} {int(tid)}\n")
-            lines += ["*TOOLPATH_FILE", crs]
+            lines += ["*TOOLPATH_FILE", ref(crs)]
         else:
             st = self.single_track or (1.0, 0.5e-3, 1.0e-3, 1.0)
             lines += ["*SINGLE_TRACK_TOOL", "$ lasertime xstart ystart scanvel",
@@ -171,7 +198,7 @@ def config0(steps: Optional[int] = None) -> Deck:
              z_zones=[(0.5e-3, 15, -1.5), (0.2e-3, 25, 1.0)],
              single_track=(1.0, 0.5e-3, 1.0e-3, 1.0), finaltime=2e-3)
     if steps is not None:
-        d.finaltime = (steps + 0.5) * d.dt
+        d.finaltime = (steps - 0.5) * d.dt
     return d
 
 
@@ -192,7 +219,7 @@ def config1(steps: Optional[int] = None) -> Deck:
              power=300.0, radius=60e-6, dt=5e-6, finaltime=2.5e-3)
     d.toolpath = diagonal_toolpath(1.5e-3, 1.5e-3, _top(zz), 0.8, 45.0, 3.0e-3)
     if steps is not None:
-        d.finaltime = (steps + 0.5) * d.dt
+        d.finaltime = (steps - 0.5) * d.dt
     return d
 
 
@@ -229,7 +256,7 @@ def config3_eval(steps: Optional[int] = None) -> Deck:
              z_zones=[(lz * 5 / 7, 22, -1.5), (lz * 2 / 7, 38, 1.0)],
              power=250.0, single_track=(1.0, lx * 0.1, ly * 0.5, 1.2), finaltime=1e-2)
     if steps is not None:
-        d.finaltime = (steps + 0.5) * d.dt
+        d.finaltime = (steps - 0.5) * d.dt
     return d
 
 
@@ -275,7 +302,7 @@ def config4(steps: Optional[int] = None) -> Deck:
     d.toolpath = raster_toolpath(3.2e-3, 6.8e-3, 2.3e-3, 100e-6, 5, _top(zz), 1.0, 1e-3)
     d.finaltime = d.toolpath[-2][0]
     if steps is not None:
-        d.finaltime = (steps + 0.5) * d.dt
+        d.finaltime = (steps - 0.5) * d.dt
     return d
 
 
@@ -293,7 +320,7 @@ def small(name="small", nx=24, ny=14, nz=10, steps=6, power=300.0, speed=1.0,
     zy = [(ly * 0.3, ny1, -1.2), (ly * 0.4, ny - 2 * ny1, 1.0), (ly * 0.3, ny1, 1.2)]
     d = Deck(name=name, x_zones=[(lx, nx, 1.0)], y_zones=zy, z_zones=zz, power=power,
              scheme=scheme, fluid_flow=fluid_flow, maxit=maxit, urf=(urf,) * 5)
-    d.finaltime = (steps + 0.5) * d.dt
+    d.finaltime = (steps - 0.5) * d.dt
     lasertime = 1.0 if laser_off_after is None else laser_off_after * d.dt
     if toolpath:
         d.toolpath = diagonal_toolpath(lx * 0.3, ly * 0.35, _top(zz), speed, 30.0, d.finaltime * 4)

@@ -47,7 +47,7 @@ struct amcfd_ctx {
     cudaStream_t stream = nullptr;
     Status *st_dev = nullptr;
     Status *st_host = nullptr;  // pinned
-    cudaEvent_t ev[16];
+    cudaEvent_t ev[16] = {};
     double last_ms[16] = {0};
     bool events = false;
     long long launches = 0;  // kernels launched since creation

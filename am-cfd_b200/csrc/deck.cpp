@@ -163,7 +163,9 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         case 11:
             v = numbers(line);
             if (v.size() < 2) return fail(AMCFD_E_PARSE, "*CONTROL_TIMESTEP needs dt and output interval");
+            // a later *CONTROL_TIMESTEP switches the variable table off (Mesh.cpp:288-290)
             p.delt = v[0]; p.outtime = v[1]; have_timestep = true;
+            d->vardt.clear();
             break;
         case 12:
             v = numbers(line);

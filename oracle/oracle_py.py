@@ -65,6 +65,10 @@ class Oracle:
     """One oracle instance built from an amcfd_params block (ctypes Structure)."""
 
     def __init__(self, params):
+        # params: an amcfd.Deck (kept alive: its tables back the pointers in the
+        # parameter block) or an AmcfdParams whose owner outlives this call
+        self._deck = params if hasattr(params, "params") else None
+        params = params.params if self._deck is not None else params
         self._params = params
         self._h = C.c_void_p(lib().orc_create(C.byref(params)))
         ni, nj, nk = C.c_int(), C.c_int(), C.c_int()

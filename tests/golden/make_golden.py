@@ -1,0 +1,63 @@
+"""Generate the golden records of the reference solver (run in the build container).
+
+For each small deck below this script writes the deck, its mesh (and toolpath)
+into tests/golden/<name>/ with relative file names, runs the reference solver
+compiled from its own sources (oracle/_ref/amcfd_ref_dump, built by
+oracle/build_ref.sh) single-threaded in that directory, and stores
+<name>/ref.npz: the per-step scalars of every step and the fields after the
+first and the last step.  The oracle tests replay the same decks.
+
+usage: python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path[:0] = [os.path.join(ROOT, "am-cfd_b200"), os.path.join(ROOT, "oracle")]
+
+import amcfd_decks as D  # noqa: E402
+from amcfd_dump import read_dump  # noqa: E402
+
+FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
+SCALARS = ("niter", "timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
+           "depth", "width", "ratio", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat",
+           "jstart")
+
+
+def decks():
+    return [
+        D.small("g_track", nx=16, ny=10, nz=8, steps=4),
+        D.small("g_toolpath", nx=16, ny=10, nz=8, steps=4, toolpath=True),
+        D.small("g_noflow", nx=16, ny=10, nz=8, steps=4, fluid_flow=False),
+        D.small("g_cooling", nx=16, ny=10, nz=8, steps=6, laser_off_after=3, scheme="upwind"),
+    ]
+
+
+def main():
+    exe = os.path.join(ROOT, "oracle", "_ref", "amcfd_ref_dump")
+    if not os.path.exists(exe):
+        sys.exit("build the reference first: bash oracle/build_ref.sh")
+    for d in decks():
+        out = os.path.join(HERE, d.name)
+        path = d.write(out, relative=True)
+        subprocess.check_call([exe, os.path.basename(path), "--out", "ref.bin"], cwd=out,
+                              env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
+        dump = read_dump(os.path.join(out, "ref.bin"))
+        os.unlink(os.path.join(out, "ref.bin"))
+        steps = dump["steps"]
+        rec = {f"s_{k}": np.array([s[k] for s in steps]) for k in SCALARS}
+        for tag, s in (("first", steps[0]), ("last", steps[-1])):
+            for f in FIELDS:
+                rec[f"{tag}_{f}"] = s[f]
+        for g, v in dump["geom"].items():
+            rec[f"geom_{g}"] = v
+        np.savez_compressed(os.path.join(out, "ref.npz"), **rec)
+        print(d.name, len(steps), "steps")
+
+
+if __name__ == "__main__":
+    main()

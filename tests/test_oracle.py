@@ -1,0 +1,89 @@
+"""The CPU oracle against the reference solver.
+
+1. Golden records (tests/golden/*/ref.npz, made by tests/golden/make_golden.py
+   from the reference compiled from its own sources): the oracle must reproduce
+   them bit for bit -- every step's iteration count and scalars, the fields
+   after the first and the last step, and the grid.
+2. Live comparison with oracle/_ref/amcfd_ref_dump (only where it was built):
+   deck features the golden set does not cover.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling"]
+FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
+SCALARS = ("niter", "tpeak", "alen", "depth", "width", "ratio", "resorh", "resorm", "resoru",
+           "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart")
+
+
+def _same(a, b):
+    return (a == b) or (np.isnan(a) and np.isnan(b))
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
+    import amcfd
+    import oracle_py
+    monkeypatch.chdir(os.path.join(GOLDEN, case))
+    deck = amcfd.Deck(f"{case}.k")
+    ref = np.load("ref.npz")
+    o = oracle_py.Oracle(deck.params)
+    for g in ("x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"):
+        assert np.array_equal(o.field(g), ref[f"geom_{g}"]), g
+    n = len(ref["s_niter"])
+    for s in range(n):
+        r = o.step()
+        for k in SCALARS:
+            assert _same(r[k], ref[f"s_{k}"][s]), (case, s, k, r[k], ref[f"s_{k}"][s])
+        tag = "first" if s == 0 else "last" if s == n - 1 else None
+        if tag:
+            for f in FIELDS:
+                assert np.array_equal(o.field(f), ref[f"{tag}_{f}"], equal_nan=True), (case, s, f)
+
+
+def _variants():
+    import amcfd_decks as D
+    out = []
+    d = D.small("v_evap", steps=3, power=120.0)
+    d.evaporation = (6.0e6, 3100.0, 1e-3, 0.056)
+    out.append(d)
+    d = D.small("v_vol", steps=3, power=100.0)
+    d.volumetric = (150.0, 0.4, 60e-6, 50e-6, 2.0)
+    out.append(d)
+    d = D.small("v_table", steps=4, power=100.0)
+    d.heat_table = [(0.0, 150.0, 0.4, 60e-6, 50e-6, 2.0), (2.5e-5, 250.0, 0.4, 80e-6, 40e-6, 2.0),
+                    (1.0, 250.0, 0.4, 80e-6, 40e-6, 2.0)]
+    out.append(d)
+    d = D.small("v_vardt", steps=5)
+    d.vardt = [(2e-5, 1e-5, 1.0), (1.0, 5e-6, 1.0)]
+    d.finaltime = 4.2e-5
+    out.append(d)
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
+                                                    "amcfd_ref_dump")),
+                    reason="reference not built in this checkout (oracle/build_ref.sh)")
+@pytest.mark.parametrize("idx", range(4))
+def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
+    import amcfd
+    import oracle_py
+    from amcfd_dump import read_dump
+    deck = _variants()[idx]
+    path = deck.write(str(tmp_path))
+    out = str(tmp_path / "ref.bin")
+    subprocess.check_call([oracle_py.REF_DUMP, path, "--out", out],
+                          env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
+    ref = read_dump(out)
+    o = oracle_py.Oracle(amcfd.Deck(path))
+    for s in ref["steps"]:
+        r = o.step()
+        assert r["niter"] == s["niter"]
+        assert _same(r["tpeak"], s["tpeak"])
+        for f in FIELDS:
+            assert np.array_equal(o.field(f), s[f], equal_nan=True), (deck.name, s["step"], f)
