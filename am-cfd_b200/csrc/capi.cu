@@ -8,6 +8,7 @@
 // CFDSolverManager::iterativeLoopSolve (CFDSolverManager.cpp:595-722) as a
 // chain of kernels per outer iteration, and updateSolutions.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,8 @@
 namespace amcfd {
 template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
 template <typename T> void set_sweep_smem_limit(size_t smem);
+dim3 energy_assemble_grid(const Params &p);
+template <typename T> int h2t_blocks_per_sm();
 }  // namespace amcfd
 
 using namespace amcfd;
@@ -270,9 +273,9 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     I.order = ctx->order;
     I.nb_las = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 255) / 256));
     I.nb_bc = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 2 * p.nk * (p.ni + p.nj) + 255) / 256));
-    I.asm_grid = dim3((p.ni + 31) / 32, (p.nj + 7) / 8, (p.nk + 3) / 4);
+    I.asm_grid = energy_assemble_grid(p);
     I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
-    I.nb_h2t = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
+    I.nb_h2t = std::max(1, std::min(I.sm_count * h2t_blocks_per_sm<T>(), (int)((n3 + 255) / 256)));
     I.nb_mom = I.sm_count * 2;
     I.grid_1d = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
     double *red;
@@ -287,6 +290,14 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     g.npart = I.asm_grid.y * I.asm_grid.z;
     if ((rc = alloc3<double>(ctx, &g.bc, (size_t)g.npart * 4 * p.nip))) return rc;
     if ((rc = alloc3<double>(ctx, &g.delphi, (size_t)p.nip))) return rc;
+    if ((rc = alloc3<double>(ctx, &g.bcsum, (size_t)4 * p.nip))) return rc;
+    if ((rc = alloc3<int>(ctx, &g.mp_kb, (size_t)p.nip))) return rc;
+    if ((rc = alloc3<int>(ctx, &g.mp_jdn, (size_t)p.nip))) return rc;
+    if ((rc = alloc3<int>(ctx, &g.mp_jup, (size_t)p.nip))) return rc;
+    {
+        std::vector<int> jup(p.nip, p.njm1);  // "no cell below Ts" sentinel
+        CK(cudaMemcpy(g.mp_jup, jup.data(), jup.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
     // exact-order scheduling
     I.max_lines = (p.nj - 2) * (p.nk - 2);
     if ((rc = alloc3<int>(ctx, &g.flags, (size_t)p.nk * p.nj))) return rc;
@@ -315,10 +326,15 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     g.st = ctx->st_dev;
     I.check_finite = 0;
     I.exact_warps = 4;
-    I.line_smem = (size_t)I.exact_warps * 3 * p.nip * sizeof(T);
+    // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
+    I.line_smem = (size_t)I.exact_warps * 8 * p.nip * sizeof(T) + (size_t)I.exact_warps * 8;
     set_sweep_smem_limit<T>(I.line_smem);
     int bps = exact_sweep_blocks_per_sm<T>(I.exact_warps, I.line_smem);
-    I.exact_grid = std::max(1, I.sm_count * bps);
+    // A wave of the exact-order sweep holds about 2(nj-2)/3 lines; about three
+    // waves of lines in flight keep the dependency chain fed without flooding L2
+    // with flag polls from warps that are waves ahead.
+    I.exact_grid = std::max(1, std::min(I.sm_count * bps, (2 * (p.nj - 2) + I.exact_warps - 1) /
+                                                              I.exact_warps));
 
     // initializeSolver (CFDSolverManager.cpp:402-525)
     std::vector<double> hv(n3, 0.0);
@@ -591,6 +607,8 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         s.avolpow = p.avolpow; s.apowseta = p.apowseta; s.heatthick = p.heatthick;
         s.heatrb = p.heatrb; s.avolfact = p.avolfact;
         s.delt = ctx->delt;
+        s.mp_imax = INT_MAX;
+        s.mp_imin = INT_MIN;
         CK(cudaMemcpy(ctx->st_dev, &s, sizeof(s), cudaMemcpyHostToDevice));
     }
     for (int q = 0; q < 16; q++) CK(cudaEventCreate(&ctx->ev[q]));

@@ -56,6 +56,7 @@ struct Status {
     int istat, iend, jstat, jend, kstat, istatp1, iendm1;
     int imin, imax, jmin, jmax, kmin, kmax;
     int momentum_active, box_cells;
+    int mp_imax, mp_imin;  // melt-pool length scan candidates, gathered by h2t_kernel
     int niter, itertot, converged;
     int error;         // 0, or an AMCFD_E_* code set by a kernel
     int error_where;   // kernel-specific detail (e.g. the line that timed out)
@@ -88,8 +89,13 @@ struct Fields {
     // reductions
     double *red;        // [nblocks][R_NSLOTS] per-CTA partials
     double *bc;         // block correction: [npart][4][nip] per-CTA partial sums
+    double *bcsum;      // [4][nip] reduced sums
     double *delphi;     // nip
     int npart;          // number of block-correction partial rows
+    // melt-pool column scans (getMeltPoolShape), gathered with integer atomics by
+    // h2t_kernel: per column i the deepest k with T < Ts on the beam plane, and the
+    // first/last j around the beam with T < Ts on the top plane
+    int *mp_kb, *mp_jup, *mp_jdn;
     // exact-order line sweep scheduling
     int *flags;         // (nk*nj) per-line visit counters (monotone across calls)
     int2 *tickets_energy;  // precomputed topological order of the energy visits
@@ -103,6 +109,12 @@ __host__ __device__ __forceinline__ size_t cidx(int i, int j, int k, int nj, int
 {
     return ((size_t)k * nj + j) * (size_t)nip + i;
 }
+
+// Division in the bulk precision: IEEE in FP64 (the parity build), the fast
+// approximate reciprocal form in FP32 (about 2 ulp; the FP32 build is judged
+// against the FP64 oracle, not bit for bit).
+__device__ __forceinline__ double bdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float bdiv(float a, float b) { return __fdividef(a, b); }
 
 // Discretisation scheme A(|Pe|) (CFDSolverManager.cpp:3071-3101).
 template <typename R>
@@ -123,7 +135,7 @@ __device__ __forceinline__ R scheme_fn(int scheme, R pe)
 template <typename R>
 __device__ __forceinline__ void face_coef(int scheme, R d, R f, R &plus, R &minus)
 {
-    R a = d * scheme_fn<R>(scheme, fabs(f) / d);
+    R a = d * scheme_fn<R>(scheme, bdiv(fabs(f), d));
     plus = a + maxd(R(0), -f);
     minus = a + maxd(R(0), f);
 }

@@ -116,223 +116,28 @@ __global__ void energy_bc_kernel(Params p, Fields<T> g, double *red)
 }
 
 // ---------------------------------------------------------------------------
-// Fused energy assembly: discretizeEquations(5) (CFDSolverManager.cpp:1157-1264),
-// calculateSource(5) (:1677-1843), calculateResiduals(5) (:2073-2101), the
-// coefficient/residual sums of enhanceConvergenceSpeed(5) (:2310-2332) and
-// bareplateMaterialProps (:2137-2189, written to the *_nxt buffers so the
-// old properties stay readable by neighbouring cells).
-// Block (32, 8); each thread walks KB planes.  Grid covers boundary cells too
-// (they only update properties).
-// ---------------------------------------------------------------------------
-constexpr int kAsmKB = 4;
-
-template <typename T>
-__global__ void __launch_bounds__(256) energy_assemble_kernel(Params p, Fields<T> g, double *red)
-{
-    using R = T;
-    const Status *st = g.st;
-    const int i = blockIdx.x * 32 + threadIdx.x;
-    const int j = blockIdx.y * 8 + threadIdx.y;
-    const int k0 = blockIdx.z * kAsmKB;
-    const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
-    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
-              nkm2 = p.nkm2;
-    const int sch = p.scheme;
-    const double delt = st->delt;
-    const bool volsrc = p.volsrc != 0;
-    double sumd = 0.0, sumh = 0.0;
-    double bl = 0.0, blp = 0.0, blm = 0.0, blc = 0.0;
-    const size_t sj = nip, sk = (size_t)nj * nip;
-    for (int k = k0; k < k0 + kAsmKB && k < nk; ++k) {
-        if (i >= ni || j >= nj) break;
-        const size_t c = cidx(i, j, k, nj, nip);
-        // ---- material properties (all nodes) ----
-        {
-            double t = (double)g.temp[c], fl = (double)g.fracl[c];
-            double diffl = (p.thconla * t + p.thconlb) / p.acpl;
-            double dn = diffl, rn = p.denl, vn = p.viscos;
-            if (!(t >= p.tliquid)) {
-                double diffs = (p.thconsa * (t * t) + p.thconsb * t + p.thconsc) / (p.acpa * t + p.acpb);
-                dn = diffs; rn = p.dens; vn = 1e10;
-                if (!(t <= p.tsolid)) {
-                    dn = fl * diffl + (1.0 - fl) * diffs;
-                    rn = fl * p.denl + (1.0 - fl) * p.dens;
-                    vn = p.viscos;
-                }
-            }
-            g.diff_nxt[c] = (T)dn;
-            g.rho_nxt[c] = (T)rn;
-            g.vis_nxt[c] = (T)vn;
-        }
-        if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
-        const R *df = g.diff_cur, *rh = g.rho_cur, *h = g.h, *fl = g.fracl;
-        const R dcc = df[c], rhc = rh[c];
-        const R aik = (R)area_ik(p, g, i, k), ajk = (R)area_jk(p, g, j, k), aij = (R)area_ij(p, g, i, j);
-        R an, as_, ae, aw, at, ab, tmp;
-        // north face
-        if (j == njm2) {
-            R vn = g.vvel[c + sj];
-            R fn = rh[c + sj] * vn * aik;
-            R dn = df[c] * aik * (R)g.dypsinv[njm1];
-            face_coef<R>(sch, dn, fn, an, tmp);
-        } else {
-            R vn = g.vvel[c + sj];
-            R fn = rh[c + sj] * vn * aik;
-            R difn = dcc * df[c + sj] / ((R(1) - (R)g.fracy[j]) * df[c + sj] + (R)g.fracy[j] * dcc);
-            R dn = difn * aik * (R)g.dypsinv[j + 1];
-            face_coef<R>(sch, dn, fn, an, tmp);
-        }
-        // south face
-        if (j == 1) {
-            R vs = g.vvel[c];
-            R fs = rhc * vs * aik;
-            R ds = dcc * aik * (R)g.dypsinv[1];
-            face_coef<R>(sch, ds, fs, tmp, as_);
-        } else {
-            R vn = g.vvel[c];
-            R fn = rhc * vn * aik;
-            R difn = df[c - sj] * dcc / ((R(1) - (R)g.fracy[j - 1]) * dcc + (R)g.fracy[j - 1] * df[c - sj]);
-            R dn = difn * aik * (R)g.dypsinv[j];
-            face_coef<R>(sch, dn, fn, tmp, as_);
-        }
-        // east face
-        if (i == nim2) {
-            R ue = g.uvel[c + 1];
-            R fe = rh[c + 1] * ue * ajk;
-            R de = df[c] * ajk * (R)g.dxpwinv[nim1];
-            face_coef<R>(sch, de, fe, ae, tmp);
-        } else {
-            R ue = g.uvel[c + 1];
-            R fe = rh[c + 1] * ue * ajk;
-            R dife = dcc * df[c + 1] / ((R(1) - (R)g.fracx[i]) * df[c + 1] + (R)g.fracx[i] * dcc);
-            R de = dife * ajk * (R)g.dxpwinv[i + 1];
-            face_coef<R>(sch, de, fe, ae, tmp);
-        }
-        // west face
-        if (i == 1) {
-            R uw = g.uvel[c];
-            R fw = rhc * uw * ajk;
-            R dw = dcc * ajk * (R)g.dxpwinv[1];
-            face_coef<R>(sch, dw, fw, tmp, aw);
-        } else {
-            R ue = g.uvel[c];
-            R fe = rhc * ue * ajk;
-            R dife = df[c - 1] * dcc / ((R(1) - (R)g.fracx[i - 1]) * dcc + (R)g.fracx[i - 1] * df[c - 1]);
-            R de = dife * ajk * (R)g.dxpwinv[i];
-            face_coef<R>(sch, de, fe, tmp, aw);
-        }
-        // top face
-        if (k == nkm2) {
-            R wt = g.wvel[c + sk];
-            R ft = rh[c + sk] * wt * aij;
-            R dt = df[c] * aij * (R)g.dzpbinv[nkm1];
-            face_coef<R>(sch, dt, ft, at, tmp);
-        } else {
-            R wt = g.wvel[c + sk];
-            R ft = rh[c + sk] * wt * aij;
-            R dift = dcc * df[c + sk] / ((R(1) - (R)g.fracz[k]) * df[c + sk] + (R)g.fracz[k] * dcc);
-            R dt = dift * aij * (R)g.dzpbinv[k + 1];
-            face_coef<R>(sch, dt, ft, at, tmp);
-        }
-        // bottom face
-        if (k == 1) {
-            R wb = g.wvel[c];
-            R fb = rhc * wb * aij;
-            R db = dcc * aij * (R)g.dzpbinv[1];
-            face_coef<R>(sch, db, fb, tmp, ab);
-        } else {
-            R wt = g.wvel[c];
-            R ft = rhc * wt * aij;
-            R dift = df[c - sk] * dcc / ((R(1) - (R)g.fracz[k - 1]) * dcc + (R)g.fracz[k - 1] * df[c - sk]);
-            R dt = dift * aij * (R)g.dzpbinv[k];
-            face_coef<R>(sch, dt, ft, tmp, ab);
-        }
-        const R vol = (R)volume_p(p, g, i, j, k);
-        const R densbydt = rhc / (R)delt;
-        const R apnot = densbydt * vol;
-        R sp = R(0);
-        R su = apnot * g.hnot[c];
-        // ---- calculateSource(5) ----
-        if (volsrc) {
-            R srcin = R(0);
-            if (g.z[nkm1] - g.z[k] <= st->heatthick) {
-                double hr2 = st->heatrb * st->heatrb;
-                double bx = st->beamposx - g.x[i], by = st->beamposy - g.y[j];
-                srcin = (R)(st->avolpow * st->avolfact / M_PI / hr2 / st->heatthick * st->apowseta *
-                            exp(-st->avolfact / hr2 * ((bx * bx) + (by * by))) *
-                            (double)st->powerindicator);
-                su += vol * srcin;
-            }
-            g.sourceinput[c] = srcin;
-        }
-        const R hlatnt = (R)p.hlatnt;
-        const R variable1 = hlatnt * rhc / (R)delt;
-        const R volht = vol * variable1;
-        const R flc = fl[c];
-        su -= volht * (flc - g.fraclnot[c]);
-        {
-            const R *u = g.uvel, *v = g.vvel, *w = g.wvel;
-            R uc = u[c], up = u[c + 1], vc = v[c], vp = v[c + sj], wc = w[c], wp = w[c + sk];
-            R flew = ajk * (maxd(uc, R(0)) * fl[c - 1] - maxd(-uc, R(0)) * flc +
-                            maxd(-up, R(0)) * fl[c + 1] - maxd(up, R(0)) * flc);
-            R flns = aik * (maxd(vc, R(0)) * fl[c - sj] - maxd(-vc, R(0)) * flc +
-                            maxd(-vp, R(0)) * fl[c + sj] - maxd(vp, R(0)) * flc);
-            R fltb = aij * (maxd(wc, R(0)) * fl[c - sk] - maxd(-wc, R(0)) * flc +
-                            maxd(-wp, R(0)) * fl[c + sk] - maxd(wp, R(0)) * flc);
-            su += rhc * hlatnt * (flew + flns + fltb);
-        }
-        const R hc = h[c];
-        const R hjp = h[c + sj], hjm = h[c - sj], hip = h[c + 1], him = h[c - 1], hkp = h[c + sk],
-                hkm = h[c - sk];
-        // boundary folds, in the reference's order: k, j, i
-        if (k == 1) { su += ab * hkm; sp -= ab; ab = R(0); }
-        if (k == nkm2) { su += at * hkp; sp -= at; at = R(0); }
-        if (j == 1) { su += as_ * hjm; sp -= as_; as_ = R(0); }
-        if (j == njm2) { su += an * hjp; sp -= an; an = R(0); }
-        if (i == 1) { su += aw * him; sp -= aw; aw = R(0); }
-        if (i == nim2) { su += ae * hip; sp -= ae; ae = R(0); }
-        R ap = an + as_ + ae + aw + at + ab + apnot - sp;
-        const R urfh = (R)p.urfh;
-        ap /= urfh;
-        su += (R(1) - urfh) * ap * hc;
-        g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw;
-        g.at[c] = at; g.ab[c] = ab; g.ap[c] = ap; g.su[c] = su;
-        // ---- residual (calculateResiduals(5)) ----
-        R r = (an * hjp + as_ * hjm + ae * hip + aw * him + at * hkp + ab * hkm + su) / ap - hc;
-        sumd += fabs((double)r);
-        sumh += fabs((double)hc);
-        // ---- block-correction sums (enhanceConvergenceSpeed(5)) ----
-        bl += (double)(ap - an - as_ - at - ab);
-        blp += (double)ae;
-        blm += (double)aw;
-        blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
-    }
-    // per-i partial sums over this block's j-rows and planes
-    __shared__ double sb[4][8][33];
-    sb[0][threadIdx.y][threadIdx.x] = bl;
-    sb[1][threadIdx.y][threadIdx.x] = blp;
-    sb[2][threadIdx.y][threadIdx.x] = blm;
-    sb[3][threadIdx.y][threadIdx.x] = blc;
-    __syncthreads();
-    if (threadIdx.y < 4 && i < nip) {
-        double s = 0.0;
-        for (int y = 0; y < 8; ++y) s += sb[threadIdx.y][y][threadIdx.x];
-        const int part = blockIdx.z * gridDim.y + blockIdx.y;
-        g.bc[((size_t)part * 4 + threadIdx.y) * nip + i] = s;
-    }
-    __syncthreads();
-    double v[2] = {sumd, sumh};
-    const int s[2] = {R_SUMD, R_SUMH};
-    const bool m[2] = {false, false};
-    const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    block_reduce_store<2>(v, s, m, red, blk);
-    (void)ni;
-}
-
-// ---------------------------------------------------------------------------
 // Block correction solve (enhanceConvergenceSpeed(5), CFDSolverManager.cpp:2334-2349)
 // and the energy residual resorh (:2099).  One CTA.
 // ---------------------------------------------------------------------------
+// Per-i sums of the block-correction partial rows in a fixed order: CTA (32 i x
+// 8 part-strides) per i-chunk and quantity.
+template <typename T>
+__global__ void __launch_bounds__(256) bc_reduce_kernel(Params p, Fields<T> g)
+{
+    __shared__ double sh[8][33];
+    const int i = blockIdx.x * 32 + threadIdx.x, w = blockIdx.y, nip = p.nip;
+    double s = 0.0;
+    for (int part = threadIdx.y; part < g.npart; part += 8)
+        s += g.bc[((size_t)part * 4 + w) * nip + i];
+    sh[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0) {
+        double t = 0.0;
+        for (int y = 0; y < 8; ++y) t += sh[y][threadIdx.x];
+        g.bcsum[(size_t)w * nip + i] = t;
+    }
+}
+
 template <typename T>
 __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, int nblk_asm,
                                      int check_finite)
@@ -340,12 +145,7 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
     extern __shared__ double sm[];  // 4 * nip
     const int nip = p.nip, nim1 = p.nim1, nim2 = p.nim2;
     double *bl = sm, *blp = sm + nip, *blm = sm + 2 * nip, *blc = sm + 3 * nip;
-    for (int q = threadIdx.x; q < 4 * nip; q += blockDim.x) {
-        int w = q / nip, i = q - w * nip;
-        double s = 0.0;
-        for (int part = 0; part < gd.npart; ++part) s += gd.bc[((size_t)part * 4 + w) * nip + i];
-        sm[q] = s;
-    }
+    for (int q = threadIdx.x; q < 4 * nip; q += blockDim.x) sm[q] = gd.bcsum[q];
     double sd = 0.0, sh = 0.0;
     for (int b = threadIdx.x; b < nblk_asm; b += blockDim.x) {
         sd += red_asm[(size_t)b * R_NSLOTS + R_SUMD];
@@ -397,6 +197,11 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
 template <typename T>
 __global__ void h2t_kernel(Params p, Fields<T> g, double *red)
 {
+    // Work unit: a 32-cell chunk of one x-line (the pitch nip is a multiple of
+    // 32, so every chunk lies in one row and each warp's lanes share j and k).
+    // A warp takes U chunks at a time and issues all their loads before any
+    // store, so the latency of one chunk overlaps the others.
+    constexpr int U = 4;
     const Status *st = g.st;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
     const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
@@ -405,49 +210,103 @@ __global__ void h2t_kernel(Params p, Fields<T> g, double *red)
     const double delt = st->delt;
     double tmax = -INFINITY, accul = 0.0, heatvol = 0.0;
     double fw = 0.0, fe = 0.0, fb = 0.0, ft = 0.0, fs = 0.0, fn = 0.0;
-    const size_t total = (size_t)nk * nj * nip;
     const size_t sj = nip, sk = (size_t)nj * nip;
-    for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-         c += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(c % nip);
-        if (i >= ni) continue;
-        const int j = (int)((c / nip) % nj), k = (int)(c / sk);
-        const double h = (double)g.h[c];
-        double fl, t;
-        if (h >= p.hlcal) {
-            fl = 1.0;
-            t = (h - p.hlcal) / p.acpl + p.tliquid;
-        } else if (h <= p.hsmelt) {
-            fl = 0.0;
-            t = (sqrt(p.acpb * p.acpb + 2 * p.acpa * h) - p.acpb) / p.acpa;
-        } else {
-            fl = (h - p.hsmelt) / (p.hlcal - p.hsmelt);
-            t = deltemp * fl + p.tsolid;
+    const int js = st->jstart, is0 = st->istart;
+    const double ts = p.tsolid;
+    const bool steady = p.steady != 0;
+    const int lane = threadIdx.x & 31;
+    const int cpr = nip >> 5;  // chunks per row
+    const long long nchunks = (long long)nk * nj * cpr;
+    const long long W = (long long)gridDim.x * (blockDim.x >> 5);
+    const long long w0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const double *dxw = g.dxpwinv, *dys = g.dypsinv, *dzb = g.dzpbinv;
+    for (long long q0 = w0; q0 < nchunks; q0 += W * U) {
+        T hv[U], hn[U], fln[U], rn[U], sv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long q = q0 + (long long)u * W;
+            const int r = (int)(q / cpr);
+            const int i = (int)(q - (long long)r * cpr) * 32 + lane;
+            const int k = r / nj, j = r - k * nj;
+            const bool ok = q < nchunks && i < ni;
+            const bool interior = ok && !steady && i >= 1 && i <= nim2 && j >= 1 && j <= njm2 &&
+                                  k >= 1 && k <= nkm2;
+            const size_t c = ok ? (size_t)r * nip + i : 0;
+            hv[u] = ok ? g.h[c] : T(0);
+            hn[u] = interior ? g.hnot[c] : T(0);
+            fln[u] = interior ? g.fraclnot[c] : T(0);
+            rn[u] = interior ? g.rho_nxt[c] : T(0);
+            sv[u] = interior ? g.sourceinput[c] : T(0);
         }
-        g.fracl[c] = (T)fl;
-        g.temp[c] = (T)t;
-        double tt = (double)(T)t;
-        if (tt > tmax) tmax = tt;
-        if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
-        if (!p.steady) {
-            double dh1 = h - (double)g.hnot[c] + ((double)(T)fl - (double)g.fraclnot[c]) * p.hlatnt;
-            double vol = volume_p(p, g, i, j, k);
-            accul += vol * (double)g.rho_nxt[c] * dh1 / delt;
-            heatvol += (double)g.sourceinput[c] * vol;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const long long q = q0 + (long long)u * W;
+            if (q >= nchunks) break;  // warp-uniform
+            const int r = (int)(q / cpr);
+            const int i = (int)(q - (long long)r * cpr) * 32 + lane;
+            const int k = r / nj, j = r - k * nj;
+            const size_t c = (size_t)r * nip + i;
+            const int ibase = i - lane;
+            if (ibase >= ni) continue;  // a padding chunk: warp-uniform
+            const unsigned act = (ibase + 32 <= ni) ? 0xffffffffu : ((1u << (ni - ibase)) - 1u);
+            if (i >= ni) continue;
+            const double h = (double)hv[u];
+            double fl, t;
+            if (h >= p.hlcal) {
+                fl = 1.0;
+                t = (h - p.hlcal) / p.acpl + p.tliquid;
+            } else if (h <= p.hsmelt) {
+                fl = 0.0;
+                t = (sqrt(p.acpb * p.acpb + 2 * p.acpa * h) - p.acpb) / p.acpa;
+            } else {
+                fl = (h - p.hsmelt) / (p.hlcal - p.hsmelt);
+                t = deltemp * fl + p.tsolid;
+            }
+            g.fracl[c] = (T)fl;
+            g.temp[c] = (T)t;
+            const double tt = (double)(T)t;
+            if (tt > tmax) tmax = tt;
+            // melt-pool scan candidates (BoundCondManager.cpp:318-417).  Most cells
+            // are solid, so each atomic is issued only when it can still change the
+            // value (candidates only move one way); the beam-row scalars are
+            // warp-reduced.
+            if (j == js && k >= 1 && k <= nkm2 && tt < ts && k > *(volatile int *)&g.mp_kb[i])
+                atomicMax(&g.mp_kb[i], k);
+            if (k == nkm1) {
+                if (j >= js && j <= njm2 && tt < ts && j < *(volatile int *)&g.mp_jup[i])
+                    atomicMin(&g.mp_jup[i], j);
+                if (j >= 1 && j <= js && tt < ts && j > *(volatile int *)&g.mp_jdn[i])
+                    atomicMax(&g.mp_jdn[i], j);
+                if (j == js) {  // row-uniform: every lane of the chunk with i < ni is here
+                    const int cmax = (i >= is0 && i < nim1 && tt <= ts) ? i : INT_MAX;
+                    const int cmin = (i >= 1 && i <= is0 && tt < ts) ? i : INT_MIN;
+                    const int wmin = __reduce_min_sync(act, cmax), wmax = __reduce_max_sync(act, cmin);
+                    if (lane == 0) {
+                        if (wmin != INT_MAX) atomicMin(&g.st->mp_imax, wmin);
+                        if (wmax != INT_MIN) atomicMax(&g.st->mp_imin, wmax);
+                    }
+                }
+            }
+            if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
+            if (!steady) {
+                const double dh1 = h - (double)hn[u] + ((double)(T)fl - (double)fln[u]) * p.hlatnt;
+                const double vol = volume_p(p, g, i, j, k);
+                accul += vol * (double)rn[u] * dh1 / delt;
+                heatvol += (double)sv[u] * vol;
+            }
+            if (i == 1)
+                fw += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - 1] - h) * dxw[1]);
+            if (i == nim2)
+                fe += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + 1] - h) * dxw[nim1]);
+            if (k == 1)
+                fb += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c - sk] - h) * dzb[1]);
+            if (k == nkm2)
+                ft += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c + sk] - h) * dzb[nkm1]);
+            if (j == 1)
+                fs += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - sj] - h) * dys[1]);
+            if (j == njm2)
+                fn += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + sj] - h) * dys[njm1]);
         }
-        const double *dx = g.dxpwinv, *dy = g.dypsinv, *dz = g.dzpbinv;
-        if (i == 1)
-            fw += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - 1] - h) * dx[1]);
-        if (i == nim2)
-            fe += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + 1] - h) * dx[nim1]);
-        if (k == 1)
-            fb += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c - sk] - h) * dz[1]);
-        if (k == nkm2)
-            ft += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c + sk] - h) * dz[nkm1]);
-        if (j == 1)
-            fs += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - sj] - h) * dy[1]);
-        if (j == njm2)
-            fn += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + sj] - h) * dy[njm1]);
     }
     double v[8] = {tmax, accul, heatvol, fw, fe, fb, ft, fs};
     const int s[8] = {R_TPEAK, R_ACCUL, R_HEATVOL, R_FW, R_FE, R_FB, R_FT, R_FS};
@@ -485,6 +344,21 @@ __device__ double reduce_slot(const double *red, int nb, int slot, bool is_max, 
     return r;
 }
 
+// Sentinels of the melt-pool scan candidates for the next outer iteration.
+template <typename T>
+__device__ void reset_scan_candidates(const Params &p, Fields<T> &g)
+{
+    for (int i = threadIdx.x; i < p.nip; i += blockDim.x) {
+        g.mp_kb[i] = 0;
+        g.mp_jup[i] = p.njm1;
+        g.mp_jdn[i] = 0;
+    }
+    if (threadIdx.x == 0) {
+        g.st->mp_imax = INT_MAX;
+        g.st->mp_imin = INT_MIN;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // getMeltPoolShape (BoundCondManager.cpp:280-447), one CTA.  The scans along
 // i/j/k are evaluated per column in parallel; the folds whose result depends on
@@ -513,6 +387,7 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
             st->width = 0.0;
             st->momentum_active = 0;
         }
+        reset_scan_candidates(p, g);
         return;
     }
     const int js = st->jstart, is0 = st->istart;
@@ -526,37 +401,25 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
     double *depv = colv, *wmax = colv + nip, *wmin = colv + 2 * nip;
     int *imaxc = (int *)(colv + 3 * nip);
     // length: first i >= istart on the top row with T <= Ts; last i <= istart with T < Ts
-    int cand_max = INT_MAX, cand_min = INT_MIN;
-    for (int i = is0 + (int)threadIdx.x; i < nim1; i += blockDim.x)
-        if (TT(i, js, nkm1) <= ts) cand_max = min(cand_max, i);
-    for (int i = 1 + (int)threadIdx.x; i <= is0; i += blockDim.x)
-        if (TT(i, js, nkm1) < ts) cand_min = max(cand_min, i);
-    // depth scan per column i: kb = first k (descending from nkm2) with T < Ts
-    // width scans per column i on the top plane
+    // (candidates gathered by h2t_kernel with integer atomics, read and reset here)
+    // depth: per column i, mp_kb = the largest k in 1..nkm2 with T < Ts on the beam
+    // plane (0 if none) -- the scan from nkm2 down visits nkm2..mp_kb+1.
+    // width: mp_jup = first j >= jstart with T < Ts (njm1 if none), mp_jdn = first
+    // j <= jstart going down with T < Ts (0 if none).
     int kmin_c = INT_MAX, jmax_c = INT_MIN, jmin_c = INT_MAX;
     for (int i = 1 + (int)threadIdx.x; i < nim1; i += blockDim.x) {
-        int k = nkm2;
-        for (; k > 0; k--)
-            if (TT(i, js, k) < ts) break;
-        if (k < nkm2) kmin_c = min(kmin_c, k + 1);
-        int j = js;
-        for (; j < njm1; j++)
-            if (TT(i, j, nkm1) < ts) break;
-        if (j > js) jmax_c = max(jmax_c, j - 1);
-        j = js;
-        for (; j > 0; j--)
-            if (TT(i, j, nkm1) < ts) break;
-        if (j < js) jmin_c = min(jmin_c, j + 1);
+        const int kb = g.mp_kb[i], ju = g.mp_jup[i], jd = g.mp_jdn[i];
+        if (kb < nkm2) kmin_c = min(kmin_c, kb + 1);
+        if (ju > js) jmax_c = max(jmax_c, ju - 1);
+        if (jd < js) jmin_c = min(jmin_c, jd + 1);
     }
     // block min/max of the integer candidates
     __shared__ int red_i[6];
     if (threadIdx.x == 0) {
-        red_i[0] = INT_MAX; red_i[1] = INT_MIN; red_i[2] = INT_MAX; red_i[3] = INT_MIN;
+        red_i[0] = st->mp_imax; red_i[1] = st->mp_imin; red_i[2] = INT_MAX; red_i[3] = INT_MIN;
         red_i[4] = INT_MAX;
     }
     __syncthreads();
-    atomicMin(&red_i[0], cand_max);
-    atomicMax(&red_i[1], cand_min);
     atomicMin(&red_i[2], kmin_c);
     atomicMax(&red_i[3], jmax_c);
     atomicMin(&red_i[4], jmin_c);
@@ -567,26 +430,27 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
     int jmax = max(js, red_i[3]) + 1;
     int jmin = min(js, red_i[4]) - 1;
     // per-column interpolated values for the order-dependent folds
+    // imaxc[i] bits: 1 = column enters the depth fold, 2 = the max-width fold,
+    // 4 = the min-width fold (the reference's `continue` tests), so that the
+    // sequential folds below read shared memory only.
     for (int i = 1 + (int)threadIdx.x; i < nim1; i += blockDim.x) {
-        imaxc[i] = 1;
-        if (kmin != 0) {
-            if (TT(i, js, kmin + 1) < ts) {
-                imaxc[i] = 0;
-            } else {
-                double dtdzzinv = (g.z[kmin] - g.z[kmin - 1]) / (TT(i, js, kmin) - TT(i, js, kmin - 1));
-                depv[i] = g.z[nkm1] - g.z[kmin] + (TT(i, js, kmin) - ts) * dtdzzinv;
-            }
+        int fl = 0;
+        if (kmin != 0 && !(TT(i, js, kmin + 1) < ts)) {
+            fl |= 1;
+            double dtdzzinv = (g.z[kmin] - g.z[kmin - 1]) / (TT(i, js, kmin) - TT(i, js, kmin - 1));
+            depv[i] = g.z[nkm1] - g.z[kmin] + (TT(i, js, kmin) - ts) * dtdzzinv;
         }
-        wmax[i] = NAN;
         if (jmax != js && !(TT(i, jmax - 1, nkm1) < ts)) {
+            fl |= 2;
             double dtdyyinv = (YY(jmax) - YY(jmax + 1)) / (TT(i, jmax, nkm1) - TT(i, jmax + 1, nkm1));
             wmax[i] = YY(jmax) + (ts - TT(i, jmax, nkm1)) * dtdyyinv;
         }
-        wmin[i] = NAN;
         if (jmin != js && !(TT(i, jmin + 1, nkm1) < ts)) {
+            fl |= 4;
             double dtdyyinv = (YY(jmin) - YY(jmin - 1)) / (TT(i, jmin, nkm1) - TT(i, jmin - 1, nkm1));
             wmin[i] = YY(jmin) + (ts - TT(i, jmin, nkm1)) * dtdyyinv;
         }
+        imaxc[i] = fl;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -601,17 +465,17 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
             depth = g.z[nkm1] - g.z[0];
         } else {
             for (int i = 1; i < nim1; i++)
-                if (imaxc[i]) depth = maxd(depv[i], depth);
+                if (imaxc[i] & 1) depth = maxd(depv[i], depth);
         }
         st->depth = depth;
         double yymax = g.y[0];
         if (jmax != js)
             for (int i = 1; i < nim1; i++)
-                if (!(TT(i, jmax - 1, nkm1) < ts)) yymax = maxd(wmax[i], yymax);
+                if (imaxc[i] & 2) yymax = maxd(wmax[i], yymax);
         double yymin = YY(js);
         if (jmin != js)
             for (int i = 1; i < nim1; i++)
-                if (!(TT(i, jmin + 1, nkm1) < ts)) yymin = mind(wmin[i], yymin);
+                if (imaxc[i] & 4) yymin = mind(wmin[i], yymin);
         st->width = yymax - yymin;
         st->imax = imax; st->imin = imin; st->kmin = kmin; st->kmax = nkm2;
         st->jmax = jmax; st->jmin = jmin;
@@ -627,6 +491,7 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
             ? max(0, st->iendm1 - st->istatp1 + 1) * max(0, st->jend - st->jstat + 1) * max(0, nkm1 - st->kstat)
             : 0;
     }
+    reset_scan_candidates(p, g);  // every reader passed the __syncthreads above
 }
 
 // ---------------------------------------------------------------------------
@@ -713,14 +578,18 @@ template <typename T> void launch_energy_bc(Inst<T> &I)
 {
     energy_bc_kernel<T><<<I.nb_bc, 256, 0, I.stream>>>(I.p, I.g, I.red_bc);
 }
-template <typename T> void launch_energy_assemble(Inst<T> &I)
-{
-    energy_assemble_kernel<T><<<I.asm_grid, dim3(32, 8), 0, I.stream>>>(I.p, I.g, I.red_asm);
-}
 template <typename T> void launch_block_correct(Inst<T> &I)
 {
+    bc_reduce_kernel<T><<<dim3(I.p.nip / 32, 4), dim3(32, 8), 0, I.stream>>>(I.p, I.g);
     block_correct_kernel<T><<<1, 1024, 4 * I.p.nip * sizeof(double), I.stream>>>(
         I.p, I.g, I.red_asm, I.nb_asm, I.check_finite);
+}
+// Resident 256-thread CTAs of h2t_kernel per SM (its grid is one full wave).
+template <typename T> int h2t_blocks_per_sm()
+{
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, h2t_kernel<T>, 256, 0);
+    return nb > 0 ? nb : 1;
 }
 template <typename T> void launch_h2t(Inst<T> &I)
 {
@@ -745,9 +614,9 @@ template <typename T> void launch_update_solutions(Inst<T> &I)
 #define AMCFD_INST(T)                                        \
     template void launch_laser<T>(Inst<T> &);               \
     template void launch_energy_bc<T>(Inst<T> &);           \
-    template void launch_energy_assemble<T>(Inst<T> &);     \
     template void launch_block_correct<T>(Inst<T> &);       \
     template void launch_h2t<T>(Inst<T> &);                 \
+    template int h2t_blocks_per_sm<T>();                    \
     template void launch_meltpool<T>(Inst<T> &);            \
     template void launch_converge<T>(Inst<T> &, double);    \
     template void launch_update_solutions<T>(Inst<T> &);

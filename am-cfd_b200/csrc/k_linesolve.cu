@@ -99,33 +99,112 @@ __global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g)
 template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) { return __ldcg(ptr); }
 
 // ---------------------------------------------------------------------------
-// One x-line solved by one warp.  `row` is the offset of node (0, j, k);
-// cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] are the fixed ends.
-// sb: 3 * nmax values of per-warp shared scratch.
+// Per-warp staging of one x-line.  The eight pass-invariant coefficient rows of
+// the line (at ab an as su cf pr iden) are brought into shared memory with
+// TMA bulk copies completing on a per-warp mbarrier; the copies are issued
+// before the exact-order kernel waits on its neighbours, so their latency
+// overlaps the wait.  Rows start 16-byte aligned: the copy starts at the
+// aligned cell ib <= i0 and is rounded up to whole 16-byte units (never past
+// the padded row, nip being a multiple of 32 cells).
+// ---------------------------------------------------------------------------
+enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Bounded wait for the phase `parity` of a per-warp mbarrier (all lanes poll).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Status *st)
+{
+    const uint32_t a = smem_u32(bar);
+    for (long long it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -1;
+    return false;
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int ib, int ie, T *sl,
+                                           int nmax, uint64_t *bar)
+{
+    // lane 0 only.  Previous generic-proxy use of this shared buffer is ordered
+    // before the asynchronous copies by the proxy fence.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
+    const uint32_t b = smem_u32(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
+                 "r"(bytes * S_N) : "memory");
+    const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.cf, g.pr, g.iden};
+#pragma unroll
+    for (int q = 0; q < S_N; ++q) {
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+            ::"r"(smem_u32(sl + (size_t)q * nmax)), "l"(src[q] + row + ib), "r"(bytes), "r"(b)
+            : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// One x-line solved by one warp from its staged rows.  `row` is the offset of
+// node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
+// ends; sl holds the line from cell ib on.
 // ---------------------------------------------------------------------------
 template <typename T, bool COHERENT>
-__device__ __forceinline__ void solve_line(const Fields<T> &g, T *phi, size_t row, int i0, int i1,
-                                           size_t sj, size_t sk, T *sb, int nmax)
+__device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
+                                             size_t sj, size_t sk, T *sl, int nmax)
 {
     const int lane = threadIdx.x & 31;
+    T *sat = sl + S_AT * nmax, *sab = sl + S_AB * nmax, *san = sl + S_AN * nmax,
+      *sas = sl + S_AS * nmax, *se = sl + S_SU * nmax, *sc = sl + S_CF * nmax,
+      *sp = sl + S_PR * nmax, *sid = sl + S_ID * nmax;
+    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
+    // right-hand side e_i = d_i / den_i, coalesced neighbour rows; four
+    // iterations' neighbour loads are issued before any result is stored
+    constexpr int U = 4;
+    for (int i = ib + lane; i <= i1; i += 32 * U) {
+        T nt[U], nb[U], nn[U], ns[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int iu = i + 32 * u;
+            const bool ok = iu >= i0 && iu <= i1;
+            const size_t c = row + (ok ? iu : i0);
+            nt[u] = ok ? ldp(c + sk) : T(0);
+            nb[u] = ok ? ldp(c - sk) : T(0);
+            nn[u] = ok ? ldp(c + sj) : T(0);
+            ns[u] = ok ? ldp(c - sj) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int iu = i + 32 * u;
+            if (iu < i0 || iu > i1) continue;
+            const int s = iu - ib;
+            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + se[s];
+            se[s] = d * sid[s];
+        }
+    }
+    __syncwarp();
     const int n = i1 - i0 + 1;
     const int L = (n + 31) >> 5;
     const int a = i0 + lane * L;
     const int b = min(a + L, i1 + 1);
-    T *se = sb, *sc = sb + nmax, *sp = sb + 2 * nmax;
-    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
-    // forward: qr_i = cf_i qr_{i-1} + e_i,  e_i = d_i / den_i
+    // forward: qr_i = cf_i qr_{i-1} + e_i
     T A = T(1), B = T(0);
     for (int i = a; i < b; ++i) {
-        size_t c = row + i;
-        T d = g.at[c] * ldp(c + sk) + g.ab[c] * ldp(c - sk) + g.an[c] * ldp(c + sj) +
-              g.as[c] * ldp(c - sj) + g.su[c];
-        T e = d * g.iden[c];
-        T cfi = g.cf[c];
-        se[i - i0] = e;
-        sc[i - i0] = cfi;
-        sp[i - i0] = g.pr[c];
-        B = cfi * B + e;
+        const T cfi = sc[i - ib];
+        B = cfi * B + se[i - ib];
         A = cfi * A;
     }
 #pragma unroll
@@ -142,15 +221,15 @@ __device__ __forceinline__ void solve_line(const Fields<T> &g, T *phi, size_t ro
     if (lane == 0) { Ae = T(1); Be = T(0); }
     T q = Ae * ldp(row + i0 - 1) + Be;
     for (int i = a; i < b; ++i) {
-        q = sc[i - i0] * q + se[i - i0];
-        se[i - i0] = q;
+        q = sc[i - ib] * q + se[i - ib];
+        se[i - ib] = q;
     }
     // backward: phi_i = pr_i phi_{i+1} + qr_i
     A = T(1);
     B = T(0);
     for (int i = b - 1; i >= a; --i) {
-        T pri = sp[i - i0];
-        B = pri * B + se[i - i0];
+        const T pri = sp[i - ib];
+        B = pri * B + se[i - ib];
         A = pri * A;
     }
 #pragma unroll
@@ -167,9 +246,20 @@ __device__ __forceinline__ void solve_line(const Fields<T> &g, T *phi, size_t ro
     if (lane == 31) { Ae = T(1); Be = T(0); }
     T x = Ae * ldp(row + i1 + 1) + Be;
     for (int i = b - 1; i >= a; --i) {
-        x = sp[i - i0] * x + se[i - i0];
-        phi[row + i] = x;
+        x = sp[i - ib] * x + se[i - ib];
+        se[i - ib] = x;
     }
+    __syncwarp();
+    for (int i = i0 + lane; i <= i1; i += 32) phi[row + i] = se[i - ib];
+}
+
+// Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).
+template <typename T>
+__device__ __forceinline__ void stage_window(int i0, int i1, int &ib, int &ie)
+{
+    constexpr int V = 16 / sizeof(T);
+    ib = i0 & ~(V - 1);
+    ie = (i1 + 1 + V - 1) & ~(V - 1);
 }
 
 // Bounded wait until *f >= target (wrap-safe); false on timeout or a raised error.
@@ -219,16 +309,24 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
     }
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
     const int nmax = p.nip;
-    T *sb = reinterpret_cast<T *>(smraw) + (size_t)warp * 3 * nmax;
+    T *sl = reinterpret_cast<T *>(smraw) + (size_t)warp * S_N * nmax;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<T *>(smraw) +
+                                                 (size_t)nwarps * S_N * nmax) + warp;
+    if (lane == 0) mbar_init(bar);
+    __syncwarp();
+    uint32_t parity = 0;
     const int base = (int)(seq_s * 4ull);
-    if (active_s) {
-        int i0, i1, j0, j1, k0, k1;
-        box_of<BOX>(p, st, i0, i1, j0, j1, k0, k1);
+    int i0, i1, j0, j1, k0, k1;
+    box_of<BOX>(p, st, i0, i1, j0, j1, k0, k1);
+    if (active_s && i1 >= i0) {
         const int M = k1 - k0 + 1;
         const int nj = p.nj, nip = p.nip;
         const size_t sj = nip, sk = (size_t)nj * nip;
         const int nt = nt_s;
+        int ib, ie;
+        stage_window<T>(i0, i1, ib, ie);
         while (true) {
             unsigned long long tk = 0;
             if (lane == 0) tk = atomicAdd(ticketp, 1ull);
@@ -237,8 +335,10 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
             int2 e = tickets[tk];
             const int m = e.x, s = e.y >> 16, jj = e.y & 0xffff;
             const int ks = m / M, k = k1 - (m - ks * M), j = j0 + jj, v = 2 * ks + s;
+            const size_t row = cidx(0, j, k, nj, nip);
             int ok = 1;
             if (lane == 0) {
+                stage_line<T>(g, row, ib, ie, sl, nmax, bar);  // overlaps the waits below
                 const int where = k * nj + j;
                 if (ok && j > j0) ok = wait_ge(&flags[k * nj + j - 1], base + v + 1, st, where);
                 if (ok && j < j1 && v > 0) ok = wait_ge(&flags[k * nj + j + 1], base + v, st, where);
@@ -247,9 +347,12 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
                 __threadfence();
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);
-            if (!ok) break;
+            // the staged copies complete whatever the waits decided
+            const bool staged = mbar_wait(bar, parity, st);
+            parity ^= 1u;
+            if (!ok || !staged) break;
             __syncwarp();
-            solve_line<T, true>(g, phi, cidx(0, j, k, nj, nip), i0, i1, sj, sk, sb, nmax);
+            solve_staged<T, true>(phi, row, i0, i1, ib, sj, sk, sl, nmax);
             __threadfence();
             __syncwarp();
             if (lane == 0) atomicExch(&flags[k * nj + j], base + v + 1);
@@ -281,12 +384,19 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
     box_of<BOX>(p, st, i0, i1, j0, j1, k0, k1);
     const int J = j1 - j0 + 1, K = k1 - k0 + 1;
     if (J <= 0 || K <= 0 || i1 < i0) return;
-    const int warp = threadIdx.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
     const int nmax = p.nip;
-    T *sb = reinterpret_cast<T *>(smraw) + (size_t)warp * 3 * nmax;
+    T *sl = reinterpret_cast<T *>(smraw) + (size_t)warp * S_N * nmax;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<T *>(smraw) +
+                                                 (size_t)wpb * S_N * nmax) + warp;
+    if (lane == 0) mbar_init(bar);
+    __syncwarp();
+    uint32_t parity = 0;
     const int nj = p.nj, nip = p.nip;
     const size_t sj = nip, sk = (size_t)nj * nip;
-    const int wpb = blockDim.x >> 5;
+    int ib, ie;
+    stage_window<T>(i0, i1, ib, ie);
     // lines of this colour: for each k, j runs over one parity
     const int half = (J + 1) / 2;
     const int nl = half * K;
@@ -296,7 +406,14 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
         int jpar = ((color - k - j0) % 2 + 2) % 2;  // offset of the first j of this colour
         int j = j0 + jpar + 2 * r;
         if (j > j1) continue;
-        solve_line<T, false>(g, phi, cidx(0, j, k, nj, nip), i0, i1, sj, sk, sb, nmax);
+        const size_t row = cidx(0, j, k, nj, nip);
+        if (lane == 0) stage_line<T>(g, row, ib, ie, sl, nmax, bar);
+        const bool staged = mbar_wait(bar, parity, g.st);
+        parity ^= 1u;
+        if (!staged) return;
+        __syncwarp();
+        solve_staged<T, false>(phi, row, i0, i1, ib, sj, sk, sl, nmax);
+        __syncwarp();
     }
 }
 
@@ -365,13 +482,14 @@ template <typename T> void launch_energy_factor(Inst<T> &I)
 }
 template <typename T> void launch_box_factor(Inst<T> &I)
 {
-    int grid = std::min((I.max_lines + 31) / 32, I.sm_count * 4);
+    // the box is small (a melt pool); one CTA per SM covers up to 4736 lines per pass
+    int grid = std::min((I.max_lines + 31) / 32, I.sm_count);
     factor_kernel<T, true><<<grid, 256, 0, I.stream>>>(I.p, I.g);
 }
 template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
 {
     const int warps = I.exact_warps;
-    const size_t smem = (size_t)warps * 3 * I.p.nip * sizeof(T);
+    const size_t smem = I.line_smem;
     if (I.order == AMCFD_ORDER_EXACT) {
         Status *st = I.g.st;
         if (box)
@@ -385,6 +503,7 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
     } else {
         int lines = box ? I.max_lines : (I.p.nj - 2) * (I.p.nk - 2);
         int grid = std::max(1, std::min((lines / 2 + warps - 1) / warps + 1, I.sm_count * 16));
+        if (box) grid = std::min(grid, I.sm_count);  // melt-pool box: a few hundred lines
         for (int sweep = 0; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color) {
                 if (box)
