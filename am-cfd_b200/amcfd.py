@@ -14,7 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import Dict, Optional
+from typing import Dict, Optional, Sequence
 
 import numpy as np
 
@@ -116,6 +116,7 @@ def lib() -> C.CDLL:
             L.amcfd_run_steps.argtypes = [VP, _I, P(AmcfdReport), P(_D)]
             L.amcfd_kernel_launches.argtypes = [VP]
             L.amcfd_kernel_launches.restype = C.c_longlong
+            L.amcfd_run_batch.argtypes = [P(VP), _I, _I, _I, P(AmcfdReport), P(_I)]
         _lib = L
     return _lib
 
@@ -157,6 +158,21 @@ class Deck:
             self.close()
         except Exception:
             pass
+
+
+def run_batch(solvers: Sequence["Solver"], nsteps: int, nthreads: int = 0):
+    """amcfd_run_batch: nsteps steps of every solver, concurrently on one GPU.
+    Returns (reports, status codes) in the order of `solvers`; raises on the first
+    failure after all instances have finished."""
+    n = len(solvers)
+    hs = (C.c_void_p * max(n, 1))(*[s._h for s in solvers])
+    reps = (AmcfdReport * max(n, 1))()
+    st = (_I * max(n, 1))()
+    rc = lib().amcfd_run_batch(hs, n, nsteps, nthreads, reps, st)
+    if rc != 0:
+        q = next(i for i in range(n) if st[i] != 0)
+        raise AmcfdError(rc, f"instance {q}: " + lib().amcfd_last_error(solvers[q]._h).decode())
+    return [reps[q].as_dict() for q in range(n)], [st[q] for q in range(n)]
 
 
 class Solver:

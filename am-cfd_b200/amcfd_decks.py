@@ -223,7 +223,7 @@ def config1(steps: Optional[int] = None) -> Deck:
     return d
 
 
-def config2(n: int = 64, seed: int = SEED) -> List[Deck]:
+def config2(n: int = 64, seed: int = SEED, steps: int = 300) -> List[Deck]:
     """Process-parameter sweep: n single-track instances, grids drawn
     uniformly between 60 x 30 x 20 and 240 x 120 x 60 cells with the domain
     scaled from the config-0 domain by the same factor; P ~ U[100, 400] W,
@@ -242,7 +242,7 @@ def config2(n: int = 64, seed: int = SEED) -> List[Deck]:
                  y_zones=[(ly * 0.35, ny1, -1.5), (ly * 0.30, ny - 2 * ny1, 1.0), (ly * 0.35, ny1, 1.5)],
                  z_zones=[(lz * 5 / 7, nz1, -1.5), (lz * 2 / 7, nz - nz1, 1.0)],
                  power=P, radius=rb, single_track=(1.0, lx * 0.125, ly * 0.5, v),
-                 finaltime=300 * 1e-5)
+                 finaltime=(steps - 0.5) * 1e-5)
         decks.append(d)
     return decks
 

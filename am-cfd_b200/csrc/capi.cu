@@ -54,6 +54,11 @@ struct amcfd_ctx {
     double last_ms[16] = {0};
     bool events = false;
     long long launches = 0;  // kernels launched since creation
+    // CUDA graphs of one outer iteration, by [timing events recorded][property parity]:
+    // the iteration swaps the current/next property buffers, so two graphs alternate.
+    bool use_graphs = false;
+    cudaGraphExec_t gexec[2][2] = {};
+    const void *diff_a = nullptr;  // the current-property buffer of parity 0
 };
 
 #define CK(call)                                                                          \
@@ -482,6 +487,75 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase)
 // 0 energy BC+assembly+block correction, 1 line factorisation, 2 energy line
 // sweeps, 3 H->T + melt pool, 4 momentum chain, 5 convergence, 6 laser,
 // 7 push-back, 8 outer iterations run, 9 energy-sweep launches.
+// Event record; under stream capture it must become an event node of the graph
+// (the external flag is only valid while capturing).
+static inline void rec(amcfd_ctx *ctx, int q, bool capturing)
+{
+    if (capturing)
+        cudaEventRecordWithFlags(ctx->ev[q], ctx->stream, cudaEventRecordExternal);
+    else
+        cudaEventRecord(ctx->ev[q], ctx->stream);
+}
+
+// The launch sequence of one outer iteration (iterativeLoopSolve body,
+// CFDSolverManager.cpp:601-719); ends with the property-buffer swap.
+template <typename T>
+static void launch_iteration(amcfd_ctx *ctx, Inst<T> &I, bool capturing)
+{
+    const bool ev = ctx->events;
+    if (ev) rec(ctx, 0, capturing);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_ASSEMBLE);
+    if (ev) rec(ctx, 1, capturing);
+    launch_energy_factor<T>(I);
+    if (ev) rec(ctx, 2, capturing);
+    launch_energy_sweeps<T>(I);
+    if (ev) rec(ctx, 3, capturing);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
+    if (ev) rec(ctx, 4, capturing);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_MOMENTUM);
+    if (ev) rec(ctx, 5, capturing);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_CONVERGE);
+    if (ev) rec(ctx, 6, capturing);
+}
+
+// One outer iteration replayed from a CUDA graph.  Every launch of an iteration
+// has a fixed grid and reads its data-dependent extents (the momentum box, the
+// sweep tickets) from the device status block, so the graph captured on the
+// first iteration of each parity is valid for every later one.
+template <typename T>
+static int launch_iteration_graph(amcfd_ctx *ctx, Inst<T> &I)
+{
+    const int par = (const void *)I.g.diff_cur == ctx->diff_a ? 0 : 1;
+    cudaGraphExec_t &ge = ctx->gexec[ctx->events ? 1 : 0][par];
+    if (!ge) {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        launch_iteration<T>(ctx, I, true);  // swaps the property buffers
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (e != cudaSuccess || !graph) {
+            cudaGetLastError();
+            ctx->err = std::string("graph capture: ") + cudaGetErrorString(e);
+            return AMCFD_E_CUDA;
+        }
+        e = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ge = nullptr;
+            ctx->err = std::string("graph instantiate: ") + cudaGetErrorString(e);
+            return AMCFD_E_CUDA;
+        }
+    } else {
+        swap_props<T>(I);
+    }
+    CK(cudaGraphLaunch(ge, ctx->stream));
+    return 0;
+}
+
+// Timing slots of amcfd_last_timing (accumulated device ms while profiling):
+// 0 energy BC+assembly+block correction, 1 line factorisation, 2 energy line
+// sweeps, 3 H->T + melt pool, 4 momentum chain, 5 convergence, 6 laser,
+// 7 push-back, 8 outer iterations run, 9 energy-sweep launches.
 template <typename T>
 static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
 {
@@ -491,20 +565,11 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
         ctx->niter++;
         ctx->itertot++;
         const bool ev = ctx->events;
-        if (ev) cudaEventRecord(ctx->ev[0], ctx->stream);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_ASSEMBLE);
-        if (ev) cudaEventRecord(ctx->ev[1], ctx->stream);
-        launch_energy_factor<T>(I);
-        if (ev) cudaEventRecord(ctx->ev[2], ctx->stream);
-        launch_energy_sweeps<T>(I);
-        if (ev) cudaEventRecord(ctx->ev[3], ctx->stream);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
-        if (ev) cudaEventRecord(ctx->ev[4], ctx->stream);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_MOMENTUM);
-        if (ev) cudaEventRecord(ctx->ev[5], ctx->stream);
-        run_phase_impl<T>(ctx, I, AMCFD_PHASE_CONVERGE);
-        if (ev) cudaEventRecord(ctx->ev[6], ctx->stream);
+        if (ctx->use_graphs) {
+            if ((rc = launch_iteration_graph<T>(ctx, I))) return rc;
+        } else {
+            launch_iteration<T>(ctx, I, false);
+        }
         for (int ph = AMCFD_PHASE_ENERGY_ASSEMBLE; ph <= AMCFD_PHASE_CONVERGE; ++ph)
             ctx->launches += phase_launches(ctx, ph);
         if ((rc = read_status(ctx))) return rc;
@@ -563,6 +628,7 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->device = opts->device;
         ctx->order = opts->order;
         ctx->precision = opts->precision;
+        ctx->use_graphs = opts->use_graphs != 0;
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");
@@ -615,6 +681,8 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     int rc = ctx->precision == AMCFD_PREC_FP64 ? setup_instance<double>(ctx, ctx->I64)
                                                : setup_instance<float>(ctx, ctx->I32);
     if (rc) return rc;
+    ctx->diff_a = ctx->precision == AMCFD_PREC_FP64 ? (const void *)ctx->I64.g.diff_cur
+                                                    : (const void *)ctx->I32.g.diff_cur;
     int cf = opts ? opts->check_finite : 0;
     ctx->I64.check_finite = cf;
     ctx->I32.check_finite = cf;
@@ -629,6 +697,9 @@ void amcfd_destroy(amcfd_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    for (auto &row : ctx->gexec)
+        for (auto &ge : row)
+            if (ge) cudaGraphExecDestroy(ge);
     for (int q = 0; q < 16; q++)
         if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -16,9 +16,12 @@
 namespace amcfd {
 
 constexpr int kTX = 32, kTY = 8, kKSEG = 16;
+// resident CTAs per SM the register budget is sized for (three FP32 CTAs spill and
+// measured slower than two)
+template <typename T> constexpr int asm_min_blocks() { return 2; }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 2) energy_assemble_kernel(Params p, Fields<T> g, double *red)
+__global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kernel(Params p, Fields<T> g, double *red)
 {
     using R = T;
     __shared__ R s_d[kTY + 2][kTX + 2], s_h[kTY + 2][kTX + 2], s_f[kTY + 2][kTX + 2],

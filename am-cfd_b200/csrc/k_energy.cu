@@ -195,7 +195,7 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
 // heat accumulation and volumetric heat input.  H->T is evaluated in FP64.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void h2t_kernel(Params p, Fields<T> g, double *red)
+__global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, double *red)
 {
     // Work unit: a 32-cell chunk of one x-line (the pitch nip is a multiple of
     // 32, so every chunk lies in one row and each warp's lanes share j and k).
@@ -208,8 +208,12 @@ __global__ void h2t_kernel(Params p, Fields<T> g, double *red)
               nkm2 = p.nkm2;
     const double deltemp = p.tliquid - p.tsolid;
     const double delt = st->delt;
+    // The FP64 build divides exactly as the reference; the FP32 build keeps the
+    // inversion in FP64 but multiplies by reciprocals formed once per launch.
+    constexpr bool kExact = sizeof(T) == sizeof(double);
+    const double inv_acpl = 1.0 / p.acpl, inv_acpa = 1.0 / p.acpa,
+                 inv_mush = 1.0 / (p.hlcal - p.hsmelt), inv_delt = 1.0 / delt;
     double tmax = -INFINITY, accul = 0.0, heatvol = 0.0;
-    double fw = 0.0, fe = 0.0, fb = 0.0, ft = 0.0, fs = 0.0, fn = 0.0;
     const size_t sj = nip, sk = (size_t)nj * nip;
     const int js = st->jstart, is0 = st->istart;
     const double ts = p.tsolid;
@@ -254,12 +258,13 @@ __global__ void h2t_kernel(Params p, Fields<T> g, double *red)
             double fl, t;
             if (h >= p.hlcal) {
                 fl = 1.0;
-                t = (h - p.hlcal) / p.acpl + p.tliquid;
+                t = (kExact ? (h - p.hlcal) / p.acpl : (h - p.hlcal) * inv_acpl) + p.tliquid;
             } else if (h <= p.hsmelt) {
                 fl = 0.0;
-                t = (sqrt(p.acpb * p.acpb + 2 * p.acpa * h) - p.acpb) / p.acpa;
+                const double root = sqrt(p.acpb * p.acpb + 2 * p.acpa * h) - p.acpb;
+                t = kExact ? root / p.acpa : root * inv_acpa;
             } else {
-                fl = (h - p.hsmelt) / (p.hlcal - p.hsmelt);
+                fl = kExact ? (h - p.hsmelt) / (p.hlcal - p.hsmelt) : (h - p.hsmelt) * inv_mush;
                 t = deltemp * fl + p.tsolid;
             }
             g.fracl[c] = (T)fl;
@@ -291,21 +296,42 @@ __global__ void h2t_kernel(Params p, Fields<T> g, double *red)
             if (!steady) {
                 const double dh1 = h - (double)hn[u] + ((double)(T)fl - (double)fln[u]) * p.hlatnt;
                 const double vol = volume_p(p, g, i, j, k);
-                accul += vol * (double)rn[u] * dh1 / delt;
+                accul += kExact ? vol * (double)rn[u] * dh1 / delt : vol * (double)rn[u] * dh1 * inv_delt;
                 heatvol += (double)sv[u] * vol;
             }
-            if (i == 1)
-                fw += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - 1] - h) * dxw[1]);
-            if (i == nim2)
-                fe += area_jk(p, g, j, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + 1] - h) * dxw[nim1]);
-            if (k == 1)
-                fb += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c - sk] - h) * dzb[1]);
-            if (k == nkm2)
-                ft += area_ij(p, g, i, j) * ((double)g.diff_nxt[c] * ((double)g.h[c + sk] - h) * dzb[nkm1]);
-            if (j == 1)
-                fs += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c - sj] - h) * dys[1]);
-            if (j == njm2)
-                fn += area_ik(p, g, i, k) * ((double)g.diff_nxt[c] * ((double)g.h[c + sj] - h) * dys[njm1]);
+        }
+    }
+    // Boundary conduction fluxes (BoundCondManager.cpp:778-843): a second pass
+    // over the six interior boundary layers only, so that the bulk loop above
+    // carries no flux accumulators.  Face f's layer is a 2-D index set.
+    double fw = 0.0, fe = 0.0, fb = 0.0, ft = 0.0, fs = 0.0, fn = 0.0;
+    {
+        const int I = nim2, J = njm2, K = nkm2;  // interior extents
+        const long long nx = (long long)J * K, ny = (long long)I * K, nz = (long long)I * J;
+        const long long nall = 2 * (nx + ny + nz);
+        const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long nthr = (long long)gridDim.x * blockDim.x;
+        for (long long q = tid; q < nall; q += nthr) {
+            long long r = q;
+            int face, a, b;  // face 0..5 = W E B T S N
+            if (r < 2 * nx) { face = (int)(r / nx); r %= nx; a = (int)(r % J); b = (int)(r / J); }
+            else if ((r -= 2 * nx) < 2 * nz) { face = 2 + (int)(r / nz); r %= nz; a = (int)(r % I); b = (int)(r / I); }
+            else { r -= 2 * nz; face = 4 + (int)(r / ny); r %= ny; a = (int)(r % I); b = (int)(r / I); }
+            int i, j, k;
+            if (face < 2) { i = face == 0 ? 1 : nim2; j = 1 + a; k = 1 + b; }
+            else if (face < 4) { k = face == 2 ? 1 : nkm2; i = 1 + a; j = 1 + b; }
+            else { j = face == 4 ? 1 : njm2; i = 1 + a; k = 1 + b; }
+            const size_t c = cidx(i, j, k, nj, nip);
+            const double h = (double)g.h[c];
+            const double dn = (double)g.diff_nxt[c];
+            switch (face) {
+            case 0: fw += area_jk(p, g, j, k) * (dn * ((double)g.h[c - 1] - h) * dxw[1]); break;
+            case 1: fe += area_jk(p, g, j, k) * (dn * ((double)g.h[c + 1] - h) * dxw[nim1]); break;
+            case 2: fb += area_ij(p, g, i, j) * (dn * ((double)g.h[c - sk] - h) * dzb[1]); break;
+            case 3: ft += area_ij(p, g, i, j) * (dn * ((double)g.h[c + sk] - h) * dzb[nkm1]); break;
+            case 4: fs += area_ik(p, g, i, k) * (dn * ((double)g.h[c - sj] - h) * dys[1]); break;
+            default: fn += area_ik(p, g, i, k) * (dn * ((double)g.h[c + sj] - h) * dys[njm1]); break;
+            }
         }
     }
     double v[8] = {tmax, accul, heatvol, fw, fe, fb, ft, fs};

@@ -144,6 +144,8 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--order", default="redblack", choices=["redblack", "exact"])
     ap.add_argument("--config", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--graphs", type=int, default=1, choices=[0, 1],
+                    help="replay each outer iteration from a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 exact-order comparison run")
     args = ap.parse_args()
@@ -200,7 +202,7 @@ def main():
     d = amcfd.Deck(path)
     ni, nj, nk = d.dims
     ncell = (ni - 2) * (nj - 2) * (nk - 2)
-    s = amcfd.Solver(d, order=order, precision=prec, device=dev)
+    s = amcfd.Solver(d, order=order, precision=prec, device=dev, use_graphs=args.graphs)
     s.run_steps(warmup)
 
     def barrier():
@@ -250,9 +252,10 @@ def main():
     peak, peak_kind = _peaks()
     w = 4 if prec == amcfd.PREC_FP32 else 8
     fam = max(WORDS, key=lambda k: prof[k])
-    nlaunch = iters * (1 if fam != "energy_sweeps" else 1)
+    # the sweep family is 8 (red-black) or 1 (exact order) launches per iteration
+    nlaunch = prof["sweep_launches"] if fam == "energy_sweeps" else iters
     avg_ms = prof[fam] / max(nlaunch, 1)
-    alg_bytes = WORDS[fam] * ncell * w
+    alg_bytes = WORDS[fam] * ncell * w * iters / max(nlaunch, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     tr = TRAFFIC_PER_CELL.get(f"{fam}:{args.precision}:{args.order}")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -264,7 +267,8 @@ def main():
     extra = {}
     if not args.no_compare and rank == 0:
         # the plain FP64 exact-order solve of the same steps, for the speed-up at equal iterations
-        s64 = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, device=dev)
+        s64 = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, device=dev,
+                           use_graphs=args.graphs)
         s64.run_steps(1)
         nref = min(args.steps, 3)
         _, ms64 = s64.run_steps(nref)
@@ -288,7 +292,7 @@ def main():
                 "steps": args.steps, "warmup": warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32" if prec == amcfd.PREC_FP32 else "f64", "data": "synthetic deck",
-                "config": dict(cfg_desc, precision=args.precision, order=args.order,
+                "config": dict(cfg_desc, precision=args.precision, order=args.order, graphs=args.graphs,
                                parallelism=f"replicas{world}"),
                 "cell_iters_per_s": cips, "outer_iters": iters, "gpu_launches": launches,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,

@@ -198,6 +198,18 @@ int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, doubl
 /* Number of kernels the context has launched since creation. */
 long long amcfd_kernel_launches(const amcfd_ctx *ctx);
 
+/* Parameter sweep over independent instances: runs nsteps time steps of every
+ * context in ctxs[0..n), each on its own stream, spread over nthreads host threads
+ * (0 = one per context, at most 64).  A thread takes the next context in array
+ * order and runs all its steps, so pass the contexts largest first.  reports[q]
+ * receives the last step's report of ctxs[q] and status[q] its return code (0, or
+ * a negative AMCFD_E_* code; that context's amcfd_last_error says why); either may
+ * be NULL.  Returns 0 when every context succeeded, else the first failing code in
+ * array order.  The reference runs one instance per process (main.cpp:25-233); a
+ * sweep is many such runs. */
+int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nthreads,
+                    amcfd_step_report *reports, int *status);
+
 /* Energy residual without any device allocation.  No counterpart in the reference:
  * it exists for callers that cannot let a library allocate device memory (an
  * application that owns all device memory through its own pool, or one under a

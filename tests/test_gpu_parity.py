@@ -152,3 +152,24 @@ def test_fp32_close_to_fp64(deckdir):
     assert rel_l2(s32.get("temp"), s64.get("temp")) < 1e-3
     s64.close()
     s32.close()
+
+
+@pytest.mark.parametrize("prec,order", [(0, 0), (1, 1)])
+def test_graph_replay_bit_identical(prec, order, deckdir):
+    """Outer iterations replayed from CUDA graphs give the same bits as direct
+    launches (FP64 exact order and FP32 red-black), with and without timing."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.small("graphs", steps=5, toolpath=True).write(deckdir))
+    a = amcfd.Solver(d, order=order, precision=prec, use_graphs=0)
+    b = amcfd.Solver(d, order=order, precision=prec, use_graphs=1)
+    for s in range(5):
+        a.profile(s % 2 == 1)  # alternate timed and untimed iterations on both paths
+        b.profile(s % 2 == 1)
+        ra, rb = a.step(), b.step()
+        for k in ("niter", "tpeak", "alen", "depth", "width", "resorh", "resorm", "ratio"):
+            assert ra[k] == rb[k], (s, k, ra[k], rb[k])
+        for f in FIELDS:
+            assert np.array_equal(a.get(f), b.get(f)), (s, f)
+    a.close()
+    b.close()
