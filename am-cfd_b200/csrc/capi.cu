@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "amcfd.h"
+#include "async.cuh"
 #include "kernels.cuh"
 
 namespace amcfd {
@@ -23,6 +24,33 @@ template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
 template <typename T> void set_sweep_smem_limit(size_t smem);
 dim3 energy_assemble_grid(const Params &p);
 template <typename T> int h2t_blocks_per_sm();
+template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
+                                             long long rows, int sm_count, cudaStream_t s);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+int encode_field_map(CUtensorMap *map, const void *base, int elem, int nip, int nj, int nk, int bx,
+                     int by)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &qr) !=
+                cudaSuccess ||
+            qr != cudaDriverEntryPointSuccess || !ptr)
+            return -1;
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)nip, (cuuint64_t)nj, (cuuint64_t)nk};
+    const cuuint64_t strides[2] = {(cuuint64_t)nip * elem, (cuuint64_t)nip * nj * elem};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r;
+}
 }  // namespace amcfd
 
 using namespace amcfd;
@@ -59,6 +87,8 @@ struct amcfd_ctx {
     bool use_graphs = false;
     cudaGraphExec_t gexec[2][2] = {};
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
+    double *pack = nullptr;        // FP64 read-out staging (ni*nj*nk), made on first use
+    int sm_count = 0;
 };
 
 #define CK(call)                                                                          \
@@ -292,6 +322,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     I.red_h2t = I.red_asm + (size_t)I.nb_asm * R_NSLOTS;
     I.red_mom = I.red_h2t + (size_t)I.nb_h2t * R_NSLOTS;
     g.red = red;
+    if (make_assemble_maps<T>(I, g.diff_cur, g.diff_nxt, g.rho_cur, g.rho_nxt))
+        return fail(ctx, AMCFD_E_CUDA, "tensor-map encoding for the energy assembly failed");
     g.npart = I.asm_grid.y * I.asm_grid.z;
     if ((rc = alloc3<double>(ctx, &g.bc, (size_t)g.npart * 4 * p.nip))) return rc;
     if ((rc = alloc3<double>(ctx, &g.delphi, (size_t)p.nip))) return rc;
@@ -697,6 +729,7 @@ void amcfd_destroy(amcfd_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    if (ctx->pack) cudaFree(ctx->pack);
     for (auto &row : ctx->gexec)
         for (auto &ge : row)
             if (ge) cudaGraphExecDestroy(ge);
@@ -827,17 +860,23 @@ int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
     void *d;
     int rc;
     if ((rc = field_ptr(ctx, name, &d))) return rc;
-    CK(cudaStreamSynchronize(ctx->stream));
-    const size_t rows = (size_t)ctx->nj * ctx->nk;
-    if (ctx->precision == AMCFD_PREC_FP64) {
-        CK(cudaMemcpy2D(host_out, ctx->ni * sizeof(double), d, ctx->nip * sizeof(double),
-                        ctx->ni * sizeof(double), rows, cudaMemcpyDeviceToHost));
-    } else {
-        std::vector<float> tmp((size_t)ctx->ni * rows);
-        CK(cudaMemcpy2D(tmp.data(), ctx->ni * sizeof(float), d, ctx->nip * sizeof(float),
-                        ctx->ni * sizeof(float), rows, cudaMemcpyDeviceToHost));
-        for (size_t q = 0; q < tmp.size(); q++) host_out[q] = tmp[q];
+    CK(cudaSetDevice(ctx->device));
+    const long long rows = (long long)ctx->nj * ctx->nk;
+    const size_t bytes = (size_t)rows * ctx->ni * sizeof(double);
+    if (!ctx->pack) {
+        CK(cudaMalloc(&ctx->pack, bytes));
+        CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device));
     }
+    // widen and pack on the device, then one contiguous copy (full speed into pinned memory)
+    if (ctx->precision == AMCFD_PREC_FP64)
+        launch_pack_field<double>((const double *)d, ctx->pack, ctx->ni, ctx->nip, rows, ctx->sm_count,
+                                  ctx->stream);
+    else
+        launch_pack_field<float>((const float *)d, ctx->pack, ctx->ni, ctx->nip, rows, ctx->sm_count,
+                                 ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host_out, ctx->pack, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return 0;
 }
 

@@ -4,33 +4,59 @@
 // bareplateMaterialProps (:2137-2189, written to the *_nxt buffers so that the
 // old properties stay readable by neighbouring cells).
 //
-// 2.5-D stencil: a CTA owns a 32 (i) x 8 (j) tile and walks a segment of k
-// planes.  Each thread keeps its column's k-1 / k / k+1 values in registers and
-// loads plane k+2 one plane ahead; i+-1 and j+-1 neighbours come from a
-// shared-memory copy of the current plane with a one-cell halo.  Face areas and
-// volumes are products of per-column (x, y) and per-plane (z) widths, formed in
-// FP64 in the reference's order.  The arithmetic is the reference's expression
-// by expression; the FP32 build evaluates properties and divisions in FP32.
+// 2.5-D stencil fed by TMA.  A CTA owns a 32 (i) x 8 (j) tile and walks a
+// segment of k planes.  The ten input fields arrive in shared memory as 3-D
+// tensor tiles (the tile plus a one-cell j halo and an i halo widened to 16
+// bytes on each side, so every box starts on a 16-byte boundary) through two
+// rings completing on mbarriers:
+//   ring A (diff, h, f_l, rho, w): planes k-1, k, k+1 resident, k+2 in flight;
+//   ring B (u, v, T, hnot, f_l,not): plane k resident, k+1 in flight.
+// One thread issues the copies one plane ahead, so the loads of plane k+1
+// overlap the arithmetic of plane k and no thread waits on a global load.
+// Face areas and volumes are products of per-column (x, y) and per-plane (z)
+// widths, formed in FP64 in the reference's order.  The arithmetic is the
+// reference's expression by expression; the FP32 build evaluates properties
+// and divisions in FP32.
 #include "kernels.cuh"
+#include "async.cuh"
 
 namespace amcfd {
 
 constexpr int kTX = 32, kTY = 8, kKSEG = 16;
-// resident CTAs per SM the register budget is sized for (three FP32 CTAs spill and
-// measured slower than two)
-template <typename T> constexpr int asm_min_blocks() { return 2; }
+
+// Box geometry of the staged tiles, per element type.
+template <typename T> struct AsmBox {
+    static constexpr int OX = 16 / (int)sizeof(T);  // i halo: one 16-byte unit
+    static constexpr int BX = kTX + 2 * OX;         // box width (elements)
+    static constexpr int BY = kTY + 2;              // box height (rows)
+    static constexpr int BYTES = BX * BY * (int)sizeof(T);
+    static constexpr int FE = ((BYTES + 127) / 128 * 128) / (int)sizeof(T);  // 128-B aligned stride
+    static constexpr int NA = 5, NB = 5, SA = 4, SB = 2;  // fields and ring slots
+    // rings + mbarriers + slack to align the dynamic region to 128 bytes
+    static constexpr size_t SMEM = (size_t)(SA * NA + SB * NB) * FE * sizeof(T) + 8 * (SA + SB) + 128;
+};
+enum { FA_D = 0, FA_H, FA_F, FA_R, FA_W };
+enum { FB_U = 0, FB_V, FB_T, FB_HN, FB_FN };
 
 template <typename T>
-__global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kernel(Params p, Fields<T> g, double *red)
+__global__ void __launch_bounds__(256, 2)
+energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp)
 {
     using R = T;
-    __shared__ R s_d[kTY + 2][kTX + 2], s_h[kTY + 2][kTX + 2], s_f[kTY + 2][kTX + 2],
-        s_r[kTY + 2][kTX + 2];
-    __shared__ R s_u[kTY][kTX + 1], s_v[kTY + 1][kTX];
+    using B = AsmBox<T>;
+    constexpr int OX = B::OX, BX = B::BX, FE = B::FE;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    unsigned char *base = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
+    T *bufA = reinterpret_cast<T *>(base);
+    T *bufB = bufA + B::SA * B::NA * FE;
+    uint64_t *barA = reinterpret_cast<uint64_t *>(bufB + B::SB * B::NB * FE);
+    uint64_t *barB = barA + B::SA;
     __shared__ double sb[4][kTY][kTX + 1];
-    const Status *st = g.st;
-    const int tx = threadIdx.x, ty = threadIdx.y;
+
+    Status *st = g.st;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
     const int i = blockIdx.x * kTX + tx, j = blockIdx.y * kTY + ty;
+    const int x0 = blockIdx.x * kTX - OX, y0 = blockIdx.y * kTY - 1;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
     const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
               nkm2 = p.nkm2;
@@ -38,12 +64,63 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
     const int kb = blockIdx.z * kseg, ke = min(kb + kseg, nk);
     const bool in = (i < ni && j < nj);
     const bool colint = in && i >= 1 && i <= nim2 && j >= 1 && j <= njm2;
-    const size_t sj = nip, sk = (size_t)nj * nip;
+    const size_t sk = (size_t)nj * nip;
     const size_t col = in ? cidx(i, j, 0, nj, nip) : 0;
     const int sch = p.scheme;
     const double delt = st->delt;
     const bool volsrc = p.volsrc != 0;
-    auto ld = [&](const R *a, int k) -> R { return (in && k >= 0 && k < nk) ? a[col + (size_t)k * sk] : R(0); };
+
+    // ---- copy pipeline (thread 0 issues; all threads wait) ----
+    auto issueA = [&](int q) {
+        const int s = q & 3;
+        T *dst = bufA + s * B::NA * FE;
+        fence_proxy_async();
+        mbar_expect_tx(&barA[s], B::NA * B::BYTES);
+        tma_load_3d(dst + FA_D * FE, &mp.diff, x0, y0, q, &barA[s]);
+        tma_load_3d(dst + FA_H * FE, &mp.h, x0, y0, q, &barA[s]);
+        tma_load_3d(dst + FA_F * FE, &mp.fracl, x0, y0, q, &barA[s]);
+        tma_load_3d(dst + FA_R * FE, &mp.rho, x0, y0, q, &barA[s]);
+        tma_load_3d(dst + FA_W * FE, &mp.w, x0, y0, q, &barA[s]);
+    };
+    auto issueB = [&](int q) {
+        const int s = q & 1;
+        T *dst = bufB + s * B::NB * FE;
+        fence_proxy_async();
+        mbar_expect_tx(&barB[s], B::NB * B::BYTES);
+        tma_load_3d(dst + FB_U * FE, &mp.u, x0, y0, q, &barB[s]);
+        tma_load_3d(dst + FB_V * FE, &mp.v, x0, y0, q, &barB[s]);
+        tma_load_3d(dst + FB_T * FE, &mp.temp, x0, y0, q, &barB[s]);
+        tma_load_3d(dst + FB_HN * FE, &mp.hnot, x0, y0, q, &barB[s]);
+        tma_load_3d(dst + FB_FN * FE, &mp.flnot, x0, y0, q, &barB[s]);
+    };
+    // The n-th completion of a slot's barrier has parity n & 1; ring A receives
+    // planes kb-1, kb, ... in order over four slots, ring B planes kb, ... over two.
+    auto parA = [&](int q) { return (uint32_t)(((q - (kb - 1)) >> 2) & 1); };
+    auto parB = [&](int q) { return (uint32_t)(((q - kb) >> 1) & 1); };
+    // planes issued but not yet waited for: A [pa0, pa1], B [pb0, pb1]; thread 0
+    // drains them before an early exit so that no copy lands in a finished CTA
+    int pa0 = kb - 1, pa1 = kb - 2, pb0 = kb, pb1 = kb - 1;
+
+    if (tid == 0) {
+        for (int s = 0; s < B::SA; ++s) mbar_init(&barA[s]);
+        for (int s = 0; s < B::SB; ++s) mbar_init(&barB[s]);
+    }
+    __syncthreads();
+    if (kb >= ke) return;
+    if (tid == 0) {
+        issueA(kb - 1);
+        issueA(kb);
+        issueA(kb + 1);
+        issueB(kb);
+    }
+    pa1 = kb + 1;
+    pb1 = kb;
+    bool ok = mbar_wait(&barA[(kb - 1) & 3], parA(kb - 1), st, 1);
+    if (ok) {
+        pa0 = kb;
+        ok = mbar_wait(&barA[kb & 3], parA(kb), st, 1);
+        if (ok) pa0 = kb + 1;
+    }
 
     // per-column metrics (interior columns only)
     double dx = 0.0, dy = 0.0;
@@ -64,58 +141,30 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
             thsb = (R)p.thconsb, thsc = (R)p.thconsc, acpa = (R)p.acpa, acpb = (R)p.acpb,
             tliq = (R)p.tliquid, tsol = (R)p.tsolid, denl = (R)p.denl, dens = (R)p.dens,
             visc = (R)p.viscos;
-
-    R d_m = ld(g.diff_cur, kb - 1), d_c = ld(g.diff_cur, kb), d_p = ld(g.diff_cur, kb + 1);
-    R h_m = ld(g.h, kb - 1), h_c = ld(g.h, kb), h_p = ld(g.h, kb + 1);
-    R f_m = ld(g.fracl, kb - 1), f_c = ld(g.fracl, kb), f_p = ld(g.fracl, kb + 1);
-    R r_c = ld(g.rho_cur, kb), r_p = ld(g.rho_cur, kb + 1);
-    R w_c = ld(g.wvel, kb), w_p = ld(g.wvel, kb + 1);
     double sumd = 0.0, sumh = 0.0;
     double bl = 0.0, blp = 0.0, blm = 0.0, blc = 0.0;
+    const int o = (ty + 1) * BX + tx + OX;  // this thread's cell inside a box
 
     for (int k = kb; k < ke; ++k) {
-        // one plane ahead for the rolling registers
-        const R d_n = ld(g.diff_cur, k + 2), h_n = ld(g.h, k + 2), f_n = ld(g.fracl, k + 2),
-                r_n = ld(g.rho_cur, k + 2), w_n = ld(g.wvel, k + 2);
-        const size_t c = col + (size_t)k * sk;
-        const R t_c = in ? g.temp[c] : R(0);
-        const R hnot_c = in ? g.hnot[c] : R(0);
-        const R flnot_c = in ? g.fraclnot[c] : R(0);
-        // ---- stage plane k with a one-cell halo ----
-        s_d[ty + 1][tx + 1] = d_c;
-        s_h[ty + 1][tx + 1] = h_c;
-        s_f[ty + 1][tx + 1] = f_c;
-        s_r[ty + 1][tx + 1] = r_c;
-        s_u[ty][tx] = in ? g.uvel[c] : R(0);
-        s_v[ty][tx] = in ? g.vvel[c] : R(0);
-        if (in) {
-            if (tx == 0 && i >= 1) {
-                s_d[ty + 1][0] = g.diff_cur[c - 1];
-                s_h[ty + 1][0] = g.h[c - 1];
-                s_f[ty + 1][0] = g.fracl[c - 1];
-            }
-            if (tx == kTX - 1 && i + 1 < ni) {
-                s_d[ty + 1][kTX + 1] = g.diff_cur[c + 1];
-                s_h[ty + 1][kTX + 1] = g.h[c + 1];
-                s_f[ty + 1][kTX + 1] = g.fracl[c + 1];
-                s_r[ty + 1][kTX + 1] = g.rho_cur[c + 1];
-                s_u[ty][kTX] = g.uvel[c + 1];
-            }
-            if (ty == 0 && j >= 1) {
-                s_d[0][tx + 1] = g.diff_cur[c - sj];
-                s_h[0][tx + 1] = g.h[c - sj];
-                s_f[0][tx + 1] = g.fracl[c - sj];
-            }
-            if (ty == kTY - 1 && j + 1 < nj) {
-                s_d[kTY + 1][tx + 1] = g.diff_cur[c + sj];
-                s_h[kTY + 1][tx + 1] = g.h[c + sj];
-                s_f[kTY + 1][tx + 1] = g.fracl[c + sj];
-                s_r[kTY + 1][tx + 1] = g.rho_cur[c + sj];
-                s_v[kTY][tx] = g.vvel[c + sj];
-            }
+        if (tid == 0 && ok) {
+            if (k + 2 <= ke) { issueA(k + 2); pa1 = k + 2; }
+            if (k + 1 < ke) { issueB(k + 1); pb1 = k + 1; }
         }
-        __syncthreads();
-        if (in) {
+        if (ok) {
+            ok = mbar_wait(&barA[(k + 1) & 3], parA(k + 1), st, 2);
+            if (ok) pa0 = k + 2;
+        }
+        if (ok) {
+            ok = mbar_wait(&barB[k & 1], parB(k), st, 3);
+            if (ok) pb0 = k + 1;
+        }
+        const T *Am = bufA + ((k - 1) & 3) * B::NA * FE + o;  // plane k-1
+        const T *Ac = bufA + (k & 3) * B::NA * FE + o;        // plane k
+        const T *Ap = bufA + ((k + 1) & 3) * B::NA * FE + o;  // plane k+1
+        const T *Bc = bufB + (k & 1) * B::NB * FE + o;        // plane k
+        const size_t c = col + (size_t)k * sk;
+        if (in && ok) {
+            const R d_c = Ac[FA_D * FE], f_c = Ac[FA_F * FE], t_c = Bc[FB_T * FE];
             // ---- material properties (every node) ----
             {
                 const R t = t_c, fl = f_c;
@@ -140,15 +189,16 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 const R vol = (R)(dx * dy * dz);
                 const R fz_k = (R)g.fracz[k], fz_m = (R)g.fracz[k - 1];
                 const R dzp_k = (R)g.dzpbinv[k], dzp_p = (R)g.dzpbinv[k + 1];
-                const R dcc = d_c, rhc = r_c;
-                const R d_e = s_d[ty + 1][tx + 2], d_w = s_d[ty + 1][tx], d_nn = s_d[ty + 2][tx + 1],
-                        d_s = s_d[ty][tx + 1];
+                const R dcc = d_c, rhc = Ac[FA_R * FE];
+                const R d_e = Ac[FA_D * FE + 1], d_w = Ac[FA_D * FE - 1], d_nn = Ac[FA_D * FE + BX],
+                        d_s = Ac[FA_D * FE - BX], d_m = Am[FA_D * FE], d_p = Ap[FA_D * FE];
                 R an, as_, ae, aw, at, ab, tmp;
-                const R u_c = s_u[ty][tx], u_e = s_u[ty][tx + 1];
-                const R v_c = s_v[ty][tx], v_n = s_v[ty + 1][tx];
+                const R u_c = Bc[FB_U * FE], u_e = Bc[FB_U * FE + 1];
+                const R v_c = Bc[FB_V * FE], v_n = Bc[FB_V * FE + BX];
+                const R w_c = Ac[FA_W * FE], w_p = Ap[FA_W * FE];
                 // north face
                 {
-                    R fn = s_r[ty + 2][tx + 1] * v_n * aik;
+                    R fn = Ac[FA_R * FE + BX] * v_n * aik;
                     R dn;
                     if (j == njm2) {
                         dn = dcc * aik * dyp_n;
@@ -172,7 +222,7 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 }
                 // east face
                 {
-                    R fe = s_r[ty + 1][tx + 2] * u_e * ajk;
+                    R fe = Ac[FA_R * FE + 1] * u_e * ajk;
                     R de;
                     if (i == nim2) {
                         de = dcc * ajk * dxp_e;
@@ -196,7 +246,7 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 }
                 // top face
                 {
-                    R ft = r_p * w_p * aij;
+                    R ft = Ap[FA_R * FE] * w_p * aij;
                     R dt;
                     if (k == nkm2) {
                         dt = dcc * aij * dzp_t;
@@ -221,7 +271,7 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 const R densbydt = bdiv(rhc, (R)delt);
                 const R apnot = densbydt * vol;
                 R sp = R(0);
-                R su = apnot * hnot_c;
+                R su = apnot * Bc[FB_HN * FE];
                 // ---- calculateSource(5) ----
                 if (volsrc) {
                     R srcin = R(0);
@@ -239,10 +289,11 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 const R variable1 = bdiv(hlatnt * rhc, (R)delt);
                 const R volht = vol * variable1;
                 const R flc = f_c;
-                su -= volht * (flc - flnot_c);
+                su -= volht * (flc - Bc[FB_FN * FE]);
                 {
-                    const R fl_w = s_f[ty + 1][tx], fl_e = s_f[ty + 1][tx + 2], fl_s = s_f[ty][tx + 1],
-                            fl_n = s_f[ty + 2][tx + 1];
+                    const R fl_w = Ac[FA_F * FE - 1], fl_e = Ac[FA_F * FE + 1],
+                            fl_s = Ac[FA_F * FE - BX], fl_n = Ac[FA_F * FE + BX];
+                    const R f_m = Am[FA_F * FE], f_p = Ap[FA_F * FE];
                     R flew = ajk * (maxd(u_c, R(0)) * fl_w - maxd(-u_c, R(0)) * flc +
                                     maxd(-u_e, R(0)) * fl_e - maxd(u_e, R(0)) * flc);
                     R flns = aik * (maxd(v_c, R(0)) * fl_s - maxd(-v_c, R(0)) * flc +
@@ -251,9 +302,9 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                                     maxd(-w_p, R(0)) * f_p - maxd(w_p, R(0)) * flc);
                     su += rhc * hlatnt * (flew + flns + fltb);
                 }
-                const R hc = h_c;
-                const R hjp = s_h[ty + 2][tx + 1], hjm = s_h[ty][tx + 1], hip = s_h[ty + 1][tx + 2],
-                        him = s_h[ty + 1][tx], hkp = h_p, hkm = h_m;
+                const R hc = Ac[FA_H * FE];
+                const R hjp = Ac[FA_H * FE + BX], hjm = Ac[FA_H * FE - BX], hip = Ac[FA_H * FE + 1],
+                        him = Ac[FA_H * FE - 1], hkp = Ap[FA_H * FE], hkm = Am[FA_H * FE];
                 // boundary folds, in the reference's order: k, j, i
                 if (k == 1) { su += ab * hkm; sp -= ab; ab = R(0); }
                 if (k == nkm2) { su += at * hkp; sp -= at; at = R(0); }
@@ -278,12 +329,16 @@ __global__ void __launch_bounds__(256, asm_min_blocks<T>()) energy_assemble_kern
                 blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
             }
         }
-        __syncthreads();
-        d_m = d_c; d_c = d_p; d_p = d_n;
-        h_m = h_c; h_c = h_p; h_p = h_n;
-        f_m = f_c; f_c = f_p; f_p = f_n;
-        r_c = r_p; r_p = r_n;
-        w_c = w_p; w_p = w_n;
+        // every thread is done with plane k-1 (ring A) and plane k (ring B)
+        // before thread 0 refills those slots
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                // drain what is still in flight (bounded), then leave
+                for (int q = pa0; q <= pa1; ++q) mbar_try(&barA[q & 3], parA(q), kSpinLimit);
+                for (int q = pb0; q <= pb1; ++q) mbar_try(&barB[q & 1], parB(q), kSpinLimit);
+            }
+            return;
+        }
     }
     // per-i partial sums over this block's j-rows and planes
     sb[0][ty][tx] = bl;
@@ -315,12 +370,47 @@ dim3 energy_assemble_grid(const Params &p)
     return dim3((p.ni + kTX - 1) / kTX, (p.nj + kTY - 1) / kTY, (p.nk + seg - 1) / seg);
 }
 
+// Tensor maps of the ten staged fields; set [q] reads diff/rho from the
+// buffers that are current at property parity q (parity 0: diff_a, rho_a).
+template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T *rho_a, T *rho_b)
+{
+    using B = AsmBox<T>;
+    const Params &p = I.p;
+    const int e = (int)sizeof(T);
+    auto enc = [&](CUtensorMap *m, const T *base) {
+        return encode_field_map(m, base, e, p.nip, p.nj, p.nk, B::BX, B::BY);
+    };
+    for (int q = 0; q < 2; ++q) {
+        AsmMaps &m = I.asm_maps[q];
+        int rc = 0;
+        if (!rc) rc = enc(&m.diff, q == 0 ? diff_a : diff_b);
+        if (!rc) rc = enc(&m.rho, q == 0 ? rho_a : rho_b);
+        if (!rc) rc = enc(&m.h, I.g.h);
+        if (!rc) rc = enc(&m.fracl, I.g.fracl);
+        if (!rc) rc = enc(&m.w, I.g.wvel);
+        if (!rc) rc = enc(&m.u, I.g.uvel);
+        if (!rc) rc = enc(&m.v, I.g.vvel);
+        if (!rc) rc = enc(&m.temp, I.g.temp);
+        if (!rc) rc = enc(&m.hnot, I.g.hnot);
+        if (!rc) rc = enc(&m.flnot, I.g.fraclnot);
+        if (rc) return rc;
+    }
+    I.asm_diff_a = diff_a;
+    cudaFuncSetAttribute(energy_assemble_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)B::SMEM);
+    return 0;
+}
+
 template <typename T> void launch_energy_assemble(Inst<T> &I)
 {
-    energy_assemble_kernel<T><<<I.asm_grid, dim3(kTX, kTY), 0, I.stream>>>(I.p, I.g, I.red_asm);
+    const AsmMaps &m = I.g.diff_cur == I.asm_diff_a ? I.asm_maps[0] : I.asm_maps[1];
+    energy_assemble_kernel<T><<<I.asm_grid, dim3(kTX, kTY), AsmBox<T>::SMEM, I.stream>>>(
+        I.p, I.g, I.red_asm, m);
 }
 
 template void launch_energy_assemble<double>(Inst<double> &);
 template void launch_energy_assemble<float>(Inst<float> &);
+template int make_assemble_maps<double>(Inst<double> &, double *, double *, double *, double *);
+template int make_assemble_maps<float>(Inst<float> &, float *, float *, float *, float *);
 
 }  // namespace amcfd

@@ -610,6 +610,26 @@ template <typename T> void launch_block_correct(Inst<T> &I)
     block_correct_kernel<T><<<1, 1024, 4 * I.p.nip * sizeof(double), I.stream>>>(
         I.p, I.g, I.red_asm, I.nb_asm, I.check_finite);
 }
+// Field read-out: the padded [k][j][nip] array widened to FP64 and packed to
+// the reference's unpadded [k][j][ni] layout (CFDSolverManager.cpp:249), so
+// that a single contiguous copy moves it to the host.
+template <typename T>
+__global__ void pack_field_kernel(const T *src, double *dst, int ni, int nip, long long rows)
+{
+    const long long n = rows * ni;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const long long r = q / ni;
+        const int i = (int)(q - r * ni);
+        dst[q] = (double)src[r * nip + i];
+    }
+}
+template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
+                                             long long rows, int sm_count, cudaStream_t s)
+{
+    pack_field_kernel<T><<<sm_count * 4, 256, 0, s>>>(src, dst, ni, nip, rows);
+}
+
 // Resident 256-thread CTAs of h2t_kernel per SM (its grid is one full wave).
 template <typename T> int h2t_blocks_per_sm()
 {
@@ -643,6 +663,7 @@ template <typename T> void launch_update_solutions(Inst<T> &I)
     template void launch_block_correct<T>(Inst<T> &);       \
     template void launch_h2t<T>(Inst<T> &);                 \
     template int h2t_blocks_per_sm<T>();                    \
+    template void launch_pack_field<T>(const T *, double *, int, int, long long, int, cudaStream_t); \
     template void launch_meltpool<T>(Inst<T> &);            \
     template void launch_converge<T>(Inst<T> &, double);    \
     template void launch_update_solutions<T>(Inst<T> &);

@@ -22,6 +22,7 @@
 // colour at once.
 #include "kernels.cuh"
 #include "amcfd.h"
+#include "async.cuh"
 
 namespace amcfd {
 
@@ -109,52 +110,18 @@ template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) {
 // ---------------------------------------------------------------------------
 enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// Bounded wait for the phase `parity` of a per-warp mbarrier (all lanes poll).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, Status *st)
-{
-    const uint32_t a = smem_u32(bar);
-    for (long long it = 0; it < kSpinLimit; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-            " selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done) : "r"(a), "r"(parity) : "memory");
-        if (done) return true;
-    }
-    if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -1;
-    return false;
-}
-
 template <typename T>
 __device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int ib, int ie, T *sl,
                                            int nmax, uint64_t *bar)
 {
     // lane 0 only.  Previous generic-proxy use of this shared buffer is ordered
     // before the asynchronous copies by the proxy fence.
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_proxy_async();
     const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
-    const uint32_t b = smem_u32(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b),
-                 "r"(bytes * S_N) : "memory");
+    mbar_expect_tx(bar, bytes * S_N);
     const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.cf, g.pr, g.iden};
 #pragma unroll
-    for (int q = 0; q < S_N; ++q) {
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-            ::"r"(smem_u32(sl + (size_t)q * nmax)), "l"(src[q] + row + ib), "r"(bytes), "r"(b)
-            : "memory");
-    }
+    for (int q = 0; q < S_N; ++q) bulk_load(sl + (size_t)q * nmax, src[q] + row + ib, bytes, bar);
 }
 
 // ---------------------------------------------------------------------------
@@ -162,6 +129,72 @@ __device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int i
 // node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
 // ends; sl holds the line from cell ib on.
 // ---------------------------------------------------------------------------
+// Thomas recurrences of one line by one warp, from shared-memory rows indexed
+// by i - i0: e (right-hand side / den on entry, the solution on exit), cf and
+// pr.  Each lane owns a contiguous chunk; the chunks are chained by warp scans
+// of affine maps (x -> A x + B), forward for qr_i = cf_i qr_{i-1} + e_i and
+// backward for phi_i = pr_i phi_{i+1} + qr_i; then the line is stored.
+template <typename T, bool COHERENT>
+__device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T *se, const T *sc,
+                                          const T *sp)
+{
+    const int lane = threadIdx.x & 31;
+    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
+    const int n = i1 - i0 + 1;
+    const int L = (n + 31) >> 5;
+    const int a = lane * L;
+    const int b = min(a + L, n);
+    T A = T(1), B = T(0);
+    for (int i = a; i < b; ++i) {
+        const T cfi = sc[i];
+        B = cfi * B + se[i];
+        A = cfi * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_up_sync(0xffffffffu, A, o);
+        T B2 = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    T Ae = __shfl_up_sync(0xffffffffu, A, 1);
+    T Be = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) { Ae = T(1); Be = T(0); }
+    T q = Ae * ldp(row + i0 - 1) + Be;
+    for (int i = a; i < b; ++i) {
+        q = sc[i] * q + se[i];
+        se[i] = q;
+    }
+    A = T(1);
+    B = T(0);
+    for (int i = b - 1; i >= a; --i) {
+        const T pri = sp[i];
+        B = pri * B + se[i];
+        A = pri * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_down_sync(0xffffffffu, A, o);
+        T B2 = __shfl_down_sync(0xffffffffu, B, o);
+        if (lane + o < 32) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    Ae = __shfl_down_sync(0xffffffffu, A, 1);
+    Be = __shfl_down_sync(0xffffffffu, B, 1);
+    if (lane == 31) { Ae = T(1); Be = T(0); }
+    T x = Ae * ldp(row + i1 + 1) + Be;
+    for (int i = b - 1; i >= a; --i) {
+        x = sp[i] * x + se[i];
+        se[i] = x;
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) phi[row + i0 + i] = se[i];
+}
+
 template <typename T, bool COHERENT>
 __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
                                              size_t sj, size_t sk, T *sl, int nmax)
@@ -196,61 +229,8 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
         }
     }
     __syncwarp();
-    const int n = i1 - i0 + 1;
-    const int L = (n + 31) >> 5;
-    const int a = i0 + lane * L;
-    const int b = min(a + L, i1 + 1);
-    // forward: qr_i = cf_i qr_{i-1} + e_i
-    T A = T(1), B = T(0);
-    for (int i = a; i < b; ++i) {
-        const T cfi = sc[i - ib];
-        B = cfi * B + se[i - ib];
-        A = cfi * A;
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T A2 = __shfl_up_sync(0xffffffffu, A, o);
-        T B2 = __shfl_up_sync(0xffffffffu, B, o);
-        if (lane >= o) {
-            B = A * B2 + B;
-            A = A * A2;
-        }
-    }
-    T Ae = __shfl_up_sync(0xffffffffu, A, 1);
-    T Be = __shfl_up_sync(0xffffffffu, B, 1);
-    if (lane == 0) { Ae = T(1); Be = T(0); }
-    T q = Ae * ldp(row + i0 - 1) + Be;
-    for (int i = a; i < b; ++i) {
-        q = sc[i - ib] * q + se[i - ib];
-        se[i - ib] = q;
-    }
-    // backward: phi_i = pr_i phi_{i+1} + qr_i
-    A = T(1);
-    B = T(0);
-    for (int i = b - 1; i >= a; --i) {
-        const T pri = sp[i - ib];
-        B = pri * B + se[i - ib];
-        A = pri * A;
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T A2 = __shfl_down_sync(0xffffffffu, A, o);
-        T B2 = __shfl_down_sync(0xffffffffu, B, o);
-        if (lane + o < 32) {
-            B = A * B2 + B;
-            A = A * A2;
-        }
-    }
-    Ae = __shfl_down_sync(0xffffffffu, A, 1);
-    Be = __shfl_down_sync(0xffffffffu, B, 1);
-    if (lane == 31) { Ae = T(1); Be = T(0); }
-    T x = Ae * ldp(row + i1 + 1) + Be;
-    for (int i = b - 1; i >= a; --i) {
-        x = sp[i - ib] * x + se[i - ib];
-        se[i - ib] = x;
-    }
-    __syncwarp();
-    for (int i = i0 + lane; i <= i1; i += 32) phi[row + i] = se[i - ib];
+    const int o = i0 - ib;
+    scan_line<T, COHERENT>(phi, row, i0, i1, se + o, sc + o, sp + o);
 }
 
 // Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).

@@ -1,5 +1,6 @@
 // Geometry helpers, the host-side instance record and the kernel launchers.
 #pragma once
+#include <cuda.h>
 #include <cstdio>
 #include "dev.cuh"
 
@@ -60,6 +61,11 @@ template <typename T>
 __device__ __forceinline__ double volume_w(const Fields<T> &g, int i, int j, int k)
 { return (g.xu[i + 1] - g.xu[i]) * (g.yv[j + 1] - g.yv[j]) * (g.z[k] - g.z[k - 1]); }
 
+// TMA tensor maps of the fields the energy assembly stages (k_assemble.cu).
+struct AsmMaps {
+    CUtensorMap diff, h, fracl, rho, w, u, v, temp, hnot, flnot;
+};
+
 // Host-side record of one instance on the device.
 template <typename T>
 struct Inst {
@@ -80,12 +86,15 @@ struct Inst {
     size_t line_smem = 0;     // dynamic smem of a line-sweep CTA
     int *flags_mom = nullptr;
     int max_lines = 0;        // (nj-2)*(nk-2)
+    AsmMaps asm_maps[2];      // by property parity
+    const T *asm_diff_a = nullptr;  // diff_cur at parity 0
 };
 
 // launchers (k_energy.cu)
 template <typename T> void launch_laser(Inst<T> &I);
 template <typename T> void launch_energy_bc(Inst<T> &I);
 template <typename T> void launch_energy_assemble(Inst<T> &I);
+template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T *rho_a, T *rho_b);
 template <typename T> void launch_block_correct(Inst<T> &I);
 template <typename T> void launch_h2t(Inst<T> &I);
 template <typename T> void launch_meltpool(Inst<T> &I);
