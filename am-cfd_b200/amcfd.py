@@ -69,7 +69,7 @@ class AmcfdReport(C.Structure):
 
 class AmcfdOptions(C.Structure):
     _fields_ = [("device", _I), ("order", _I), ("precision", _I), ("use_graphs", _I),
-                ("check_finite", _I), ("reserved", _I * 8)]
+                ("check_finite", _I), ("no_small_box", _I), ("reserved", _I * 7)]
 
 
 class AmcfdError(RuntimeError):
@@ -179,11 +179,13 @@ class Solver:
     """One melt-pool instance on one GPU (amcfd_create ... amcfd_destroy)."""
 
     def __init__(self, deck: Deck, order: int = ORDER_EXACT, precision: int = PREC_FP64,
-                 device: int = 0, use_graphs: int = 0, check_finite: int = 1):
+                 device: int = 0, use_graphs: int = 0, check_finite: int = 1,
+                 small_box: int = 1):
         L = lib()
         self.deck = deck  # keeps toolpath storage alive
         opts = AmcfdOptions(device=device, order=order, precision=precision,
-                            use_graphs=use_graphs, check_finite=check_finite)
+                            use_graphs=use_graphs, check_finite=check_finite,
+                            no_small_box=0 if small_box else 1)
         self._h = C.c_void_p()
         rc = L.amcfd_create(C.byref(deck.params), C.byref(opts), C.byref(self._h))
         if rc != 0:

@@ -85,7 +85,9 @@ struct amcfd_ctx {
     // CUDA graphs of one outer iteration, by [timing events recorded][property parity]:
     // the iteration swaps the current/next property buffers, so two graphs alternate.
     bool use_graphs = false;
-    cudaGraphExec_t gexec[2][2] = {};
+    cudaGraphExec_t gexec[2][2][2] = {};  // [events][parity][small-box momentum]
+    int last_box = -1;             // momentum box cells seen by the last outer iteration
+    bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
     double *pack = nullptr;        // FP64 read-out staging (ni*nj*nk), made on first use
     int sm_count = 0;
@@ -359,6 +361,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         g.ntickets_energy = (int)tk.size();
         if ((rc = alloc3<int2>(ctx, &g.tickets_mom, tk.size()))) return rc;
         if ((rc = alloc3<int>(ctx, &g.ntickets_mom, 1))) return rc;
+        if ((rc = alloc3<T>(ctx, &I.mom_scratch, n3))) return rc;
+        setup_mom_small<T>(I);
     }
     g.st = ctx->st_dev;
     I.check_finite = 0;
@@ -415,6 +419,16 @@ static void swap_props(Inst<T> &I)
     std::swap(I.g.vis_cur, I.g.vis_nxt);
 }
 
+// The one-CTA momentum chain serves red-black runs whose melt-pool box, as of
+// the last outer iteration, fits its shared memory (it stays correct, only
+// slower, if the box has grown past that since).
+template <typename T>
+static bool mom_small(const amcfd_ctx *ctx, const Inst<T> &I)
+{
+    return ctx->small_box && ctx->order == AMCFD_ORDER_REDBLACK && ctx->last_box >= 0 &&
+           ctx->last_box <= mom_small_capacity<T>(I);
+}
+
 template <typename T>
 static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
 {
@@ -430,7 +444,7 @@ static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
         break;
     case AMCFD_PHASE_H2T: launch_h2t<T>(I); break;
     case AMCFD_PHASE_MELTPOOL: launch_meltpool<T>(I); break;
-    case AMCFD_PHASE_MOMENTUM: launch_momentum<T>(I); break;
+    case AMCFD_PHASE_MOMENTUM: launch_momentum<T>(I, mom_small<T>(ctx, I)); break;
     case AMCFD_PHASE_CONVERGE:
         launch_converge<T>(I, ctx->prm.nonlintol);
         swap_props<T>(I);
@@ -499,7 +513,7 @@ static int read_status(amcfd_ctx *ctx)
 }
 
 // Kernel launches issued by one phase (the launch counter of the bench).
-static long long phase_launches(const amcfd_ctx *ctx, int phase)
+static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
 {
     const long long sweeps = ctx->order == AMCFD_ORDER_EXACT ? 1 : 8;
     switch (phase) {
@@ -508,7 +522,7 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase)
     case AMCFD_PHASE_ENERGY_SOLVE: return 1 + sweeps;
     case AMCFD_PHASE_H2T: return 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
-    case AMCFD_PHASE_MOMENTUM: return 2 + 4 * (3 + sweeps) + 2 + 1;
+    case AMCFD_PHASE_MOMENTUM: return small ? 9 : 2 + 4 * (3 + sweeps) + 2 + 1;
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return 1;
     default: return 0;
@@ -559,7 +573,7 @@ template <typename T>
 static int launch_iteration_graph(amcfd_ctx *ctx, Inst<T> &I)
 {
     const int par = (const void *)I.g.diff_cur == ctx->diff_a ? 0 : 1;
-    cudaGraphExec_t &ge = ctx->gexec[ctx->events ? 1 : 0][par];
+    cudaGraphExec_t &ge = ctx->gexec[ctx->events ? 1 : 0][par][mom_small<T>(ctx, I) ? 1 : 0];
     if (!ge) {
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -597,14 +611,16 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
         ctx->niter++;
         ctx->itertot++;
         const bool ev = ctx->events;
+        const bool small = mom_small<T>(ctx, I);
         if (ctx->use_graphs) {
             if ((rc = launch_iteration_graph<T>(ctx, I))) return rc;
         } else {
             launch_iteration<T>(ctx, I, false);
         }
         for (int ph = AMCFD_PHASE_ENERGY_ASSEMBLE; ph <= AMCFD_PHASE_CONVERGE; ++ph)
-            ctx->launches += phase_launches(ctx, ph);
+            ctx->launches += phase_launches(ctx, ph, small);
         if ((rc = read_status(ctx))) return rc;
+        ctx->last_box = ctx->st_host->momentum_active ? ctx->st_host->box_cells : 0;
         if (ev) {
             for (int q = 0; q < 6; q++) {
                 float ms = 0.f;
@@ -661,6 +677,7 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->order = opts->order;
         ctx->precision = opts->precision;
         ctx->use_graphs = opts->use_graphs != 0;
+        ctx->small_box = opts->no_small_box == 0;
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");
@@ -730,9 +747,10 @@ void amcfd_destroy(amcfd_ctx *ctx)
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->pack) cudaFree(ctx->pack);
-    for (auto &row : ctx->gexec)
-        for (auto &ge : row)
-            if (ge) cudaGraphExecDestroy(ge);
+    for (auto &plane : ctx->gexec)
+        for (auto &row : plane)
+            for (auto &ge : row)
+                if (ge) cudaGraphExecDestroy(ge);
     for (int q = 0; q < 16; q++)
         if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -4,6 +4,8 @@
 // calculateResiduals (fused per cell), the line solver, and correctPressure.
 // The box (istat..iend, jstat..jend, kstat..nkm1) lives in the device status
 // block, so every launch has a fixed grid and walks the box with a stride.
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "amcfd.h"
 
@@ -31,23 +33,28 @@ __device__ __forceinline__ void box_cell(const Box &b, int q, int &i, int &j, in
     k = b.k0 + r / b.nj_;
 }
 
-// cleanVelocities (CFDSolverManager.cpp:2577-2620)
+// cleanVelocities (CFDSolverManager.cpp:2577-2620), one box cell.
+template <typename T>
+__device__ __forceinline__ void clean_cell(const Params &p, const Fields<T> &g, int i, int j, int k)
+{
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const T ts = (T)p.tsolid;
+    size_t c = cidx(i, j, k, nj, nip);
+    T tc = g.temp[c];
+    if (mind(tc, g.temp[c + 1]) <= ts) g.uvel[c + 1] = T(0);
+    if (mind(tc, g.temp[c + sj]) <= ts) g.vvel[c + sj] = T(0);
+    if (mind(tc, g.temp[c + sk]) <= ts) g.wvel[c + sk] = T(0);
+}
 template <typename T>
 __global__ void clean_velocities_kernel(Params p, Fields<T> g)
 {
     Box b;
     if (!get_box(g.st, p, b)) return;
-    const int nj = p.nj, nip = p.nip;
-    const size_t sj = nip, sk = (size_t)nj * nip;
-    const T ts = (T)p.tsolid;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
         int i, j, k;
         box_cell(b, q, i, j, k);
-        size_t c = cidx(i, j, k, nj, nip);
-        T tc = g.temp[c];
-        if (mind(tc, g.temp[c + 1]) <= ts) g.uvel[c + 1] = T(0);
-        if (mind(tc, g.temp[c + sj]) <= ts) g.vvel[c + sj] = T(0);
-        if (mind(tc, g.temp[c + sk]) <= ts) g.wvel[c + sk] = T(0);
+        clean_cell<T>(p, g, i, j, k);
     }
 }
 
@@ -63,9 +70,52 @@ __device__ __forceinline__ double surface_tension_gradient(double t, double a0, 
 }
 
 // applyBCs(1..4) (BoundCondManager.cpp:472-564): Marangoni shear on the top
-// plane for u and v, zero values on the box's east/west faces.  For u it also
-// records max |u| on the top plane (the reference momentum of
-// calculateResiduals(1), CFDSolverManager.cpp:1983-1991).
+// plane for u and v, zero values on the box's east/west faces.  Item q < ntop is
+// a top-plane cell, the rest are east/west edge pairs.  For u it returns |u| on
+// the top plane (the reference momentum of calculateResiduals(1),
+// CFDSolverManager.cpp:1983-1991), else 0.
+__device__ __forceinline__ int mom_bc_items(const Params &p, const Status *st, const Box &b, int ivar,
+                                            int &ntop)
+{
+    ntop = (ivar <= 2) ? b.ni_ * b.nj_ : 0;
+    return ntop + b.nj_ * (p.nkm1 - b.k0);
+}
+template <typename T>
+__device__ __forceinline__ double mom_bc_item(const Params &p, const Fields<T> &g, const Status *st,
+                                              const Box &b, int ivar, int q, int ntop)
+{
+    const int nj = p.nj, nip = p.nip, nkm1 = p.nkm1, nkm2 = p.nkm2;
+    T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
+    if (q < ntop) {
+        int i = b.i0 + q % b.ni_, j = b.j0 + q / b.ni_;
+        size_t ct = cidx(i, j, nkm1, nj, nip), cb = cidx(i, j, nkm2, nj, nip);
+        double tt = (double)g.temp[ct];
+        double grad, fl, vis1;
+        if (ivar == 1) {
+            double fx = g.fracx[i - 1];
+            grad = (tt - (double)g.temp[ct - 1]) * g.dxpwinv[i];
+            fl = (double)g.fracl[ct] * (1.0 - fx) + (double)g.fracl[ct - 1] * fx;
+            double vc = (double)g.vis_nxt[cb], vw = (double)g.vis_nxt[cb - 1];
+            vis1 = vc * vw / (vc * (1.0 - fx) + vw * fx);
+        } else {
+            double fy = g.fracy[j - 1];
+            grad = (tt - (double)g.temp[ct - nip]) * g.dypsinv[j];
+            fl = (double)g.fracl[ct] * (1.0 - fy) + (double)g.fracl[ct - nip] * fy;
+            double vc = (double)g.vis_nxt[cb], vs = (double)g.vis_nxt[cb - nip];
+            vis1 = vc * vs / (vc * (1.0 - fy) + vs * fy);
+        }
+        double term1 = fl * surface_tension_gradient(tt, p.a_oxygen, p.dgdtp) * grad /
+                       (vis1 * g.dzpbinv[nkm1]);
+        T val = (T)((double)phi[cb] + term1);
+        phi[ct] = val;
+        return ivar == 1 ? fabs((double)val) : 0.0;
+    }
+    int r = q - ntop;
+    int j = b.j0 + r % b.nj_, k = b.k0 + r / b.nj_;
+    phi[cidx(st->istat, j, k, nj, nip)] = T(0);
+    phi[cidx(st->iend, j, k, nj, nip)] = T(0);
+    return 0.0;
+}
 template <typename T>
 __global__ void mom_bc_kernel(Params p, Fields<T> g, int ivar, double *red_umax)
 {
@@ -73,43 +123,10 @@ __global__ void mom_bc_kernel(Params p, Fields<T> g, int ivar, double *red_umax)
     const Status *st = g.st;
     double umax = 0.0;
     if (get_box(st, p, b)) {
-        const int nj = p.nj, nip = p.nip, nkm1 = p.nkm1, nkm2 = p.nkm2;
-        const int istat = st->istat, iend = st->iend;
-        const int ntop = (ivar <= 2) ? b.ni_ * b.nj_ : 0;
-        const int nedge = b.nj_ * (nkm1 - b.k0);
-        T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
-        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < ntop + nedge;
-             q += gridDim.x * blockDim.x) {
-            if (q < ntop) {
-                int i = b.i0 + q % b.ni_, j = b.j0 + q / b.ni_;
-                size_t ct = cidx(i, j, nkm1, nj, nip), cb = cidx(i, j, nkm2, nj, nip);
-                double tt = (double)g.temp[ct];
-                double grad, fl, vis1;
-                if (ivar == 1) {
-                    double fx = g.fracx[i - 1];
-                    grad = (tt - (double)g.temp[ct - 1]) * g.dxpwinv[i];
-                    fl = (double)g.fracl[ct] * (1.0 - fx) + (double)g.fracl[ct - 1] * fx;
-                    double vc = (double)g.vis_nxt[cb], vw = (double)g.vis_nxt[cb - 1];
-                    vis1 = vc * vw / (vc * (1.0 - fx) + vw * fx);
-                } else {
-                    double fy = g.fracy[j - 1];
-                    grad = (tt - (double)g.temp[ct - nip]) * g.dypsinv[j];
-                    fl = (double)g.fracl[ct] * (1.0 - fy) + (double)g.fracl[ct - nip] * fy;
-                    double vc = (double)g.vis_nxt[cb], vs = (double)g.vis_nxt[cb - nip];
-                    vis1 = vc * vs / (vc * (1.0 - fy) + vs * fy);
-                }
-                double term1 = fl * surface_tension_gradient(tt, p.a_oxygen, p.dgdtp) * grad /
-                               (vis1 * g.dzpbinv[nkm1]);
-                T val = (T)((double)phi[cb] + term1);
-                phi[ct] = val;
-                if (ivar == 1) umax = maxd(umax, fabs((double)val));
-            } else {
-                int r = q - ntop;
-                int j = b.j0 + r % b.nj_, k = b.k0 + r / b.nj_;
-                phi[cidx(istat, j, k, nj, nip)] = T(0);
-                phi[cidx(iend, j, k, nj, nip)] = T(0);
-            }
-        }
+        int ntop;
+        const int n = mom_bc_items(p, st, b, ivar, ntop);
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+            umax = maxd(umax, mom_bc_item<T>(p, g, st, b, ivar, q, ntop));
     }
     if (ivar == 1) {
         double v[1] = {umax};
@@ -119,219 +136,227 @@ __global__ void mom_bc_kernel(Params p, Fields<T> g, int ivar, double *red_umax)
     }
 }
 
+// One cell of the u/v/w equation (ivar 1..3) of the momentum box: coefficients,
+// source, under-relaxation, the solid freeze and d = A/ap, written to the shared
+// coefficient arrays; returns |residual| of the cell (calculateResiduals(1..3)).
+template <typename T>
+__device__ __forceinline__ double mom_assemble_cell(const Params &p, const Fields<T> &g, const Status *st,
+                                                    int ivar, int i, int j, int k)
+{
+    using R = T;
+    const int nj = p.nj, nip = p.nip, nkm2 = p.nkm2, njm2 = p.njm2, nim2 = p.nim2;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const int sch = p.scheme;
+    const R delt = (R)st->delt;
+    const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt, *vis = g.vis_nxt;
+    const double *fx = g.fracx, *fy = g.fracy, *fz = g.fracz, *xu = g.xu, *yv = g.yv, *zw = g.zw;
+    const size_t c = cidx(i, j, k, nj, nip);
+    R an, as_, ae, aw, at, ab, apnot, su, sp, tmp, areaD, vol;
+    const R rc = rho[c];
+    R *phi;
+    const R *phinot;
+    size_t cn;  // upstream scalar node of the staggered cell
+    R urf, flv;
+    if (ivar == 1) {
+        const R fxm = (R)fx[i - 1];
+        R vn = v[c + sj] * (R(1) - fxm) + v[c + sj - 1] * fxm;
+        R vs = v[c] * (R(1) - fxm) + v[c - 1] * fxm;
+        R ue = (u[c + 1] + u[c]) * R(0.5);
+        R uw = (u[c - 1] + u[c]) * R(0.5);
+        R wt = w[c + sk] * (R(1) - fxm) + w[c + sk - 1] * fxm;
+        R wb = w[c] * (R(1) - fxm) + w[c - 1] * fxm;
+        const R auik = (R)area_uik(g, i, k), ajk = (R)area_jk(p, g, j, k), auij = (R)area_uij(g, i, j);
+        R fn = vn * rc * auik, fs = vs * rc * auik, fe = ue * rc * ajk, fw = uw * rc * ajk;
+        R ft = wt * rc * auij, fb = wb * rc * auij;
+        R visu = vis[c] * vis[c - 1] / (fxm * vis[c - 1] + (R(1) - fxm) * vis[c]);
+        R visun = vis[c + sj] * vis[c + sj - 1] / (fxm * vis[c + sj - 1] + (R(1) - fxm) * vis[c + sj]);
+        R visus = vis[c - sj] * vis[c - sj - 1] / (fxm * vis[c - sj - 1] + (R(1) - fxm) * vis[c - sj]);
+        R visn = (j == njm2) ? visu : visu * visun / ((R(1) - (R)fy[j]) * visun + (R)fy[j] * visu);
+        R viss = (j == 1) ? visu : visu * visus / ((R)fy[j - 1] * visus + (R(1) - (R)fy[j - 1]) * visu);
+        R vise = vis[c], visw = vis[c - 1];
+        R visut = vis[c + sk] * vis[c + sk - 1] / (fxm * vis[c + sk - 1] + (R(1) - fxm) * vis[c + sk]);
+        R visub = vis[c - sk] * vis[c - sk - 1] / (fxm * vis[c - sk - 1] + (R(1) - fxm) * vis[c - sk]);
+        R vist = (k == nkm2) ? visu : visut * visu / ((R)fz[k] * visu + (R(1) - (R)fz[k]) * visut);
+        R visb = (k == 1) ? visu : visub * visu / ((R(1) - (R)fz[k - 1]) * visu + (R)fz[k - 1] * visub);
+        R dn = visn * auik * (R)g.dypsinv[j + 1], ds = viss * auik * (R)g.dypsinv[j];
+        R de = vise * ajk / (R)(xu[i + 1] - xu[i]), dw = visw * ajk / (R)(xu[i] - xu[i - 1]);
+        R dt = vist * auij * (R)g.dzpbinv[k + 1], db = visb * auij * (R)g.dzpbinv[k];
+        face_coef<R>(sch, dn, fn, an, tmp);
+        face_coef<R>(sch, ds, fs, tmp, as_);
+        face_coef<R>(sch, de, fe, ae, tmp);
+        face_coef<R>(sch, dw, fw, tmp, aw);
+        face_coef<R>(sch, dt, ft, at, tmp);
+        face_coef<R>(sch, db, fb, tmp, ab);
+        vol = (R)volume_u(g, i, j, k);
+        apnot = rc * vol / delt;
+        R delf = fn - fs + fe - fw + ft - fb;
+        R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+        su = -cp1 * u[c];
+        su += ajk * (g.pressure[c - 1] - g.pressure[c]);
+        sp = -cp0;
+        su += apnot * g.unot[c];
+        R dudxp = (u[c + 1] - u[c]) / (R)(xu[i + 1] - xu[i]);
+        R dudxm = (u[c] - u[c - 1]) / (R)(xu[i] - xu[i - 1]);
+        su += (vise * dudxp - visw * dudxm) * ajk;
+        R dvdxp = (v[c + sj] - v[c + sj - 1]) * (R)g.dxpwinv[i];
+        R dvdxm = (v[c] - v[c - 1]) * (R)g.dxpwinv[i];
+        su += (visn * dvdxp - viss * dvdxm) * auik;
+        R dwdxp = (w[c + sk] - w[c + sk - 1]) * (R)g.dxpwinv[i];
+        R dwdxm = (w[c] - w[c - 1]) * (R)g.dxpwinv[i];
+        su += (vist * dwdxp - visb * dwdxm) * auij;
+        phi = g.uvel; phinot = g.unot; cn = c - 1; urf = (R)p.urfu; areaD = ajk;
+        flv = g.fracl[c] * (R(1) - fxm) + g.fracl[c - 1] * fxm;
+    } else if (ivar == 2) {
+        const R fym = (R)fy[j - 1];
+        R vn = (v[c] + v[c + sj]) * R(0.5);
+        R vs = (v[c] + v[c - sj]) * R(0.5);
+        R ue = u[c + 1] * (R(1) - fym) + u[c + 1 - sj] * fym;
+        R uw = u[c] * (R(1) - fym) + u[c - sj] * fym;
+        R wt = w[c + sk] * (R(1) - fym) + w[c + sk - sj] * fym;
+        R wb = w[c] * (R(1) - fym) + w[c - sj] * fym;
+        const R aik = (R)area_ik(p, g, i, k), avjk = (R)area_vjk(g, j, k), avij = (R)area_vij(g, i, j);
+        R fn = vn * rc * aik, fs = vs * rc * aik, fe = ue * rc * avjk, fw = uw * rc * avjk;
+        R ft = wt * rc * avij, fb = wb * rc * avij;
+        R visn = vis[c], viss = vis[c - sj];
+        R visv = vis[c] * vis[c - sj] / (fym * vis[c - sj] + (R(1) - fym) * vis[c]);
+        R visve = vis[c + 1] * vis[c + 1 - sj] / (fym * vis[c + 1 - sj] + (R(1) - fym) * vis[c + 1]);
+        R visvw = vis[c - 1] * vis[c - 1 - sj] / (fym * vis[c - 1 - sj] + (R(1) - fym) * vis[c - 1]);
+        R vise = (i == nim2) ? visv : visv * visve / ((R(1) - (R)fx[i]) * visve + (R)fx[i] * visv);
+        R visw = (i == 1) ? visv : visv * visvw / ((R)fx[i - 1] * visvw + (R(1) - (R)fx[i - 1]) * visv);
+        R visvt = vis[c + sk] * vis[c + sk - sj] / (fym * vis[c + sk - sj] + (R(1) - fym) * vis[c + sk]);
+        R visvb = vis[c - sk] * vis[c - sk - sj] / (fym * vis[c - sk - sj] + (R(1) - fym) * vis[c - sk]);
+        R vist = (k == nkm2) ? visv : visv * visvt / ((R(1) - (R)fz[k]) * visvt + (R)fz[k] * visv);
+        R visb = (k == 1) ? visv : visv * visvb / ((R)fz[k - 1] * visvb + (R(1) - (R)fz[k - 1]) * visv);
+        R dn = visn * aik / (R)(yv[j + 1] - yv[j]), ds = viss * aik / (R)(yv[j] - yv[j - 1]);
+        R de = vise * avjk * (R)g.dxpwinv[i + 1], dw = visw * avjk * (R)g.dxpwinv[i];
+        R dt = vist * avij * (R)g.dzpbinv[k + 1], db = visb * avij * (R)g.dzpbinv[k];
+        face_coef<R>(sch, dn, fn, an, tmp);
+        face_coef<R>(sch, ds, fs, tmp, as_);
+        face_coef<R>(sch, de, fe, ae, tmp);
+        face_coef<R>(sch, dw, fw, tmp, aw);
+        face_coef<R>(sch, dt, ft, at, tmp);
+        face_coef<R>(sch, db, fb, tmp, ab);
+        vol = (R)volume_v(g, i, j, k);
+        apnot = rc * vol / delt;
+        R delf = fn - fs + fe - fw + ft - fb;
+        R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+        su = -cp1 * v[c];
+        su += aik * (g.pressure[c - sj] - g.pressure[c]);
+        sp = -cp0;
+        su += apnot * g.vnot[c];
+        R dudyp = (u[c + 1] - u[c + 1 - sj]) * (R)g.dypsinv[j];
+        R dudym = (u[c] - u[c - sj]) * (R)g.dypsinv[j];
+        su += (vise * dudyp - visw * dudym) * avjk;
+        R dvdyp = (v[c + sj] - v[c]) / (R)(yv[j + 1] - yv[j]);
+        R dvdym = (v[c] - v[c - sj]) / (R)(yv[j] - yv[j - 1]);
+        su += (visn * dvdyp - viss * dvdym) * aik;
+        R dwdyp = (w[c + sk] - w[c + sk - sj]) * (R)g.dypsinv[j];
+        R dwdym = (w[c] - w[c - sj]) * (R)g.dypsinv[j];
+        su += (vist * dwdyp - visb * dwdym) * avij;
+        phi = g.vvel; phinot = g.vnot; cn = c - sj; urf = (R)p.urfv; areaD = aik;
+        flv = g.fracl[c] * (R(1) - fym) + g.fracl[c - sj] * fym;
+    } else {
+        const R fzm = (R)fz[k - 1];
+        R vn = v[c + sj] * (R(1) - fzm) + v[c + sj - sk] * fzm;
+        R vs = v[c] * (R(1) - fzm) + v[c - sk] * fzm;
+        R ue = u[c + 1] * (R(1) - fzm) + u[c + 1 - sk] * fzm;
+        R uw = u[c] * (R(1) - fzm) + u[c - sk] * fzm;
+        R wt = (w[c] + w[c + sk]) * R(0.5);
+        R wb = (w[c] + w[c - sk]) * R(0.5);
+        const R awik = (R)area_wik(g, i, k), awjk = (R)area_wjk(g, j, k), aij = (R)area_ij(p, g, i, j);
+        R fn = vn * rc * awik, fs = vs * rc * awik, fe = ue * rc * awjk, fw = uw * rc * awjk;
+        R ft = wt * rc * aij, fb = wb * rc * aij;
+        R vis_w = vis[c] * vis[c - sk] / (fzm * vis[c - sk] + (R(1) - fzm) * vis[c]);
+        R viswn = vis[c + sj] * vis[c + sj - sk] / (fzm * vis[c + sj - sk] + (R(1) - fzm) * vis[c + sj]);
+        R visws = vis[c - sj] * vis[c - sj - sk] / (fzm * vis[c - sj - sk] + (R(1) - fzm) * vis[c - sj]);
+        R visn = (j == njm2) ? vis_w : vis_w * viswn / ((R(1) - (R)fy[j]) * viswn + (R)fy[j] * vis_w);
+        R viss = (j == 1) ? vis_w : vis_w * visws / ((R)fy[j - 1] * visws + (R(1) - (R)fy[j - 1]) * vis_w);
+        R viswe = vis[c + 1] * vis[c + 1 - sk] / (fzm * vis[c + 1 - sk] + (R(1) - fzm) * vis[c + 1]);
+        R visww = vis[c - 1] * vis[c - 1 - sk] / (fzm * vis[c - 1 - sk] + (R(1) - fzm) * vis[c - 1]);
+        R vise = (i == nim2) ? vis_w : vis_w * viswe / ((R(1) - (R)fx[i]) * viswe + (R)fx[i] * vis_w);
+        R visw = (i == 1) ? vis_w : vis_w * visww / ((R)fx[i - 1] * visww + (R(1) - (R)fx[i - 1]) * vis_w);
+        R vist = vis[c], visb = vis[c - sk];
+        R dn = visn * awik * (R)g.dypsinv[j + 1], ds = viss * awik * (R)g.dypsinv[j];
+        R de = vise * awjk * (R)g.dxpwinv[i + 1], dw = visw * awjk * (R)g.dxpwinv[i];
+        R dt = vist * aij / (R)(zw[k + 1] - zw[k]), db = visb * aij / (R)(zw[k] - zw[k - 1]);
+        face_coef<R>(sch, dn, fn, an, tmp);
+        face_coef<R>(sch, ds, fs, tmp, as_);
+        face_coef<R>(sch, de, fe, ae, tmp);
+        face_coef<R>(sch, dw, fw, tmp, aw);
+        face_coef<R>(sch, dt, ft, at, tmp);
+        face_coef<R>(sch, db, fb, tmp, ab);
+        vol = (R)volume_w(g, i, j, k);
+        apnot = rc * vol / delt;
+        R delf = fn - fs + fe - fw + ft - fb;
+        R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
+        su = -cp1 * w[c];
+        su += aij * (g.pressure[c - sk] - g.pressure[c]);
+        sp = -cp0;
+        su += apnot * g.wnot[c];
+        R dudzp = (u[c + 1] - u[c + 1 - sk]) * (R)g.dzpbinv[k];
+        R dudzm = (u[c] - u[c - sk]) * (R)g.dzpbinv[k];
+        su += (vise * dudzp - visw * dudzm) * awjk;
+        R dvdzp = (v[c + sj] - v[c + sj - sk]) * (R)g.dzpbinv[k];
+        R dvdzm = (v[c] - v[c - sk]) * (R)g.dzpbinv[k];
+        su += (visn * dvdzp - viss * dvdzm) * awik;
+        R dwdzp = (w[c + sk] - w[c]) / (R)(zw[k + 1] - zw[k]);
+        R dwdzm = (w[c] - w[c - sk]) / (R)(zw[k] - zw[k - 1]);
+        su += (vist * dwdzp - visb * dwdzm) * aij;
+        phi = g.wvel; phinot = g.wnot; cn = c - sk; urf = (R)p.urfw; areaD = aij;
+        flv = g.fracl[c] * (R(1) - fzm) + g.fracl[c - sk] * fzm;
+    }
+    (void)phinot;
+    // ---- calculateSource ----
+    if (flv > R(0)) {
+        R term = (R)p.darcyKo * ((R(1) - flv) * (R(1) - flv)) / ((flv * flv * flv) + (R)kSmall);
+        sp -= term * vol;
+        if (p.steady) {
+            R area = ivar == 1 ? (R)area_jk(p, g, j, k) : ivar == 2 ? (R)area_vjk(g, j, k)
+                                                                    : (R)area_wjk(g, j, k);
+            su += rc * (R)st->scanvel * area * (phi[c - 1] - phi[c]);
+        }
+        if (ivar == 3) {
+            R fzm = (R)fz[k - 1];
+            R boufac = rc * (R)p.grav * (R)p.beta;
+            R tw = g.temp[c] * (R(1) - fzm) + g.temp[c - sk] * fzm;
+            su += boufac * vol * (tw - (R)p.tsolid);
+        }
+    }
+    if (ivar != 3 && k == nkm2) {
+        su += at * phi[c + sk];
+        sp -= at;
+        at = R(0);
+    }
+    R ap = an + as_ + ae + aw + at + ab + apnot - sp;
+    R dcoef = areaD / ap;
+    ap /= urf;
+    su += (R(1) - urf) * ap * phi[c];
+    dcoef *= urf;
+    if (mind(g.temp[c], g.temp[cn]) <= (R)p.tsolid) {
+        su = R(0);
+        an = as_ = ae = aw = at = ab = R(0);
+        ap = (R)kLarge;
+    }
+    g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
+    g.ap[c] = ap; g.su[c] = su;
+    (ivar == 1 ? g.dux : ivar == 2 ? g.dvy : g.dwz)[c] = dcoef;
+    R r = an * phi[c + sj] + as_ * phi[c - sj] + ae * phi[c + 1] + aw * phi[c - 1] +
+          at * phi[c + sk] + ab * phi[c - sk] + su - ap * phi[c];
+    return fabs((double)r);
+}
+
 // discretizeEquations(1..3) + calculateSource(1..3) + calculateResiduals(1..3)
 // (CFDSolverManager.cpp:771-1111, 1408-1644, 1960-2046), one box cell per thread.
 template <typename T>
 __global__ void __launch_bounds__(256) mom_assemble_kernel(Params p, Fields<T> g, int ivar, double *red)
 {
-    using R = T;
     Box b;
-    const Status *st = g.st;
     double sumd = 0.0;
-    if (get_box(st, p, b)) {
-        const int nj = p.nj, nip = p.nip, nkm1 = p.nkm1, nkm2 = p.nkm2, njm2 = p.njm2, nim2 = p.nim2;
-        const size_t sj = nip, sk = (size_t)nj * nip;
-        const int sch = p.scheme;
-        const R delt = (R)st->delt;
-        const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt, *vis = g.vis_nxt;
-        const double *fx = g.fracx, *fy = g.fracy, *fz = g.fracz, *xu = g.xu, *yv = g.yv, *zw = g.zw;
+    if (get_box(g.st, p, b)) {
         for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
             int i, j, k;
             box_cell(b, q, i, j, k);
-            const size_t c = cidx(i, j, k, nj, nip);
-            R an, as_, ae, aw, at, ab, apnot, su, sp, tmp, areaD, vol;
-            const R rc = rho[c];
-            R *phi;
-            const R *phinot;
-            size_t cn;  // upstream scalar node of the staggered cell
-            R urf, flv;
-            if (ivar == 1) {
-                const R fxm = (R)fx[i - 1];
-                R vn = v[c + sj] * (R(1) - fxm) + v[c + sj - 1] * fxm;
-                R vs = v[c] * (R(1) - fxm) + v[c - 1] * fxm;
-                R ue = (u[c + 1] + u[c]) * R(0.5);
-                R uw = (u[c - 1] + u[c]) * R(0.5);
-                R wt = w[c + sk] * (R(1) - fxm) + w[c + sk - 1] * fxm;
-                R wb = w[c] * (R(1) - fxm) + w[c - 1] * fxm;
-                const R auik = (R)area_uik(g, i, k), ajk = (R)area_jk(p, g, j, k), auij = (R)area_uij(g, i, j);
-                R fn = vn * rc * auik, fs = vs * rc * auik, fe = ue * rc * ajk, fw = uw * rc * ajk;
-                R ft = wt * rc * auij, fb = wb * rc * auij;
-                R visu = vis[c] * vis[c - 1] / (fxm * vis[c - 1] + (R(1) - fxm) * vis[c]);
-                R visun = vis[c + sj] * vis[c + sj - 1] / (fxm * vis[c + sj - 1] + (R(1) - fxm) * vis[c + sj]);
-                R visus = vis[c - sj] * vis[c - sj - 1] / (fxm * vis[c - sj - 1] + (R(1) - fxm) * vis[c - sj]);
-                R visn = (j == njm2) ? visu : visu * visun / ((R(1) - (R)fy[j]) * visun + (R)fy[j] * visu);
-                R viss = (j == 1) ? visu : visu * visus / ((R)fy[j - 1] * visus + (R(1) - (R)fy[j - 1]) * visu);
-                R vise = vis[c], visw = vis[c - 1];
-                R visut = vis[c + sk] * vis[c + sk - 1] / (fxm * vis[c + sk - 1] + (R(1) - fxm) * vis[c + sk]);
-                R visub = vis[c - sk] * vis[c - sk - 1] / (fxm * vis[c - sk - 1] + (R(1) - fxm) * vis[c - sk]);
-                R vist = (k == nkm2) ? visu : visut * visu / ((R)fz[k] * visu + (R(1) - (R)fz[k]) * visut);
-                R visb = (k == 1) ? visu : visub * visu / ((R(1) - (R)fz[k - 1]) * visu + (R)fz[k - 1] * visub);
-                R dn = visn * auik * (R)g.dypsinv[j + 1], ds = viss * auik * (R)g.dypsinv[j];
-                R de = vise * ajk / (R)(xu[i + 1] - xu[i]), dw = visw * ajk / (R)(xu[i] - xu[i - 1]);
-                R dt = vist * auij * (R)g.dzpbinv[k + 1], db = visb * auij * (R)g.dzpbinv[k];
-                face_coef<R>(sch, dn, fn, an, tmp);
-                face_coef<R>(sch, ds, fs, tmp, as_);
-                face_coef<R>(sch, de, fe, ae, tmp);
-                face_coef<R>(sch, dw, fw, tmp, aw);
-                face_coef<R>(sch, dt, ft, at, tmp);
-                face_coef<R>(sch, db, fb, tmp, ab);
-                vol = (R)volume_u(g, i, j, k);
-                apnot = rc * vol / delt;
-                R delf = fn - fs + fe - fw + ft - fb;
-                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
-                su = -cp1 * u[c];
-                su += ajk * (g.pressure[c - 1] - g.pressure[c]);
-                sp = -cp0;
-                su += apnot * g.unot[c];
-                R dudxp = (u[c + 1] - u[c]) / (R)(xu[i + 1] - xu[i]);
-                R dudxm = (u[c] - u[c - 1]) / (R)(xu[i] - xu[i - 1]);
-                su += (vise * dudxp - visw * dudxm) * ajk;
-                R dvdxp = (v[c + sj] - v[c + sj - 1]) * (R)g.dxpwinv[i];
-                R dvdxm = (v[c] - v[c - 1]) * (R)g.dxpwinv[i];
-                su += (visn * dvdxp - viss * dvdxm) * auik;
-                R dwdxp = (w[c + sk] - w[c + sk - 1]) * (R)g.dxpwinv[i];
-                R dwdxm = (w[c] - w[c - 1]) * (R)g.dxpwinv[i];
-                su += (vist * dwdxp - visb * dwdxm) * auij;
-                phi = g.uvel; phinot = g.unot; cn = c - 1; urf = (R)p.urfu; areaD = ajk;
-                flv = g.fracl[c] * (R(1) - fxm) + g.fracl[c - 1] * fxm;
-            } else if (ivar == 2) {
-                const R fym = (R)fy[j - 1];
-                R vn = (v[c] + v[c + sj]) * R(0.5);
-                R vs = (v[c] + v[c - sj]) * R(0.5);
-                R ue = u[c + 1] * (R(1) - fym) + u[c + 1 - sj] * fym;
-                R uw = u[c] * (R(1) - fym) + u[c - sj] * fym;
-                R wt = w[c + sk] * (R(1) - fym) + w[c + sk - sj] * fym;
-                R wb = w[c] * (R(1) - fym) + w[c - sj] * fym;
-                const R aik = (R)area_ik(p, g, i, k), avjk = (R)area_vjk(g, j, k), avij = (R)area_vij(g, i, j);
-                R fn = vn * rc * aik, fs = vs * rc * aik, fe = ue * rc * avjk, fw = uw * rc * avjk;
-                R ft = wt * rc * avij, fb = wb * rc * avij;
-                R visn = vis[c], viss = vis[c - sj];
-                R visv = vis[c] * vis[c - sj] / (fym * vis[c - sj] + (R(1) - fym) * vis[c]);
-                R visve = vis[c + 1] * vis[c + 1 - sj] / (fym * vis[c + 1 - sj] + (R(1) - fym) * vis[c + 1]);
-                R visvw = vis[c - 1] * vis[c - 1 - sj] / (fym * vis[c - 1 - sj] + (R(1) - fym) * vis[c - 1]);
-                R vise = (i == nim2) ? visv : visv * visve / ((R(1) - (R)fx[i]) * visve + (R)fx[i] * visv);
-                R visw = (i == 1) ? visv : visv * visvw / ((R)fx[i - 1] * visvw + (R(1) - (R)fx[i - 1]) * visv);
-                R visvt = vis[c + sk] * vis[c + sk - sj] / (fym * vis[c + sk - sj] + (R(1) - fym) * vis[c + sk]);
-                R visvb = vis[c - sk] * vis[c - sk - sj] / (fym * vis[c - sk - sj] + (R(1) - fym) * vis[c - sk]);
-                R vist = (k == nkm2) ? visv : visv * visvt / ((R(1) - (R)fz[k]) * visvt + (R)fz[k] * visv);
-                R visb = (k == 1) ? visv : visv * visvb / ((R)fz[k - 1] * visvb + (R(1) - (R)fz[k - 1]) * visv);
-                R dn = visn * aik / (R)(yv[j + 1] - yv[j]), ds = viss * aik / (R)(yv[j] - yv[j - 1]);
-                R de = vise * avjk * (R)g.dxpwinv[i + 1], dw = visw * avjk * (R)g.dxpwinv[i];
-                R dt = vist * avij * (R)g.dzpbinv[k + 1], db = visb * avij * (R)g.dzpbinv[k];
-                face_coef<R>(sch, dn, fn, an, tmp);
-                face_coef<R>(sch, ds, fs, tmp, as_);
-                face_coef<R>(sch, de, fe, ae, tmp);
-                face_coef<R>(sch, dw, fw, tmp, aw);
-                face_coef<R>(sch, dt, ft, at, tmp);
-                face_coef<R>(sch, db, fb, tmp, ab);
-                vol = (R)volume_v(g, i, j, k);
-                apnot = rc * vol / delt;
-                R delf = fn - fs + fe - fw + ft - fb;
-                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
-                su = -cp1 * v[c];
-                su += aik * (g.pressure[c - sj] - g.pressure[c]);
-                sp = -cp0;
-                su += apnot * g.vnot[c];
-                R dudyp = (u[c + 1] - u[c + 1 - sj]) * (R)g.dypsinv[j];
-                R dudym = (u[c] - u[c - sj]) * (R)g.dypsinv[j];
-                su += (vise * dudyp - visw * dudym) * avjk;
-                R dvdyp = (v[c + sj] - v[c]) / (R)(yv[j + 1] - yv[j]);
-                R dvdym = (v[c] - v[c - sj]) / (R)(yv[j] - yv[j - 1]);
-                su += (visn * dvdyp - viss * dvdym) * aik;
-                R dwdyp = (w[c + sk] - w[c + sk - sj]) * (R)g.dypsinv[j];
-                R dwdym = (w[c] - w[c - sj]) * (R)g.dypsinv[j];
-                su += (vist * dwdyp - visb * dwdym) * avij;
-                phi = g.vvel; phinot = g.vnot; cn = c - sj; urf = (R)p.urfv; areaD = aik;
-                flv = g.fracl[c] * (R(1) - fym) + g.fracl[c - sj] * fym;
-            } else {
-                const R fzm = (R)fz[k - 1];
-                R vn = v[c + sj] * (R(1) - fzm) + v[c + sj - sk] * fzm;
-                R vs = v[c] * (R(1) - fzm) + v[c - sk] * fzm;
-                R ue = u[c + 1] * (R(1) - fzm) + u[c + 1 - sk] * fzm;
-                R uw = u[c] * (R(1) - fzm) + u[c - sk] * fzm;
-                R wt = (w[c] + w[c + sk]) * R(0.5);
-                R wb = (w[c] + w[c - sk]) * R(0.5);
-                const R awik = (R)area_wik(g, i, k), awjk = (R)area_wjk(g, j, k), aij = (R)area_ij(p, g, i, j);
-                R fn = vn * rc * awik, fs = vs * rc * awik, fe = ue * rc * awjk, fw = uw * rc * awjk;
-                R ft = wt * rc * aij, fb = wb * rc * aij;
-                R vis_w = vis[c] * vis[c - sk] / (fzm * vis[c - sk] + (R(1) - fzm) * vis[c]);
-                R viswn = vis[c + sj] * vis[c + sj - sk] / (fzm * vis[c + sj - sk] + (R(1) - fzm) * vis[c + sj]);
-                R visws = vis[c - sj] * vis[c - sj - sk] / (fzm * vis[c - sj - sk] + (R(1) - fzm) * vis[c - sj]);
-                R visn = (j == njm2) ? vis_w : vis_w * viswn / ((R(1) - (R)fy[j]) * viswn + (R)fy[j] * vis_w);
-                R viss = (j == 1) ? vis_w : vis_w * visws / ((R)fy[j - 1] * visws + (R(1) - (R)fy[j - 1]) * vis_w);
-                R viswe = vis[c + 1] * vis[c + 1 - sk] / (fzm * vis[c + 1 - sk] + (R(1) - fzm) * vis[c + 1]);
-                R visww = vis[c - 1] * vis[c - 1 - sk] / (fzm * vis[c - 1 - sk] + (R(1) - fzm) * vis[c - 1]);
-                R vise = (i == nim2) ? vis_w : vis_w * viswe / ((R(1) - (R)fx[i]) * viswe + (R)fx[i] * vis_w);
-                R visw = (i == 1) ? vis_w : vis_w * visww / ((R)fx[i - 1] * visww + (R(1) - (R)fx[i - 1]) * vis_w);
-                R vist = vis[c], visb = vis[c - sk];
-                R dn = visn * awik * (R)g.dypsinv[j + 1], ds = viss * awik * (R)g.dypsinv[j];
-                R de = vise * awjk * (R)g.dxpwinv[i + 1], dw = visw * awjk * (R)g.dxpwinv[i];
-                R dt = vist * aij / (R)(zw[k + 1] - zw[k]), db = visb * aij / (R)(zw[k] - zw[k - 1]);
-                face_coef<R>(sch, dn, fn, an, tmp);
-                face_coef<R>(sch, ds, fs, tmp, as_);
-                face_coef<R>(sch, de, fe, ae, tmp);
-                face_coef<R>(sch, dw, fw, tmp, aw);
-                face_coef<R>(sch, dt, ft, at, tmp);
-                face_coef<R>(sch, db, fb, tmp, ab);
-                vol = (R)volume_w(g, i, j, k);
-                apnot = rc * vol / delt;
-                R delf = fn - fs + fe - fw + ft - fb;
-                R cp0 = maxd(R(0), delf), cp1 = mind(R(0), delf);
-                su = -cp1 * w[c];
-                su += aij * (g.pressure[c - sk] - g.pressure[c]);
-                sp = -cp0;
-                su += apnot * g.wnot[c];
-                R dudzp = (u[c + 1] - u[c + 1 - sk]) * (R)g.dzpbinv[k];
-                R dudzm = (u[c] - u[c - sk]) * (R)g.dzpbinv[k];
-                su += (vise * dudzp - visw * dudzm) * awjk;
-                R dvdzp = (v[c + sj] - v[c + sj - sk]) * (R)g.dzpbinv[k];
-                R dvdzm = (v[c] - v[c - sk]) * (R)g.dzpbinv[k];
-                su += (visn * dvdzp - viss * dvdzm) * awik;
-                R dwdzp = (w[c + sk] - w[c]) / (R)(zw[k + 1] - zw[k]);
-                R dwdzm = (w[c] - w[c - sk]) / (R)(zw[k] - zw[k - 1]);
-                su += (vist * dwdzp - visb * dwdzm) * aij;
-                phi = g.wvel; phinot = g.wnot; cn = c - sk; urf = (R)p.urfw; areaD = aij;
-                flv = g.fracl[c] * (R(1) - fzm) + g.fracl[c - sk] * fzm;
-            }
-            (void)phinot;
-            // ---- calculateSource ----
-            if (flv > R(0)) {
-                R term = (R)p.darcyKo * ((R(1) - flv) * (R(1) - flv)) / ((flv * flv * flv) + (R)kSmall);
-                sp -= term * vol;
-                if (p.steady) {
-                    R area = ivar == 1 ? (R)area_jk(p, g, j, k) : ivar == 2 ? (R)area_vjk(g, j, k)
-                                                                            : (R)area_wjk(g, j, k);
-                    su += rc * (R)st->scanvel * area * (phi[c - 1] - phi[c]);
-                }
-                if (ivar == 3) {
-                    R fzm = (R)fz[k - 1];
-                    R boufac = rc * (R)p.grav * (R)p.beta;
-                    R tw = g.temp[c] * (R(1) - fzm) + g.temp[c - sk] * fzm;
-                    su += boufac * vol * (tw - (R)p.tsolid);
-                }
-            }
-            if (ivar != 3 && k == nkm2) {
-                su += at * phi[c + sk];
-                sp -= at;
-                at = R(0);
-            }
-            R ap = an + as_ + ae + aw + at + ab + apnot - sp;
-            R dcoef = areaD / ap;
-            ap /= urf;
-            su += (R(1) - urf) * ap * phi[c];
-            dcoef *= urf;
-            if (mind(g.temp[c], g.temp[cn]) <= (R)p.tsolid) {
-                su = R(0);
-                an = as_ = ae = aw = at = ab = R(0);
-                ap = (R)kLarge;
-            }
-            g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
-            g.ap[c] = ap; g.su[c] = su;
-            (ivar == 1 ? g.dux : ivar == 2 ? g.dvy : g.dwz)[c] = dcoef;
-            R r = an * phi[c + sj] + as_ * phi[c - sj] + ae * phi[c + 1] + aw * phi[c - 1] +
-                  at * phi[c + sk] + ab * phi[c - sk] + su - ap * phi[c];
-            sumd += fabs((double)r);
-            (void)nkm1;
+            sumd += mom_assemble_cell<T>(p, g, g.st, ivar, i, j, k);
         }
     }
     double v[1] = {sumd};
@@ -341,48 +366,54 @@ __global__ void __launch_bounds__(256) mom_assemble_kernel(Params p, Fields<T> g
 }
 
 // discretizeEquations(4) + calculateSource(4) + calculateResiduals(4)
-// (CFDSolverManager.cpp:1112-1156, 1645-1676, 2047-2071).
+// (CFDSolverManager.cpp:1112-1156, 1645-1676, 2047-2071), one box cell: p'
+// coefficients, |mass imbalance| and the mass-flux denominator added to the sums.
+template <typename T>
+__device__ __forceinline__ void pp_assemble_cell(const Params &p, const Fields<T> &g, int i, int j, int k,
+                                                 double &resorm, double &denom)
+{
+    using R = T;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt;
+    const size_t c = cidx(i, j, k, nj, nip);
+    const R rc = rho[c];
+    const R aik = (R)area_ik(p, g, i, k), ajk = (R)area_jk(p, g, j, k), aij = (R)area_ij(p, g, i, j);
+    R an = aik * g.dvy[c + sj] * rc;
+    R as_ = aik * g.dvy[c] * rc;
+    R ae = ajk * g.dux[c + 1] * rc;
+    R aw = ajk * g.dux[c] * rc;
+    R at = aij * g.dwz[c + sk] * rc;
+    R ab = aij * g.dwz[c] * rc;
+    R fn = v[c + sj] * aik * rc, fs = v[c] * aik * rc;
+    R fe = u[c + 1] * ajk * rc, fw = u[c] * ajk * rc;
+    R ft = w[c + sk] * aij * rc, fb = w[c] * aij * rc;
+    R delf = fn - fs + fe - fw + ft - fb;
+    R sp = R(0), su = -delf;
+    resorm += fabs((double)delf);
+    R ap = an + as_ + ae + aw + at + ab - sp;
+    if (g.temp[c] <= (R)p.tsolid) {
+        su = R(0);
+        an = as_ = ae = aw = at = ab = R(0);
+        ap = (R)kLarge;
+    }
+    g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
+    g.ap[c] = ap; g.su[c] = su;
+    double dtp = (fabs((double)u[c]) + fabs((double)u[c + 1])) * (double)ajk +
+                 (fabs((double)v[c]) + fabs((double)v[c + sj])) * (double)aik +
+                 (fabs((double)w[c]) + fabs((double)w[c + sk])) * (double)aij;
+    denom += 0.5 * fabs(dtp);
+}
 template <typename T>
 __global__ void __launch_bounds__(256) pp_assemble_kernel(Params p, Fields<T> g, double *red)
 {
-    using R = T;
     Box b;
-    const Status *st = g.st;
     double resorm = 0.0, denom = 0.0;
-    if (get_box(st, p, b)) {
-        const int nj = p.nj, nip = p.nip;
-        const size_t sj = nip, sk = (size_t)nj * nip;
-        const R *u = g.uvel, *v = g.vvel, *w = g.wvel, *rho = g.rho_nxt;
+    if (get_box(g.st, p, b)) {
         for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
             int i, j, k;
             box_cell(b, q, i, j, k);
-            const size_t c = cidx(i, j, k, nj, nip);
-            const R rc = rho[c];
-            const R aik = (R)area_ik(p, g, i, k), ajk = (R)area_jk(p, g, j, k), aij = (R)area_ij(p, g, i, j);
-            R an = aik * g.dvy[c + sj] * rc;
-            R as_ = aik * g.dvy[c] * rc;
-            R ae = ajk * g.dux[c + 1] * rc;
-            R aw = ajk * g.dux[c] * rc;
-            R at = aij * g.dwz[c + sk] * rc;
-            R ab = aij * g.dwz[c] * rc;
-            R fn = v[c + sj] * aik * rc, fs = v[c] * aik * rc;
-            R fe = u[c + 1] * ajk * rc, fw = u[c] * ajk * rc;
-            R ft = w[c + sk] * aij * rc, fb = w[c] * aij * rc;
-            R delf = fn - fs + fe - fw + ft - fb;
-            R sp = R(0), su = -delf;
-            resorm += fabs((double)delf);
-            R ap = an + as_ + ae + aw + at + ab - sp;
-            if (g.temp[c] <= (R)p.tsolid) {
-                su = R(0);
-                an = as_ = ae = aw = at = ab = R(0);
-                ap = (R)kLarge;
-            }
-            g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw; g.at[c] = at; g.ab[c] = ab;
-            g.ap[c] = ap; g.su[c] = su;
-            double dtp = (fabs((double)u[c]) + fabs((double)u[c + 1])) * (double)ajk +
-                         (fabs((double)v[c]) + fabs((double)v[c + sj])) * (double)aik +
-                         (fabs((double)w[c]) + fabs((double)w[c + sk])) * (double)aij;
-            denom += 0.5 * fabs(dtp);
+            pp_assemble_cell<T>(p, g, i, j, k, resorm, denom);
         }
     }
     double vv[2] = {resorm, denom};
@@ -392,23 +423,37 @@ __global__ void __launch_bounds__(256) pp_assemble_kernel(Params p, Fields<T> g,
 }
 
 // correctPressure (CFDSolverManager.cpp:2692-2758): velocity correction, then
-// pressure update (two launches: the second zeroes p' that the first reads).
+// pressure update (two passes: the second zeroes p' that the first reads).
+template <typename T>
+__device__ __forceinline__ void correct_velocity_cell(const Params &p, const Fields<T> &g, int i, int j, int k)
+{
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const T ts = (T)p.tsolid;
+    size_t c = cidx(i, j, k, nj, nip);
+    T tc = g.temp[c], ppc = g.pp[c];
+    if (mind(tc, g.temp[c - 1]) > ts) g.uvel[c] += g.dux[c] * (g.pp[c - 1] - ppc);
+    if (mind(tc, g.temp[c - sj]) > ts) g.vvel[c] += g.dvy[c] * (g.pp[c - sj] - ppc);
+    if (mind(tc, g.temp[c - sk]) > ts) g.wvel[c] += g.dwz[c] * (g.pp[c - sk] - ppc);
+}
+template <typename T>
+__device__ __forceinline__ void correct_pressure_cell(const Params &p, const Fields<T> &g, int i, int j, int k)
+{
+    size_t c = cidx(i, j, k, p.nj, p.nip);
+    if (g.temp[c] > (T)p.tsolid) {
+        g.pressure[c] += (T)p.urfp * g.pp[c];
+        g.pp[c] = T(0);
+    }
+}
 template <typename T>
 __global__ void correct_velocity_kernel(Params p, Fields<T> g)
 {
     Box b;
     if (!get_box(g.st, p, b)) return;
-    const int nj = p.nj, nip = p.nip;
-    const size_t sj = nip, sk = (size_t)nj * nip;
-    const T ts = (T)p.tsolid;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
         int i, j, k;
         box_cell(b, q, i, j, k);
-        size_t c = cidx(i, j, k, nj, nip);
-        T tc = g.temp[c], ppc = g.pp[c];
-        if (mind(tc, g.temp[c - 1]) > ts) g.uvel[c] += g.dux[c] * (g.pp[c - 1] - ppc);
-        if (mind(tc, g.temp[c - sj]) > ts) g.vvel[c] += g.dvy[c] * (g.pp[c - sj] - ppc);
-        if (mind(tc, g.temp[c - sk]) > ts) g.wvel[c] += g.dwz[c] * (g.pp[c - sk] - ppc);
+        correct_velocity_cell<T>(p, g, i, j, k);
     }
 }
 template <typename T>
@@ -416,16 +461,10 @@ __global__ void correct_pressure_kernel(Params p, Fields<T> g)
 {
     Box b;
     if (!get_box(g.st, p, b)) return;
-    const int nj = p.nj, nip = p.nip;
-    const T ts = (T)p.tsolid, urfp = (T)p.urfp;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
         int i, j, k;
         box_cell(b, q, i, j, k);
-        size_t c = cidx(i, j, k, nj, nip);
-        if (g.temp[c] > ts) {
-            g.pressure[c] += urfp * g.pp[c];
-            g.pp[c] = T(0);
-        }
+        correct_pressure_cell<T>(p, g, i, j, k);
     }
 }
 
@@ -454,40 +493,381 @@ __device__ double reduce_region(const double *red, int nb, int slot, bool is_max
     return r;
 }
 
-template <typename T>
-__global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, int nb)
+// Normalised momentum residuals from the reduced sums (one thread).
+__device__ __forceinline__ void mom_finalize_status(const Params &p, Status *st, double s1, double s2,
+                                                    double s3, double rm, double dn, double umax)
 {
-    __shared__ double scratch[40];
-    Status *st = g.st;
-    if (!st->momentum_active) return;
+    umax = fmax(umax, 0.0);
+    double refmom = 0.25 * M_PI * (st->width * st->width) * p.dens * (umax * umax);
+    st->umaxt = umax;
+    st->refmom = refmom;
+    st->resoru = s1 / refmom;
+    st->resorv = s2 / refmom;
+    st->resorw = s3 / refmom;
+    dn *= p.dens;
+    st->mass_denom = dn;
+    st->resorm = rm / (dn + kSmall);
+}
+
+// Reduces the per-CTA partials of the four equations (regions 0..3, nb CTAs each)
+// and max |u| on the top plane (region 4, nb_umax entries).
+__device__ void mom_finalize_body(const Params &p, Status *st, const double *red, int nb, int nb_umax,
+                                  double *scratch)
+{
     const size_t region = (size_t)nb * R_NSLOTS;
     double s1 = reduce_region(red + 0 * region, nb, R_MSUMD, false, scratch);
     double s2 = reduce_region(red + 1 * region, nb, R_MSUMD, false, scratch);
     double s3 = reduce_region(red + 2 * region, nb, R_MSUMD, false, scratch);
     double rm = reduce_region(red + 3 * region, nb, R_MRESORM, false, scratch);
     double dn = reduce_region(red + 3 * region, nb, R_MDENOM, false, scratch);
-    double umax = reduce_region(red + 4 * region, nb, R_UMAX, true, scratch);
-    if (threadIdx.x == 0) {
-        umax = fmax(umax, 0.0);
-        double refmom = 0.25 * M_PI * (st->width * st->width) * p.dens * (umax * umax);
-        st->umaxt = umax;
-        st->refmom = refmom;
-        st->resoru = s1 / refmom;
-        st->resorv = s2 / refmom;
-        st->resorw = s3 / refmom;
-        dn *= p.dens;
-        st->mass_denom = dn;
-        st->resorm = rm / (dn + kSmall);
+    double umax = reduce_region(red + 4 * region, nb_umax, R_UMAX, true, scratch);
+    if (threadIdx.x == 0) mom_finalize_status(p, st, s1, s2, s3, rm, dn, umax);
+}
+
+template <typename T>
+__global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, int nb)
+{
+    __shared__ double scratch[40];
+    Status *st = g.st;
+    if (!st->momentum_active) return;
+    mom_finalize_body(p, st, red, nb, nb, scratch);
+}
+
+// ---------------------------------------------------------------------------
+// Small melt-pool boxes (red-black line order).  A melt pool spans a few
+// hundred to a few thousand cells; as ~50 grid launches the momentum chain is
+// bound by launch and drain latency, not by work.  Here the coefficient
+// assembly of each equation stays a grid launch (the arithmetic-heavy part),
+// and everything between two assemblies -- the line solve, applyBCs of the next
+// equation, cleanVelocities, correctPressure and the residual normalisation --
+// runs in one CTA: 9 launches instead of ~50.  For the solve the box's
+// coefficients and unknown (with its one-cell halo) are held in shared memory
+// while one warp per x-line runs the Thomas recurrences of solveLiquidDomain
+// (CFDSolverManager.cpp:2367-2454) for the four sweeps x two colours, as warp
+// scans of affine maps over per-lane chunks (the factorisation is one thread
+// per line, once per equation).  A box
+// larger than the shared memory is solved in place in global memory by the
+// same code (views carry the strides).
+// ---------------------------------------------------------------------------
+constexpr int kMomThreads = 512;
+
+template <typename T> struct V3 {
+    T *b;
+    int sj;
+    long long sk;
+    __device__ __forceinline__ T &operator()(int i, int j, int k) const { return b[i + (long long)j * sj + k * sk]; }
+};
+
+// Deterministic CTA reductions; the result is valid in thread 0.
+__device__ __forceinline__ double cta_sum(double v, double *sh)
+{
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+    return r;
+}
+__device__ __forceinline__ double cta_max(double v, double *sh)
+{
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    double r = -INFINITY;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r = fmax(r, sh[w]);
+    return r;
+}
+
+template <typename T>
+__device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &b, T *phi, T *sm,
+                                int smem_elems, T *scratch)
+{
+    const int NI = b.ni_, NJ = b.nj_, NK = b.k1 - b.k0 + 1;
+    const int ncell = NI * NJ * NK;
+    const int HI = NI + 2, HJ = NJ + 2;
+    const int nhalo = HI * HJ * (NK + 2);
+    const bool fits = 9ll * ncell + nhalo <= (long long)smem_elems;
+    const int gsj = p.nip;
+    const long long gsk = (long long)p.nj * p.nip;
+    const size_t g0 = cidx(b.i0, b.j0, b.k0, p.nj, p.nip);
+    const int tid = threadIdx.x, nth = blockDim.x;
+    V3<T> at, ab, an, as, su, pr, cf, id, qr, ph;
+    const T *ae_src, *aw_src, *ap_src;
+    if (fits) {
+        const int cj = NI;
+        const long long ck = (long long)NI * NJ;
+        T *q0 = sm;
+        at = {q0 + 0ll * ncell, cj, ck}; ab = {q0 + 1ll * ncell, cj, ck};
+        an = {q0 + 2ll * ncell, cj, ck}; as = {q0 + 3ll * ncell, cj, ck};
+        su = {q0 + 4ll * ncell, cj, ck}; pr = {q0 + 5ll * ncell, cj, ck};
+        cf = {q0 + 6ll * ncell, cj, ck}; id = {q0 + 7ll * ncell, cj, ck};
+        qr = {q0 + 8ll * ncell, cj, ck};
+        ph = {q0 + 9ll * ncell + 1 + HI + (long long)HI * HJ, HI, (long long)HI * HJ};
+        for (int q = tid; q < ncell; q += nth) {
+            const int ii = q % NI, r = q / NI, jj = r % NJ, kk = r / NJ;
+            const size_t c = g0 + ii + (size_t)jj * gsj + (size_t)kk * gsk;
+            at(ii, jj, kk) = g.at[c]; ab(ii, jj, kk) = g.ab[c];
+            an(ii, jj, kk) = g.an[c]; as(ii, jj, kk) = g.as[c];
+            su(ii, jj, kk) = g.su[c];
+            pr(ii, jj, kk) = g.ae[c]; cf(ii, jj, kk) = g.aw[c]; id(ii, jj, kk) = g.ap[c];
+        }
+        for (int q = tid; q < nhalo; q += nth) {
+            const int ii = q % HI, r = q / HI, jj = r % HJ, kk = r / HJ;
+            ph(ii - 1, jj - 1, kk - 1) =
+                phi[(long long)g0 + (ii - 1) + (long long)(jj - 1) * gsj + (kk - 1) * gsk];
+        }
+        ae_src = nullptr; aw_src = nullptr; ap_src = nullptr;
+        __syncthreads();
+    } else {
+        at = {g.at + g0, gsj, gsk}; ab = {g.ab + g0, gsj, gsk};
+        an = {g.an + g0, gsj, gsk}; as = {g.as + g0, gsj, gsk};
+        su = {g.su + g0, gsj, gsk}; pr = {g.pr + g0, gsj, gsk};
+        cf = {g.cf + g0, gsj, gsk}; id = {g.iden + g0, gsj, gsk};
+        qr = {scratch + g0, gsj, gsk};
+        ph = {phi + g0, gsj, gsk};
+        ae_src = g.ae + g0; aw_src = g.aw + g0; ap_src = g.ap + g0;
     }
+    // factorisation, one thread per line (pr = ae/den, cf = aw/den, id = 1/den),
+    // with solveLiquidDomain's guard on |den| (:2438-2439)
+    for (int l = tid; l < NJ * NK; l += nth) {
+        const int jj = l % NJ, kk = l / NJ;
+        T prv = T(0);
+        for (int ii = 0; ii < NI; ++ii) {
+            const long long o = ii + (long long)jj * gsj + kk * gsk;
+            const T apv = fits ? id(ii, jj, kk) : ap_src[o];
+            const T aev = fits ? pr(ii, jj, kk) : ae_src[o];
+            const T awv = fits ? cf(ii, jj, kk) : aw_src[o];
+            T den = apv - awv * prv;
+            if (fabs(den) <= T(1e-12)) den += T(kSmall);
+            const T iv = T(1) / den;
+            const T pv = aev * iv;
+            pr(ii, jj, kk) = pv;
+            cf(ii, jj, kk) = awv * iv;
+            id(ii, jj, kk) = iv;
+            prv = pv;
+        }
+    }
+    __syncthreads();
+    // 4 sweeps x 2 colours; a line of one colour reads only rows of the other.
+    // Short lines (the usual melt-pool box): one thread per line, sequential
+    // recurrences over per-line base pointers.  Long lines: one warp per line,
+    // warp scans of affine maps over per-lane chunks.
+    const int half = (NJ + 1) / 2;
+    if (NI <= 48) {
+        for (int sweep = 0; sweep < 4; ++sweep)
+            for (int color = 0; color < 2; ++color) {
+                for (int l = tid; l < half * NK; l += nth) {
+                    const int kk = l / half, r = l - kk * half;
+                    const int k = b.k0 + kk;
+                    const int jpar = ((color - k - b.j0) % 2 + 2) % 2;
+                    const int jj = jpar + 2 * r;
+                    if (jj >= NJ) continue;
+                    const T *pat = &at(0, jj, kk), *pab = &ab(0, jj, kk), *pan = &an(0, jj, kk),
+                            *pas = &as(0, jj, kk), *psu = &su(0, jj, kk), *pcf = &cf(0, jj, kk),
+                            *pid = &id(0, jj, kk), *ppr = &pr(0, jj, kk);
+                    T *pqr = &qr(0, jj, kk), *pph = &ph(0, jj, kk);
+                    const T *pt = &ph(0, jj, kk + 1), *pb = &ph(0, jj, kk - 1), *pn = &ph(0, jj + 1, kk),
+                            *ps = &ph(0, jj - 1, kk);
+                    T q = pph[-1];
+                    for (int ii = 0; ii < NI; ++ii) {
+                        const T d = pat[ii] * pt[ii] + pab[ii] * pb[ii] + pan[ii] * pn[ii] + pas[ii] * ps[ii] + psu[ii];
+                        q = pcf[ii] * q + d * pid[ii];
+                        pqr[ii] = q;
+                    }
+                    T x = pph[NI];
+                    for (int ii = NI - 1; ii >= 0; --ii) {
+                        x = ppr[ii] * x + pqr[ii];
+                        pph[ii] = x;
+                    }
+                }
+                __syncthreads();
+            }
+    } else {
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
+        const int L = (NI + 31) >> 5;
+        const int a = min(lane * L, NI), e = min(a + L, NI);
+        for (int sweep = 0; sweep < 4; ++sweep)
+            for (int color = 0; color < 2; ++color) {
+                for (int l = warp; l < half * NK; l += nwarp) {
+                    const int kk = l / half, r = l - kk * half;
+                    const int k = b.k0 + kk;
+                    const int jpar = ((color - k - b.j0) % 2 + 2) % 2;
+                    const int jj = jpar + 2 * r;
+                    if (jj >= NJ) continue;  // warp-uniform
+                    // right-hand side over this lane's chunk, and its forward map
+                    T A = T(1), B = T(0);
+                    for (int ii = a; ii < e; ++ii) {
+                        const T d = at(ii, jj, kk) * ph(ii, jj, kk + 1) + ab(ii, jj, kk) * ph(ii, jj, kk - 1) +
+                                    an(ii, jj, kk) * ph(ii, jj + 1, kk) + as(ii, jj, kk) * ph(ii, jj - 1, kk) +
+                                    su(ii, jj, kk);
+                        const T ev = d * id(ii, jj, kk), c = cf(ii, jj, kk);
+                        qr(ii, jj, kk) = ev;
+                        B = c * B + ev;
+                        A = c * A;
+                    }
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const T A2 = __shfl_up_sync(0xffffffffu, A, o), B2 = __shfl_up_sync(0xffffffffu, B, o);
+                        if (lane >= o) { B = A * B2 + B; A = A * A2; }
+                    }
+                    T Ae = __shfl_up_sync(0xffffffffu, A, 1), Be = __shfl_up_sync(0xffffffffu, B, 1);
+                    if (lane == 0) { Ae = T(1); Be = T(0); }
+                    T q = Ae * ph(-1, jj, kk) + Be;
+                    for (int ii = a; ii < e; ++ii) {
+                        q = cf(ii, jj, kk) * q + qr(ii, jj, kk);
+                        qr(ii, jj, kk) = q;
+                    }
+                    A = T(1);
+                    B = T(0);
+                    for (int ii = e - 1; ii >= a; --ii) {
+                        const T pv = pr(ii, jj, kk);
+                        B = pv * B + qr(ii, jj, kk);
+                        A = pv * A;
+                    }
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const T A2 = __shfl_down_sync(0xffffffffu, A, o), B2 = __shfl_down_sync(0xffffffffu, B, o);
+                        if (lane + o < 32) { B = A * B2 + B; A = A * A2; }
+                    }
+                    Ae = __shfl_down_sync(0xffffffffu, A, 1);
+                    Be = __shfl_down_sync(0xffffffffu, B, 1);
+                    if (lane == 31) { Ae = T(1); Be = T(0); }
+                    T x = Ae * ph(NI, jj, kk) + Be;
+                    for (int ii = e - 1; ii >= a; --ii) {
+                        x = pr(ii, jj, kk) * x + qr(ii, jj, kk);
+                        ph(ii, jj, kk) = x;
+                    }
+                    __syncwarp();
+                }
+                __syncthreads();
+            }
+    }
+    if (fits) {
+        for (int q = tid; q < ncell; q += nth) {
+            const int ii = q % NI, r = q / NI, jj = r % NJ, kk = r / NJ;
+            phi[g0 + ii + (size_t)jj * gsj + (size_t)kk * gsk] = ph(ii, jj, kk);
+        }
+        __syncthreads();
+    }
+}
+
+// Phase helpers of the one-CTA kernels.
+template <typename T>
+__device__ __forceinline__ void small_bc(const Params &p, const Fields<T> &g, Status *st, const Box &b,
+                                         int ivar, double *red_umax, double *sh)
+{
+    int ntop;
+    const int nbc = mom_bc_items(p, st, b, ivar, ntop);
+    double um = 0.0;
+    for (int q = threadIdx.x; q < nbc; q += blockDim.x) um = maxd(um, mom_bc_item<T>(p, g, st, b, ivar, q, ntop));
+    if (ivar == 1) {
+        um = cta_max(um, sh);
+        if (threadIdx.x == 0) red_umax[R_UMAX] = um;  // entry 0 of the umax region
+    }
+}
+
+// cleanVelocities + applyBCs(1): one CTA.
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1) mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax)
+{
+    __shared__ double sh[32];
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b)) return;
+    for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        clean_cell<T>(p, g, i, j, k);
+    }
+    __syncthreads();
+    small_bc<T>(p, g, st, b, 1, red_umax, sh);
+}
+
+// Line solve of equation ivar (1..3) on the box, then applyBCs(ivar + 1): one CTA.
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems, double *red_umax)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double sh[32];
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b)) return;
+    T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : g.wvel;
+    solve_box_small<T>(p, g, b, phi, reinterpret_cast<T *>(smraw), smem_elems, scratch);
+    small_bc<T>(p, g, st, b, ivar + 1, red_umax, sh);
+}
+
+// Line solve of p', correctPressure and the residual normalisation: one CTA.
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double scratch_r[40];
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b)) return;
+    solve_box_small<T>(p, g, b, g.pp, reinterpret_cast<T *>(smraw), smem_elems, scratch);
+    for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_velocity_cell<T>(p, g, i, j, k);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_pressure_cell<T>(p, g, i, j, k);
+    }
+    __syncthreads();
+    mom_finalize_body(p, st, red, nb, 1, scratch_r);
+}
+
+// Largest box (cells) the small-box path keeps in shared memory, with room
+// for the halo of a thin box.
+template <typename T> int mom_small_capacity(const Inst<T> &I) { return (int)(I.mom_small_smem / sizeof(T) / 12); }
+
+template <typename T> void setup_mom_small(Inst<T> &I)
+{
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    size_t bytes = std::min<size_t>((size_t)std::max(optin, 48 * 1024) - 1024, 200 * 1024);
+    bytes = bytes / 16 * 16;
+    cudaFuncSetAttribute(mom_small_mid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(mom_small_post_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    I.mom_small_smem = bytes;
 }
 
 // ---------------------------------------------------------------------------
 // launcher: the whole momentum chain of one outer iteration
 // ---------------------------------------------------------------------------
-template <typename T> void launch_momentum(Inst<T> &I)
+template <typename T> void launch_momentum(Inst<T> &I, bool small)
 {
     const int nb = I.nb_mom;
     const size_t region = (size_t)nb * R_NSLOTS;
+    if (small) {
+        // assembly on the whole GPU, everything latency-bound in one CTA between
+        const int se = (int)(I.mom_small_smem / sizeof(T));
+        double *red_umax = I.red_mom + 4 * region;
+        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax);
+        for (int ivar = 1; ivar <= 3; ++ivar) {
+            mom_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * region);
+            mom_small_mid_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
+                I.p, I.g, ivar, I.mom_scratch, se, red_umax);
+        }
+        pp_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * region);
+        mom_small_post_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
+            I.p, I.g, I.mom_scratch, se, I.red_mom, nb);
+        return;
+    }
     launch_box_tickets<T>(I);
     clean_velocities_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
     for (int ivar = 1; ivar <= 4; ++ivar) {
@@ -506,7 +886,11 @@ template <typename T> void launch_momentum(Inst<T> &I)
     mom_finalize_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_mom, nb);
 }
 
-template void launch_momentum<double>(Inst<double> &);
-template void launch_momentum<float>(Inst<float> &);
+template void launch_momentum<double>(Inst<double> &, bool);
+template void launch_momentum<float>(Inst<float> &, bool);
+template int mom_small_capacity<double>(const Inst<double> &);
+template int mom_small_capacity<float>(const Inst<float> &);
+template void setup_mom_small<double>(Inst<double> &);
+template void setup_mom_small<float>(Inst<float> &);
 
 }  // namespace amcfd

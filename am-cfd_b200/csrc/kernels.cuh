@@ -87,6 +87,8 @@ struct Inst {
     int *flags_mom = nullptr;
     int max_lines = 0;        // (nj-2)*(nk-2)
     AsmMaps asm_maps[2];      // by property parity
+    T *mom_scratch = nullptr; // one field: line-solve scratch of the small-box momentum path
+    size_t mom_small_smem = 0;  // its dynamic shared memory
     const T *asm_diff_a = nullptr;  // diff_cur at parity 0
 };
 
@@ -107,6 +109,8 @@ template <typename T> void launch_box_factor(Inst<T> &I);
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
 template <typename T> void launch_box_tickets(Inst<T> &I);
 // momentum (k_momentum.cu)
-template <typename T> void launch_momentum(Inst<T> &I);
+template <typename T> void launch_momentum(Inst<T> &I, bool small);
+template <typename T> int mom_small_capacity(const Inst<T> &I);
+template <typename T> void setup_mom_small(Inst<T> &I);
 
 }  // namespace amcfd

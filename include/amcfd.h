@@ -120,7 +120,9 @@ typedef struct amcfd_options {
     int precision;       /* AMCFD_PREC_* */
     int use_graphs;      /* capture the fixed-shape part of an outer iteration */
     int check_finite;    /* fail with AMCFD_E_NONFINITE when a reduction is not finite */
-    int reserved[8];
+    int no_small_box;    /* 1: never run the momentum chain of a small melt-pool box in one
+                            CTA (red-black order only; 0 lets the solver choose) */
+    int reserved[7];
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;

@@ -173,3 +173,30 @@ def test_graph_replay_bit_identical(prec, order, deckdir):
             assert np.array_equal(a.get(f), b.get(f)), (s, f)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_small_box_momentum_matches_grid_path(prec, deckdir):
+    """Red-black runs with the one-CTA momentum chain (small melt-pool box held
+    in shared memory) stay within 1e-6 (FP64) / 1e-3 (FP32) relative L2 of the
+    same runs with the multi-kernel chain, with the same iteration counts in FP64."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.small("smallbox", steps=4, power=350.0).write(deckdir))
+    a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, small_box=0)
+    b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, small_box=1)
+    tol = 1e-6 if prec == 0 else 1e-3
+    saw_box = False
+    for s in range(4):
+        ra, rb = a.step(), b.step()
+        saw_box |= rb["momentum_cells"] > 0
+        if prec == 0:
+            assert ra["niter"] == rb["niter"], (s, ra["niter"], rb["niter"])
+        for f in ("temp", "uvel", "vvel", "wvel", "pressure"):
+            x, y = b.get(f), a.get(f)
+            if np.linalg.norm(y) > 0:
+                assert rel_l2(x, y) < tol, (s, f, rel_l2(x, y))
+    assert saw_box
+    assert b.launches < a.launches
+    a.close()
+    b.close()
