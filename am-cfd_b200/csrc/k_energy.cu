@@ -138,6 +138,99 @@ __global__ void __launch_bounds__(256) bc_reduce_kernel(Params p, Fields<T> g)
     }
 }
 
+// 1-D TDMA of the block correction (enhanceConvergenceSpeed(5),
+// CFDSolverManager.cpp:2334-2349) for cells i0..i1 by one warp:
+//   den_i = bl_i - blm_i pib_{i-1},  pib_i = blp_i / den_i,
+//   qib_i = (blc_i + blm_i qib_{i-1}) / den_i,  delphi_i = pib_i delphi_{i+1} + qib_i,
+// with pib_{i0-1} = qib_{i0-1} = 0 and delphi_{i1+1} = 0.  Each lane owns a
+// contiguous chunk.  pib follows x -> blp / (bl - blm x), a Moebius map: the
+// chunks' 2x2 matrices (rescaled as they are multiplied; the map ignores
+// scale) are combined by a warp scan to give each chunk its entry value, and
+// the chunk then runs the reference recurrence.  qib and delphi are affine in
+// their predecessor and use warp scans of affine maps.  All in FP64.  On
+// return bl holds den, blm holds pib and blp holds qib.
+__device__ __forceinline__ double moebius_scale(double a, double b, double c, double d)
+{
+    const double mx = fmax(fmax(fabs(a), fabs(b)), fmax(fabs(c), fabs(d)));
+    return mx > 0.0 ? 1.0 / mx : 1.0;
+}
+
+__device__ void block_tdma_warp(double *bl, double *blp, double *blm, const double *blc, int i0, int i1,
+                                double *delphi)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = i1 - i0 + 1;
+    if (n <= 0) return;
+    const int L = (n + 31) >> 5;
+    const int a = i0 + min(lane * L, n), e = i0 + min(lane * L + L, n);
+    // chunk product of the Moebius matrices [[0, blp], [-blm, bl]] (later cells on the left)
+    double m00 = 1.0, m01 = 0.0, m10 = 0.0, m11 = 1.0;
+    for (int i = a; i < e; ++i) {
+        const double n00 = blp[i] * m10, n01 = blp[i] * m11;
+        const double n10 = -blm[i] * m00 + bl[i] * m10, n11 = -blm[i] * m01 + bl[i] * m11;
+        const double sc = moebius_scale(n00, n01, n10, n11);
+        m00 = n00 * sc; m01 = n01 * sc; m10 = n10 * sc; m11 = n11 * sc;
+    }
+    // inclusive scan: M_lane <- M_lane * M_{lane-o}
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double p00 = __shfl_up_sync(0xffffffffu, m00, o), p01 = __shfl_up_sync(0xffffffffu, m01, o);
+        const double p10 = __shfl_up_sync(0xffffffffu, m10, o), p11 = __shfl_up_sync(0xffffffffu, m11, o);
+        if (lane >= o) {
+            const double n00 = m00 * p00 + m01 * p10, n01 = m00 * p01 + m01 * p11;
+            const double n10 = m10 * p00 + m11 * p10, n11 = m10 * p01 + m11 * p11;
+            const double sc = moebius_scale(n00, n01, n10, n11);
+            m00 = n00 * sc; m01 = n01 * sc; m10 = n10 * sc; m11 = n11 * sc;
+        }
+    }
+    // entry value pib_{a-1}: the exclusive prefix applied to x = 0
+    double e01 = __shfl_up_sync(0xffffffffu, m01, 1), e11 = __shfl_up_sync(0xffffffffu, m11, 1);
+    double pib = (lane == 0) ? 0.0 : e01 / e11;
+    // the chunk runs the reference recurrence for den and pib; qib's affine maps
+    double A = 1.0, B = 0.0;
+    for (int i = a; i < e; ++i) {
+        const double den = bl[i] - blm[i] * pib;
+        const double pv = blp[i] / den;
+        const double ca = blm[i] / den, cb = blc[i] / den;  // qib_i = ca qib_{i-1} + cb
+        bl[i] = den;
+        blm[i] = pv;
+        blp[i] = cb;  // temporarily the affine offset
+        pib = pv;
+        B = ca * B + cb;
+        A = ca * A;
+        delphi[i] = ca;  // temporarily the affine slope
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double A2 = __shfl_up_sync(0xffffffffu, A, o), B2 = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) { B = A * B2 + B; A = A * A2; }
+    }
+    double Be = __shfl_up_sync(0xffffffffu, B, 1);
+    double q = (lane == 0) ? 0.0 : Be;  // qib_{a-1} (qib_{i0-1} = 0)
+    for (int i = a; i < e; ++i) {
+        q = delphi[i] * q + blp[i];
+        blp[i] = q;
+    }
+    // back substitution delphi_i = pib_i delphi_{i+1} + qib_i, delphi_{i1+1} = 0
+    A = 1.0;
+    B = 0.0;
+    for (int i = e - 1; i >= a; --i) {
+        B = blm[i] * B + blp[i];
+        A = blm[i] * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double A2 = __shfl_down_sync(0xffffffffu, A, o), B2 = __shfl_down_sync(0xffffffffu, B, o);
+        if (lane + o < 32) { B = A * B2 + B; A = A * A2; }
+    }
+    Be = __shfl_down_sync(0xffffffffu, B, 1);
+    double d = (lane == 31) ? 0.0 : Be;
+    for (int i = e - 1; i >= a; --i) {
+        d = blm[i] * d + blp[i];
+        delphi[i] = d;
+    }
+}
+
 template <typename T>
 __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, int nblk_asm,
                                      int check_finite)
@@ -163,31 +256,9 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
         double resorh = tot[0] / (tot[1] + kSmall);
         st->resorh = resorh;
         if (check_finite && !isfinite(resorh)) st->nonfinite = 1;
-        // 1-D TDMA in i
-        double *delphi = gd.delphi;
-        double pib_prev = blp[1] / bl[1];
-        double qib_prev = blc[1] / bl[1];
-        // pib/qib stored in bl/blm scratch (bl[i] no longer needed after use)
-        blm[1] = pib_prev;
-        blp[1] = qib_prev;
-        for (int i = 2; i < nim1; i++) {
-            double denom = bl[i] - blm[i] * pib_prev;
-            double pib = blp[i] / denom;
-            double qib = (blc[i] + blm[i] * qib_prev) / denom;
-            blm[i] = pib;
-            blp[i] = qib;
-            pib_prev = pib;
-            qib_prev = qib;
-        }
-        double d = blp[nim2];
-        delphi[nim2] = d;
-        for (int i = nim2 - 1; i > 0; i--) {
-            d = blm[i] * d + blp[i];
-            delphi[i] = d;
-        }
     }
+    if (threadIdx.x < 32) block_tdma_warp(bl, blp, blm, blc, 1, nim2, gd.delphi);
 }
-
 // ---------------------------------------------------------------------------
 // convertEnthalpyToTemp (CFDSolverManager.cpp:2531-2571), fused with the
 // peak-temperature maximum (BoundCondManager.cpp:301) and the reductions of
