@@ -125,10 +125,6 @@ __device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int i
 }
 
 // ---------------------------------------------------------------------------
-// One x-line solved by one warp from its staged rows.  `row` is the offset of
-// node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
-// ends; sl holds the line from cell ib on.
-// ---------------------------------------------------------------------------
 // Thomas recurrences of one line by one warp, from shared-memory rows indexed
 // by i - i0: e (right-hand side / den on entry, the solution on exit), cf and
 // pr.  Each lane owns a contiguous chunk; the chunks are chained by warp scans
@@ -195,6 +191,9 @@ __device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T 
     for (int i = lane; i < n; i += 32) phi[row + i0 + i] = se[i];
 }
 
+// One x-line solved by one warp from its staged rows.  `row` is the offset of
+// node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
+// ends; sl holds the line from cell ib on.
 template <typename T, bool COHERENT>
 __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
                                              size_t sj, size_t sk, T *sl, int nmax)
