@@ -37,9 +37,11 @@ METRIC = "sim-ms/wall-s"
 # Algorithmic words per interior cell per outer iteration, by kernel family
 # (energy path; the contract total is 92 words per cell per outer iteration).
 WORDS = {"energy_assemble": 40, "factor": 2, "energy_sweeps": 40, "h2t_meltpool": 10}
-# DRAM traffic per interior cell per launch measured with ncu on the 120x60x40
-# deck, scaled by cell count (profiles/*.md).
-TRAFFIC_PER_CELL = {}
+# DRAM bytes per interior cell per launch (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum, one capture of each kernel on the 400x200x100 deck,
+# FP32 bulk); the line reports them scaled by the cell count.
+TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 85.5, "energy_sweeps:fp32:redblack": 20.3,
+                    "h2t_meltpool:fp32:redblack": 28.6, "factor:fp32:redblack": 27.8}
 
 
 def _peaks():
