@@ -117,6 +117,17 @@ def lib() -> C.CDLL:
             L.amcfd_kernel_launches.argtypes = [VP]
             L.amcfd_kernel_launches.restype = C.c_longlong
             L.amcfd_run_batch.argtypes = [P(VP), _I, _I, _I, P(AmcfdReport), P(_I)]
+            L.amcfd_net_param_count.restype = C.c_size_t
+            L.amcfd_net_create.argtypes = [_I, C.c_ulonglong, P(VP)]
+            L.amcfd_net_destroy.argtypes = [VP]
+            L.amcfd_net_last_error.argtypes = [VP]
+            L.amcfd_net_last_error.restype = C.c_char_p
+            for f in ("get_params", "get_grads"):
+                getattr(L, "amcfd_net_" + f).argtypes = [VP, P(C.c_float), C.c_size_t]
+            L.amcfd_net_set_params.argtypes = [VP, P(C.c_float), C.c_size_t]
+            L.amcfd_net_forward.argtypes = [VP, VP, _I, _I, _I, VP]
+            L.amcfd_net_backward.argtypes = [VP, VP, P(_D)]
+            L.amcfd_net_adam.argtypes = [VP, C.c_float]
         _lib = L
     return _lib
 
@@ -151,6 +162,59 @@ class Deck:
     def close(self):
         if self._h:
             lib().amcfd_deck_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Net:
+    """The warm-start network (amcfd_net_*).  Device arrays are passed as raw
+    pointers (e.g. torch.Tensor.data_ptr()) of FP32 channels-last data."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self._h = C.c_void_p()
+        rc = lib().amcfd_net_create(device, seed, C.byref(self._h))
+        if rc != 0:
+            raise AmcfdError(rc, lib().amcfd_net_last_error(self._h).decode() if self._h else "create failed")
+        self.nparams = int(lib().amcfd_net_param_count())
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise AmcfdError(rc, lib().amcfd_net_last_error(self._h).decode())
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.nparams, dtype=np.float32)
+        self._check(lib().amcfd_net_get_params(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), self.nparams))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        self._check(lib().amcfd_net_set_params(self._h, a.ctypes.data_as(C.POINTER(C.c_float)), self.nparams))
+
+    def grads(self) -> np.ndarray:
+        out = np.empty(self.nparams, dtype=np.float32)
+        self._check(lib().amcfd_net_get_grads(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), self.nparams))
+        return out
+
+    def forward(self, feat_ptr: int, dims, y_ptr: int = 0):
+        ni, nj, nk = dims
+        self._check(lib().amcfd_net_forward(self._h, feat_ptr, ni, nj, nk, y_ptr or None))
+
+    def backward(self, target_ptr: int) -> float:
+        loss = C.c_double()
+        self._check(lib().amcfd_net_backward(self._h, target_ptr, C.byref(loss)))
+        return loss.value
+
+    def adam(self, lr: float):
+        self._check(lib().amcfd_net_adam(self._h, lr))
+
+    def close(self):
+        if self._h:
+            lib().amcfd_net_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

@@ -1,0 +1,735 @@
+// Learned warm start: a 4-layer 3x3x3 convolutional network on the solver grid
+// (no counterpart in the reference; it only supplies an initial guess, the
+// reference's own outer loop still decides convergence).
+//
+//   features (16 ch, 9 used) -> conv 16->32, ReLU -> conv 32->32, ReLU
+//                            -> conv 32->32, ReLU -> conv 32->16 (2 used)
+//
+// Activations are BF16, channels-last [cell][C] over the full node grid
+// (cell = (k*nj + j)*ni + i); boundary nodes are held at zero after every
+// layer, which makes each convolution a zero-padded convolution over the
+// interior.  Weights are FP32 masters [tap][cout][cin] (tap = 9(dk+1) +
+// 3(dj+1) + (di+1)) packed to BF16 for the tensor cores.
+//
+// Convolutions are implicit GEMMs on the 5th-generation tensor cores: an
+// output tile is 128 consecutive cells (M = 128), N = output channels, and the
+// reduction runs over 27 taps x input channels in K = 16 slices
+// (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in tensor memory).
+// A CTA stages the nine (dk, dj) row groups of 136 cells that its tile needs
+// once in shared memory; the three di taps of a group are the same rows
+// shifted by one, i.e. operand descriptors 16 bytes apart.  The whole weight
+// set of the layer stays in shared memory.  Tiles are double-buffered: the
+// gather of tile q+1 and the epilogue of tile q overlap the MMAs.  The same
+// kernel computes input gradients (transposed, tap-reversed weights) with the
+// ReLU derivative applied in the epilogue.  Weight gradients are reduced on
+// the CUDA cores (FP32).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "amcfd.h"
+#include "async.cuh"
+
+namespace amcfd {
+namespace cnn {
+
+constexpr int kThreads = 256;
+constexpr int kM = 128;  // cells per tile
+constexpr int kR = 136;  // rows per (dk, dj) group: 128 + 2 halo, rounded up to 8
+constexpr int kG = 9;    // (dk, dj) groups
+constexpr int kLayers = 4;
+constexpr int kCin[kLayers] = {16, 32, 32, 32};
+constexpr int kCout[kLayers] = {32, 32, 32, 16};
+constexpr int kFeat = 9;  // real input channels
+constexpr int kOut = 2;   // real output channels
+
+template <int CIN, int COUT> struct ConvSmem {
+    static constexpr int A_BYTES = (CIN / 8) * kG * kR * 16;
+    static constexpr int B_BYTES = 27 * CIN * COUT * 2;
+    static constexpr size_t BYTES = 2 * (size_t)A_BYTES + B_BYTES + 64 + 128;
+};
+
+struct ConvArgs {
+    const __nv_bfloat16 *x;   // [ncell][CIN]
+    const __nv_bfloat16 *w;   // packed [27][CIN/8][COUT][8]
+    const float *bias;        // [COUT] or null
+    const __nv_bfloat16 *gate;  // [ncell][COUT]: multiply by (gate > 0), or null
+    __nv_bfloat16 *y;         // [ncell][COUT]
+    float *y32;               // [ncell][n32] FP32 copy of the first n32 channels, or null
+    int n32;
+    int relu;
+    int ni, nj, nk;
+    long long ncell;
+    int *err;
+};
+
+// ---- tensor-core plumbing (PTX) ------------------------------------------------
+// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows
+// x 16 bytes stored as 128 contiguous bytes; lbo = byte distance between the two
+// K-adjacent core matrices of one K=16 slice, sbo = between 8-row groups.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, no swizzle
+}
+// Instruction descriptor, kind::f16: D F32, A and B BF16, both K-major, M = 128.
+template <int N> __host__ __device__ constexpr uint32_t idesc_bf16()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n"
+        ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+template <int N> __device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[N]);
+template <> __device__ __forceinline__ void tmem_ld<16>(uint32_t t, uint32_t (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                   "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(t));
+}
+template <> __device__ __forceinline__ void tmem_ld<32>(uint32_t t, uint32_t (&r)[32])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                   "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                   "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+                   "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+                   "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+                   "=r"(r[31])
+                 : "r"(t));
+}
+
+__device__ __forceinline__ bool interior_cell(long long c, int ni, int nj, int nk)
+{
+    const long long plane = (long long)ni * nj;
+    const int k = (int)(c / plane);
+    const long long r = c - (long long)k * plane;
+    const int j = (int)(r / ni), i = (int)(r - (long long)j * ni);
+    return i >= 1 && i <= ni - 2 && j >= 1 && j <= nj - 2 && k >= 1 && k <= nk - 2;
+}
+
+// Nine (dk, dj) groups of kR consecutive cells starting one cell before the
+// tile, stored chunk-major: element (row r, channel c) of group g at byte
+// ((c/8 * kG + g) * kR + r) * 16 + (c%8) * 2.
+template <int CIN>
+__device__ __forceinline__ void gather_tile(const __nv_bfloat16 *x, long long ncell, int ni, int nj,
+                                            long long c0, unsigned char *A)
+{
+    constexpr int KC = CIN / 8;
+    const long long plane = (long long)ni * nj;
+    for (int idx = threadIdx.x; idx < kG * kR * KC; idx += blockDim.x) {
+        const int r = idx % kR, rest = idx / kR, g = rest % kG, kc = rest / kG;
+        const int dk = g / 3 - 1, dj = g % 3 - 1;
+        const long long s = c0 - 1 + r + dk * plane + (long long)dj * ni;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (s >= 0 && s < ncell) v = *reinterpret_cast<const uint4 *>(x + s * CIN + kc * 8);
+        *reinterpret_cast<uint4 *>(A + ((size_t)(kc * kG + g) * kR + r) * 16) = v;
+    }
+}
+
+template <int CIN, int COUT>
+__device__ __forceinline__ void issue_tile(uint32_t a_base, uint32_t b_base, uint32_t tmem_d)
+{
+    constexpr uint32_t idesc = idesc_bf16<COUT>();
+    constexpr uint32_t lbo_a = kG * kR * 16, lbo_b = COUT * 16;
+    bool first = true;
+    for (int g = 0; g < kG; ++g)
+        for (int di = 0; di < 3; ++di) {
+            const int t = g * 3 + di;
+#pragma unroll
+            for (int s = 0; s < CIN / 16; ++s) {
+                const uint32_t a = a_base + (uint32_t)(((2 * s * kG + g) * kR + di) * 16);
+                const uint32_t b = b_base + (uint32_t)(t * CIN * COUT * 2 + 2 * s * COUT * 16);
+                mma_bf16(tmem_d, smem_desc(a, lbo_a, 128), smem_desc(b, lbo_b, 128), idesc, first ? 0u : 1u);
+                first = false;
+            }
+        }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads, 1) conv_tc_kernel(ConvArgs args)
+{
+    using S = ConvSmem<CIN, COUT>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    unsigned char *base = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
+    unsigned char *A0 = base, *A1 = base + S::A_BYTES, *Bs = base + 2 * S::A_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + S::B_BYTES);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr uint32_t kCols = COUT * 2 < 32 ? 32 : COUT * 2;  // two accumulators
+    const long long ntiles = (args.ncell + kM - 1) / kM;
+
+    if (tid == 0) {
+        mbar_init(&bar[0]);
+        mbar_init(&bar[1]);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tslot)), "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // weights: whole layer into shared memory
+    for (int q = tid; q < S::B_BYTES / 16; q += blockDim.x)
+        reinterpret_cast<uint4 *>(Bs)[q] = reinterpret_cast<const uint4 *>(args.w)[q];
+    fence_proxy_async();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tbase = *tslot;
+    const uint32_t a_addr[2] = {smem_u32(A0), smem_u32(A1)};
+    const uint32_t b_addr = smem_u32(Bs);
+    unsigned char *Abuf[2] = {A0, A1};
+
+    long long q = blockIdx.x;
+    if (q < ntiles) gather_tile<CIN>(args.x, args.ncell, args.ni, args.nj, q * kM, A0);
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0 && q < ntiles) {
+        tc_after_sync();
+        issue_tile<CIN, COUT>(a_addr[0], b_addr, tbase);
+        mma_commit(&bar[0]);
+    }
+    bool ok = true;
+    int it = 0;
+    for (; q < ntiles; q += gridDim.x, ++it) {
+        const long long qn = q + gridDim.x;
+        const int b = it & 1, bn = b ^ 1;
+        if (qn < ntiles) gather_tile<CIN>(args.x, args.ncell, args.ni, args.nj, qn * kM, Abuf[bn]);
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0 && qn < ntiles) {
+            tc_after_sync();
+            issue_tile<CIN, COUT>(a_addr[bn], b_addr, tbase + (uint32_t)(bn * COUT));
+            mma_commit(&bar[bn]);
+        }
+        ok = mbar_try(&bar[b], (uint32_t)((it >> 1) & 1), kSpinLimit);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicExch(args.err, AMCFD_E_TIMEOUT);
+                if (qn < ntiles) mbar_try(&bar[bn], (uint32_t)(((it + 1) >> 1) & 1), kSpinLimit);
+            }
+            break;
+        }
+        tc_after_sync();
+        if (warp < 4) {
+            uint32_t r[COUT];
+            tmem_ld<COUT>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(b * COUT), r);
+            tmem_wait_ld();
+            const long long cell = q * kM + 32 * warp + lane;
+            if (cell < args.ncell) {
+                const bool in = interior_cell(cell, args.ni, args.nj, args.nk);
+                float v[COUT];
+#pragma unroll
+                for (int c = 0; c < COUT; ++c) {
+                    float x = __uint_as_float(r[c]);
+                    if (args.bias) x += args.bias[c];
+                    if (args.relu) x = fmaxf(x, 0.f);
+                    v[c] = in ? x : 0.f;
+                }
+                if (args.gate) {
+                    const __nv_bfloat16 *gp = args.gate + cell * COUT;
+#pragma unroll
+                    for (int c = 0; c < COUT; ++c)
+                        if (!(__bfloat162float(gp[c]) > 0.f)) v[c] = 0.f;
+                }
+                __nv_bfloat16 *yp = args.y + cell * COUT;
+#pragma unroll
+                for (int c = 0; c < COUT; c += 8) {
+                    __nv_bfloat162 h[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[c + 2 * e], v[c + 2 * e + 1]);
+                    *reinterpret_cast<uint4 *>(yp + c) = *reinterpret_cast<uint4 *>(h);
+                }
+                if (args.y32)
+                    for (int c = 0; c < args.n32; ++c) args.y32[cell * args.n32 + c] = v[c];
+            }
+        }
+        tc_before_sync();
+        __syncthreads();
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kCols) : "memory");
+}
+
+// ---- weight packing, gradients, loss, optimiser (CUDA cores) -----------------------
+// forward operand B[t][n = cout][k = cin]: packed [t][cin/8][cout][8]
+__global__ void pack_fwd_kernel(const float *w, __nv_bfloat16 *wp, int cin, int cout)
+{
+    const int n = 27 * cin * cout;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int e = q % 8, r = q / 8, nn = r % cout, r2 = r / cout, kc = r2 % (cin / 8), t = r2 / (cin / 8);
+        wp[q] = __float2bfloat16_rn(w[((size_t)t * cout + nn) * cin + kc * 8 + e]);
+    }
+}
+// input-gradient operand B'[t'][n = cin][k = cout] = W[26 - t'][cout][cin]: packed [t'][cout/8][cin][8]
+__global__ void pack_bwd_kernel(const float *w, __nv_bfloat16 *wp, int cin, int cout)
+{
+    const int n = 27 * cin * cout;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const int e = q % 8, r = q / 8, nn = r % cin, r2 = r / cin, kc = r2 % (cout / 8), t = r2 / (cout / 8);
+        wp[q] = __float2bfloat16_rn(w[((size_t)(26 - t) * cout + kc * 8 + e) * cin + nn]);
+    }
+}
+
+// dW[t][cout][cin] = sum over interior cells c of dz[c][cout] * x[c + off(t)][cin],
+// db[cout] = sum of dz[c][cout]; per-CTA partials, reduced in a fixed order.
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kThreads, 1) wgrad_kernel(const __nv_bfloat16 *x, const __nv_bfloat16 *dz,
+                                                           long long ncell, int ni, int nj, float *part)
+{
+    constexpr int NW = 27 * COUT * CIN;
+    constexpr int PER = (NW + kThreads - 1) / kThreads;
+    constexpr int TC = 32;  // cells per step
+    __shared__ float sx[kG][TC + 2][CIN];
+    __shared__ float sdz[TC][COUT];
+    const long long plane = (long long)ni * nj;
+    float acc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) acc[q] = 0.f;
+    float bacc = 0.f;
+    const long long nsteps = (ncell + TC - 1) / TC;
+    for (long long st = blockIdx.x; st < nsteps; st += gridDim.x) {
+        const long long c0 = st * TC;
+        for (int idx = threadIdx.x; idx < kG * (TC + 2) * CIN; idx += blockDim.x) {
+            const int cc = idx % CIN, rest = idx / CIN, r = rest % (TC + 2), g = rest / (TC + 2);
+            const int dk = g / 3 - 1, dj = g % 3 - 1;
+            const long long s = c0 - 1 + r + dk * plane + (long long)dj * ni;
+            sx[g][r][cc] = (s >= 0 && s < ncell) ? __bfloat162float(x[s * CIN + cc]) : 0.f;
+        }
+        for (int idx = threadIdx.x; idx < TC * COUT; idx += blockDim.x) {
+            const int cc = idx % COUT, r = idx / COUT;
+            const long long c = c0 + r;
+            sdz[r][cc] = (c < ncell) ? __bfloat162float(dz[c * COUT + cc]) : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+            const int o = threadIdx.x + q * kThreads;
+            if (o < NW) {
+                const int ci = o % CIN, rest = o / CIN, co = rest % COUT, t = rest / COUT;
+                const int g = t / 3, di = t % 3;
+                float a = acc[q];
+                for (int r = 0; r < TC; ++r) a = fmaf(sdz[r][co], sx[g][r + di][ci], a);
+                acc[q] = a;
+            }
+        }
+        if (threadIdx.x < COUT)
+            for (int r = 0; r < TC; ++r) bacc += sdz[r][threadIdx.x];
+        __syncthreads();
+    }
+    float *p = part + (size_t)blockIdx.x * (NW + COUT);
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+        const int o = threadIdx.x + q * kThreads;
+        if (o < NW) p[o] = acc[q];
+    }
+    if (threadIdx.x < COUT) p[NW + threadIdx.x] = bacc;
+}
+
+__global__ void reduce_parts_kernel(const float *part, int nparts, int n, float *out)
+{
+    for (int o = blockIdx.x * blockDim.x + threadIdx.x; o < n; o += gridDim.x * blockDim.x) {
+        float s = 0.f;
+        for (int b = 0; b < nparts; ++b) s += part[(size_t)b * n + o];
+        out[o] = s;
+    }
+}
+
+// Features [cell][9] FP32 -> BF16 [cell][16], zero on boundary nodes and padding.
+__global__ void features_kernel(const float *f, __nv_bfloat16 *x0, long long ncell, int ni, int nj, int nk)
+{
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const bool in = interior_cell(c, ni, nj, nk);
+        __nv_bfloat16 v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = __float2bfloat16_rn((in && q < kFeat) ? f[c * kFeat + q] : 0.f);
+        reinterpret_cast<uint4 *>(x0 + c * 16)[0] = reinterpret_cast<uint4 *>(v)[0];
+        reinterpret_cast<uint4 *>(x0 + c * 16)[1] = reinterpret_cast<uint4 *>(v)[1];
+    }
+}
+
+// Mean squared error over interior cells and the kOut outputs; dy = dL/dy as
+// BF16 [cell][16] (zero elsewhere); per-CTA FP64 partial losses.
+__global__ void mse_kernel(const float *y, const float *t, __nv_bfloat16 *dy, long long ncell, int ni, int nj,
+                           int nk, double inv_n, double *part)
+{
+    double s = 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
+         c += (long long)gridDim.x * blockDim.x) {
+        const bool in = interior_cell(c, ni, nj, nk);
+        __nv_bfloat16 v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) v[q] = __float2bfloat16_rn(0.f);
+        if (in) {
+#pragma unroll
+            for (int q = 0; q < kOut; ++q) {
+                const double d = (double)y[c * kOut + q] - (double)t[c * kOut + q];
+                s += d * d;
+                v[q] = __float2bfloat16_rn((float)(2.0 * d * inv_n));
+            }
+        }
+        reinterpret_cast<uint4 *>(dy + c * 16)[0] = reinterpret_cast<uint4 *>(v)[0];
+        reinterpret_cast<uint4 *>(dy + c * 16)[1] = reinterpret_cast<uint4 *>(v)[1];
+    }
+    s = warp_sum(s);
+    __shared__ double sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) r += sh[w];
+        part[blockIdx.x] = r * inv_n;
+    }
+}
+
+__global__ void adam_kernel(float *p, const float *g, float *m, float *v, const unsigned char *live, int n,
+                            float lr, float b1, float b2, float eps, float c1, float c2)
+{
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        if (!live[q]) continue;
+        const float gq = g[q];
+        const float mq = b1 * m[q] + (1.f - b1) * gq, vq = b2 * v[q] + (1.f - b2) * gq * gq;
+        m[q] = mq;
+        v[q] = vq;
+        p[q] -= lr * (mq / c1) / (sqrtf(vq / c2) + eps);
+    }
+}
+
+// ---- host side ------------------------------------------------------------------------
+template <int CIN, int COUT> void set_conv_smem()
+{
+    cudaFuncSetAttribute(conv_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)ConvSmem<CIN, COUT>::BYTES);
+}
+
+template <int CIN, int COUT> void launch_conv(const ConvArgs &a, int grid, cudaStream_t s)
+{
+    conv_tc_kernel<CIN, COUT><<<grid, kThreads, ConvSmem<CIN, COUT>::BYTES, s>>>(a);
+}
+
+static void conv(int cin, int cout, const ConvArgs &a, int grid, cudaStream_t s)
+{
+    if (cin == 16 && cout == 32) launch_conv<16, 32>(a, grid, s);
+    else if (cin == 32 && cout == 32) launch_conv<32, 32>(a, grid, s);
+    else if (cin == 32 && cout == 16) launch_conv<32, 16>(a, grid, s);
+    else if (cin == 16 && cout == 16) launch_conv<16, 16>(a, grid, s);
+}
+
+static void wgrad(int cin, int cout, const __nv_bfloat16 *x, const __nv_bfloat16 *dz, long long ncell, int ni,
+                  int nj, float *part, int grid, cudaStream_t s)
+{
+    if (cin == 16 && cout == 32) wgrad_kernel<16, 32><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
+    else if (cin == 32 && cout == 32) wgrad_kernel<32, 32><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
+    else if (cin == 32 && cout == 16) wgrad_kernel<32, 16><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
+}
+
+}  // namespace cnn
+}  // namespace amcfd
+
+using namespace amcfd;
+using namespace amcfd::cnn;
+
+// Parameter vector layout: for each layer, W [27][cout][cin] then b [cout].
+static size_t layer_off(int l)
+{
+    size_t o = 0;
+    for (int q = 0; q < l; ++q) o += (size_t)27 * kCin[q] * kCout[q] + kCout[q];
+    return o;
+}
+static size_t nparams() { return layer_off(kLayers); }
+
+struct amcfd_net {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    int sm = 148;
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // FP32 parameters, grads, moments
+    unsigned char *live = nullptr;                                  // 1 where a parameter is not padding
+    __nv_bfloat16 *wf[kLayers] = {}, *wb[kLayers] = {};             // packed operands
+    __nv_bfloat16 *act[kLayers + 1] = {};                           // act[0] features, act[l+1] layer l out
+    __nv_bfloat16 *grad[2] = {};                                    // dZ ping-pong [cell][32]
+    float *y = nullptr, *part = nullptr;
+    double *lpart = nullptr;
+    int *errd = nullptr;
+    long long ncap = 0, ncell = 0;
+    int ni = 0, nj = 0, nk = 0;
+    long long step = 0;
+};
+
+#define NCK(call)                                                                         \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) {                                                          \
+            net->err = std::string(#call) + ": " + cudaGetErrorString(e_);                \
+            return AMCFD_E_CUDA;                                                          \
+        }                                                                                 \
+    } while (0)
+
+static int net_pack(amcfd_net *net)
+{
+    for (int l = 0; l < kLayers; ++l) {
+        const float *w = net->p + layer_off(l);
+        pack_fwd_kernel<<<64, 256, 0, net->stream>>>(w, net->wf[l], kCin[l], kCout[l]);
+        pack_bwd_kernel<<<64, 256, 0, net->stream>>>(w, net->wb[l], kCin[l], kCout[l]);
+    }
+    NCK(cudaGetLastError());
+    return 0;
+}
+
+static int net_reserve(amcfd_net *net, int ni, int nj, int nk)
+{
+    const long long n = (long long)ni * nj * nk;
+    net->ni = ni; net->nj = nj; net->nk = nk; net->ncell = n;
+    if (n <= net->ncap) return 0;
+    for (auto &a : net->act) if (a) cudaFree(a), a = nullptr;
+    for (auto &a : net->grad) if (a) cudaFree(a), a = nullptr;
+    if (net->y) cudaFree(net->y), net->y = nullptr;
+    NCK(cudaMalloc(&net->act[0], n * 16 * sizeof(__nv_bfloat16)));
+    for (int l = 0; l < kLayers; ++l) NCK(cudaMalloc(&net->act[l + 1], n * kCout[l] * sizeof(__nv_bfloat16)));
+    for (auto &a : net->grad) NCK(cudaMalloc(&a, n * 32 * sizeof(__nv_bfloat16)));
+    NCK(cudaMalloc(&net->y, n * kOut * sizeof(float)));
+    net->ncap = n;
+    return 0;
+}
+
+extern "C" {
+
+size_t amcfd_net_param_count(void) { return nparams(); }
+
+int amcfd_net_create(int device, unsigned long long seed, amcfd_net **out)
+{
+    if (!out) return AMCFD_E_ARG;
+    amcfd_net *net = new amcfd_net();
+    *out = net;
+    net->device = device;
+    NCK(cudaSetDevice(device));
+    NCK(cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking));
+    cudaDeviceGetAttribute(&net->sm, cudaDevAttrMultiProcessorCount, device);
+    const size_t np = nparams();
+    NCK(cudaMalloc(&net->p, np * sizeof(float)));
+    NCK(cudaMalloc(&net->g, np * sizeof(float)));
+    NCK(cudaMalloc(&net->m, np * sizeof(float)));
+    NCK(cudaMalloc(&net->v, np * sizeof(float)));
+    NCK(cudaMalloc(&net->live, np));
+    NCK(cudaMalloc(&net->errd, sizeof(int)));
+    NCK(cudaMemset(net->errd, 0, sizeof(int)));
+    NCK(cudaMemset(net->g, 0, np * sizeof(float)));
+    NCK(cudaMemset(net->m, 0, np * sizeof(float)));
+    NCK(cudaMemset(net->v, 0, np * sizeof(float)));
+    for (int l = 0; l < kLayers; ++l) {
+        NCK(cudaMalloc(&net->wf[l], (size_t)27 * kCin[l] * kCout[l] * sizeof(__nv_bfloat16)));
+        NCK(cudaMalloc(&net->wb[l], (size_t)27 * kCin[l] * kCout[l] * sizeof(__nv_bfloat16)));
+    }
+    NCK(cudaMalloc(&net->part, (size_t)net->sm * (27 * 32 * 32 + 32) * sizeof(float)));
+    NCK(cudaMalloc(&net->lpart, (size_t)net->sm * 4 * sizeof(double)));
+    set_conv_smem<16, 32>();
+    set_conv_smem<32, 32>();
+    set_conv_smem<32, 16>();
+    set_conv_smem<16, 16>();
+    // initialisation: uniform(-a, a), a = sqrt(6 / fan_in) (ReLU layers), the last
+    // layer scaled by 0.1 so that the first predictions are near zero; padding 0
+    std::vector<float> h(np, 0.f);
+    std::vector<unsigned char> live(np, 0);
+    unsigned long long x = seed ? seed : 0x9e3779b97f4a7c15ull;
+    auto rnd = [&]() {
+        x += 0x9e3779b97f4a7c15ull;
+        unsigned long long z = x;
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    for (int l = 0; l < kLayers; ++l) {
+        const int cin_real = l == 0 ? kFeat : kCin[l], cout_real = l == kLayers - 1 ? kOut : kCout[l];
+        const double a = std::sqrt(6.0 / (27.0 * cin_real)) * (l == kLayers - 1 ? 0.1 : 1.0);
+        const size_t o = layer_off(l);
+        for (int t = 0; t < 27; ++t)
+            for (int co = 0; co < kCout[l]; ++co)
+                for (int ci = 0; ci < kCin[l]; ++ci) {
+                    const size_t q = o + ((size_t)t * kCout[l] + co) * kCin[l] + ci;
+                    if (ci < cin_real && co < cout_real) {
+                        h[q] = (float)((2.0 * rnd() - 1.0) * a);
+                        live[q] = 1;
+                    }
+                }
+        for (int co = 0; co < cout_real; ++co) live[o + (size_t)27 * kCin[l] * kCout[l] + co] = 1;
+    }
+    NCK(cudaMemcpy(net->p, h.data(), np * sizeof(float), cudaMemcpyHostToDevice));
+    NCK(cudaMemcpy(net->live, live.data(), np, cudaMemcpyHostToDevice));
+    return net_pack(net);
+}
+
+void amcfd_net_destroy(amcfd_net *net)
+{
+    if (!net) return;
+    if (net->stream) cudaStreamSynchronize(net->stream);
+    void *ptrs[] = {net->p, net->g, net->m, net->v, net->live, net->y, net->part, net->lpart, net->errd};
+    for (void *q : ptrs) if (q) cudaFree(q);
+    for (int l = 0; l < kLayers; ++l) {
+        if (net->wf[l]) cudaFree(net->wf[l]);
+        if (net->wb[l]) cudaFree(net->wb[l]);
+    }
+    for (auto a : net->act) if (a) cudaFree(a);
+    for (auto a : net->grad) if (a) cudaFree(a);
+    if (net->stream) cudaStreamDestroy(net->stream);
+    delete net;
+}
+
+const char *amcfd_net_last_error(const amcfd_net *net) { return net ? net->err.c_str() : "null network"; }
+
+int amcfd_net_get_params(amcfd_net *net, float *host, size_t n)
+{
+    if (!net || !host || n != nparams()) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaMemcpy(host, net->p, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int amcfd_net_set_params(amcfd_net *net, const float *host, size_t n)
+{
+    if (!net || !host || n != nparams()) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaMemcpy(net->p, host, n * sizeof(float), cudaMemcpyHostToDevice));
+    return net_pack(net);
+}
+
+int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n)
+{
+    if (!net || !host || n != nparams()) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaMemcpy(host, net->g, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+// Forward pass on device features [ncell][9] (FP32) over an ni x nj x nk node
+// grid; y_dev (may be null) receives the two outputs [ncell][2] (FP32).
+int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev)
+{
+    if (!net || !feat_dev || ni < 3 || nj < 3 || nk < 3) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    int rc = net_reserve(net, ni, nj, nk);
+    if (rc) return rc;
+    const long long n = net->ncell;
+    features_kernel<<<net->sm * 4, 256, 0, net->stream>>>(feat_dev, net->act[0], n, ni, nj, nk);
+    const long long ntiles = (n + kM - 1) / kM;
+    const int grid = (int)std::min<long long>(ntiles, net->sm);
+    for (int l = 0; l < kLayers; ++l) {
+        ConvArgs a{};
+        a.x = net->act[l];
+        a.w = net->wf[l];
+        a.bias = net->p + layer_off(l) + (size_t)27 * kCin[l] * kCout[l];
+        a.y = net->act[l + 1];
+        a.relu = l < kLayers - 1;
+        a.y32 = l == kLayers - 1 ? net->y : nullptr;
+        a.n32 = kOut;
+        a.ni = ni; a.nj = nj; a.nk = nk; a.ncell = n;
+        a.err = net->errd;
+        conv(kCin[l], kCout[l], a, grid, net->stream);
+    }
+    NCK(cudaGetLastError());
+    if (y_dev) NCK(cudaMemcpyAsync(y_dev, net->y, n * kOut * sizeof(float), cudaMemcpyDeviceToDevice, net->stream));
+    NCK(cudaStreamSynchronize(net->stream));
+    int e = 0;
+    NCK(cudaMemcpy(&e, net->errd, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) { net->err = "tensor-core pipeline wait gave up"; return e; }
+    return 0;
+}
+
+// Loss and gradients of the last forward pass against targets [ncell][2]
+// (FP32, device): MSE over interior cells; grads of every parameter into the
+// gradient buffer (amcfd_net_get_grads).  *loss receives the loss.
+int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
+{
+    if (!net || !target_dev || net->ncell == 0) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    const long long n = net->ncell;
+    const int ni = net->ni, nj = net->nj, nk = net->nk;
+    const double nint = (double)(ni - 2) * (nj - 2) * (nk - 2) * kOut;
+    const int lg = net->sm;
+    mse_kernel<<<lg, 256, 0, net->stream>>>(net->y, target_dev, net->grad[0], n, ni, nj, nk, 1.0 / nint,
+                                            net->lpart);
+    const long long ntiles = (n + kM - 1) / kM;
+    const int grid = (int)std::min<long long>(ntiles, net->sm);
+    // grad[cur] holds dZ of layer l ([cell][kCout[l]], gradient w.r.t. its pre-activation)
+    int cur = 0;
+    for (int l = kLayers - 1; l >= 0; --l) {
+        const size_t nw = (size_t)27 * kCin[l] * kCout[l];
+        wgrad(kCin[l], kCout[l], net->act[l], net->grad[cur], n, ni, nj, net->part, net->sm, net->stream);
+        reduce_parts_kernel<<<64, 256, 0, net->stream>>>(net->part, net->sm, (int)(nw + kCout[l]),
+                                                          net->g + layer_off(l));
+        if (l > 0) {
+            ConvArgs a{};
+            a.x = net->grad[cur];
+            a.w = net->wb[l];
+            a.gate = net->act[l];  // ReLU derivative of the previous layer's output
+            a.y = net->grad[cur ^ 1];
+            a.ni = ni; a.nj = nj; a.nk = nk; a.ncell = n;
+            a.err = net->errd;
+            conv(kCout[l], kCin[l], a, grid, net->stream);
+            cur ^= 1;
+        }
+    }
+    NCK(cudaGetLastError());
+    std::vector<double> lp(lg);
+    NCK(cudaMemcpyAsync(lp.data(), net->lpart, lg * sizeof(double), cudaMemcpyDeviceToHost, net->stream));
+    NCK(cudaStreamSynchronize(net->stream));
+    if (loss) {
+        double s = 0.0;
+        for (double q : lp) s += q;
+        *loss = s;
+    }
+    int e = 0;
+    NCK(cudaMemcpy(&e, net->errd, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) { net->err = "tensor-core pipeline wait gave up"; return e; }
+    return 0;
+}
+
+// One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) with the current gradients.
+int amcfd_net_adam(amcfd_net *net, float lr)
+{
+    if (!net) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    net->step += 1;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.f - std::pow(b1, (float)net->step), c2 = 1.f - std::pow(b2, (float)net->step);
+    adam_kernel<<<64, 256, 0, net->stream>>>(net->p, net->g, net->m, net->v, net->live, (int)nparams(), lr, b1,
+                                             b2, 1e-8f, c1, c2);
+    NCK(cudaGetLastError());
+    int rc = net_pack(net);
+    if (rc) return rc;
+    NCK(cudaStreamSynchronize(net->stream));
+    return 0;
+}
+
+}  // extern "C"

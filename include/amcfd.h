@@ -212,6 +212,28 @@ long long amcfd_kernel_launches(const amcfd_ctx *ctx);
 int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nthreads,
                     amcfd_step_report *reports, int *status);
 
+/* ---- Learned warm start: a 4-layer 3x3x3 convolutional network --------------
+ * No counterpart in the reference.  Layers 16->32->32->32->16 channels (9 input
+ * features and 2 outputs used), ReLU between layers, BF16 operands on the tensor
+ * cores with FP32 accumulation, FP32 master parameters laid out per layer as
+ * W[27][cout][cin] then b[cout] (tap = 9(dk+1) + 3(dj+1) + (di+1)).  Inputs and
+ * outputs are device arrays over a full ni x nj x nk node grid, channels last;
+ * boundary nodes are held at zero (a zero-padded convolution over the interior). */
+typedef struct amcfd_net amcfd_net;
+size_t amcfd_net_param_count(void);
+int amcfd_net_create(int device, unsigned long long seed, amcfd_net **out);
+void amcfd_net_destroy(amcfd_net *net);
+const char *amcfd_net_last_error(const amcfd_net *net);
+int amcfd_net_get_params(amcfd_net *net, float *host, size_t n);
+int amcfd_net_set_params(amcfd_net *net, const float *host, size_t n);
+int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n);
+/* feat_dev: [ncell][9] FP32; y_dev (nullable): [ncell][2] FP32 */
+int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev);
+/* MSE of the last forward pass against target_dev [ncell][2] over interior cells;
+ * all parameter gradients into the net's gradient buffer */
+int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss);
+int amcfd_net_adam(amcfd_net *net, float lr);
+
 /* Energy residual without any device allocation.  No counterpart in the reference:
  * it exists for callers that cannot let a library allocate device memory (an
  * application that owns all device memory through its own pool, or one under a
