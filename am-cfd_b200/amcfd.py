@@ -25,6 +25,7 @@ MAX_ZONES = 32
 SCHEME_UPWIND, SCHEME_POWER_LAW, SCHEME_EXPONENTIAL = 0, 1, 2
 ORDER_EXACT, ORDER_REDBLACK = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
+WS_OFF, WS_PREDICT, WS_RECORD, WS_PREDICT_H = 0, 1, 2, 3
 PHASES = {"laser": 1, "energy_assemble": 2, "energy_solve": 3, "h2t": 4, "meltpool": 5,
           "momentum": 6, "converge": 7, "update": 8}
 ERRORS = {0: "AMCFD_OK", -1: "AMCFD_E_ARG", -2: "AMCFD_E_IO", -3: "AMCFD_E_PARSE",
@@ -128,6 +129,9 @@ def lib() -> C.CDLL:
             L.amcfd_net_forward.argtypes = [VP, VP, _I, _I, _I, VP]
             L.amcfd_net_backward.argtypes = [VP, VP, P(_D)]
             L.amcfd_net_adam.argtypes = [VP, C.c_float]
+            L.amcfd_ws_attach.argtypes = [VP, VP, _I]
+            L.amcfd_ws_buffers.argtypes = [VP, P(VP), P(VP)]
+            L.amcfd_ws_stats.argtypes = [VP, P(C.c_longlong), P(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -305,6 +309,23 @@ class Solver:
     def get_into(self, name: str, ptr: int):
         """Copy a field into caller memory at address `ptr` (ni*nj*nk doubles)."""
         self._check(lib().amcfd_get_field(self._h, name.encode(), C.cast(ptr, C.POINTER(_D))))
+
+    def ws_attach(self, net: Optional["Net"], mode: int):
+        """Attach the warm-start network (WS_OFF, WS_PREDICT, WS_RECORD)."""
+        self._net = net
+        self._check(lib().amcfd_ws_attach(self._h, net._h if net is not None else None, mode))
+
+    def ws_buffers(self):
+        """Device pointers of the last step's features [ncell][11] and scaled
+        increments [ncell][2] (FP32)."""
+        f, t = C.c_void_p(), C.c_void_p()
+        self._check(lib().amcfd_ws_buffers(self._h, C.byref(f), C.byref(t)))
+        return f.value, t.value
+
+    def ws_stats(self):
+        a, r = C.c_longlong(), C.c_longlong()
+        self._check(lib().amcfd_ws_stats(self._h, C.byref(a), C.byref(r)))
+        return a.value, r.value
 
     TIMING_SLOTS = ("energy_assemble", "factor", "energy_sweeps", "h2t_meltpool", "momentum",
                     "converge", "laser", "update", "outer_iters", "sweep_launches")

@@ -1,0 +1,100 @@
+"""Learned warm start: training on fields the solver generates, and evaluation.
+
+Training (``train``): solver instances run in record mode; after every time
+step the network takes ``updates`` Adam steps on that step's pair (features
+at the start of the step -> realised enthalpy and pressure increments), all on
+the GPU with the tensor-core kernels of k_cnn.cu.
+
+Evaluation (``evaluate``): the same deck is solved twice, plainly and with
+the network's prediction as the starting guess of every step (rejected when
+it raises the step's initial energy residual); the outer-iteration counts,
+device times, acceptance counts and the final fields are returned.
+"""
+from __future__ import annotations
+
+import time
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+import amcfd
+
+
+class DeviceArray:
+    """Zero-copy view of a device pointer for torch.as_tensor (FP32)."""
+
+    def __init__(self, ptr: int, shape):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f4",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def device_view(ptr: int, shape):
+    import torch
+    return torch.as_tensor(DeviceArray(ptr, shape), device="cuda")
+
+
+def train(net: amcfd.Net, deck_paths: Sequence[str], steps: int, lr: float = 1e-3, updates: int = 4,
+          precision: int = amcfd.PREC_FP32, order: int = amcfd.ORDER_REDBLACK, device: int = 0) -> List[float]:
+    """Online training on every step of every deck; returns the loss history."""
+    losses: List[float] = []
+    for path in deck_paths:
+        s = amcfd.Solver(amcfd.Deck(path), order=order, precision=precision, device=device, use_graphs=1)
+        s.ws_attach(net, amcfd.WS_RECORD)
+        feat, target = s.ws_buffers()
+        nk, nj, ni = s.shape
+        for _ in range(steps):
+            s.step()
+            for _ in range(updates):
+                net.forward(feat, (ni, nj, nk))
+                losses.append(net.backward(target))
+                net.adam(lr)
+        s.ws_attach(None, amcfd.WS_OFF)
+        s.close()
+    return losses
+
+
+def evaluate(net: amcfd.Net, deck_path: str, steps: int, precision: int = amcfd.PREC_FP32,
+             order: int = amcfd.ORDER_REDBLACK, device: int = 0, ref_maxit: int = 200,
+             mode: int = amcfd.WS_PREDICT) -> Dict:
+    """Plain vs warm-started solve of the same deck, both against a reference
+    solve that may take up to ``ref_maxit`` outer iterations per step (the
+    deck's own limit, 20 in the reference's decks, often stops a step before
+    its convergence test passes)."""
+    out = {}
+    for run in ("plain", "warm", "reference"):
+        deck = amcfd.Deck(deck_path)
+        if run == "reference":
+            deck.params.maxit = ref_maxit
+        s = amcfd.Solver(deck, order=order, precision=precision, device=device, use_graphs=1)
+        if run == "warm":
+            s.ws_attach(net, mode)
+        iters, fallback, resorh = [], [], []
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r = s.step()
+            iters.append(r["niter"])
+            fallback.append(r["fallback"])
+            resorh.append(r["resorh"])
+        wall = time.perf_counter() - t0
+        acc, rej = s.ws_stats()
+        out[run] = {"iters": iters, "fallback": fallback, "resorh": resorh, "wall_s": wall, "accepted": acc,
+                     "rejected": rej, "temp": s.get("temp"), "uvel": s.get("uvel"),
+                     "dims": (r["alen"], r["depth"], r["width"])}
+        s.close()
+    p, w, ref = out["plain"], out["warm"], out["reference"]
+
+    def err(a, f):
+        return float(np.linalg.norm(a[f] - ref[f]) / max(np.linalg.norm(ref[f]), 1e-300))
+
+    out["summary"] = {
+        "steps": steps,
+        "iters_plain": float(np.mean(p["iters"])), "iters_warm": float(np.mean(w["iters"])),
+        "iters_reference": float(np.mean(ref["iters"])),
+        "wall_plain_s": p["wall_s"], "wall_warm_s": w["wall_s"],
+        "fallback_rate": w["rejected"] / max(1, w["accepted"] + w["rejected"]),
+        "resorh_plain": float(np.mean(p["resorh"])), "resorh_warm": float(np.mean(w["resorh"])),
+        "temp_err_plain": err(p, "temp"), "temp_err_warm": err(w, "temp"),
+        "uvel_err_plain": err(p, "uvel"), "uvel_err_warm": err(w, "uvel"),
+        "dims_plain": p["dims"], "dims_warm": w["dims"], "dims_reference": ref["dims"],
+    }
+    return out

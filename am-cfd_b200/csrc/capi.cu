@@ -26,6 +26,11 @@ dim3 energy_assemble_grid(const Params &p);
 template <typename T> int h2t_blocks_per_sm();
 template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
                                              long long rows, int sm_count, cudaStream_t s);
+template <typename T> void ws_features(Inst<T> &I, float *feat, const float *prev, double bx, double by,
+                                       double power);
+template <typename T> void ws_copy(Inst<T> &I, T *const *save, int dir);
+template <typename T> void ws_apply(Inst<T> &I, const float *y, double alpha, int with_p);
+template <typename T> void ws_target(Inst<T> &I, T *const *save, float *target);
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
 int encode_field_map(CUtensorMap *map, const void *base, int elem, int nip, int nj, int nk, int bx,
@@ -91,6 +96,13 @@ struct amcfd_ctx {
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
     double *pack = nullptr;        // FP64 read-out staging (ni*nj*nk), made on first use
     int sm_count = 0;
+    // learned warm start (amcfd_ws_attach)
+    amcfd_net *net = nullptr;
+    int ws_mode = 0;
+    float *ws_feat = nullptr, *ws_y = nullptr, *ws_target = nullptr;
+    void *ws_save[4] = {};         // h, p, T, f_l at the start of the step
+    long long ws_accepted = 0, ws_rejected = 0;
+    int ws_fallback = 0;           // the last step's prediction was rejected
 };
 
 #define CK(call)                                                                          \
@@ -652,6 +664,73 @@ static void fill_report(amcfd_ctx *ctx, amcfd_step_report *r)
     r->istat = s->istat; r->iend = s->iend; r->jstat = s->jstat; r->jend = s->jend;
     r->kstat = s->kstat; r->jstart = ctx->jstart; r->powerindicator = ctx->powerindicator;
     r->momentum_cells = s->box_cells;
+    r->fallback = ctx->ws_fallback;
+}
+
+// ---- learned warm start ----------------------------------------------------------------
+// Energy residual of the current state (assembly + calculateResiduals(5),
+// CFDSolverManager.cpp:2073-2101) without touching the step's BC or source
+// state; a non-finite value comes back as +inf and clears the device flag.
+template <typename T>
+static int ws_residual(amcfd_ctx *ctx, Inst<T> &I, double &r)
+{
+    launch_energy_assemble<T>(I);
+    launch_block_correct<T>(I);
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st_dev, sizeof(Status), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    if (ctx->st_host->error) return read_status(ctx);
+    r = ctx->st_host->resorh;
+    if (ctx->st_host->nonfinite || !std::isfinite(r)) {
+        const int zero = 0;
+        CK(cudaMemcpyAsync(&ctx->st_dev->nonfinite, &zero, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        r = INFINITY;
+    }
+    ctx->launches += 3;
+    return 0;
+}
+
+// Start of a step (after the laser moved): features of the current state,
+// snapshot of h, p, T, f_l; in predict mode the network's increments (full,
+// then half) are applied and the first that lowers the energy residual of the
+// start of the step is kept.
+template <typename T>
+static int ws_before(amcfd_ctx *ctx, Inst<T> &I)
+{
+    T *const *save = reinterpret_cast<T *const *>(ctx->ws_save);
+    const double power = ctx->prm.alaspow * (double)ctx->powerindicator;
+    ws_features<T>(I, ctx->ws_feat, ctx->ws_target, ctx->beamposx, ctx->beamposy, power);
+    ws_copy<T>(I, save, 0);
+    ctx->launches += 2;
+    ctx->ws_fallback = 0;
+    if (ctx->ws_mode != AMCFD_WS_PREDICT && ctx->ws_mode != AMCFD_WS_PREDICT_H) return 0;
+    int rc;
+    double r0, r1;
+    if ((rc = ws_residual<T>(ctx, I, r0))) return rc;
+    if ((rc = amcfd_net_forward(ctx->net, ctx->ws_feat, ctx->ni, ctx->nj, ctx->nk, ctx->ws_y)))
+        return fail(ctx, rc, std::string("warm-start network: ") + amcfd_net_last_error(ctx->net));
+    for (double alpha : {1.0, 0.5}) {
+        ws_apply<T>(I, ctx->ws_y, alpha, ctx->ws_mode == AMCFD_WS_PREDICT ? 1 : 0);
+        if ((rc = ws_residual<T>(ctx, I, r1))) return rc;
+        ctx->launches += 1;
+        if (r1 < r0) {
+            ctx->ws_accepted++;
+            return 0;
+        }
+        ws_copy<T>(I, save, 1);
+        ctx->launches += 1;
+    }
+    ctx->ws_rejected++;
+    ctx->ws_fallback = 1;
+    return 0;
+}
+
+template <typename T>
+static void ws_after(amcfd_ctx *ctx, Inst<T> &I)
+{
+    ws_target<T>(I, reinterpret_cast<T *const *>(ctx->ws_save), ctx->ws_target);
+    ctx->launches += 1;
 }
 
 // =========================================================================================
@@ -747,6 +826,9 @@ void amcfd_destroy(amcfd_ctx *ctx)
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->pack) cudaFree(ctx->pack);
+    for (void *q : {(void *)ctx->ws_feat, (void *)ctx->ws_y, (void *)ctx->ws_target, ctx->ws_save[0],
+                    ctx->ws_save[1], ctx->ws_save[2], ctx->ws_save[3]})
+        if (q) cudaFree(q);
     for (auto &plane : ctx->gexec)
         for (auto &row : plane)
             for (auto &ge : row)
@@ -772,6 +854,11 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
     CK(cudaSetDevice(ctx->device));
     int rc = begin_step(ctx);
     if (rc) return rc;
+    if (ctx->ws_mode) {
+        rc = ctx->precision == AMCFD_PREC_FP64 ? ws_before<double>(ctx, ctx->I64)
+                                               : ws_before<float>(ctx, ctx->I32);
+        if (rc) return rc;
+    }
     rc = ctx->precision == AMCFD_PREC_FP64 ? outer_loop<double>(ctx, ctx->I64)
                                            : outer_loop<float>(ctx, ctx->I32);
     if (rc) return rc;
@@ -790,9 +877,52 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
             ctx->last_ms[7] += ms;
         }
     }
+    if (ctx->ws_mode) {
+        if (ctx->precision == AMCFD_PREC_FP64)
+            ws_after<double>(ctx, ctx->I64);
+        else
+            ws_after<float>(ctx, ctx->I32);
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaGetLastError());
     fill_report(ctx, report);
+    return 0;
+}
+
+int amcfd_ws_attach(amcfd_ctx *ctx, amcfd_net *net, int mode)
+{
+    if (!ctx || mode < AMCFD_WS_OFF || mode > AMCFD_WS_PREDICT_H || (mode != AMCFD_WS_OFF && !net))
+        return AMCFD_E_ARG;
+    if (mode != AMCFD_WS_OFF && ctx->prm.nheattable > 0)
+        return fail(ctx, AMCFD_E_ARG, "warm start with a volumetric heat-source table is not supported");
+    CK(cudaSetDevice(ctx->device));
+    ctx->net = net;
+    ctx->ws_mode = mode;
+    if (mode == AMCFD_WS_OFF || ctx->ws_feat) return 0;
+    const size_t n = (size_t)ctx->ni * ctx->nj * ctx->nk;
+    const size_t n3 = (size_t)ctx->nk * ctx->nj * ctx->nip;
+    const size_t e = ctx->precision == AMCFD_PREC_FP64 ? sizeof(double) : sizeof(float);
+    CK(cudaMalloc(&ctx->ws_feat, n * 11 * sizeof(float)));
+    CK(cudaMalloc(&ctx->ws_y, n * 2 * sizeof(float)));
+    CK(cudaMalloc(&ctx->ws_target, n * 2 * sizeof(float)));
+    CK(cudaMemset(ctx->ws_target, 0, n * 2 * sizeof(float)));
+    for (auto &q : ctx->ws_save) CK(cudaMalloc(&q, n3 * e));
+    return 0;
+}
+
+int amcfd_ws_buffers(amcfd_ctx *ctx, float **feat_dev, float **target_dev)
+{
+    if (!ctx || !ctx->ws_feat) return AMCFD_E_ARG;
+    if (feat_dev) *feat_dev = ctx->ws_feat;
+    if (target_dev) *target_dev = ctx->ws_target;
+    return 0;
+}
+
+int amcfd_ws_stats(const amcfd_ctx *ctx, long long *accepted, long long *rejected)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    if (accepted) *accepted = ctx->ws_accepted;
+    if (rejected) *rejected = ctx->ws_rejected;
     return 0;
 }
 

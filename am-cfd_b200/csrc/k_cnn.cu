@@ -2,7 +2,7 @@
 // (no counterpart in the reference; it only supplies an initial guess, the
 // reference's own outer loop still decides convergence).
 //
-//   features (16 ch, 9 used) -> conv 16->32, ReLU -> conv 32->32, ReLU
+//   features (16 ch, 11 used) -> conv 16->32, ReLU -> conv 32->32, ReLU
 //                            -> conv 32->32, ReLU -> conv 32->16 (2 used)
 //
 // Activations are BF16, channels-last [cell][C] over the full node grid
@@ -44,7 +44,7 @@ constexpr int kG = 9;    // (dk, dj) groups
 constexpr int kLayers = 4;
 constexpr int kCin[kLayers] = {16, 32, 32, 32};
 constexpr int kCout[kLayers] = {32, 32, 32, 16};
-constexpr int kFeat = 9;  // real input channels
+constexpr int kFeat = 11;  // real input channels
 constexpr int kOut = 2;   // real output channels
 
 template <int CIN, int COUT> struct ConvSmem {
@@ -362,7 +362,7 @@ __global__ void reduce_parts_kernel(const float *part, int nparts, int n, float 
     }
 }
 
-// Features [cell][9] FP32 -> BF16 [cell][16], zero on boundary nodes and padding.
+// Features [cell][11] FP32 -> BF16 [cell][16], zero on boundary nodes and padding.
 __global__ void features_kernel(const float *f, __nv_bfloat16 *x0, long long ncell, int ni, int nj, int nk)
 {
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncell;
@@ -632,7 +632,7 @@ int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n)
     return 0;
 }
 
-// Forward pass on device features [ncell][9] (FP32) over an ni x nj x nk node
+// Forward pass on device features [ncell][11] (FP32) over an ni x nj x nk node
 // grid; y_dev (may be null) receives the two outputs [ncell][2] (FP32).
 int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev)
 {

@@ -227,12 +227,29 @@ const char *amcfd_net_last_error(const amcfd_net *net);
 int amcfd_net_get_params(amcfd_net *net, float *host, size_t n);
 int amcfd_net_set_params(amcfd_net *net, const float *host, size_t n);
 int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n);
-/* feat_dev: [ncell][9] FP32; y_dev (nullable): [ncell][2] FP32 */
+/* feat_dev: [ncell][11] FP32; y_dev (nullable): [ncell][2] FP32 */
 int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev);
 /* MSE of the last forward pass against target_dev [ncell][2] over interior cells;
  * all parameter gradients into the net's gradient buffer */
 int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss);
 int amcfd_net_adam(amcfd_net *net, float lr);
+
+/* Attach a warm-start network to a solver context (same device).  Modes:
+ * AMCFD_WS_OFF; AMCFD_WS_PREDICT: each step starts from the network's predicted
+ * enthalpy and pressure increments, kept only if they lower the step's initial
+ * energy residual (the report's `fallback` is 1 when they were rejected);
+ * AMCFD_WS_PREDICT_H: the same with the enthalpy increment only;
+ * AMCFD_WS_RECORD: no prediction.  In all active modes every step leaves its
+ * features ([ncell][11]) and realised scaled increments ([ncell][2]) in device
+ * buffers (amcfd_ws_buffers) for training with amcfd_net_forward/backward.
+ * Decks with a volumetric heat-source table are refused. */
+#define AMCFD_WS_OFF 0
+#define AMCFD_WS_PREDICT 1
+#define AMCFD_WS_RECORD 2
+#define AMCFD_WS_PREDICT_H 3
+int amcfd_ws_attach(amcfd_ctx *ctx, amcfd_net *net, int mode);
+int amcfd_ws_buffers(amcfd_ctx *ctx, float **feat_dev, float **target_dev);
+int amcfd_ws_stats(const amcfd_ctx *ctx, long long *accepted, long long *rejected);
 
 /* Energy residual without any device allocation.  No counterpart in the reference:
  * it exists for callers that cannot let a library allocate device memory (an

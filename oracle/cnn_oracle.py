@@ -15,7 +15,7 @@ import numpy as np
 
 CIN = (16, 32, 32, 32)
 COUT = (32, 32, 32, 16)
-NFEAT, NOUT = 9, 2
+NFEAT, NOUT = 11, 2
 
 
 def bf16(a):
@@ -69,7 +69,7 @@ def conv(x, w, offs):
 
 
 def forward(params, feat, dims):
-    """Returns (y [ncell][2], activations list) for features [ncell][9]."""
+    """Returns (y [ncell][2], activations list) for features [ncell][11]."""
     ni, nj, nk = dims
     offs = offsets(ni, nj)
     inner = interior_mask(ni, nj, nk)[:, None]

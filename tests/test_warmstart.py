@@ -1,0 +1,65 @@
+"""Learned warm start inside the solver (GPU).
+
+* record mode leaves the step's features and its realised enthalpy/pressure
+  increments in the device buffers (checked against the fields read back);
+* a network trained on solver-generated pairs from four single-track decks
+  (energy equation only: these steps converge before the iteration limit),
+  then used as the starting guess of a held-out deck, needs fewer outer
+  iterations per step than the plain solve, and its temperature field stays
+  as close to a tightly converged solve (up to 200 outer iterations a step)
+  as the plain solve's does.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _deck(tmp, name, power, speed, steps, flow=False):
+    import amcfd_decks as D
+    d = D.small(name, nx=40, ny=20, nz=14, steps=steps, power=power, speed=speed, fluid_flow=flow)
+    return d.write(str(tmp / name))
+
+
+def test_record_mode_targets_are_the_step_increments(tmp_path):
+    import amcfd
+    import amcfd_warmstart as W
+    path = _deck(tmp_path, "rec", 300.0, 1.0, 4, flow=True)
+    s = amcfd.Solver(amcfd.Deck(path), order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP64)
+    net = amcfd.Net(seed=1)
+    s.ws_attach(net, amcfd.WS_RECORD)
+    f, t = s.ws_buffers()
+    nk, nj, ni = s.shape
+    n = ni * nj * nk
+    q = amcfd.Deck(path).params
+    # enthalpy at the liquidus (DomainManager.cpp:252-254 with the mean cp)
+    hlcal = q.hsmelt + 0.5 * (q.acpa * q.tsolid + q.acpb + q.acpl) * (q.tliquid - q.tsolid)
+    for _ in range(3):
+        h0, p0 = s.get("enthalpy"), s.get("pressure")
+        s.step()
+        h1, p1 = s.get("enthalpy"), s.get("pressure")
+        tt = W.device_view(t, (n, 2)).cpu().numpy()
+        dh, dp = (h1 - h0).reshape(-1), (p1 - p0).reshape(-1)
+        assert np.allclose(tt[:, 0] * 0.1 * hlcal, dh, rtol=1e-5, atol=1e-6 * np.abs(dh).max())
+        assert np.allclose(tt[:, 1] * 1e4, dp, rtol=1e-5, atol=1e-6 * max(np.abs(dp).max(), 1e-30))
+        ff = W.device_view(f, (n, 11)).cpu().numpy()
+        assert np.isfinite(ff).all()
+    s.close()
+    net.close()
+
+
+def test_trained_warm_start_saves_outer_iterations(tmp_path):
+    import amcfd
+    import amcfd_warmstart as W
+    train = [_deck(tmp_path, f"t{q}", P, v, 50) for q, (P, v) in
+             enumerate([(250.0, 0.8), (320.0, 1.0), (200.0, 1.2), (360.0, 0.6)])]
+    held = _deck(tmp_path, "held", 290.0, 0.9, 30)
+    net = amcfd.Net(seed=3)
+    losses = W.train(net, train, steps=40, lr=1e-3, updates=4)
+    assert np.isfinite(losses).all()
+    ev = W.evaluate(net, held, 25, precision=amcfd.PREC_FP32, ref_maxit=200)
+    s = ev["summary"]
+    assert s["fallback_rate"] < 0.5, s
+    assert s["iters_warm"] < s["iters_plain"], s
+    assert s["temp_err_warm"] <= 1.5 * s["temp_err_plain"] + 1e-3, s
+    net.close()
