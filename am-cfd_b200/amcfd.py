@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
             L.amcfd_net_forward.argtypes = [VP, VP, _I, _I, _I, VP]
             L.amcfd_net_backward.argtypes = [VP, VP, P(_D)]
             L.amcfd_net_adam.argtypes = [VP, C.c_float]
+            L.amcfd_net_last_ms.argtypes = [VP, P(C.c_float), P(C.c_float)]
             L.amcfd_ws_attach.argtypes = [VP, VP, _I]
             L.amcfd_ws_buffers.argtypes = [VP, P(VP), P(VP)]
             L.amcfd_ws_stats.argtypes = [VP, P(C.c_longlong), P(C.c_longlong)]
@@ -215,6 +216,12 @@ class Net:
 
     def adam(self, lr: float):
         self._check(lib().amcfd_net_adam(self._h, lr))
+
+    def last_ms(self):
+        """(forward ms, backward ms) of the last passes, from CUDA events."""
+        f, b = C.c_float(), C.c_float()
+        self._check(lib().amcfd_net_last_ms(self._h, C.byref(f), C.byref(b)))
+        return f.value, b.value
 
     def close(self):
         if self._h:

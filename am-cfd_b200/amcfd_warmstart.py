@@ -98,3 +98,70 @@ def evaluate(net: amcfd.Net, deck_path: str, steps: int, precision: int = amcfd.
         "dims_plain": p["dims"], "dims_warm": w["dims"], "dims_reference": ref["dims"],
     }
     return out
+
+
+# Tensor-core FLOPs per cell of one forward pass (padded channels, as executed):
+# 2 x 27 taps x sum over layers of cin x cout.
+FWD_FLOP_PER_CELL = 2 * 27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16)
+# input-gradient convolutions of layers 3, 2, 1 (tensor cores)
+BWD_TC_FLOP_PER_CELL = 2 * 27 * (16 * 32 + 32 * 32 + 32 * 32)
+
+
+def bench_network(dims=(202, 102, 62), reps: int = 10, device: int = 0) -> Dict:
+    """Forward/backward throughput of the network on a node grid (the config-3
+    evaluation grid by default), CUDA-event timed, random features."""
+    import torch
+    ni, nj, nk = dims
+    n = ni * nj * nk
+    g = torch.Generator(device="cuda").manual_seed(5)
+    feat = torch.randn((n, 11), device="cuda", generator=g)
+    target = torch.randn((n, 2), device="cuda", generator=g) * 0.1
+    net = amcfd.Net(device=device, seed=5)
+    for _ in range(3):
+        net.forward(feat.data_ptr(), dims)
+        net.backward(target.data_ptr())
+    f_ms, b_ms = [], []
+    for _ in range(reps):
+        net.forward(feat.data_ptr(), dims)
+        net.backward(target.data_ptr())
+        f, b = net.last_ms()
+        f_ms.append(f)
+        b_ms.append(b)
+    net.close()
+    f, b = float(np.median(f_ms)), float(np.median(b_ms))
+    return {"cells": n, "fwd_ms": f, "bwd_ms": b,
+            "fwd_tflops": FWD_FLOP_PER_CELL * n / (f * 1e-3) / 1e12,
+            "bwd_tc_tflops": BWD_TC_FLOP_PER_CELL * n / (b * 1e-3) / 1e12}
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    import os
+    import tempfile
+
+    import amcfd_decks as D
+
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--bench", action="store_true", help="network throughput on the config-3 grid")
+    ap.add_argument("--eval", type=int, default=0, help="train, then evaluate N steps of config 3")
+    ap.add_argument("--train-steps", type=int, default=60)
+    args = ap.parse_args()
+    if args.bench:
+        print(json.dumps(bench_network()))
+    if args.eval:
+        tmp = tempfile.mkdtemp(prefix="amcfd_ws_")
+        # training decks: config-2 instances (seeded draws of power, speed,
+        # radius), the smaller half of the size range to keep training short
+        decks = [d for d in D.config2(n=16, steps=args.train_steps + 1)][:8]
+        paths = [d.write(os.path.join(tmp, d.name)) for d in decks]
+        net = amcfd.Net(seed=3)
+        t0 = time.perf_counter()
+        losses = train(net, paths, steps=args.train_steps, lr=1e-3, updates=4)
+        train_s = time.perf_counter() - t0
+        held = D.config3_eval(steps=args.eval + 1).write(os.path.join(tmp, "config3"))
+        ev = evaluate(net, held, args.eval, ref_maxit=60)
+        s = ev["summary"]
+        s.update({"train_pairs": len(paths) * args.train_steps, "train_s": train_s,
+                  "loss_first": losses[0], "loss_last": losses[-1]})
+        print(json.dumps(s))

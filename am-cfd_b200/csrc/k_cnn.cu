@@ -482,6 +482,8 @@ struct amcfd_net {
     long long ncap = 0, ncell = 0;
     int ni = 0, nj = 0, nk = 0;
     long long step = 0;
+    cudaEvent_t ev[4] = {};        // forward and backward bracketing events
+    float fwd_ms = 0.f, bwd_ms = 0.f;
 };
 
 #define NCK(call)                                                                         \
@@ -549,6 +551,7 @@ int amcfd_net_create(int device, unsigned long long seed, amcfd_net **out)
         NCK(cudaMalloc(&net->wb[l], (size_t)27 * kCin[l] * kCout[l] * sizeof(__nv_bfloat16)));
     }
     NCK(cudaMalloc(&net->part, (size_t)net->sm * (27 * 32 * 32 + 32) * sizeof(float)));
+    for (auto &e : net->ev) NCK(cudaEventCreate(&e));
     NCK(cudaMalloc(&net->lpart, (size_t)net->sm * 4 * sizeof(double)));
     set_conv_smem<16, 32>();
     set_conv_smem<32, 32>();
@@ -599,6 +602,7 @@ void amcfd_net_destroy(amcfd_net *net)
     }
     for (auto a : net->act) if (a) cudaFree(a);
     for (auto a : net->grad) if (a) cudaFree(a);
+    for (auto e : net->ev) if (e) cudaEventDestroy(e);
     if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
 }
@@ -641,6 +645,7 @@ int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int
     int rc = net_reserve(net, ni, nj, nk);
     if (rc) return rc;
     const long long n = net->ncell;
+    NCK(cudaEventRecord(net->ev[0], net->stream));
     features_kernel<<<net->sm * 4, 256, 0, net->stream>>>(feat_dev, net->act[0], n, ni, nj, nk);
     const long long ntiles = (n + kM - 1) / kM;
     const int grid = (int)std::min<long long>(ntiles, net->sm);
@@ -657,9 +662,11 @@ int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int
         a.err = net->errd;
         conv(kCin[l], kCout[l], a, grid, net->stream);
     }
+    NCK(cudaEventRecord(net->ev[1], net->stream));
     NCK(cudaGetLastError());
     if (y_dev) NCK(cudaMemcpyAsync(y_dev, net->y, n * kOut * sizeof(float), cudaMemcpyDeviceToDevice, net->stream));
     NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaEventElapsedTime(&net->fwd_ms, net->ev[0], net->ev[1]));
     int e = 0;
     NCK(cudaMemcpy(&e, net->errd, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) { net->err = "tensor-core pipeline wait gave up"; return e; }
@@ -677,6 +684,7 @@ int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
     const int ni = net->ni, nj = net->nj, nk = net->nk;
     const double nint = (double)(ni - 2) * (nj - 2) * (nk - 2) * kOut;
     const int lg = net->sm;
+    NCK(cudaEventRecord(net->ev[2], net->stream));
     mse_kernel<<<lg, 256, 0, net->stream>>>(net->y, target_dev, net->grad[0], n, ni, nj, nk, 1.0 / nint,
                                             net->lpart);
     const long long ntiles = (n + kM - 1) / kM;
@@ -700,10 +708,12 @@ int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
             cur ^= 1;
         }
     }
+    NCK(cudaEventRecord(net->ev[3], net->stream));
     NCK(cudaGetLastError());
     std::vector<double> lp(lg);
     NCK(cudaMemcpyAsync(lp.data(), net->lpart, lg * sizeof(double), cudaMemcpyDeviceToHost, net->stream));
     NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaEventElapsedTime(&net->bwd_ms, net->ev[2], net->ev[3]));
     if (loss) {
         double s = 0.0;
         for (double q : lp) s += q;
@@ -712,6 +722,16 @@ int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
     int e = 0;
     NCK(cudaMemcpy(&e, net->errd, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) { net->err = "tensor-core pipeline wait gave up"; return e; }
+    return 0;
+}
+
+// Device times (CUDA events on the network's stream) of the last forward and
+// backward passes, ms.
+int amcfd_net_last_ms(const amcfd_net *net, float *fwd_ms, float *bwd_ms)
+{
+    if (!net) return AMCFD_E_ARG;
+    if (fwd_ms) *fwd_ms = net->fwd_ms;
+    if (bwd_ms) *bwd_ms = net->bwd_ms;
     return 0;
 }
 

@@ -233,6 +233,8 @@ int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int
  * all parameter gradients into the net's gradient buffer */
 int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss);
 int amcfd_net_adam(amcfd_net *net, float lr);
+/* device ms (CUDA events) of the last forward and backward passes */
+int amcfd_net_last_ms(const amcfd_net *net, float *fwd_ms, float *bwd_ms);
 
 /* Attach a warm-start network to a solver context (same device).  Modes:
  * AMCFD_WS_OFF; AMCFD_WS_PREDICT: each step starts from the network's predicted
