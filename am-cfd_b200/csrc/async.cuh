@@ -28,6 +28,18 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Arrival count n: completes a phase once n threads have arrived.
+__device__ __forceinline__ void mbar_init_n(uint64_t *bar, uint32_t n)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(n) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
@@ -83,6 +95,12 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z),
           "r"(smem_u32(bar)) : "memory");
 }
+
+// Host: tiled 3-D tensor map (zero fill out of range); dims innermost first,
+// strides in bytes of dims 1 and 2; swizzle_bytes 0 (none), 32, 64 or 128.
+// Returns 0 or a CUDA driver error code.
+int encode_tiled_3d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base, const uint64_t dims[3],
+                    const uint64_t strides[2], const uint32_t box[3], int swizzle_bytes);
 
 // Host: tiled 3-D tensor map over a padded field [nk][nj][nip] of `elem`-byte
 // elements, box (bx, by, 1).  Returns 0 or a CUDA driver error code.

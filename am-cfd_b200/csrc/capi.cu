@@ -33,8 +33,8 @@ template <typename T> void ws_apply(Inst<T> &I, const float *y, double alpha, in
 template <typename T> void ws_target(Inst<T> &I, T *const *save, float *target);
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
-int encode_field_map(CUtensorMap *map, const void *base, int elem, int nip, int nj, int nk, int bx,
-                     int by)
+int encode_tiled_3d(CUtensorMap *map, CUtensorMapDataType dtype, const void *base, const uint64_t dims[3],
+                    const uint64_t strides[2], const uint32_t box[3], int swizzle_bytes)
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     if (!fn) {
@@ -46,15 +46,27 @@ int encode_field_map(CUtensorMap *map, const void *base, int elem, int nip, int 
             return -1;
         fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
     }
-    const cuuint64_t dims[3] = {(cuuint64_t)nip, (cuuint64_t)nj, (cuuint64_t)nk};
-    const cuuint64_t strides[2] = {(cuuint64_t)nip * elem, (cuuint64_t)nip * nj * elem};
-    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint64_t d[3] = {dims[0], dims[1], dims[2]};
+    const cuuint64_t st[2] = {strides[0], strides[1]};
+    const cuuint32_t bx[3] = {box[0], box[1], box[2]};
     const cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = fn(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
-                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = fn(map, dtype, 3, const_cast<void *>(base), d, st, bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    swizzle_bytes == 128 ? CU_TENSOR_MAP_SWIZZLE_128B
+                    : swizzle_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                    : swizzle_bytes == 32 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                          : CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : (int)r;
+}
+
+int encode_field_map(CUtensorMap *map, const void *base, int elem, int nip, int nj, int nk, int bx,
+                     int by)
+{
+    const uint64_t dims[3] = {(uint64_t)nip, (uint64_t)nj, (uint64_t)nk};
+    const uint64_t strides[2] = {(uint64_t)nip * elem, (uint64_t)nip * nj * elem};
+    const uint32_t box[3] = {(uint32_t)bx, (uint32_t)by, 1};
+    return encode_tiled_3d(map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                           base, dims, strides, box, 0);
 }
 }  // namespace amcfd
 

@@ -37,7 +37,8 @@
 namespace amcfd {
 namespace cnn {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 256;      // weight-gradient kernel
+constexpr int kConvThreads = 160;  // convolution kernel: four epilogue warps + one TMA/MMA warp
 constexpr int kM = 128;  // cells per tile
 constexpr int kR = 136;  // rows per (dk, dj) group: 128 + 2 halo, rounded up to 8
 constexpr int kG = 9;    // (dk, dj) groups
@@ -47,13 +48,19 @@ constexpr int kCout[kLayers] = {32, 32, 32, 16};
 constexpr int kFeat = 11;  // real input channels
 constexpr int kOut = 2;   // real output channels
 
+constexpr int kStages = 6;  // shared-memory ring of A units
+
 template <int CIN, int COUT> struct ConvSmem {
-    static constexpr int A_BYTES = (CIN / 8) * kG * kR * 16;
+    static constexpr int ROW = CIN * 2;                             // bytes per cell (one swizzled row)
+    static constexpr int SLAB = (kR * ROW + 1023) / 1024 * 1024;    // one row group, 1 KiB aligned
+    static constexpr int U_BYTES = 3 * SLAB;                        // one unit: three row groups
     static constexpr int B_BYTES = 27 * CIN * COUT * 2;
-    static constexpr size_t BYTES = 2 * (size_t)A_BYTES + B_BYTES + 64 + 128;
+    // ring + weights + (2 kStages + 4) barriers + TMEM slot + alignment slack
+    static constexpr size_t BYTES = (size_t)kStages * U_BYTES + B_BYTES + 8 * (2 * kStages + 4) + 16 + 1024;
 };
 
 struct ConvArgs {
+    CUtensorMap xmap;         // x as [cell][CIN], box CIN x kR, rows swizzled (32 or 64 B)
     const __nv_bfloat16 *x;   // [ncell][CIN]
     const __nv_bfloat16 *w;   // packed [27][CIN/8][COUT][8]
     const float *bias;        // [COUT] or null
@@ -68,16 +75,21 @@ struct ConvArgs {
 };
 
 // ---- tensor-core plumbing (PTX) ------------------------------------------------
-// Shared-memory matrix descriptor, K-major, no swizzle: core matrices of 8 rows
-// x 16 bytes stored as 128 contiguous bytes; lbo = byte distance between the two
-// K-adjacent core matrices of one K=16 slice, sbo = between 8-row groups.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+// Shared-memory matrix descriptor, K-major.  No swizzle (the weights): core
+// matrices of 8 rows x 16 bytes stored as 128 contiguous bytes; lbo = byte
+// distance between the two K-adjacent core matrices of one K=16 slice, sbo =
+// between 8-row groups.  Swizzled (the activations): rows of CIN*2 bytes in the
+// TMA's 32/64-byte swizzle, sbo = 8 rows.  The swizzle is a function of the
+// shared-memory address, so an operand may start any whole row or 32 bytes
+// into a 1 KiB-aligned slab.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout = 0)
 {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
     d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
-    return d;                // base offset 0, no swizzle
+    d |= (uint64_t)1 << 46;         // descriptor version of sm_100
+    d |= (uint64_t)layout << 61;    // 0 no swizzle, 6 = 32-byte, 4 = 64-byte swizzle
+    return d;                       // base offset 0
 }
 // Instruction descriptor, kind::f16: D F32, A and B BF16, both K-major, M = 128.
 template <int N> __host__ __device__ constexpr uint32_t idesc_bf16()
@@ -132,67 +144,135 @@ __device__ __forceinline__ bool interior_cell(long long c, int ni, int nj, int n
     return i >= 1 && i <= ni - 2 && j >= 1 && j <= nj - 2 && k >= 1 && k <= nk - 2;
 }
 
-// Nine (dk, dj) groups of kR consecutive cells starting one cell before the
-// tile, stored chunk-major: element (row r, channel c) of group g at byte
-// ((c/8 * kG + g) * kR + r) * 16 + (c%8) * 2.
-template <int CIN>
-__device__ __forceinline__ void gather_tile(const __nv_bfloat16 *x, long long ncell, int ni, int nj,
-                                            long long c0, unsigned char *A)
+// Operand A of a tile, by thirds: unit (tile, dk) holds the three (dj) row
+// groups of kR consecutive cells, starting one cell before the tile, of plane
+// offset dk: slab j (1 KiB aligned) holds rows of CIN channels (CIN*2 bytes)
+// as the TMA's swizzled box of the activation [cell][CIN] (rows outside the
+// grid read zeros).
+template <int CIN, int COUT>
+__device__ __forceinline__ void tma_unit(const CUtensorMap *xmap, long long c0, int dk, int plane, int ni,
+                                         unsigned char *A, uint64_t *bar)
 {
-    constexpr int KC = CIN / 8;
-    const long long plane = (long long)ni * nj;
-    for (int idx = threadIdx.x; idx < kG * kR * KC; idx += blockDim.x) {
-        const int r = idx % kR, rest = idx / kR, g = rest % kG, kc = rest / kG;
-        const int dk = g / 3 - 1, dj = g % 3 - 1;
-        const long long s = c0 - 1 + r + dk * plane + (long long)dj * ni;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (s >= 0 && s < ncell) v = *reinterpret_cast<const uint4 *>(x + s * CIN + kc * 8);
-        *reinterpret_cast<uint4 *>(A + ((size_t)(kc * kG + g) * kR + r) * 16) = v;
+    using S = ConvSmem<CIN, COUT>;
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)(3 * kR * S::ROW));
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const int row0 = (int)(c0 - 1 + (long long)dk * plane + (long long)(j - 1) * ni);
+        tma_load_3d(A + (size_t)j * S::SLAB, xmap, 0, row0, 0, bar);
     }
 }
 
+// The MMAs of one unit: taps (dk, dj, di) for its dk, 3 x 3 taps x CIN/16
+// slices; tap di starts di rows into its slab, slice s 32 bytes into the row.
 template <int CIN, int COUT>
-__device__ __forceinline__ void issue_tile(uint32_t a_base, uint32_t b_base, uint32_t tmem_d)
+__device__ __forceinline__ void issue_unit(uint32_t a_base, uint32_t b_base, int dk, uint32_t tmem_d,
+                                           bool first)
 {
+    using S = ConvSmem<CIN, COUT>;
     constexpr uint32_t idesc = idesc_bf16<COUT>();
-    constexpr uint32_t lbo_a = kG * kR * 16, lbo_b = COUT * 16;
-    bool first = true;
-    for (int g = 0; g < kG; ++g)
+    constexpr uint32_t layout = CIN == 32 ? 4u : 6u;  // 64- / 32-byte swizzle
+    const uint64_t a0 = smem_desc(a_base, 16, 8 * S::ROW, layout), b0 = smem_desc(b_base, COUT * 16, 128);
+    uint32_t acc = first ? 0u : 1u;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
         for (int di = 0; di < 3; ++di) {
-            const int t = g * 3 + di;
+            const int t = (dk + 1) * 9 + j * 3 + di;
 #pragma unroll
             for (int s = 0; s < CIN / 16; ++s) {
-                const uint32_t a = a_base + (uint32_t)(((2 * s * kG + g) * kR + di) * 16);
-                const uint32_t b = b_base + (uint32_t)(t * CIN * COUT * 2 + 2 * s * COUT * 16);
-                mma_bf16(tmem_d, smem_desc(a, lbo_a, 128), smem_desc(b, lbo_b, 128), idesc, first ? 0u : 1u);
-                first = false;
+                const uint64_t a = a0 + (uint64_t)((j * S::SLAB + di * S::ROW + s * 32) >> 4);
+                const uint64_t b = b0 + (uint64_t)((t * CIN * COUT * 2 + 2 * s * COUT * 16) >> 4);
+                mma_bf16(tmem_d, a, b, idesc, acc);
+                acc = 1u;
             }
         }
 }
 
+// Epilogue of one tile by four warps: accumulator row m = TMEM lane m = cell
+// c0 + m; bias, ReLU, input-gradient gate, boundary nodes to zero; BF16 store
+// (and FP32 copy of the first n32 channels).
+template <int COUT>
+__device__ __forceinline__ void epilogue(const ConvArgs &args, long long c0, uint32_t taddr)
+{
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t r[COUT];
+    tmem_ld<COUT>(taddr + ((uint32_t)(32 * warp) << 16), r);
+    tmem_wait_ld();
+    const long long cell = c0 + 32 * warp + lane;
+    if (cell >= args.ncell) return;
+    const bool in = interior_cell(cell, args.ni, args.nj, args.nk);
+    float v[COUT];
+#pragma unroll
+    for (int c = 0; c < COUT; ++c) {
+        float x = __uint_as_float(r[c]);
+        if (args.bias) x += args.bias[c];
+        if (args.relu) x = fmaxf(x, 0.f);
+        v[c] = in ? x : 0.f;
+    }
+    if (args.gate) {
+        const uint4 *gp = reinterpret_cast<const uint4 *>(args.gate + cell * COUT);
+#pragma unroll
+        for (int c = 0; c < COUT; c += 8) {
+            uint4 gv = gp[c / 8];
+            const __nv_bfloat16 *gh = reinterpret_cast<const __nv_bfloat16 *>(&gv);
+#pragma unroll
+            for (int e = 0; e < 8; ++e)
+                if (!(__bfloat162float(gh[e]) > 0.f)) v[c + e] = 0.f;
+        }
+    }
+    __nv_bfloat16 *yp = args.y + cell * COUT;
+#pragma unroll
+    for (int c = 0; c < COUT; c += 8) {
+        __nv_bfloat162 h[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[c + 2 * e], v[c + 2 * e + 1]);
+        *reinterpret_cast<uint4 *>(yp + c) = *reinterpret_cast<uint4 *>(h);
+    }
+    if (args.y32)
+#pragma unroll
+        for (int c = 0; c < COUT; ++c)
+            if (c < args.n32) args.y32[cell * args.n32 + c] = v[c];
+}
+
+// One CTA per SM walks tiles it = 0, 1, ... (cells (blockIdx.x + it*gridDim.x)*128 ...).
+// Warp 4 (one thread) streams units (tile, dk) through a ring of kStages
+// shared-memory stages with TMA and issues their MMAs; warps 0-3 run the
+// epilogues.  mbarriers: loaded[s] (TMA bytes), freed[s] (the MMAs reading
+// stage s are done), full[b] (accumulator b holds a finished tile), drained[b]
+// (the 128 epilogue threads have read accumulator b).  Every wait is bounded.
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kThreads, 1) conv_tc_kernel(ConvArgs args)
+__global__ void __launch_bounds__(kConvThreads, 1) conv_tc_kernel(const __grid_constant__ ConvArgs args)
 {
     using S = ConvSmem<CIN, COUT>;
-    extern __shared__ __align__(128) unsigned char smraw[];
-    unsigned char *base = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
-    unsigned char *A0 = base, *A1 = base + S::A_BYTES, *Bs = base + 2 * S::A_BYTES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Bs + S::B_BYTES);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    unsigned char *base = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    unsigned char *Bs = base + (size_t)kStages * S::U_BYTES;
+    uint64_t *loaded = reinterpret_cast<uint64_t *>(Bs + S::B_BYTES);
+    uint64_t *freed = loaded + kStages, *full = freed + kStages, *drained = full + 2;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(drained + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr uint32_t kCols = COUT * 2 < 32 ? 32 : COUT * 2;  // two accumulators
     const long long ntiles = (args.ncell + kM - 1) / kM;
+    const long long nmy = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int plane = args.ni * args.nj;
+    auto tile_c0 = [&](long long it) { return (blockIdx.x + it * (long long)gridDim.x) * kM; };
 
     if (tid == 0) {
-        mbar_init(&bar[0]);
-        mbar_init(&bar[1]);
+        for (int q = 0; q < kStages; ++q) {
+            mbar_init(&loaded[q]);
+            mbar_init(&freed[q]);
+        }
+        for (int q = 0; q < 2; ++q) {
+            mbar_init(&full[q]);
+            mbar_init_n(&drained[q], 128);
+        }
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
                      ::"r"(smem_u32(tslot)), "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // weights: whole layer into shared memory
     for (int q = tid; q < S::B_BYTES / 16; q += blockDim.x)
         reinterpret_cast<uint4 *>(Bs)[q] = reinterpret_cast<const uint4 *>(args.w)[q];
     fence_proxy_async();
@@ -200,76 +280,62 @@ __global__ void __launch_bounds__(kThreads, 1) conv_tc_kernel(ConvArgs args)
     __syncthreads();
     tc_after_sync();
     const uint32_t tbase = *tslot;
-    const uint32_t a_addr[2] = {smem_u32(A0), smem_u32(A1)};
-    const uint32_t b_addr = smem_u32(Bs);
-    unsigned char *Abuf[2] = {A0, A1};
-
-    long long q = blockIdx.x;
-    if (q < ntiles) gather_tile<CIN>(args.x, args.ncell, args.ni, args.nj, q * kM, A0);
-    fence_proxy_async();
-    __syncthreads();
-    if (tid == 0 && q < ntiles) {
-        tc_after_sync();
-        issue_tile<CIN, COUT>(a_addr[0], b_addr, tbase);
-        mma_commit(&bar[0]);
-    }
     bool ok = true;
-    int it = 0;
-    for (; q < ntiles; q += gridDim.x, ++it) {
-        const long long qn = q + gridDim.x;
-        const int b = it & 1, bn = b ^ 1;
-        if (qn < ntiles) gather_tile<CIN>(args.x, args.ncell, args.ni, args.nj, qn * kM, Abuf[bn]);
-        fence_proxy_async();
-        __syncthreads();
-        if (tid == 0 && qn < ntiles) {
-            tc_after_sync();
-            issue_tile<CIN, COUT>(a_addr[bn], b_addr, tbase + (uint32_t)(bn * COUT));
-            mma_commit(&bar[bn]);
-        }
-        ok = mbar_try(&bar[b], (uint32_t)((it >> 1) & 1), kSpinLimit);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
+
+    if (warp == 4) {
+        if (lane == 0) {
+            const long long nunits = nmy * 3;
+            const uint32_t b_addr = smem_u32(Bs);
+            auto load = [&](long long v) {
+                const int s = (int)(v % kStages);
+                tma_unit<CIN, COUT>(&args.xmap, tile_c0(v / 3), (int)(v % 3) - 1, plane, args.ni,
+                                    base + (size_t)s * S::U_BYTES, &loaded[s]);
+            };
+            long long ul = 0, u = 0;  // units loaded, units whose MMAs are issued
+            for (; ul < nunits && ul < kStages; ++ul) load(ul);
+            for (; u < nunits; ++u) {
+                const int s = (int)(u % kStages);
+                const long long it = u / 3;
+                const int dk = (int)(u % 3) - 1, b = (int)(it & 1);
+                ok = mbar_try(&loaded[s], (uint32_t)((u / kStages) & 1), kSpinLimit);
+                if (ok && dk == -1 && it >= 2)  // accumulator b: epilogue of tile it - 2 done
+                    ok = mbar_try(&drained[b], (uint32_t)(((it - 2) >> 1) & 1), kSpinLimit);
+                if (!ok) break;
+                tc_after_sync();
+                issue_unit<CIN, COUT>(smem_u32(base + (size_t)s * S::U_BYTES), b_addr, dk,
+                                      tbase + (uint32_t)(b * COUT), dk == -1);
+                mma_commit(&freed[s]);
+                if (dk == 1) mma_commit(&full[b]);
+                // refill the stage of unit u - 1 (its MMAs run ahead of unit u's)
+                if (u >= 1 && ul < nunits) {
+                    const int sp = (int)((u - 1) % kStages);
+                    ok = mbar_try(&freed[sp], (uint32_t)(((u - 1) / kStages) & 1), kSpinLimit);
+                    if (!ok) { ++u; break; }
+                    load(ul++);
+                }
+            }
+            if (!ok) {
                 atomicExch(args.err, AMCFD_E_TIMEOUT);
-                if (qn < ntiles) mbar_try(&bar[bn], (uint32_t)(((it + 1) >> 1) & 1), kSpinLimit);
+                for (long long v = u; v < ul; ++v)  // loads issued, not consumed
+                    mbar_try(&loaded[v % kStages], (uint32_t)((v / kStages) & 1), kSpinLimit);
             }
-            break;
+            // the last MMA batch of each stage completes before the CTA releases its memory
+            for (long long v = (u > kStages ? u - kStages : 0); v < u; ++v)
+                mbar_try(&freed[v % kStages], (uint32_t)((v / kStages) & 1), kSpinLimit);
         }
-        tc_after_sync();
-        if (warp < 4) {
-            uint32_t r[COUT];
-            tmem_ld<COUT>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)(b * COUT), r);
-            tmem_wait_ld();
-            const long long cell = q * kM + 32 * warp + lane;
-            if (cell < args.ncell) {
-                const bool in = interior_cell(cell, args.ni, args.nj, args.nk);
-                float v[COUT];
-#pragma unroll
-                for (int c = 0; c < COUT; ++c) {
-                    float x = __uint_as_float(r[c]);
-                    if (args.bias) x += args.bias[c];
-                    if (args.relu) x = fmaxf(x, 0.f);
-                    v[c] = in ? x : 0.f;
-                }
-                if (args.gate) {
-                    const __nv_bfloat16 *gp = args.gate + cell * COUT;
-#pragma unroll
-                    for (int c = 0; c < COUT; ++c)
-                        if (!(__bfloat162float(gp[c]) > 0.f)) v[c] = 0.f;
-                }
-                __nv_bfloat16 *yp = args.y + cell * COUT;
-#pragma unroll
-                for (int c = 0; c < COUT; c += 8) {
-                    __nv_bfloat162 h[4];
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(v[c + 2 * e], v[c + 2 * e + 1]);
-                    *reinterpret_cast<uint4 *>(yp + c) = *reinterpret_cast<uint4 *>(h);
-                }
-                if (args.y32)
-                    for (int c = 0; c < args.n32; ++c) args.y32[cell * args.n32 + c] = v[c];
+        __syncwarp();
+    } else {
+        for (long long it = 0; it < nmy; ++it) {
+            const int b = (int)(it & 1);
+            if (!mbar_try(&full[b], (uint32_t)((it >> 1) & 1), kSpinLimit)) {
+                if (tid == 0) atomicExch(args.err, AMCFD_E_TIMEOUT);
+                break;
             }
+            tc_after_sync();
+            epilogue<COUT>(args, tile_c0(it), tbase + (uint32_t)(b * COUT));
+            tc_before_sync();
+            mbar_arrive(&drained[b]);
         }
-        tc_before_sync();
-        __syncthreads();
     }
     tc_before_sync();
     __syncthreads();
@@ -432,15 +498,20 @@ template <int CIN, int COUT> void set_conv_smem()
 
 template <int CIN, int COUT> void launch_conv(const ConvArgs &a, int grid, cudaStream_t s)
 {
-    conv_tc_kernel<CIN, COUT><<<grid, kThreads, ConvSmem<CIN, COUT>::BYTES, s>>>(a);
+    conv_tc_kernel<CIN, COUT><<<grid, kConvThreads, ConvSmem<CIN, COUT>::BYTES, s>>>(a);
 }
 
-static void conv(int cin, int cout, const ConvArgs &a, int grid, cudaStream_t s)
+static int conv(int cin, int cout, ConvArgs a, int grid, cudaStream_t s)
 {
+    const uint64_t dims[3] = {(uint64_t)cin, (uint64_t)a.ncell, 1};
+    const uint64_t strides[2] = {(uint64_t)cin * 2, (uint64_t)cin * 2 * (uint64_t)a.ncell};
+    const uint32_t box[3] = {(uint32_t)cin, (uint32_t)kR, 1};
+    if (encode_tiled_3d(&a.xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, a.x, dims, strides, box, cin * 2)) return -1;
     if (cin == 16 && cout == 32) launch_conv<16, 32>(a, grid, s);
     else if (cin == 32 && cout == 32) launch_conv<32, 32>(a, grid, s);
     else if (cin == 32 && cout == 16) launch_conv<32, 16>(a, grid, s);
     else if (cin == 16 && cout == 16) launch_conv<16, 16>(a, grid, s);
+    return 0;
 }
 
 static void wgrad(int cin, int cout, const __nv_bfloat16 *x, const __nv_bfloat16 *dz, long long ncell, int ni,
@@ -660,7 +731,10 @@ int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int
         a.n32 = kOut;
         a.ni = ni; a.nj = nj; a.nk = nk; a.ncell = n;
         a.err = net->errd;
-        conv(kCin[l], kCout[l], a, grid, net->stream);
+        if (conv(kCin[l], kCout[l], a, grid, net->stream)) {
+            net->err = "tensor-map encoding failed";
+            return AMCFD_E_CUDA;
+        }
     }
     NCK(cudaEventRecord(net->ev[1], net->stream));
     NCK(cudaGetLastError());
@@ -704,7 +778,10 @@ int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
             a.y = net->grad[cur ^ 1];
             a.ni = ni; a.nj = nj; a.nk = nk; a.ncell = n;
             a.err = net->errd;
-            conv(kCout[l], kCin[l], a, grid, net->stream);
+            if (conv(kCout[l], kCin[l], a, grid, net->stream)) {
+                net->err = "tensor-map encoding failed";
+                return AMCFD_E_CUDA;
+            }
             cur ^= 1;
         }
     }
