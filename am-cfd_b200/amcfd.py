@@ -130,6 +130,12 @@ def lib() -> C.CDLL:
             L.amcfd_net_backward.argtypes = [VP, VP, P(_D)]
             L.amcfd_net_adam.argtypes = [VP, C.c_float]
             L.amcfd_net_last_ms.argtypes = [VP, P(C.c_float), P(C.c_float)]
+            L.amcfd_writer_create.argtypes = [VP, VP, C.c_char_p, P(VP)]
+            for f in ("step", "finish"):
+                getattr(L, "amcfd_writer_" + f).argtypes = [VP]
+            L.amcfd_writer_last_error.argtypes = [VP]
+            L.amcfd_writer_last_error.restype = C.c_char_p
+            L.amcfd_writer_destroy.argtypes = [VP]
             L.amcfd_ws_attach.argtypes = [VP, VP, _I]
             L.amcfd_ws_buffers.argtypes = [VP, P(VP), P(VP)]
             L.amcfd_ws_stats.argtypes = [VP, P(C.c_longlong), P(C.c_longlong)]
@@ -167,6 +173,42 @@ class Deck:
     def close(self):
         if self._h:
             lib().amcfd_deck_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Writer:
+    """The reference's output files for a run (amcfd_writer_*): .vts/.pvd,
+    _Residuals.txt and the final-geometry file, under `root` (default: the
+    working directory)."""
+
+    def __init__(self, solver: "Solver", deck: "Deck", root: Optional[str] = None):
+        self._solver, self._deck = solver, deck
+        self._h = C.c_void_p()
+        rc = lib().amcfd_writer_create(solver._h, deck._h, root.encode() if root else None, C.byref(self._h))
+        if rc != 0:
+            raise AmcfdError(rc, lib().amcfd_writer_last_error(self._h).decode() if self._h else "writer")
+
+    def _check(self, rc: int) -> int:
+        if rc < 0:
+            raise AmcfdError(rc, lib().amcfd_writer_last_error(self._h).decode())
+        return rc
+
+    def step(self) -> bool:
+        """After each Solver.step(); True when an output was written."""
+        return self._check(lib().amcfd_writer_step(self._h)) == 1
+
+    def finish(self):
+        self._check(lib().amcfd_writer_finish(self._h))
+
+    def close(self):
+        if self._h:
+            lib().amcfd_writer_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

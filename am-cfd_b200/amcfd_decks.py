@@ -91,6 +91,8 @@ class Deck:
     heat_table: Optional[List[Tuple[float, float, float, float, float, float]]] = None
     # *CONTROL_TIMESTEP_VARIABLE rows (t, dt, output interval)
     vardt: Optional[List[Tuple[float, float, float]]] = None
+    # *OUTPUT_FINAL_GEOMETRY file name (None: not requested)
+    final_geometry: Optional[str] = None
 
     @property
     def cells(self) -> Tuple[int, int, int]:
@@ -166,6 +168,8 @@ class Deck:
                 for row in self.vardt:
                     f.write(" ".join(repr(float(v)) for v in row) + "\n")
             lines += ["*CONTROL_TIMESTEP_VARIABLE", ref(tab)]
+        if self.final_geometry is not None:
+            lines += ["*OUTPUT_FINAL_GEOMETRY", self.final_geometry]
         lines += ["*MESH_FILE", ref(mesh)]
         if self.toolpath is not None:
             crs = os.path.join(directory, f"{self.name}.crs")

@@ -26,6 +26,7 @@ dim3 energy_assemble_grid(const Params &p);
 template <typename T> int h2t_blocks_per_sm();
 template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
                                              long long rows, int sm_count, cudaStream_t s);
+template <typename T> void launch_centre_velocity(Inst<T> &I, int comp, double *dst);
 template <typename T> void ws_features(Inst<T> &I, float *feat, const float *prev, double bx, double by,
                                        double power);
 template <typename T> void ws_copy(Inst<T> &I, T *const *save, int dir);
@@ -901,6 +902,56 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
     return 0;
 }
 
+}  // extern "C"
+
+// ---- internal accessors for the output writer (output.cu) -------------------------------
+extern "C" {
+static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr);
+}
+namespace amcfd {
+void ctx_report(amcfd_ctx *ctx, amcfd_step_report *r) { fill_report(ctx, r); }
+double ctx_delt(const amcfd_ctx *ctx) { return ctx->delt; }
+double ctx_outtime(const amcfd_ctx *ctx) { return ctx->outtime; }
+const amcfd_params &ctx_params(const amcfd_ctx *ctx) { return ctx->prm; }
+void ctx_grid(const amcfd_ctx *ctx, const std::vector<double> **x, const std::vector<double> **y,
+              const std::vector<double> **z)
+{
+    *x = &ctx->x; *y = &ctx->y; *z = &ctx->z;
+}
+// boundary heat fluxes of the last outer iteration: north south top bottom west east
+void ctx_fluxes(const amcfd_ctx *ctx, double f[6])
+{
+    const Status *s = ctx->st_host;
+    f[0] = s->fluxnorth; f[1] = s->fluxsouth; f[2] = s->fluxtop;
+    f[3] = s->fluxbottom; f[4] = s->fluxwest; f[5] = s->fluxeast;
+}
+// plane k of a field, FP64 [nj][ni]
+int ctx_plane(amcfd_ctx *ctx, const char *name, int k, std::vector<double> &out)
+{
+    void *d;
+    int rc;
+    if ((rc = field_ptr(ctx, name, &d))) return rc;
+    if (k < 0 || k >= ctx->nk) return fail(ctx, AMCFD_E_ARG, "plane index out of range");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t ni = ctx->ni, nj = ctx->nj, nip = ctx->nip;
+    out.resize(ni * nj);
+    if (ctx->precision == AMCFD_PREC_FP64) {
+        CK(cudaMemcpy2D(out.data(), ni * sizeof(double), (const double *)d + (size_t)k * nj * nip,
+                        nip * sizeof(double), ni * sizeof(double), nj, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(ni * nj);
+        CK(cudaMemcpy2D(tmp.data(), ni * sizeof(float), (const float *)d + (size_t)k * nj * nip,
+                        nip * sizeof(float), ni * sizeof(float), nj, cudaMemcpyDeviceToHost));
+        for (size_t q = 0; q < tmp.size(); ++q) out[q] = tmp[q];
+    }
+    return 0;
+}
+const char *ctx_error(const amcfd_ctx *ctx) { return ctx->err.c_str(); }
+}  // namespace amcfd
+
+extern "C" {
+
 int amcfd_ws_attach(amcfd_ctx *ctx, amcfd_net *net, int mode)
 {
     if (!ctx || mode < AMCFD_WS_OFF || mode > AMCFD_WS_PREDICT_H || (mode != AMCFD_WS_OFF && !net))
@@ -1017,9 +1068,11 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
 int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
 {
     if (!ctx || !name || !host_out) return AMCFD_E_ARG;
-    void *d;
+    void *d = nullptr;
     int rc;
-    if ((rc = field_ptr(ctx, name, &d))) return rc;
+    // the output writer's cell-centred velocities (PrintManager.cpp:283-285)
+    const int centre = !strcmp(name, "auvel") ? 0 : !strcmp(name, "avvel") ? 1 : !strcmp(name, "awvel") ? 2 : -1;
+    if (centre < 0 && (rc = field_ptr(ctx, name, &d))) return rc;
     CK(cudaSetDevice(ctx->device));
     const long long rows = (long long)ctx->nj * ctx->nk;
     const size_t bytes = (size_t)rows * ctx->ni * sizeof(double);
@@ -1028,7 +1081,12 @@ int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
         CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device));
     }
     // widen and pack on the device, then one contiguous copy (full speed into pinned memory)
-    if (ctx->precision == AMCFD_PREC_FP64)
+    if (centre >= 0) {
+        if (ctx->precision == AMCFD_PREC_FP64)
+            launch_centre_velocity<double>(ctx->I64, centre, ctx->pack);
+        else
+            launch_centre_velocity<float>(ctx->I32, centre, ctx->pack);
+    } else if (ctx->precision == AMCFD_PREC_FP64)
         launch_pack_field<double>((const double *)d, ctx->pack, ctx->ni, ctx->nip, rows, ctx->sm_count,
                                   ctx->stream);
     else

@@ -62,6 +62,7 @@ struct amcfd_deck {
     std::string path, keyword_id, directory = "Results", mesh_file, tool_file, heat_table_file,
                                   vardt_file, geom_out;
     std::vector<std::string> scalar_out, vector_out, cell_out;
+    mutable std::string scalar_joined, vector_joined;
     std::vector<double> tool_txyz, heattable, vardt;
     std::vector<int> tool_on, tool_id;
     bool output_geometry = false, output_tec = false;
@@ -344,6 +345,14 @@ extern "C" const char *amcfd_deck_string(const amcfd_deck *d, const char *what)
     if (!strcmp(what, "directory")) return d->directory.c_str();
     if (!strcmp(what, "geometry_file")) return d->output_geometry ? d->geom_out.c_str() : nullptr;
     if (!strcmp(what, "mesh_file")) return d->mesh_file.c_str();
+    // space-separated *SCALAR_OUT / *VECTOR_OUT names (Mesh.cpp:316-325)
+    if (!strcmp(what, "scalar_out") || !strcmp(what, "vector_out")) {
+        const auto &v = what[0] == 's' ? d->scalar_out : d->vector_out;
+        std::string &j = what[0] == 's' ? d->scalar_joined : d->vector_joined;
+        j.clear();
+        for (size_t q = 0; q < v.size(); ++q) j += (q ? " " : "") + v[q];
+        return j.c_str();
+    }
     return nullptr;
 }
 

@@ -701,6 +701,35 @@ template <typename T> void launch_pack_field(const T *src, double *dst, int ni, 
     pack_field_kernel<T><<<sm_count * 4, 256, 0, s>>>(src, dst, ni, nip, rows);
 }
 
+// Cell-centred velocity for output (vtsBinWriter::transferVelNodes,
+// vtsBinWriter.cpp:497-522): the mean of the two faces of component `comp`
+// (0 u, 1 v, 2 w) on interior nodes, zero where T <= T_solidus and on the
+// boundary nodes, packed to FP64 [k][j][ni].
+template <typename T>
+__global__ void centre_velocity_kernel(Params p, Fields<T> g, int comp, double *dst)
+{
+    const long long n = (long long)p.ni * p.nj * p.nk;
+    const T *f = comp == 0 ? g.uvel : comp == 1 ? g.vvel : g.wvel;
+    const size_t step = comp == 0 ? 1 : comp == 1 ? (size_t)p.nip : (size_t)p.nj * p.nip;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % p.ni);
+        const long long r = q / p.ni;
+        const int j = (int)(r % p.nj), k = (int)(r / p.nj);
+        double v = 0.0;
+        if (i >= 1 && i < p.nim1 && j >= 1 && j < p.njm1 && k >= 1 && k < p.nkm1) {
+            const size_t c = cidx(i, j, k, p.nj, p.nip);
+            v = ((double)f[c] + (double)f[c + step]) * 0.5;
+            if ((double)g.temp[c] <= p.tsolid) v = 0.0;
+        }
+        dst[q] = v;
+    }
+}
+template <typename T> void launch_centre_velocity(Inst<T> &I, int comp, double *dst)
+{
+    centre_velocity_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g, comp, dst);
+}
+
 // Resident 256-thread CTAs of h2t_kernel per SM (its grid is one full wave).
 template <typename T> int h2t_blocks_per_sm()
 {
@@ -735,6 +764,7 @@ template <typename T> void launch_update_solutions(Inst<T> &I)
     template void launch_h2t<T>(Inst<T> &);                 \
     template int h2t_blocks_per_sm<T>();                    \
     template void launch_pack_field<T>(const T *, double *, int, int, long long, int, cudaStream_t); \
+    template void launch_centre_velocity<T>(Inst<T> &, int, double *);                                \
     template void launch_meltpool<T>(Inst<T> &);            \
     template void launch_converge<T>(Inst<T> &, double);    \
     template void launch_update_solutions<T>(Inst<T> &);

@@ -137,7 +137,8 @@ int amcfd_deck_params(const amcfd_deck *deck, amcfd_params *out);
 const char *amcfd_deck_error(void);
 void amcfd_deck_free(amcfd_deck *deck);
 /* "keyword_id", "directory", "geometry_file" (NULL unless *OUTPUT_FINAL_GEOMETRY),
- * "mesh_file": the names PrintManager derives its output files from. */
+ * "mesh_file": the names PrintManager derives its output files from;
+ * "scalar_out", "vector_out": the requested output fields, space-separated. */
 const char *amcfd_deck_string(const amcfd_deck *deck, const char *what);
 /* sizeof(amcfd_params) / sizeof(amcfd_step_report), for bindings that mirror the structs */
 size_t amcfd_sizeof_params(void);
@@ -211,6 +212,24 @@ long long amcfd_kernel_launches(const amcfd_ctx *ctx);
  * sweep is many such runs. */
 int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nthreads,
                     amcfd_step_report *reports, int *status);
+
+/* ---- Output writer (main.cpp:92-226, PrintManager.cpp, vtsBinWriter.cpp) ------
+ * Writes what the reference's transient run writes, in its formats:
+ * <directory>/<keyword_id>_<n>.vts (VTK StructuredGrid, appended raw Float64
+ * point data of the deck's *SCALAR_OUT fields, uvel/vvel/wvel as the cell-centred
+ * auvel/avvel/awvel), <keyword_id>.pvd, <keyword_id>_Residuals.txt and, with
+ * *OUTPUT_FINAL_GEOMETRY, the final-geometry file; paths relative to `root`
+ * (NULL or "" = the working directory).  Create it before the first step: like
+ * the reference it writes the initial state as <keyword_id>_0.vts. */
+typedef struct amcfd_writer amcfd_writer;
+int amcfd_writer_create(amcfd_ctx *ctx, const amcfd_deck *deck, const char *root, amcfd_writer **out);
+/* after each amcfd_step: 1 when the output interval has passed and an output
+ * was written, 0 when not, a negative AMCFD_E_* code on failure */
+int amcfd_writer_step(amcfd_writer *w);
+/* the final output and final-geometry file (after the last step) */
+int amcfd_writer_finish(amcfd_writer *w);
+const char *amcfd_writer_last_error(const amcfd_writer *w);
+void amcfd_writer_destroy(amcfd_writer *w);
 
 /* ---- Learned warm start: a 4-layer 3x3x3 convolutional network --------------
  * No counterpart in the reference.  Layers 16->32->32->32->16 channels (9 input
