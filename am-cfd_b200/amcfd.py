@@ -27,7 +27,7 @@ ORDER_EXACT, ORDER_REDBLACK = 0, 1
 PREC_FP64, PREC_FP32 = 0, 1
 WS_OFF, WS_PREDICT, WS_RECORD, WS_PREDICT_H = 0, 1, 2, 3
 PHASES = {"laser": 1, "energy_assemble": 2, "energy_solve": 3, "h2t": 4, "meltpool": 5,
-          "momentum": 6, "converge": 7, "update": 8}
+          "momentum": 6, "converge": 7, "update": 8, "species": 9}
 ERRORS = {0: "AMCFD_OK", -1: "AMCFD_E_ARG", -2: "AMCFD_E_IO", -3: "AMCFD_E_PARSE",
           -4: "AMCFD_E_CUDA", -5: "AMCFD_E_NONFINITE", -6: "AMCFD_E_TIMEOUT",
           -7: "AMCFD_E_NOMEM", -8: "AMCFD_E_CAPACITY"}
@@ -53,7 +53,8 @@ class AmcfdParams(C.Structure):
         [("tool_txyz", C.POINTER(_D)), ("tool_on", C.POINTER(_I)), ("tool_id", C.POINTER(_I)),
          ("nheattable", _I), ("heattable", C.POINTER(_D)),
          ("nvardt", _I), ("vardt", C.POINTER(_D))] + \
-        [(n, _I) for n in "powderbed movingmesh species freesurface".split()]
+        [(n, _I) for n in "powderbed movingmesh species freesurface".split()] + \
+        [(n, _D) for n in "initconc massdiff kp urfc".split()]
 
 
 class AmcfdReport(C.Structure):
@@ -62,7 +63,7 @@ class AmcfdReport(C.Structure):
                            "heatinlaser ahtoploss accul heatout heatvol beamposx beamposy "
                            "scanvel").split()] + \
         [(n, _I) for n in ("istat iend jstat jend kstat jstart powerindicator momentum_cells "
-                           "fallback").split()]
+                           "fallback").split()] + [("resorc", _D)]
 
     def as_dict(self) -> Dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -377,7 +378,7 @@ class Solver:
         return a.value, r.value
 
     TIMING_SLOTS = ("energy_assemble", "factor", "energy_sweeps", "h2t_meltpool", "momentum",
-                    "converge", "laser", "update", "outer_iters", "sweep_launches")
+                    "converge", "laser", "update", "outer_iters", "sweep_launches", "species")
 
     def timing(self, n: int = 16) -> Dict:
         out = np.zeros(n, dtype=np.float64)

@@ -93,6 +93,9 @@ class Deck:
     vardt: Optional[List[Tuple[float, float, float]]] = None
     # *OUTPUT_FINAL_GEOMETRY file name (None: not requested)
     final_geometry: Optional[str] = None
+    # *SOLVE_SPECIES: (initial concentration, mass diffusivity, partition coefficient kp,
+    # under-relaxation urfc); its two fields are added to *SCALAR_OUT
+    species: Optional[Tuple[float, float, float, float]] = None
 
     @property
     def cells(self) -> Tuple[int, int, int]:
@@ -128,6 +131,7 @@ class Deck:
             f"ambientTemp {self.t_amb!r}", f"ambientPres {self.p_amb!r}",
             f"gasConstant {self.gas_const!r}",
             "*SCALAR_OUT", "temp", "uvel", "vvel", "wvel",
+            *(["avgconcentration", "concentration"] if self.species is not None else []),
             "*CONTROL_TERMINATION", "$ total_time max_iter nonlin_tolerance",
             f"  {self.finaltime!r} {self.maxit} {self.tol!r}",
             "*CONTROL_TIMESTEP", "$ sim_timestep output_timestep",
@@ -156,6 +160,9 @@ class Deck:
             lines += ["*BOUNDARY_EVAPORATION", "  " + " ".join(repr(float(v)) for v in self.evaporation)]
         if self.volumetric is not None:
             lines += ["*VOLUMETRIC_HEAT_SOURCE", "  " + " ".join(repr(float(v)) for v in self.volumetric)]
+        if self.species is not None:
+            lines += ["*SOLVE_SPECIES", "$ initconc massdiff kp urfc",
+                      "  " + " ".join(repr(float(v)) for v in self.species)]
         if self.heat_table is not None:
             tab = os.path.join(directory, f"{self.name}_heat.txt")
             with open(tab, "w") as f:

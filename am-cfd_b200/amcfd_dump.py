@@ -8,12 +8,12 @@ from typing import Dict, List
 import numpy as np
 
 FIELDS = ["temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp", "diff",
-          "rho", "vis", "hnot", "fraclnot"]
+          "rho", "vis", "hnot", "fraclnot", "avgconcentration", "concentration"]
 GEOM = ["x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"]
 SCALARS = ["timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "ahtoploss", "accul", "heatout",
            "heatvol", "fluxwest", "fluxeast", "fluxtop", "fluxbottom", "fluxnorth",
-           "fluxsouth", "beamposx", "beamposy", "scanvel"]
+           "fluxsouth", "beamposx", "beamposy", "scanvel", "resorc"]
 INDICES = ["istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator"]
 
 

@@ -300,6 +300,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     p.volsrc = (q.nheattable > 0 || q.heatthick > 0.0) ? 1 : 0;
     p.avolpow = q.avolpow; p.apowseta = q.apowseta; p.heatthick = q.heatthick;
     p.heatrb = q.heatrb; p.avolfact = q.avolfact;
+    p.species = q.species ? 1 : 0;
+    p.initconc = q.initconc; p.massdiff = q.massdiff; p.kp = q.kp; p.urfc = q.urfc;
 
     const size_t n3 = (size_t)p.nk * p.nj * p.nip;
     Fields<T> &g = I.g;
@@ -323,6 +325,9 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
                 &g.dux, &g.dvy, &g.dwz};
     for (auto f : f3)
         if ((rc = alloc3<T>(ctx, f, n3))) return rc;
+    if (p.species)
+        for (T **f : {&g.conc, &g.concnot, &g.concn})
+            if ((rc = alloc3<T>(ctx, f, n3))) return rc;
     if ((rc = alloc3<double>(ctx, &g.heatin, (size_t)p.nj * p.nip))) return rc;
     if (q.nheattable > 0) {
         if ((rc = alloc3<double>(ctx, &g.heattable, ctx->heattable.size()))) return rc;
@@ -416,6 +421,10 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         (rc = fill(g.diff_cur, diff0)) || (rc = fill(g.hnot, hpre)) ||
         (rc = fill(g.temp, q.temppreheat)))
         return rc;
+    // species (CFDSolverManager.cpp:474-479): every node at the initial concentration
+    if (p.species && ((rc = fill(g.conc, q.initconc)) || (rc = fill(g.concnot, q.initconc)) ||
+                      (rc = fill(g.concn, q.initconc))))
+        return rc;
     for (int k = 0; k < p.nk; k++)
         for (int j = 0; j < p.nj; j++)
             for (int i = 0; i < p.ni; i++) hv[cidx(i, j, k, p.nj, p.nip)] = hpre;
@@ -433,7 +442,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     return 0;
 }
 
-static bool phase_ok(int phase) { return phase >= 1 && phase <= 8; }
+static bool phase_ok(int phase) { return phase >= 1 && phase <= AMCFD_PHASE_SPECIES; }
 
 // ---- one outer iteration -----------------------------------------------------------------
 template <typename T>
@@ -474,7 +483,11 @@ static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
         launch_converge<T>(I, ctx->prm.nonlintol);
         swap_props<T>(I);
         break;
-    case AMCFD_PHASE_UPDATE: launch_update_solutions<T>(I); break;
+    case AMCFD_PHASE_UPDATE:
+        launch_update_solutions<T>(I);
+        launch_species_update<T>(I);
+        break;
+    case AMCFD_PHASE_SPECIES: launch_species<T>(I); break;
     default: break;
     }
 }
@@ -549,7 +562,8 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     case AMCFD_PHASE_MELTPOOL: return 1;
     case AMCFD_PHASE_MOMENTUM: return small ? 9 : 2 + 4 * (3 + sweeps) + 2 + 1;
     case AMCFD_PHASE_CONVERGE: return 1;
-    case AMCFD_PHASE_UPDATE: return 1;
+    case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;
+    case AMCFD_PHASE_SPECIES: return ctx->prm.species ? 4 + sweeps : 0;
     default: return 0;
     }
 }
@@ -557,7 +571,7 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
 // Timing slots of amcfd_last_timing (accumulated device ms while profiling):
 // 0 energy BC+assembly+block correction, 1 line factorisation, 2 energy line
 // sweeps, 3 H->T + melt pool, 4 momentum chain, 5 convergence, 6 laser,
-// 7 push-back, 8 outer iterations run, 9 energy-sweep launches.
+// 7 push-back, 8 outer iterations run, 9 energy-sweep launches, 10 species.
 // Event record; under stream capture it must become an event node of the graph
 // (the external flag is only valid while capturing).
 static inline void rec(amcfd_ctx *ctx, int q, bool capturing)
@@ -586,6 +600,8 @@ static void launch_iteration(amcfd_ctx *ctx, Inst<T> &I, bool capturing)
     if (ev) rec(ctx, 4, capturing);
     run_phase_impl<T>(ctx, I, AMCFD_PHASE_MOMENTUM);
     if (ev) rec(ctx, 5, capturing);
+    run_phase_impl<T>(ctx, I, AMCFD_PHASE_SPECIES);
+    if (ev) rec(ctx, 7, capturing);
     run_phase_impl<T>(ctx, I, AMCFD_PHASE_CONVERGE);
     if (ev) rec(ctx, 6, capturing);
 }
@@ -644,14 +660,23 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
         }
         for (int ph = AMCFD_PHASE_ENERGY_ASSEMBLE; ph <= AMCFD_PHASE_CONVERGE; ++ph)
             ctx->launches += phase_launches(ctx, ph, small);
+        ctx->launches += phase_launches(ctx, AMCFD_PHASE_SPECIES, small);
         if ((rc = read_status(ctx))) return rc;
         ctx->last_box = ctx->st_host->momentum_active ? ctx->st_host->box_cells : 0;
         if (ev) {
-            for (int q = 0; q < 6; q++) {
+            // events 0..5 bound slots 0..4; the species solve runs between events 5
+            // and 7, the convergence test between 7 and 6
+            for (int q = 0; q < 5; q++) {
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, ctx->ev[q], ctx->ev[q + 1]);
                 ctx->last_ms[q] += ms;
             }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev[5], ctx->ev[7]);
+            ctx->last_ms[10] += ms;
+            ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev[7], ctx->ev[6]);
+            ctx->last_ms[5] += ms;
             ctx->last_ms[8] += 1.0;
             ctx->last_ms[9] += ctx->order == AMCFD_ORDER_EXACT ? 1.0 : 8.0;
         }
@@ -678,6 +703,7 @@ static void fill_report(amcfd_ctx *ctx, amcfd_step_report *r)
     r->kstat = s->kstat; r->jstart = ctx->jstart; r->powerindicator = ctx->powerindicator;
     r->momentum_cells = s->box_cells;
     r->fallback = ctx->ws_fallback;
+    r->resorc = s->resorc;
 }
 
 // ---- learned warm start ----------------------------------------------------------------
@@ -757,9 +783,9 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     *out = ctx;
     ctx->prm = *params;
     amcfd_params &p = ctx->prm;
-    if (p.powderbed || p.movingmesh || p.species || p.freesurface)
+    if (p.powderbed || p.movingmesh || p.freesurface)
         return fail(ctx, AMCFD_E_ARG,
-                    "powder-bed mode, moving mesh, species and free surface are not implemented");
+                    "powder-bed mode, moving mesh and free surface are not implemented");
     if (p.nzx < 1 || p.nzy < 1 || p.nzz < 1 || p.nzx > AMCFD_MAX_ZONES || p.nzy > AMCFD_MAX_ZONES ||
         p.nzz > AMCFD_MAX_ZONES)
         return fail(ctx, AMCFD_E_ARG, "bad zone counts");
@@ -878,10 +904,10 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
     if (!ctx->prm.steady) {
         if (ctx->events) cudaEventRecord(ctx->ev[12], ctx->stream);
         if (ctx->precision == AMCFD_PREC_FP64)
-            launch_update_solutions<double>(ctx->I64);
+            run_phase_impl<double>(ctx, ctx->I64, AMCFD_PHASE_UPDATE);
         else
-            launch_update_solutions<float>(ctx->I32);
-        ctx->launches += 1;
+            run_phase_impl<float>(ctx, ctx->I32, AMCFD_PHASE_UPDATE);
+        ctx->launches += phase_launches(ctx, AMCFD_PHASE_UPDATE, false);
         if (ctx->events) {
             cudaEventRecord(ctx->ev[13], ctx->stream);
             cudaEventSynchronize(ctx->ev[13]);
@@ -1035,7 +1061,7 @@ int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report)
 const char *amcfd_phase_name(int phase)
 {
     static const char *names[] = {"none", "laser", "energy_assemble", "energy_solve", "h2t",
-                                  "meltpool", "momentum", "converge", "update"};
+                                  "meltpool", "momentum", "converge", "update", "species"};
     return phase_ok(phase) ? names[phase] : "unknown";
 }
 
@@ -1052,7 +1078,10 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
         {"vis", offsetof(Fields<double>, vis_cur)}, {"diff_next", offsetof(Fields<double>, diff_nxt)},
         {"rho_next", offsetof(Fields<double>, rho_nxt)}, {"vis_next", offsetof(Fields<double>, vis_nxt)},
         F(sourceinput), F(unot), F(vnot), F(wnot), F(an), F(as), F(ae), F(aw), F(at), F(ab),
-        F(ap), F(su), F(dux), F(dvy), F(dwz)};
+        F(ap), F(su), F(dux), F(dvy), F(dwz),
+        {"avgconcentration", offsetof(Fields<double>, conc)},
+        {"avgconcentrationnot", offsetof(Fields<double>, concnot)},
+        {"concentration", offsetof(Fields<double>, concn)}};
 #undef F
     // Fields<float> has the same member layout of pointers
     const char *base = ctx->precision == AMCFD_PREC_FP64 ? (const char *)&ctx->I64.g
@@ -1060,6 +1089,7 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
     for (const E &e : tab)
         if (!strcmp(e.n, name)) {
             *ptr = *(void *const *)(base + e.off);
+            if (!*ptr) return fail(ctx, AMCFD_E_ARG, std::string("field ") + name + " needs *SOLVE_SPECIES");
             return 0;
         }
     return fail(ctx, AMCFD_E_ARG, std::string("unknown field ") + name);

@@ -278,6 +278,10 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         if (evap.size() < 4) return fail(AMCFD_E_PARSE, "*BOUNDARY_EVAPORATION needs 4 values");
         p.evaplatent = evap[0]; p.evaptemp = evap[1]; p.evapfact = evap[2]; p.molarmass = evap[3];
     }
+    if (p.species) {  // DomainManager.cpp:123-129
+        if (species.size() < 4) return fail(AMCFD_E_PARSE, "*SOLVE_SPECIES needs 4 values");
+        p.initconc = species[0]; p.massdiff = species[1]; p.kp = species[2]; p.urfc = species[3];
+    }
     if (volsrc_on && !voltable) {
         if (volsrc.size() < 5) return fail(AMCFD_E_PARSE, "*VOLUMETRIC_HEAT_SOURCE needs 5 values");
         p.avolpow = volsrc[0]; p.apowseta = volsrc[1]; p.heatthick = volsrc[2];

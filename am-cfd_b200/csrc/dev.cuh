@@ -38,6 +38,8 @@ struct Params {
     int nheattable;
     int volsrc;  // a volumetric source is configured (scalar form with heatthick > 0, or a table)
     double avolpow, apowseta, heatthick, heatrb, avolfact;  // scalar volumetric source
+    int species;  // *SOLVE_SPECIES: the ivar = 6 equation is solved
+    double initconc, massdiff, kp, urfc;
 };
 
 // Device status block: per-step inputs written by the host, per-iteration
@@ -53,6 +55,7 @@ struct Status {
     double ahtoploss, resorh, tpeak, alen, depth, width, ratio, accul, heatvol, heatout;
     double fluxwest, fluxeast, fluxtop, fluxbottom, fluxnorth, fluxsouth;
     double resoru, resorv, resorw, resorm, refmom, umaxt, mass_denom;
+    double resorc;  // species residual (0 without *SOLVE_SPECIES)
     int istat, iend, jstat, jend, kstat, istatp1, iendm1;
     int imin, imax, jmin, jmax, kmin, kmax;
     int momentum_active, box_cells;
@@ -84,6 +87,9 @@ struct Fields {
     // pass-invariant line factorisation: pr = ae/den, cf = aw/den, iden = 1/den
     T *pr, *cf, *iden;
     T *dux, *dvy, *dwz;
+    // species (null without *SOLVE_SPECIES): avgconcentration, its previous-step
+    // value and the liquid concentration of updateSolutions
+    T *conc, *concnot, *concn;
     double *heatin;     // nj*nip, Gaussian surface flux of the current step
     double *heattable;  // nheattable x 6
     // reductions

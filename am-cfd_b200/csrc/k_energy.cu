@@ -233,7 +233,7 @@ __device__ void block_tdma_warp(double *bl, double *blp, double *blm, const doub
 
 template <typename T>
 __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, int nblk_asm,
-                                     int check_finite)
+                                     int check_finite, int ivar)
 {
     extern __shared__ double sm[];  // 4 * nip
     const int nip = p.nip, nim1 = p.nim1, nim2 = p.nim2;
@@ -253,9 +253,10 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
     __syncthreads();
     if (threadIdx.x == 0) {
         Status *st = gd.st;
-        double resorh = tot[0] / (tot[1] + kSmall);
-        st->resorh = resorh;
-        if (check_finite && !isfinite(resorh)) st->nonfinite = 1;
+        // resorh (calculateResiduals(5)) or resorc (calculateResiduals(6))
+        double res = tot[0] / (tot[1] + kSmall);
+        if (ivar == 6) st->resorc = res; else st->resorh = res;
+        if (check_finite && !isfinite(res)) st->nonfinite = 1;
     }
     if (threadIdx.x < 32) block_tdma_warp(bl, blp, blm, blc, 1, nim2, gd.delphi);
 }
@@ -622,7 +623,7 @@ __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, i
         st->heatout = (fn + fb + fw + fe + fs) - ahtop;
         double ratio = p.steady ? -st->heatout / heatin : (st->heatvol + heatin) / (st->accul - st->heatout);
         st->ratio = ratio;
-        double list[5] = {st->resorm, st->resoru, st->resorv, st->resorw, 0.0};
+        double list[5] = {st->resorm, st->resoru, st->resorv, st->resorw, st->resorc};
         double amaxres = list[0];
         for (int q = 1; q < 5; q++)
             if (amaxres < list[q]) amaxres = list[q];
@@ -675,11 +676,11 @@ template <typename T> void launch_energy_bc(Inst<T> &I)
 {
     energy_bc_kernel<T><<<I.nb_bc, 256, 0, I.stream>>>(I.p, I.g, I.red_bc);
 }
-template <typename T> void launch_block_correct(Inst<T> &I)
+template <typename T> void launch_block_correct(Inst<T> &I, int ivar)
 {
     bc_reduce_kernel<T><<<dim3(I.p.nip / 32, 4), dim3(32, 8), 0, I.stream>>>(I.p, I.g);
     block_correct_kernel<T><<<1, 1024, 4 * I.p.nip * sizeof(double), I.stream>>>(
-        I.p, I.g, I.red_asm, I.nb_asm, I.check_finite);
+        I.p, I.g, I.red_asm, I.nb_asm, I.check_finite, ivar);
 }
 // Field read-out: the padded [k][j][nip] array widened to FP64 and packed to
 // the reference's unpadded [k][j][ni] layout (CFDSolverManager.cpp:249), so
@@ -760,7 +761,7 @@ template <typename T> void launch_update_solutions(Inst<T> &I)
 #define AMCFD_INST(T)                                        \
     template void launch_laser<T>(Inst<T> &);               \
     template void launch_energy_bc<T>(Inst<T> &);           \
-    template void launch_block_correct<T>(Inst<T> &);       \
+    template void launch_block_correct<T>(Inst<T> &, int);  \
     template void launch_h2t<T>(Inst<T> &);                 \
     template int h2t_blocks_per_sm<T>();                    \
     template void launch_pack_field<T>(const T *, double *, int, int, long long, int, cudaStream_t); \

@@ -30,12 +30,13 @@ namespace amcfd {
 // Factorisation: pr, cf = aw/den, iden = 1/den for every line of a box.
 // 32 lines per CTA, 32-cell chunks staged through shared memory so global
 // accesses stay coalesced; one thread per line walks its chunk sequentially.
-// ENERGY also applies the block correction phi += delphi[i] (enhanceConvergenceSpeed,
-// CFDSolverManager.cpp:2351-2361); BOX applies the |den| <= 1e-12 guard of
+// The whole-domain form (enthalpy or avgconcentration as phi) also applies the block
+// correction phi += delphi[i] (enhanceConvergenceSpeed, CFDSolverManager.cpp:2351-2361);
+// BOX applies the |den| <= 1e-12 guard of
 // solveLiquidDomain (:2438-2439) and reads the box from the status block.
 // ---------------------------------------------------------------------------
 template <typename T, bool BOX>
-__global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g)
+__global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g, T *phi)
 {
     __shared__ T tap[32][33], taw[32][33], tae[32][33], tph[32][33];
     const Status *st = g.st;
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g)
                     tap[r][lane] = g.ap[c];
                     taw[r][lane] = g.aw[c];
                     tae[r][lane] = g.ae[c];
-                    if (!BOX) tph[r][lane] = g.h[c] + (T)g.delphi[i];
+                    if (!BOX) tph[r][lane] = phi[c] + (T)g.delphi[i];
                 }
             }
             __syncthreads();
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g)
                     g.pr[c] = tap[r][lane];
                     g.cf[c] = taw[r][lane];
                     g.iden[c] = tae[r][lane];
-                    if (!BOX) g.h[c] = tph[r][lane];
+                    if (!BOX) phi[c] = tph[r][lane];
                 }
             }
             __syncthreads();
@@ -453,17 +454,18 @@ __global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *ticke
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <typename T> void launch_energy_factor(Inst<T> &I)
+template <typename T> void launch_phi_factor(Inst<T> &I, T *phi)
 {
     int lines = (I.p.nj - 2) * (I.p.nk - 2);
     int grid = (lines + 31) / 32;
-    factor_kernel<T, false><<<grid, 256, 0, I.stream>>>(I.p, I.g);
+    factor_kernel<T, false><<<grid, 256, 0, I.stream>>>(I.p, I.g, phi);
 }
+template <typename T> void launch_energy_factor(Inst<T> &I) { launch_phi_factor<T>(I, I.g.h); }
 template <typename T> void launch_box_factor(Inst<T> &I)
 {
     // the box is small (a melt pool); one CTA per SM covers up to 4736 lines per pass
     int grid = std::min((I.max_lines + 31) / 32, I.sm_count);
-    factor_kernel<T, true><<<grid, 256, 0, I.stream>>>(I.p, I.g);
+    factor_kernel<T, true><<<grid, 256, 0, I.stream>>>(I.p, I.g, nullptr);
 }
 template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
 {
@@ -493,6 +495,7 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
+template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi) { sweeps<T>(I, phi, false); }
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
 {
     T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
@@ -524,6 +527,8 @@ template <typename T> void set_sweep_smem_limit(size_t smem)
     template void launch_energy_factor<T>(Inst<T> &);                    \
     template void launch_box_factor<T>(Inst<T> &);                       \
     template void launch_energy_sweeps<T>(Inst<T> &);                    \
+    template void launch_phi_factor<T>(Inst<T> &, T *);                  \
+    template void launch_phi_sweeps<T>(Inst<T> &, T *);                  \
     template void launch_box_sweeps<T>(Inst<T> &, int);                  \
     template void launch_box_tickets<T>(Inst<T> &);                      \
     template int exact_sweep_blocks_per_sm<T>(int, size_t);              \

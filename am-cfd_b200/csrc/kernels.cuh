@@ -97,7 +97,7 @@ template <typename T> void launch_laser(Inst<T> &I);
 template <typename T> void launch_energy_bc(Inst<T> &I);
 template <typename T> void launch_energy_assemble(Inst<T> &I);
 template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T *rho_a, T *rho_b);
-template <typename T> void launch_block_correct(Inst<T> &I);
+template <typename T> void launch_block_correct(Inst<T> &I, int ivar = 5);
 template <typename T> void launch_h2t(Inst<T> &I);
 template <typename T> void launch_meltpool(Inst<T> &I);
 template <typename T> void launch_converge(Inst<T> &I, double tol);
@@ -105,6 +105,8 @@ template <typename T> void launch_update_solutions(Inst<T> &I);
 // line solvers (k_linesolve.cu)
 template <typename T> void launch_energy_factor(Inst<T> &I);
 template <typename T> void launch_energy_sweeps(Inst<T> &I);
+template <typename T> void launch_phi_factor(Inst<T> &I, T *phi);   // whole-domain phi
+template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi);
 template <typename T> void launch_box_factor(Inst<T> &I);
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
 template <typename T> void launch_box_tickets(Inst<T> &I);
@@ -112,5 +114,8 @@ template <typename T> void launch_box_tickets(Inst<T> &I);
 template <typename T> void launch_momentum(Inst<T> &I, bool small);
 template <typename T> int mom_small_capacity(const Inst<T> &I);
 template <typename T> void setup_mom_small(Inst<T> &I);
+// species (k_species.cu)
+template <typename T> void launch_species(Inst<T> &I);
+template <typename T> void launch_species_update(Inst<T> &I);
 
 }  // namespace amcfd

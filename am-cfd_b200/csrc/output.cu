@@ -215,7 +215,7 @@ static int write_residuals(amcfd_writer *w)
     const double crl = (tliq - tso) / (xliq - xso) * scanvel;
     double fl[6];
     ctx_fluxes(ctx, fl);
-    const double resorc = 0.0;  // species is not solved
+    const double resorc = r.resorc;
     std::ofstream o(joinp(w->root, w->base + "_Residuals.txt"), std::ios::out | std::ios::app);
     if (!o) return werr(w, AMCFD_E_IO, "cannot open residual file");
     const char *bar = "====================================================================================================\n";
@@ -283,8 +283,11 @@ int amcfd_writer_create(amcfd_ctx *ctx, const amcfd_deck *deck, const char *root
     static const char *known[] = {"pp", "vis", "rho", "uvel", "vvel", "wvel", "temp", "diff", "hnot",
                                   "fracl", "fraclnot", "pressure", "enthalpy", "sourceinput", "auvel",
                                   "avvel", "awvel"};
+    // with *SOLVE_SPECIES the registry also holds the two concentrations
+    // (CFDSolverManager.cpp:547-551)
+    const bool species = ctx_params(ctx).species != 0;
     while (s >> name) {
-        bool ok = false;
+        bool ok = species && (name == "avgconcentration" || name == "concentration");
         for (const char *k : known) ok |= name == k;
         if (!ok) continue;
         const std::string shown = name == "uvel" ? "auvel" : name == "vvel" ? "avvel" : name == "wvel" ? "awvel" : name;

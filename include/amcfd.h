@@ -88,8 +88,11 @@ typedef struct amcfd_params {
     /* *CONTROL_TIMESTEP_VARIABLE rows (t, delt, outtime), applied per step (main.cpp:125-134) */
     int nvardt;
     const double *vardt;     /* nvardt x 3 */
-    /* features the hot path does not implement; amcfd_create rejects them */
+    /* optional features: species is solved; amcfd_create rejects the others */
     int powderbed, movingmesh, species, freesurface;
+    /* *SOLVE_SPECIES row (DomainManager.cpp:123-129): initial concentration, mass
+     * diffusivity, partition coefficient kp, under-relaxation factor urfc */
+    double initconc, massdiff, kp, urfc;
 } amcfd_params;
 
 /* Per-step results, the scalars main() and PrintManager read after
@@ -104,6 +107,7 @@ typedef struct amcfd_step_report {
     int istat, iend, jstat, jend, kstat, jstart, powerindicator;
     int momentum_cells;  /* cells of the momentum box solved in the last outer iteration */
     int fallback;        /* reserved: 1 when a warm-start guess was rejected */
+    double resorc;       /* species residual (calculateResiduals(6)); 0 without *SOLVE_SPECIES */
 } amcfd_step_report;
 
 /* Line-sweep ordering of the line-by-line solver. */
@@ -157,7 +161,8 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
 
 /* Field access by the reference's registry key (CFDSolverManager.cpp:528-541):
  * "temp","uvel","vvel","wvel","pressure","pp","enthalpy","fracl","fraclnot",
- * "hnot","diff","rho","vis","sourceinput"; grid arrays "x","y","z","xu","yv","zw".
+ * "hnot","diff","rho","vis","sourceinput"; with *SOLVE_SPECIES also "avgconcentration",
+ * "avgconcentrationnot","concentration"; grid arrays "x","y","z","xu","yv","zw".
  * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
 int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out);
 int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in);
@@ -185,6 +190,9 @@ int amcfd_dims(const amcfd_ctx *ctx, int *ni, int *nj, int *nk);
 #define AMCFD_PHASE_CONVERGE 7
 /* 8: CFDSolverManager::updateSolutions */
 #define AMCFD_PHASE_UPDATE 8
+/* 9: the species equation, applyBCs(6) ... solveEntireDomain(6) (:678-687); a no-op
+ *    without *SOLVE_SPECIES */
+#define AMCFD_PHASE_SPECIES 9
 int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report);
 const char *amcfd_phase_name(int phase);
 

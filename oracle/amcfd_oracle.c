@@ -43,6 +43,8 @@ typedef struct orc {
     double *vis, *diff, *uvel, *vvel, *wvel, *enthalpy, *temp, *pp, *hnot, *fracl, *fraclnot;
     double *sourceinput, *rho, *unot, *vnot, *wnot, *pressure;
     double *ap, *an, *as, *ae, *aw, *at, *ab, *apnot, *dux, *dvy, *dwz, *su, *sp;
+    /* species: avgconcentration, avgconcentrationnot, concentration */
+    double *conc, *concnot, *concn;
     double resoru, resorv, resorw, resorm, resorh, resorc, refmom;
     int itertot, niter;
     /* BoundCondManager state */
@@ -172,6 +174,11 @@ static void initialize_solver(orc *o)
         o->enthalpy[c] = hpre;
         o->hnot[c] = hpre;
         o->temp[c] = p->temppreheat;
+        if (p->species) {  /* CFDSolverManager.cpp:474-479 */
+            o->conc[c] = p->initconc;
+            o->concnot[c] = p->initconc;
+            o->concn[c] = p->initconc;
+        }
     }
     for (int k = 0; k < nk; k++)
         for (int j = 0; j < nj; j++) {
@@ -505,6 +512,33 @@ void orc_apply_bcs(orc *o, int ivar)
             }
         break;
     }
+    case 6: {
+        /* BoundCondManager.cpp:655-699: top (flux towards the surface value 13 where
+         * the top node is above the liquidus) and bottom planes, then the south/north
+         * rows over every (k, i), then the west/east columns over every (k, j) */
+        const double initval = p->initconc, dsl = p->dens * p->massdiff;
+        double *cn = o->conc;
+        for (j = 1; j < njm1; j++)
+            for (i = 1; i < nim1; i++) {
+                if (o->temp[ID(i, j, nkm1)] > p->tliquid)
+                    cn[ID(i, j, nkm1)] = 2.0 * (13.0 - cn[ID(i, j, nkm2)]) / o->dzpbinv[nkm1] / dsl +
+                                         cn[ID(i, j, nkm2)];
+                else
+                    cn[ID(i, j, nkm1)] = cn[ID(i, j, nkm2)];
+                cn[ID(i, j, 0)] = initval;
+            }
+        for (k = 0; k < o->nk; k++)
+            for (i = 0; i < ni; i++) {
+                cn[ID(i, 0, k)] = cn[ID(i, 1, k)];
+                cn[ID(i, njm1, k)] = cn[ID(i, njm1 - 1, k)];
+            }
+        for (k = 0; k < o->nk; k++)
+            for (j = 0; j < nj; j++) {
+                cn[ID(0, j, k)] = cn[ID(1, j, k)];
+                cn[ID(nim1, j, k)] = cn[ID(nim1 - 1, j, k)];
+            }
+        break;
+    }
     }
 }
 
@@ -808,6 +842,58 @@ void orc_discretize(orc *o, int ivar)
             }
         break;
     }
+    case 6: {
+        /* discretizeEquations(6), :1265-1362.  Cell diffusivity 1e-11 at or below the
+         * solidus, massdiff * rho above; face velocities doubled in the mass fluxes;
+         * each face conductance uses the diffusivity of the cell on its low side. */
+        const size_t n = (size_t)ni * nj * o->nk;
+        double *ds = dalloc(n);
+        for (size_t c = 0; c < n; c++) ds[c] = o->temp[c] <= o->p.tsolid ? 1e-11 : o->p.massdiff * rho[c];
+        for (k = 1; k < nkm1; k++)
+            for (j = 1; j < njm1; j++)
+                for (i = 1; i < nim1; i++) {
+                    size_t c = ID(i, j, k);
+                    double vn = v[ID(i, j + 1, k)] * 2.0;
+                    double ue = u[ID(i + 1, j, k)] * 2.0;
+                    double wt = w[ID(i, j, k + 1)] * 2.0;
+                    double fn = rho[ID(i, j + 1, k)] * vn * o->areaik[k * ni + i];
+                    double fe = rho[ID(i + 1, j, k)] * ue * o->areajk[k * nj + j];
+                    double ft = rho[ID(i, j, k + 1)] * wt * o->areaij[j * ni + i];
+                    double dn = ds[c] * o->areaik[k * ni + i] * o->dypsinv[j + 1];
+                    double de = ds[c] * o->areajk[k * nj + j] * o->dxpwinv[i + 1];
+                    double dt = ds[c] * o->areaij[j * ni + i] * o->dzpbinv[k + 1];
+                    double densbydt = rho[c] / delt;
+                    coef_pair(sch, dn, fn, &o->an[c], &o->as[ID(i, j + 1, k)]);
+                    coef_pair(sch, de, fe, &o->ae[c], &o->aw[ID(i + 1, j, k)]);
+                    coef_pair(sch, dt, ft, &o->at[c], &o->ab[ID(i, j, k + 1)]);
+                    o->apnot[c] = densbydt * o->volume[c];
+                    o->sp[c] = 0.0;
+                    o->su[c] = o->apnot[c] * o->concnot[c];
+                }
+        for (k = 1; k < nkm1; k++)
+            for (i = 1; i < nim1; i++) {
+                double vs = v[ID(i, 1, k)] * 2;
+                double fs = rho[ID(i, 1, k)] * vs * o->areaik[k * ni + i];
+                double dss = ds[ID(i, 1, k)] * o->areaik[k * ni + i] * o->dypsinv[1];
+                coef_pair(sch, dss, fs, &tmp, &o->as[ID(i, 1, k)]);
+            }
+        for (k = 1; k < nkm1; k++)
+            for (j = 1; j < njm1; j++) {
+                double uw = u[ID(1, j, k)] * 2;
+                double fw = rho[ID(1, j, k)] * uw * o->areajk[k * nj + j];
+                double dw = ds[ID(1, j, k)] * o->areajk[k * nj + j] * o->dxpwinv[1];
+                coef_pair(sch, dw, fw, &tmp, &o->aw[ID(1, j, k)]);
+            }
+        for (j = 1; j < njm1; j++)
+            for (i = 1; i < nim1; i++) {
+                double wb = w[ID(i, j, 1)] * 2;
+                double fb = rho[ID(i, j, 1)] * wb * o->areaij[j * ni + i];
+                double db = ds[ID(i, j, 1)] * o->areaij[j * ni + i] * o->dzpbinv[1];
+                coef_pair(sch, db, fb, &tmp, &o->ab[ID(i, j, 1)]);
+            }
+        free(ds);
+        break;
+    }
     }
 }
 
@@ -886,11 +972,64 @@ static void momentum_source(orc *o, int ivar)
             }
 }
 
-void orc_source(orc *o, int ivar)
+/* Boundary folds and under-relaxation shared by calculateSource(5) and (6)
+ * (CFDSolverManager.cpp:1779-1839, 1853-1920): the k, then j, then i boundary
+ * coefficients move into su/sp against the boundary values of phi, then
+ * ap = sum(a_nb) + apnot - sp, ap /= urf, su += (1 - urf) ap phi. */
+static void fold_and_relax(orc *o, const double *h, double urf)
 {
     const int ni = o->ni, nj = o->nj;
     const int nim1 = o->nim1, njm1 = o->njm1, nkm1 = o->nkm1, nim2 = o->nim2, njm2 = o->njm2,
               nkm2 = o->nkm2;
+    int i, j, k;
+    for (j = 1; j < njm1; j++)
+        for (i = 1; i < nim1; i++) {
+            size_t c = ID(i, j, 1);
+            o->su[c] += o->ab[c] * h[ID(i, j, 0)];
+            o->sp[c] -= o->ab[c];
+            o->ab[c] = 0.0;
+            c = ID(i, j, nkm2);
+            o->su[c] += o->at[c] * h[ID(i, j, nkm1)];
+            o->sp[c] -= o->at[c];
+            o->at[c] = 0.0;
+        }
+    for (k = 1; k < nkm1; k++)
+        for (i = 1; i < nim1; i++) {
+            size_t c = ID(i, 1, k);
+            o->su[c] += o->as[c] * h[ID(i, 0, k)];
+            o->sp[c] -= o->as[c];
+            o->as[c] = 0.0;
+            c = ID(i, njm2, k);
+            o->su[c] += o->an[c] * h[ID(i, njm1, k)];
+            o->sp[c] -= o->an[c];
+            o->an[c] = 0.0;
+        }
+    for (k = 1; k < nkm1; k++)
+        for (j = 1; j < njm1; j++) {
+            size_t c = ID(1, j, k);
+            o->su[c] += o->aw[c] * h[ID(0, j, k)];
+            o->sp[c] -= o->aw[c];
+            o->aw[c] = 0.0;
+            c = ID(nim2, j, k);
+            o->su[c] += o->ae[c] * h[ID(nim1, j, k)];
+            o->sp[c] -= o->ae[c];
+            o->ae[c] = 0.0;
+        }
+    for (k = 1; k < nkm1; k++)
+        for (j = 1; j < njm1; j++)
+            for (i = 1; i < nim1; i++) {
+                size_t c = ID(i, j, k);
+                o->ap[c] = o->an[c] + o->as[c] + o->ae[c] + o->aw[c] + o->at[c] + o->ab[c] +
+                           o->apnot[c] - o->sp[c];
+                o->ap[c] /= urf;
+                o->su[c] += (1.0 - urf) * o->ap[c] * h[c];
+            }
+}
+
+void orc_source(orc *o, int ivar)
+{
+    const int ni = o->ni, nj = o->nj;
+    const int nim1 = o->nim1, njm1 = o->njm1, nkm1 = o->nkm1;
     const amcfd_params *p = &o->p;
     int i, j, k;
     if (ivar >= 1 && ivar <= 3) {
@@ -909,6 +1048,10 @@ void orc_source(orc *o, int ivar)
                         o->ap[c] = LARGE;
                     }
                 }
+        return;
+    }
+    if (ivar == 6) {  /* calculateSource(6), :1844-1920 */
+        fold_and_relax(o, o->conc, p->urfc);
         return;
     }
     if (ivar != 5) return;
@@ -955,49 +1098,7 @@ void orc_source(orc *o, int ivar)
                      MAXD(-w[ID(i, j, k + 1)], 0.0) * fl[ID(i, j, k + 1)] - MAXD(w[ID(i, j, k + 1)], 0.0) * fl[c]);
                 o->su[c] += o->rho[c] * o->hlatnt * (flew + flns + fltb);
             }
-    double *h = o->enthalpy;
-    for (j = 1; j < njm1; j++)
-        for (i = 1; i < nim1; i++) {
-            size_t c = ID(i, j, 1);
-            o->su[c] += o->ab[c] * h[ID(i, j, 0)];
-            o->sp[c] -= o->ab[c];
-            o->ab[c] = 0.0;
-            c = ID(i, j, nkm2);
-            o->su[c] += o->at[c] * h[ID(i, j, nkm1)];
-            o->sp[c] -= o->at[c];
-            o->at[c] = 0.0;
-        }
-    for (k = 1; k < nkm1; k++)
-        for (i = 1; i < nim1; i++) {
-            size_t c = ID(i, 1, k);
-            o->su[c] += o->as[c] * h[ID(i, 0, k)];
-            o->sp[c] -= o->as[c];
-            o->as[c] = 0.0;
-            c = ID(i, njm2, k);
-            o->su[c] += o->an[c] * h[ID(i, njm1, k)];
-            o->sp[c] -= o->an[c];
-            o->an[c] = 0.0;
-        }
-    for (k = 1; k < nkm1; k++)
-        for (j = 1; j < njm1; j++) {
-            size_t c = ID(1, j, k);
-            o->su[c] += o->aw[c] * h[ID(0, j, k)];
-            o->sp[c] -= o->aw[c];
-            o->aw[c] = 0.0;
-            c = ID(nim2, j, k);
-            o->su[c] += o->ae[c] * h[ID(nim1, j, k)];
-            o->sp[c] -= o->ae[c];
-            o->ae[c] = 0.0;
-        }
-    for (k = 1; k < nkm1; k++)
-        for (j = 1; j < njm1; j++)
-            for (i = 1; i < nim1; i++) {
-                size_t c = ID(i, j, k);
-                o->ap[c] = o->an[c] + o->as[c] + o->ae[c] + o->aw[c] + o->at[c] + o->ab[c] +
-                           o->apnot[c] - o->sp[c];
-                o->ap[c] /= p->urfh;
-                o->su[c] += (1.0 - p->urfh) * o->ap[c] * h[c];
-            }
+    fold_and_relax(o, o->enthalpy, p->urfh);
 }
 
 /* ---- calculateResiduals: CFDSolverManager.cpp:1933-2132 --------------------------- */
@@ -1064,6 +1165,22 @@ void orc_residual(orc *o, int ivar)
                 }
         o->resorh = sumd / (sumh + SMALL);
     }
+    if (ivar == 6) {  /* :2102-2128 */
+        const double *cn = o->conc;
+        double sumc = 0.0, sumd = 0.0;
+        for (k = 1; k < nkm1; k++)
+            for (j = 1; j < njm1; j++)
+                for (i = 1; i < nim1; i++) {
+                    size_t c = ID(i, j, k);
+                    double r = (o->an[c] * cn[ID(i, j + 1, k)] + o->as[c] * cn[ID(i, j - 1, k)] +
+                                o->ae[c] * cn[ID(i + 1, j, k)] + o->aw[c] * cn[ID(i - 1, j, k)] +
+                                o->at[c] * cn[ID(i, j, k + 1)] + o->ab[c] * cn[ID(i, j, k - 1)] + o->su[c]) /
+                                   o->ap[c] - cn[c];
+                    sumd += fabs(r);
+                    sumc += fabs(cn[c]);
+                }
+        o->resorc = sumd / (sumc + SMALL);
+    }
 }
 
 /* ---- bareplateMaterialProps: CFDSolverManager.cpp:2137-2189 ----------------------- */
@@ -1090,11 +1207,10 @@ void orc_props(orc *o)
 }
 
 /* ---- enhanceConvergenceSpeed(5): CFDSolverManager.cpp:2270-2362 ------------------- */
-void orc_block_correct(orc *o)
+static void block_correct_phi(orc *o, double *phi)
 {
     const int ni = o->ni, nj = o->nj;
     const int nim1 = o->nim1, njm1 = o->njm1, nkm1 = o->nkm1, nim2 = o->nim2;
-    double *phi = o->enthalpy;
     double *bl = dalloc(ni), *blp = dalloc(ni), *blm = dalloc(ni), *blc = dalloc(ni);
     double *delphi = dalloc(ni), *pib = dalloc(ni), *qib = dalloc(ni);
     for (int k = 1; k < nkm1; k++)
@@ -1123,13 +1239,13 @@ void orc_block_correct(orc *o)
             for (int i = 1; i < nim1; i++) phi[ID(i, j, k)] += delphi[i];
     free(bl); free(blp); free(blm); free(blc); free(delphi); free(pib); free(qib);
 }
+void orc_block_correct(orc *o) { block_correct_phi(o, o->enthalpy); }
 
 /* ---- solveEntireDomain(5): CFDSolverManager.cpp:2459-2526 ------------------------- */
-void orc_solve_entire(orc *o)
+static void solve_entire_phi(orc *o, double *phi)
 {
     const int ni = o->ni, nj = o->nj;
     const int nim1 = o->nim1, njm1 = o->njm1, nim2 = o->nim2, nkm2 = o->nkm2;
-    double *phi = o->enthalpy;
     double *pr = dalloc(ni), *qr = dalloc(ni);
     for (int ks = 0; ks < 2; ks++)
         for (int k = nkm2; k > 0; k--)
@@ -1149,6 +1265,7 @@ void orc_solve_entire(orc *o)
                 }
     free(pr); free(qr);
 }
+void orc_solve_entire(orc *o) { solve_entire_phi(o, o->enthalpy); }
 
 /* ---- solveLiquidDomain(1..4): CFDSolverManager.cpp:2367-2454 ---------------------- */
 void orc_solve_liquid(orc *o, int ivar)
@@ -1305,6 +1422,10 @@ void orc_update_solutions(orc *o)
         o->wnot[c] = o->wvel[c];
         o->hnot[c] = o->enthalpy[c];
         o->fraclnot[c] = o->fracl[c];
+        if (o->p.species) {  /* :2680-2685 */
+            o->concnot[c] = o->conc[c];
+            o->concn[c] = o->conc[c] / (o->fracl[c] + o->p.kp * (1.0 - o->fracl[c]));
+        }
     }
 }
 
@@ -1333,6 +1454,18 @@ int orc_momentum(orc *o)
     return 1;
 }
 
+/* Species equation (iterativeLoopSolve :677-687). */
+void orc_species(orc *o)
+{
+    if (!o->p.species) return;
+    orc_apply_bcs(o, 6);
+    orc_discretize(o, 6);
+    orc_source(o, 6);
+    orc_residual(o, 6);
+    block_correct_phi(o, o->conc);
+    solve_entire_phi(o, o->conc);
+}
+
 /* One outer iteration (iterativeLoopSolve :612-716); returns 1 when converged. */
 int orc_outer_iteration(orc *o)
 {
@@ -1346,6 +1479,7 @@ int orc_outer_iteration(orc *o)
     orc_h2t(o);
     orc_meltpool(o);
     orc_momentum(o);
+    orc_species(o);
     double list[5] = {o->resorm, o->resoru, o->resorv, o->resorw, o->resorc};
     double amaxres = list[0];
     for (int q = 1; q < 5; q++)
@@ -1380,6 +1514,7 @@ void orc_report(const orc *o, amcfd_step_report *r)
     r->istat = o->istat; r->iend = o->iend; r->jstat = o->jstat; r->jend = o->jend;
     r->kstat = o->kstat; r->jstart = o->jstart; r->powerindicator = o->powerindicator;
     r->momentum_cells = o->last_box_cells;
+    r->resorc = o->resorc;
 }
 
 /* Start of a time step, main.cpp:125-141: variable time step, timet += delt,
@@ -1463,7 +1598,8 @@ orc *orc_create(const amcfd_params *params)
                      &o->uvel, &o->vvel, &o->wvel, &o->enthalpy, &o->temp, &o->pp, &o->hnot,
                      &o->fracl, &o->fraclnot, &o->sourceinput, &o->rho, &o->unot, &o->vnot,
                      &o->wnot, &o->pressure, &o->ap, &o->an, &o->as, &o->ae, &o->aw, &o->at,
-                     &o->ab, &o->apnot, &o->dux, &o->dvy, &o->dwz, &o->su, &o->sp};
+                     &o->ab, &o->apnot, &o->dux, &o->dvy, &o->dwz, &o->su, &o->sp, &o->conc,
+                     &o->concnot, &o->concn};
     for (size_t q = 0; q < sizeof(f3) / sizeof(f3[0]); q++) *f3[q] = dalloc(n);
     o->powerindicator = 1;
     o->init = 1;
@@ -1484,7 +1620,7 @@ void orc_free(orc *o)
                    o->uvel, o->vvel, o->wvel, o->enthalpy, o->temp, o->pp, o->hnot, o->fracl,
                    o->fraclnot, o->sourceinput, o->rho, o->unot, o->vnot, o->wnot, o->pressure,
                    o->ap, o->an, o->as, o->ae, o->aw, o->at, o->ab, o->apnot, o->dux, o->dvy,
-                   o->dwz, o->su, o->sp};
+                   o->dwz, o->su, o->sp, o->conc, o->concnot, o->concn};
     for (size_t q = 0; q < sizeof(f) / sizeof(f[0]); q++) free(f[q]);
     free(o->tool_on);
     free(o->tool_id);
@@ -1514,7 +1650,9 @@ double *orc_field(orc *o, const char *name)
         {"x", o->x}, {"y", o->y}, {"z", o->z}, {"xu", o->xu}, {"yv", o->yv}, {"zw", o->zw},
         {"dxpwinv", o->dxpwinv}, {"dypsinv", o->dypsinv}, {"dzpbinv", o->dzpbinv},
         {"fracx", o->fracx}, {"fracy", o->fracy}, {"fracz", o->fracz}, {"heatin", o->heatin},
-        {"areaij", o->areaij}, {"areajk", o->areajk}, {"areaik", o->areaik}};
+        {"areaij", o->areaij}, {"areajk", o->areajk}, {"areaik", o->areaik},
+        {"avgconcentration", o->conc}, {"avgconcentrationnot", o->concnot},
+        {"concentration", o->concn}};
     for (size_t q = 0; q < sizeof(t) / sizeof(t[0]); q++)
         if (!strcmp(t[q].n, name)) return t[q].p;
     return NULL;

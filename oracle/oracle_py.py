@@ -49,7 +49,7 @@ def lib():
         for fn in ("orc_update_laser", "orc_meltpool", "orc_props", "orc_block_correct",
                    "orc_solve_entire", "orc_h2t", "orc_clean_velocities", "orc_correct_pressure",
                    "orc_fluxes", "orc_update_solutions", "orc_energy_assemble", "orc_outer_loop",
-                   "orc_begin_step"):
+                   "orc_begin_step", "orc_species"):
             getattr(L, fn).argtypes = [VP]
         for fn in ("orc_momentum", "orc_outer_iteration"):
             getattr(L, fn).argtypes = [VP]

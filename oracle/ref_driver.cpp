@@ -34,6 +34,8 @@
 static const char *kFields[] = {"temp", "uvel", "vvel", "wvel", "pressure", "enthalpy",
                                 "fracl", "pp", "diff", "rho", "vis", "hnot", "fraclnot"};
 static const int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
+// appended after kFields when the deck solves the species equation
+static const char *kSpeciesFields[] = {"avgconcentration", "concentration"};
 static const char *kGeom[] = {"x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv",
                               "fracx", "fracy"};
 static const int kNumGeom = sizeof(kGeom) / sizeof(kGeom[0]);
@@ -87,6 +89,7 @@ int main(int argc, char **argv)
 
     const int ni = domainMgr->ni_, nj = domainMgr->nj_, nk = domainMgr->nk_;
     const size_t n = (size_t)ni * nj * nk;
+    const int nspecies = meshObj.species_ ? 2 : 0;
     FILE *f = nullptr;
     if (!timing) {
         f = fopen(out.c_str(), "wb");
@@ -94,7 +97,7 @@ int main(int argc, char **argv)
         fwrite("AMCR", 1, 4, f);
         put_i32(f, 1);
         put_i32(f, ni); put_i32(f, nj); put_i32(f, nk);
-        put_i32(f, kNumFields);
+        put_i32(f, kNumFields + nspecies);
         put_i32(f, kNumGeom);
         // geometry: 1-D arrays x,y,z (+ face arrays), each written at its own length
         for (int g = 0; g < kNumGeom; ++g) {
@@ -145,7 +148,7 @@ int main(int argc, char **argv)
                            bcMgr->ahtoploss_, bcMgr->accul_, bcMgr->heatout_, bcMgr->heatvol_,
                            bcMgr->fluxwest_, bcMgr->fluxeast_, bcMgr->fluxtop_,
                            bcMgr->fluxbottom_, bcMgr->fluxnorth_, bcMgr->fluxsouth_,
-                           bcMgr->beamposx_, bcMgr->beamposy_, domainMgr->scanvel_};
+                           bcMgr->beamposx_, bcMgr->beamposy_, domainMgr->scanvel_, cfd->resorc_};
             put_i32(f, (int)(sizeof(sc) / 8));
             fwrite(sc, 8, sizeof(sc) / 8, f);
             int ix[] = {bcMgr->istat_, bcMgr->iend_, bcMgr->jstat_, bcMgr->jend_, bcMgr->kstat_,
@@ -156,6 +159,8 @@ int main(int argc, char **argv)
                 const double *p = solVarMgr->mapSolutionVars_[kFields[q]];
                 fwrite(p, 8, n, f);
             }
+            for (int q = 0; q < nspecies; ++q)
+                fwrite(solVarMgr->mapSolutionVars_[kSpeciesFields[q]], 8, n, f);
         }
     }
     if (f) { put_i32(f, -1); fclose(f); }

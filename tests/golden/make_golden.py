@@ -23,9 +23,16 @@ import amcfd_decks as D  # noqa: E402
 from amcfd_dump import read_dump  # noqa: E402
 
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
+SPECIES_FIELDS = ("avgconcentration", "concentration")
 SCALARS = ("niter", "timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat",
-           "jstart")
+           "jstart", "resorc")
+
+
+def species_deck():
+    d = D.small("g_species", nx=16, ny=10, nz=8, steps=4)
+    d.species = (1.0, 5e-9, 0.3, 0.7)
+    return d
 
 
 def decks():
@@ -34,6 +41,7 @@ def decks():
         D.small("g_toolpath", nx=16, ny=10, nz=8, steps=4, toolpath=True),
         D.small("g_noflow", nx=16, ny=10, nz=8, steps=4, fluid_flow=False),
         D.small("g_cooling", nx=16, ny=10, nz=8, steps=6, laser_off_after=3, scheme="upwind"),
+        species_deck(),
     ]
 
 
@@ -51,7 +59,7 @@ def main():
         steps = dump["steps"]
         rec = {f"s_{k}": np.array([s[k] for s in steps]) for k in SCALARS}
         for tag, s in (("first", steps[0]), ("last", steps[-1])):
-            for f in FIELDS:
+            for f in FIELDS + tuple(f for f in SPECIES_FIELDS if f in s):
                 rec[f"{tag}_{f}"] = s[f]
         for g, v in dump["geom"].items():
             rec[f"geom_{g}"] = v

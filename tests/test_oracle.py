@@ -15,10 +15,12 @@ import pytest
 
 from conftest import GOLDEN
 
-CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling"]
+CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species"]
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
+SPECIES_FIELDS = ("avgconcentration", "concentration")
 SCALARS = ("niter", "tpeak", "alen", "depth", "width", "ratio", "resorh", "resorm", "resoru",
-           "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart")
+           "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart",
+           "resorc")
 
 
 def _same(a, b):
@@ -36,13 +38,14 @@ def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
     for g in ("x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"):
         assert np.array_equal(o.field(g), ref[f"geom_{g}"]), g
     n = len(ref["s_niter"])
+    fields = FIELDS + tuple(f for f in SPECIES_FIELDS if f"first_{f}" in ref)
     for s in range(n):
         r = o.step()
         for k in SCALARS:
             assert _same(r[k], ref[f"s_{k}"][s]), (case, s, k, r[k], ref[f"s_{k}"][s])
         tag = "first" if s == 0 else "last" if s == n - 1 else None
         if tag:
-            for f in FIELDS:
+            for f in fields:
                 assert np.array_equal(o.field(f), ref[f"{tag}_{f}"], equal_nan=True), (case, s, f)
 
 
@@ -63,13 +66,17 @@ def _variants():
     d.vardt = [(2e-5, 1e-5, 1.0), (1.0, 5e-6, 1.0)]
     d.finaltime = 4.2e-5
     out.append(d)
+    # species with the upwind scheme, a slow diffusivity and a strong partition
+    d = D.small("v_species", steps=4, power=250.0, scheme="upwind")
+    d.species = (0.5, 2e-9, 0.1, 0.5)
+    out.append(d)
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(4))
+@pytest.mark.parametrize("idx", range(5))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
@@ -81,9 +88,11 @@ def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
                           env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
     ref = read_dump(out)
     o = oracle_py.Oracle(amcfd.Deck(path))
+    fields = FIELDS + (SPECIES_FIELDS if deck.species is not None else ())
     for s in ref["steps"]:
         r = o.step()
         assert r["niter"] == s["niter"]
         assert _same(r["tpeak"], s["tpeak"])
-        for f in FIELDS:
+        assert _same(r["resorc"], s["resorc"])
+        for f in fields:
             assert np.array_equal(o.field(f), s[f], equal_nan=True), (deck.name, s["step"], f)

@@ -5,7 +5,8 @@ The reference (oracle/_ref/AM-CFD, built from the reference's sources, one
 OpenMP thread) and the GPU solver (FP64, exact sweep order) run the same deck
 from directories of their own.  Checked: the .vts XML headers and the .pvd are
 byte-identical; the point coordinates are identical; every point array agrees
-to 1e-8 relative L2 (the solver parity tolerance); the text files agree token
+to 1e-8 relative L2 (the solver parity tolerance), the species fields included
+when the deck solves them; the text files agree token
 by token, numbers to the precision they are printed with (2 digits, so within
 2 % relative).  The cooling-rate lines are left out: the reference computes
 them from uninitialised values when the beam row has no molten cell.
@@ -60,10 +61,13 @@ def text_lines(path):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_CLI), reason="reference binary not built")
-def test_output_files_match_reference(tmp_path, monkeypatch):
+@pytest.mark.parametrize("species", [False, True])
+def test_output_files_match_reference(species, tmp_path, monkeypatch):
     import amcfd
     import amcfd_decks as D
     d = D.small("outdeck", nx=20, ny=12, nz=8, steps=5, power=300.0)
+    if species:  # adds avgconcentration and concentration to the written fields
+        d.species = (1.0, 5e-9, 0.3, 0.7)
     d.outtime = 2 * d.dt
     d.final_geometry = "outdeck_geom.txt"
     ref_dir, our_dir = tmp_path / "ref", tmp_path / "ours"
