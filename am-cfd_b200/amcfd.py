@@ -54,7 +54,9 @@ class AmcfdParams(C.Structure):
          ("nheattable", _I), ("heattable", C.POINTER(_D)),
          ("nvardt", _I), ("vardt", C.POINTER(_D))] + \
         [(n, _I) for n in "powderbed movingmesh species freesurface".split()] + \
-        [(n, _D) for n in "initconc massdiff kp urfc".split()]
+        [(n, _D) for n in "initconc massdiff kp urfc".split()] + \
+        [(n, _I) for n in "numlayers ncvzlayer".split()] + \
+        [(n, _D) for n in "layerheight powderden powdercpa powdercpb powderthcona powderthconb".split()]
 
 
 class AmcfdReport(C.Structure):
@@ -63,7 +65,7 @@ class AmcfdReport(C.Structure):
                            "heatinlaser ahtoploss accul heatout heatvol beamposx beamposy "
                            "scanvel").split()] + \
         [(n, _I) for n in ("istat iend jstat jend kstat jstart powerindicator momentum_cells "
-                           "fallback").split()] + [("resorc", _D)]
+                           "fallback").split()] + [("resorc", _D), ("nk_active", _I), ("trackindx", _I)]
 
     def as_dict(self) -> Dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

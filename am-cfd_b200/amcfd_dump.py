@@ -8,13 +8,15 @@ from typing import Dict, List
 import numpy as np
 
 FIELDS = ["temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp", "diff",
-          "rho", "vis", "hnot", "fraclnot", "avgconcentration", "concentration"]
+          "rho", "vis", "hnot", "fraclnot"]
+SPECIES_FIELDS = ["avgconcentration", "concentration"]
+POWDER_FIELDS = ["csfrac", "solfrac", "mpPhase", "mpLiqPhase"]
 GEOM = ["x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"]
 SCALARS = ["timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "ahtoploss", "accul", "heatout",
            "heatvol", "fluxwest", "fluxeast", "fluxtop", "fluxbottom", "fluxnorth",
            "fluxsouth", "beamposx", "beamposy", "scanvel", "resorc"]
-INDICES = ["istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator"]
+INDICES = ["istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator", "nk_active", "trackindx"]
 
 
 def read_dump(path: str) -> Dict:
@@ -34,6 +36,9 @@ def read_dump(path: str) -> Dict:
     ni, nj, nk = i32(), i32(), i32()
     nf, ng = i32(), i32()
     n = ni * nj * nk
+    # the optional groups follow the fixed fields: species (2), then powder bed (4)
+    extra = nf - len(FIELDS)
+    names = FIELDS + {0: [], 2: SPECIES_FIELDS, 4: POWDER_FIELDS, 6: SPECIES_FIELDS + POWDER_FIELDS}[extra]
     geom = {}
     for g in range(ng):
         ln = i32()
@@ -54,7 +59,7 @@ def read_dump(path: str) -> Dict:
         off += 4 * nix
         rec.update({INDICES[q]: int(ix[q]) for q in range(nix)})
         for q in range(nf):
-            rec[FIELDS[q]] = np.frombuffer(buf, "<f8", n, off).reshape(nk, nj, ni).copy()
+            rec[names[q]] = np.frombuffer(buf, "<f8", n, off).reshape(nk, nj, ni).copy()
             off += 8 * n
         steps.append(rec)
     return {"version": version, "ni": ni, "nj": nj, "nk": nk, "geom": geom, "steps": steps}

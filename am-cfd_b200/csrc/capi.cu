@@ -81,7 +81,8 @@ struct amcfd_ctx {
     int precision = AMCFD_PREC_FP64;
     int order = AMCFD_ORDER_EXACT;
     int device = 0;
-    int ni = 0, nj = 0, nk = 0, nip = 0;
+    int ni = 0, nj = 0, nk = 0, nip = 0;  // nk: planes of every 3-D array (all powder layers)
+    int nk_active = 0;                     // DomainManager::nk_ (grows per powder layer)
     double hlcal = 0, hlatnt = 0;
     std::vector<double> x, y, z, xu, yv, zw, dxpwinv, dypsinv, dzpbinv, fracx, fracy, fracz;
     // laser / time state (BoundCondManager.h:339-349, DomainManager::timet_)
@@ -233,6 +234,11 @@ static void laser_coords(amcfd_ctx *c)
                                 (c->beamposz - c->oldbeamposz) * (c->beamposz - c->oldbeamposz));
         c->scanvel = dist / c->delt;
         if (oldpower - c->powerindicator > 0 && deltaty > small) c->trackindx++;
+        // powder bed: the beam switching on activates the next layer (:266-272)
+        if (c->powerindicator - oldpower > 0 && p.powderbed) {
+            c->trackindx++;
+            c->nk_active += p.ncvzlayer;
+        }
     }
     // nearest node to the beam (:92-126)
     int iout = 0, jout = 0;
@@ -274,6 +280,49 @@ static int upload(amcfd_ctx *ctx, T *dst, const std::vector<double> &src)
     return 0;
 }
 
+// (t, m, s) order of the visits (ks, k, s, j) of solveEntireDomain over M planes
+// and J rows (k_linesolve.cu explains the wave index t).
+static std::vector<int2> energy_tickets(int M, int J)
+{
+    std::vector<int2> tk;
+    tk.reserve((size_t)4 * M * J);
+    const int Tw = 3 * (2 * M - 1) + (J - 1) + 2 + 1;
+    for (int t = 0; t < Tw; ++t)
+        for (int m = std::max(0, (t - 2 - (J - 1)) / 3 - 1); m <= std::min(2 * M - 1, t / 3); ++m)
+            for (int s = 0; s < 2; ++s) {
+                int jj = t - 3 * m - 2 * s;
+                if (jj >= 0 && jj < J) tk.push_back(make_int2(m, (s << 16) | jj));
+            }
+    return tk;
+}
+
+static void drop_graphs(amcfd_ctx *ctx);
+
+// Resize the active domain to nk planes (powder-bed layer activation,
+// BoundCondManager.cpp:266-272; PrintManager.cpp:67-73 at start-up): the launch
+// shapes that depend on nk, the exact-order ticket list and the captured graphs
+// (their kernel arguments hold the old extents) follow.
+template <typename T>
+static int set_active_nk(amcfd_ctx *ctx, Inst<T> &I, int nk)
+{
+    Params &p = I.p;
+    if (nk == p.nk) return 0;
+    if (nk < 3 || nk > p.nk_alloc)
+        return fail(ctx, AMCFD_E_CAPACITY, "powder layer activation beyond the generated grid (nk " +
+                                               std::to_string(nk) + " of " + std::to_string(p.nk_alloc) + ")");
+    CK(cudaStreamSynchronize(ctx->stream));
+    p.nk = nk; p.nkm1 = nk - 1; p.nkm2 = nk - 2;
+    I.asm_grid = energy_assemble_grid(p);
+    I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
+    I.g.npart = I.asm_grid.y * I.asm_grid.z;
+    I.max_lines = (p.nj - 2) * (p.nk - 2);
+    const std::vector<int2> tk = energy_tickets(p.nk - 2, p.nj - 2);
+    CK(cudaMemcpy(I.g.tickets_energy, tk.data(), tk.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    I.g.ntickets_energy = (int)tk.size();
+    drop_graphs(ctx);
+    return 0;
+}
+
 template <typename T>
 static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
 {
@@ -302,6 +351,10 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     p.heatrb = q.heatrb; p.avolfact = q.avolfact;
     p.species = q.species ? 1 : 0;
     p.initconc = q.initconc; p.massdiff = q.massdiff; p.kp = q.kp; p.urfc = q.urfc;
+    p.powder = q.powderbed ? 1 : 0;
+    p.nk_alloc = ctx->nk;
+    p.powderden = q.powderden; p.powdercpa = q.powdercpa; p.powdercpb = q.powdercpb;
+    p.powderthcona = q.powderthcona; p.powderthconb = q.powderthconb;
 
     const size_t n3 = (size_t)p.nk * p.nj * p.nip;
     Fields<T> &g = I.g;
@@ -328,6 +381,9 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     if (p.species)
         for (T **f : {&g.conc, &g.concnot, &g.concn})
             if ((rc = alloc3<T>(ctx, f, n3))) return rc;
+    if (p.powder)
+        for (T **f : {&g.csfrac, &g.solfrac, &g.mpphase, &g.mpliq})
+            if ((rc = alloc3<T>(ctx, f, n3))) return rc;
     if ((rc = alloc3<double>(ctx, &g.heatin, (size_t)p.nj * p.nip))) return rc;
     if (q.nheattable > 0) {
         if ((rc = alloc3<double>(ctx, &g.heattable, ctx->heattable.size()))) return rc;
@@ -342,22 +398,32 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     I.nb_bc = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 2 * p.nk * (p.ni + p.nj) + 255) / 256));
     I.asm_grid = energy_assemble_grid(p);
     I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
+    // the assembly's per-CTA buffers hold the largest grid of any active height
+    int nb_asm_max = I.nb_asm, npart_max = I.asm_grid.y * I.asm_grid.z;
+    if (p.powder)
+        for (int nka = ctx->nk_active; nka <= p.nk; nka += std::max(1, q.ncvzlayer)) {
+            Params pa = p;
+            pa.nk = nka;
+            const dim3 ga = energy_assemble_grid(pa);
+            nb_asm_max = std::max(nb_asm_max, (int)(ga.x * ga.y * ga.z));
+            npart_max = std::max(npart_max, (int)(ga.y * ga.z));
+        }
     I.nb_h2t = std::max(1, std::min(I.sm_count * h2t_blocks_per_sm<T>(), (int)((n3 + 255) / 256)));
     I.nb_mom = I.sm_count * 2;
     I.grid_1d = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
     double *red;
-    size_t nred = (size_t)(I.nb_las + I.nb_bc + I.nb_asm + I.nb_h2t + 5 * I.nb_mom) * R_NSLOTS;
+    size_t nred = (size_t)(I.nb_las + I.nb_bc + nb_asm_max + I.nb_h2t + 5 * I.nb_mom) * R_NSLOTS;
     if ((rc = alloc3<double>(ctx, &red, nred))) return rc;
     I.red_las = red;
     I.red_bc = I.red_las + (size_t)I.nb_las * R_NSLOTS;
     I.red_asm = I.red_bc + (size_t)I.nb_bc * R_NSLOTS;
-    I.red_h2t = I.red_asm + (size_t)I.nb_asm * R_NSLOTS;
+    I.red_h2t = I.red_asm + (size_t)nb_asm_max * R_NSLOTS;
     I.red_mom = I.red_h2t + (size_t)I.nb_h2t * R_NSLOTS;
     g.red = red;
     if (make_assemble_maps<T>(I, g.diff_cur, g.diff_nxt, g.rho_cur, g.rho_nxt))
         return fail(ctx, AMCFD_E_CUDA, "tensor-map encoding for the energy assembly failed");
     g.npart = I.asm_grid.y * I.asm_grid.z;
-    if ((rc = alloc3<double>(ctx, &g.bc, (size_t)g.npart * 4 * p.nip))) return rc;
+    if ((rc = alloc3<double>(ctx, &g.bc, (size_t)npart_max * 4 * p.nip))) return rc;
     if ((rc = alloc3<double>(ctx, &g.delphi, (size_t)p.nip))) return rc;
     if ((rc = alloc3<double>(ctx, &g.bcsum, (size_t)4 * p.nip))) return rc;
     if ((rc = alloc3<int>(ctx, &g.mp_kb, (size_t)p.nip))) return rc;
@@ -372,17 +438,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     if ((rc = alloc3<int>(ctx, &g.flags, (size_t)p.nk * p.nj))) return rc;
     if ((rc = alloc3<int>(ctx, &I.flags_mom, (size_t)p.nk * p.nj))) return rc;
     {
-        // (t, m, s) order of the visits (ks, k, s, j) of solveEntireDomain
         const int M = p.nk - 2, J = p.nj - 2;
-        std::vector<int2> tk;
-        tk.reserve((size_t)4 * M * J);
-        const int Tw = 3 * (2 * M - 1) + (J - 1) + 2 + 1;
-        for (int t = 0; t < Tw; ++t)
-            for (int m = std::max(0, (t - 2 - (J - 1)) / 3 - 1); m <= std::min(2 * M - 1, t / 3); ++m)
-                for (int s = 0; s < 2; ++s) {
-                    int jj = t - 3 * m - 2 * s;
-                    if (jj >= 0 && jj < J) tk.push_back(make_int2(m, (s << 16) | jj));
-                }
+        const std::vector<int2> tk = energy_tickets(M, J);
         if (tk.size() != (size_t)4 * M * J) return fail(ctx, AMCFD_E_ARG, "ticket enumeration mismatch");
         int2 *d;
         if ((rc = alloc3<int2>(ctx, &d, tk.size()))) return rc;
@@ -417,14 +474,28 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         std::vector<double> a(n3, v);
         return upload<T>(ctx, dst, a);
     };
+    // both buffers of each property pair: planes outside the active domain (unbuilt
+    // powder layers) keep these values until they become active, as in the
+    // reference's single arrays
     if ((rc = fill(g.vis_cur, q.viscos)) || (rc = fill(g.rho_cur, q.dens)) ||
-        (rc = fill(g.diff_cur, diff0)) || (rc = fill(g.hnot, hpre)) ||
+        (rc = fill(g.diff_cur, diff0)) || (rc = fill(g.vis_nxt, q.viscos)) ||
+        (rc = fill(g.rho_nxt, q.dens)) || (rc = fill(g.diff_nxt, diff0)) || (rc = fill(g.hnot, hpre)) ||
         (rc = fill(g.temp, q.temppreheat)))
         return rc;
     // species (CFDSolverManager.cpp:474-479): every node at the initial concentration
     if (p.species && ((rc = fill(g.conc, q.initconc)) || (rc = fill(g.concnot, q.initconc)) ||
                       (rc = fill(g.concn, q.initconc))))
         return rc;
+    if (p.powder) {
+        // CFDSolverManager.cpp:482-492: the base plate is consolidated, the build
+        // layers are powder (csfrac 0); solfrac, mpPhase, mpLiqPhase start at 0
+        std::vector<double> cs(n3, 0.0);
+        const double top = ctx->z[p.nk - 1] - (double)q.numlayers * q.layerheight;
+        for (int k = 0; k < p.nk; k++)
+            if (ctx->z[k] < top)
+                for (size_t c = (size_t)k * p.nj * p.nip; c < (size_t)(k + 1) * p.nj * p.nip; ++c) cs[c] = 1.0;
+        if ((rc = upload<T>(ctx, g.csfrac, cs))) return rc;
+    }
     for (int k = 0; k < p.nk; k++)
         for (int j = 0; j < p.nj; j++)
             for (int i = 0; i < p.ni; i++) hv[cidx(i, j, k, p.nj, p.nip)] = hpre;
@@ -439,10 +510,33 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         for (int i = 0; i < p.ni; i++) hv[cidx(i, p.njm1, k, p.nj, p.nip)] = enth(q.tempnorth);
     if ((rc = upload<T>(ctx, g.h, hv))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
-    return 0;
+    // powder bed: only the first layer starts active (PrintManager.cpp:67-73)
+    return set_active_nk<T>(ctx, I, ctx->nk_active);
 }
 
 static bool phase_ok(int phase) { return phase >= 1 && phase <= AMCFD_PHASE_SPECIES; }
+
+// The track id updateSolutions tags melted cells with (CFDSolverManager.cpp:2638-2644):
+// that of the first toolpath row not earlier than the current time.  The
+// reference leaves it undefined without a toolpath or past the last row; 0 here.
+static int track_id(const amcfd_ctx *ctx)
+{
+    int id = 0;
+    for (int i = (int)ctx->tool_id.size(); i > 0; i--)
+        if (ctx->timet <= ctx->tool[4 * (i - 1)]) id = ctx->tool_id[i - 1];
+    return id;
+}
+
+static void drop_graphs(amcfd_ctx *ctx)
+{
+    for (auto &plane : ctx->gexec)
+        for (auto &row : plane)
+            for (auto &ge : row)
+                if (ge) {
+                    cudaGraphExecDestroy(ge);
+                    ge = nullptr;
+                }
+}
 
 // ---- one outer iteration -----------------------------------------------------------------
 template <typename T>
@@ -484,6 +578,8 @@ static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
         swap_props<T>(I);
         break;
     case AMCFD_PHASE_UPDATE:
+        I.trackindx = (double)ctx->trackindx;
+        I.trackid = track_id(ctx);
         launch_update_solutions<T>(I);
         launch_species_update<T>(I);
         break;
@@ -504,6 +600,11 @@ static int begin_step(amcfd_ctx *ctx)
     }
     ctx->timet += ctx->delt;
     if (!p.steady) laser_coords(ctx);
+    if (p.powderbed) {
+        const int rc = ctx->precision == AMCFD_PREC_FP64 ? set_active_nk<double>(ctx, ctx->I64, ctx->nk_active)
+                                                         : set_active_nk<float>(ctx, ctx->I32, ctx->nk_active);
+        if (rc) return rc;
+    }
     Status *h = ctx->st_host;
     h->timet = ctx->timet;
     h->delt = ctx->delt;
@@ -704,6 +805,8 @@ static void fill_report(amcfd_ctx *ctx, amcfd_step_report *r)
     r->momentum_cells = s->box_cells;
     r->fallback = ctx->ws_fallback;
     r->resorc = s->resorc;
+    r->nk_active = ctx->nk_active;
+    r->trackindx = ctx->trackindx;
 }
 
 // ---- learned warm start ----------------------------------------------------------------
@@ -783,9 +886,8 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     *out = ctx;
     ctx->prm = *params;
     amcfd_params &p = ctx->prm;
-    if (p.powderbed || p.movingmesh || p.freesurface)
-        return fail(ctx, AMCFD_E_ARG,
-                    "powder-bed mode, moving mesh and free surface are not implemented");
+    if (p.movingmesh || p.freesurface)
+        return fail(ctx, AMCFD_E_ARG, "moving mesh and free surface are not implemented");
     if (p.nzx < 1 || p.nzy < 1 || p.nzz < 1 || p.nzx > AMCFD_MAX_ZONES || p.nzy > AMCFD_MAX_ZONES ||
         p.nzz > AMCFD_MAX_ZONES)
         return fail(ctx, AMCFD_E_ARG, "bad zone counts");
@@ -818,6 +920,13 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     for (int q = 0; q < p.nzz; q++) sz += (int)p.ncvz[q];
     ctx->ni = sx + 2; ctx->nj = sy + 2; ctx->nk = sz + 2;
     if (sx < 1 || sy < 1 || sz < 1) return fail(ctx, AMCFD_E_ARG, "empty grid");
+    ctx->nk_active = ctx->nk;
+    if (p.powderbed) {
+        if (p.numlayers < 1 || p.ncvzlayer < 1 || !(p.layerheight > 0.0))
+            return fail(ctx, AMCFD_E_ARG, "*POWDER_BED_MODE needs layers, cells per layer and a height");
+        ctx->nk_active = ctx->nk - (p.numlayers - 1) * p.ncvzlayer;
+        if (ctx->nk_active < 3) return fail(ctx, AMCFD_E_ARG, "powder layers exceed the z grid");
+    }
     if (ctx->nj > 65535) return fail(ctx, AMCFD_E_CAPACITY, "nj above 65535");
     ctx->nip = (ctx->ni + 31) / 32 * 32;
     double cpavg = (p.acpa * p.tsolid + p.acpb + p.acpl) * 0.5;
@@ -868,10 +977,7 @@ void amcfd_destroy(amcfd_ctx *ctx)
     for (void *q : {(void *)ctx->ws_feat, (void *)ctx->ws_y, (void *)ctx->ws_target, ctx->ws_save[0],
                     ctx->ws_save[1], ctx->ws_save[2], ctx->ws_save[3]})
         if (q) cudaFree(q);
-    for (auto &plane : ctx->gexec)
-        for (auto &row : plane)
-            for (auto &ge : row)
-                if (ge) cudaGraphExecDestroy(ge);
+    drop_graphs(ctx);
     for (int q = 0; q < 16; q++)
         if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -984,6 +1090,8 @@ int amcfd_ws_attach(amcfd_ctx *ctx, amcfd_net *net, int mode)
         return AMCFD_E_ARG;
     if (mode != AMCFD_WS_OFF && ctx->prm.nheattable > 0)
         return fail(ctx, AMCFD_E_ARG, "warm start with a volumetric heat-source table is not supported");
+    if (mode != AMCFD_WS_OFF && ctx->prm.powderbed)
+        return fail(ctx, AMCFD_E_ARG, "warm start on a growing powder-bed domain is not supported");
     CK(cudaSetDevice(ctx->device));
     ctx->net = net;
     ctx->ws_mode = mode;
@@ -1081,7 +1189,9 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
         F(ap), F(su), F(dux), F(dvy), F(dwz),
         {"avgconcentration", offsetof(Fields<double>, conc)},
         {"avgconcentrationnot", offsetof(Fields<double>, concnot)},
-        {"concentration", offsetof(Fields<double>, concn)}};
+        {"concentration", offsetof(Fields<double>, concn)},
+        {"csfrac", offsetof(Fields<double>, csfrac)}, {"solfrac", offsetof(Fields<double>, solfrac)},
+        {"mpPhase", offsetof(Fields<double>, mpphase)}, {"mpLiqPhase", offsetof(Fields<double>, mpliq)}};
 #undef F
     // Fields<float> has the same member layout of pointers
     const char *base = ctx->precision == AMCFD_PREC_FP64 ? (const char *)&ctx->I64.g
@@ -1089,7 +1199,8 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
     for (const E &e : tab)
         if (!strcmp(e.n, name)) {
             *ptr = *(void *const *)(base + e.off);
-            if (!*ptr) return fail(ctx, AMCFD_E_ARG, std::string("field ") + name + " needs *SOLVE_SPECIES");
+            if (!*ptr)
+                return fail(ctx, AMCFD_E_ARG, std::string("field ") + name + " is not solved by this deck");
             return 0;
         }
     return fail(ctx, AMCFD_E_ARG, std::string("unknown field ") + name);

@@ -278,6 +278,15 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         if (evap.size() < 4) return fail(AMCFD_E_PARSE, "*BOUNDARY_EVAPORATION needs 4 values");
         p.evaplatent = evap[0]; p.evaptemp = evap[1]; p.evapfact = evap[2]; p.molarmass = evap[3];
     }
+    if (p.powderbed) {  // DomainManager.cpp:147-162: the build layers extend the last z-zone
+        if (powder.size() < 8) return fail(AMCFD_E_PARSE, "*POWDER_BED_MODE needs 8 values");
+        p.numlayers = (int)powder[0]; p.ncvzlayer = (int)powder[1]; p.layerheight = powder[2];
+        p.powderden = powder[3]; p.powdercpa = powder[4]; p.powdercpb = powder[5];
+        p.powderthcona = powder[6]; p.powderthconb = powder[7];
+        if (p.nzz < 1) return fail(AMCFD_E_PARSE, "*POWDER_BED_MODE needs a z grid");
+        p.zzone[p.nzz - 1] += p.numlayers * p.layerheight;
+        p.ncvz[p.nzz - 1] += p.numlayers * p.ncvzlayer;
+    }
     if (p.species) {  // DomainManager.cpp:123-129
         if (species.size() < 4) return fail(AMCFD_E_PARSE, "*SOLVE_SPECIES needs 4 values");
         p.initconc = species[0]; p.massdiff = species[1]; p.kp = species[2]; p.urfc = species[3];

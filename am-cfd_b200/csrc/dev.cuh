@@ -40,6 +40,10 @@ struct Params {
     double avolpow, apowseta, heatthick, heatrb, avolfact;  // scalar volumetric source
     int species;  // *SOLVE_SPECIES: the ivar = 6 equation is solved
     double initconc, massdiff, kp, urfc;
+    // *POWDER_BED_MODE: effective powder properties (powderMaterialProps); nk above
+    // is the active domain, nk_alloc the planes every 3-D array holds
+    int powder, nk_alloc;
+    double powderden, powdercpa, powdercpb, powderthcona, powderthconb;
 };
 
 // Device status block: per-step inputs written by the host, per-iteration
@@ -90,6 +94,9 @@ struct Fields {
     // species (null without *SOLVE_SPECIES): avgconcentration, its previous-step
     // value and the liquid concentration of updateSolutions
     T *conc, *concnot, *concn;
+    // powder bed (null otherwise): consolidated fraction, solidified-track marker and
+    // the track id of the last solid / liquid pass (updateSolutions)
+    T *csfrac, *solfrac, *mpphase, *mpliq;
     double *heatin;     // nj*nip, Gaussian surface flux of the current step
     double *heattable;  // nheattable x 6
     // reductions

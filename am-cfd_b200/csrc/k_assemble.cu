@@ -69,6 +69,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     const int sch = p.scheme;
     const double delt = st->delt;
     const bool volsrc = p.volsrc != 0;
+    const bool powder = p.powder != 0;
 
     // ---- copy pipeline (thread 0 issues; all threads wait) ----
     auto issueA = [&](int q) {
@@ -171,11 +172,24 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 const R diffl = bdiv(thla * t + thlb, acpl);
                 R dn = diffl, rn = denl, vn = visc;
                 if (!(t >= tliq)) {
-                    const R diffs = bdiv(thsa * (t * t) + thsb * t + thsc, acpa * t + acpb);
-                    dn = diffs; rn = dens; vn = R(1e10);
+                    R diffs, rs = dens;
+                    if (!powder) {
+                        diffs = bdiv(thsa * (t * t) + thsb * t + thsc, acpa * t + acpb);
+                    } else {
+                        // powderMaterialProps (CFDSolverManager.cpp:2236-2252): solid and
+                        // powder mixed by the consolidated fraction
+                        const R cs = g.csfrac[c];
+                        const R cps = acpa * t + acpb;
+                        const R conds = thsa * (t * t) + thsb * t + thsc;
+                        const R diffp = bdiv((R)p.powderthcona * t + (R)p.powderthconb,
+                                             (R)p.powdercpa * t + (R)p.powdercpb);
+                        diffs = (R(1) - cs) * diffp + bdiv(cs * conds, cps);
+                        rs = (R(1) - cs) * (R)p.powderden + cs * dens;
+                    }
+                    dn = diffs; rn = rs; vn = R(1e10);
                     if (!(t <= tsol)) {
                         dn = fl * diffl + (R(1) - fl) * diffs;
-                        rn = fl * denl + (R(1) - fl) * dens;
+                        rn = fl * denl + (R(1) - fl) * rs;
                         vn = visc;
                     }
                 }

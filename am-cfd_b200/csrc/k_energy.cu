@@ -646,7 +646,7 @@ __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, i
 // the previous-step copies.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void update_solutions_kernel(Params p, Fields<T> g)
+__global__ void update_solutions_kernel(Params p, Fields<T> g, double trackindx, int trackid)
 {
     const size_t total = (size_t)p.nk * p.nj * p.nip;
     const T ts = (T)p.tsolid;
@@ -662,6 +662,13 @@ __global__ void update_solutions_kernel(Params p, Fields<T> g)
         g.wnot[c] = g.wvel[c];
         g.hnot[c] = g.h[c];
         g.fraclnot[c] = g.fracl[c];
+        if (p.powder) {  // CFDSolverManager.cpp:2666-2678
+            const T fl = g.fracl[c];
+            g.csfrac[c] = maxd(g.csfrac[c], fl);
+            g.solfrac[c] = maxd(g.solfrac[c], (T)((double)fl * trackindx));
+            if (g.temp[c] > ts) g.mpphase[c] = (T)trackid;
+            if (g.temp[c] > (T)p.tliquid) g.mpliq[c] = (T)trackid;
+        }
     }
 }
 
@@ -704,12 +711,12 @@ template <typename T> void launch_pack_field(const T *src, double *dst, int ni, 
 
 // Cell-centred velocity for output (vtsBinWriter::transferVelNodes,
 // vtsBinWriter.cpp:497-522): the mean of the two faces of component `comp`
-// (0 u, 1 v, 2 w) on interior nodes, zero where T <= T_solidus and on the
-// boundary nodes, packed to FP64 [k][j][ni].
+// (0 u, 1 v, 2 w) on interior nodes of the active domain, zero where T <= T_solidus,
+// on the boundary nodes and on inactive powder layers, packed to FP64 [k][j][ni].
 template <typename T>
 __global__ void centre_velocity_kernel(Params p, Fields<T> g, int comp, double *dst)
 {
-    const long long n = (long long)p.ni * p.nj * p.nk;
+    const long long n = (long long)p.ni * p.nj * p.nk_alloc;  // every allocated plane
     const T *f = comp == 0 ? g.uvel : comp == 1 ? g.vvel : g.wvel;
     const size_t step = comp == 0 ? 1 : comp == 1 ? (size_t)p.nip : (size_t)p.nj * p.nip;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
@@ -755,7 +762,7 @@ template <typename T> void launch_converge(Inst<T> &I, double tol)
 }
 template <typename T> void launch_update_solutions(Inst<T> &I)
 {
-    update_solutions_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g);
+    update_solutions_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g, I.trackindx, I.trackid);
 }
 
 #define AMCFD_INST(T)                                        \

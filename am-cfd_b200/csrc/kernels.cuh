@@ -90,6 +90,9 @@ struct Inst {
     T *mom_scratch = nullptr; // one field: line-solve scratch of the small-box momentum path
     size_t mom_small_smem = 0;  // its dynamic shared memory
     const T *asm_diff_a = nullptr;  // diff_cur at parity 0
+    // updateSolutions inputs of the current step (powder bed)
+    double trackindx = 1.0;
+    int trackid = 0;
 };
 
 // launchers (k_energy.cu)

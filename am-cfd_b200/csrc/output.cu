@@ -109,6 +109,13 @@ static int write_vts(amcfd_writer *w, const std::string &path)
           << "\" />  ";
         off += (uint32_t)(sizeof(double) * npts + sizeof(int32_t));
     }
+    // powder bed: the layers not yet built are ghost points (vtsBinWriter.cpp:76-80, 235-258)
+    const bool powder = ctx_params(ctx).powderbed != 0;
+    if (powder) {
+        h << "<DataArray type=\"UInt8\" Name=\"vtkGhostType\" format=\"appended\" offset=\"" << (int32_t)off
+          << "\" />  ";
+        off += (uint32_t)(sizeof(unsigned char) * npts + sizeof(int32_t));
+    }
     h << "</PointData> ";
     h << "<CellData> ";
     h << "</CellData> ";
@@ -152,6 +159,18 @@ static int write_vts(amcfd_writer *w, const std::string &path)
         task[q & 1] = last;
     }
     if (last.valid()) last.wait();
+    if (powder) {  // visible (0) below the active top plane, hidden (2) from it up
+        amcfd_step_report r;
+        ctx_report(ctx, &r);
+        const int nkm1 = r.nk_active - 1;
+        int32_t bytes = (int32_t)npts;
+        f.write((const char *)&bytes, sizeof(bytes));
+        std::vector<unsigned char> plane((size_t)ni * nj);
+        for (int k = 0; k < gridz - 1; k++) {
+            std::fill(plane.begin(), plane.end(), (unsigned char)(k < nkm1 ? 0 : 2));
+            f.write((const char *)plane.data(), plane.size());
+        }
+    }
     f << "\n";
     f << "</AppendedData> </VTKFile>";
     if (!f) return werr(w, AMCFD_E_IO, "write failed: " + path);
@@ -182,7 +201,7 @@ static int write_residuals(amcfd_writer *w)
     const amcfd_params &prm = ctx_params(ctx);
     int ni, nj, nk;
     amcfd_dims(ctx, &ni, &nj, &nk);
-    const int nim1 = ni - 1, nkm2 = nk - 2;
+    const int nim1 = ni - 1, nkm2 = r.nk_active - 2;  // top interior plane of the active domain
     const std::vector<double> *x, *y, *z;
     ctx_grid(ctx, &x, &y, &z);
     const double tsolid = prm.tsolid, tliquid = prm.tliquid, scanvel = r.scanvel;
@@ -285,9 +304,11 @@ int amcfd_writer_create(amcfd_ctx *ctx, const amcfd_deck *deck, const char *root
                                   "avvel", "awvel"};
     // with *SOLVE_SPECIES the registry also holds the two concentrations
     // (CFDSolverManager.cpp:547-551)
-    const bool species = ctx_params(ctx).species != 0;
+    const bool species = ctx_params(ctx).species != 0, powder = ctx_params(ctx).powderbed != 0;
     while (s >> name) {
         bool ok = species && (name == "avgconcentration" || name == "concentration");
+        // with *POWDER_BED_MODE: CFDSolverManager.cpp:554-560
+        ok |= powder && (name == "csfrac" || name == "solfrac" || name == "mpPhase" || name == "mpLiqPhase");
         for (const char *k : known) ok |= name == k;
         if (!ok) continue;
         const std::string shown = name == "uvel" ? "auvel" : name == "vvel" ? "avvel" : name == "wvel" ? "awvel" : name;

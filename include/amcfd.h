@@ -88,11 +88,17 @@ typedef struct amcfd_params {
     /* *CONTROL_TIMESTEP_VARIABLE rows (t, delt, outtime), applied per step (main.cpp:125-134) */
     int nvardt;
     const double *vardt;     /* nvardt x 3 */
-    /* optional features: species is solved; amcfd_create rejects the others */
+    /* optional features: species and powder bed are solved; amcfd_create rejects the others */
     int powderbed, movingmesh, species, freesurface;
     /* *SOLVE_SPECIES row (DomainManager.cpp:123-129): initial concentration, mass
      * diffusivity, partition coefficient kp, under-relaxation factor urfc */
     double initconc, massdiff, kp, urfc;
+    /* *POWDER_BED_MODE row (DomainManager.cpp:147-158): layers, control volumes per
+     * layer, layer height, powder density, cp = powdercpa*T + powdercpb,
+     * k = powderthcona*T + powderthconb.  The deck parser has already added the
+     * layers to the last z-zone (:160-161). */
+    int numlayers, ncvzlayer;
+    double layerheight, powderden, powdercpa, powdercpb, powderthcona, powderthconb;
 } amcfd_params;
 
 /* Per-step results, the scalars main() and PrintManager read after
@@ -108,6 +114,8 @@ typedef struct amcfd_step_report {
     int momentum_cells;  /* cells of the momentum box solved in the last outer iteration */
     int fallback;        /* reserved: 1 when a warm-start guess was rejected */
     double resorc;       /* species residual (calculateResiduals(6)); 0 without *SOLVE_SPECIES */
+    int nk_active;       /* nodes in z of the active domain (grows per powder layer) */
+    int trackindx;       /* BoundCondManager::trackindx_ */
 } amcfd_step_report;
 
 /* Line-sweep ordering of the line-by-line solver. */
@@ -162,7 +170,9 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
 /* Field access by the reference's registry key (CFDSolverManager.cpp:528-541):
  * "temp","uvel","vvel","wvel","pressure","pp","enthalpy","fracl","fraclnot",
  * "hnot","diff","rho","vis","sourceinput"; with *SOLVE_SPECIES also "avgconcentration",
- * "avgconcentrationnot","concentration"; grid arrays "x","y","z","xu","yv","zw".
+ * "avgconcentrationnot","concentration"; with *POWDER_BED_MODE also "csfrac","solfrac",
+ * "mpPhase","mpLiqPhase"; grid arrays "x","y","z","xu","yv","zw".  Arrays cover the
+ * whole grid (every powder layer, active or not). 
  * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
 int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out);
 int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in);

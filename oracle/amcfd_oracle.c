@@ -33,6 +33,8 @@ typedef struct orc {
     double *tool;
     int *tool_on, *tool_id;
     int ni, nj, nk, nim1, njm1, nkm1, nim2, njm2, nkm2;
+    int nk_alloc;     /* planes of every 3-D array; nk is DomainManager::nk_ (powder: active) */
+    int layer_overflow; /* a powder layer was requested beyond the generated grid */
     double hlcal, hlatnt, enthbottom, scanvel, timet;
     /* 1-D grid */
     double *x, *y, *z, *xu, *yv, *zw, *dxpwinv, *dypsinv, *dzpbinv, *fracx, *fracy, *fracz;
@@ -45,6 +47,8 @@ typedef struct orc {
     double *ap, *an, *as, *ae, *aw, *at, *ab, *apnot, *dux, *dvy, *dwz, *su, *sp;
     /* species: avgconcentration, avgconcentrationnot, concentration */
     double *conc, *concnot, *concn;
+    /* powder bed: csfrac, solfrac, mpPhase, mpLiqPhase */
+    double *csfrac, *solfrac, *mpphase, *mpliq;
     double resoru, resorv, resorw, resorm, resorh, resorc, refmom;
     int itertot, niter;
     /* BoundCondManager state */
@@ -249,6 +253,17 @@ static void laser_coords(orc *o)
                        (o->beamposz - o->oldbeamposz) * (o->beamposz - o->oldbeamposz));
     o->scanvel = dist / p->delt;
     if (oldpower - o->powerindicator > 0 && deltaty > small) o->trackindx++;
+    /* powder bed: the beam switching on activates the next layer (BoundCondManager.cpp:266-272) */
+    if (o->powerindicator - oldpower > 0 && p->powderbed) {
+        o->trackindx++;
+        if (o->nk + p->ncvzlayer > o->nk_alloc) {
+            o->layer_overflow = 1;  /* the reference indexes past its generated grid here */
+        } else {
+            o->nk += p->ncvzlayer;
+            o->nkm1 = o->nk - 1;
+            o->nkm2 = o->nk - 2;
+        }
+    }
 }
 
 void orc_update_laser(orc *o)
@@ -1195,13 +1210,22 @@ void orc_props(orc *o)
         o->rho[c] = p->denl;
         o->vis[c] = p->viscos;
         if (t >= p->tliquid) continue;
-        double diffs = (p->thconsa * (t * t) + p->thconsb * t + p->thconsc) / (p->acpa * t + p->acpb);
+        double diffs, rhos = p->dens;
+        if (!p->powderbed) {
+            diffs = (p->thconsa * (t * t) + p->thconsb * t + p->thconsc) / (p->acpa * t + p->acpb);
+        } else {  /* powderMaterialProps, CFDSolverManager.cpp:2236-2252 */
+            double cps = p->acpa * t + p->acpb;
+            double conds = p->thconsa * (t * t) + p->thconsb * t + p->thconsc;
+            double diffp = (p->powderthcona * t + p->powderthconb) / (p->powdercpa * t + p->powdercpb);
+            diffs = (1.0 - o->csfrac[c]) * diffp + o->csfrac[c] * conds / cps;
+            rhos = (1.0 - o->csfrac[c]) * p->powderden + o->csfrac[c] * p->dens;
+        }
         o->diff[c] = diffs;
-        o->rho[c] = p->dens;
+        o->rho[c] = rhos;
         o->vis[c] = 1e10;
         if (t <= p->tsolid) continue;
         o->diff[c] = o->fracl[c] * diffl + (1.0 - o->fracl[c]) * diffs;
-        o->rho[c] = o->fracl[c] * p->denl + (1.0 - o->fracl[c]) * p->dens;
+        o->rho[c] = o->fracl[c] * p->denl + (1.0 - o->fracl[c]) * rhos;
         o->vis[c] = p->viscos;
     }
 }
@@ -1411,6 +1435,12 @@ void orc_fluxes(orc *o)
 void orc_update_solutions(orc *o)
 {
     size_t n = (size_t)o->ni * o->nj * o->nk;
+    /* :2637-2645: track id of the first toolpath row not earlier than the time
+     * (undefined in the reference without one; 0 here) */
+    const double trackindx = (double)o->trackindx;
+    int trackid = 0;
+    for (int i = o->p.ntool; i > 0; i--)
+        if (o->p.udtoolpath && o->timet <= o->tool[4 * (i - 1)]) trackid = o->tool_id[i - 1];
     for (size_t c = 0; c < n; c++) {
         if (o->temp[c] <= o->p.tsolid) {
             o->uvel[c] = 0.0;
@@ -1422,6 +1452,12 @@ void orc_update_solutions(orc *o)
         o->wnot[c] = o->wvel[c];
         o->hnot[c] = o->enthalpy[c];
         o->fraclnot[c] = o->fracl[c];
+        if (o->p.powderbed) {  /* :2666-2678 */
+            o->csfrac[c] = MAXD(o->csfrac[c], o->fracl[c]);
+            o->solfrac[c] = MAXD(o->solfrac[c], o->fracl[c] * trackindx);
+            if (o->temp[c] > o->p.tsolid) o->mpphase[c] = trackid;
+            if (o->temp[c] > o->p.tliquid) o->mpliq[c] = trackid;
+        }
         if (o->p.species) {  /* :2680-2685 */
             o->concnot[c] = o->conc[c];
             o->concn[c] = o->conc[c] / (o->fracl[c] + o->p.kp * (1.0 - o->fracl[c]));
@@ -1515,6 +1551,8 @@ void orc_report(const orc *o, amcfd_step_report *r)
     r->kstat = o->kstat; r->jstart = o->jstart; r->powerindicator = o->powerindicator;
     r->momentum_cells = o->last_box_cells;
     r->resorc = o->resorc;
+    r->nk_active = o->nk;
+    r->trackindx = o->trackindx;
 }
 
 /* Start of a time step, main.cpp:125-141: variable time step, timet += delt,
@@ -1599,13 +1637,25 @@ orc *orc_create(const amcfd_params *params)
                      &o->fracl, &o->fraclnot, &o->sourceinput, &o->rho, &o->unot, &o->vnot,
                      &o->wnot, &o->pressure, &o->ap, &o->an, &o->as, &o->ae, &o->aw, &o->at,
                      &o->ab, &o->apnot, &o->dux, &o->dvy, &o->dwz, &o->su, &o->sp, &o->conc,
-                     &o->concnot, &o->concn};
+                     &o->concnot, &o->concn, &o->csfrac, &o->solfrac, &o->mpphase, &o->mpliq};
     for (size_t q = 0; q < sizeof(f3) / sizeof(f3[0]); q++) *f3[q] = dalloc(n);
     o->powerindicator = 1;
     o->init = 1;
     o->trackindx = 1;
+    o->nk_alloc = o->nk;
     generate_grid(o);
     initialize_solver(o);
+    if (p->powderbed) {
+        /* CFDSolverManager.cpp:482-492 then PrintManager.cpp:67-73: build layers are
+         * powder, and only the first of them starts active */
+        const double top = o->z[o->nk - 1] - ((double)p->numlayers * p->layerheight);
+        for (int k = 0; k < o->nk; k++)
+            for (size_t c = (size_t)k * ni * nj; c < (size_t)(k + 1) * ni * nj; c++)
+                o->csfrac[c] = o->z[k] < top ? 1.0 : 0.0;
+        o->nk -= (p->numlayers - 1) * p->ncvzlayer;
+        o->nkm1 = o->nk - 1;
+        o->nkm2 = o->nk - 2;
+    }
     if (p->steady) orc_update_laser(o);
     return o;
 }
@@ -1620,7 +1670,8 @@ void orc_free(orc *o)
                    o->uvel, o->vvel, o->wvel, o->enthalpy, o->temp, o->pp, o->hnot, o->fracl,
                    o->fraclnot, o->sourceinput, o->rho, o->unot, o->vnot, o->wnot, o->pressure,
                    o->ap, o->an, o->as, o->ae, o->aw, o->at, o->ab, o->apnot, o->dux, o->dvy,
-                   o->dwz, o->su, o->sp, o->conc, o->concnot, o->concn};
+                   o->dwz, o->su, o->sp, o->conc, o->concnot, o->concn, o->csfrac, o->solfrac,
+                   o->mpphase, o->mpliq};
     for (size_t q = 0; q < sizeof(f) / sizeof(f[0]); q++) free(f[q]);
     free(o->tool_on);
     free(o->tool_id);
@@ -1631,7 +1682,7 @@ void orc_free(orc *o)
 
 void orc_dims(const orc *o, int *ni, int *nj, int *nk)
 {
-    *ni = o->ni; *nj = o->nj; *nk = o->nk;
+    *ni = o->ni; *nj = o->nj; *nk = o->nk_alloc;
 }
 
 /* Pointer to a named array inside the oracle state (for the test harness). */
@@ -1652,7 +1703,8 @@ double *orc_field(orc *o, const char *name)
         {"fracx", o->fracx}, {"fracy", o->fracy}, {"fracz", o->fracz}, {"heatin", o->heatin},
         {"areaij", o->areaij}, {"areajk", o->areajk}, {"areaik", o->areaik},
         {"avgconcentration", o->conc}, {"avgconcentrationnot", o->concnot},
-        {"concentration", o->concn}};
+        {"concentration", o->concn}, {"csfrac", o->csfrac}, {"solfrac", o->solfrac},
+        {"mpPhase", o->mpphase}, {"mpLiqPhase", o->mpliq}};
     for (size_t q = 0; q < sizeof(t) / sizeof(t[0]); q++)
         if (!strcmp(t[q].n, name)) return t[q].p;
     return NULL;

@@ -34,8 +34,10 @@
 static const char *kFields[] = {"temp", "uvel", "vvel", "wvel", "pressure", "enthalpy",
                                 "fracl", "pp", "diff", "rho", "vis", "hnot", "fraclnot"};
 static const int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
-// appended after kFields when the deck solves the species equation
+// appended after kFields when the deck solves the species equation, then the
+// powder-bed fields when it runs in powder-bed mode
 static const char *kSpeciesFields[] = {"avgconcentration", "concentration"};
+static const char *kPowderFields[] = {"csfrac", "solfrac", "mpPhase", "mpLiqPhase"};
 static const char *kGeom[] = {"x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv",
                               "fracx", "fracy"};
 static const int kNumGeom = sizeof(kGeom) / sizeof(kGeom[0]);
@@ -87,9 +89,13 @@ int main(int argc, char **argv)
     fflush(stdout);
     dup2(saved_stdout, 1);
 
-    const int ni = domainMgr->ni_, nj = domainMgr->nj_, nk = domainMgr->nk_;
+    // every array holds all powder layers; PrintManager::initialization has made
+    // only the first of them active (nk_)
+    const int ni = domainMgr->ni_, nj = domainMgr->nj_,
+              nk = domainMgr->nk_ + (meshObj.powderbed_ ? (domainMgr->numlayers_ - 1) * domainMgr->ncvzlayer_ : 0);
     const size_t n = (size_t)ni * nj * nk;
     const int nspecies = meshObj.species_ ? 2 : 0;
+    const int npowder = meshObj.powderbed_ ? 4 : 0;
     FILE *f = nullptr;
     if (!timing) {
         f = fopen(out.c_str(), "wb");
@@ -97,7 +103,7 @@ int main(int argc, char **argv)
         fwrite("AMCR", 1, 4, f);
         put_i32(f, 1);
         put_i32(f, ni); put_i32(f, nj); put_i32(f, nk);
-        put_i32(f, kNumFields + nspecies);
+        put_i32(f, kNumFields + nspecies + npowder);
         put_i32(f, kNumGeom);
         // geometry: 1-D arrays x,y,z (+ face arrays), each written at its own length
         for (int g = 0; g < kNumGeom; ++g) {
@@ -152,7 +158,7 @@ int main(int argc, char **argv)
             put_i32(f, (int)(sizeof(sc) / 8));
             fwrite(sc, 8, sizeof(sc) / 8, f);
             int ix[] = {bcMgr->istat_, bcMgr->iend_, bcMgr->jstat_, bcMgr->jend_, bcMgr->kstat_,
-                        bcMgr->jstart_, bcMgr->powerindicator_};
+                        bcMgr->jstart_, bcMgr->powerindicator_, domainMgr->nk_, bcMgr->trackindx_};
             put_i32(f, (int)(sizeof(ix) / 4));
             fwrite(ix, 4, sizeof(ix) / 4, f);
             for (int q = 0; q < kNumFields; ++q) {
@@ -161,6 +167,8 @@ int main(int argc, char **argv)
             }
             for (int q = 0; q < nspecies; ++q)
                 fwrite(solVarMgr->mapSolutionVars_[kSpeciesFields[q]], 8, n, f);
+            for (int q = 0; q < npowder; ++q)
+                fwrite(solVarMgr->mapSolutionVars_[kPowderFields[q]], 8, n, f);
         }
     }
     if (f) { put_i32(f, -1); fclose(f); }

@@ -24,9 +24,10 @@ from amcfd_dump import read_dump  # noqa: E402
 
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
+POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
 SCALARS = ("niter", "timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat",
-           "jstart", "resorc")
+           "jstart", "resorc", "nk_active", "trackindx")
 
 
 def species_deck():
@@ -42,6 +43,7 @@ def decks():
         D.small("g_noflow", nx=16, ny=10, nz=8, steps=4, fluid_flow=False),
         D.small("g_cooling", nx=16, ny=10, nz=8, steps=6, laser_off_after=3, scheme="upwind"),
         species_deck(),
+        D.powder_layers("g_powder"),
     ]
 
 
@@ -59,7 +61,8 @@ def main():
         steps = dump["steps"]
         rec = {f"s_{k}": np.array([s[k] for s in steps]) for k in SCALARS}
         for tag, s in (("first", steps[0]), ("last", steps[-1])):
-            for f in FIELDS + tuple(f for f in SPECIES_FIELDS if f in s):
+            extra = SPECIES_FIELDS + (POWDER_FIELDS if "csfrac" in s else ())
+            for f in FIELDS + tuple(f for f in extra if f in s):
                 rec[f"{tag}_{f}"] = s[f]
         for g, v in dump["geom"].items():
             rec[f"geom_{g}"] = v

@@ -114,10 +114,10 @@ def test_create_rejects_out_of_scope_modes(tmp_path):
     import amcfd_decks as D
     good = D.small("oos", steps=2).write(str(tmp_path))
     text = open(good).read()
-    bad = str(tmp_path / "powder.k")
-    _write(bad, text + "*POWDER_BED_MODE\n  1 8 0.04e-3 4330 0.25 357.7 0 0.995\n")
+    bad = str(tmp_path / "moving.k")
+    _write(bad, text + "*ACTIVATE_MOVING_MESH\n")
     d = amcfd.Deck(bad)
-    assert d.params.powderbed == 1
+    assert d.params.movingmesh == 1
     h = C.c_void_p()
     rc = amcfd.lib().amcfd_create(C.byref(d.params), None, C.byref(h))
     assert rc == -1  # rejected before any device work

@@ -15,12 +15,13 @@ import pytest
 
 from conftest import GOLDEN
 
-CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species"]
+CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species", "g_powder"]
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
+POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
 SCALARS = ("niter", "tpeak", "alen", "depth", "width", "ratio", "resorh", "resorm", "resoru",
            "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart",
-           "resorc")
+           "resorc", "nk_active", "trackindx")
 
 
 def _same(a, b):
@@ -38,7 +39,7 @@ def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
     for g in ("x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"):
         assert np.array_equal(o.field(g), ref[f"geom_{g}"]), g
     n = len(ref["s_niter"])
-    fields = FIELDS + tuple(f for f in SPECIES_FIELDS if f"first_{f}" in ref)
+    fields = FIELDS + tuple(f for f in SPECIES_FIELDS + POWDER_FIELDS if f"first_{f}" in ref)
     for s in range(n):
         r = o.step()
         for k in SCALARS:
@@ -70,13 +71,17 @@ def _variants():
     d = D.small("v_species", steps=4, power=250.0, scheme="upwind")
     d.species = (0.5, 2e-9, 0.1, 0.5)
     out.append(d)
+    # powder bed with the species equation: three layers of three planes each
+    d = D.powder_layers("v_powder", tracks=2, ncvzlayer=3, layerheight=40e-6, track_steps=3, dwell_steps=1)
+    d.species = (1.0, 5e-9, 0.3, 0.7)
+    out.append(d)
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(5))
+@pytest.mark.parametrize("idx", range(6))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
@@ -88,11 +93,13 @@ def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
                           env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
     ref = read_dump(out)
     o = oracle_py.Oracle(amcfd.Deck(path))
-    fields = FIELDS + (SPECIES_FIELDS if deck.species is not None else ())
+    fields = FIELDS + (SPECIES_FIELDS if deck.species is not None else ()) + \
+        (POWDER_FIELDS if deck.powder is not None else ())
     for s in ref["steps"]:
         r = o.step()
         assert r["niter"] == s["niter"]
         assert _same(r["tpeak"], s["tpeak"])
         assert _same(r["resorc"], s["resorc"])
+        assert r["nk_active"] == s["nk_active"] and r["trackindx"] == s["trackindx"]
         for f in fields:
             assert np.array_equal(o.field(f), s[f], equal_nan=True), (deck.name, s["step"], f)

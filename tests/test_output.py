@@ -27,14 +27,16 @@ REF_CLI = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 
 
 def read_vts(path):
-    """(header text, [arrays]) of an appended-raw .vts file."""
+    """(header text, [arrays]) of an appended-raw .vts file (Float64 arrays, and the
+    UInt8 vtkGhostType array of powder-bed runs, in header order)."""
     data = open(path, "rb").read()
     cut = data.index(b'<AppendedData encoding="raw">_') + len(b'<AppendedData encoding="raw">_')
     head, body = data[:cut].decode(), data[cut:]
+    types = ["<f8"] + ["u1" if 'type="UInt8"' in a else "<f8" for a in head.split("<DataArray")[2:]]
     arrays, pos = [], 0
     while body[pos:pos + 4] and not body[pos:].startswith(b"\n</AppendedData>"):
         (n,) = struct.unpack("<i", body[pos:pos + 4])
-        arrays.append(np.frombuffer(body[pos + 4:pos + 4 + n], dtype="<f8"))
+        arrays.append(np.frombuffer(body[pos + 4:pos + 4 + n], dtype=types[len(arrays)]).astype(np.float64))
         pos += 4 + n
     assert body[pos:] == b"\n</AppendedData> </VTKFile>"
     return head, arrays
@@ -61,12 +63,15 @@ def text_lines(path):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_CLI), reason="reference binary not built")
-@pytest.mark.parametrize("species", [False, True])
-def test_output_files_match_reference(species, tmp_path, monkeypatch):
+@pytest.mark.parametrize("variant", ["plain", "species", "powder"])
+def test_output_files_match_reference(variant, tmp_path, monkeypatch):
     import amcfd
     import amcfd_decks as D
-    d = D.small("outdeck", nx=20, ny=12, nz=8, steps=5, power=300.0)
-    if species:  # adds avgconcentration and concentration to the written fields
+    if variant == "powder":  # csfrac, solfrac and the vtkGhostType array of unbuilt layers
+        d = D.powder_layers("outdeck", nx=20, ny=12, nz=8)
+    else:
+        d = D.small("outdeck", nx=20, ny=12, nz=8, steps=5, power=300.0)
+    if variant == "species":  # adds avgconcentration and concentration to the written fields
         d.species = (1.0, 5e-9, 0.3, 0.7)
     d.outtime = 2 * d.dt
     d.final_geometry = "outdeck_geom.txt"
