@@ -56,7 +56,8 @@ class AmcfdParams(C.Structure):
         [(n, _I) for n in "powderbed movingmesh species freesurface".split()] + \
         [(n, _D) for n in "initconc massdiff kp urfc".split()] + \
         [(n, _I) for n in "numlayers ncvzlayer".split()] + \
-        [(n, _D) for n in "layerheight powderden powdercpa powdercpb powderthcona powderthconb".split()]
+        [(n, _D) for n in "layerheight powderden powdercpa powdercpb powderthcona powderthconb".split()] + \
+        [(n, _I) for n in "xmoveindex ymoveindex solidification".split()]
 
 
 class AmcfdReport(C.Structure):
@@ -65,7 +66,7 @@ class AmcfdReport(C.Structure):
                            "heatinlaser ahtoploss accul heatout heatvol beamposx beamposy "
                            "scanvel").split()] + \
         [(n, _I) for n in ("istat iend jstat jend kstat jstart powerindicator momentum_cells "
-                           "fallback").split()] + [("resorc", _D), ("nk_active", _I), ("trackindx", _I)]
+                           "fallback").split()] + [("resorc", _D), ("nk_active", _I), ("trackindx", _I), ("steadylength", _I)]
 
     def as_dict(self) -> Dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -99,6 +99,10 @@ class Deck:
     # *POWDER_BED_MODE: (layers, control volumes per layer, layer height, powder density,
     # powder cp a, cp b, powder conductivity a, b); csfrac and solfrac join *SCALAR_OUT
     powder: Optional[Tuple[int, int, float, float, float, float, float, float]] = None
+    # *ACTIVATE_MOVING_MESH: 1-based numbers of the x and y zones that follow the beam
+    moving_mesh: Optional[Tuple[int, int]] = None
+    # *CALCULATE_SOLIDIFICATION_PARAMETERS: G and R (grad, rate) join *SCALAR_OUT
+    solidification: bool = False
 
     @property
     def cells(self) -> Tuple[int, int, int]:
@@ -136,6 +140,7 @@ class Deck:
             "*SCALAR_OUT", "temp", "uvel", "vvel", "wvel",
             *(["avgconcentration", "concentration"] if self.species is not None else []),
             *(["csfrac", "solfrac"] if self.powder is not None else []),
+            *(["grad", "rate"] if self.solidification else []),
             "*CONTROL_TERMINATION", "$ total_time max_iter nonlin_tolerance",
             f"  {self.finaltime!r} {self.maxit} {self.tol!r}",
             "*CONTROL_TIMESTEP", "$ sim_timestep output_timestep",
@@ -167,6 +172,10 @@ class Deck:
         if self.species is not None:
             lines += ["*SOLVE_SPECIES", "$ initconc massdiff kp urfc",
                       "  " + " ".join(repr(float(v)) for v in self.species)]
+        if self.moving_mesh is not None:
+            lines += ["*ACTIVATE_MOVING_MESH", f"  {int(self.moving_mesh[0])} {int(self.moving_mesh[1])}"]
+        if self.solidification:
+            lines += ["*CALCULATE_SOLIDIFICATION_PARAMETERS"]
         if self.powder is not None:
             nl, ncv, *rest = self.powder
             lines += ["*POWDER_BED_MODE", "$ numlayers ncvlayer layerheight density cpa cpb thcona thconb",
@@ -236,6 +245,30 @@ def powder_layers(name: str = "powder", nx: int = 16, ny: int = 10, nz: int = 8,
     d.toolpath = rows
     d.single_track = None
     d.finaltime = t - 0.5 * d.dt
+    return d
+
+
+def moving_track(name: str = "moving", nx: int = 24, ny: int = 14, nz: int = 8, steps: int = 6,
+                 power: float = 250.0, speed: float = 1.0, angle_deg: float = 30.0,
+                 reverse: bool = False) -> Deck:
+    """Moving-mesh deck on the small parity grid: three x zones (fine middle zone
+    following the beam) over the small deck's three y zones, a straight toolpath
+    at angle_deg to +x (towards -x and -y with reverse=True), G and R requested.
+    A toolpath is needed: on the single-track path the reference never updates
+    the beam's previous y position, so its y zones drift by ystart every step."""
+    d = small(name, nx=nx, ny=ny, nz=nz, steps=steps, power=power)
+    lx, ly = 30e-6 * nx, 30e-6 * ny
+    nx1 = nx // 4
+    d.x_zones = [(lx * 0.3, nx1, -1.2), (lx * 0.4, nx - 2 * nx1, 1.0), (lx * 0.3, nx1, 1.2)]
+    d.moving_mesh = (2, 2)
+    d.solidification = True
+    ztop = _top(d.z_zones)
+    a = math.radians(angle_deg + (180.0 if reverse else 0.0))
+    x0, y0 = (lx * 0.35, ly * 0.4) if not reverse else (lx * 0.65, ly * 0.6)
+    t_end = d.finaltime * 4
+    d.toolpath = [(0.0, x0, y0, ztop, 0, 1),
+                  (t_end, x0 + speed * t_end * math.cos(a), y0 + speed * t_end * math.sin(a), ztop, 1, 1)]
+    d.single_track = None
     return d
 
 

@@ -16,7 +16,8 @@ SCALARS = ["timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "
            "depth", "width", "ratio", "heatinlaser", "ahtoploss", "accul", "heatout",
            "heatvol", "fluxwest", "fluxeast", "fluxtop", "fluxbottom", "fluxnorth",
            "fluxsouth", "beamposx", "beamposy", "scanvel", "resorc"]
-INDICES = ["istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator", "nk_active", "trackindx"]
+INDICES = ["istat", "iend", "jstat", "jend", "kstat", "jstart", "powerindicator", "nk_active", "trackindx",
+           "steadylength"]
 
 
 def read_dump(path: str) -> Dict:
@@ -33,12 +34,15 @@ def read_dump(path: str) -> Dict:
     assert buf[:4] == b"AMCR", "not a state dump"
     off = 4
     version = i32()
+    assert version == 2, "state dump version"
     ni, nj, nk = i32(), i32(), i32()
     nf, ng = i32(), i32()
     n = ni * nj * nk
-    # the optional groups follow the fixed fields: species (2), then powder bed (4)
-    extra = nf - len(FIELDS)
-    names = FIELDS + {0: [], 2: SPECIES_FIELDS, 4: POWDER_FIELDS, 6: SPECIES_FIELDS + POWDER_FIELDS}[extra]
+    names = []
+    for _ in range(nf):  # version 2: the field names
+        ln = i32()
+        names.append(buf[off:off + ln].decode())
+        off += ln
     geom = {}
     for g in range(ng):
         ln = i32()
@@ -61,5 +65,8 @@ def read_dump(path: str) -> Dict:
         for q in range(nf):
             rec[names[q]] = np.frombuffer(buf, "<f8", n, off).reshape(nk, nj, ni).copy()
             off += 8 * n
+        for g, ln in (("x", ni), ("y", nj)):
+            rec["grid_" + g] = np.frombuffer(buf, "<f8", ln, off).copy()
+            off += 8 * ln
         steps.append(rec)
     return {"version": version, "ni": ni, "nj": nj, "nk": nk, "geom": geom, "steps": steps}

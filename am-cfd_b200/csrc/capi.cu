@@ -91,6 +91,9 @@ struct amcfd_ctx {
            oldbeamposz = 0;
     int powerindicator = 1, init = 1, trackindx = 1, istart = 0, jstart = 0, vardt_state = 0;
     int itertot = 0, niter = 0;
+    int steadylength = 0;          // BoundCondManager::steadylength_ (moving mesh)
+    double *dmetric[12] = {};      // device copies of x y z xu yv zw dxpwinv dypsinv dzpbinv fracx fracy fracz
+    double *mesh_old = nullptr;    // moving mesh: centres before the move, x (ni) then y (nj)
     Inst<double> I64;
     Inst<float> I32;
     std::vector<void *> allocs;
@@ -156,25 +159,30 @@ static void zone_faces(int nz, const double *len, const double *ncv, const doubl
     }
 }
 
-static void build_grid(amcfd_ctx *c)
+// nkz: the z nodes whose centres are (re)computed -- every node at start-up, the
+// active ones when a moving mesh regenerates a powder-bed grid (the reference
+// then loops to nk_, leaving the planes above as they were).
+static void build_grid(amcfd_ctx *c, int nkz)
 {
     const amcfd_params &p = c->prm;
-    auto axis = [](int n, int nz, const double *len, const double *ncv, const double *powr,
+    auto axis = [](int n, int na, int nz, const double *len, const double *ncv, const double *powr,
                    std::vector<double> &face, std::vector<double> &cen, std::vector<double> &inv,
                    std::vector<double> &frac) {
-        face.assign(n + 1, 0.0);
-        cen.assign(n + 1, 0.0);
-        inv.assign(n + 1, 0.0);
-        frac.assign(n + 1, 0.0);
+        if (face.size() != (size_t)n + 1) {
+            face.assign(n + 1, 0.0);
+            cen.assign(n + 1, 0.0);
+            inv.assign(n + 1, 0.0);
+            frac.assign(n + 1, 0.0);
+        }
         zone_faces(nz, len, ncv, powr, face);
-        for (int q = 0; q < n - 1; q++) cen[q] = (face[q + 1] + face[q]) * 0.5;
-        cen[n - 1] = face[n - 1];
-        for (int q = 1; q < n; q++) inv[q] = 1.0 / (cen[q] - cen[q - 1]);
-        for (int q = 0; q < n - 1; q++) frac[q] = (cen[q + 1] - face[q + 1]) / (cen[q + 1] - cen[q]);
+        for (int q = 0; q < na - 1; q++) cen[q] = (face[q + 1] + face[q]) * 0.5;
+        cen[na - 1] = face[na - 1];
+        for (int q = 1; q < na; q++) inv[q] = 1.0 / (cen[q] - cen[q - 1]);
+        for (int q = 0; q < na - 1; q++) frac[q] = (cen[q + 1] - face[q + 1]) / (cen[q + 1] - cen[q]);
     };
-    axis(c->ni, p.nzx, p.xzone, p.ncvx, p.powrx, c->xu, c->x, c->dxpwinv, c->fracx);
-    axis(c->nj, p.nzy, p.yzone, p.ncvy, p.powry, c->yv, c->y, c->dypsinv, c->fracy);
-    axis(c->nk, p.nzz, p.zzone, p.ncvz, p.powrz, c->zw, c->z, c->dzpbinv, c->fracz);
+    axis(c->ni, c->ni, p.nzx, p.xzone, p.ncvx, p.powrx, c->xu, c->x, c->dxpwinv, c->fracx);
+    axis(c->nj, c->nj, p.nzy, p.yzone, p.ncvy, p.powry, c->yv, c->y, c->dypsinv, c->fracy);
+    axis(c->nk, nkz, p.nzz, p.zzone, p.ncvz, p.powrz, c->zw, c->z, c->dzpbinv, c->fracz);
 }
 
 // ---- laser position: BoundCondManager::getLaserCoords / updateLaser (:68-275) ----------
@@ -371,6 +379,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     g.x = m1[0]; g.y = m1[1]; g.z = m1[2]; g.xu = m1[3]; g.yv = m1[4]; g.zw = m1[5];
     g.dxpwinv = m1[6]; g.dypsinv = m1[7]; g.dzpbinv = m1[8]; g.fracx = m1[9]; g.fracy = m1[10];
     g.fracz = m1[11];
+    for (int a = 0; a < 12; a++) ctx->dmetric[a] = m1[a];
+    if (q.movingmesh && (rc = alloc3<double>(ctx, &ctx->mesh_old, (size_t)p.ni + p.nj))) return rc;
     T **f3[] = {&g.uvel, &g.vvel, &g.wvel, &g.unot, &g.vnot, &g.wnot, &g.pressure, &g.pp,
                 &g.h, &g.hnot, &g.temp, &g.fracl, &g.fraclnot, &g.sourceinput,
                 &g.diff_cur, &g.rho_cur, &g.vis_cur, &g.diff_nxt, &g.rho_nxt, &g.vis_nxt,
@@ -383,6 +393,9 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
             if ((rc = alloc3<T>(ctx, f, n3))) return rc;
     if (p.powder)
         for (T **f : {&g.csfrac, &g.solfrac, &g.mpphase, &g.mpliq})
+            if ((rc = alloc3<T>(ctx, f, n3))) return rc;
+    if (q.solidification)  // CFDSolverManager.cpp:469-472: zero until first written
+        for (T **f : {&g.grad, &g.rate})
             if ((rc = alloc3<T>(ctx, f, n3))) return rc;
     if ((rc = alloc3<double>(ctx, &g.heatin, (size_t)p.nj * p.nip))) return rc;
     if (q.nheattable > 0) {
@@ -588,6 +601,40 @@ static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
     }
 }
 
+// CFDSolverManager::generateGrid with the mesh following the beam (:72-124, 345-346):
+// the moving zones shift by the beam's displacement of this step, the grid is
+// rebuilt, its metrics replace the device copies and the fields are remapped.
+// Runs after the step's laser update, whose surface flux used the old grid.
+template <typename T>
+static int move_mesh(amcfd_ctx *ctx, Inst<T> &I)
+{
+    amcfd_params &p = ctx->prm;
+    const double dx = ctx->beamposx - ctx->oldbeamposx, dy = ctx->beamposy - ctx->oldbeamposy;
+    const int dirx = dx < 0 ? -1 : 1, diry = dy < 0 ? -1 : 1;
+    const int ix = p.xmoveindex, iy = ctx->steadylength ? p.ymoveindex : p.xmoveindex;
+    p.xzone[ix - 1] += dx;
+    p.xzone[ix + 1] -= dx;
+    p.yzone[iy - 1] += dy;
+    p.yzone[iy + 1] -= dy;
+    std::vector<double> old(ctx->x.begin(), ctx->x.begin() + ctx->ni);
+    old.insert(old.end(), ctx->y.begin(), ctx->y.begin() + ctx->nj);
+    build_grid(ctx, ctx->nk_active);
+    const std::vector<double> *src[12] = {&ctx->x, &ctx->y, &ctx->z, &ctx->xu, &ctx->yv, &ctx->zw,
+                                          &ctx->dxpwinv, &ctx->dypsinv, &ctx->dzpbinv,
+                                          &ctx->fracx, &ctx->fracy, &ctx->fracz};
+    for (int a = 0; a < 12; a++)
+        CK(cudaMemcpyAsync(ctx->dmetric[a], src[a]->data(), src[a]->size() * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->mesh_old, old.data(), old.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    launch_remap<T>(I, ctx->mesh_old, ctx->mesh_old + ctx->ni, dirx, diry);
+    // the host vectors above are pageable: each copy has been staged when its call returns,
+    // except for the local one, which must outlive its transfer
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->launches += 2;
+    return 0;
+}
+
 static int begin_step(amcfd_ctx *ctx)
 {
     const amcfd_params &p = ctx->prm;
@@ -631,6 +678,11 @@ static int begin_step(amcfd_ctx *ctx)
     }
     ctx->launches += 1;
     ctx->niter = 0;
+    if (p.movingmesh) {
+        const int rc = ctx->precision == AMCFD_PREC_FP64 ? move_mesh<double>(ctx, ctx->I64)
+                                                         : move_mesh<float>(ctx, ctx->I32);
+        if (rc) return rc;
+    }
     return 0;
 }
 
@@ -807,6 +859,7 @@ static void fill_report(amcfd_ctx *ctx, amcfd_step_report *r)
     r->resorc = s->resorc;
     r->nk_active = ctx->nk_active;
     r->trackindx = ctx->trackindx;
+    r->steadylength = ctx->steadylength;
 }
 
 // ---- learned warm start ----------------------------------------------------------------
@@ -886,8 +939,14 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     *out = ctx;
     ctx->prm = *params;
     amcfd_params &p = ctx->prm;
-    if (p.movingmesh || p.freesurface)
-        return fail(ctx, AMCFD_E_ARG, "moving mesh and free surface are not implemented");
+    if (p.freesurface) return fail(ctx, AMCFD_E_ARG, "the energy-balance free surface is not implemented");
+    if (p.movingmesh) {
+        // the zones either side of the moving one change length; before the melt pool
+        // reaches a steady length the y shift uses the x zone index (CFDSolverManager.cpp:108-115)
+        const int ix = p.xmoveindex, iy = p.ymoveindex;
+        if (ix < 1 || ix > p.nzx - 2 || iy < 1 || iy > p.nzy - 2 || ix > p.nzy - 2)
+            return fail(ctx, AMCFD_E_ARG, "*ACTIVATE_MOVING_MESH zones need a zone on either side");
+    }
     if (p.nzx < 1 || p.nzy < 1 || p.nzz < 1 || p.nzx > AMCFD_MAX_ZONES || p.nzy > AMCFD_MAX_ZONES ||
         p.nzz > AMCFD_MAX_ZONES)
         return fail(ctx, AMCFD_E_ARG, "bad zone counts");
@@ -935,7 +994,7 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     ctx->delt = p.nvardt > 0 ? ctx->vardt[1] : p.delt;
     ctx->outtime = p.nvardt > 0 ? ctx->vardt[2] : p.outtime;
     ctx->scanvel = p.scanvel;
-    build_grid(ctx);
+    build_grid(ctx, ctx->nk);
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     CK(cudaMalloc(&ctx->st_dev, sizeof(Status)));
@@ -1004,9 +1063,22 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report)
                                                : ws_before<float>(ctx, ctx->I32);
         if (rc) return rc;
     }
+    const double alenold = ctx->st_host->alen;
     rc = ctx->precision == AMCFD_PREC_FP64 ? outer_loop<double>(ctx, ctx->I64)
                                            : outer_loop<float>(ctx, ctx->I32);
     if (rc) return rc;
+    // iterativeLoopSolve :719-721: a step that used every outer iteration with an
+    // unchanged melt-pool length marks the length steady (for the moving mesh)
+    if (!(ctx->niter > 0 && ctx->st_host->converged) && std::fabs(ctx->st_host->alen - alenold) < 1.0e-6)
+        ctx->steadylength = 1;
+    // main.cpp:151-152
+    if (ctx->prm.solidification && ctx->st_host->tpeak > ctx->prm.tsolid) {
+        if (ctx->precision == AMCFD_PREC_FP64)
+            launch_solidification<double>(ctx->I64, ctx->scanvel);
+        else
+            launch_solidification<float>(ctx->I32, ctx->scanvel);
+        ctx->launches += 1;
+    }
     if (!ctx->prm.steady) {
         if (ctx->events) cudaEventRecord(ctx->ev[12], ctx->stream);
         if (ctx->precision == AMCFD_PREC_FP64)
@@ -1090,8 +1162,8 @@ int amcfd_ws_attach(amcfd_ctx *ctx, amcfd_net *net, int mode)
         return AMCFD_E_ARG;
     if (mode != AMCFD_WS_OFF && ctx->prm.nheattable > 0)
         return fail(ctx, AMCFD_E_ARG, "warm start with a volumetric heat-source table is not supported");
-    if (mode != AMCFD_WS_OFF && ctx->prm.powderbed)
-        return fail(ctx, AMCFD_E_ARG, "warm start on a growing powder-bed domain is not supported");
+    if (mode != AMCFD_WS_OFF && (ctx->prm.powderbed || ctx->prm.movingmesh))
+        return fail(ctx, AMCFD_E_ARG, "warm start on a growing or moving grid is not supported");
     CK(cudaSetDevice(ctx->device));
     ctx->net = net;
     ctx->ws_mode = mode;
@@ -1191,7 +1263,8 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
         {"avgconcentrationnot", offsetof(Fields<double>, concnot)},
         {"concentration", offsetof(Fields<double>, concn)},
         {"csfrac", offsetof(Fields<double>, csfrac)}, {"solfrac", offsetof(Fields<double>, solfrac)},
-        {"mpPhase", offsetof(Fields<double>, mpphase)}, {"mpLiqPhase", offsetof(Fields<double>, mpliq)}};
+        {"mpPhase", offsetof(Fields<double>, mpphase)}, {"mpLiqPhase", offsetof(Fields<double>, mpliq)},
+        {"grad", offsetof(Fields<double>, grad)}, {"rate", offsetof(Fields<double>, rate)}};
 #undef F
     // Fields<float> has the same member layout of pointers
     const char *base = ctx->precision == AMCFD_PREC_FP64 ? (const char *)&ctx->I64.g

@@ -126,7 +126,7 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
             {"*OUTPUT_SECTION", 29}, {"*VOLUMETRIC_HEAT_SOURCE_TABLE", 30},
             {"*CONTROL_TIMESTEP_VARIABLE", 31}};
         if (line == "*FLUID_FLOW_OFF") { p.navierstokes = 0; continue; }
-        if (line == "*CALCULATE_SOLIDIFICATION_PARAMETERS") continue;
+        if (line == "*CALCULATE_SOLIDIFICATION_PARAMETERS") { p.solidification = 1; continue; }
         auto it = kw.find(line);
         if (it != kw.end()) {
             option = it->second;
@@ -183,6 +183,11 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         case 20: v = numbers(line); evap.insert(evap.end(), v.begin(), v.end()); break;
         case 21: v = numbers(line); species.insert(species.end(), v.begin(), v.end()); break;
         case 22: w = words(line); if (!w.empty()) d->tool_file = w[0]; break;
+        case 23:  // Mesh.cpp:364-370: 1-based zone numbers
+            v = numbers(line);
+            if (v.size() < 2) return fail(AMCFD_E_PARSE, "*ACTIVATE_MOVING_MESH needs x and y zone numbers");
+            p.xmoveindex = (int)v[0] - 1; p.ymoveindex = (int)v[1] - 1;
+            break;
         case 25:
             w = words(line);
             if (!w.empty() && w[0] == "power_law") p.scheme = AMCFD_SCHEME_POWER_LAW;

@@ -97,6 +97,8 @@ struct Fields {
     // powder bed (null otherwise): consolidated fraction, solidified-track marker and
     // the track id of the last solid / liquid pass (updateSolutions)
     T *csfrac, *solfrac, *mpphase, *mpliq;
+    // solidification parameters (null otherwise): temperature gradient G and growth rate R
+    T *grad, *rate;
     double *heatin;     // nj*nip, Gaussian surface flux of the current step
     double *heattable;  // nheattable x 6
     // reductions

@@ -120,5 +120,8 @@ template <typename T> void setup_mom_small(Inst<T> &I);
 // species (k_species.cu)
 template <typename T> void launch_species(Inst<T> &I);
 template <typename T> void launch_species_update(Inst<T> &I);
+// moving mesh and solidification parameters (k_mesh.cu)
+template <typename T> void launch_remap(Inst<T> &I, const double *oldx, const double *oldy, int dirx, int diry);
+template <typename T> void launch_solidification(Inst<T> &I, double scanvel);
 
 }  // namespace amcfd

@@ -309,6 +309,8 @@ int amcfd_writer_create(amcfd_ctx *ctx, const amcfd_deck *deck, const char *root
         bool ok = species && (name == "avgconcentration" || name == "concentration");
         // with *POWDER_BED_MODE: CFDSolverManager.cpp:554-560
         ok |= powder && (name == "csfrac" || name == "solfrac" || name == "mpPhase" || name == "mpLiqPhase");
+        // with *CALCULATE_SOLIDIFICATION_PARAMETERS: :542-546
+        ok |= ctx_params(ctx).solidification && (name == "grad" || name == "rate");
         for (const char *k : known) ok |= name == k;
         if (!ok) continue;
         const std::string shown = name == "uvel" ? "auvel" : name == "vvel" ? "avvel" : name == "wvel" ? "awvel" : name;

@@ -88,7 +88,7 @@ typedef struct amcfd_params {
     /* *CONTROL_TIMESTEP_VARIABLE rows (t, delt, outtime), applied per step (main.cpp:125-134) */
     int nvardt;
     const double *vardt;     /* nvardt x 3 */
-    /* optional features: species and powder bed are solved; amcfd_create rejects the others */
+    /* optional features: amcfd_create rejects freesurface, solves the others */
     int powderbed, movingmesh, species, freesurface;
     /* *SOLVE_SPECIES row (DomainManager.cpp:123-129): initial concentration, mass
      * diffusivity, partition coefficient kp, under-relaxation factor urfc */
@@ -99,6 +99,11 @@ typedef struct amcfd_params {
      * layers to the last z-zone (:160-161). */
     int numlayers, ncvzlayer;
     double layerheight, powderden, powdercpa, powdercpb, powderthcona, powderthconb;
+    /* *ACTIVATE_MOVING_MESH row (Mesh.cpp:364-370): 0-based x and y zones that follow the
+     * beam (their neighbours grow and shrink, CFDSolverManager.cpp:72-124) */
+    int xmoveindex, ymoveindex;
+    /* *CALCULATE_SOLIDIFICATION_PARAMETERS (Mesh.cpp:58-61): G and R after every step */
+    int solidification;
 } amcfd_params;
 
 /* Per-step results, the scalars main() and PrintManager read after
@@ -116,6 +121,7 @@ typedef struct amcfd_step_report {
     double resorc;       /* species residual (calculateResiduals(6)); 0 without *SOLVE_SPECIES */
     int nk_active;       /* nodes in z of the active domain (grows per powder layer) */
     int trackindx;       /* BoundCondManager::trackindx_ */
+    int steadylength;    /* BoundCondManager::steadylength_ (moving mesh) */
 } amcfd_step_report;
 
 /* Line-sweep ordering of the line-by-line solver. */
@@ -171,8 +177,9 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
  * "temp","uvel","vvel","wvel","pressure","pp","enthalpy","fracl","fraclnot",
  * "hnot","diff","rho","vis","sourceinput"; with *SOLVE_SPECIES also "avgconcentration",
  * "avgconcentrationnot","concentration"; with *POWDER_BED_MODE also "csfrac","solfrac",
- * "mpPhase","mpLiqPhase"; grid arrays "x","y","z","xu","yv","zw".  Arrays cover the
- * whole grid (every powder layer, active or not). 
+ * "mpPhase","mpLiqPhase"; with *CALCULATE_SOLIDIFICATION_PARAMETERS also "grad","rate";
+ * grid arrays "x","y","z","xu","yv","zw" (the current ones under a moving mesh).  Arrays
+ * cover the whole grid (every powder layer, active or not). 
  * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
 int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out);
 int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in);

@@ -49,6 +49,8 @@ typedef struct orc {
     double *conc, *concnot, *concn;
     /* powder bed: csfrac, solfrac, mpPhase, mpLiqPhase */
     double *csfrac, *solfrac, *mpphase, *mpliq;
+    /* solidification parameters: G and R */
+    double *grad, *rate;
     double resoru, resorv, resorw, resorm, resorh, resorc, refmom;
     int itertot, niter;
     /* BoundCondManager state */
@@ -1490,6 +1492,83 @@ int orc_momentum(orc *o)
     return 1;
 }
 
+/* ---- moving mesh: generateGrid with !init_ (CFDSolverManager.cpp:72-124, 345-346) and
+ * remapSolutions (:2810-3051) ------------------------------------------------------- */
+static double interp_ref(double x0, double x1, double y0, double y1, double x)
+{
+    double yd = y1 - y0, xd = x1 - x0;
+    return y0 + (x - x0) * (yd / xd);
+}
+
+void orc_move_mesh(orc *o)
+{
+    amcfd_params *p = &o->p;
+    const int ni = o->ni, nj = o->nj, nk = o->nk;
+    const double dx = o->beamposx - o->oldbeamposx, dy = o->beamposy - o->oldbeamposy;
+    const int dirx = dx < 0 ? -1 : 1, diry = dy < 0 ? -1 : 1;
+    const int indx = p->xmoveindex, indy = p->ymoveindex;
+    p->xzone[indx - 1] += dx;
+    p->xzone[indx + 1] -= dx;
+    if (o->steadylength) {
+        p->yzone[indy - 1] += dy;
+        p->yzone[indy + 1] -= dy;
+    } else { /* the reference uses the x zone index here (:111-112) */
+        p->yzone[indx - 1] += dy;
+        p->yzone[indx + 1] -= dy;
+    }
+    double *oldx = dalloc(ni), *oldy = dalloc(nj);
+    memcpy(oldx, o->x, sizeof(double) * ni);
+    memcpy(oldy, o->y, sizeof(double) * nj);
+    generate_grid(o);
+    double *f[14] = {o->enthalpy, o->hnot, o->temp, o->fracl, o->uvel, o->vvel, o->wvel, o->unot,
+                     o->vnot, o->wnot, o->pressure, o->pp, o->conc, o->concnot};
+    const int nf = p->species ? 14 : 12;
+    for (int k = 0; k < nk; k++)
+        for (int j = 0; j < nj - 1; j++)
+            for (int i = 1; i < ni - 1; i++) {
+                size_t loc = ID(i, j, k);
+                if (fabs(oldx[i] - o->x[i]) > 1e-6)
+                    for (int q = 0; q < nf; q++)
+                        f[q][loc] = interp_ref(oldx[i], oldx[i + dirx], f[q][loc], f[q][loc + dirx], o->x[i]);
+            }
+    for (int k = 0; k < nk; k++)
+        for (int j = 0; j < nj - 1; j++)
+            for (int i = 1; i < ni - 1; i++) {
+                size_t loc = ID(i, j, k);
+                if (fabs(oldy[j] - o->y[j]) > 1e-6 && j + diry >= 0)
+                    for (int q = 0; q < nf; q++)
+                        f[q][loc] = interp_ref(oldy[j], oldy[j + diry], f[q][loc],
+                                               f[q][(size_t)((long long)loc + (long long)diry * ni)], o->y[j]);
+            }
+    free(oldx);
+    free(oldy);
+}
+
+/* ---- getSolidificationParameters: CFDSolverManager.cpp:2764-2804 ------------------
+ * Rows whose front lies at i < 2, on the j = 0 / nj-1 rows or the k = 0 plane are
+ * skipped: the reference reads outside its arrays there. */
+void orc_solidification(orc *o)
+{
+    if (o->tpeak <= o->p.tsolid) return;
+    const int ni = o->ni, nj = o->nj;
+    const double *t = o->temp;
+    for (int k = 0; k < o->nkm1; k++)
+        for (int j = 0; j < nj; j++)
+            for (int i = 0; i < ni; i++) {
+                if (t[ID(i, j, k)] >= o->p.tsolid) {
+                    if (i >= 2 && j >= 1 && j <= nj - 2 && k >= 1) {
+                        double gx = (t[ID(i, j, k)] - t[ID(i - 2, j, k)]) / (o->x[i] - o->x[i - 1]) / 2;
+                        double gy = (t[ID(i - 1, j + 1, k)] - t[ID(i - 1, j - 1, k)]) / (o->y[j] - o->y[j - 1]) / 2;
+                        double gz = (t[ID(i - 1, j, k + 1)] - t[ID(i - 1, j, k - 1)]) / (o->z[k] - o->z[k - 1]) / 2;
+                        size_t c = ID(i - 1, j, k);
+                        o->grad[c] = sqrt(gx * gx + gy * gy + gz * gz);
+                        o->rate[c] = o->scanvel * gx / o->grad[c];
+                    }
+                    break;
+                }
+            }
+}
+
 /* Species equation (iterativeLoopSolve :677-687). */
 void orc_species(orc *o)
 {
@@ -1553,6 +1632,7 @@ void orc_report(const orc *o, amcfd_step_report *r)
     r->resorc = o->resorc;
     r->nk_active = o->nk;
     r->trackindx = o->trackindx;
+    r->steadylength = o->steadylength;
 }
 
 /* Start of a time step, main.cpp:125-141: variable time step, timet += delt,
@@ -1574,7 +1654,9 @@ void orc_begin_step(orc *o)
 void orc_step(orc *o, amcfd_step_report *r)
 {
     orc_begin_step(o);
+    if (o->p.movingmesh) orc_move_mesh(o);    /* main.cpp:144-145 */
     orc_outer_loop(o);
+    if (o->p.solidification) orc_solidification(o);  /* :151-152 */
     if (!o->p.steady) orc_update_solutions(o);
     if (r) orc_report(o, r);
 }
@@ -1637,7 +1719,8 @@ orc *orc_create(const amcfd_params *params)
                      &o->fracl, &o->fraclnot, &o->sourceinput, &o->rho, &o->unot, &o->vnot,
                      &o->wnot, &o->pressure, &o->ap, &o->an, &o->as, &o->ae, &o->aw, &o->at,
                      &o->ab, &o->apnot, &o->dux, &o->dvy, &o->dwz, &o->su, &o->sp, &o->conc,
-                     &o->concnot, &o->concn, &o->csfrac, &o->solfrac, &o->mpphase, &o->mpliq};
+                     &o->concnot, &o->concn, &o->csfrac, &o->solfrac, &o->mpphase, &o->mpliq,
+                     &o->grad, &o->rate};
     for (size_t q = 0; q < sizeof(f3) / sizeof(f3[0]); q++) *f3[q] = dalloc(n);
     o->powerindicator = 1;
     o->init = 1;
@@ -1671,7 +1754,7 @@ void orc_free(orc *o)
                    o->fraclnot, o->sourceinput, o->rho, o->unot, o->vnot, o->wnot, o->pressure,
                    o->ap, o->an, o->as, o->ae, o->aw, o->at, o->ab, o->apnot, o->dux, o->dvy,
                    o->dwz, o->su, o->sp, o->conc, o->concnot, o->concn, o->csfrac, o->solfrac,
-                   o->mpphase, o->mpliq};
+                   o->mpphase, o->mpliq, o->grad, o->rate};
     for (size_t q = 0; q < sizeof(f) / sizeof(f[0]); q++) free(f[q]);
     free(o->tool_on);
     free(o->tool_id);
@@ -1704,7 +1787,7 @@ double *orc_field(orc *o, const char *name)
         {"areaij", o->areaij}, {"areajk", o->areajk}, {"areaik", o->areaik},
         {"avgconcentration", o->conc}, {"avgconcentrationnot", o->concnot},
         {"concentration", o->concn}, {"csfrac", o->csfrac}, {"solfrac", o->solfrac},
-        {"mpPhase", o->mpphase}, {"mpLiqPhase", o->mpliq}};
+        {"mpPhase", o->mpphase}, {"mpLiqPhase", o->mpliq}, {"grad", o->grad}, {"rate", o->rate}};
     for (size_t q = 0; q < sizeof(t) / sizeof(t[0]); q++)
         if (!strcmp(t[q].n, name)) return t[q].p;
     return NULL;

@@ -1,8 +1,9 @@
 // Dump/timing driver around the reference AM-CFD managers (test infrastructure).
 //
 // It reproduces the reference time loop of src/main.cpp:52-162 (construction,
-// PrintManager::initialization, updateLaser -> iterativeLoopSolve ->
-// updateSolutions per step) without the VTK/residual output, and writes a
+// PrintManager::initialization, updateLaser -> generateGrid (moving mesh) ->
+// iterativeLoopSolve -> getSolidificationParameters -> updateSolutions per
+// step) without the VTK/residual output, and writes a
 // binary record of the state after each selected step so that the C
 // restatement (oracle/amcfd_oracle.c) and the GPU path can be compared with
 // the reference's own arithmetic.  Built by oracle/build_ref.sh against the
@@ -38,6 +39,7 @@ static const int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
 // powder-bed fields when it runs in powder-bed mode
 static const char *kSpeciesFields[] = {"avgconcentration", "concentration"};
 static const char *kPowderFields[] = {"csfrac", "solfrac", "mpPhase", "mpLiqPhase"};
+static const char *kSolidFields[] = {"grad", "rate"};
 static const char *kGeom[] = {"x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv",
                               "fracx", "fracy"};
 static const int kNumGeom = sizeof(kGeom) / sizeof(kGeom[0]);
@@ -96,15 +98,24 @@ int main(int argc, char **argv)
     const size_t n = (size_t)ni * nj * nk;
     const int nspecies = meshObj.species_ ? 2 : 0;
     const int npowder = meshObj.powderbed_ ? 4 : 0;
+    const int nsolid = meshObj.solidificationparams_ ? 2 : 0;
+    std::vector<const char *> names(kFields, kFields + kNumFields);
+    names.insert(names.end(), kSpeciesFields, kSpeciesFields + nspecies);
+    names.insert(names.end(), kPowderFields, kPowderFields + npowder);
+    names.insert(names.end(), kSolidFields, kSolidFields + nsolid);
     FILE *f = nullptr;
     if (!timing) {
         f = fopen(out.c_str(), "wb");
         if (!f) { perror("fopen"); return 1; }
         fwrite("AMCR", 1, 4, f);
-        put_i32(f, 1);
+        put_i32(f, 2);  // version 2: the field names follow the field count
         put_i32(f, ni); put_i32(f, nj); put_i32(f, nk);
-        put_i32(f, kNumFields + nspecies + npowder);
+        put_i32(f, (int)names.size());
         put_i32(f, kNumGeom);
+        for (const char *nm : names) {
+            put_i32(f, (int)strlen(nm));
+            fwrite(nm, 1, strlen(nm), f);
+        }
         // geometry: 1-D arrays x,y,z (+ face arrays), each written at its own length
         for (int g = 0; g < kNumGeom; ++g) {
             const char *nm = kGeom[g];
@@ -135,7 +146,9 @@ int main(int argc, char **argv)
         auto t0 = std::chrono::high_resolution_clock::now();
         domainMgr->timet_ += meshObj.delt_;
         if (!domainMgr->steady_) bcMgr->updateLaser();
+        if (meshObj.movingmesh_) cfd->generateGrid();
         cfd->iterativeLoopSolve();
+        if (meshObj.solidificationparams_) cfd->getSolidificationParameters();
         if (!domainMgr->steady_) cfd->updateSolutions();
         auto t1 = std::chrono::high_resolution_clock::now();
         double dt_s = 1e-9 * std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count();
@@ -158,17 +171,13 @@ int main(int argc, char **argv)
             put_i32(f, (int)(sizeof(sc) / 8));
             fwrite(sc, 8, sizeof(sc) / 8, f);
             int ix[] = {bcMgr->istat_, bcMgr->iend_, bcMgr->jstat_, bcMgr->jend_, bcMgr->kstat_,
-                        bcMgr->jstart_, bcMgr->powerindicator_, domainMgr->nk_, bcMgr->trackindx_};
+                        bcMgr->jstart_, bcMgr->powerindicator_, domainMgr->nk_, bcMgr->trackindx_,
+                        (int)bcMgr->steadylength_};
             put_i32(f, (int)(sizeof(ix) / 4));
             fwrite(ix, 4, sizeof(ix) / 4, f);
-            for (int q = 0; q < kNumFields; ++q) {
-                const double *p = solVarMgr->mapSolutionVars_[kFields[q]];
-                fwrite(p, 8, n, f);
-            }
-            for (int q = 0; q < nspecies; ++q)
-                fwrite(solVarMgr->mapSolutionVars_[kSpeciesFields[q]], 8, n, f);
-            for (int q = 0; q < npowder; ++q)
-                fwrite(solVarMgr->mapSolutionVars_[kPowderFields[q]], 8, n, f);
+            for (const char *nm : names) fwrite(solVarMgr->mapSolutionVars_[nm], 8, n, f);
+            // the grid of this step (it moves with a moving mesh)
+            for (const char *nm : {"x", "y"}) fwrite(solVarMgr->mapGeometryVars_[nm], 8, nm[0] == 'x' ? ni : nj, f);
         }
     }
     if (f) { put_i32(f, -1); fclose(f); }

@@ -25,9 +25,10 @@ from amcfd_dump import read_dump  # noqa: E402
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
 POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
+MOVING_FIELDS = ("grad", "rate", "hnot", "grid_x", "grid_y")
 SCALARS = ("niter", "timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat",
-           "jstart", "resorc", "nk_active", "trackindx")
+           "jstart", "resorc", "nk_active", "trackindx", "steadylength")
 
 
 def species_deck():
@@ -44,6 +45,7 @@ def decks():
         D.small("g_cooling", nx=16, ny=10, nz=8, steps=6, laser_off_after=3, scheme="upwind"),
         species_deck(),
         D.powder_layers("g_powder"),
+        D.moving_track("g_moving"),
     ]
 
 
@@ -61,7 +63,8 @@ def main():
         steps = dump["steps"]
         rec = {f"s_{k}": np.array([s[k] for s in steps]) for k in SCALARS}
         for tag, s in (("first", steps[0]), ("last", steps[-1])):
-            extra = SPECIES_FIELDS + (POWDER_FIELDS if "csfrac" in s else ())
+            extra = SPECIES_FIELDS + (POWDER_FIELDS if "csfrac" in s else ()) + \
+                (MOVING_FIELDS if "grad" in s else ())
             for f in FIELDS + tuple(f for f in extra if f in s):
                 rec[f"{tag}_{f}"] = s[f]
         for g, v in dump["geom"].items():

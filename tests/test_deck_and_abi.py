@@ -114,10 +114,10 @@ def test_create_rejects_out_of_scope_modes(tmp_path):
     import amcfd_decks as D
     good = D.small("oos", steps=2).write(str(tmp_path))
     text = open(good).read()
-    bad = str(tmp_path / "moving.k")
-    _write(bad, text + "*ACTIVATE_MOVING_MESH\n")
+    bad = str(tmp_path / "freesurface.k")
+    _write(bad, text + "*TRACK_ENERGY_BASED_FREE_SURFACE\n")
     d = amcfd.Deck(bad)
-    assert d.params.movingmesh == 1
+    assert d.params.freesurface == 1
     h = C.c_void_p()
     rc = amcfd.lib().amcfd_create(C.byref(d.params), None, C.byref(h))
     assert rc == -1  # rejected before any device work

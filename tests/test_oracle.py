@@ -15,13 +15,14 @@ import pytest
 
 from conftest import GOLDEN
 
-CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species", "g_powder"]
+CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species", "g_powder", "g_moving"]
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
 POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
+MOVING_FIELDS = ("grad", "rate", "hnot")
 SCALARS = ("niter", "tpeak", "alen", "depth", "width", "ratio", "resorh", "resorm", "resoru",
            "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart",
-           "resorc", "nk_active", "trackindx")
+           "resorc", "nk_active", "trackindx", "steadylength")
 
 
 def _same(a, b):
@@ -39,7 +40,7 @@ def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
     for g in ("x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"):
         assert np.array_equal(o.field(g), ref[f"geom_{g}"]), g
     n = len(ref["s_niter"])
-    fields = FIELDS + tuple(f for f in SPECIES_FIELDS + POWDER_FIELDS if f"first_{f}" in ref)
+    fields = FIELDS + tuple(f for f in SPECIES_FIELDS + POWDER_FIELDS + MOVING_FIELDS if f"first_{f}" in ref)
     for s in range(n):
         r = o.step()
         for k in SCALARS:
@@ -48,6 +49,9 @@ def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
         if tag:
             for f in fields:
                 assert np.array_equal(o.field(f), ref[f"{tag}_{f}"], equal_nan=True), (case, s, f)
+            for g in ("x", "y"):  # the grid after the step (moves with a moving mesh)
+                if f"{tag}_grid_{g}" in ref:
+                    assert np.array_equal(o.field(g), ref[f"{tag}_grid_{g}"]), (case, s, g)
 
 
 def _variants():
@@ -75,13 +79,15 @@ def _variants():
     d = D.powder_layers("v_powder", tracks=2, ncvzlayer=3, layerheight=40e-6, track_steps=3, dwell_steps=1)
     d.species = (1.0, 5e-9, 0.3, 0.7)
     out.append(d)
+    # moving mesh towards -x and -y (the remap partner is the already-remapped node), with G/R
+    out.append(D.moving_track("v_moving", reverse=True, steps=5))
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(6))
+@pytest.mark.parametrize("idx", range(7))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
@@ -94,12 +100,14 @@ def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     ref = read_dump(out)
     o = oracle_py.Oracle(amcfd.Deck(path))
     fields = FIELDS + (SPECIES_FIELDS if deck.species is not None else ()) + \
-        (POWDER_FIELDS if deck.powder is not None else ())
+        (POWDER_FIELDS if deck.powder is not None else ()) + (MOVING_FIELDS if deck.solidification else ())
     for s in ref["steps"]:
         r = o.step()
         assert r["niter"] == s["niter"]
         assert _same(r["tpeak"], s["tpeak"])
         assert _same(r["resorc"], s["resorc"])
         assert r["nk_active"] == s["nk_active"] and r["trackindx"] == s["trackindx"]
+        assert r["steadylength"] == s["steadylength"]
+        assert np.array_equal(o.field("x"), s["grid_x"]) and np.array_equal(o.field("y"), s["grid_y"])
         for f in fields:
             assert np.array_equal(o.field(f), s[f], equal_nan=True), (deck.name, s["step"], f)

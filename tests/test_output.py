@@ -63,12 +63,14 @@ def text_lines(path):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_CLI), reason="reference binary not built")
-@pytest.mark.parametrize("variant", ["plain", "species", "powder"])
+@pytest.mark.parametrize("variant", ["plain", "species", "powder", "moving"])
 def test_output_files_match_reference(variant, tmp_path, monkeypatch):
     import amcfd
     import amcfd_decks as D
     if variant == "powder":  # csfrac, solfrac and the vtkGhostType array of unbuilt layers
         d = D.powder_layers("outdeck", nx=20, ny=12, nz=8)
+    elif variant == "moving":  # points follow the moving grid; grad and rate written
+        d = D.moving_track("outdeck", nx=20, ny=12, nz=8, steps=5)
     else:
         d = D.small("outdeck", nx=20, ny=12, nz=8, steps=5, power=300.0)
     if variant == "species":  # adds avgconcentration and concentration to the written fields
