@@ -57,7 +57,14 @@ class AmcfdParams(C.Structure):
         [(n, _D) for n in "initconc massdiff kp urfc".split()] + \
         [(n, _I) for n in "numlayers ncvzlayer".split()] + \
         [(n, _D) for n in "layerheight powderden powdercpa powdercpb powderthcona powderthconb".split()] + \
-        [(n, _I) for n in "xmoveindex ymoveindex solidification".split()]
+        [(n, _I) for n in "xmoveindex ymoveindex solidification".split()] + \
+        [(n, _D) for n in ("fs_lam1 fs_lam2 fs_surftens fs_maxiterenergy fs_tolenergy fs_maxiterbisect "
+                           "fs_tolbisect fs_urfree").split()]
+
+
+class AmcfdFreeSurface(C.Structure):
+    _fields_ = [(n, _D) for n in "lambda residual fi_min fi_max volume".split()] + \
+        [("iterations", _I), ("bracketed", _I)]
 
 
 class AmcfdReport(C.Structure):
@@ -118,6 +125,7 @@ def lib() -> C.CDLL:
             L.amcfd_phase_name.restype = C.c_char_p
             L.amcfd_last_timing.argtypes = [VP, P(_D), _I]
             L.amcfd_profile.argtypes = [VP, _I]
+            L.amcfd_free_surface.argtypes = [VP, P(AmcfdFreeSurface)]
             L.amcfd_run_steps.argtypes = [VP, _I, P(AmcfdReport), P(_D)]
             L.amcfd_kernel_launches.argtypes = [VP]
             L.amcfd_kernel_launches.restype = C.c_longlong
@@ -382,6 +390,12 @@ class Solver:
 
     TIMING_SLOTS = ("energy_assemble", "factor", "energy_sweeps", "h2t_meltpool", "momentum",
                     "converge", "laser", "update", "outer_iters", "sweep_launches", "species")
+
+    def free_surface(self) -> Dict:
+        """amcfd_free_surface: the energy-balance free surface on the current state."""
+        r = AmcfdFreeSurface()
+        self._check(lib().amcfd_free_surface(self._h, C.byref(r)))
+        return {name: getattr(r, name) for name, _ in r._fields_}
 
     def timing(self, n: int = 16) -> Dict:
         out = np.zeros(n, dtype=np.float64)

@@ -103,6 +103,10 @@ class Deck:
     moving_mesh: Optional[Tuple[int, int]] = None
     # *CALCULATE_SOLIDIFICATION_PARAMETERS: G and R (grad, rate) join *SCALAR_OUT
     solidification: bool = False
+    # *TRACK_ENERGY_BASED_FREE_SURFACE: (lambda1, lambda2, surface tension, energy iterations,
+    # energy tolerance, bisection iterations, bisection tolerance, under-relaxation); zr and
+    # tempr join *SCALAR_OUT
+    free_surface: Optional[Tuple[float, float, float, int, float, int, float, float]] = None
 
     @property
     def cells(self) -> Tuple[int, int, int]:
@@ -141,6 +145,7 @@ class Deck:
             *(["avgconcentration", "concentration"] if self.species is not None else []),
             *(["csfrac", "solfrac"] if self.powder is not None else []),
             *(["grad", "rate"] if self.solidification else []),
+            *(["zr", "tempr"] if self.free_surface is not None else []),
             "*CONTROL_TERMINATION", "$ total_time max_iter nonlin_tolerance",
             f"  {self.finaltime!r} {self.maxit} {self.tol!r}",
             "*CONTROL_TIMESTEP", "$ sim_timestep output_timestep",
@@ -176,6 +181,10 @@ class Deck:
             lines += ["*ACTIVATE_MOVING_MESH", f"  {int(self.moving_mesh[0])} {int(self.moving_mesh[1])}"]
         if self.solidification:
             lines += ["*CALCULATE_SOLIDIFICATION_PARAMETERS"]
+        if self.free_surface is not None:
+            lines += ["*TRACK_ENERGY_BASED_FREE_SURFACE",
+                      "$ lambda1 lambda2 surftens maxiter_energy tol_energy maxiter_bisect tol_bisect urf",
+                      "  " + " ".join(repr(float(v)) for v in self.free_surface)]
         if self.powder is not None:
             nl, ncv, *rest = self.powder
             lines += ["*POWDER_BED_MODE", "$ numlayers ncvlayer layerheight density cpa cpb thcona thconb",
@@ -269,6 +278,15 @@ def moving_track(name: str = "moving", nx: int = 24, ny: int = 14, nz: int = 8, 
     d.toolpath = [(0.0, x0, y0, ztop, 0, 1),
                   (t_end, x0 + speed * t_end * math.cos(a), y0 + speed * t_end * math.sin(a), ztop, 1, 1)]
     d.single_track = None
+    return d
+
+
+def free_surface_track(name: str = "freesurf", steps: int = 4, power: float = 250.0) -> Deck:
+    """The small parity deck with the energy-balance free surface: multiplier bracket
+    [-1e5, 1e5], surface tension 1.8 N/m, 30 relaxation sweeps (tolerance 1e-6),
+    up to 40 bisections to a volume residual of 1e-18 m^3, relaxation 0.5."""
+    d = small(name, steps=steps, power=power)
+    d.free_surface = (-1e5, 1e5, 1.8, 30, 1e-6, 40, 1e-18, 0.5)
     return d
 
 

@@ -94,6 +94,7 @@ struct amcfd_ctx {
     int steadylength = 0;          // BoundCondManager::steadylength_ (moving mesh)
     double *dmetric[12] = {};      // device copies of x y z xu yv zw dxpwinv dypsinv dzpbinv fracx fracy fracz
     double *mesh_old = nullptr;    // moving mesh: centres before the move, x (ni) then y (nj)
+    FsOut *fs_out = nullptr;       // free surface: the bisection's results (device)
     Inst<double> I64;
     Inst<float> I32;
     std::vector<void *> allocs;
@@ -397,6 +398,15 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     if (q.solidification)  // CFDSolverManager.cpp:469-472: zero until first written
         for (T **f : {&g.grad, &g.rate})
             if ((rc = alloc3<T>(ctx, f, n3))) return rc;
+    if (q.freesurface) {
+        if ((rc = alloc3<double>(ctx, &g.fs_fi, (size_t)p.nj * p.nip)) ||
+            (rc = alloc3<double>(ctx, &g.fs_zz, (size_t)p.nj * p.nip)) || (rc = alloc3<T>(ctx, &g.fs_zr, n3)) ||
+            (rc = alloc3<T>(ctx, &g.fs_tempr, n3)))
+            return rc;
+        double *o = nullptr;
+        if ((rc = alloc3<double>(ctx, &o, (sizeof(FsOut) + 7) / 8))) return rc;
+        ctx->fs_out = reinterpret_cast<FsOut *>(o);
+    }
     if ((rc = alloc3<double>(ctx, &g.heatin, (size_t)p.nj * p.nip))) return rc;
     if (q.nheattable > 0) {
         if ((rc = alloc3<double>(ctx, &g.heattable, ctx->heattable.size()))) return rc;
@@ -499,6 +509,13 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     if (p.species && ((rc = fill(g.conc, q.initconc)) || (rc = fill(g.concnot, q.initconc)) ||
                       (rc = fill(g.concn, q.initconc))))
         return rc;
+    if (q.freesurface) {
+        // FreeSurfaceManager::initializeFreeSurface (:34-69): zr = z, tempr = T, fi = 0
+        std::vector<double> zr(n3);
+        for (int k = 0; k < p.nk; k++)
+            std::fill(zr.begin() + (size_t)k * p.nj * p.nip, zr.begin() + (size_t)(k + 1) * p.nj * p.nip, ctx->z[k]);
+        if ((rc = upload<T>(ctx, g.fs_zr, zr)) || (rc = fill(g.fs_tempr, q.temppreheat))) return rc;
+    }
     if (p.powder) {
         // CFDSolverManager.cpp:482-492: the base plate is consolidated, the build
         // layers are powder (csfrac 0); solfrac, mpPhase, mpLiqPhase start at 0
@@ -939,7 +956,8 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     *out = ctx;
     ctx->prm = *params;
     amcfd_params &p = ctx->prm;
-    if (p.freesurface) return fail(ctx, AMCFD_E_ARG, "the energy-balance free surface is not implemented");
+    if (p.freesurface && (p.fs_maxiterenergy < 0 || p.fs_maxiterbisect < 0))
+        return fail(ctx, AMCFD_E_ARG, "*TRACK_ENERGY_BASED_FREE_SURFACE iteration counts must not be negative");
     if (p.movingmesh) {
         // the zones either side of the moving one change length; before the melt pool
         // reaches a steady length the y shift uses the x zone index (CFDSolverManager.cpp:108-115)
@@ -1214,6 +1232,43 @@ int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, doubl
 
 long long amcfd_kernel_launches(const amcfd_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
+int amcfd_free_surface(amcfd_ctx *ctx, amcfd_free_surface_report *out)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    const amcfd_params &p = ctx->prm;
+    if (!p.freesurface) return fail(ctx, AMCFD_E_ARG, "the deck has no *TRACK_ENERGY_BASED_FREE_SURFACE");
+    CK(cudaSetDevice(ctx->device));
+    // the evaporated volume to match (FreeSurfaceManager.cpp:93-124; vdp and the
+    // start delay are constants there)
+    const double vdp = 2e-9, startdeltn = 0.0;
+    double melttime = ctx->delt * (1.0 + startdeltn), vd;
+    if (ctx->st_host->tpeak <= p.tsolid) {
+        vd = 0.0;
+        melttime = 0.0;
+    } else {
+        vd = vdp * (ctx->timet - melttime - startdeltn * ctx->delt);
+        if (ctx->powerindicator < 1) vd = vdp * (p.lasertime - melttime);
+    }
+    FsIn a;
+    a.lam1 = p.fs_lam1; a.lam2 = p.fs_lam2; a.gamma = p.fs_surftens; a.c1 = p.dens * p.grav;
+    a.urf = p.fs_urfree; a.tol_e = p.fs_tolenergy; a.tol_b = p.fs_tolbisect; a.vd = vd;
+    a.maxit_e = (int)p.fs_maxiterenergy; a.maxit_b = (int)p.fs_maxiterbisect;
+    if (ctx->precision == AMCFD_PREC_FP64)
+        launch_free_surface<double>(ctx->I64, a, ctx->fs_out);
+    else
+        launch_free_surface<float>(ctx->I32, a, ctx->fs_out);
+    ctx->launches += 2;
+    FsOut h;
+    CK(cudaMemcpyAsync(&h, ctx->fs_out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaGetLastError());
+    if (out) {
+        out->lambda = h.xmid; out->residual = h.fmid; out->fi_min = h.fimin; out->fi_max = h.fimax;
+        out->volume = vd; out->iterations = h.niter; out->bracketed = h.bracketed;
+    }
+    return 0;
+}
+
 int amcfd_run_phase(amcfd_ctx *ctx, int phase, amcfd_step_report *report)
 {
     if (!ctx) return AMCFD_E_ARG;
@@ -1264,7 +1319,8 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
         {"concentration", offsetof(Fields<double>, concn)},
         {"csfrac", offsetof(Fields<double>, csfrac)}, {"solfrac", offsetof(Fields<double>, solfrac)},
         {"mpPhase", offsetof(Fields<double>, mpphase)}, {"mpLiqPhase", offsetof(Fields<double>, mpliq)},
-        {"grad", offsetof(Fields<double>, grad)}, {"rate", offsetof(Fields<double>, rate)}};
+        {"grad", offsetof(Fields<double>, grad)}, {"rate", offsetof(Fields<double>, rate)},
+        {"zr", offsetof(Fields<double>, fs_zr)}, {"tempr", offsetof(Fields<double>, fs_tempr)}};
 #undef F
     // Fields<float> has the same member layout of pointers
     const char *base = ctx->precision == AMCFD_PREC_FP64 ? (const char *)&ctx->I64.g

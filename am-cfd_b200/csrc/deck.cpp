@@ -104,7 +104,7 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
     p.scheme = AMCFD_SCHEME_UPWIND;  // Mesh.h:59
     p.navierstokes = 1;
     std::vector<double> proc, mat, relax, btemp, benergy, bmom, gauss, evap, volsrc, species,
-        powder;
+        powder, freesurf;
     std::map<std::string, double> parameters;
     bool have_timestep = false, have_term = false, udtool = false, volsrc_on = false,
          voltable = false;
@@ -183,6 +183,7 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         case 20: v = numbers(line); evap.insert(evap.end(), v.begin(), v.end()); break;
         case 21: v = numbers(line); species.insert(species.end(), v.begin(), v.end()); break;
         case 22: w = words(line); if (!w.empty()) d->tool_file = w[0]; break;
+        case 24: v = numbers(line); freesurf.insert(freesurf.end(), v.begin(), v.end()); break;
         case 23:  // Mesh.cpp:364-370: 1-based zone numbers
             v = numbers(line);
             if (v.size() < 2) return fail(AMCFD_E_PARSE, "*ACTIVATE_MOVING_MESH needs x and y zone numbers");
@@ -291,6 +292,12 @@ extern "C" int amcfd_deck_load(const char *path, amcfd_deck **out)
         if (p.nzz < 1) return fail(AMCFD_E_PARSE, "*POWDER_BED_MODE needs a z grid");
         p.zzone[p.nzz - 1] += p.numlayers * p.layerheight;
         p.ncvz[p.nzz - 1] += p.numlayers * p.ncvzlayer;
+    }
+    if (p.freesurface) {  // DomainManager.cpp:133-143
+        if (freesurf.size() < 8) return fail(AMCFD_E_PARSE, "*TRACK_ENERGY_BASED_FREE_SURFACE needs 8 values");
+        p.fs_lam1 = freesurf[0]; p.fs_lam2 = freesurf[1]; p.fs_surftens = freesurf[2];
+        p.fs_maxiterenergy = freesurf[3]; p.fs_tolenergy = freesurf[4]; p.fs_maxiterbisect = freesurf[5];
+        p.fs_tolbisect = freesurf[6]; p.fs_urfree = freesurf[7];
     }
     if (p.species) {  // DomainManager.cpp:123-129
         if (species.size() < 4) return fail(AMCFD_E_PARSE, "*SOLVE_SPECIES needs 4 values");

@@ -99,6 +99,10 @@ struct Fields {
     T *csfrac, *solfrac, *mpphase, *mpliq;
     // solidification parameters (null otherwise): temperature gradient G and growth rate R
     T *grad, *rate;
+    // energy-balance free surface (null otherwise): deflection fi and its iterate
+    // ([j][nip], FP64), deformed heights zr and the temperatures on them
+    double *fs_fi, *fs_zz;
+    T *fs_zr, *fs_tempr;
     double *heatin;     // nj*nip, Gaussian surface flux of the current step
     double *heattable;  // nheattable x 6
     // reductions

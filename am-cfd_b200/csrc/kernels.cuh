@@ -123,5 +123,15 @@ template <typename T> void launch_species_update(Inst<T> &I);
 // moving mesh and solidification parameters (k_mesh.cu)
 template <typename T> void launch_remap(Inst<T> &I, const double *oldx, const double *oldy, int dirx, int diry);
 template <typename T> void launch_solidification(Inst<T> &I, double scanvel);
+// energy-balance free surface (k_freesurf.cu)
+struct FsIn {
+    double lam1, lam2, gamma, c1, urf, tol_e, tol_b, vd;
+    int maxit_e, maxit_b;
+};
+struct FsOut {
+    double xmid, fmid, fimin, fimax;
+    int niter, bracketed;
+};
+template <typename T> void launch_free_surface(Inst<T> &I, const FsIn &a, FsOut *out_dev);
 
 }  // namespace amcfd

@@ -123,8 +123,14 @@ static int write_vts(amcfd_writer *w, const std::string &path)
     h << "</StructuredGrid> ";
     h << "<AppendedData encoding=\"raw\">_";
     f << h.str();
-    // points
+    // points; with the free surface z is the deformed height zr (vtsBinWriter.cpp:164-171)
     {
+        const bool deformed = ctx_params(ctx).freesurface != 0;
+        if (deformed) {
+            const int rc = amcfd_get_field(ctx, "zr", w->pinned[0]);
+            if (rc) return werr(w, rc, ctx_error(ctx));
+        }
+        const double *zr = w->pinned[0];
         int32_t bytes = (int32_t)(sizeof(double) * npts * 3);
         f.write((const char *)&bytes, sizeof(bytes));
         std::vector<double> row((size_t)ni * 3);
@@ -133,7 +139,7 @@ static int write_vts(amcfd_writer *w, const std::string &path)
                 for (int i = 0; i < ni; i++) {
                     row[3 * i] = (*x)[i];
                     row[3 * i + 1] = (*y)[j];
-                    row[3 * i + 2] = (*z)[k];
+                    row[3 * i + 2] = deformed ? zr[((size_t)k * nj + j) * ni + i] : (*z)[k];
                 }
                 f.write((const char *)row.data(), row.size() * sizeof(double));
             }
@@ -268,11 +274,33 @@ static int write_residuals(amcfd_writer *w)
     return o ? 0 : werr(w, AMCFD_E_IO, "write failed: residuals");
 }
 
+// FreeSurfaceManager::execute and its monitor line (FreeSurfaceManager.cpp:74-209)
+static int free_surface(amcfd_writer *w)
+{
+    amcfd_free_surface_report f;
+    const int rc = amcfd_free_surface(w->ctx, &f);
+    if (rc) return werr(w, rc, ctx_error(w->ctx));
+    amcfd_step_report r;
+    ctx_report(w->ctx, &r);
+    std::ofstream o(joinp(w->root, w->base + "_FreeSurfaceMonitor.txt"), std::ios::out | std::ios::app);
+    if (!o) return werr(w, AMCFD_E_IO, "cannot open free-surface monitor file");
+    const char *bar = "====================================================================================================\n";
+    o << bar;
+    o << "  time         lambda        res_bisect    min_fi         max_fi        droplet_volume   iter_bisect\n";
+    o << std::setprecision(4) << std::scientific << std::setw(12) << r.timet << std::setw(14) << f.lambda
+      << std::setw(14) << f.residual << std::setw(14) << f.fi_min << std::setw(14) << f.fi_max << std::setw(14)
+      << f.volume << std::setw(9) << f.iterations << "\n";
+    o << bar;
+    return o ? 0 : werr(w, AMCFD_E_IO, "write failed: free-surface monitor");
+}
+
 static int write_output(amcfd_writer *w, bool residuals = true)
 {
     if (residuals) w->outct++;
     const std::string file = w->directory + "/" + w->base + "_" + std::to_string(w->outct) + ".vts";
     int rc;
+    // main.cpp:174-176, 210-212: the free surface is updated before each output but the first
+    if (residuals && ctx_params(w->ctx).freesurface && (rc = free_surface(w))) return rc;
     if (residuals && (rc = write_residuals(w))) return rc;
     if ((rc = write_vts(w, file))) return rc;
     amcfd_step_report r;
@@ -311,6 +339,7 @@ int amcfd_writer_create(amcfd_ctx *ctx, const amcfd_deck *deck, const char *root
         ok |= powder && (name == "csfrac" || name == "solfrac" || name == "mpPhase" || name == "mpLiqPhase");
         // with *CALCULATE_SOLIDIFICATION_PARAMETERS: :542-546
         ok |= ctx_params(ctx).solidification && (name == "grad" || name == "rate");
+        ok |= ctx_params(ctx).freesurface && (name == "zr" || name == "tempr");  // FreeSurfaceManager.cpp:67-68
         for (const char *k : known) ok |= name == k;
         if (!ok) continue;
         const std::string shown = name == "uvel" ? "auvel" : name == "vvel" ? "avvel" : name == "wvel" ? "awvel" : name;

@@ -88,7 +88,7 @@ typedef struct amcfd_params {
     /* *CONTROL_TIMESTEP_VARIABLE rows (t, delt, outtime), applied per step (main.cpp:125-134) */
     int nvardt;
     const double *vardt;     /* nvardt x 3 */
-    /* optional features: amcfd_create rejects freesurface, solves the others */
+    /* optional features (all solved) */
     int powderbed, movingmesh, species, freesurface;
     /* *SOLVE_SPECIES row (DomainManager.cpp:123-129): initial concentration, mass
      * diffusivity, partition coefficient kp, under-relaxation factor urfc */
@@ -104,6 +104,11 @@ typedef struct amcfd_params {
     int xmoveindex, ymoveindex;
     /* *CALCULATE_SOLIDIFICATION_PARAMETERS (Mesh.cpp:58-61): G and R after every step */
     int solidification;
+    /* *TRACK_ENERGY_BASED_FREE_SURFACE row (DomainManager.cpp:133-143): bisection interval
+     * of the pressure multiplier, surface tension, energy-balance iterations and
+     * tolerance, bisection iterations and tolerance, under-relaxation */
+    double fs_lam1, fs_lam2, fs_surftens, fs_maxiterenergy, fs_tolenergy, fs_maxiterbisect,
+        fs_tolbisect, fs_urfree;
 } amcfd_params;
 
 /* Per-step results, the scalars main() and PrintManager read after
@@ -178,6 +183,7 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
  * "hnot","diff","rho","vis","sourceinput"; with *SOLVE_SPECIES also "avgconcentration",
  * "avgconcentrationnot","concentration"; with *POWDER_BED_MODE also "csfrac","solfrac",
  * "mpPhase","mpLiqPhase"; with *CALCULATE_SOLIDIFICATION_PARAMETERS also "grad","rate";
+ * with *TRACK_ENERGY_BASED_FREE_SURFACE also "zr","tempr" (as of the last amcfd_free_surface);
  * grid arrays "x","y","z","xu","yv","zw" (the current ones under a moving mesh).  Arrays
  * cover the whole grid (every powder layer, active or not). 
  * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
@@ -237,6 +243,23 @@ long long amcfd_kernel_launches(const amcfd_ctx *ctx);
  * sweep is many such runs. */
 int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nthreads,
                     amcfd_step_report *reports, int *status);
+
+/* Energy-balance free surface (FreeSurfaceManager::execute, FreeSurfaceManager.cpp:74-209):
+ * the surface deflection of the molten top nodes that balances gravity, surface
+ * tension and a pressure multiplier found by bisection so that the deflected volume
+ * matches the evaporated volume; then the deformed node heights "zr" and the
+ * temperatures interpolated onto them, "tempr".  The reference runs it before each
+ * output (main.cpp:174-176, 210-212); the output writer does the same.  Decks without
+ * *TRACK_ENERGY_BASED_FREE_SURFACE: AMCFD_E_ARG. */
+typedef struct amcfd_free_surface_report {
+    double lambda;     /* the last multiplier tried (xmid) */
+    double residual;   /* its volume residual (fmid) */
+    double fi_min, fi_max;  /* extremes of the deflection over the surface */
+    double volume;     /* the target volume vd */
+    int iterations;    /* bisection iterations run */
+    int bracketed;     /* 0 where the initial interval did not bracket the root (the reference warns) */
+} amcfd_free_surface_report;
+int amcfd_free_surface(amcfd_ctx *ctx, amcfd_free_surface_report *out);
 
 /* ---- Output writer (main.cpp:92-226, PrintManager.cpp, vtsBinWriter.cpp) ------
  * Writes what the reference's transient run writes, in its formats:

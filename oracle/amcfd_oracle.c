@@ -21,6 +21,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <float.h>
+
 #include "../include/amcfd.h"
 
 #define MAXD(a, b) (((a) < (b)) ? (b) : (a))
@@ -51,6 +53,9 @@ typedef struct orc {
     double *csfrac, *solfrac, *mpphase, *mpliq;
     /* solidification parameters: G and R */
     double *grad, *rate;
+    /* free surface: deflection fi and its iterate zzm ([j][i]), deformed heights zr and
+     * the temperatures on them */
+    double *fi, *zzm, *zr, *tempr;
     double resoru, resorv, resorw, resorm, resorh, resorc, refmom;
     int itertot, niter;
     /* BoundCondManager state */
@@ -1569,6 +1574,119 @@ void orc_solidification(orc *o)
             }
 }
 
+/* ---- energy-balance free surface: FreeSurfaceManager.cpp:74-341 -------------------- */
+static void fs_ebal(orc *o, double alambda)
+{
+    const int ni = o->ni, nj = o->nj, nim1 = o->nim1, njm1 = o->njm1, nkm1 = o->nkm1;
+    const amcfd_params *p = &o->p;
+    const int nitermax = (int)p->fs_maxiterenergy;
+    const double c1 = p->dens * p->grav, gamma = p->fs_surftens, urfree = p->fs_urfree, tol = p->fs_tolenergy;
+    const double *x = o->x, *y = o->y, *xu = o->xu, *yv = o->yv;
+    double *zzm = o->zzm, *fi = o->fi;
+    int niter = 0;
+    double difmax = 0.0;  /* not reset per sweep (:262, 298-300) */
+    for (int loc = 0; loc < ni * nj; loc++) zzm[loc] = 0.0;
+    while (niter < nitermax) {
+        niter++;
+        /* one thread of the reference's max reduction: a private maximum starting at the
+         * lowest double, folded into the shared one after the sweep */
+        double priv = -DBL_MAX;
+        for (int j = 1; j < njm1; j++)
+            for (int i = 1; i < nim1; i++) {
+                if (o->temp[ID(i, j, nkm1)] < p->tsolid) continue;
+                double dely = yv[j + 1] - yv[j - 1], dely1 = y[j + 1] - y[j - 1];
+                double delyp = y[j + 1] - y[j], delym = y[j] - y[j - 1];
+                double delx = xu[i + 1] - xu[i - 1], delx1 = x[i + 1] - x[i - 1];
+                double delxp = x[i + 1] - x[i], delxm = x[i] - x[i - 1];
+                double c2 = 0.0 + alambda; /* apdis = 0 */
+                double dzdx = (zzm[j * ni + i + 1] - zzm[j * ni + i - 1]) / delx1;
+                double dzdy = (zzm[(j + 1) * ni + i] - zzm[(j - 1) * ni + i]) / dely1;
+                double dzdyp1 = (zzm[(j + 1) * ni + i + 1] - zzm[(j - 1) * ni + i + 1]) / dely1;
+                double dzdym1 = (zzm[(j + 1) * ni + i - 1] - zzm[(j - 1) * ni + i - 1]) / dely1;
+                double d2zdxdy = (dzdyp1 - dzdym1) / delx1;
+                double c3 = pow(1.0 + dzdx * dzdx + dzdy * dzdy, 1.5);
+                double c4 = 1.0 + dzdy * dzdy, c5 = 1.0 + dzdx * dzdx;
+                double c6 = 2.0 * dzdx * dzdy * d2zdxdy;
+                double c7 = zzm[j * ni + i + 1] / (delxp * delx) + zzm[j * ni + i - 1] / (delxm * delx);
+                double c8 = zzm[(j + 1) * ni + i] / (delyp * dely) + zzm[(j - 1) * ni + i] / (delym * dely);
+                double c9 = 1.0 / (delxp * delx) + 1.0 / (delxm * delx);
+                double c10 = 1.0 / (delyp * dely) + 1.0 / (delym * dely);
+                double c11 = gamma / c3;
+                double term1 = c2 + c11 * (c4 * c7 + c5 * c8 - c6);
+                double term2 = c1 + c11 * (c4 * c9 + c5 * c10);
+                fi[j * ni + i] = urfree * term1 / term2 + (1.0 - urfree) * zzm[j * ni + i];
+                double diff1 = fabs((fi[j * ni + i] - zzm[j * ni + i]) / zzm[j * ni + i]);
+                priv = (diff1 < priv) ? priv : diff1;  /* std::max(diff1, difmax) */
+            }
+        difmax = (priv > difmax) ? priv : difmax;
+        if (difmax < tol) break;
+        for (int loc = 0; loc < ni * nj; loc++) zzm[loc] = fi[loc];
+    }
+}
+
+static double fs_delta_vol(orc *o, double alambda)
+{
+    const int ni = o->ni;
+    fs_ebal(o, alambda);
+    double delv = 0.0;
+    for (int j = 1; j < o->njm1; j++)
+        for (int i = 1; i < o->nim1; i++) delv += o->areaij[j * ni + i] * o->fi[j * ni + i];
+    return delv;
+}
+
+void orc_free_surface(orc *o, double *rep /* lambda, residual, fi_min, fi_max, volume, iterations, bracketed */)
+{
+    const amcfd_params *p = &o->p;
+    const int ni = o->ni, nj = o->nj, nk = o->nk, nkm1 = o->nkm1;
+    const int nitermax = (int)p->fs_maxiterbisect;
+    const double alam1 = p->fs_lam1, alam2 = p->fs_lam2, tol = p->fs_tolbisect, delt = p->delt;
+    const double startdeltn = 0.0, vdp = 2e-9;
+    double melttime = delt * (1.0 + startdeltn), vd;
+    if (o->tpeak <= p->tsolid) {
+        vd = 0.0;
+        melttime = 0.0;
+    } else {
+        vd = vdp * (o->timet - melttime - startdeltn * delt);
+        if (o->powerindicator < 1) vd = vdp * (p->lasertime - melttime);
+    }
+    double f = fs_delta_vol(o, alam1) + vd;
+    double fmid = fs_delta_vol(o, alam2) + vd;
+    int bracketed = !(f * fmid >= 0.0 && f != vd);
+    double alamopt, dx, xmid = 0.0;
+    if (f < 0.0) { alamopt = alam1; dx = alam2 - alam1; }
+    else { alamopt = alam2; dx = alam1 - alam2; }
+    int niter;
+    for (niter = 0; niter < nitermax; niter++) {
+        dx *= 0.5;
+        xmid = alamopt + dx;
+        fmid = fs_delta_vol(o, xmid) + vd;
+        if (fmid < 0.0) alamopt = xmid;
+        if (fabs(dx) < 1.0e-5 || (fabs(fmid) < tol && niter != 0)) break;
+    }
+    for (int k = 0; k < nk; k++)
+        for (int j = 0; j < nj; j++)
+            for (int i = 0; i < ni; i++) {
+                size_t c = ID(i, j, k);
+                double factor = o->fi[j * ni + i] / o->z[nkm1];
+                o->zr[c] = o->z[k] * (1.0 - factor);
+                if (o->zr[c] > o->z[nkm1]) continue;
+                if (o->zr[c] == o->z[nkm1]) o->tempr[c] = o->temp[ID(i, j, nkm1)];
+                for (int l = nkm1 - 1; l >= 0; l--)
+                    if (o->z[l] <= o->zr[c]) {
+                        o->tempr[c] = (o->zr[c] - o->z[l]) / (o->z[l + 1] - o->z[l]) *
+                                          (o->temp[ID(i, j, l + 1)] - o->temp[ID(i, j, l)]) + o->temp[ID(i, j, l)];
+                        break;
+                    }
+            }
+    double mn = o->fi[0], mx = o->fi[0];
+    for (int q = 1; q < ni * nj; q++) {
+        if (o->fi[q] < mn) mn = o->fi[q];
+        if (mx < o->fi[q]) mx = o->fi[q];
+    }
+    rep[0] = xmid; rep[1] = fmid; rep[2] = mn; rep[3] = mx; rep[4] = vd;
+    rep[5] = niter; rep[6] = bracketed;
+}
+
 /* Species equation (iterativeLoopSolve :677-687). */
 void orc_species(orc *o)
 {
@@ -1720,14 +1838,21 @@ orc *orc_create(const amcfd_params *params)
                      &o->wnot, &o->pressure, &o->ap, &o->an, &o->as, &o->ae, &o->aw, &o->at,
                      &o->ab, &o->apnot, &o->dux, &o->dvy, &o->dwz, &o->su, &o->sp, &o->conc,
                      &o->concnot, &o->concn, &o->csfrac, &o->solfrac, &o->mpphase, &o->mpliq,
-                     &o->grad, &o->rate};
+                     &o->grad, &o->rate, &o->zr, &o->tempr};
     for (size_t q = 0; q < sizeof(f3) / sizeof(f3[0]); q++) *f3[q] = dalloc(n);
     o->powerindicator = 1;
     o->init = 1;
     o->trackindx = 1;
     o->nk_alloc = o->nk;
+    o->fi = dalloc(ni * nj);
+    o->zzm = dalloc(ni * nj);
     generate_grid(o);
     initialize_solver(o);
+    if (p->freesurface)  /* FreeSurfaceManager::initializeFreeSurface (:34-69) */
+        for (size_t c = 0; c < n; c++) {
+            o->zr[c] = o->z[c / (ni * nj)];
+            o->tempr[c] = o->temp[c];
+        }
     if (p->powderbed) {
         /* CFDSolverManager.cpp:482-492 then PrintManager.cpp:67-73: build layers are
          * powder, and only the first of them starts active */
@@ -1754,7 +1879,7 @@ void orc_free(orc *o)
                    o->fraclnot, o->sourceinput, o->rho, o->unot, o->vnot, o->wnot, o->pressure,
                    o->ap, o->an, o->as, o->ae, o->aw, o->at, o->ab, o->apnot, o->dux, o->dvy,
                    o->dwz, o->su, o->sp, o->conc, o->concnot, o->concn, o->csfrac, o->solfrac,
-                   o->mpphase, o->mpliq, o->grad, o->rate};
+                   o->mpphase, o->mpliq, o->grad, o->rate, o->zr, o->tempr, o->fi, o->zzm};
     for (size_t q = 0; q < sizeof(f) / sizeof(f[0]); q++) free(f[q]);
     free(o->tool_on);
     free(o->tool_id);
@@ -1787,7 +1912,8 @@ double *orc_field(orc *o, const char *name)
         {"areaij", o->areaij}, {"areajk", o->areajk}, {"areaik", o->areaik},
         {"avgconcentration", o->conc}, {"avgconcentrationnot", o->concnot},
         {"concentration", o->concn}, {"csfrac", o->csfrac}, {"solfrac", o->solfrac},
-        {"mpPhase", o->mpphase}, {"mpLiqPhase", o->mpliq}, {"grad", o->grad}, {"rate", o->rate}};
+        {"mpPhase", o->mpphase}, {"mpLiqPhase", o->mpliq}, {"grad", o->grad}, {"rate", o->rate},
+        {"zr", o->zr}, {"tempr", o->tempr}, {"fi", o->fi}};
     for (size_t q = 0; q < sizeof(t) / sizeof(t[0]); q++)
         if (!strcmp(t[q].n, name)) return t[q].p;
     return NULL;

@@ -51,6 +51,7 @@ def lib():
                    "orc_fluxes", "orc_update_solutions", "orc_energy_assemble", "orc_outer_loop",
                    "orc_begin_step", "orc_species"):
             getattr(L, fn).argtypes = [VP]
+        L.orc_free_surface.argtypes = [VP, C.POINTER(C.c_double)]
         for fn in ("orc_momentum", "orc_outer_iteration"):
             getattr(L, fn).argtypes = [VP]
             getattr(L, fn).restype = C.c_int
@@ -85,7 +86,7 @@ class Oracle:
                  "y": self.nj, "yv": self.nj, "dypsinv": self.nj, "fracy": self.nj,
                  "z": self.nk, "zw": self.nk, "dzpbinv": self.nk, "fracz": self.nk,
                  "heatin": self.ni * self.nj, "areaij": self.ni * self.nj,
-                 "areajk": self.nj * self.nk, "areaik": self.ni * self.nk}
+                 "areajk": self.nj * self.nk, "areaik": self.ni * self.nk, "fi": self.ni * self.nj}
         n = one_d.get(name, self.ni * self.nj * self.nk)
         arr = np.ctypeslib.as_array(ptr, shape=(n,))
         return arr if name in one_d else arr.reshape(self.shape)
@@ -101,6 +102,13 @@ class Oracle:
         r = AmcfdReport()
         lib().orc_report(self._h, C.byref(r))
         return r.as_dict()
+
+    def free_surface(self) -> Dict:
+        """FreeSurfaceManager::execute on the current state; its monitor values."""
+        r = (C.c_double * 7)()
+        lib().orc_free_surface(self._h, r)
+        return {"lambda": r[0], "residual": r[1], "fi_min": r[2], "fi_max": r[3], "volume": r[4],
+                "iterations": int(r[5]), "bracketed": int(r[6])}
 
     def box(self):
         t = C.c_double()

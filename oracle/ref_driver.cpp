@@ -40,6 +40,7 @@ static const int kNumFields = sizeof(kFields) / sizeof(kFields[0]);
 static const char *kSpeciesFields[] = {"avgconcentration", "concentration"};
 static const char *kPowderFields[] = {"csfrac", "solfrac", "mpPhase", "mpLiqPhase"};
 static const char *kSolidFields[] = {"grad", "rate"};
+static const char *kFreeSurfFields[] = {"zr", "tempr"};
 static const char *kGeom[] = {"x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv",
                               "fracx", "fracy"};
 static const int kNumGeom = sizeof(kGeom) / sizeof(kGeom[0]);
@@ -103,6 +104,7 @@ int main(int argc, char **argv)
     names.insert(names.end(), kSpeciesFields, kSpeciesFields + nspecies);
     names.insert(names.end(), kPowderFields, kPowderFields + npowder);
     names.insert(names.end(), kSolidFields, kSolidFields + nsolid);
+    if (meshObj.energyfreesurface_) names.insert(names.end(), kFreeSurfFields, kFreeSurfFields + 2);
     FILE *f = nullptr;
     if (!timing) {
         f = fopen(out.c_str(), "wb");
@@ -150,6 +152,16 @@ int main(int argc, char **argv)
         cfd->iterativeLoopSolve();
         if (meshObj.solidificationparams_) cfd->getSolidificationParameters();
         if (!domainMgr->steady_) cfd->updateSolutions();
+        // the free surface, which main.cpp:174-176 runs at output times, after every step here
+        // (it feeds nothing back into the solution)
+        if (meshObj.energyfreesurface_) {
+            fflush(stdout);
+            dup2(devnull, 1);
+            fs->execute();
+            std::cout.flush();
+            fflush(stdout);
+            dup2(saved_stdout, 1);
+        }
         auto t1 = std::chrono::high_resolution_clock::now();
         double dt_s = 1e-9 * std::chrono::duration_cast<std::chrono::nanoseconds>(t1 - t0).count();
         total_s += dt_s;

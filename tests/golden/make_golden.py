@@ -26,6 +26,7 @@ FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
 POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
 MOVING_FIELDS = ("grad", "rate", "hnot", "grid_x", "grid_y")
+FREESURF_FIELDS = ("zr", "tempr")
 SCALARS = ("niter", "timet", "resorh", "resorm", "resoru", "resorv", "resorw", "tpeak", "alen",
            "depth", "width", "ratio", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat",
            "jstart", "resorc", "nk_active", "trackindx", "steadylength")
@@ -46,6 +47,7 @@ def decks():
         species_deck(),
         D.powder_layers("g_powder"),
         D.moving_track("g_moving"),
+        D.free_surface_track("g_freesurf"),
     ]
 
 
@@ -64,11 +66,17 @@ def main():
         rec = {f"s_{k}": np.array([s[k] for s in steps]) for k in SCALARS}
         for tag, s in (("first", steps[0]), ("last", steps[-1])):
             extra = SPECIES_FIELDS + (POWDER_FIELDS if "csfrac" in s else ()) + \
-                (MOVING_FIELDS if "grad" in s else ())
+                (MOVING_FIELDS if "grad" in s else ()) + FREESURF_FIELDS
             for f in FIELDS + tuple(f for f in extra if f in s):
                 rec[f"{tag}_{f}"] = s[f]
         for g, v in dump["geom"].items():
             rec[f"geom_{g}"] = v
+        mon = os.path.join(out, f"{d.name}_FreeSurfaceMonitor.txt")
+        if os.path.exists(mon):  # the free surface's monitor values, as printed, one row per step
+            rows = [l.split()[1:] for l in open(mon).read().splitlines()
+                    if l.startswith("  ") and l.split()[0][:1].isdigit()]
+            rec["fs_monitor"] = np.array(rows)
+            os.unlink(mon)
         np.savez_compressed(os.path.join(out, "ref.npz"), **rec)
         print(d.name, len(steps), "steps")
 

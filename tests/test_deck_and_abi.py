@@ -109,16 +109,22 @@ def test_deck_comments_blank_lines_and_unknown_keywords(tmp_path):
     assert (a.dens, a.urfu, a.maxit, a.finaltime) == (b.dens, b.urfu, b.maxit, b.finaltime)
 
 
-def test_create_rejects_out_of_scope_modes(tmp_path):
+def test_feature_rows_are_checked(tmp_path):
+    """A feature keyword without its full parameter row is a parse error; a free
+    surface with a negative iteration count is rejected before any device work."""
     import amcfd
     import amcfd_decks as D
-    good = D.small("oos", steps=2).write(str(tmp_path))
+    good = D.small("rows", steps=2).write(str(tmp_path))
     text = open(good).read()
-    bad = str(tmp_path / "freesurface.k")
-    _write(bad, text + "*TRACK_ENERGY_BASED_FREE_SURFACE\n")
-    d = amcfd.Deck(bad)
-    assert d.params.freesurface == 1
+    for kw in ("*TRACK_ENERGY_BASED_FREE_SURFACE", "*POWDER_BED_MODE", "*SOLVE_SPECIES",
+               "*ACTIVATE_MOVING_MESH"):
+        bad = str(tmp_path / "short.k")
+        _write(bad, text + kw + "\n  1\n")
+        with pytest.raises(amcfd.AmcfdError):
+            amcfd.Deck(bad)
+    neg = str(tmp_path / "neg.k")
+    _write(neg, text + "*TRACK_ENERGY_BASED_FREE_SURFACE\n  -1e5 1e5 1.8 -3 1e-6 40 1e-18 0.5\n")
+    d = amcfd.Deck(neg)
     h = C.c_void_p()
-    rc = amcfd.lib().amcfd_create(C.byref(d.params), None, C.byref(h))
-    assert rc == -1  # rejected before any device work
+    assert amcfd.lib().amcfd_create(C.byref(d.params), None, C.byref(h)) == -1
     amcfd.lib().amcfd_destroy(h)

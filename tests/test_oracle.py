@@ -15,11 +15,17 @@ import pytest
 
 from conftest import GOLDEN
 
-CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species", "g_powder", "g_moving"]
+CASES = ["g_track", "g_toolpath", "g_noflow", "g_cooling", "g_species", "g_powder", "g_moving", "g_freesurf"]
 FIELDS = ("temp", "uvel", "vvel", "wvel", "pressure", "enthalpy", "fracl", "pp")
 SPECIES_FIELDS = ("avgconcentration", "concentration")
 POWDER_FIELDS = ("csfrac", "solfrac", "mpPhase", "mpLiqPhase", "diff", "rho")
 MOVING_FIELDS = ("grad", "rate", "hnot")
+FREESURF_FIELDS = ("zr", "tempr")
+
+
+def fs_row(f):
+    """The free surface's values as FreeSurfaceManager::execute prints them."""
+    return ["%.4e" % f[k] for k in ("lambda", "residual", "fi_min", "fi_max", "volume")] + [str(f["iterations"])]
 SCALARS = ("niter", "tpeak", "alen", "depth", "width", "ratio", "resorh", "resorm", "resoru",
            "resorv", "resorw", "heatinlaser", "istat", "iend", "jstat", "jend", "kstat", "jstart",
            "resorc", "nk_active", "trackindx", "steadylength")
@@ -40,9 +46,12 @@ def test_oracle_bit_exact_on_golden(case, oracle_lib, monkeypatch):
     for g in ("x", "y", "z", "xu", "yv", "dxpwinv", "dypsinv", "dzpbinv", "fracx", "fracy"):
         assert np.array_equal(o.field(g), ref[f"geom_{g}"]), g
     n = len(ref["s_niter"])
-    fields = FIELDS + tuple(f for f in SPECIES_FIELDS + POWDER_FIELDS + MOVING_FIELDS if f"first_{f}" in ref)
+    fields = FIELDS + tuple(f for f in SPECIES_FIELDS + POWDER_FIELDS + MOVING_FIELDS + FREESURF_FIELDS
+                            if f"first_{f}" in ref)
     for s in range(n):
         r = o.step()
+        if "fs_monitor" in ref:
+            assert fs_row(o.free_surface()) == list(ref["fs_monitor"][s]), (case, s)
         for k in SCALARS:
             assert _same(r[k], ref[f"s_{k}"][s]), (case, s, k, r[k], ref[f"s_{k}"][s])
         tag = "first" if s == 0 else "last" if s == n - 1 else None
@@ -81,13 +90,17 @@ def _variants():
     out.append(d)
     # moving mesh towards -x and -y (the remap partner is the already-remapped node), with G/R
     out.append(D.moving_track("v_moving", reverse=True, steps=5))
+    # free surface on the upwind scheme, beam off after two steps (the volume from lasertime)
+    d = D.free_surface_track("v_freesurf", steps=4)
+    d.scheme, d.single_track = "upwind", (2e-5,) + d.single_track[1:]
+    out.append(d)
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(7))
+@pytest.mark.parametrize("idx", range(8))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
@@ -95,12 +108,16 @@ def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     deck = _variants()[idx]
     path = deck.write(str(tmp_path))
     out = str(tmp_path / "ref.bin")
-    subprocess.check_call([oracle_py.REF_DUMP, path, "--out", out],
+    subprocess.check_call([oracle_py.REF_DUMP, path, "--out", out], cwd=str(tmp_path),
                           env=dict(os.environ, OMP_NUM_THREADS="1"), stdout=subprocess.DEVNULL)
     ref = read_dump(out)
+    mon = tmp_path / f"{deck.name}_FreeSurfaceMonitor.txt"
+    mon = [l.split()[1:] for l in open(mon).read().splitlines()
+           if l.startswith("  ") and l.split()[0][:1].isdigit()] if mon.exists() else None
     o = oracle_py.Oracle(amcfd.Deck(path))
     fields = FIELDS + (SPECIES_FIELDS if deck.species is not None else ()) + \
-        (POWDER_FIELDS if deck.powder is not None else ()) + (MOVING_FIELDS if deck.solidification else ())
+        (POWDER_FIELDS if deck.powder is not None else ()) + (MOVING_FIELDS if deck.solidification else ()) + \
+        (FREESURF_FIELDS if deck.free_surface is not None else ())
     for s in ref["steps"]:
         r = o.step()
         assert r["niter"] == s["niter"]
@@ -108,6 +125,8 @@ def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
         assert _same(r["resorc"], s["resorc"])
         assert r["nk_active"] == s["nk_active"] and r["trackindx"] == s["trackindx"]
         assert r["steadylength"] == s["steadylength"]
+        if mon is not None:
+            assert fs_row(o.free_surface()) == mon[s["step"] - 1], (deck.name, s["step"])
         assert np.array_equal(o.field("x"), s["grid_x"]) and np.array_equal(o.field("y"), s["grid_y"])
         for f in fields:
             assert np.array_equal(o.field(f), s[f], equal_nan=True), (deck.name, s["step"], f)

@@ -63,7 +63,7 @@ def text_lines(path):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_CLI), reason="reference binary not built")
-@pytest.mark.parametrize("variant", ["plain", "species", "powder", "moving"])
+@pytest.mark.parametrize("variant", ["plain", "species", "powder", "moving", "freesurf"])
 def test_output_files_match_reference(variant, tmp_path, monkeypatch):
     import amcfd
     import amcfd_decks as D
@@ -71,6 +71,8 @@ def test_output_files_match_reference(variant, tmp_path, monkeypatch):
         d = D.powder_layers("outdeck", nx=20, ny=12, nz=8)
     elif variant == "moving":  # points follow the moving grid; grad and rate written
         d = D.moving_track("outdeck", nx=20, ny=12, nz=8, steps=5)
+    elif variant == "freesurf":  # points at the deformed heights zr; zr, tempr and the monitor file
+        d = D.free_surface_track("outdeck", steps=5)
     else:
         d = D.small("outdeck", nx=20, ny=12, nz=8, steps=5, power=300.0)
     if variant == "species":  # adds avgconcentration and concentration to the written fields
@@ -113,7 +115,10 @@ def test_output_files_match_reference(variant, tmp_path, monkeypatch):
             else:
                 assert rel_l2(y, x) < 1e-8, (name, q, rel_l2(y, x))
     assert open(ref_dir / "outdeck.pvd").read() == open(our_dir / "outdeck.pvd").read()
-    for fname in ("outdeck_Residuals.txt", "outdeck_geom.txt"):
+    names = ["outdeck_Residuals.txt", "outdeck_geom.txt"]
+    if variant == "freesurf":
+        names.append("outdeck_FreeSurfaceMonitor.txt")
+    for fname in names:
         la, lb = text_lines(ref_dir / fname), text_lines(our_dir / fname)
         assert len(la) == len(lb), fname
         for x, y in zip(la, lb):
