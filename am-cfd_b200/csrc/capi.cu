@@ -94,6 +94,7 @@ struct amcfd_ctx {
     int steadylength = 0;          // BoundCondManager::steadylength_ (moving mesh)
     double *dmetric[12] = {};      // device copies of x y z xu yv zw dxpwinv dypsinv dzpbinv fracx fracy fracz
     double *mesh_old = nullptr;    // moving mesh: centres before the move, x (ni) then y (nj)
+    double *mesh_pinned = nullptr; // moving mesh: pinned staging of the new metrics and old centres
     FsOut *fs_out = nullptr;       // free surface: the bisection's results (device)
     Inst<double> I64;
     Inst<float> I32;
@@ -381,7 +382,12 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     g.dxpwinv = m1[6]; g.dypsinv = m1[7]; g.dzpbinv = m1[8]; g.fracx = m1[9]; g.fracy = m1[10];
     g.fracz = m1[11];
     for (int a = 0; a < 12; a++) ctx->dmetric[a] = m1[a];
-    if (q.movingmesh && (rc = alloc3<double>(ctx, &ctx->mesh_old, (size_t)p.ni + p.nj))) return rc;
+    if (q.movingmesh) {
+        if ((rc = alloc3<double>(ctx, &ctx->mesh_old, (size_t)p.ni + p.nj))) return rc;
+        size_t nst = (size_t)p.ni + p.nj;
+        for (int a = 0; a < 12; a++) nst += src1[a]->size();
+        CK(cudaMallocHost(&ctx->mesh_pinned, nst * sizeof(double)));
+    }
     T **f3[] = {&g.uvel, &g.vvel, &g.wvel, &g.unot, &g.vnot, &g.wnot, &g.pressure, &g.pp,
                 &g.h, &g.hnot, &g.temp, &g.fracl, &g.fraclnot, &g.sourceinput,
                 &g.diff_cur, &g.rho_cur, &g.vis_cur, &g.diff_nxt, &g.rho_nxt, &g.vis_nxt,
@@ -633,21 +639,27 @@ static int move_mesh(amcfd_ctx *ctx, Inst<T> &I)
     p.xzone[ix + 1] -= dx;
     p.yzone[iy - 1] += dy;
     p.yzone[iy + 1] -= dy;
-    std::vector<double> old(ctx->x.begin(), ctx->x.begin() + ctx->ni);
-    old.insert(old.end(), ctx->y.begin(), ctx->y.begin() + ctx->nj);
+    // staged in pinned memory so that the copies stay asynchronous; event 8 marks
+    // the end of the previous step's copies out of the staging
+    CK(cudaEventSynchronize(ctx->ev[8]));
+    double *st = ctx->mesh_pinned;
+    std::copy(ctx->x.begin(), ctx->x.begin() + ctx->ni, st);
+    std::copy(ctx->y.begin(), ctx->y.begin() + ctx->nj, st + ctx->ni);
+    CK(cudaMemcpyAsync(ctx->mesh_old, st, ((size_t)ctx->ni + ctx->nj) * sizeof(double),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    st += (size_t)ctx->ni + ctx->nj;
     build_grid(ctx, ctx->nk_active);
     const std::vector<double> *src[12] = {&ctx->x, &ctx->y, &ctx->z, &ctx->xu, &ctx->yv, &ctx->zw,
                                           &ctx->dxpwinv, &ctx->dypsinv, &ctx->dzpbinv,
                                           &ctx->fracx, &ctx->fracy, &ctx->fracz};
-    for (int a = 0; a < 12; a++)
-        CK(cudaMemcpyAsync(ctx->dmetric[a], src[a]->data(), src[a]->size() * sizeof(double),
-                           cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(ctx->mesh_old, old.data(), old.size() * sizeof(double), cudaMemcpyHostToDevice,
-                       ctx->stream));
+    for (int a = 0; a < 12; a++) {
+        std::copy(src[a]->begin(), src[a]->end(), st);
+        CK(cudaMemcpyAsync(ctx->dmetric[a], st, src[a]->size() * sizeof(double), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        st += src[a]->size();
+    }
+    CK(cudaEventRecord(ctx->ev[8], ctx->stream));
     launch_remap<T>(I, ctx->mesh_old, ctx->mesh_old + ctx->ni, dirx, diry);
-    // the host vectors above are pageable: each copy has been staged when its call returns,
-    // except for the local one, which must outlive its transfer
-    CK(cudaStreamSynchronize(ctx->stream));
     ctx->launches += 2;
     return 0;
 }
@@ -1050,6 +1062,7 @@ void amcfd_destroy(amcfd_ctx *ctx)
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    if (ctx->mesh_pinned) cudaFreeHost(ctx->mesh_pinned);
     if (ctx->pack) cudaFree(ctx->pack);
     for (void *q : {(void *)ctx->ws_feat, (void *)ctx->ws_y, (void *)ctx->ws_target, ctx->ws_save[0],
                     ctx->ws_save[1], ctx->ws_save[2], ctx->ws_save[3]})

@@ -10,8 +10,9 @@
 // the direction the mesh moved.  The reference updates in place in ascending
 // index order, so when the mesh moved towards lower coordinates the partner
 // is the already-remapped neighbour: each row (column) is one sequential
-// recurrence, and each is run by one thread in that order here.  Rows are
-// j = 0..nj-2 and i = 1..ni-2 as in the reference loops.
+// recurrence, and each is run by one thread in that order here (one thread
+// per line and field; the fields are independent).  Rows are j = 0..nj-2 and
+// i = 1..ni-2 as in the reference loops.
 //
 // getSolidificationParameters (:2764-2804): per (k, j) row below the top
 // plane, the first node i with T >= T_solidus defines the solidification
@@ -35,86 +36,74 @@ __device__ __forceinline__ double lerp_ref(double x0, double x1, double y0, doub
     return y0 + (x - x0) * ((y1 - y0) / (x1 - x0));
 }
 
-// x pass: 32 rows per CTA; rows are staged through shared memory in 32-node
-// chunks (coalesced loads and stores) and warp 0 runs each row's recurrence.
+// One thread per (line, field): a row of nodes along x (stride 1) or a column
+// along y (stride nip), walked in ascending order in chunks of kChunk nodes.
+// A chunk's kChunk + 1 values are loaded together (the loads overlap), updated
+// in registers in the reference's order, and stored: towards higher
+// coordinates the partner is the next node's old value (the extra load), towards
+// lower ones the previous node's remapped value (carried across chunks).
+constexpr int kChunk = 8;
+
+template <typename T>
+__device__ __forceinline__ void remap_line(T *f, long long stride, int n0, int n1, const double *oldc,
+                                           const double *newc, int dir)
+{
+    // nodes n0..n1 of the line f[m * stride]
+    T prev = f[(long long)(n0 - 1) * stride];  // the node before n0 (never remapped in this pass)
+    for (int mb = n0; mb <= n1; mb += kChunk) {
+        T v[kChunk + 1];
+#pragma unroll
+        for (int q = 0; q <= kChunk; ++q)
+            if (mb + q <= n1 + 1) v[q] = f[(long long)(mb + q) * stride];
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q) {
+            const int m = mb + q;
+            if (m > n1) break;
+            const double co = oldc[m], cn = newc[m];
+            if (fabs(co - cn) > 1e-6 && m + dir >= 0) {
+                const double y1 = dir > 0 ? (double)v[q + 1] : (double)(q == 0 ? prev : v[q - 1]);
+                v[q] = (T)lerp_ref(co, oldc[m + dir], (double)v[q], y1, cn);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kChunk; ++q)
+            if (mb + q <= n1) f[(long long)(mb + q) * stride] = v[q];
+        prev = v[kChunk - 1];
+    }
+}
+
+// x pass: rows (k, j), j = 0..nj-2, nodes i = 1..ni-2
 template <typename T>
 __global__ void __launch_bounds__(256) remap_x_kernel(Params p, RemapSet<T> set, const double *oldx,
                                                       const double *newx, int dir)
 {
-    __shared__ T tile[32][34];
-    const int nj = p.nj, nip = p.nip, ni = p.ni;
-    const int J = nj - 1, nrows = J * p.nk;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int l0 = blockIdx.x * 32; l0 < nrows; l0 += gridDim.x * 32) {
-        for (int q = 0; q < set.n; ++q) {
-            T *f = set.f[q];
-            T prev = T(0);  // remapped value of node i-1 (warp 0, one row per lane)
-            if (warp == 0 && l0 + lane < nrows) {
-                const int l = l0 + lane, k = l / J, j = l - k * J;
-                prev = f[cidx(0, j, k, nj, nip)];
-            }
-            for (int ib = 1; ib <= ni - 2; ib += 32) {
-                for (int r = warp; r < 32; r += 8) {
-                    const int l = l0 + r;
-                    if (l < nrows) {
-                        const int k = l / J, j = l - k * J;
-                        const size_t row = cidx(0, j, k, nj, nip);
-                        const int i = ib + lane;
-                        if (i <= ni - 1) tile[r][lane] = f[row + i];
-                        if (lane == 0 && ib + 32 <= ni - 1) tile[r][32] = f[row + ib + 32];
-                    }
-                }
-                __syncthreads();
-                if (warp == 0 && l0 + lane < nrows) {
-                    const int r = lane, n = min(32, ni - 1 - ib);
-                    for (int qq = 0; qq < n; ++qq) {
-                        const int i = ib + qq;
-                        const double xo = oldx[i], xn = newx[i];
-                        if (fabs(xo - xn) > 1e-6) {
-                            const double y1 = dir > 0 ? (double)tile[r][qq + 1] : (double)prev;
-                            tile[r][qq] = (T)lerp_ref(xo, oldx[i + dir], (double)tile[r][qq], y1, xn);
-                        }
-                        prev = tile[r][qq];
-                    }
-                }
-                __syncthreads();
-                for (int r = warp; r < 32; r += 8) {
-                    const int l = l0 + r;
-                    const int i = ib + lane;
-                    if (l < nrows && i <= ni - 2) {
-                        const int k = l / J, j = l - k * J;
-                        f[cidx(i, j, k, nj, nip)] = tile[r][lane];
-                    }
-                }
-                __syncthreads();
-            }
-        }
+    const int nj = p.nj, nip = p.nip, J = nj - 1;
+    const long long nrows = (long long)J * p.nk, total = nrows * set.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(t / nrows);
+        const long long l = t - (long long)q * nrows;
+        const int k = (int)(l / J), j = (int)(l - (long long)k * J);
+        remap_line<T>(set.f[q] + cidx(0, j, k, nj, nip), 1, 1, p.ni - 2, oldx, newx, dir);
     }
 }
 
-// y pass: one thread per (k, i) column, j ascending (consecutive threads take
-// consecutive i, so every step of the recurrence is a coalesced access).
+// y pass: columns (k, i), i = 1..ni-2, nodes j = 0..nj-2; consecutive threads take
+// consecutive i, so every load and store of a chunk is coalesced
 template <typename T>
 __global__ void __launch_bounds__(256) remap_y_kernel(Params p, RemapSet<T> set, const double *oldy,
                                                       const double *newy, int dir)
 {
-    const int nj = p.nj, nip = p.nip, ni = p.ni, nk = p.nk;
-    const int I = ni - 2;
-    const size_t sj = nip;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < (long long)I * nk;
+    const int nj = p.nj, nip = p.nip, I = p.ni - 2;
+    const long long ncols = (long long)I * p.nk, total = ncols * set.n;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t / I), i = 1 + (int)(t - (long long)k * I);
-        for (int q = 0; q < set.n; ++q) {
-            T *f = set.f[q];
-            T *col = f + cidx(i, 0, k, nj, nip);
-            for (int j = 0; j <= nj - 2; ++j) {
-                const double yo = oldy[j], yn = newy[j];
-                // y(0) = 0 never moves; the guard keeps row j-1 inside the array regardless
-                if (fabs(yo - yn) > 1e-6 && j + dir >= 0)
-                    col[j * sj] = (T)lerp_ref(yo, oldy[j + dir], (double)col[j * sj],
-                                              (double)col[(j + dir) * (long long)sj], yn);
-            }
-        }
+        const int q = (int)(t / ncols);
+        const long long l = t - (long long)q * ncols;
+        const int k = (int)(l / I), i = 1 + (int)(l - (long long)k * I);
+        // node 0 never moves (y(0) = 0); the walk starts at node 1 with node 0 as its
+        // predecessor, which is what the reference's in-place loop sees
+        remap_line<T>(set.f[q] + cidx(i, 0, k, nj, nip), nip, 1, nj - 2, oldy, newy, dir);
     }
 }
 
@@ -159,11 +148,11 @@ void launch_remap(Inst<T> &I, const double *oldx, const double *oldy, int dirx, 
                  g.pressure, g.pp, g.conc, g.concnot};
     for (T *f : list)
         if (f) s.f[s.n++] = f;
-    const int rows = (I.p.nj - 1) * I.p.nk;
-    remap_x_kernel<T><<<(rows + 31) / 32, 256, 0, I.stream>>>(I.p, s, oldx, g.x, dirx);
-    const long long cols = (long long)(I.p.ni - 2) * I.p.nk;
-    const int grid = (int)std::min<long long>((cols + 255) / 256, (long long)I.sm_count * 8);
-    remap_y_kernel<T><<<std::max(grid, 1), 256, 0, I.stream>>>(I.p, s, oldy, g.y, diry);
+    const long long rows = (long long)(I.p.nj - 1) * I.p.nk * s.n;
+    const long long cols = (long long)(I.p.ni - 2) * I.p.nk * s.n;
+    auto grid = [&](long long n) { return (int)std::max(1ll, std::min((n + 255) / 256, (long long)I.sm_count * 16)); };
+    remap_x_kernel<T><<<grid(rows), 256, 0, I.stream>>>(I.p, s, oldx, g.x, dirx);
+    remap_y_kernel<T><<<grid(cols), 256, 0, I.stream>>>(I.p, s, oldy, g.y, diry);
 }
 
 template <typename T> void launch_solidification(Inst<T> &I, double scanvel)

@@ -107,20 +107,38 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def make_deck(tmp: str, steps: int, config: str):
+FEATURES = {
+    "none": "",
+    "species": "species equation (initial 1.0, D=5e-9 m^2/s, kp=0.3, urfc=0.7)",
+    "powder": "powder bed: 2 layers of 10 cells, 40 um, powder at 90 % density, k=5 W/m/K",
+    "moving": "moving mesh (middle x and y zones follow the beam) with G/R every step",
+    "freesurf": "energy-balance free surface (timed separately: it runs before outputs)",
+}
+
+
+def make_deck(tmp: str, steps: int, config: str, feature: str = "none"):
     import amcfd_decks as D
     deck = {"config1": D.config1, "config0": D.config0}[config](steps=steps)
+    if feature == "species":
+        deck.species = (1.0, 5e-9, 0.3, 0.7)
+    elif feature == "powder":
+        deck.powder = (2, 10, 40e-6, 0.9 * deck.material.dens, 1e-6, 500.0, 0.0, 5.0)
+    elif feature == "moving":
+        deck.moving_mesh = (2, 2)
+        deck.solidification = True
+    elif feature == "freesurf":
+        deck.free_surface = (-1e5, 1e5, 1.8, 30, 1e-6, 40, 1e-18, 0.5)
     return deck, deck.write(tmp)
 
 
-def reference_arm(args, steps: int, warmup: int, config: str, threads: int):
+def reference_arm(args, steps: int, warmup: int, config: str, threads: int, feature: str = "none"):
     """The reference CPU solver (oracle/_ref/amcfd_ref_dump --time) on the same deck."""
     import oracle_py
     exe = oracle_py.REF_DUMP
     if not os.path.exists(exe):
         return None, "reference binary oracle/_ref/amcfd_ref_dump not built"
     with tempfile.TemporaryDirectory() as tmp:
-        deck, path = make_deck(tmp, warmup + steps, config)
+        deck, path = make_deck(tmp, warmup + steps, config, feature)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         out = subprocess.run([exe, path, "--time", "--steps", str(warmup + steps)], env=env,
                              capture_output=True, text=True, timeout=1800)
@@ -150,6 +168,8 @@ def main():
                     help="replay each outer iteration from a CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 exact-order comparison run")
+    ap.add_argument("--feature", default="none", choices=sorted(FEATURES),
+                    help="solve the deck with one of the optional models switched on")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", "0"))
@@ -161,13 +181,15 @@ def main():
                              "iterations/step" if args.config == "config1" else
                              "single track +x, 120x60x40 cells, P=200 W, dt=1e-5 s"),
                 "deck": args.config, "l2": "working set 1.2-2.5 GB > 126 MB L2 (no flush needed)"}
+    if args.feature != "none":
+        cfg_desc["feature"] = FEATURES[args.feature]
 
     if args.impl == "reference":
         if rank != 0:
             return
         ksteps = min(args.steps, 8)
         kwarm = min(warmup, 1)
-        r, why = reference_arm(args, ksteps, kwarm, args.config, threads)
+        r, why = reference_arm(args, ksteps, kwarm, args.config, threads, args.feature)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
@@ -200,7 +222,7 @@ def main():
     order = amcfd.ORDER_REDBLACK if args.order == "redblack" else amcfd.ORDER_EXACT
     tmp = tempfile.mkdtemp(prefix=f"amcfd_bench{rank}_")
     total_steps = warmup + 2 * args.steps + 2
-    deck, path = make_deck(tmp, total_steps, args.config)
+    deck, path = make_deck(tmp, total_steps, args.config, args.feature)
     d = amcfd.Deck(path)
     ni, nj, nk = d.dims
     ncell = (ni - 2) * (nj - 2) * (nk - 2)
@@ -267,6 +289,15 @@ def main():
                 "iteration_frac": (92 * ncell * w * iters / (ms / 1e3) / 1e9) / peak}
 
     extra = {}
+    if args.feature == "freesurf":
+        # one free-surface update (bisection + projection) on the final state; the call
+        # returns after its kernels and the read-back of the monitor values
+        s.free_surface()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fs = s.free_surface()
+        extra["free_surface_ms"] = 1e3 * (time.perf_counter() - t0)
+        extra["free_surface"] = fs
     if not args.no_compare and rank == 0:
         # the plain FP64 exact-order solve of the same steps, for the speed-up at equal iterations
         s64 = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, device=dev,
@@ -280,7 +311,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r, why = reference_arm(args, 2, 0, args.config, threads)
+        r, why = reference_arm(args, 2, 0, args.config, threads, args.feature)
         if r is not None:
             cpu = {"value": r["value"], "unit": METRIC, "cores": r["threads"], "kind": "reference",
                    "sample": f"first {r['steps']} steps of the same deck, OpenMP build of the reference",
