@@ -1017,6 +1017,9 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         if (ctx->nk_active < 3) return fail(ctx, AMCFD_E_ARG, "powder layers exceed the z grid");
     }
     if (ctx->nj > 65535) return fail(ctx, AMCFD_E_CAPACITY, "nj above 65535");
+    // 32-bit chunk indices in the pointwise kernels (32-node chunks of x-lines)
+    if ((long long)ctx->nk * ctx->nj * ((sx + 2 + 31) / 32) > (1ll << 30))
+        return fail(ctx, AMCFD_E_CAPACITY, "grid above 2^35 nodes");
     ctx->nip = (ctx->ni + 31) / 32 * 32;
     double cpavg = (p.acpa * p.tsolid + p.acpb + p.acpl) * 0.5;
     ctx->hlcal = p.hsmelt + cpavg * (p.tliquid - p.tsolid);

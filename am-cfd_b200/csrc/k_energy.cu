@@ -236,7 +236,7 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
                                      int check_finite, int ivar)
 {
     extern __shared__ double sm[];  // 4 * nip
-    const int nip = p.nip, nim1 = p.nim1, nim2 = p.nim2;
+    const int nip = p.nip, nim2 = p.nim2;
     double *bl = sm, *blp = sm + nip, *blm = sm + 2 * nip, *blc = sm + 3 * nip;
     for (int q = threadIdx.x; q < 4 * nip; q += blockDim.x) sm[q] = gd.bcsum[q];
     double sd = 0.0, sh = 0.0;
@@ -291,19 +291,25 @@ __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, doub
     const double ts = p.tsolid;
     const bool steady = p.steady != 0;
     const int lane = threadIdx.x & 31;
-    const int cpr = nip >> 5;  // chunks per row
-    const long long nchunks = (long long)nk * nj * cpr;
-    const long long W = (long long)gridDim.x * (blockDim.x >> 5);
-    const long long w0 = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    // chunk indices in 32-bit unsigned arithmetic (a chunk count far below 2^31 is
+    // checked at context creation): a 64-bit division per chunk costs more than
+    // the chunk's enthalpy inversion
+    const unsigned cpr = (unsigned)nip >> 5;  // chunks per row
+    const unsigned unj = (unsigned)nj;
+    const unsigned nchunks = (unsigned)nk * unj * cpr;
+    const unsigned W = gridDim.x * (blockDim.x >> 5);
+    const unsigned w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const double *dxw = g.dxpwinv, *dys = g.dypsinv, *dzb = g.dzpbinv;
-    for (long long q0 = w0; q0 < nchunks; q0 += W * U) {
+    for (unsigned q0 = w0; q0 < nchunks; q0 += W * U) {
         T hv[U], hn[U], fln[U], rn[U], sv[U];
+        int iu[U], ju[U], ku[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const long long q = q0 + (long long)u * W;
-            const int r = (int)(q / cpr);
-            const int i = (int)(q - (long long)r * cpr) * 32 + lane;
-            const int k = r / nj, j = r - k * nj;
+            const unsigned q = q0 + (unsigned)u * W;
+            const unsigned r = q / cpr;
+            const int i = (int)(q - r * cpr) * 32 + lane;
+            const int k = (int)(r / unj), j = (int)(r - (unsigned)k * unj);
+            iu[u] = i; ju[u] = j; ku[u] = k;
             const bool ok = q < nchunks && i < ni;
             const bool interior = ok && !steady && i >= 1 && i <= nim2 && j >= 1 && j <= njm2 &&
                                   k >= 1 && k <= nkm2;
@@ -316,12 +322,10 @@ __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, doub
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const long long q = q0 + (long long)u * W;
+            const unsigned q = q0 + (unsigned)u * W;
             if (q >= nchunks) break;  // warp-uniform
-            const int r = (int)(q / cpr);
-            const int i = (int)(q - (long long)r * cpr) * 32 + lane;
-            const int k = r / nj, j = r - k * nj;
-            const size_t c = (size_t)r * nip + i;
+            const int i = iu[u], j = ju[u], k = ku[u];
+            const size_t c = ((size_t)k * nj + j) * nip + i;
             const int ibase = i - lane;
             if (ibase >= ni) continue;  // a padding chunk: warp-uniform
             const unsigned act = (ibase + 32 <= ni) ? 0xffffffffu : ((1u << (ni - ibase)) - 1u);
@@ -471,8 +475,7 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
     __shared__ double scratch[40];
     extern __shared__ double colv[];  // 3 * nip doubles + nip ints
     const int nj = p.nj, nip = p.nip;
-    const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
-              nkm2 = p.nkm2;
+    const int nim1 = p.nim1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2, nkm2 = p.nkm2;
     const double ts = p.tsolid;
     double tp = reduce_slot(red_h2t, nblk_h2t, R_TPEAK, true, scratch);
     double t0 = (double)g.temp[0];
