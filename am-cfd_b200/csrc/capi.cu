@@ -22,6 +22,7 @@
 namespace amcfd {
 template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
 template <typename T> void set_sweep_smem_limit(size_t smem);
+template <typename T> bool set_rounds_smem_limit(const Params &p);
 dim3 energy_assemble_grid(const Params &p);
 template <typename T> int h2t_blocks_per_sm();
 template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
@@ -486,6 +487,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
     I.line_smem = (size_t)I.exact_warps * 8 * p.nip * sizeof(T) + (size_t)I.exact_warps * 8;
     set_sweep_smem_limit<T>(I.line_smem);
+    if (!set_rounds_smem_limit<T>(p)) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
     int bps = exact_sweep_blocks_per_sm<T>(I.exact_warps, I.line_smem);
     // A wave of the exact-order sweep holds about 2(nj-2)/3 lines; about three
     // waves of lines in flight keep the dependency chain fed without flooding L2

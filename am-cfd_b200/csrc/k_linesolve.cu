@@ -398,6 +398,168 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 }
 
 // ---------------------------------------------------------------------------
+// Red-black sweep of the whole domain (enthalpy, avgconcentration) in rounds,
+// one warp per line.  In round m lane l holds the 16-byte vector of V cells
+// starting at i = ib + 32 V m + V l (V = 4 in FP32, 2 in FP64; ib = i0 rounded
+// down to 32, so every row access is an aligned 16-byte vector and a round is
+// 12 coalesced row segments of 32 V cells in flight per warp).
+//   forward:  e_i = (at phi_t + ab phi_b + an phi_n + as phi_s + su) * iden_i;
+//             each lane composes the maps x -> cf_i x + e_i of its V cells, an
+//             inclusive warp scan chains the lanes, the chain is applied to qr
+//             carried from the round before (qr_{i0-1} = phi_{i0-1}), and the
+//             lane then runs its cells to get qr; qr and pr go to a per-warp
+//             buffer;
+//   backward: rounds in reverse, the maps x -> pr_i x + qr_i likewise with a
+//             suffix scan, applied to phi carried from the round after
+//             (phi_{i1+1} fixed); phi is stored.
+// Cells outside i0..i1 carry the identity map.  The neighbours phi_t, phi_b,
+// phi_n, phi_s lie on lines of the other colour, which this launch does not
+// write; vectors past the end of the padded row read its first vector and are
+// masked.
+// ---------------------------------------------------------------------------
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; };
+template <> struct Vec16<double> { using type = double2; };
+
+template <typename T>
+__device__ __forceinline__ void ld16(const T *ptr, T (&o)[16 / sizeof(T)])
+{
+    const typename Vec16<T>::type v = *reinterpret_cast<const typename Vec16<T>::type *>(ptr);
+    memcpy(o, &v, 16);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color)
+{
+    constexpr int V = 16 / (int)sizeof(T);
+    constexpr int RC = 32 * V;
+    extern __shared__ unsigned char smraw[];
+    const int i0 = 1, i1 = p.nim2, j0 = 1, j1 = p.njm2, k0 = 1, k1 = p.nkm2;
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const unsigned full = 0xffffffffu;
+    const int ib = i0 & ~31;
+    const int R = (i1 - ib) / RC + 1;
+    T *sq = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * R * RC;
+    T *spr = sq + (size_t)R * RC;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    const int half = (J + 1) / 2;
+    const int nl = half * K;
+    for (int q = blockIdx.x * wpb + warp; q < nl; q += gridDim.x * wpb) {
+        const int kk = q / half, r = q - kk * half;
+        const int k = k0 + kk;
+        const int jpar = ((color - k - j0) % 2 + 2) % 2;  // offset of the first j of this colour
+        const int j = j0 + jpar + 2 * r;
+        if (j > j1) continue;  // warp-uniform
+        const size_t row = cidx(0, j, k, nj, nip);
+        T carry = phi[row + i0 - 1];
+        for (int m = 0; m < R; ++m) {
+            const int base = ib + RC * m + V * lane;
+            const size_t c = row + (base + V <= nip ? base : 0);
+            T vt[V], vb[V], vn[V], vs[V], wt[V], wb[V], wn[V], ws[V], wu[V], wc[V], wi[V], wp[V];
+            ld16(phi + c + sk, vt); ld16(phi + c - sk, vb); ld16(phi + c + sj, vn); ld16(phi + c - sj, vs);
+            ld16(g.at + c, wt); ld16(g.ab + c, wb); ld16(g.an + c, wn); ld16(g.as + c, ws);
+            ld16(g.su + c, wu); ld16(g.cf + c, wc); ld16(g.iden + c, wi); ld16(g.pr + c, wp);
+            T a[V], e[V];
+            T Al = T(1), Bl = T(0);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const bool ok = base + v >= i0 && base + v <= i1;
+                const T d = wt[v] * vt[v] + wb[v] * vb[v] + wn[v] * vn[v] + ws[v] * vs[v] + wu[v];
+                a[v] = ok ? wc[v] : T(1);
+                e[v] = ok ? d * wi[v] : T(0);
+                Bl = a[v] * Bl + e[v];
+                Al = a[v] * Al;
+            }
+            T A = Al, B = Bl;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T A2 = __shfl_up_sync(full, A, o), B2 = __shfl_up_sync(full, B, o);
+                if (lane >= o) {
+                    B = A * B2 + B;
+                    A = A * A2;
+                }
+            }
+            T Ae = __shfl_up_sync(full, A, 1), Be = __shfl_up_sync(full, B, 1);
+            if (lane == 0) { Ae = T(1); Be = T(0); }
+            T x = Ae * carry + Be;
+            T qv[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                x = a[v] * x + e[v];
+                qv[v] = x;
+            }
+            T *dq = sq + (size_t)m * RC + V * lane, *dp = spr + (size_t)m * RC + V * lane;
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                dq[v] = qv[v];
+                dp[v] = wp[v];
+            }
+            carry = __shfl_sync(full, A * carry + B, 31);
+        }
+        __syncwarp();
+        T next = phi[row + i1 + 1];
+        for (int m = R - 1; m >= 0; --m) {
+            const int base = ib + RC * m + V * lane;
+            const T *dq = sq + (size_t)m * RC + V * lane, *dp = spr + (size_t)m * RC + V * lane;
+            T qv[V], pv[V];
+            bool okv[V];
+            T Al = T(1), Bl = T(0);
+#pragma unroll
+            for (int v = V - 1; v >= 0; --v) {
+                okv[v] = base + v >= i0 && base + v <= i1;
+                qv[v] = okv[v] ? dq[v] : T(0);
+                pv[v] = okv[v] ? dp[v] : T(1);
+                Bl = pv[v] * Bl + qv[v];
+                Al = pv[v] * Al;
+            }
+            T A = Al, B = Bl;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T A2 = __shfl_down_sync(full, A, o), B2 = __shfl_down_sync(full, B, o);
+                if (lane + o < 32) {
+                    B = A * B2 + B;
+                    A = A * A2;
+                }
+            }
+            T Ae = __shfl_down_sync(full, A, 1), Be = __shfl_down_sync(full, B, 1);
+            if (lane == 31) { Ae = T(1); Be = T(0); }
+            T x = Ae * next + Be;
+            T out[V];
+#pragma unroll
+            for (int v = V - 1; v >= 0; --v) {
+                x = pv[v] * x + qv[v];
+                out[v] = x;
+            }
+            bool all = true;
+#pragma unroll
+            for (int v = 0; v < V; ++v) all = all && okv[v];
+            if (all) {
+                typename Vec16<T>::type w;
+                memcpy(&w, out, 16);
+                *reinterpret_cast<typename Vec16<T>::type *>(phi + row + base) = w;
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v)
+                    if (okv[v]) phi[row + base + v] = out[v];
+            }
+            next = __shfl_sync(full, A * next + B, 0);
+        }
+        __syncwarp();
+    }
+}
+
+// Dynamic shared memory of sweep_rb_rounds_kernel: qr and pr of every round.
+template <typename T> size_t rounds_smem(const Params &p, int warps)
+{
+    const int RC = 32 * (16 / (int)sizeof(T));
+    const int R = (p.nim2 - 0) / RC + 1;
+    return (size_t)warps * 2 * R * RC * sizeof(T);
+}
+
+// ---------------------------------------------------------------------------
 // Ticket list of the momentum box, in (t, m, s) order (one CTA).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *tickets, int *ntickets,
@@ -481,17 +643,19 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
             sweep_exact_kernel<T, false><<<I.exact_grid, 32 * warps, smem, I.stream>>>(
                 I.p, I.g, phi, I.g.flags, I.g.tickets_energy, I.g.ntickets_energy,
                 &st->seq_energy, &st->done_energy, &st->ticket_energy);
-    } else {
-        int lines = box ? I.max_lines : (I.p.nj - 2) * (I.p.nk - 2);
-        int grid = std::max(1, std::min((lines / 2 + warps - 1) / warps + 1, I.sm_count * 16));
-        if (box) grid = std::min(grid, I.sm_count);  // melt-pool box: a few hundred lines
+    } else if (box) {
+        int grid = std::max(1, std::min((I.max_lines / 2 + warps - 1) / warps + 1, I.sm_count));
         for (int sweep = 0; sweep < 4; ++sweep)
-            for (int color = 0; color < 2; ++color) {
-                if (box)
-                    sweep_rb_kernel<T, true><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
-                else
-                    sweep_rb_kernel<T, false><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
-            }
+            for (int color = 0; color < 2; ++color)
+                sweep_rb_kernel<T, true><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
+    } else {
+        // whole domain: 4 warps per CTA, one line per warp
+        const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
+        const int grid = std::max(1, (lines + 3) / 4);
+        const size_t rs = rounds_smem<T>(I.p, 4);
+        for (int sweep = 0; sweep < 4; ++sweep)
+            for (int color = 0; color < 2; ++color)
+                sweep_rb_rounds_kernel<T><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color);
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
@@ -519,8 +683,16 @@ template <typename T> void set_sweep_smem_limit(size_t smem)
 {
     cudaFuncSetAttribute(sweep_exact_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(sweep_exact_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(sweep_rb_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(sweep_rb_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+// The whole-domain red-black kernel's buffer (qr and pr of 4 warps); false when it
+// does not fit a CTA.
+template <typename T> bool set_rounds_smem_limit(const Params &p)
+{
+    const size_t need = rounds_smem<T>(p, 4);
+    if (need > 200 * 1024) return false;
+    return cudaFuncSetAttribute(sweep_rb_rounds_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)need) == cudaSuccess;
 }
 
 #define AMCFD_INST(T)                                                     \
@@ -532,7 +704,8 @@ template <typename T> void set_sweep_smem_limit(size_t smem)
     template void launch_box_sweeps<T>(Inst<T> &, int);                  \
     template void launch_box_tickets<T>(Inst<T> &);                      \
     template int exact_sweep_blocks_per_sm<T>(int, size_t);              \
-    template void set_sweep_smem_limit<T>(size_t);
+    template void set_sweep_smem_limit<T>(size_t);                       \
+    template bool set_rounds_smem_limit<T>(const Params &);
 AMCFD_INST(double)
 AMCFD_INST(float)
 #undef AMCFD_INST
