@@ -551,6 +551,114 @@ __global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T
     }
 }
 
+// ---------------------------------------------------------------------------
+// Whole-domain factorisation in the same 16-byte-vector rounds (one warp per
+// line): den_i = ap_i - aw_i pr_{i-1}, pr_i = ae_i/den_i, cf_i = aw_i/den_i,
+// iden_i = 1/den_i from pr_{i0-1} = 0, and phi += delphi (the block correction).
+// pr follows the projective map x -> ae/(ap - aw x), i.e. the 2x2 matrix
+// [[0, ae], [-aw, ap]]: each lane multiplies the matrices of its cells, a warp
+// scan (rescaled as it goes; the map ignores scale) gives each lane the product
+// of the lanes below, applied to the carried pr of the previous round it is
+// the lane's entry value, and the lane then runs the recurrence itself.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d)
+{
+    const T mx = fmax(fmax(fabs(a), fabs(b)), fmax(fabs(c), fabs(d)));
+    if (mx > T(0)) {
+        const T s = T(1) / mx;
+        a *= s; b *= s; c *= s; d *= s;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) factor_rounds_kernel(Params p, Fields<T> g, T *phi)
+{
+    constexpr int V = 16 / (int)sizeof(T);
+    constexpr int RC = 32 * V;
+    const int i0 = 1, i1 = p.nim2;
+    const int J = p.njm2, K = p.nkm2;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const unsigned full = 0xffffffffu;
+    const int ib = i0 & ~31;
+    const int R = (i1 - ib) / RC + 1;
+    const int nj = p.nj, nip = p.nip, nl = J * K;
+    for (int q = blockIdx.x * wpb + warp; q < nl; q += gridDim.x * wpb) {
+        const int k = 1 + q / J, j = 1 + q % J;
+        const size_t row = cidx(0, j, k, nj, nip);
+        T carry = T(0);  // pr at cell i0 - 1
+        for (int m = 0; m < R; ++m) {
+            const int base = ib + RC * m + V * lane;
+            const bool inrow = base + V <= nip;
+            const size_t c = row + (inrow ? base : 0);
+            T ap[V], aw[V], ae[V], ph[V];
+            ld16(g.ap + c, ap); ld16(g.aw + c, aw); ld16(g.ae + c, ae); ld16(phi + c, ph);
+            bool ok[V];
+            // product of this lane's matrices, last cell leftmost
+            T m00 = T(1), m01 = T(0), m10 = T(0), m11 = T(1);
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                ok[v] = base + v >= i0 && base + v <= i1;
+                if (ok[v]) {  // [[0, ae], [-aw, ap]] * M
+                    const T n00 = ae[v] * m10, n01 = ae[v] * m11;
+                    const T n10 = -aw[v] * m00 + ap[v] * m10, n11 = -aw[v] * m01 + ap[v] * m11;
+                    m00 = n00; m01 = n01; m10 = n10; m11 = n11;
+                }
+            }
+            mat_rescale(m00, m01, m10, m11);
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const T b00 = __shfl_up_sync(full, m00, o), b01 = __shfl_up_sync(full, m01, o);
+                const T b10 = __shfl_up_sync(full, m10, o), b11 = __shfl_up_sync(full, m11, o);
+                if (lane >= o) {  // own * lower
+                    const T n00 = m00 * b00 + m01 * b10, n01 = m00 * b01 + m01 * b11;
+                    const T n10 = m10 * b00 + m11 * b10, n11 = m10 * b01 + m11 * b11;
+                    m00 = n00; m01 = n01; m10 = n10; m11 = n11;
+                    mat_rescale(m00, m01, m10, m11);
+                }
+            }
+            // exclusive product applied to the carried pr
+            T e00 = __shfl_up_sync(full, m00, 1), e01 = __shfl_up_sync(full, m01, 1);
+            T e10 = __shfl_up_sync(full, m10, 1), e11 = __shfl_up_sync(full, m11, 1);
+            T x = carry;
+            if (lane > 0) x = (e00 * carry + e01) / (e10 * carry + e11);
+            T pr[V], cf[V], id[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                if (ok[v]) {
+                    const T den = ap[v] - aw[v] * x;
+                    const T idv = T(1) / den;
+                    pr[v] = ae[v] * idv;
+                    cf[v] = aw[v] * idv;
+                    id[v] = idv;
+                    x = pr[v];
+                    ph[v] = ph[v] + (T)g.delphi[base + v];
+                } else {
+                    pr[v] = cf[v] = id[v] = T(0);
+                }
+            }
+            carry = __shfl_sync(full, x, 31);
+            bool all = true;
+#pragma unroll
+            for (int v = 0; v < V; ++v) all = all && ok[v];
+            if (all) {
+                typename Vec16<T>::type w;
+                memcpy(&w, pr, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.pr + c) = w;
+                memcpy(&w, cf, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.cf + c) = w;
+                memcpy(&w, id, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.iden + c) = w;
+                memcpy(&w, ph, 16); *reinterpret_cast<typename Vec16<T>::type *>(phi + c) = w;
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v)
+                    if (ok[v]) {
+                        g.pr[c + v] = pr[v]; g.cf[c + v] = cf[v]; g.iden[c + v] = id[v]; phi[c + v] = ph[v];
+                    }
+            }
+        }
+    }
+}
+
 // Dynamic shared memory of sweep_rb_rounds_kernel: qr and pr of every round.
 template <typename T> size_t rounds_smem(const Params &p, int warps)
 {
@@ -618,9 +726,8 @@ __global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *ticke
 // ---------------------------------------------------------------------------
 template <typename T> void launch_phi_factor(Inst<T> &I, T *phi)
 {
-    int lines = (I.p.nj - 2) * (I.p.nk - 2);
-    int grid = (lines + 31) / 32;
-    factor_kernel<T, false><<<grid, 256, 0, I.stream>>>(I.p, I.g, phi);
+    const int lines = (I.p.nj - 2) * (I.p.nk - 2);
+    factor_rounds_kernel<T><<<std::max(1, (lines + 3) / 4), 128, 0, I.stream>>>(I.p, I.g, phi);
 }
 template <typename T> void launch_energy_factor(Inst<T> &I) { launch_phi_factor<T>(I, I.g.h); }
 template <typename T> void launch_box_factor(Inst<T> &I)
