@@ -202,6 +202,19 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], const int (&
     (void)tid;
 }
 
+// One aligned 16-byte vector of a field (4 FP32 or 2 FP64 elements): the unit of
+// the coalesced row loads of the line-sweep, factorisation and H->T kernels.
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; };
+template <> struct Vec16<double> { using type = double2; };
+
+template <typename T>
+__device__ __forceinline__ void ld16(const T *ptr, T (&o)[16 / sizeof(T)])
+{
+    const typename Vec16<T>::type v = *reinterpret_cast<const typename Vec16<T>::type *>(ptr);
+    memcpy(o, &v, 16);
+}
+
 // Bounded spin budget for every device-side wait (about one second).
 constexpr long long kSpinLimit = 1ll << 24;
 

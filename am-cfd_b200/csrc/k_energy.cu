@@ -269,11 +269,6 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
 template <typename T>
 __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, double *red)
 {
-    // Work unit: a 32-cell chunk of one x-line (the pitch nip is a multiple of
-    // 32, so every chunk lies in one row and each warp's lanes share j and k).
-    // A warp takes U chunks at a time and issues all their loads before any
-    // store, so the latency of one chunk overlaps the others.
-    constexpr int U = 4;
     const Status *st = g.st;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
     const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
@@ -291,46 +286,38 @@ __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, doub
     const double ts = p.tsolid;
     const bool steady = p.steady != 0;
     const int lane = threadIdx.x & 31;
-    // chunk indices in 32-bit unsigned arithmetic (a chunk count far below 2^31 is
-    // checked at context creation): a 64-bit division per chunk costs more than
-    // the chunk's enthalpy inversion
-    const unsigned cpr = (unsigned)nip >> 5;  // chunks per row
+    // Work unit: a chunk of 32 V cells of one x-line, V = 16 bytes per element;
+    // lane l holds the 16-byte vector of cells base = chunk start + V l (the pitch
+    // nip is a multiple of 32, so a vector lies wholly inside or wholly past the
+    // padded row).  Chunk indices are 32-bit (the chunk count is bounded at
+    // context creation): a 64-bit division per chunk costs more than the
+    // chunk's enthalpy inversions.
+    constexpr int V = 16 / (int)sizeof(T);
+    constexpr int RC = 32 * V;
+    const unsigned cpr = ((unsigned)nip + RC - 1) / RC;  // chunks per row
     const unsigned unj = (unsigned)nj;
     const unsigned nchunks = (unsigned)nk * unj * cpr;
     const unsigned W = gridDim.x * (blockDim.x >> 5);
     const unsigned w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const double *dxw = g.dxpwinv, *dys = g.dypsinv, *dzb = g.dzpbinv;
-    for (unsigned q0 = w0; q0 < nchunks; q0 += W * U) {
-        T hv[U], hn[U], fln[U], rn[U], sv[U];
-        int iu[U], ju[U], ku[U];
+    for (unsigned q = w0; q < nchunks; q += W) {
+        const unsigned r = q / cpr;
+        const int base = (int)(q - r * cpr) * RC + V * lane;
+        const int k = (int)(r / unj), j = (int)(r - (unsigned)k * unj);
+        const bool inrow = base < nip;
+        const size_t c0 = (size_t)r * nip + (inrow ? base : 0);
+        T hv[V], hn[V], fln[V], rn[V], sv[V];
+        ld16(g.h + c0, hv); ld16(g.hnot + c0, hn); ld16(g.fraclnot + c0, fln);
+        ld16(g.rho_nxt + c0, rn); ld16(g.sourceinput + c0, sv);
+        const bool rowint = !steady && j >= 1 && j <= njm2 && k >= 1 && k <= nkm2;
+        T tout[V], fout[V];
+        int cmaxl = INT_MAX, cminl = INT_MIN;  // beam-row length candidates of this lane
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const unsigned q = q0 + (unsigned)u * W;
-            const unsigned r = q / cpr;
-            const int i = (int)(q - r * cpr) * 32 + lane;
-            const int k = (int)(r / unj), j = (int)(r - (unsigned)k * unj);
-            iu[u] = i; ju[u] = j; ku[u] = k;
-            const bool ok = q < nchunks && i < ni;
-            const bool interior = ok && !steady && i >= 1 && i <= nim2 && j >= 1 && j <= njm2 &&
-                                  k >= 1 && k <= nkm2;
-            const size_t c = ok ? (size_t)r * nip + i : 0;
-            hv[u] = ok ? g.h[c] : T(0);
-            hn[u] = interior ? g.hnot[c] : T(0);
-            fln[u] = interior ? g.fraclnot[c] : T(0);
-            rn[u] = interior ? g.rho_nxt[c] : T(0);
-            sv[u] = interior ? g.sourceinput[c] : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const unsigned q = q0 + (unsigned)u * W;
-            if (q >= nchunks) break;  // warp-uniform
-            const int i = iu[u], j = ju[u], k = ku[u];
-            const size_t c = ((size_t)k * nj + j) * nip + i;
-            const int ibase = i - lane;
-            if (ibase >= ni) continue;  // a padding chunk: warp-uniform
-            const unsigned act = (ibase + 32 <= ni) ? 0xffffffffu : ((1u << (ni - ibase)) - 1u);
-            if (i >= ni) continue;
-            const double h = (double)hv[u];
+        for (int v = 0; v < V; ++v) {
+            const int i = base + v;
+            tout[v] = fout[v] = T(0);
+            if (!inrow || i >= ni) continue;
+            const double h = (double)hv[v];
             double fl, t;
             if (h >= p.hlcal) {
                 fl = 1.0;
@@ -343,14 +330,14 @@ __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, doub
                 fl = kExact ? (h - p.hsmelt) / (p.hlcal - p.hsmelt) : (h - p.hsmelt) * inv_mush;
                 t = deltemp * fl + p.tsolid;
             }
-            g.fracl[c] = (T)fl;
-            g.temp[c] = (T)t;
+            fout[v] = (T)fl;
+            tout[v] = (T)t;
             const double tt = (double)(T)t;
             if (tt > tmax) tmax = tt;
             // melt-pool scan candidates (BoundCondManager.cpp:318-417).  Most cells
             // are solid, so each atomic is issued only when it can still change the
             // value (candidates only move one way); the beam-row scalars are
-            // warp-reduced.
+            // warp-reduced below.
             if (j == js && k >= 1 && k <= nkm2 && tt < ts && k > *(volatile int *)&g.mp_kb[i])
                 atomicMax(&g.mp_kb[i], k);
             if (k == nkm1) {
@@ -358,22 +345,39 @@ __global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, doub
                     atomicMin(&g.mp_jup[i], j);
                 if (j >= 1 && j <= js && tt < ts && j > *(volatile int *)&g.mp_jdn[i])
                     atomicMax(&g.mp_jdn[i], j);
-                if (j == js) {  // row-uniform: every lane of the chunk with i < ni is here
-                    const int cmax = (i >= is0 && i < nim1 && tt <= ts) ? i : INT_MAX;
-                    const int cmin = (i >= 1 && i <= is0 && tt < ts) ? i : INT_MIN;
-                    const int wmin = __reduce_min_sync(act, cmax), wmax = __reduce_max_sync(act, cmin);
-                    if (lane == 0) {
-                        if (wmin != INT_MAX) atomicMin(&g.st->mp_imax, wmin);
-                        if (wmax != INT_MIN) atomicMax(&g.st->mp_imin, wmax);
-                    }
+                if (j == js) {
+                    if (i >= is0 && i < nim1 && tt <= ts) cmaxl = min(cmaxl, i);
+                    if (i >= 1 && i <= is0 && tt < ts) cminl = max(cminl, i);
                 }
             }
-            if (i < 1 || i > nim2 || j < 1 || j > njm2 || k < 1 || k > nkm2) continue;
-            if (!steady) {
-                const double dh1 = h - (double)hn[u] + ((double)(T)fl - (double)fln[u]) * p.hlatnt;
-                const double vol = volume_p(p, g, i, j, k);
-                accul += kExact ? vol * (double)rn[u] * dh1 / delt : vol * (double)rn[u] * dh1 * inv_delt;
-                heatvol += (double)sv[u] * vol;
+            if (!rowint || i < 1 || i > nim2) continue;
+            const double dh1 = h - (double)hn[v] + ((double)(T)fl - (double)fln[v]) * p.hlatnt;
+            const double vol = volume_p(p, g, i, j, k);
+            accul += kExact ? vol * (double)rn[v] * dh1 / delt : vol * (double)rn[v] * dh1 * inv_delt;
+            heatvol += (double)sv[v] * vol;
+        }
+        if (inrow) {
+            if (base + V <= ni) {
+                typename Vec16<T>::type w;
+                memcpy(&w, tout, 16);
+                *reinterpret_cast<typename Vec16<T>::type *>(g.temp + c0) = w;
+                memcpy(&w, fout, 16);
+                *reinterpret_cast<typename Vec16<T>::type *>(g.fracl + c0) = w;
+            } else {
+#pragma unroll
+                for (int v = 0; v < V; ++v)
+                    if (base + v < ni) {
+                        g.temp[c0 + v] = tout[v];
+                        g.fracl[c0 + v] = fout[v];
+                    }
+            }
+        }
+        if (k == nkm1 && j == js) {  // chunk-uniform: every lane takes part
+            const int wmin = __reduce_min_sync(0xffffffffu, cmaxl);
+            const int wmax = __reduce_max_sync(0xffffffffu, cminl);
+            if (lane == 0) {
+                if (wmin != INT_MAX) atomicMin(&g.st->mp_imax, wmin);
+                if (wmax != INT_MIN) atomicMax(&g.st->mp_imin, wmax);
             }
         }
     }

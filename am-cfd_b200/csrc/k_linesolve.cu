@@ -417,17 +417,6 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 // write; vectors past the end of the padded row read its first vector and are
 // masked.
 // ---------------------------------------------------------------------------
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; };
-template <> struct Vec16<double> { using type = double2; };
-
-template <typename T>
-__device__ __forceinline__ void ld16(const T *ptr, T (&o)[16 / sizeof(T)])
-{
-    const typename Vec16<T>::type v = *reinterpret_cast<const typename Vec16<T>::type *>(ptr);
-    memcpy(o, &v, 16);
-}
-
 template <typename T>
 __global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color)
 {
