@@ -38,7 +38,9 @@ template <typename T> struct AsmBox {
 enum { FA_D = 0, FA_H, FA_F, FA_R, FA_W };
 enum { FB_U = 0, FB_V, FB_T, FB_HN, FB_FN };
 
-template <typename T>
+// SCH: the discretisation scheme as a compile-time constant (one instantiation per
+// scheme), so that the six face coefficients carry no untaken scheme branches.
+template <typename T, int SCH>
 __global__ void __launch_bounds__(256, 2)
 energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp)
 {
@@ -66,7 +68,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     const bool colint = in && i >= 1 && i <= nim2 && j >= 1 && j <= njm2;
     const size_t sk = (size_t)nj * nip;
     const size_t col = in ? cidx(i, j, 0, nj, nip) : 0;
-    const int sch = p.scheme;
+    constexpr int sch = SCH;
     const double delt = st->delt;
     const bool volsrc = p.volsrc != 0;
     const bool powder = p.powder != 0;
@@ -410,16 +412,28 @@ template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T
         if (rc) return rc;
     }
     I.asm_diff_a = diff_a;
-    cudaFuncSetAttribute(energy_assemble_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)B::SMEM);
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
     return 0;
 }
 
 template <typename T> void launch_energy_assemble(Inst<T> &I)
 {
     const AsmMaps &m = I.g.diff_cur == I.asm_diff_a ? I.asm_maps[0] : I.asm_maps[1];
-    energy_assemble_kernel<T><<<I.asm_grid, dim3(kTX, kTY), AsmBox<T>::SMEM, I.stream>>>(
-        I.p, I.g, I.red_asm, m);
+    const dim3 blk(kTX, kTY);
+    const size_t sm = AsmBox<T>::SMEM;
+    switch (I.p.scheme) {
+    case AMCFD_SCHEME_UPWIND:
+        energy_assemble_kernel<T, 0><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
+        break;
+    case AMCFD_SCHEME_POWER_LAW:
+        energy_assemble_kernel<T, 1><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
+        break;
+    default:
+        energy_assemble_kernel<T, 2><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
+        break;
+    }
 }
 
 template void launch_energy_assemble<double>(Inst<double> &);

@@ -660,31 +660,79 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     // warp scans of affine maps over per-lane chunks.
     const int half = (NJ + 1) / 2;
     if (NI <= 48) {
+        // Short lines (the usual melt-pool box): a group of G lanes per line, each
+        // lane a chunk of at most 6 cells, chained by segmented shuffle scans of
+        // the affine maps (x -> cf x + e forward, x -> pr x + qr backward).  The
+        // loop over lines advances a warp's four groups together, so that every
+        // shuffle has all 32 lanes; a group without a line carries identity maps.
+        constexpr int G = 8;
+        const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
+        const int sub = lane & (G - 1), gw = lane / G;  // lane in its group, group in its warp
+        const int L = (NI + G - 1) / G;
+        const int a = min(sub * L, NI), e = min(a + L, NI);
+        const int nline = half * NK;
         for (int sweep = 0; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color) {
-                for (int l = tid; l < half * NK; l += nth) {
-                    const int kk = l / half, r = l - kk * half;
-                    const int k = b.k0 + kk;
-                    const int jpar = ((color - k - b.j0) % 2 + 2) % 2;
-                    const int jj = jpar + 2 * r;
-                    if (jj >= NJ) continue;
-                    const T *pat = &at(0, jj, kk), *pab = &ab(0, jj, kk), *pan = &an(0, jj, kk),
-                            *pas = &as(0, jj, kk), *psu = &su(0, jj, kk), *pcf = &cf(0, jj, kk),
-                            *pid = &id(0, jj, kk), *ppr = &pr(0, jj, kk);
-                    T *pqr = &qr(0, jj, kk), *pph = &ph(0, jj, kk);
-                    const T *pt = &ph(0, jj, kk + 1), *pb = &ph(0, jj, kk - 1), *pn = &ph(0, jj + 1, kk),
-                            *ps = &ph(0, jj - 1, kk);
-                    T q = pph[-1];
-                    for (int ii = 0; ii < NI; ++ii) {
-                        const T d = pat[ii] * pt[ii] + pab[ii] * pb[ii] + pan[ii] * pn[ii] + pas[ii] * ps[ii] + psu[ii];
-                        q = pcf[ii] * q + d * pid[ii];
-                        pqr[ii] = q;
+                for (int l0 = warp * (32 / G); l0 < nline; l0 += nwarp * (32 / G)) {
+                    const int l = l0 + gw;
+                    int kk = 0, jj = 0;
+                    bool act = l < nline;
+                    if (act) {
+                        kk = l / half;
+                        const int r = l - kk * half;
+                        const int k = b.k0 + kk;
+                        const int jpar = ((color - k - b.j0) % 2 + 2) % 2;
+                        jj = jpar + 2 * r;
+                        act = jj < NJ;
                     }
-                    T x = pph[NI];
-                    for (int ii = NI - 1; ii >= 0; --ii) {
-                        x = ppr[ii] * x + pqr[ii];
-                        pph[ii] = x;
+                    T A = T(1), B = T(0);
+                    if (act)
+                        for (int ii = a; ii < e; ++ii) {
+                            const T d = at(ii, jj, kk) * ph(ii, jj, kk + 1) + ab(ii, jj, kk) * ph(ii, jj, kk - 1) +
+                                        an(ii, jj, kk) * ph(ii, jj + 1, kk) + as(ii, jj, kk) * ph(ii, jj - 1, kk) +
+                                        su(ii, jj, kk);
+                            const T ev = d * id(ii, jj, kk), c = cf(ii, jj, kk);
+                            qr(ii, jj, kk) = ev;
+                            B = c * B + ev;
+                            A = c * A;
+                        }
+#pragma unroll
+                    for (int o = 1; o < G; o <<= 1) {
+                        const T A2 = __shfl_up_sync(0xffffffffu, A, o, G), B2 = __shfl_up_sync(0xffffffffu, B, o, G);
+                        if (sub >= o) { B = A * B2 + B; A = A * A2; }
                     }
+                    T Ae = __shfl_up_sync(0xffffffffu, A, 1, G), Be = __shfl_up_sync(0xffffffffu, B, 1, G);
+                    if (sub == 0) { Ae = T(1); Be = T(0); }
+                    A = T(1);
+                    B = T(0);
+                    if (act) {
+                        T q = Ae * ph(-1, jj, kk) + Be;
+                        for (int ii = a; ii < e; ++ii) {
+                            q = cf(ii, jj, kk) * q + qr(ii, jj, kk);
+                            qr(ii, jj, kk) = q;
+                        }
+                        for (int ii = e - 1; ii >= a; --ii) {
+                            const T pv = pr(ii, jj, kk);
+                            B = pv * B + qr(ii, jj, kk);
+                            A = pv * A;
+                        }
+                    }
+#pragma unroll
+                    for (int o = 1; o < G; o <<= 1) {
+                        const T A2 = __shfl_down_sync(0xffffffffu, A, o, G), B2 = __shfl_down_sync(0xffffffffu, B, o, G);
+                        if (sub + o < G) { B = A * B2 + B; A = A * A2; }
+                    }
+                    Ae = __shfl_down_sync(0xffffffffu, A, 1, G);
+                    Be = __shfl_down_sync(0xffffffffu, B, 1, G);
+                    if (sub == G - 1) { Ae = T(1); Be = T(0); }
+                    if (act) {
+                        T x = Ae * ph(NI, jj, kk) + Be;
+                        for (int ii = e - 1; ii >= a; --ii) {
+                            x = pr(ii, jj, kk) * x + qr(ii, jj, kk);
+                            ph(ii, jj, kk) = x;
+                        }
+                    }
+                    __syncwarp();
                 }
                 __syncthreads();
             }
