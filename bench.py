@@ -40,8 +40,8 @@ WORDS = {"energy_assemble": 40, "factor": 2, "energy_sweeps": 40, "h2t_meltpool"
 # DRAM bytes per interior cell per launch (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum, one capture of each kernel on the 400x200x100 deck,
 # FP32 bulk); the line reports them scaled by the cell count.
-TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 85.5, "energy_sweeps:fp32:redblack": 20.3,
-                    "h2t_meltpool:fp32:redblack": 28.6, "factor:fp32:redblack": 27.8}
+TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 85.3, "energy_sweeps:fp32:redblack": 20.2,
+                    "h2t_meltpool:fp32:redblack": 28.7, "factor:fp32:redblack": 27.2}
 
 
 def _peaks():
