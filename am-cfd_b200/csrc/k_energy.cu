@@ -471,6 +471,42 @@ __device__ void reset_scan_candidates(const Params &p, Fields<T> &g)
 // order (the NaN behaviour of std::max/min) run sequentially in thread 0.
 // Also activates the momentum box and builds its exact-order ticket list.
 // ---------------------------------------------------------------------------
+// acc = f(x_i, acc) in ascending i over the flagged i of [lo, hi), from init,
+// with f = std::max or std::min as the reference folds (maxd/mind): a NaN element
+// makes acc NaN and the next element replaces it.  The fold therefore equals the
+// extreme of the flagged elements after the last NaN, NaN when that NaN is the
+// last flagged element, and includes init only when no NaN occurs -- which a
+// block can compute in two passes.  Every thread of the block calls it.
+__device__ double ordered_fold(const double *x, const int *fl, int bit, int lo, int hi, double init,
+                               bool is_max, int *si, double *sd)
+{
+    const int tid = threadIdx.x, nth = blockDim.x;
+    if (tid == 0) { si[0] = -1; si[1] = -1; }
+    __syncthreads();
+    int lastf = -1, lastn = -1;  // per thread, indices ascend
+    for (int i = lo + tid; i < hi; i += nth)
+        if (fl[i] & bit) {
+            lastf = i;
+            if (isnan(x[i])) lastn = i;
+        }
+    if (lastf >= 0) atomicMax(&si[0], lastf);
+    if (lastn >= 0) atomicMax(&si[1], lastn);
+    __syncthreads();
+    const int L = si[0], P = si[1];
+    double v = is_max ? -INFINITY : INFINITY;
+    for (int i = max(lo, P + 1) + tid; i < hi; i += nth)
+        if (fl[i] & bit) v = is_max ? fmax(v, x[i]) : fmin(v, x[i]);
+    v = is_max ? warp_max(v) : -warp_max(-v);
+    if ((tid & 31) == 0) sd[tid >> 5] = v;
+    __syncthreads();
+    double r = is_max ? -INFINITY : INFINITY;
+    for (int w = 0; w < (nth + 31) / 32; ++w) r = is_max ? fmax(r, sd[w]) : fmin(r, sd[w]);
+    __syncthreads();
+    if (L < 0) return init;
+    if (P >= 0) return P == L ? (double)NAN : r;
+    return is_max ? ((r < init) ? init : r) : ((init < r) ? init : r);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, const double *red_h2t,
                                                         int nblk_h2t)
@@ -558,6 +594,13 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
         imaxc[i] = fl;
     }
     __syncthreads();
+    // the reference's three folds over the columns (BoundCondManager.cpp:360-417),
+    // in parallel with the same NaN behaviour
+    __shared__ int fsi[2];
+    __shared__ double fsd[32];
+    const double depth_f = ordered_fold(depv, imaxc, 1, 1, nim1, 0.0, true, fsi, fsd);
+    const double ymax_f = ordered_fold(wmax, imaxc, 2, 1, nim1, g.y[0], true, fsi, fsd);
+    const double ymin_f = ordered_fold(wmin, imaxc, 4, 1, nim1, YY(js), false, fsi, fsd);
     if (threadIdx.x == 0) {
         auto XX = [&](int i) { return (i < 0 || i >= p.ni) ? (double)NAN : g.x[i]; };
         double dtdxxinv = (XX(imax) - XX(imax + 1)) / (TT(imax, js, nkm1) - TT(imax + 1, js, nkm1));
@@ -565,22 +608,9 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
         dtdxxinv = (XX(imin) - XX(imin - 1)) / (TT(imin, js, nkm1) - TT(imin - 1, js, nkm1));
         double xxmin = XX(imin) + (ts - TT(imin, js, nkm1)) * dtdxxinv;
         st->alen = xxmax - xxmin;
-        double depth = 0.0;
-        if (kmin == 0) {
-            depth = g.z[nkm1] - g.z[0];
-        } else {
-            for (int i = 1; i < nim1; i++)
-                if (imaxc[i] & 1) depth = maxd(depv[i], depth);
-        }
-        st->depth = depth;
-        double yymax = g.y[0];
-        if (jmax != js)
-            for (int i = 1; i < nim1; i++)
-                if (imaxc[i] & 2) yymax = maxd(wmax[i], yymax);
-        double yymin = YY(js);
-        if (jmin != js)
-            for (int i = 1; i < nim1; i++)
-                if (imaxc[i] & 4) yymin = mind(wmin[i], yymin);
+        st->depth = kmin == 0 ? g.z[nkm1] - g.z[0] : depth_f;
+        const double yymax = jmax != js ? ymax_f : g.y[0];
+        const double yymin = jmin != js ? ymin_f : YY(js);
         st->width = yymax - yymin;
         st->imax = imax; st->imin = imin; st->kmin = kmin; st->kmax = nkm2;
         st->jmax = jmax; st->jmin = jmin;
