@@ -11,8 +11,11 @@
 // rings completing on mbarriers:
 //   ring A (diff, h, f_l, rho, w): planes k-1, k, k+1 resident, k+2 in flight;
 //   ring B (u, v, T, hnot, f_l,not): plane k resident, k+1 in flight.
-// One thread issues the copies one plane ahead, so the loads of plane k+1
-// overlap the arithmetic of plane k and no thread waits on a global load.
+// There is no CTA-wide barrier per plane: each warp counts itself done with a
+// plane in a shared counter, and the last warp to finish plane k refills the
+// slots that held planes k-1 (ring A) and k (ring B).  Warps therefore drift up
+// to one plane apart instead of waiting for the slowest, and no thread waits on
+// a global load.
 // Face areas and volumes are products of per-column (x, y) and per-plane (z)
 // widths, formed in FP64 in the reference's order.  The arithmetic is the
 // reference's expression by expression; the FP32 build evaluates properties
@@ -31,17 +34,26 @@ template <typename T> struct AsmBox {
     static constexpr int BY = kTY + 2;              // box height (rows)
     static constexpr int BYTES = BX * BY * (int)sizeof(T);
     static constexpr int FE = ((BYTES + 127) / 128 * 128) / (int)sizeof(T);  // 128-B aligned stride
-    static constexpr int NA = 5, NB = 5, SA = 4, SB = 2;  // fields and ring slots
+    // fields per ring and ring slots (planes): FP32 rings take 50 KB, FP64 88 KB.
+    // Deeper FP32 rings (5 + 3 planes, 67 KB) measured slower on the 400x200x100
+    // deck: 328 against 286 us a launch.
+    static constexpr int NA = 5, NB = 5, SA = 4, SB = 2;
     // rings + mbarriers + slack to align the dynamic region to 128 bytes
     static constexpr size_t SMEM = (size_t)(SA * NA + SB * NB) * FE * sizeof(T) + 8 * (SA + SB) + 128;
+    // resident CTAs per SM: three in FP32 (80 registers a thread still hold the
+    // whole stencil), two in FP64
+    static constexpr int MINB = sizeof(T) == 4 ? 3 : 2;
 };
+// Warps of a CTA, and the plane-completion counters (a warp is at most one
+// plane ahead of the slowest, so four counters never mix two planes).
+constexpr int kAsmWarps = kTX * kTY / 32, kAsmCounters = 4;
 enum { FA_D = 0, FA_H, FA_F, FA_R, FA_W };
 enum { FB_U = 0, FB_V, FB_T, FB_HN, FB_FN };
 
 // SCH: the discretisation scheme as a compile-time constant (one instantiation per
 // scheme), so that the six face coefficients carry no untaken scheme branches.
 template <typename T, int SCH>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, AsmBox<T>::MINB)
 energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp)
 {
     using R = T;
@@ -53,10 +65,11 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     T *bufB = bufA + B::SA * B::NA * FE;
     uint64_t *barA = reinterpret_cast<uint64_t *>(bufB + B::SB * B::NB * FE);
     uint64_t *barB = barA + B::SA;
-    __shared__ double sb[4][kTY][kTX + 1];
+    __shared__ uint32_t done_cnt[kAsmCounters];  // warps done, per plane (k - kb) mod 4
+    __shared__ int lastA[B::SA], lastB[B::SB];  // last plane issued into each slot
 
     Status *st = g.st;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx, lane = tid & 31;
     const int i = blockIdx.x * kTX + tx, j = blockIdx.y * kTY + ty;
     const int x0 = blockIdx.x * kTX - OX, y0 = blockIdx.y * kTY - 1;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
@@ -73,10 +86,17 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     const bool volsrc = p.volsrc != 0;
     const bool powder = p.powder != 0;
 
-    // ---- copy pipeline (thread 0 issues; all threads wait) ----
+    // ---- copy pipeline ----
+    // Slots are filled in plane order (ring A from plane kb-1, ring B from kb),
+    // so the n-th fill of a slot completes its barrier's phase of parity n & 1.
+    auto slotA = [&](int q) { return (q - kb + 1) % B::SA; };
+    auto parA = [&](int q) { return (uint32_t)(((q - kb + 1) / B::SA) & 1); };
+    auto slotB = [&](int q) { return (q - kb) % B::SB; };
+    auto parB = [&](int q) { return (uint32_t)(((q - kb) / B::SB) & 1); };
     auto issueA = [&](int q) {
-        const int s = q & 3;
+        const int s = slotA(q);
         T *dst = bufA + s * B::NA * FE;
+        lastA[s] = q;
         fence_proxy_async();
         mbar_expect_tx(&barA[s], B::NA * B::BYTES);
         tma_load_3d(dst + FA_D * FE, &mp.diff, x0, y0, q, &barA[s]);
@@ -86,8 +106,9 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
         tma_load_3d(dst + FA_W * FE, &mp.w, x0, y0, q, &barA[s]);
     };
     auto issueB = [&](int q) {
-        const int s = q & 1;
+        const int s = slotB(q);
         T *dst = bufB + s * B::NB * FE;
+        lastB[s] = q;
         fence_proxy_async();
         mbar_expect_tx(&barB[s], B::NB * B::BYTES);
         tma_load_3d(dst + FB_U * FE, &mp.u, x0, y0, q, &barB[s]);
@@ -96,34 +117,21 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
         tma_load_3d(dst + FB_HN * FE, &mp.hnot, x0, y0, q, &barB[s]);
         tma_load_3d(dst + FB_FN * FE, &mp.flnot, x0, y0, q, &barB[s]);
     };
-    // The n-th completion of a slot's barrier has parity n & 1; ring A receives
-    // planes kb-1, kb, ... in order over four slots, ring B planes kb, ... over two.
-    auto parA = [&](int q) { return (uint32_t)(((q - (kb - 1)) >> 2) & 1); };
-    auto parB = [&](int q) { return (uint32_t)(((q - kb) >> 1) & 1); };
-    // planes issued but not yet waited for: A [pa0, pa1], B [pb0, pb1]; thread 0
-    // drains them before an early exit so that no copy lands in a finished CTA
-    int pa0 = kb - 1, pa1 = kb - 2, pb0 = kb, pb1 = kb - 1;
+    constexpr int kNone = -(1 << 30);
 
     if (tid == 0) {
-        for (int s = 0; s < B::SA; ++s) mbar_init(&barA[s]);
-        for (int s = 0; s < B::SB; ++s) mbar_init(&barB[s]);
+        for (int s = 0; s < B::SA; ++s) { mbar_init(&barA[s]); lastA[s] = kNone; }
+        for (int s = 0; s < B::SB; ++s) { mbar_init(&barB[s]); lastB[s] = kNone; }
+        for (int s = 0; s < kAsmCounters; ++s) done_cnt[s] = 0u;
     }
     __syncthreads();
     if (kb >= ke) return;
     if (tid == 0) {
-        issueA(kb - 1);
-        issueA(kb);
-        issueA(kb + 1);
-        issueB(kb);
+        for (int q = kb - 1; q <= min(kb - 2 + B::SA, ke); ++q) issueA(q);
+        for (int q = kb; q <= min(kb - 1 + B::SB, ke - 1); ++q) issueB(q);
     }
-    pa1 = kb + 1;
-    pb1 = kb;
-    bool ok = mbar_wait(&barA[(kb - 1) & 3], parA(kb - 1), st, 1);
-    if (ok) {
-        pa0 = kb;
-        ok = mbar_wait(&barA[kb & 3], parA(kb), st, 1);
-        if (ok) pa0 = kb + 1;
-    }
+    bool ok = mbar_wait(&barA[slotA(kb - 1)], parA(kb - 1), st, 1);
+    if (ok) ok = mbar_wait(&barA[slotA(kb)], parA(kb), st, 1);
 
     // per-column metrics (interior columns only)
     double dx = 0.0, dy = 0.0;
@@ -149,24 +157,16 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     const int o = (ty + 1) * BX + tx + OX;  // this thread's cell inside a box
 
     for (int k = kb; k < ke; ++k) {
-        if (tid == 0 && ok) {
-            if (k + 2 <= ke) { issueA(k + 2); pa1 = k + 2; }
-            if (k + 1 < ke) { issueB(k + 1); pb1 = k + 1; }
-        }
-        if (ok) {
-            ok = mbar_wait(&barA[(k + 1) & 3], parA(k + 1), st, 2);
-            if (ok) pa0 = k + 2;
-        }
-        if (ok) {
-            ok = mbar_wait(&barB[k & 1], parB(k), st, 3);
-            if (ok) pb0 = k + 1;
-        }
-        const T *Am = bufA + ((k - 1) & 3) * B::NA * FE + o;  // plane k-1
-        const T *Ac = bufA + (k & 3) * B::NA * FE + o;        // plane k
-        const T *Ap = bufA + ((k + 1) & 3) * B::NA * FE + o;  // plane k+1
-        const T *Bc = bufB + (k & 1) * B::NB * FE + o;        // plane k
+        if (ok) ok = mbar_wait(&barA[slotA(k + 1)], parA(k + 1), st, 2);
+        if (ok) ok = mbar_wait(&barB[slotB(k)], parB(k), st, 3);
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        const T *Am = bufA + slotA(k - 1) * B::NA * FE + o;  // plane k-1
+        const T *Ac = bufA + slotA(k) * B::NA * FE + o;      // plane k
+        const T *Ap = bufA + slotA(k + 1) * B::NA * FE + o;  // plane k+1
+        const T *Bc = bufB + slotB(k) * B::NB * FE + o;      // plane k
         const size_t c = col + (size_t)k * sk;
-        if (in && ok) {
+        if (in) {
             const R d_c = Ac[FA_D * FE], f_c = Ac[FA_F * FE], t_c = Bc[FB_T * FE];
             // ---- material properties (every node) ----
             {
@@ -345,18 +345,35 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
             }
         }
-        // every thread is done with plane k-1 (ring A) and plane k (ring B)
-        // before thread 0 refills those slots
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                // drain what is still in flight (bounded), then leave
-                for (int q = pa0; q <= pa1; ++q) mbar_try(&barA[q & 3], parA(q), kSpinLimit);
-                for (int q = pb0; q <= pb1; ++q) mbar_try(&barB[q & 1], parB(q), kSpinLimit);
+        // this warp is done with planes k-1 (ring A) and k (ring B); the last warp
+        // to finish plane k refills both slots (its reads are ordered before the
+        // copies by the warp sync, the CTA-scope fences and the proxy fence)
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            const int r = k - kb;
+            const uint32_t n = atomicAdd(&done_cnt[r % kAsmCounters], 1u);
+            if (n == (uint32_t)(kAsmWarps * (r / kAsmCounters + 1) - 1)) {
+                __threadfence_block();
+                if (k - 1 + B::SA <= ke) issueA(k - 1 + B::SA);
+                if (k + B::SB < ke) issueB(k + B::SB);
             }
-            return;
         }
     }
-    // per-i partial sums over this block's j-rows and planes
+    // every warp has left the plane loop: nothing is issued after this point
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+            // drain the copies still in flight (bounded), then leave
+            for (int s = 0; s < B::SA; ++s)
+                if (lastA[s] != kNone) mbar_try(&barA[s], parA(lastA[s]), kSpinLimit);
+            for (int s = 0; s < B::SB; ++s)
+                if (lastB[s] != kNone) mbar_try(&barB[s], parB(lastB[s]), kSpinLimit);
+        }
+        return;
+    }
+    // per-i partial sums over this block's j-rows and planes, staged in ring A
+    // (every copy has been consumed)
+    double (*sb)[kTY][kTX + 1] = reinterpret_cast<double (*)[kTY][kTX + 1]>(base);
     sb[0][ty][tx] = bl;
     sb[1][ty][tx] = blp;
     sb[2][ty][tx] = blm;
