@@ -111,6 +111,9 @@ struct amcfd_ctx {
     // the iteration swaps the current/next property buffers, so two graphs alternate.
     bool use_graphs = false;
     cudaGraphExec_t gexec[2][2][2] = {};  // [events][parity][small-box momentum]
+    // the whole outer loop of a step as one graph, by property parity at its start
+    cudaGraphExec_t gloop[2] = {};
+    bool host_loop = false;        // drive the outer iterations from the host even with graphs
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
@@ -574,6 +577,11 @@ static void drop_graphs(amcfd_ctx *ctx)
                     cudaGraphExecDestroy(ge);
                     ge = nullptr;
                 }
+    for (auto &ge : ctx->gloop)
+        if (ge) {
+            cudaGraphExecDestroy(ge);
+            ge = nullptr;
+        }
 }
 
 // ---- one outer iteration -----------------------------------------------------------------
@@ -692,6 +700,10 @@ static int begin_step(amcfd_ctx *ctx)
     h->powerindicator = ctx->powerindicator;
     h->istart = ctx->istart;
     h->jstart = ctx->jstart;
+    h->lp_niter = 0;
+    h->lp_box = ctx->last_box;
+    h->lp_mode = 0;
+    h->lp_small = 0;
     // the per-step block is the leading members of Status, up to heat_iter
     CK(cudaMemcpyAsync(ctx->st_dev, h, offsetof(Status, heat_iter), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -823,6 +835,152 @@ static int launch_iteration_graph(amcfd_ctx *ctx, Inst<T> &I)
     return 0;
 }
 
+// ---- the outer loop of a step as one CUDA graph ----------------------------------------
+// Outer iterations 1..maxit are chained by conditional if-nodes: iteration k+1
+// runs when the convergence kernel of iteration k sets its condition (the host
+// loop's test: not converged, finite, no device error, fewer than maxit
+// iterations), and an if/else node in each iteration takes the momentum path
+// that the host would have chosen from the previous iteration's box.  The chain
+// has no loop node, so a condition that is never set only ends the step early.
+// Iterations alternate the property parity, so the graph is built per parity of
+// its first iteration.  The host launches it once per step and reads the status
+// once.
+constexpr int kMaxChain = 64;  // longer maxit: the host drives the loop
+
+template <typename T>
+static int build_loop_graph(amcfd_ctx *ctx, Inst<T> &I, cudaGraphExec_t &ge)
+{
+    const int maxit = ctx->prm.maxit;
+    const int cap = ctx->small_box && ctx->order == AMCFD_ORDER_REDBLACK ? mom_small_capacity<T>(I) : -1;
+    const double tol = ctx->prm.nonlintol;
+    std::vector<cudaGraph_t> parts;  // captured pieces; child nodes hold copies
+    cudaGraph_t top = nullptr;
+    cudaError_t err = cudaSuccess;
+    auto keep = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+        return err == cudaSuccess;
+    };
+    auto capture = [&](auto &&launch) -> cudaGraph_t {
+        if (!keep(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal))) return nullptr;
+        launch();
+        cudaGraph_t g = nullptr;
+        if (!keep(cudaStreamEndCapture(ctx->stream, &g))) return nullptr;
+        parts.push_back(g);
+        return g;
+    };
+    auto child = [&](cudaGraph_t parent, cudaGraphNode_t dep, cudaGraph_t g) -> cudaGraphNode_t {
+        cudaGraphNode_t n = nullptr;
+        if (err == cudaSuccess) keep(cudaGraphAddChildGraphNode(&n, parent, dep ? &dep : nullptr, dep ? 1 : 0, g));
+        return n;
+    };
+    auto cond = [&](cudaGraph_t parent, cudaGraphNode_t dep, cudaGraphConditionalHandle h, unsigned size,
+                    cudaGraph_t *bodies) -> cudaGraphNode_t {
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = size;
+        cudaGraphNode_t n = nullptr;
+        if (err == cudaSuccess && keep(cudaGraphAddNode(&n, parent, dep ? &dep : nullptr, dep ? 1 : 0, &np)))
+            for (unsigned q = 0; q < size; ++q) bodies[q] = np.conditional.phGraph_out[q];
+        return n;
+    };
+    keep(cudaGraphCreate(&top, 0));
+    std::vector<cudaGraphConditionalHandle> hc(maxit + 1), hm(maxit + 1);
+    for (int k = 1; k <= maxit && err == cudaSuccess; ++k) {
+        keep(cudaGraphConditionalHandleCreate(&hm[k], top, 0, cudaGraphCondAssignDefault));
+        if (k < maxit) keep(cudaGraphConditionalHandleCreate(&hc[k], top, 0, cudaGraphCondAssignDefault));
+    }
+    // the energy part and the momentum paths depend only on the parity
+    cudaGraph_t energy[2] = {}, mom_small_g[2] = {}, mom_grid_g[2] = {};
+    for (int q = 0; q < 2; ++q) {
+        energy[q] = capture([&] {
+            run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_ASSEMBLE);
+            run_phase_impl<T>(ctx, I, AMCFD_PHASE_ENERGY_SOLVE);
+            run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
+            run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
+        });
+        if (cap >= 0) mom_small_g[q] = capture([&] { launch_momentum<T>(I, true); });
+        mom_grid_g[q] = capture([&] { launch_momentum<T>(I, false); });
+        swap_props<T>(I);
+    }
+    cudaGraph_t g_init = capture([&] {
+        const LoopCtl lc{0, hm[1], 1, 1, maxit, cap};
+        launch_loop_init(ctx->st_dev, lc, I.stream);
+    });
+    // top: init, iteration 1, then iterations 2..maxit in sequence, each inside an
+    // if-node on the condition its predecessor sets (a skipped iteration leaves the
+    // next condition at its default 0, so the rest of the chain is skipped too)
+    cudaGraphNode_t last = child(top, nullptr, g_init);
+    for (int k = 1; k <= maxit && err == cudaSuccess; ++k) {
+        const int q = (k - 1) & 1;  // parity relative to the first iteration
+        cudaGraph_t g = top;
+        cudaGraphNode_t n = last;
+        if (k > 1) {
+            cudaGraph_t body[1] = {};
+            last = cond(top, last, hc[k - 1], 1, body);
+            g = body[0];
+            n = nullptr;
+        }
+        if (err != cudaSuccess) break;
+        n = child(g, n, energy[q]);
+        cudaGraph_t br[2] = {};
+        n = cond(g, n, hm[k], 2, br);
+        if (err != cudaSuccess) break;
+        if (cap >= 0) child(br[0], nullptr, mom_small_g[q]);
+        child(br[1], nullptr, mom_grid_g[q]);
+        // species and the convergence test, with the loop control of iteration k
+        const LoopCtl lc{k < maxit ? hc[k] : 0, k < maxit ? hm[k + 1] : 0, 1, k < maxit ? 1 : 0, maxit, cap};
+        if (q) swap_props<T>(I);
+        cudaGraph_t tail = capture([&] {
+            run_phase_impl<T>(ctx, I, AMCFD_PHASE_SPECIES);
+            launch_converge<T>(I, tol, lc);
+        });
+        if (q) swap_props<T>(I);
+        n = child(g, n, tail);
+        if (k == 1) last = n;
+    }
+    if (err == cudaSuccess) keep(cudaGraphInstantiate(&ge, top, 0));
+    for (cudaGraph_t g : parts)
+        if (g) cudaGraphDestroy(g);
+    if (top) cudaGraphDestroy(top);
+    if (err != cudaSuccess) {
+        cudaGetLastError();
+        ge = nullptr;
+        ctx->err = std::string("outer-loop graph: ") + cudaGetErrorString(err);
+        return AMCFD_E_CUDA;
+    }
+    return 0;
+}
+
+// Kernel launches of one outer iteration on the small-box or the grid momentum path.
+static long long iteration_launches(const amcfd_ctx *ctx, bool small)
+{
+    long long n = 0;
+    for (int ph = AMCFD_PHASE_ENERGY_ASSEMBLE; ph <= AMCFD_PHASE_CONVERGE; ++ph) n += phase_launches(ctx, ph, small);
+    return n + phase_launches(ctx, AMCFD_PHASE_SPECIES, small);
+}
+
+template <typename T>
+static int outer_loop_graph(amcfd_ctx *ctx, Inst<T> &I)
+{
+    const int par = (const void *)I.g.diff_cur == ctx->diff_a ? 0 : 1;
+    cudaGraphExec_t &ge = ctx->gloop[par];
+    int rc;
+    if (!ge && (rc = build_loop_graph<T>(ctx, I, ge))) return rc;
+    CK(cudaGraphLaunch(ge, ctx->stream));
+    rc = read_status(ctx);
+    const Status *s = ctx->st_host;
+    const int n = s->lp_niter;
+    ctx->niter = n;
+    ctx->itertot += n;
+    ctx->launches += 1 + (long long)s->lp_small * iteration_launches(ctx, true) +
+                     (long long)(n - s->lp_small) * iteration_launches(ctx, false);
+    ctx->last_box = s->lp_box;
+    if (n & 1) swap_props<T>(I);
+    return rc;
+}
+
 // Timing slots of amcfd_last_timing (accumulated device ms while profiling):
 // 0 energy BC+assembly+block correction, 1 line factorisation, 2 energy line
 // sweeps, 3 H->T + melt pool, 4 momentum chain, 5 convergence, 6 laser,
@@ -832,6 +990,9 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
 {
     const int maxit = ctx->prm.maxit;
     int rc;
+    if (ctx->use_graphs && !ctx->events && !ctx->host_loop && ctx->niter == 0 && maxit >= 1 &&
+        maxit <= kMaxChain)
+        return outer_loop_graph<T>(ctx, I);
     while (ctx->niter < maxit) {
         ctx->niter++;
         ctx->itertot++;
@@ -989,6 +1150,7 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->precision = opts->precision;
         ctx->use_graphs = opts->use_graphs != 0;
         ctx->small_box = opts->no_small_box == 0;
+        ctx->host_loop = opts->host_loop != 0;
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");

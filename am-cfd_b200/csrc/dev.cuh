@@ -51,6 +51,10 @@ struct Params {
 struct Status {
     // per step
     double timet, delt, beamposx, beamposy, scanvel;
+    // device-driven outer loop: iterations run in this step, momentum-box cells of
+    // the last one (-1: none yet), momentum path of the current one (1: small box)
+    // and iterations that took the small-box path
+    int lp_niter, lp_box, lp_mode, lp_small;
     int powerindicator, istart, jstart, heat_iter;
     double heatinlaser;
     // current volumetric-source parameters (advanced per outer iteration)
@@ -70,6 +74,15 @@ struct Status {
     int nonfinite;     // a reduction produced NaN/Inf
     unsigned long long seq_energy, done_energy, ticket_energy;
     unsigned long long seq_mom, done_mom, ticket_mom;
+};
+
+// Outer-loop control of a step captured as one CUDA graph (a chain of
+// conditional nodes): the convergence kernel of iteration k sets whether
+// iteration k+1 runs and which momentum path it takes.  active = 0 outside such
+// a graph; has_next = 0 for the last iteration of the chain.
+struct LoopCtl {
+    cudaGraphConditionalHandle cont, mode_next;
+    int active, has_next, maxit, cap;  // cap: small-box capacity in cells, -1 when disabled
 };
 
 // Fixed-size reduction slots written per CTA and reduced in a fixed order.

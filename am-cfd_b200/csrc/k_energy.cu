@@ -636,7 +636,8 @@ __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, c
 template <typename T>
 __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, int nb_h2t,
                                 const double *red_bc, int nb_bc, const double *red_las, int nb_las,
-                                const double *red_mom, int nb_mom, double tol, int check_finite)
+                                const double *red_mom, int nb_mom, double tol, int check_finite,
+                                LoopCtl lc)
 {
     __shared__ double scratch[40];
     Status *st = gd.st;
@@ -674,8 +675,37 @@ __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, i
         st->converged = conv;
         if (check_finite && (!isfinite(st->tpeak) || !isfinite(ratio) || !isfinite(st->resorh)))
             st->nonfinite = 1;
+        if (lc.active) {
+            // the host loop's bookkeeping: count the iteration, remember its box, and
+            // continue unless converged, failed or out of iterations
+            const int it = st->lp_niter + 1;
+            st->lp_niter = it;
+            st->lp_small += st->lp_mode;
+            const int box = st->momentum_active ? st->box_cells : 0;
+            st->lp_box = box;
+            const int mode = lc.cap >= 0 && box <= lc.cap;
+            st->lp_mode = mode;
+            const int cont = !conv && !st->nonfinite && !*(volatile int *)&st->error && it < lc.maxit;
+            if (lc.has_next) {
+                cudaGraphSetConditional(lc.mode_next, (unsigned)mode);
+                cudaGraphSetConditional(lc.cont, (unsigned)cont);
+            }
+        }
     }
     (void)red_mom; (void)nb_mom;
+}
+
+// Head of a step captured as one graph: the momentum path of its first outer
+// iteration, from the box of the last iteration before it.
+__global__ void loop_init_kernel(Status *st, LoopCtl lc)
+{
+    const int mode = lc.cap >= 0 && st->lp_box >= 0 && st->lp_box <= lc.cap;
+    st->lp_mode = mode;
+    cudaGraphSetConditional(lc.mode_next, (unsigned)mode);
+}
+void launch_loop_init(Status *st, const LoopCtl &lc, cudaStream_t s)
+{
+    loop_init_kernel<<<1, 1, 0, s>>>(st, lc);
 }
 
 // ---------------------------------------------------------------------------
@@ -791,11 +821,11 @@ template <typename T> void launch_meltpool(Inst<T> &I)
     size_t smem = 3 * (size_t)I.p.nip * sizeof(double) + (size_t)I.p.nip * sizeof(int);
     meltpool_kernel<T><<<1, 1024, smem, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t);
 }
-template <typename T> void launch_converge(Inst<T> &I, double tol)
+template <typename T> void launch_converge(Inst<T> &I, double tol, const LoopCtl &lc)
 {
     converge_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t, I.red_bc, I.nb_bc,
                                                   I.red_las, I.nb_las, I.red_mom, I.nb_mom, tol,
-                                                  I.check_finite);
+                                                  I.check_finite, lc);
 }
 template <typename T> void launch_update_solutions(Inst<T> &I)
 {
@@ -811,7 +841,7 @@ template <typename T> void launch_update_solutions(Inst<T> &I)
     template void launch_pack_field<T>(const T *, double *, int, int, long long, int, cudaStream_t); \
     template void launch_centre_velocity<T>(Inst<T> &, int, double *);                                \
     template void launch_meltpool<T>(Inst<T> &);            \
-    template void launch_converge<T>(Inst<T> &, double);    \
+    template void launch_converge<T>(Inst<T> &, double, const LoopCtl &); \
     template void launch_update_solutions<T>(Inst<T> &);
 AMCFD_INST(double)
 AMCFD_INST(float)

@@ -103,7 +103,8 @@ template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T
 template <typename T> void launch_block_correct(Inst<T> &I, int ivar = 5);
 template <typename T> void launch_h2t(Inst<T> &I);
 template <typename T> void launch_meltpool(Inst<T> &I);
-template <typename T> void launch_converge(Inst<T> &I, double tol);
+template <typename T> void launch_converge(Inst<T> &I, double tol, const LoopCtl &lc = LoopCtl{});
+void launch_loop_init(Status *st, const LoopCtl &lc, cudaStream_t s);
 template <typename T> void launch_update_solutions(Inst<T> &I);
 // line solvers (k_linesolve.cu)
 template <typename T> void launch_energy_factor(Inst<T> &I);

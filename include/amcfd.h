@@ -145,7 +145,10 @@ typedef struct amcfd_options {
     int check_finite;    /* fail with AMCFD_E_NONFINITE when a reduction is not finite */
     int no_small_box;    /* 1: never run the momentum chain of a small melt-pool box in one
                             CTA (red-black order only; 0 lets the solver choose) */
-    int reserved[7];
+    int host_loop;       /* 1: with use_graphs, still launch one graph per outer iteration and
+                            test convergence on the host (0: one graph per step, the
+                            iterations chained on the device) */
+    int reserved[6];
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;

@@ -175,6 +175,35 @@ def test_graph_replay_bit_identical(prec, order, deckdir):
     b.close()
 
 
+@pytest.mark.parametrize("prec,order", [(0, 0), (0, 1), (1, 1)])
+def test_device_outer_loop_matches_host_loop(prec, order, deckdir):
+    """A step launched as one graph (outer iterations chained by conditional
+    nodes, convergence tested on the device) gives the same bits and iteration
+    counts as one graph per outer iteration with the test on the host, and the
+    same launches plus the chain's head kernel once a step.  The deck converges
+    before maxit in some steps and not in others (odd and even counts, so the
+    property parity of later steps differs), and its melt-pool box is small
+    enough for the one-CTA momentum path."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.small("devloop", steps=8, maxit=11, power=60.0, toolpath=True).write(deckdir))
+    a = amcfd.Solver(d, order=order, precision=prec, use_graphs=1, host_loop=1)
+    b = amcfd.Solver(d, order=order, precision=prec, use_graphs=1, host_loop=0)
+    counts = []
+    for s in range(8):
+        ra, rb = a.step(), b.step()
+        for k in ("niter", "itertot", "tpeak", "alen", "depth", "width", "resorh", "resorm", "ratio",
+                  "momentum_cells"):
+            assert ra[k] == rb[k], (s, k, ra[k], rb[k])
+        for f in FIELDS:
+            assert np.array_equal(a.get(f), b.get(f)), (s, f)
+        counts.append(rb["niter"])
+    assert b.launches == a.launches + 8
+    assert min(counts) < 11 and {c % 2 for c in counts} == {0, 1}, counts
+    a.close()
+    b.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_small_box_momentum_matches_grid_path(prec, deckdir):
     """Red-black runs with the one-CTA momentum chain (small melt-pool box held
