@@ -584,6 +584,118 @@ __device__ __forceinline__ double cta_max(double v, double *sh)
     return r;
 }
 
+// The four sweeps of an FP32 box held in shared memory whose lines are short (at
+// most 3 cells a lane in groups of 8 lanes) and few enough for one line a group
+// per colour: each lane keeps its cells' coefficients (at ab an as su) and
+// factorisation (cf id pr) of both colours in registers across the sweeps, so a
+// pass reads only the neighbour values of phi.  The recurrences and their order
+// of operations are those of the shared-memory path below.
+constexpr int kShortG = 8, kShortL = 3;
+template <typename T>
+__device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, int NK, const T *sm, int ncell,
+                                                 T *ph0, int HI, int HJ)
+{
+    constexpr int G = kShortG, LM = kShortL;
+    const unsigned full = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int sub = lane & (G - 1), gid = warp * (32 / G) + lane / G;
+    const int L = (NI + G - 1) / G;
+    const int a = min(sub * L, NI), n = min(a + L, NI) - a;  // this lane's cells a .. a+n-1
+    const int half = (NJ + 1) / 2, nline = half * NK, HIJ = HI * HJ;
+    T rat[2][LM], rab[2][LM], ran[2][LM], ras[2][LM], rsu[2][LM], rpr[2][LM], rcf[2][LM], rid[2][LM];
+    int oh[2];
+    bool act[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        int kk = 0, jj = 0;
+        bool ac = gid < nline;
+        if (ac) {
+            kk = gid / half;
+            const int r = gid - kk * half, k = b.k0 + kk;
+            jj = ((c - k - b.j0) % 2 + 2) % 2 + 2 * r;
+            ac = jj < NJ;
+        }
+        act[c] = ac;
+        oh[c] = jj * HI + kk * HIJ;
+        const int o = a + jj * NI + kk * NI * NJ;
+#pragma unroll
+        for (int v = 0; v < LM; ++v) {
+            const bool in = ac && v < n;
+            rat[c][v] = in ? sm[o + v] : T(0);
+            rab[c][v] = in ? sm[ncell + o + v] : T(0);
+            ran[c][v] = in ? sm[2 * ncell + o + v] : T(0);
+            ras[c][v] = in ? sm[3 * ncell + o + v] : T(0);
+            rsu[c][v] = in ? sm[4 * ncell + o + v] : T(0);
+            rpr[c][v] = in ? sm[5 * ncell + o + v] : T(0);
+            rcf[c][v] = in ? sm[6 * ncell + o + v] : T(0);
+            rid[c][v] = in ? sm[7 * ncell + o + v] : T(0);
+        }
+    }
+    for (int sweep = 0; sweep < 4; ++sweep) {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int h = oh[c] + a;
+            T qv[LM];
+            T A = T(1), B = T(0);
+#pragma unroll
+            for (int v = 0; v < LM; ++v) {
+                qv[v] = T(0);
+                if (act[c] && v < n) {
+                    const T d = rat[c][v] * ph0[h + v + HIJ] + rab[c][v] * ph0[h + v - HIJ] +
+                                ran[c][v] * ph0[h + v + HI] + ras[c][v] * ph0[h + v - HI] + rsu[c][v];
+                    const T ev = d * rid[c][v], cc = rcf[c][v];
+                    qv[v] = ev;
+                    B = cc * B + ev;
+                    A = cc * A;
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) {
+                const T A2 = __shfl_up_sync(full, A, o, G), B2 = __shfl_up_sync(full, B, o, G);
+                if (sub >= o) { B = A * B2 + B; A = A * A2; }
+            }
+            T Ae = __shfl_up_sync(full, A, 1, G), Be = __shfl_up_sync(full, B, 1, G);
+            if (sub == 0) { Ae = T(1); Be = T(0); }
+            A = T(1);
+            B = T(0);
+            if (act[c]) {
+                T q = Ae * ph0[oh[c] - 1] + Be;
+#pragma unroll
+                for (int v = 0; v < LM; ++v)
+                    if (v < n) {
+                        q = rcf[c][v] * q + qv[v];
+                        qv[v] = q;
+                    }
+#pragma unroll
+                for (int v = LM - 1; v >= 0; --v)
+                    if (v < n) {
+                        const T pv = rpr[c][v];
+                        B = pv * B + qv[v];
+                        A = pv * A;
+                    }
+            }
+#pragma unroll
+            for (int o = 1; o < G; o <<= 1) {
+                const T A2 = __shfl_down_sync(full, A, o, G), B2 = __shfl_down_sync(full, B, o, G);
+                if (sub + o < G) { B = A * B2 + B; A = A * A2; }
+            }
+            Ae = __shfl_down_sync(full, A, 1, G);
+            Be = __shfl_down_sync(full, B, 1, G);
+            if (sub == G - 1) { Ae = T(1); Be = T(0); }
+            if (act[c]) {
+                T x = Ae * ph0[oh[c] + NI] + Be;
+#pragma unroll
+                for (int v = LM - 1; v >= 0; --v)
+                    if (v < n) {
+                        x = rpr[c][v] * x + qv[v];
+                        ph0[h + v] = x;
+                    }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 template <typename T>
 __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &b, T *phi, T *sm,
                                 int smem_elems, T *scratch)
@@ -609,18 +721,46 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
         cf = {q0 + 6ll * ncell, cj, ck}; id = {q0 + 7ll * ncell, cj, ck};
         qr = {q0 + 8ll * ncell, cj, ck};
         ph = {q0 + 9ll * ncell + 1 + HI + (long long)HI * HJ, HI, (long long)HI * HJ};
-        for (int q = tid; q < ncell; q += nth) {
-            const int ii = q % NI, r = q / NI, jj = r % NJ, kk = r / NJ;
-            const size_t c = g0 + ii + (size_t)jj * gsj + (size_t)kk * gsk;
-            at(ii, jj, kk) = g.at[c]; ab(ii, jj, kk) = g.ab[c];
-            an(ii, jj, kk) = g.an[c]; as(ii, jj, kk) = g.as[c];
-            su(ii, jj, kk) = g.su[c];
-            pr(ii, jj, kk) = g.ae[c]; cf(ii, jj, kk) = g.aw[c]; id(ii, jj, kk) = g.ap[c];
+        // every load of a batch is issued before its shared-memory stores; the
+        // arrays at ab an as su pr(=ae) cf(=aw) id(=ap) follow one another, cell
+        // (ii, jj, kk) at q = ii + NI (jj + NJ kk), and the halo of phi after them
+        constexpr int kBc = 2, kBh = 4;
+        for (int q0 = tid; q0 < ncell; q0 += kBc * nth) {
+            T v[kBc][8];
+#pragma unroll
+            for (int u = 0; u < kBc; ++u) {
+                const int q = q0 + u * nth;
+                if (q < ncell) {
+                    const int ii = q % NI, r = q / NI, jj = r % NJ, kk = r / NJ;
+                    const size_t c = g0 + ii + (size_t)jj * gsj + (size_t)kk * gsk;
+                    v[u][0] = g.at[c]; v[u][1] = g.ab[c]; v[u][2] = g.an[c]; v[u][3] = g.as[c];
+                    v[u][4] = g.su[c]; v[u][5] = g.ae[c]; v[u][6] = g.aw[c]; v[u][7] = g.ap[c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kBc; ++u) {
+                const int q = q0 + u * nth;
+                if (q < ncell) {
+#pragma unroll
+                    for (int f = 0; f < 8; ++f) sm[(size_t)f * ncell + q] = v[u][f];
+                }
+            }
         }
-        for (int q = tid; q < nhalo; q += nth) {
-            const int ii = q % HI, r = q / HI, jj = r % HJ, kk = r / HJ;
-            ph(ii - 1, jj - 1, kk - 1) =
-                phi[(long long)g0 + (ii - 1) + (long long)(jj - 1) * gsj + (kk - 1) * gsk];
+        for (int q0 = tid; q0 < nhalo; q0 += kBh * nth) {
+            T v[kBh];
+#pragma unroll
+            for (int u = 0; u < kBh; ++u) {
+                const int q = q0 + u * nth;
+                if (q < nhalo) {
+                    const int ii = q % HI, r = q / HI, jj = r % HJ, kk = r / HJ;
+                    v[u] = phi[(long long)g0 + (ii - 1) + (long long)(jj - 1) * gsj + (kk - 1) * gsk];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kBh; ++u) {
+                const int q = q0 + u * nth;
+                if (q < nhalo) sm[9ll * ncell + q] = v[u];
+            }
         }
         ae_src = nullptr; aw_src = nullptr; ap_src = nullptr;
         __syncthreads();
@@ -659,7 +799,13 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     // recurrences over per-line base pointers.  Long lines: one warp per line,
     // warp scans of affine maps over per-lane chunks.
     const int half = (NJ + 1) / 2;
-    if (NI <= 48) {
+    // (FP64 registers for both colours would spill: FP64 keeps the shared-memory path)
+    bool regs = false;
+    if constexpr (sizeof(T) == 4)
+        regs = fits && NI <= kShortG * kShortL && half * NK <= (nth >> 5) * (32 / kShortG);
+    if (regs) {
+        if constexpr (sizeof(T) == 4) sweep_short_regs<T>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ);
+    } else if (NI <= 48) {
         // Short lines (the usual melt-pool box): a group of G lanes per line, each
         // lane a chunk of at most 6 cells, chained by segmented shuffle scans of
         // the affine maps (x -> cf x + e forward, x -> pr x + qr backward).  The
@@ -902,18 +1048,21 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
     const int nb = I.nb_mom;
     const size_t region = (size_t)nb * R_NSLOTS;
     if (small) {
-        // assembly on the whole GPU, everything latency-bound in one CTA between
+        // assemblies over a grid sized for the box capacity (one cell a thread),
+        // everything latency-bound in one CTA between them
         const int se = (int)(I.mom_small_smem / sizeof(T));
-        double *red_umax = I.red_mom + 4 * region;
+        const int nbs = std::max(1, std::min(nb, (mom_small_capacity<T>(I) + 255) / 256));
+        const size_t rs = (size_t)nbs * R_NSLOTS;
+        double *red_umax = I.red_mom + 4 * rs;
         mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax);
         for (int ivar = 1; ivar <= 3; ++ivar) {
-            mom_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * region);
+            mom_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * rs);
             mom_small_mid_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
                 I.p, I.g, ivar, I.mom_scratch, se, red_umax);
         }
-        pp_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * region);
+        pp_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * rs);
         mom_small_post_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
-            I.p, I.g, I.mom_scratch, se, I.red_mom, nb);
+            I.p, I.g, I.mom_scratch, se, I.red_mom, nbs);
         return;
     }
     launch_box_tickets<T>(I);
