@@ -753,13 +753,13 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     switch (phase) {
     case AMCFD_PHASE_LASER: return 1;
     case AMCFD_PHASE_ENERGY_ASSEMBLE: return 3;
-    case AMCFD_PHASE_ENERGY_SOLVE: return 1 + sweeps;
+    case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : sweeps;
     case AMCFD_PHASE_H2T: return 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
     case AMCFD_PHASE_MOMENTUM: return small ? 9 : 2 + 4 * (3 + sweeps) + 2 + 1;
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;
-    case AMCFD_PHASE_SPECIES: return ctx->prm.species ? 4 + sweeps : 0;
+    case AMCFD_PHASE_SPECIES: return ctx->prm.species ? (ctx->order == AMCFD_ORDER_EXACT ? 4 : 3) + sweeps : 0;
     default: return 0;
     }
 }

@@ -416,9 +416,20 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 // phi_n, phi_s lie on lines of the other colour, which this launch does not
 // write; vectors past the end of the padded row read its first vector and are
 // masked.
+// FACTOR (the first pass of each colour): the line's factorisation is formed in
+// the same rounds from ap, aw, ae, exactly as factor_rounds_kernel forms it, and
+// stored for the later passes.  With `correct` (the first colour's first pass)
+// the block correction phi += delphi, which the factorisation kernel would have
+// stored into every interior line, is added to the neighbour values read from
+// interior lines instead: each line's own values are overwritten by its pass,
+// and the second colour reads the first colour's lines only after that.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color)
+__device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d);
+
+template <typename T, bool FACTOR>
+__global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
+                                                              int correct)
 {
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int RC = 32 * V;
@@ -444,13 +455,85 @@ __global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T
         if (j > j1) continue;  // warp-uniform
         const size_t row = cidx(0, j, k, nj, nip);
         T carry = phi[row + i0 - 1];
+        T carry_pr = T(0);  // FACTOR: pr at cell i0 - 1
+        // FACTOR: which neighbour lines are interior (block-corrected)
+        const bool ct = correct && k + 1 <= k1, cb = correct && k - 1 >= k0, cn = correct && j + 1 <= j1,
+                   cs = correct && j - 1 >= j0;
         for (int m = 0; m < R; ++m) {
             const int base = ib + RC * m + V * lane;
-            const size_t c = row + (base + V <= nip ? base : 0);
+            const bool inrow = base + V <= nip;
+            const size_t c = row + (inrow ? base : 0);
             T vt[V], vb[V], vn[V], vs[V], wt[V], wb[V], wn[V], ws[V], wu[V], wc[V], wi[V], wp[V];
             ld16(phi + c + sk, vt); ld16(phi + c - sk, vb); ld16(phi + c + sj, vn); ld16(phi + c - sj, vs);
             ld16(g.at + c, wt); ld16(g.ab + c, wb); ld16(g.an + c, wn); ld16(g.as + c, ws);
-            ld16(g.su + c, wu); ld16(g.cf + c, wc); ld16(g.iden + c, wi); ld16(g.pr + c, wp);
+            ld16(g.su + c, wu);
+            if constexpr (FACTOR) {
+                // wc, wi, wp receive aw, ap, ae, then cf, iden, pr
+                ld16(g.aw + c, wc); ld16(g.ap + c, wi); ld16(g.ae + c, wp);
+                T m00 = T(1), m01 = T(0), m10 = T(0), m11 = T(1);
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    if (base + v >= i0 && base + v <= i1) {  // [[0, ae], [-aw, ap]] * M
+                        const T n00 = wp[v] * m10, n01 = wp[v] * m11;
+                        const T n10 = -wc[v] * m00 + wi[v] * m10, n11 = -wc[v] * m01 + wi[v] * m11;
+                        m00 = n00; m01 = n01; m10 = n10; m11 = n11;
+                    }
+                }
+                mat_rescale(m00, m01, m10, m11);
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const T b00 = __shfl_up_sync(full, m00, o), b01 = __shfl_up_sync(full, m01, o);
+                    const T b10 = __shfl_up_sync(full, m10, o), b11 = __shfl_up_sync(full, m11, o);
+                    if (lane >= o) {  // own * lower
+                        const T n00 = m00 * b00 + m01 * b10, n01 = m00 * b01 + m01 * b11;
+                        const T n10 = m10 * b00 + m11 * b10, n11 = m10 * b01 + m11 * b11;
+                        m00 = n00; m01 = n01; m10 = n10; m11 = n11;
+                        mat_rescale(m00, m01, m10, m11);
+                    }
+                }
+                const T e00 = __shfl_up_sync(full, m00, 1), e01 = __shfl_up_sync(full, m01, 1);
+                const T e10 = __shfl_up_sync(full, m10, 1), e11 = __shfl_up_sync(full, m11, 1);
+                T x = carry_pr;
+                if (lane > 0) x = (e00 * carry_pr + e01) / (e10 * carry_pr + e11);
+                T fpr[V], fcf[V], fid[V];
+                bool all = true;
+#pragma unroll
+                for (int v = 0; v < V; ++v) {
+                    const bool ok = base + v >= i0 && base + v <= i1;
+                    all = all && ok;
+                    if (ok) {
+                        const T den = wi[v] - wc[v] * x;
+                        const T idv = T(1) / den;
+                        fpr[v] = wp[v] * idv;
+                        fcf[v] = wc[v] * idv;
+                        fid[v] = idv;
+                        x = fpr[v];
+                        const T dl = (T)g.delphi[base + v];
+                        if (ct) vt[v] = vt[v] + dl;
+                        if (cb) vb[v] = vb[v] + dl;
+                        if (cn) vn[v] = vn[v] + dl;
+                        if (cs) vs[v] = vs[v] + dl;
+                    } else {
+                        fpr[v] = fcf[v] = fid[v] = T(0);
+                    }
+                    wp[v] = fpr[v]; wc[v] = fcf[v]; wi[v] = fid[v];
+                }
+                carry_pr = __shfl_sync(full, x, 31);
+                if (all) {
+                    typename Vec16<T>::type w;
+                    memcpy(&w, fpr, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.pr + c) = w;
+                    memcpy(&w, fcf, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.cf + c) = w;
+                    memcpy(&w, fid, 16); *reinterpret_cast<typename Vec16<T>::type *>(g.iden + c) = w;
+                } else if (inrow) {
+#pragma unroll
+                    for (int v = 0; v < V; ++v)
+                        if (base + v >= i0 && base + v <= i1) {
+                            g.pr[c + v] = fpr[v]; g.cf[c + v] = fcf[v]; g.iden[c + v] = fid[v];
+                        }
+                }
+            } else {
+                ld16(g.cf + c, wc); ld16(g.iden + c, wi); ld16(g.pr + c, wp);
+            }
             T a[V], e[V];
             T Al = T(1), Bl = T(0);
 #pragma unroll
@@ -713,8 +796,11 @@ __global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *ticke
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// Red-black order forms the factorisation inside the first sweep of each colour
+// (sweep_rb_rounds_kernel<T, true>), so this launch is the exact order's only.
 template <typename T> void launch_phi_factor(Inst<T> &I, T *phi)
 {
+    if (I.order != AMCFD_ORDER_EXACT) return;
     const int lines = (I.p.nj - 2) * (I.p.nk - 2);
     factor_rounds_kernel<T><<<std::max(1, (lines + 3) / 4), 128, 0, I.stream>>>(I.p, I.g, phi);
 }
@@ -749,9 +835,11 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
         const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
         const int grid = std::max(1, (lines + 3) / 4);
         const size_t rs = rounds_smem<T>(I.p, 4);
-        for (int sweep = 0; sweep < 4; ++sweep)
+        for (int color = 0; color < 2; ++color)
+            sweep_rb_rounds_kernel<T, true><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color, color == 0);
+        for (int sweep = 1; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color)
-                sweep_rb_rounds_kernel<T><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color);
+                sweep_rb_rounds_kernel<T, false><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color, 0);
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
@@ -787,7 +875,9 @@ template <typename T> bool set_rounds_smem_limit(const Params &p)
 {
     const size_t need = rounds_smem<T>(p, 4);
     if (need > 200 * 1024) return false;
-    return cudaFuncSetAttribute(sweep_rb_rounds_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)need) == cudaSuccess &&
+           cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)need) == cudaSuccess;
 }
 

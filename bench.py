@@ -36,7 +36,10 @@ sys.path[:0] = [os.path.join(ROOT, "am-cfd_b200"), os.path.join(ROOT, "oracle")]
 METRIC = "sim-ms/wall-s"
 # Algorithmic words per interior cell per outer iteration, by kernel family
 # (energy path; the contract total is 92 words per cell per outer iteration).
+# In red-black order the line factorisation runs inside the first sweep of each
+# colour, so its 2 words belong to the sweep family.
 WORDS = {"energy_assemble": 40, "factor": 2, "energy_sweeps": 40, "h2t_meltpool": 10}
+WORDS_REDBLACK = {"energy_assemble": 40, "factor": 0, "energy_sweeps": 42, "h2t_meltpool": 10}
 # DRAM bytes per interior cell per launch (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum, one capture of each kernel on the 400x200x100 deck,
 # FP32 bulk); the line reports them scaled by the cell count.
@@ -275,11 +278,12 @@ def main():
     # roofline of the dominant kernel family
     peak, peak_kind = _peaks()
     w = 4 if prec == amcfd.PREC_FP32 else 8
-    fam = max(WORDS, key=lambda k: prof[k])
+    words = WORDS_REDBLACK if args.order == "redblack" else WORDS
+    fam = max(words, key=lambda k: prof[k])
     # the sweep family is 8 (red-black) or 1 (exact order) launches per iteration
     nlaunch = prof["sweep_launches"] if fam == "energy_sweeps" else iters
     avg_ms = prof[fam] / max(nlaunch, 1)
-    alg_bytes = WORDS[fam] * ncell * w * iters / max(nlaunch, 1)
+    alg_bytes = words[fam] * ncell * w * iters / max(nlaunch, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
     tr = TRAFFIC_PER_CELL.get(f"{fam}:{args.precision}:{args.order}")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
