@@ -118,6 +118,8 @@ def lib() -> C.CDLL:
             L.amcfd_last_error.restype = C.c_char_p
             L.amcfd_step.argtypes = [VP, P(AmcfdReport)]
             L.amcfd_get_field.argtypes = [VP, C.c_char_p, P(_D)]
+            L.amcfd_get_field_async.argtypes = [VP, C.c_char_p, P(_D)]
+            L.amcfd_wait_reads.argtypes = [VP]
             L.amcfd_set_field.argtypes = [VP, C.c_char_p, P(_D)]
             L.amcfd_get_grid.argtypes = [VP, C.c_char_p, P(_D)]
             L.amcfd_dims.argtypes = [VP, P(_I), P(_I), P(_I)]
@@ -371,6 +373,15 @@ class Solver:
     def get_into(self, name: str, ptr: int):
         """Copy a field into caller memory at address `ptr` (ni*nj*nk doubles)."""
         self._check(lib().amcfd_get_field(self._h, name.encode(), C.cast(ptr, C.POINTER(_D))))
+
+    def get_into_async(self, name: str, ptr: int):
+        """Queue the copy of a field into caller memory at `ptr` (ni*nj*nk doubles,
+        pinned for overlap) and return; the memory holds the field after wait_reads()."""
+        self._check(lib().amcfd_get_field_async(self._h, name.encode(), C.cast(ptr, C.POINTER(_D))))
+
+    def wait_reads(self):
+        """Block until the last get_into_async copy has landed."""
+        self._check(lib().amcfd_wait_reads(self._h))
 
     def ws_attach(self, net: Optional["Net"], mode: int):
         """Attach the warm-start network (WS_OFF, WS_PREDICT, WS_RECORD)."""

@@ -118,6 +118,10 @@ struct amcfd_ctx {
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
     double *pack = nullptr;        // FP64 read-out staging (ni*nj*nk), made on first use
+    // asynchronous read-out: the staging is copied to the host on its own stream
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_packed = nullptr, ev_copied = nullptr;
+    bool copy_pending = false;     // a copy out of the staging may still be running
     int sm_count = 0;
     // learned warm start (amcfd_ws_attach)
     amcfd_net *net = nullptr;
@@ -1226,6 +1230,7 @@ void amcfd_destroy(amcfd_ctx *ctx)
 {
     if (!ctx) return;
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->st_dev) cudaFree(ctx->st_dev);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
@@ -1237,6 +1242,9 @@ void amcfd_destroy(amcfd_ctx *ctx)
     drop_graphs(ctx);
     for (int q = 0; q < 16; q++)
         if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
+    if (ctx->ev_packed) cudaEventDestroy(ctx->ev_packed);
+    if (ctx->ev_copied) cudaEventDestroy(ctx->ev_copied);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1515,7 +1523,9 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr)
     return fail(ctx, AMCFD_E_ARG, std::string("unknown field ") + name);
 }
 
-int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
+// Field read-out through the FP64 staging buffer; with `async` the copy to the
+// host runs on the copy stream and the call returns once it is queued.
+static int get_field_impl(amcfd_ctx *ctx, const char *name, double *host_out, bool async)
 {
     if (!ctx || !name || !host_out) return AMCFD_E_ARG;
     void *d = nullptr;
@@ -1530,6 +1540,8 @@ int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
         CK(cudaMalloc(&ctx->pack, bytes));
         CK(cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device));
     }
+    // the staging may still be read by an asynchronous copy
+    if (ctx->copy_pending) CK(cudaStreamWaitEvent(ctx->stream, ctx->ev_copied, 0));
     // widen and pack on the device, then one contiguous copy (full speed into pinned memory)
     if (centre >= 0) {
         if (ctx->precision == AMCFD_PREC_FP64)
@@ -1543,8 +1555,43 @@ int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
         launch_pack_field<float>((const float *)d, ctx->pack, ctx->ni, ctx->nip, rows, ctx->sm_count,
                                  ctx->stream);
     CK(cudaGetLastError());
+    if (async) {
+        if (!ctx->copy_stream) {
+            CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+            CK(cudaEventCreateWithFlags(&ctx->ev_packed, cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->ev_copied, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(ctx->ev_packed, ctx->stream));
+        CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_packed, 0));
+        CK(cudaMemcpyAsync(host_out, ctx->pack, bytes, cudaMemcpyDeviceToHost, ctx->copy_stream));
+        CK(cudaEventRecord(ctx->ev_copied, ctx->copy_stream));
+        ctx->copy_pending = true;
+        return 0;
+    }
     CK(cudaMemcpyAsync(host_out, ctx->pack, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    ctx->copy_pending = false;  // the stream waited for it
+    return 0;
+}
+
+int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out)
+{
+    return get_field_impl(ctx, name, host_out, false);
+}
+
+int amcfd_get_field_async(amcfd_ctx *ctx, const char *name, double *host_out)
+{
+    return get_field_impl(ctx, name, host_out, true);
+}
+
+int amcfd_wait_reads(amcfd_ctx *ctx)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    if (!ctx->copy_pending) return 0;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaEventSynchronize(ctx->ev_copied));
+    CK(cudaGetLastError());
+    ctx->copy_pending = false;
     return 0;
 }
 

@@ -267,7 +267,7 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
 // heat accumulation and volumetric heat input.  H->T is evaluated in FP64.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256, 3) h2t_kernel(Params p, Fields<T> g, double *red)
+__global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, double *red)
 {
     const Status *st = g.st;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;

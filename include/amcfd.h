@@ -191,6 +191,15 @@ int amcfd_step(amcfd_ctx *ctx, amcfd_step_report *report);
  * cover the whole grid (every powder layer, active or not). 
  * host buffers hold ni*nj*nk doubles in [k][j][i] order (i fastest). */
 int amcfd_get_field(amcfd_ctx *ctx, const char *name, double *host_out);
+/* amcfd_get_field that returns as soon as the copy is queued (no counterpart in the
+ * reference, whose writers read host arrays in place).  The field is packed on the
+ * solver's stream, so later steps may change it at once, and copied to host_out on a
+ * second stream while the caller goes on; with pinned host_out the copy overlaps the
+ * next step.  host_out must stay valid and is complete only after amcfd_wait_reads.
+ * Any later read of a field waits for the copy before it reuses the staging. */
+int amcfd_get_field_async(amcfd_ctx *ctx, const char *name, double *host_out);
+/* Blocks until the last amcfd_get_field_async copy has landed in host memory. */
+int amcfd_wait_reads(amcfd_ctx *ctx);
 int amcfd_set_field(amcfd_ctx *ctx, const char *name, const double *host_in);
 int amcfd_get_grid(amcfd_ctx *ctx, const char *name, double *host_out);
 int amcfd_dims(const amcfd_ctx *ctx, int *ni, int *nj, int *nk);
