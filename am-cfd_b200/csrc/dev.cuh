@@ -215,6 +215,44 @@ __device__ __forceinline__ void block_reduce_store(double (&v)[NV], const int (&
     (void)tid;
 }
 
+// N sums of per-CTA partials (item q: slot slot[q] of the nb entries at base[q]) in
+// one pass, each in the order of a one-slot reduction with one CTA: strided
+// partial sums per thread, a warp shuffle tree, then warp 0 over the warps' sums.
+// The loads of all items are in flight together.  scr holds N * 33 doubles.
+template <int N>
+__device__ void reduce_sums(const double *const (&base)[N], const int (&slot)[N], int nb, double (&out)[N],
+                            double *scr)
+{
+    double acc[N];
+#pragma unroll
+    for (int q = 0; q < N; ++q) acc[q] = 0.0;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) acc[q] = acc[q] + base[q][(size_t)b * R_NSLOTS + slot[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < N; ++q) acc[q] = warp_sum(acc[q]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) scr[q * 33 + warp] = acc[q];
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            double r = lane < nw ? scr[q * 33 + lane] : 0.0;
+            r = warp_sum(r);
+            if (lane == 0) scr[q * 33 + 32] = r;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < N; ++q) out[q] = scr[q * 33 + 32];
+    __syncthreads();
+}
+
 // One aligned 16-byte vector of a field (4 FP32 or 2 FP64 elements): the unit of
 // the coalesced row loads of the line-sweep, factorisation and H->T kernels.
 template <typename T> struct Vec16;

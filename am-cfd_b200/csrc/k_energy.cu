@@ -640,15 +640,14 @@ __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, i
                                 LoopCtl lc)
 {
     __shared__ double scratch[40];
+    __shared__ double scr8[8 * 33];
     Status *st = gd.st;
-    double accul = reduce_slot(red_h2t, nb_h2t, R_ACCUL, false, scratch);
-    double heatvol = reduce_slot(red_h2t, nb_h2t, R_HEATVOL, false, scratch);
-    double fw = reduce_slot(red_h2t, nb_h2t, R_FW, false, scratch);
-    double fe = reduce_slot(red_h2t, nb_h2t, R_FE, false, scratch);
-    double fb = reduce_slot(red_h2t, nb_h2t, R_FB, false, scratch);
-    double ft = reduce_slot(red_h2t, nb_h2t, R_FT, false, scratch);
-    double fs = reduce_slot(red_h2t, nb_h2t, R_FS, false, scratch);
-    double fn = reduce_slot(red_h2t, nb_h2t, R_FN, false, scratch);
+    const double *hb[8] = {red_h2t, red_h2t, red_h2t, red_h2t, red_h2t, red_h2t, red_h2t, red_h2t};
+    const int hs[8] = {R_ACCUL, R_HEATVOL, R_FW, R_FE, R_FB, R_FT, R_FS, R_FN};
+    double hv[8];
+    reduce_sums<8>(hb, hs, nb_h2t, hv, scr8);
+    const double accul = hv[0], heatvol = hv[1], fw = hv[2], fe = hv[3], fb = hv[4], ft = hv[5],
+                 fs = hv[6], fn = hv[7];
     double ahtop = reduce_slot(red_bc, nb_bc, R_AHTOP, false, scratch);
     double heatin = reduce_slot(red_las, nb_las, R_HEATIN, false, scratch);
     if (threadIdx.x == 0) {

@@ -515,11 +515,12 @@ __device__ void mom_finalize_body(const Params &p, Status *st, const double *red
                                   double *scratch)
 {
     const size_t region = (size_t)nb * R_NSLOTS;
-    double s1 = reduce_region(red + 0 * region, nb, R_MSUMD, false, scratch);
-    double s2 = reduce_region(red + 1 * region, nb, R_MSUMD, false, scratch);
-    double s3 = reduce_region(red + 2 * region, nb, R_MSUMD, false, scratch);
-    double rm = reduce_region(red + 3 * region, nb, R_MRESORM, false, scratch);
-    double dn = reduce_region(red + 3 * region, nb, R_MDENOM, false, scratch);
+    __shared__ double scr5[5 * 33];
+    const double *rb[5] = {red, red + region, red + 2 * region, red + 3 * region, red + 3 * region};
+    const int rs[5] = {R_MSUMD, R_MSUMD, R_MSUMD, R_MRESORM, R_MDENOM};
+    double sv[5];
+    reduce_sums<5>(rb, rs, nb, sv, scr5);
+    const double s1 = sv[0], s2 = sv[1], s3 = sv[2], rm = sv[3], dn = sv[4];
     double umax = reduce_region(red + 4 * region, nb_umax, R_UMAX, true, scratch);
     if (threadIdx.x == 0) mom_finalize_status(p, st, s1, s2, s3, rm, dn, umax);
 }
