@@ -118,6 +118,20 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
         tma_load_3d(dst + FB_FN * FE, &mp.flnot, x0, y0, q, &barB[s]);
     };
     constexpr int kNone = -(1 << 30);
+    // per-plane metrics of this segment, converted once for the CTA (the same
+    // values every thread would form)
+    __shared__ double pl_dz[kKSEG];
+    __shared__ T pl_m[4][kKSEG];  // fracz[k], fracz[k-1], dzpbinv[k], dzpbinv[k+1]
+    if (tid < ke - kb) {
+        const int k = kb + tid;
+        if (k >= 1 && k <= nkm2) {
+            pl_dz[tid] = g.zw[k + 1] - g.zw[k];
+            pl_m[0][tid] = (T)g.fracz[k];
+            pl_m[1][tid] = (T)g.fracz[k - 1];
+            pl_m[2][tid] = (T)g.dzpbinv[k];
+            pl_m[3][tid] = (T)g.dzpbinv[k + 1];
+        }
+    }
 
     if (tid == 0) {
         for (int s = 0; s < B::SA; ++s) { mbar_init(&barA[s]); lastA[s] = kNone; }
@@ -200,11 +214,12 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 g.vis_nxt[c] = vn;
             }
             if (colint && k >= 1 && k <= nkm2) {
-                const double dz = g.zw[k + 1] - g.zw[k];
+                const int kl = k - kb;
+                const double dz = pl_dz[kl];
                 const R aik = (R)(dx * dz), ajk = (R)(dy * dz);
                 const R vol = (R)(dx * dy * dz);
-                const R fz_k = (R)g.fracz[k], fz_m = (R)g.fracz[k - 1];
-                const R dzp_k = (R)g.dzpbinv[k], dzp_p = (R)g.dzpbinv[k + 1];
+                const R fz_k = pl_m[0][kl], fz_m = pl_m[1][kl];
+                const R dzp_k = pl_m[2][kl], dzp_p = pl_m[3][kl];
                 const R dcc = d_c, rhc = Ac[FA_R * FE];
                 const R d_e = Ac[FA_D * FE + 1], d_w = Ac[FA_D * FE - 1], d_nn = Ac[FA_D * FE + BX],
                         d_s = Ac[FA_D * FE - BX], d_m = Am[FA_D * FE], d_p = Ap[FA_D * FE];

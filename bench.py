@@ -271,6 +271,8 @@ def main():
     # Each step's field is packed on the device at once and copied to the host
     # while the next step computes; the clock stops after the last copy landed.
     host = torch.empty(ni * nj * nk, dtype=torch.float64, pin_memory=True)
+    s.get_into_async("temp", host.data_ptr())  # warm-up: the copy stream is made on first use
+    s.wait_reads()
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
