@@ -143,7 +143,7 @@ __host__ __device__ __forceinline__ size_t cidx(int i, int j, int k, int nj, int
 }
 
 // Division in the bulk precision: IEEE in FP64 (the parity build), the fast
-// approximate reciprocal form in FP32 (about 2 ulp; the FP32 build is judged
+// approximate reciprocal form in FP32 (about 2 ulp; the FP32 build is checked
 // against the FP64 oracle, not bit for bit).
 __device__ __forceinline__ double bdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float bdiv(float a, float b) { return __fdividef(a, b); }
