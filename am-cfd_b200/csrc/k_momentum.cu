@@ -585,16 +585,86 @@ __device__ __forceinline__ double cta_max(double v, double *sh)
     return r;
 }
 
-// The four sweeps of an FP32 box held in shared memory whose lines are short (at
-// most 3 cells a lane in groups of 8 lanes) and few enough for one line a group
-// per colour: each lane keeps its cells' coefficients (at ab an as su) and
-// factorisation (cf id pr) of both colours in registers across the sweeps, so a
-// pass reads only the neighbour values of phi.  The recurrences and their order
-// of operations are those of the shared-memory path below.
 constexpr int kShortG = 8, kShortL = 3;
+
+// One line of a box held in shared memory, solved by a group of G = 8 lanes: each
+// lane runs its chunk a..e-1, and segmented shuffle scans of the affine maps
+// chain the chunks (x -> cf x + e forward, x -> pr x + qr backward).  Every lane
+// of the warp calls it (shuffles take all 32 lanes); a group without a line
+// (act false) carries identity maps.
+struct BoxLine {
+    int NI, sub, a, e;
+};
 template <typename T>
+__device__ __forceinline__ void group_line_shared(const V3<T> &at, const V3<T> &ab, const V3<T> &an,
+                                                  const V3<T> &as, const V3<T> &su, const V3<T> &pr,
+                                                  const V3<T> &cf, const V3<T> &id, const V3<T> &qr,
+                                                  const V3<T> &ph, const BoxLine &bl, int jj, int kk, bool act)
+{
+    constexpr int G = kShortG;
+    const int NI = bl.NI, sub = bl.sub, a = bl.a, e = bl.e;
+        T A = T(1), B = T(0);
+        if (act)
+            for (int ii = a; ii < e; ++ii) {
+                const T d = at(ii, jj, kk) * ph(ii, jj, kk + 1) + ab(ii, jj, kk) * ph(ii, jj, kk - 1) +
+                            an(ii, jj, kk) * ph(ii, jj + 1, kk) + as(ii, jj, kk) * ph(ii, jj - 1, kk) +
+                            su(ii, jj, kk);
+                const T ev = d * id(ii, jj, kk), c = cf(ii, jj, kk);
+                qr(ii, jj, kk) = ev;
+                B = c * B + ev;
+                A = c * A;
+            }
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+            const T A2 = __shfl_up_sync(0xffffffffu, A, o, G), B2 = __shfl_up_sync(0xffffffffu, B, o, G);
+            if (sub >= o) { B = A * B2 + B; A = A * A2; }
+        }
+        T Ae = __shfl_up_sync(0xffffffffu, A, 1, G), Be = __shfl_up_sync(0xffffffffu, B, 1, G);
+        if (sub == 0) { Ae = T(1); Be = T(0); }
+        A = T(1);
+        B = T(0);
+        if (act) {
+            T q = Ae * ph(-1, jj, kk) + Be;
+            for (int ii = a; ii < e; ++ii) {
+                q = cf(ii, jj, kk) * q + qr(ii, jj, kk);
+                qr(ii, jj, kk) = q;
+            }
+            for (int ii = e - 1; ii >= a; --ii) {
+                const T pv = pr(ii, jj, kk);
+                B = pv * B + qr(ii, jj, kk);
+                A = pv * A;
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < G; o <<= 1) {
+            const T A2 = __shfl_down_sync(0xffffffffu, A, o, G), B2 = __shfl_down_sync(0xffffffffu, B, o, G);
+            if (sub + o < G) { B = A * B2 + B; A = A * A2; }
+        }
+        Ae = __shfl_down_sync(0xffffffffu, A, 1, G);
+        Be = __shfl_down_sync(0xffffffffu, B, 1, G);
+        if (sub == G - 1) { Ae = T(1); Be = T(0); }
+        if (act) {
+            T x = Ae * ph(NI, jj, kk) + Be;
+            for (int ii = e - 1; ii >= a; --ii) {
+                x = pr(ii, jj, kk) * x + qr(ii, jj, kk);
+                ph(ii, jj, kk) = x;
+            }
+        }
+}
+
+// The four sweeps of an FP32 box held in shared memory whose lines are short (at
+// most 3 cells a lane in groups of 8 lanes): each lane keeps its cells'
+// coefficients (at ab an as su) and factorisation (cf id pr) of its group's first
+// line of each colour in registers across the sweeps, so a pass reads only the
+// neighbour values of phi; a group's second line of a colour, where the box has
+// more lines than groups, is solved from shared memory (group_line_shared).  The
+// recurrences and their order of operations are those of the shared-memory path.
+template <typename T, bool TWO>  // TWO: some groups have a second line of a colour
 __device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, int NK, const T *sm, int ncell,
-                                                 T *ph0, int HI, int HJ)
+                                                 T *ph0, int HI, int HJ, const V3<T> &at, const V3<T> &ab,
+                                                 const V3<T> &an, const V3<T> &as, const V3<T> &su,
+                                                 const V3<T> &pr, const V3<T> &cf, const V3<T> &id,
+                                                 const V3<T> &qr, const V3<T> &ph)
 {
     constexpr int G = kShortG, LM = kShortL;
     const unsigned full = 0xffffffffu;
@@ -603,6 +673,7 @@ __device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, i
     const int L = (NI + G - 1) / G;
     const int a = min(sub * L, NI), n = min(a + L, NI) - a;  // this lane's cells a .. a+n-1
     const int half = (NJ + 1) / 2, nline = half * NK, HIJ = HI * HJ;
+    const int ngroups = (int)(blockDim.x >> 5) * (32 / G);
     T rat[2][LM], rab[2][LM], ran[2][LM], ras[2][LM], rsu[2][LM], rpr[2][LM], rcf[2][LM], rid[2][LM];
     int oh[2];
     bool act[2];
@@ -691,6 +762,19 @@ __device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, i
                         x = rpr[c][v] * x + qv[v];
                         ph0[h + v] = x;
                     }
+            }
+            if (TWO) {  // the CTA's groups all take part
+                const int l = gid + ngroups;
+                int kk = 0, jj = 0;
+                bool ac = l < nline;
+                if (ac) {
+                    kk = l / half;
+                    const int r = l - kk * half, k = b.k0 + kk;
+                    jj = ((c - k - b.j0) % 2 + 2) % 2 + 2 * r;
+                    ac = jj < NJ;
+                }
+                __syncwarp();
+                group_line_shared<T>(at, ab, an, as, su, pr, cf, id, qr, ph, BoxLine{NI, sub, a, a + n}, jj, kk, ac);
             }
             __syncthreads();
         }
@@ -803,9 +887,16 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     // (FP64 registers for both colours would spill: FP64 keeps the shared-memory path)
     bool regs = false;
     if constexpr (sizeof(T) == 4)
-        regs = fits && NI <= kShortG * kShortL && half * NK <= (nth >> 5) * (32 / kShortG);
+        regs = fits && NI <= kShortG * kShortL && half * NK <= 2 * (nth >> 5) * (32 / kShortG);
     if (regs) {
-        if constexpr (sizeof(T) == 4) sweep_short_regs<T>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ);
+        if constexpr (sizeof(T) == 4) {
+            if (half * NK <= (nth >> 5) * (32 / kShortG))
+                sweep_short_regs<T, false>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ, at, ab, an, as, su, pr,
+                                           cf, id, qr, ph);
+            else
+                sweep_short_regs<T, true>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ, at, ab, an, as, su, pr,
+                                          cf, id, qr, ph);
+        }
     } else if (NI <= 48) {
         // Short lines (the usual melt-pool box): a group of G lanes per line, each
         // lane a chunk of at most 6 cells, chained by segmented shuffle scans of
@@ -832,53 +923,7 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
                         jj = jpar + 2 * r;
                         act = jj < NJ;
                     }
-                    T A = T(1), B = T(0);
-                    if (act)
-                        for (int ii = a; ii < e; ++ii) {
-                            const T d = at(ii, jj, kk) * ph(ii, jj, kk + 1) + ab(ii, jj, kk) * ph(ii, jj, kk - 1) +
-                                        an(ii, jj, kk) * ph(ii, jj + 1, kk) + as(ii, jj, kk) * ph(ii, jj - 1, kk) +
-                                        su(ii, jj, kk);
-                            const T ev = d * id(ii, jj, kk), c = cf(ii, jj, kk);
-                            qr(ii, jj, kk) = ev;
-                            B = c * B + ev;
-                            A = c * A;
-                        }
-#pragma unroll
-                    for (int o = 1; o < G; o <<= 1) {
-                        const T A2 = __shfl_up_sync(0xffffffffu, A, o, G), B2 = __shfl_up_sync(0xffffffffu, B, o, G);
-                        if (sub >= o) { B = A * B2 + B; A = A * A2; }
-                    }
-                    T Ae = __shfl_up_sync(0xffffffffu, A, 1, G), Be = __shfl_up_sync(0xffffffffu, B, 1, G);
-                    if (sub == 0) { Ae = T(1); Be = T(0); }
-                    A = T(1);
-                    B = T(0);
-                    if (act) {
-                        T q = Ae * ph(-1, jj, kk) + Be;
-                        for (int ii = a; ii < e; ++ii) {
-                            q = cf(ii, jj, kk) * q + qr(ii, jj, kk);
-                            qr(ii, jj, kk) = q;
-                        }
-                        for (int ii = e - 1; ii >= a; --ii) {
-                            const T pv = pr(ii, jj, kk);
-                            B = pv * B + qr(ii, jj, kk);
-                            A = pv * A;
-                        }
-                    }
-#pragma unroll
-                    for (int o = 1; o < G; o <<= 1) {
-                        const T A2 = __shfl_down_sync(0xffffffffu, A, o, G), B2 = __shfl_down_sync(0xffffffffu, B, o, G);
-                        if (sub + o < G) { B = A * B2 + B; A = A * A2; }
-                    }
-                    Ae = __shfl_down_sync(0xffffffffu, A, 1, G);
-                    Be = __shfl_down_sync(0xffffffffu, B, 1, G);
-                    if (sub == G - 1) { Ae = T(1); Be = T(0); }
-                    if (act) {
-                        T x = Ae * ph(NI, jj, kk) + Be;
-                        for (int ii = e - 1; ii >= a; --ii) {
-                            x = pr(ii, jj, kk) * x + qr(ii, jj, kk);
-                            ph(ii, jj, kk) = x;
-                        }
-                    }
+                    group_line_shared<T>(at, ab, an, as, su, pr, cf, id, qr, ph, BoxLine{NI, sub, a, e}, jj, kk, act);
                     __syncwarp();
                 }
                 __syncthreads();
