@@ -797,15 +797,12 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     V3<T> at, ab, an, as, su, pr, cf, id, qr, ph;
     const T *ae_src, *aw_src, *ap_src;
     if (fits) {
-        const int cj = NI;
-        const long long ck = (long long)NI * NJ;
-        T *q0 = sm;
-        at = {q0 + 0ll * ncell, cj, ck}; ab = {q0 + 1ll * ncell, cj, ck};
-        an = {q0 + 2ll * ncell, cj, ck}; as = {q0 + 3ll * ncell, cj, ck};
-        su = {q0 + 4ll * ncell, cj, ck}; pr = {q0 + 5ll * ncell, cj, ck};
-        cf = {q0 + 6ll * ncell, cj, ck}; id = {q0 + 7ll * ncell, cj, ck};
-        qr = {q0 + 8ll * ncell, cj, ck};
-        ph = {q0 + 9ll * ncell + 1 + HI + (long long)HI * HJ, HI, (long long)HI * HJ};
+        // array f of the box: cell (ii, jj, kk) at f * ncell + ii + NI (jj + NJ kk)
+        auto box_array = [&](long long f) { return V3<T>{sm + f * ncell, NI, (long long)NI * NJ}; };
+        at = box_array(0); ab = box_array(1); an = box_array(2); as = box_array(3);
+        su = box_array(4); pr = box_array(5); cf = box_array(6); id = box_array(7);
+        qr = box_array(8);
+        ph = {sm + 9ll * ncell + 1 + HI + (long long)HI * HJ, HI, (long long)HI * HJ};
         // every load of a batch is issued before its shared-memory stores; the
         // arrays at ab an as su pr(=ae) cf(=aw) id(=ap) follow one another, cell
         // (ii, jj, kk) at q = ii + NI (jj + NJ kk), and the halo of phi after them
