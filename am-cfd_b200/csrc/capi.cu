@@ -114,6 +114,7 @@ struct amcfd_ctx {
     // the whole outer loop of a step as one graph, by property parity at its start
     cudaGraphExec_t gloop[2] = {};
     bool host_loop = false;        // drive the outer iterations from the host even with graphs
+    long long wait_polls = 0;      // budget of the exact-order sweep's line waits (0: default)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
@@ -489,6 +490,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         setup_mom_small<T>(I);
     }
     g.st = ctx->st_dev;
+    p.wait_polls = ctx->wait_polls > 0 ? ctx->wait_polls : kSpinLimit;
     I.check_finite = 0;
     I.exact_warps = 4;
     // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
@@ -1155,6 +1157,8 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->use_graphs = opts->use_graphs != 0;
         ctx->small_box = opts->no_small_box == 0;
         ctx->host_loop = opts->host_loop != 0;
+        if (opts->wait_polls < 0) return fail(ctx, AMCFD_E_ARG, "wait_polls must not be negative");
+        ctx->wait_polls = opts->wait_polls;
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");

@@ -44,6 +44,9 @@ struct Params {
     // is the active domain, nk_alloc the planes every 3-D array holds
     int powder, nk_alloc;
     double powderden, powdercpa, powdercpb, powderthcona, powderthconb;
+    // polls of one bounded wait on another warp's line counter before the wait
+    // gives up with AMCFD_E_TIMEOUT (exact-order sweeps)
+    long long wait_polls;
 };
 
 // Device status block: per-step inputs written by the host, per-iteration

@@ -242,15 +242,16 @@ __device__ __forceinline__ void stage_window(int i0, int i1, int &ib, int &ie)
     ie = (i1 + 1 + V - 1) & ~(V - 1);
 }
 
-// Bounded wait until *f >= target (wrap-safe); false on timeout or a raised error.
-__device__ bool wait_ge(const int *f, int target, Status *st, int where)
+// Bounded wait until *f >= target (wrap-safe); false after `limit` polls or once
+// another warp has raised an error.
+__device__ bool wait_ge(const int *f, int target, Status *st, int where, long long limit)
 {
     long long it = 0;
     while (true) {
         int v = *(volatile const int *)f;
         if (v - target >= 0) return true;
         if ((it & 63) == 63 && *(volatile int *)&st->error) return false;
-        if (++it > kSpinLimit) {
+        if (++it > limit) {
             if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
             return false;
         }
@@ -320,10 +321,11 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
             if (lane == 0) {
                 stage_line<T>(g, row, ib, ie, sl, nmax, bar);  // overlaps the waits below
                 const int where = k * nj + j;
-                if (ok && j > j0) ok = wait_ge(&flags[k * nj + j - 1], base + v + 1, st, where);
-                if (ok && j < j1 && v > 0) ok = wait_ge(&flags[k * nj + j + 1], base + v, st, where);
-                if (ok && k < k1) ok = wait_ge(&flags[(k + 1) * nj + j], base + 2 * ks + 2, st, where);
-                if (ok && k > k0 && ks > 0) ok = wait_ge(&flags[(k - 1) * nj + j], base + 2 * ks, st, where);
+                const long long lim = p.wait_polls;
+                if (ok && j > j0) ok = wait_ge(&flags[k * nj + j - 1], base + v + 1, st, where, lim);
+                if (ok && j < j1 && v > 0) ok = wait_ge(&flags[k * nj + j + 1], base + v, st, where, lim);
+                if (ok && k < k1) ok = wait_ge(&flags[(k + 1) * nj + j], base + 2 * ks + 2, st, where, lim);
+                if (ok && k > k0 && ks > 0) ok = wait_ge(&flags[(k - 1) * nj + j], base + 2 * ks, st, where, lim);
                 __threadfence();
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);

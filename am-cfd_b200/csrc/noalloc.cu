@@ -12,9 +12,15 @@
 // array that exists on every GPU from the moment the library is loaded until the
 // process exits (64 KiB per GPU).  Host code cannot use the array's name as a
 // device address, so the first call on each device looks the address up with
-// cudaGetSymbolAddress (with that device current) and caches it; make that first
-// call before any stream capture.  The function allocates nothing and calls no
-// allocating library routine.
+// cudaGetSymbolAddress (with that device current) and caches it together with the
+// device's current CUDA context; make that first call before any stream capture.
+// A later call under a different context (after cudaDeviceReset, say) looks the
+// address up again.  The function allocates nothing and calls no allocating
+// library routine.
+//
+// Errors: a CUDA error already pending on the calling thread when the call starts
+// (left by the caller's own earlier work) is neither reported as this call's nor
+// cleared: the call returns AMCFD_E_CUDA at once and leaves it for the caller.
 //
 // Limits and sharing: at most kMaxPlanes = 4096 interior k-planes (nk - 2); larger
 // grids are rejected with AMCFD_E_CAPACITY before anything is launched.  All calls
@@ -24,6 +30,7 @@
 #include <cstdio>
 #include <mutex>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "amcfd.h"
@@ -37,6 +44,25 @@ static __device__ __align__(256) double g_resid_scratch[2 * kMaxPlanes];
 
 std::mutex g_mu;
 double *g_scratch_ptr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};  // the context each address belongs to
+
+// The calling thread's current driver context (cuCtxGetCurrent through the
+// runtime's entry-point query, so the library needs no -lcuda); null if unknown.
+CUcontext current_context()
+{
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = nullptr;
+    if (!fn) {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult qr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &ptr, cudaEnableDefault, &qr) != cudaSuccess ||
+            qr != cudaDriverEntryPointSuccess || !ptr)
+            return nullptr;
+        fn = reinterpret_cast<Fn>(ptr);
+    }
+    CUcontext c = nullptr;
+    return fn(&c) == CUDA_SUCCESS ? c : nullptr;
+}
 
 __device__ __forceinline__ double wsum(double v)
 {
@@ -113,12 +139,23 @@ extern "C" int amcfd_energy_residual_noalloc(const double *an, const double *as,
                 "capacity of %d planes\n", nk - 2, kMaxPlanes);
         return AMCFD_E_CAPACITY;
     }
+    // an error the caller's own earlier work left pending stays the caller's
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        fprintf(stderr, "amcfd_energy_residual_noalloc: a CUDA error was already pending (%s); nothing launched\n",
+                cudaGetErrorString(pending));
+        return AMCFD_E_CUDA;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return AMCFD_E_CUDA;
     double *part;
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch_ptr[dev]) {
+        // the first call, or the device's context changed since the address was taken
+        // (a thread with no current context yet looks it up again, which makes the
+        // device's primary context current)
+        const CUcontext cur = current_context();
+        if (!g_scratch_ptr[dev] || !cur || cur != g_scratch_ctx[dev]) {
             void *ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_resid_scratch);
             if (e != cudaSuccess || !ptr) {
@@ -127,6 +164,7 @@ extern "C" int amcfd_energy_residual_noalloc(const double *an, const double *as,
                 return AMCFD_E_CUDA;
             }
             g_scratch_ptr[dev] = (double *)ptr;
+            g_scratch_ctx[dev] = current_context();
         }
         part = g_scratch_ptr[dev];
     }

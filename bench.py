@@ -2,21 +2,29 @@
 
 Workload (one line per run): the 45-degree diagonal scan on a 400 x 200 x 100
 non-uniform grid (8 M interior cells; P = 300 W, r = 60 um, v = 0.8 m/s,
-dt = 5e-6 s, <= 20 SIMPLE outer iterations per step), synthetic deck from
-am-cfd_b200/amcfd_decks.py.  A "step" is one time step of the solver
-(updateLaser + iterativeLoopSolve + updateSolutions).
+dt = 5e-6 s, <= 20 SIMPLE outer iterations per step, tolerance 1e-5),
+synthetic deck from am-cfd_b200/amcfd_decks.py.  A "step" is one time step of
+the solver (updateLaser + iterativeLoopSolve + updateSolutions).
 
-value  = simulated milliseconds per wall second over K timed steps (device time
-         between CUDA events on the solver stream, max over ranks, all ranks'
-         replicas counted); cell-iters/s alongside.
-e2e    = the same metric through the C ABI with, every step, the host->device
-         copy of the step's laser/time block and the device->host read of the
-         step report and of the temperature field into pinned host memory.
+Window: --start-step S untimed steps carry the run into the steady melt pool
+(the momentum box has stopped growing), then W warm-up steps, then the K timed
+steps S+W+1 .. S+W+K.  Every figure on the line (the FP64 comparator, e2e and
+the reference arm) is taken on that same window of the same deck.
+
+value  = simulated milliseconds per wall second over the K timed steps (device
+         time between CUDA events on the solver stream, max over ranks, all
+         ranks' replicas counted); cell-iters/s alongside.
+e2e    = the same metric through the C ABI (Solver.step() + the asynchronous
+         read of the FP64 temperature field into pinned host memory every step,
+         the clock stopped after the last copy landed) on a fresh solver over the
+         same window.
+fp64_redblack_* = the plain FP64 solve on the same production path (red-black
+         order, graphs, device-driven outer loop), same window and tolerance.
 Each rank (one per GPU) runs an independent replica of the single-domain case
 ("replicas only": the case does not shard).
 
---impl reference times the reference's own CPU solver (oracle/_ref, OpenMP,
-all host threads) on the same deck.
+--impl reference times the reference's own CPU solver (oracle/_ref, OpenMP on
+all physical cores) on the same deck and the same window.
 """
 from __future__ import annotations
 
@@ -27,7 +35,6 @@ import shutil
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -123,7 +130,7 @@ FEATURES = {
 
 def make_deck(tmp: str, steps: int, config: str, feature: str = "none"):
     import amcfd_decks as D
-    deck = {"config1": D.config1, "config0": D.config0}[config](steps=steps)
+    deck = {"config1": D.config1, "config0": D.config0, "config4": D.config4}[config](steps=steps)
     if feature == "species":
         deck.species = (1.0, 5e-9, 0.3, 0.7)
     elif feature == "powder":
@@ -136,22 +143,35 @@ def make_deck(tmp: str, steps: int, config: str, feature: str = "none"):
     return deck, deck.write(tmp)
 
 
-def reference_arm(args, steps: int, warmup: int, config: str, threads: int, feature: str = "none"):
-    """The reference CPU solver (oracle/_ref/amcfd_ref_dump --time) on the same deck."""
+def physical_cores() -> int:
+    """Physical cores of this host (logical CPUs when the count is unknown)."""
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except Exception:
+        pass
+    return os.cpu_count() or 1
+
+
+def reference_arm(skip: int, steps: int, config: str, threads: int, feature: str = "none"):
+    """The reference CPU solver (oracle/_ref/amcfd_ref_dump --time, OpenMP) on the same
+    deck: skip + steps time steps, the last `steps` of them timed."""
     import oracle_py
     exe = oracle_py.REF_DUMP
     if not os.path.exists(exe):
         return None, "reference binary oracle/_ref/amcfd_ref_dump not built"
     with tempfile.TemporaryDirectory() as tmp:
-        deck, path = make_deck(tmp, warmup + steps, config, feature)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        out = subprocess.run([exe, path, "--time", "--steps", str(warmup + steps)], env=env,
-                             capture_output=True, text=True, timeout=1800)
+        deck, path = make_deck(tmp, skip + steps, config, feature)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread", OMP_PLACES="cores")
+        out = subprocess.run([exe, path, "--time", "--steps", str(skip + steps)], env=env,
+                             capture_output=True, text=True, timeout=3600)
         if out.returncode != 0:
             return None, f"reference run failed: {out.stderr[-300:]}"
         js = json.loads(out.stdout.strip().splitlines()[-1])
-    st = js["step_seconds"][warmup:]
-    it = js["step_iters"][warmup:]
+    st = js["step_seconds"][skip:]
+    it = js["step_iters"][skip:]
     secs = sum(st)
     ncell = js["interior_cells"]
     sim_ms = 1e3 * deck.dt * len(st)
@@ -160,56 +180,70 @@ def reference_arm(args, steps: int, warmup: int, config: str, threads: int, feat
             "ms_per_step": 1e3 * secs / max(len(st), 1)}, None
 
 
+CONFIG_DESC = {
+    "config1": ("diagonal 45-degree single track, 400x200x100 non-uniform cells (8.0 M), P=300 W, "
+                "r=60 um, v=0.8 m/s, dt=5e-6 s, <=20 outer iterations/step, tolerance 1e-5"),
+    "config0": "single track +x, 120x60x40 cells, P=200 W, dt=1e-5 s, <=20 outer iterations/step",
+    "config4": ("2 layers x 5 tracks bidirectional raster (hatch 100 um, 1 ms dwell, 90-degree rotation), "
+                "600x300x120 non-uniform cells (21.6 M), P=200 W, v=1.0 m/s, dt=1e-5 s, <=20 outer "
+                "iterations/step, tolerance 1e-5"),
+}
+# untimed steps before the warm-up, by deck: config 1's momentum box stops growing
+# by then; config 4's toolpath opens with a 1 ms (100-step) dwell with the beam off
+START_STEP = {"config1": 60, "config0": 20, "config4": 130}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--start-step", type=int, default=None,
+                    help="untimed steps before the warm-up (default: per deck, into the steady melt pool)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--order", default="redblack", choices=["redblack", "exact"])
-    ap.add_argument("--config", default="config1", choices=["config1", "config0"])
+    ap.add_argument("--config", default="config1", choices=sorted(CONFIG_DESC))
     ap.add_argument("--graphs", type=int, default=1, choices=[0, 1],
                     help="replay each outer iteration from a CUDA graph")
     ap.add_argument("--host-loop", action="store_true",
                     help="with graphs, one graph per outer iteration and the convergence test on the "
                          "host (default: one graph per step, iterations chained on the device)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 exact-order comparison run")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--feature", default="none", choices=sorted(FEATURES),
                     help="solve the deck with one of the optional models switched on")
     args = ap.parse_args()
     warmup = max(3, args.warmup)
+    start = START_STEP[args.config] if args.start_step is None else max(0, args.start_step)
+    skip = start + warmup  # steps before the timed window
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    threads = os.cpu_count() or 1
-    cfg_desc = {"workload": ("diagonal 45-degree single track, 400x200x100 non-uniform cells "
-                             "(8.0 M), P=300 W, r=60 um, v=0.8 m/s, dt=5e-6 s, <=20 outer "
-                             "iterations/step" if args.config == "config1" else
-                             "single track +x, 120x60x40 cells, P=200 W, dt=1e-5 s"),
-                "deck": args.config, "l2": "working set 1.2-2.5 GB > 126 MB L2 (no flush needed)"}
+    cores = physical_cores()
+    window = f"steps {skip + 1}-{skip + args.steps} (after {start} untimed steps and {warmup} warm-up steps)"
+    cfg_desc = {"workload": CONFIG_DESC[args.config], "deck": args.config, "window": window,
+                "l2": "working set 1.2-6.4 GB > 126 MB L2 (no flush needed)"}
     if args.feature != "none":
         cfg_desc["feature"] = FEATURES[args.feature]
 
     if args.impl == "reference":
         if rank != 0:
             return
-        ksteps = min(args.steps, 8)
-        kwarm = min(warmup, 1)
-        r, why = reference_arm(args, ksteps, kwarm, args.config, threads, args.feature)
+        r, why = reference_arm(skip, args.steps, args.config, cores, args.feature)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
         line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
-                "n_gpus": args.gpus, "steps": r["steps"], "warmup": kwarm,
+                "n_gpus": args.gpus, "steps": r["steps"], "warmup": warmup,
                 "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic deck",
                 "config": dict(cfg_desc, solver="reference OpenMP build (oracle/_ref)"),
-                "cell_iters_per_s": r["cell_iters_per_s"],
+                "cell_iters_per_s": r["cell_iters_per_s"], "outer_iters": r["outer_iters"],
                 "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["threads"],
-                                 "kind": "reference",
-                                 "sample": f"{r['steps']} steps after {kwarm} warm-up of the same deck"},
+                                 "kind": "reference", "logical_cpus": os.cpu_count(),
+                                 "sample": f"the timed window ({window}) of the same deck, "
+                                           f"OpenMP on {r['threads']} physical cores"},
                 "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -229,14 +263,18 @@ def main():
     prec = amcfd.PREC_FP32 if args.precision == "fp32" else amcfd.PREC_FP64
     order = amcfd.ORDER_REDBLACK if args.order == "redblack" else amcfd.ORDER_EXACT
     tmp = tempfile.mkdtemp(prefix=f"amcfd_bench{rank}_")
-    total_steps = warmup + 3 * args.steps + 2
+    total_steps = skip + 2 * args.steps + 2
     deck, path = make_deck(tmp, total_steps, args.config, args.feature)
     d = amcfd.Deck(path)
     ni, nj, nk = d.dims
     ncell = (ni - 2) * (nj - 2) * (nk - 2)
-    s = amcfd.Solver(d, order=order, precision=prec, device=dev, use_graphs=args.graphs,
-                     host_loop=1 if args.host_loop else 0)
-    s.run_steps(warmup)
+
+    def solver(p=prec):
+        return amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
+                            host_loop=1 if args.host_loop else 0)
+
+    s = solver()
+    s.run_steps(skip)
 
     def barrier():
         if world > 1:
@@ -264,31 +302,38 @@ def main():
     barrier()
     ck = clocks.stop()
     ms = allmax(ms)
-    # the per-phase split: the next steps again, with CUDA events around each phase
+    # the per-phase split: the next steps, with CUDA events around each phase
     # (the host drives those iterations), per outer iteration
     s.profile(True)
     s.run_steps(args.steps)
     prof = s.timing()
     s.profile(False)
     torch.cuda.synchronize()
+    s.close()
     value = world * 1e3 * deck.dt * args.steps / (ms / 1e3)
     cips = world * ncell * iters / (ms / 1e3)
 
-    # end to end: per step, laser block in, report + temperature field out (pinned).
-    # Each step's field is packed on the device at once and copied to the host
-    # while the next step computes; the clock stops after the last copy landed.
+    # end to end on a fresh solver over the same window: per step, laser block in,
+    # report + temperature field out (pinned).  Each step's field is packed on the
+    # device at once and copied to the host while the next step computes; the clock
+    # stops after the last copy landed.
+    se = solver()
+    se.run_steps(skip)
     host = torch.empty(ni * nj * nk, dtype=torch.float64, pin_memory=True)
-    s.get_into_async("temp", host.data_ptr())  # warm-up: the copy stream is made on first use
-    s.wait_reads()
+    se.get_into_async("temp", host.data_ptr())  # warm-up: the copy stream is made on first use
+    se.wait_reads()
+    boxes = []
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        s.step()
-        s.get_into_async("temp", host.data_ptr())
-    s.wait_reads()
+        r = se.step()
+        se.get_into_async("temp", host.data_ptr())
+        boxes.append(r["momentum_cells"])
+    se.wait_reads()
     t1 = time.perf_counter()
     barrier()
+    se.close()
     e2e_s = allmax(t1 - t0)
     e2e = {"value": world * 1e3 * deck.dt * args.steps / e2e_s, "unit": METRIC,
            "h2d_bytes_per_step": 52, "d2h_bytes_per_step": int(ni * nj * nk * 8 + 512)}
@@ -311,38 +356,47 @@ def main():
                 "traffic": tr * ncell if tr else None,
                 "iteration_frac": (92 * ncell * w * iters / (ms / 1e3) / 1e9) / peak}
 
-    extra = {}
+    extra = {"momentum_box_cells": {"mean": float(np.mean(boxes)), "min": int(min(boxes)),
+                                    "max": int(max(boxes))}}
     if args.feature == "freesurf":
-        # one free-surface update (bisection + projection) on the final state; the call
+        # one free-surface update (bisection + projection) on a fresh state; the call
         # returns after its kernels and the read-back of the monitor values
-        s.free_surface()
+        sf = solver()
+        sf.run_steps(2)
+        sf.free_surface()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        fs = s.free_surface()
+        fs = sf.free_surface()
         extra["free_surface_ms"] = 1e3 * (time.perf_counter() - t0)
         extra["free_surface"] = fs
-    if not args.no_compare and rank == 0:
-        # the plain FP64 exact-order solve of the same steps, for the speed-up at equal iterations
-        s64 = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, device=dev,
-                           use_graphs=args.graphs)
-        s64.run_steps(1)
-        nref = min(args.steps, 3)
-        _, ms64 = s64.run_steps(nref)
-        extra["fp64_exact_sim_ms_per_wall_s"] = 1e3 * deck.dt * nref / (ms64 / 1e3)
-        extra["speedup_vs_fp64_exact"] = (value / world) / extra["fp64_exact_sim_ms_per_wall_s"]
+        sf.close()
+    if not args.no_compare and rank == 0 and prec == amcfd.PREC_FP32:
+        # the plain FP64 solve on the same production path and the same window
+        s64 = solver(amcfd.PREC_FP64)
+        s64.run_steps(skip)
+        i64 = s64.report.itertot
+        r64, ms64 = s64.run_steps(args.steps)
+        v64 = 1e3 * deck.dt * args.steps / (ms64 / 1e3)
+        extra["fp64_redblack_sim_ms_per_wall_s"] = v64
+        extra["fp64_redblack_cell_iters_per_s"] = ncell * (r64["itertot"] - i64) / (ms64 / 1e3)
+        extra["fp64_redblack_outer_iters"] = r64["itertot"] - i64
+        extra["speedup_vs_fp64_redblack"] = (value / world) / v64
         s64.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r, why = reference_arm(args, 2, 0, args.config, threads, args.feature)
+        # a bounded sample: the first steps of the same deck (the reference arm,
+        # a separate run, times the full window)
+        r, why = reference_arm(0, 3, args.config, cores, args.feature)
         if r is not None:
             cpu = {"value": r["value"], "unit": METRIC, "cores": r["threads"], "kind": "reference",
-                   "sample": f"first {r['steps']} steps of the same deck, OpenMP build of the reference",
+                   "logical_cpus": os.cpu_count(),
+                   "sample": f"steps 1-{r['steps']} of the same deck, OpenMP build of the reference "
+                             f"on {r['threads']} physical cores",
                    "cell_iters_per_s": r["cell_iters_per_s"]}
         else:
-            cpu = {"value": None, "unit": METRIC, "cores": threads, "kind": "reference",
+            cpu = {"value": None, "unit": METRIC, "cores": cores, "kind": "reference",
                    "sample": why}
-    s.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": warmup, "ms_per_step": ms / args.steps,

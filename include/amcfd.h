@@ -148,7 +148,11 @@ typedef struct amcfd_options {
     int host_loop;       /* 1: with use_graphs, still launch one graph per outer iteration and
                             test convergence on the host (0: one graph per step, the
                             iterations chained on the device) */
-    int reserved[6];
+    int wait_polls;      /* polls (about 64 ns each) a warp of the exact-order line sweep
+                            waits for a neighbouring line before the step fails with
+                            AMCFD_E_TIMEOUT; 0 = the default 2^24 (about one second).  The
+                            reference has no such wait (its sweeps are sequential). */
+    int reserved[5];
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;
@@ -342,8 +346,11 @@ int amcfd_ws_stats(const amcfd_ctx *ctx, long long *accepted, long long *rejecte
  * array held by every GPU that loads the library (64 KiB) that supports at most
  * 4096 interior k-planes (nk - 2); larger grids get AMCFD_E_CAPACITY.  The first
  * call on a device looks up that array's address (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race.  Work is
- * queued on `stream` (a cudaStream_t, NULL for the default stream). */
+ * capture); a call under a new context of the device (after cudaDeviceReset) looks
+ * it up again.  Calls share the array: calls that overlap on the GPU race.  Work is
+ * queued on `stream` (a cudaStream_t, NULL for the default stream).  A CUDA error
+ * already pending from the caller's own earlier work makes the call return
+ * AMCFD_E_CUDA without launching and without clearing that error. */
 int amcfd_energy_residual_noalloc(const double *an, const double *as, const double *ae,
                                   const double *aw, const double *at, const double *ab,
                                   const double *ap, const double *su, const double *h,

@@ -11,11 +11,14 @@
  * reference bit for bit.  std::max/std::min are restated as MAXD/MIND with
  * the same NaN behaviour ((a<b)?b:a and (b<a)?b:a).  It is pinned against the
  * compiled reference (oracle/_ref/amcfd_ref_dump, built by
- * oracle/build_ref.sh) by tests/test_oracle_vs_ref.py and the committed
- * golden records under tests/golden/.
+ * oracle/build_ref.sh) by tests/test_oracle.py (live runs of the reference)
+ * and the committed golden records under tests/golden/.
  *
- * Not restated (outside the hot path): moving mesh, powder-bed properties and
- * layer activation, solidification G/R, free surface, output writers.
+ * Restated beyond the SIMPLE loop itself: the species equation, powder-bed
+ * properties and layer activation, the moving mesh with its remap,
+ * solidification G/R and the energy-balance free surface (orc_species,
+ * orc_move_mesh, orc_free_surface ...).  Not restated: the output writers
+ * (their files are compared with the compiled reference's directly).
  */
 #include <math.h>
 #include <stdlib.h>

@@ -15,11 +15,12 @@
 #      arrays.  The bounds become 610 x 310 x 130 (enough for the 602 x 302 x
 #      122-node deck, and a smaller footprint than the original 42 M cells).
 #
-# Usage: oracle/build_ref.sh [reference-root]   (default: $AMCFD_REFERENCE or
-#        /root/reference).  Exits 0 without building when the tree is absent.
+# Usage: oracle/build_ref.sh [reference-root]   (default: $AMCFD_REFERENCE, else a
+#        "reference" directory beside the repository).  Exits 0 without building
+#        when the tree is absent.
 set -euo pipefail
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-${AMCFD_REFERENCE:-/root/reference}}
+REF=${1:-${AMCFD_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}}
 OUT="$HERE/_ref"
 if [ ! -f "$REF/src/main.cpp" ]; then
     echo "build_ref: reference tree not found at $REF; nothing built"

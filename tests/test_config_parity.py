@@ -1,0 +1,139 @@
+"""GPU parity on the benchmark decks themselves, against the CPU oracle.
+
+Config 0 (120 x 60 x 40 cells, single track along +x, 4 steps) and the first
+two steps of config 1 (400 x 200 x 100 cells, 45-degree diagonal scan, the deck
+bench.py times) run through the oracle (single-threaded FP64, bit-identical to
+the compiled reference) and through the C ABI:
+
+* FP64 in the reference's exact sweep order: per step the oracle's outer
+  iteration count and momentum-box indices, and T, u, v, w, h within 1e-8
+  relative L2 (the bar of the small parity decks, now at the sizes where the
+  line solvers run many 16-byte rounds per line, the assembly many 32 x 8 tiles
+  and the TMA boxes span 400-node rows);
+* the production path that bench.py times (FP32 bulk with FP64 reductions,
+  red-black line order, the one-CTA momentum path for small boxes, the whole
+  outer loop of a step as one CUDA graph): melt-pool length, depth and width
+  within one cell of the oracle's (the cell widths of the grid where each is
+  measured), and T, u, v, w within the stated relative L2 of the oracle.  The
+  red-black order is a different iteration from the reference's sweep, and
+  the outer loop stops at 20 iterations unconverged, so the fields differ by
+  what the unconverged iterations leave, not by rounding alone.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SNAP = ("temp", "uvel", "vvel", "wvel", "enthalpy")
+BOX = ("istat", "iend", "jstat", "jend", "kstat")
+STEPS = {"config0": 4, "config1": 2}
+# production path against the oracle: relative L2 bounds per field (measured
+# values are printed by the test)
+PROD_TOL = {"temp": 1e-3, "enthalpy": 1e-3, "uvel": 0.3, "vvel": 0.3, "wvel": 0.3}
+
+_cache = {}
+
+
+def _deck(name, tmp_factory):
+    import amcfd
+    import amcfd_decks as D
+    dk = {"config0": D.config0, "config1": D.config1}[name](steps=STEPS[name])
+    return amcfd.Deck(dk.write(str(tmp_factory.mktemp(name))))
+
+
+def _oracle(name, tmp_factory):
+    """The oracle's reports and fields after every step (computed once per deck)."""
+    if name not in _cache:
+        import oracle_py
+        d = _deck(name, tmp_factory)
+        o = oracle_py.Oracle(d)
+        steps = []
+        for _ in range(STEPS[name]):
+            r = o.step()
+            steps.append((r, {f: o.field(f).copy() for f in SNAP}))
+        grid = {a: o.field(a).copy() for a in ("x", "y", "z")}
+        o.close()
+        _cache[name] = (d, steps, grid)
+    return _cache[name]
+
+
+def _one_cell(grid, r):
+    """Widths of the cells where the oracle measured L, W and D (getMeltPoolShape,
+    BoundCondManager.cpp:280-447): x over the box's i range, y over its j range,
+    z from its lowest plane to the top."""
+    dx = np.diff(grid["x"][max(r["istat"] - 1, 0): r["iend"] + 2]).max()
+    dy = np.diff(grid["y"][max(r["jstat"] - 1, 0): r["jend"] + 2]).max()
+    dz = np.diff(grid["z"][max(r["kstat"] - 2, 0):]).max()
+    return {"alen": dx, "width": dy, "depth": dz}
+
+
+@pytest.mark.parametrize("name", ["config0", "config1"])
+def test_exact_fp64_matches_oracle(name, tmp_path_factory):
+    import amcfd
+    d, steps, _ = _oracle(name, tmp_path_factory)
+    s = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, use_graphs=1)
+    for q, (ro, fo) in enumerate(steps):
+        rg = s.step()
+        where = f"{name} step {q + 1}"
+        assert rg["niter"] == ro["niter"], (where, rg["niter"], ro["niter"])
+        for k in BOX:
+            assert rg[k] == ro[k], (where, k, rg[k], ro[k])
+        for k in ("alen", "depth", "width", "tpeak"):
+            assert abs(rg[k] - ro[k]) <= 1e-8 * max(abs(ro[k]), 1e-12) + 1e-14, (where, k, rg[k], ro[k])
+        for f in SNAP:
+            err = rel_l2(s.get(f), fo[f])
+            print(f"{where} exact fp64 {f} rel-L2 {err:.3e}")
+            assert err < 1e-8, (where, f, err)
+    s.close()
+
+
+@pytest.mark.parametrize("name", ["config0", "config1"])
+def test_production_path_melt_pool_within_one_cell(name, tmp_path_factory):
+    import amcfd
+    d, steps, grid = _oracle(name, tmp_path_factory)
+    s = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1,
+                     host_loop=0, small_box=1)
+    for q, (ro, fo) in enumerate(steps):
+        rg = s.step()
+        where = f"{name} step {q + 1}"
+        cell = _one_cell(grid, ro)
+        errs = {f: rel_l2(s.get(f), fo[f]) for f in SNAP}
+        print(where, "fp32 red-black niter", rg["niter"], "oracle", ro["niter"],
+              " ".join(f"{f} {e:.3e}" for f, e in errs.items()),
+              " ".join(f"{k} {rg[k]:.6e}/{ro[k]:.6e} (cell {cell[k]:.2e})" for k in cell))
+        for k, w in cell.items():
+            assert abs(rg[k] - ro[k]) <= w, (where, k, rg[k], ro[k], w)
+        for f, e in errs.items():
+            assert e < PROD_TOL[f], (where, f, e)
+    s.close()
+
+
+def test_small_box_two_lines_per_group_matches_grid_path(tmp_path):
+    """The FP32 register sweep of the one-CTA momentum path keeps one line of a
+    colour per 8-lane group in registers; with 65 to 128 lines of a colour a group
+    solves a second line from shared memory.  On the config-1 deck the box passes
+    64 lines of one colour within the first 20 steps; those steps agree with the
+    multi-kernel momentum path to 1e-3 relative L2."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.config1(steps=20).write(str(tmp_path)))
+    a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1, small_box=0)
+    b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1, small_box=1)
+    capacity = 4266  # cells of the FP32 one-CTA path (mom_small_capacity)
+    two = 0
+    for q in range(20):
+        ra, rb = a.step(), b.step()
+        lines = (rb["jend"] - rb["jstat"] + 1) * (d.dims[2] - 2 - rb["kstat"] + 1)
+        per_colour = (lines + 1) // 2
+        if 64 < per_colour <= 128 and 0 < rb["momentum_cells"] <= capacity:
+            two += 1
+            for f in ("temp", "uvel", "vvel", "wvel", "pressure"):
+                x, y = b.get(f), a.get(f)
+                if np.linalg.norm(y) > 0:
+                    assert rel_l2(x, y) < 1e-3, (q + 1, f, rel_l2(x, y))
+    assert two > 0, "the box never had 65-128 lines of one colour within the small-box capacity"
+    assert b.launches < a.launches
+    a.close()
+    b.close()

@@ -167,12 +167,30 @@ def test_graph_replay_bit_identical(prec, order, deckdir):
         a.profile(s % 2 == 1)  # alternate timed and untimed iterations on both paths
         b.profile(s % 2 == 1)
         ra, rb = a.step(), b.step()
+        ctx = _mismatch_context(s, ra, rb)
         for k in ("niter", "tpeak", "alen", "depth", "width", "resorh", "resorm", "ratio"):
-            assert ra[k] == rb[k], (s, k, ra[k], rb[k])
+            assert ra[k] == rb[k], (k, ctx)
         for f in FIELDS:
-            assert np.array_equal(a.get(f), b.get(f)), (s, f)
+            x, y = a.get(f), b.get(f)
+            assert np.array_equal(x, y), _field_mismatch(f, x, y, ctx)
     a.close()
     b.close()
+
+
+def _mismatch_context(step, ra, rb):
+    keys = ("niter", "itertot", "resorh", "resorm", "ratio", "tpeak", "momentum_cells")
+    return f"step {step + 1}: direct " + str({k: ra[k] for k in keys}) + " graph " + str({k: rb[k] for k in keys})
+
+
+def _field_mismatch(name, x, y, ctx):
+    """Where two fields that should be bit-identical differ: the largest
+    difference, the number of differing nodes and the first one as (k, j, i)."""
+    diff = x != y
+    if not diff.any():
+        return f"{name}: equal ({ctx})"
+    first = tuple(int(q) for q in np.argwhere(diff)[0])
+    return (f"{name}: {int(diff.sum())} nodes differ, max |diff| {float(np.nanmax(np.abs(x - y)))}, "
+            f"first (k, j, i) = {first}: {x[first]!r} vs {y[first]!r}; {ctx}")
 
 
 @pytest.mark.parametrize("prec,order", [(0, 0), (0, 1), (1, 1)])
