@@ -24,7 +24,7 @@ MAX_ZONES = 32
 
 SCHEME_UPWIND, SCHEME_POWER_LAW, SCHEME_EXPONENTIAL = 0, 1, 2
 ORDER_EXACT, ORDER_REDBLACK = 0, 1
-PREC_FP64, PREC_FP32 = 0, 1
+PREC_FP64, PREC_FP32, PREC_FP32_DC = 0, 1, 2
 WS_OFF, WS_PREDICT, WS_RECORD, WS_PREDICT_H = 0, 1, 2, 3
 PHASES = {"laser": 1, "energy_assemble": 2, "energy_solve": 3, "h2t": 4, "meltpool": 5,
           "momentum": 6, "converge": 7, "update": 8, "species": 9}

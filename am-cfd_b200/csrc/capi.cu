@@ -79,7 +79,8 @@ struct amcfd_ctx {
     amcfd_params prm;
     std::vector<double> tool, heattable, vardt;
     std::vector<int> tool_on, tool_id;
-    int precision = AMCFD_PREC_FP64;
+    int precision = AMCFD_PREC_FP64;  // FP64 also under defect correction (FP64 instance)
+    bool dc = false;                   // AMCFD_PREC_FP32_DC: energy line solves on the FP32 correction
     int order = AMCFD_ORDER_EXACT;
     int device = 0;
     int ni = 0, nj = 0, nk = 0, nip = 0;  // nk: planes of every 3-D array (all powder layers)
@@ -491,6 +492,16 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     }
     g.st = ctx->st_dev;
     p.wait_polls = ctx->wait_polls > 0 ? ctx->wait_polls : kSpinLimit;
+    if (ctx->dc) {
+        // FP32 coefficients, defect, factorisation and correction of the energy solve
+        DcBuf &d = I.dc;
+        for (float **f : {&d.an, &d.as, &d.ae, &d.aw, &d.at, &d.ab, &d.ap, &d.su, &d.pr, &d.cf, &d.iden,
+                          &d.delta})
+            if ((rc = alloc3<float>(ctx, f, n3))) return rc;
+        if (!set_rounds_smem_limit<float>(p))
+            return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
+        I.dc_on = true;
+    }
     I.check_finite = 0;
     I.exact_warps = 4;
     // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
@@ -609,6 +620,28 @@ static bool mom_small(const amcfd_ctx *ctx, const Inst<T> &I)
            ctx->last_box <= mom_small_capacity<T>(I);
 }
 
+// The energy line solve: with defect correction the FP32 passes on the correction.
+template <typename T>
+static void energy_sweeps(Inst<T> &I)
+{
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (I.dc_on) {
+            launch_dc_sweeps(I);
+            return;
+        }
+    }
+    launch_energy_sweeps<T>(I);
+}
+
+// H->T; with defect correction the correction is added to the FP64 enthalpy first.
+template <typename T>
+static void h2t(Inst<T> &I)
+{
+    if constexpr (sizeof(T) == sizeof(double))
+        if (I.dc_on) launch_dc_apply(I);
+    launch_h2t<T>(I);
+}
+
 template <typename T>
 static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
 {
@@ -620,9 +653,9 @@ static void run_phase_impl(amcfd_ctx *ctx, Inst<T> &I, int phase)
         break;
     case AMCFD_PHASE_ENERGY_SOLVE:
         launch_energy_factor<T>(I);
-        launch_energy_sweeps<T>(I);
+        energy_sweeps<T>(I);
         break;
-    case AMCFD_PHASE_H2T: launch_h2t<T>(I); break;
+    case AMCFD_PHASE_H2T: h2t<T>(I); break;
     case AMCFD_PHASE_MELTPOOL: launch_meltpool<T>(I); break;
     case AMCFD_PHASE_MOMENTUM: launch_momentum<T>(I, mom_small<T>(ctx, I)); break;
     case AMCFD_PHASE_CONVERGE:
@@ -760,7 +793,7 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     case AMCFD_PHASE_LASER: return 1;
     case AMCFD_PHASE_ENERGY_ASSEMBLE: return 3;
     case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : sweeps;
-    case AMCFD_PHASE_H2T: return 1;
+    case AMCFD_PHASE_H2T: return ctx->dc ? 2 : 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
     case AMCFD_PHASE_MOMENTUM: return small ? 9 : 2 + 4 * (3 + sweeps) + 2 + 1;
     case AMCFD_PHASE_CONVERGE: return 1;
@@ -795,7 +828,7 @@ static void launch_iteration(amcfd_ctx *ctx, Inst<T> &I, bool capturing)
     if (ev) rec(ctx, 1, capturing);
     launch_energy_factor<T>(I);
     if (ev) rec(ctx, 2, capturing);
-    launch_energy_sweeps<T>(I);
+    energy_sweeps<T>(I);
     if (ev) rec(ctx, 3, capturing);
     run_phase_impl<T>(ctx, I, AMCFD_PHASE_H2T);
     run_phase_impl<T>(ctx, I, AMCFD_PHASE_MELTPOOL);
@@ -1162,6 +1195,12 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");
+    if (ctx->precision == AMCFD_PREC_FP32_DC) {
+        if (ctx->order != AMCFD_ORDER_REDBLACK)
+            return fail(ctx, AMCFD_E_ARG, "defect correction runs in red-black order only");
+        ctx->dc = true;
+        ctx->precision = AMCFD_PREC_FP64;  // the FP64 instance carries the state
+    }
     if (ctx->precision != AMCFD_PREC_FP64 && ctx->precision != AMCFD_PREC_FP32)
         return fail(ctx, AMCFD_E_ARG, "unknown precision");
     if (p.udtoolpath) {

@@ -52,9 +52,13 @@ enum { FB_U = 0, FB_V, FB_T, FB_HN, FB_FN };
 
 // SCH: the discretisation scheme as a compile-time constant (one instantiation per
 // scheme), so that the six face coefficients carry no untaken scheme branches.
-template <typename T, int SCH>
+// DC (FP64 only, defect correction): the coefficients are formed in FP64 exactly
+// as without it, but stored rounded to FP32 in `dco`, and the FP32 `su` slot
+// receives the FP64 defect su + sum a_nb h_nb - ap h of the current enthalpy;
+// the FP64 coefficient arrays are not written.
+template <typename T, int SCH, bool DC>
 __global__ void __launch_bounds__(256, AsmBox<T>::MINB)
-energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp)
+energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp, DcBuf dco)
 {
     using R = T;
     using B = AsmBox<T>;
@@ -159,6 +163,12 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
         dyp_j = (R)g.dypsinv[j]; dyp_p = (R)g.dypsinv[j + 1];
     }
     const R aij = (R)(dx * dy);
+    // FP32: column widths rounded once, face areas and volumes as FP32 products; the
+    // divisions by per-launch constants become multiplications by their reciprocals
+    // (the FP64 build keeps the reference's FP64 products and exact divisions)
+    constexpr bool kF32 = sizeof(R) == 4;
+    const R fdx = (R)dx, fdy = (R)dy;
+    const R inv_acpl = (R)(1.0 / p.acpl), inv_delt = (R)(1.0 / delt), inv_urfh = (R)(1.0 / p.urfh);
     const R dxp_e = (R)g.dxpwinv[nim1], dxp_w = (R)g.dxpwinv[1];
     const R dyp_n = (R)g.dypsinv[njm1], dyp_s = (R)g.dypsinv[1];
     const R dzp_t = (R)g.dzpbinv[nkm1], dzp_b = (R)g.dzpbinv[1];
@@ -185,7 +195,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
             // ---- material properties (every node) ----
             {
                 const R t = t_c, fl = f_c;
-                const R diffl = bdiv(thla * t + thlb, acpl);
+                const R diffl = kF32 ? (thla * t + thlb) * inv_acpl : bdiv(thla * t + thlb, acpl);
                 R dn = diffl, rn = denl, vn = visc;
                 if (!(t >= tliq)) {
                     R diffs, rs = dens;
@@ -216,8 +226,9 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
             if (colint && k >= 1 && k <= nkm2) {
                 const int kl = k - kb;
                 const double dz = pl_dz[kl];
-                const R aik = (R)(dx * dz), ajk = (R)(dy * dz);
-                const R vol = (R)(dx * dy * dz);
+                const R fdz = (R)dz;
+                const R aik = kF32 ? fdx * fdz : (R)(dx * dz), ajk = kF32 ? fdy * fdz : (R)(dy * dz);
+                const R vol = kF32 ? aij * fdz : (R)(dx * dy * dz);
                 const R fz_k = pl_m[0][kl], fz_m = pl_m[1][kl];
                 const R dzp_k = pl_m[2][kl], dzp_p = pl_m[3][kl];
                 const R dcc = d_c, rhc = Ac[FA_R * FE];
@@ -299,7 +310,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                     }
                     face_coef<R>(sch, db, fb, tmp, ab);
                 }
-                const R densbydt = bdiv(rhc, (R)delt);
+                const R densbydt = kF32 ? rhc * inv_delt : bdiv(rhc, (R)delt);
                 const R apnot = densbydt * vol;
                 R sp = R(0);
                 R su = apnot * Bc[FB_HN * FE];
@@ -317,7 +328,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                     g.sourceinput[c] = srcin;
                 }
                 const R hlatnt = (R)p.hlatnt;
-                const R variable1 = bdiv(hlatnt * rhc, (R)delt);
+                const R variable1 = kF32 ? hlatnt * rhc * inv_delt : bdiv(hlatnt * rhc, (R)delt);
                 const R volht = vol * variable1;
                 const R flc = f_c;
                 su -= volht * (flc - Bc[FB_FN * FE]);
@@ -345,10 +356,19 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 if (i == nim2) { su += ae * hip; sp -= ae; ae = R(0); }
                 R ap = an + as_ + ae + aw + at + ab + apnot - sp;
                 const R urfh = (R)p.urfh;
-                ap = bdiv(ap, urfh);
+                ap = kF32 ? ap * inv_urfh : bdiv(ap, urfh);
                 su += (R(1) - urfh) * ap * hc;
-                g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw;
-                g.at[c] = at; g.ab[c] = ab; g.ap[c] = ap; g.su[c] = su;
+                if constexpr (DC) {
+                    const double dfc = ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc;
+                    dco.an[c] = (float)an; dco.as[c] = (float)as_; dco.ae[c] = (float)ae; dco.aw[c] = (float)aw;
+                    dco.at[c] = (float)at; dco.ab[c] = (float)ab; dco.ap[c] = (float)ap; dco.su[c] = (float)dfc;
+                    blc += dfc;
+                } else {
+                    g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw;
+                    g.at[c] = at; g.ab[c] = ab; g.ap[c] = ap; g.su[c] = su;
+                    // ---- block-correction sum of the defect (enhanceConvergenceSpeed(5)) ----
+                    blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
+                }
                 // ---- residual (calculateResiduals(5)) ----
                 R r = bdiv(an * hjp + as_ * hjm + ae * hip + aw * him + at * hkp + ab * hkm + su, ap) - hc;
                 sumd += fabs((double)r);
@@ -357,7 +377,6 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 bl += (double)(ap - an - as_ - at - ab);
                 blp += (double)ae;
                 blm += (double)aw;
-                blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
             }
         }
         // this warp is done with planes k-1 (ring A) and k (ring B); the last warp
@@ -444,28 +463,45 @@ template <typename T> int make_assemble_maps(Inst<T> &I, T *diff_a, T *diff_b, T
         if (rc) return rc;
     }
     I.asm_diff_a = diff_a;
-    cudaFuncSetAttribute(energy_assemble_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
-    cudaFuncSetAttribute(energy_assemble_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
-    cudaFuncSetAttribute(energy_assemble_kernel<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B::SMEM);
+    const int sm = (int)B::SMEM;
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute(energy_assemble_kernel<T, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if constexpr (sizeof(T) == sizeof(double)) {
+        cudaFuncSetAttribute(energy_assemble_kernel<T, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(energy_assemble_kernel<T, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute(energy_assemble_kernel<T, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
     return 0;
+}
+
+template <typename T, bool DC> static void assemble_scheme(Inst<T> &I, const AsmMaps &m)
+{
+    const dim3 blk(kTX, kTY);
+    const size_t sm = AsmBox<T>::SMEM;
+    switch (I.p.scheme) {
+    case AMCFD_SCHEME_UPWIND:
+        energy_assemble_kernel<T, 0, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        break;
+    case AMCFD_SCHEME_POWER_LAW:
+        energy_assemble_kernel<T, 1, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        break;
+    default:
+        energy_assemble_kernel<T, 2, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        break;
+    }
 }
 
 template <typename T> void launch_energy_assemble(Inst<T> &I)
 {
     const AsmMaps &m = I.g.diff_cur == I.asm_diff_a ? I.asm_maps[0] : I.asm_maps[1];
-    const dim3 blk(kTX, kTY);
-    const size_t sm = AsmBox<T>::SMEM;
-    switch (I.p.scheme) {
-    case AMCFD_SCHEME_UPWIND:
-        energy_assemble_kernel<T, 0><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
-        break;
-    case AMCFD_SCHEME_POWER_LAW:
-        energy_assemble_kernel<T, 1><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
-        break;
-    default:
-        energy_assemble_kernel<T, 2><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m);
-        break;
+    if constexpr (sizeof(T) == sizeof(double)) {
+        if (I.dc_on) {
+            assemble_scheme<T, true>(I, m);
+            return;
+        }
     }
+    assemble_scheme<T, false>(I, m);
 }
 
 template void launch_energy_assemble<double>(Inst<double> &);

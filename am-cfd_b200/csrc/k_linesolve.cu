@@ -425,6 +425,10 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 // stored into every interior line, is added to the neighbour values read from
 // interior lines instead: each line's own values are overwritten by its pass,
 // and the second colour reads the first colour's lines only after that.
+// correct = 2 (defect correction, phi = the correction of the current iterate):
+// every interior line's correction starts at delphi, so the first colour's
+// neighbour values are delphi on interior lines and zero on boundary lines,
+// and nothing is read from phi for them.
 // ---------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d);
@@ -466,7 +470,12 @@ __global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T
             const bool inrow = base + V <= nip;
             const size_t c = row + (inrow ? base : 0);
             T vt[V], vb[V], vn[V], vs[V], wt[V], wb[V], wn[V], ws[V], wu[V], wc[V], wi[V], wp[V];
-            ld16(phi + c + sk, vt); ld16(phi + c - sk, vb); ld16(phi + c + sj, vn); ld16(phi + c - sj, vs);
+            if (FACTOR && correct == 2) {
+#pragma unroll
+                for (int v = 0; v < V; ++v) vt[v] = vb[v] = vn[v] = vs[v] = T(0);
+            } else {
+                ld16(phi + c + sk, vt); ld16(phi + c - sk, vb); ld16(phi + c + sj, vn); ld16(phi + c - sj, vs);
+            }
             ld16(g.at + c, wt); ld16(g.ab + c, wb); ld16(g.an + c, wn); ld16(g.as + c, ws);
             ld16(g.su + c, wu);
             if constexpr (FACTOR) {
@@ -845,6 +854,55 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
+
+// ---------------------------------------------------------------------------
+// Defect correction of the energy solve (AMCFD_PREC_FP32_DC).  The assembly left
+// FP32 coefficients and the FP64 defect r = su + sum a_nb h_nb - ap h in the DC
+// buffers; the red-black passes solve A delta = r in FP32 with delta starting at
+// the block correction delphi, which in exact arithmetic are the iterates the
+// FP64 passes would reach for h (the system is linear), and h += delta is then
+// applied in FP64.  The rounding error is that of delta, not of h.
+// ---------------------------------------------------------------------------
+void launch_dc_sweeps(Inst<double> &I)
+{
+    Fields<float> f;
+    memset(&f, 0, sizeof(f));
+    const DcBuf &d = I.dc;
+    f.an = d.an; f.as = d.as; f.ae = d.ae; f.aw = d.aw; f.at = d.at; f.ab = d.ab; f.ap = d.ap; f.su = d.su;
+    f.pr = d.pr; f.cf = d.cf; f.iden = d.iden;
+    f.delphi = I.g.delphi;
+    f.st = I.g.st;
+    const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
+    const int grid = std::max(1, (lines + 3) / 4);
+    const size_t rs = rounds_smem<float>(I.p, 4);
+    for (int color = 0; color < 2; ++color)
+        sweep_rb_rounds_kernel<float, true><<<grid, 128, rs, I.stream>>>(I.p, f, d.delta, color,
+                                                                          color == 0 ? 2 : 0);
+    for (int sweep = 1; sweep < 4; ++sweep)
+        for (int color = 0; color < 2; ++color)
+            sweep_rb_rounds_kernel<float, false><<<grid, 128, rs, I.stream>>>(I.p, f, d.delta, color, 0);
+}
+
+// h += delta over the interior (delta is zero elsewhere), 16-byte vectors of
+// delta: four FP32 corrections onto two FP64 vectors of h.
+__global__ void __launch_bounds__(256) dc_apply_kernel(double *h, const float *delta, size_t n4)
+{
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
+        const float4 d = reinterpret_cast<const float4 *>(delta)[q];
+        double2 *hp = reinterpret_cast<double2 *>(h) + 2 * q;
+        double2 a = hp[0], b = hp[1];
+        a.x += (double)d.x; a.y += (double)d.y; b.x += (double)d.z; b.y += (double)d.w;
+        hp[0] = a;
+        hp[1] = b;
+    }
+}
+
+void launch_dc_apply(Inst<double> &I)
+{
+    // the padded pitch is a multiple of 32, so the array is a whole number of 4-vectors
+    const size_t n4 = (size_t)I.p.nk * I.p.nj * I.p.nip / 4;
+    dc_apply_kernel<<<I.grid_1d, 256, 0, I.stream>>>(I.g.h, I.dc.delta, n4);
+}
 template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi) { sweeps<T>(I, phi, false); }
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
 {

@@ -66,6 +66,15 @@ struct AsmMaps {
     CUtensorMap diff, h, fracl, rho, w, u, v, temp, hnot, flnot;
 };
 
+// Defect-correction buffers (AMCFD_PREC_FP32_DC, FP64 instances only): the
+// energy coefficients rounded to FP32, with `su` holding the FP64 defect
+// su + sum a_nb h_nb - ap h of the current enthalpy instead of the source; the
+// FP32 line factorisation; and the FP32 enthalpy correction `delta` the line
+// sweeps solve for (zero on every boundary node, never written there).
+struct DcBuf {
+    float *an, *as, *ae, *aw, *at, *ab, *ap, *su, *pr, *cf, *iden, *delta;
+};
+
 // Host-side record of one instance on the device.
 template <typename T>
 struct Inst {
@@ -93,6 +102,9 @@ struct Inst {
     // updateSolutions inputs of the current step (powder bed)
     double trackindx = 1.0;
     int trackid = 0;
+    // defect correction of the energy line solves (FP64 instances only)
+    bool dc_on = false;
+    DcBuf dc{};
 };
 
 // launchers (k_energy.cu)
@@ -114,6 +126,9 @@ template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi);
 template <typename T> void launch_box_factor(Inst<T> &I);
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
 template <typename T> void launch_box_tickets(Inst<T> &I);
+// defect correction: the energy line sweeps in FP32 on the correction, and h += delta
+void launch_dc_sweeps(Inst<double> &I);
+void launch_dc_apply(Inst<double> &I);
 // momentum (k_momentum.cu)
 template <typename T> void launch_momentum(Inst<T> &I, bool small);
 template <typename T> int mom_small_capacity(const Inst<T> &I);

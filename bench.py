@@ -201,7 +201,9 @@ def main():
     ap.add_argument("--start-step", type=int, default=None,
                     help="untimed steps before the warm-up (default: per deck, into the steady melt pool)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32dc", "fp64"],
+                    help="fp32: FP32 bulk with FP64 reductions; fp32dc: FP64 fields with the energy line "
+                         "solves in FP32 on the correction (defect correction); fp64: plain FP64")
     ap.add_argument("--order", default="redblack", choices=["redblack", "exact"])
     ap.add_argument("--config", default="config1", choices=sorted(CONFIG_DESC))
     ap.add_argument("--graphs", type=int, default=1, choices=[0, 1],
@@ -260,7 +262,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = local
     torch.cuda.set_device(dev)
-    prec = amcfd.PREC_FP32 if args.precision == "fp32" else amcfd.PREC_FP64
+    prec = {"fp32": amcfd.PREC_FP32, "fp32dc": amcfd.PREC_FP32_DC, "fp64": amcfd.PREC_FP64}[args.precision]
     order = amcfd.ORDER_REDBLACK if args.order == "redblack" else amcfd.ORDER_EXACT
     tmp = tempfile.mkdtemp(prefix=f"amcfd_bench{rank}_")
     total_steps = skip + 2 * args.steps + 2
@@ -340,9 +342,13 @@ def main():
 
     # roofline of the dominant kernel family
     peak, peak_kind = _peaks()
-    w = 4 if prec == amcfd.PREC_FP32 else 8
     words = WORDS_REDBLACK if args.order == "redblack" else WORDS
+    # bytes per word of each family: FP32 bulk, FP64, or defect correction (FP64 fields,
+    # FP32 coefficients and correction in the line sweeps)
+    wsize = {f: (4 if prec == amcfd.PREC_FP32 or (prec == amcfd.PREC_FP32_DC and f in ("energy_sweeps", "factor"))
+                 else 8) for f in words}
     fam = max(words, key=lambda k: prof[k])
+    w = wsize[fam]
     # the sweep family is 8 (red-black) or 1 (exact order) launches per iteration
     piters = prof["outer_iters"]  # outer iterations of the profiling steps
     nlaunch = prof["sweep_launches"] if fam == "energy_sweeps" else piters
@@ -354,7 +360,7 @@ def main():
                 "frac": achieved / peak, "peak_kind": peak_kind, "kernel": fam,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
                 "traffic": tr * ncell if tr else None,
-                "iteration_frac": (92 * ncell * w * iters / (ms / 1e3) / 1e9) / peak}
+                "iteration_frac": (sum(words[f] * wsize[f] for f in words) * ncell * iters / (ms / 1e3) / 1e9) / peak}
 
     extra = {"momentum_box_cells": {"mean": float(np.mean(boxes)), "min": int(min(boxes)),
                                     "max": int(max(boxes))}}
@@ -370,7 +376,7 @@ def main():
         extra["free_surface_ms"] = 1e3 * (time.perf_counter() - t0)
         extra["free_surface"] = fs
         sf.close()
-    if not args.no_compare and rank == 0 and prec == amcfd.PREC_FP32:
+    if not args.no_compare and rank == 0 and prec != amcfd.PREC_FP64:
         # the plain FP64 solve on the same production path and the same window
         s64 = solver(amcfd.PREC_FP64)
         s64.run_steps(skip)
@@ -401,7 +407,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
                 "steps": args.steps, "warmup": warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32" if prec == amcfd.PREC_FP32 else "f64", "data": "synthetic deck",
+                "dtype": {amcfd.PREC_FP32: "f32", amcfd.PREC_FP32_DC: "f64 (energy line solves f32 on the correction)",
+                          amcfd.PREC_FP64: "f64"}[prec], "data": "synthetic deck",
                 "config": dict(cfg_desc, precision=args.precision, order=args.order, graphs=args.graphs,
                                outer_loop="host" if args.host_loop or not args.graphs else "device",
                                parallelism=f"replicas{world}"),

@@ -136,6 +136,12 @@ typedef struct amcfd_step_report {
 /* Arithmetic of the bulk fields and coefficients. */
 #define AMCFD_PREC_FP64 0
 #define AMCFD_PREC_FP32 1      /* FP32 bulk, FP64 reductions and H->T inversion */
+/* FP64 fields, properties, reductions and momentum; the energy line solves (the
+ * bulk of the bandwidth) in FP32 on the correction: each outer iteration forms the
+ * FP64 defect of the enthalpy equation, solves for the correction with FP32
+ * coefficients and adds it to the FP64 enthalpy (mixed-precision defect
+ * correction).  Red-black order only. */
+#define AMCFD_PREC_FP32_DC 2
 
 typedef struct amcfd_options {
     int device;          /* CUDA device ordinal */
