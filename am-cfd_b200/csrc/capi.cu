@@ -116,6 +116,7 @@ struct amcfd_ctx {
     cudaGraphExec_t gloop[2] = {};
     bool host_loop = false;        // drive the outer iterations from the host even with graphs
     long long wait_polls = 0;      // budget of the exact-order sweep's line waits (0: default)
+    int mom_cluster = 1;           // CTAs of the cluster momentum path (1: none)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
@@ -489,6 +490,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         if ((rc = alloc3<int>(ctx, &g.ntickets_mom, 1))) return rc;
         if ((rc = alloc3<T>(ctx, &I.mom_scratch, n3))) return rc;
         setup_mom_small<T>(I);
+        ctx->mom_cluster = I.mom_cluster;
     }
     g.st = ctx->st_dev;
     p.wait_polls = ctx->wait_polls > 0 ? ctx->wait_polls : kSpinLimit;
@@ -795,7 +797,7 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : sweeps;
     case AMCFD_PHASE_H2T: return ctx->dc ? 2 : 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
-    case AMCFD_PHASE_MOMENTUM: return small ? 9 : 2 + 4 * (3 + sweeps) + 2 + 1;
+    case AMCFD_PHASE_MOMENTUM: return small ? (ctx->mom_cluster > 1 ? 14 : 9) : 2 + 4 * (3 + sweeps) + 2 + 1;
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;
     case AMCFD_PHASE_SPECIES: return ctx->prm.species ? (ctx->order == AMCFD_ORDER_EXACT ? 4 : 3) + sweeps : 0;

@@ -6,8 +6,12 @@
 // block, so every launch has a fixed grid and walks the box with a stride.
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "kernels.cuh"
 #include "amcfd.h"
+
+namespace cg = cooperative_groups;
 
 namespace amcfd {
 
@@ -659,12 +663,12 @@ __device__ __forceinline__ void group_line_shared(const V3<T> &at, const V3<T> &
 // neighbour values of phi; a group's second line of a colour, where the box has
 // more lines than groups, is solved from shared memory (group_line_shared).  The
 // recurrences and their order of operations are those of the shared-memory path.
-template <typename T, bool TWO>  // TWO: some groups have a second line of a colour
+template <typename T, bool TWO, class Between>  // TWO: some groups have a second line of a colour
 __device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, int NK, const T *sm, int ncell,
                                                  T *ph0, int HI, int HJ, const V3<T> &at, const V3<T> &ab,
                                                  const V3<T> &an, const V3<T> &as, const V3<T> &su,
                                                  const V3<T> &pr, const V3<T> &cf, const V3<T> &id,
-                                                 const V3<T> &qr, const V3<T> &ph)
+                                                 const V3<T> &qr, const V3<T> &ph, Between &between)
 {
     constexpr int G = kShortG, LM = kShortL;
     const unsigned full = 0xffffffffu;
@@ -776,20 +780,51 @@ __device__ __forceinline__ void sweep_short_regs(const Box &b, int NI, int NJ, i
                 __syncwarp();
                 group_line_shared<T>(at, ab, an, as, su, pr, cf, id, qr, ph, BoxLine{NI, sub, a, a + n}, jj, kk, ac);
             }
-            __syncthreads();
+            between(sweep, c);
         }
     }
 }
 
-template <typename T>
-__device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &b, T *phi, T *sm,
-                                int smem_elems, T *scratch)
+// Shared-memory elements a slab of nj rows of a box needs: nine arrays of its
+// cells and phi with a one-cell halo.
+__host__ __device__ __forceinline__ long long slab_elems(int ni, int nj, int nk)
 {
+    return 9ll * ni * nj * nk + (long long)(ni + 2) * (nj + 2) * (nk + 2);
+}
+
+// Rows [jl0, jl0 + njl) of a box: what one CTA of a cluster holds (the whole box
+// on the one-CTA path).
+struct Slab {
+    int jl0, njl;
+};
+// Rows of the slab of CTA `rank` of `nc` over a box of nj rows.
+__host__ __device__ __forceinline__ Slab slab_of(int nj, int rank, int nc)
+{
+    const int a = (int)((long long)nj * rank / nc), e = (int)((long long)nj * (rank + 1) / nc);
+    return Slab{a, e - a};
+}
+
+// solveLiquidDomain over the lines of one slab of the box: load (fits: into
+// shared memory, else views of the global arrays), factorise, and the four
+// red-black sweeps; `between(sweep, colour)` runs after every colour pass (a CTA
+// barrier on the one-CTA path; on a cluster the cluster barrier and the exchange
+// of the rows next to the slab).  Every thread of the CTA calls it, also for an
+// empty slab.
+// REGS: the FP32 register-resident sweep may be used (the one-CTA path; a cluster's
+// slabs take the shared-memory sweep, which keeps the kernel within its registers).
+template <typename T, bool REGS, class Between>
+__device__ void solve_box_slab(const Params &p, const Fields<T> &g, const Box &bx, const Slab &sl, T *phi,
+                               T *sm, bool fits, T *scratch, Between &between)
+{
+    // the slab as a box of its own: its first row fixes the colour parity
+    Box b = bx;
+    b.j0 = bx.j0 + sl.jl0;
+    b.nj_ = sl.njl;
+    b.j1 = b.j0 + sl.njl - 1;
     const int NI = b.ni_, NJ = b.nj_, NK = b.k1 - b.k0 + 1;
     const int ncell = NI * NJ * NK;
     const int HI = NI + 2, HJ = NJ + 2;
     const int nhalo = HI * HJ * (NK + 2);
-    const bool fits = 9ll * ncell + nhalo <= (long long)smem_elems;
     const int gsj = p.nip;
     const long long gsk = (long long)p.nj * p.nip;
     const size_t g0 = cidx(b.i0, b.j0, b.k0, p.nj, p.nip);
@@ -828,7 +863,7 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
                 }
             }
         }
-        for (int q0 = tid; q0 < nhalo; q0 += kBh * nth) {
+        for (int q0 = tid; NJ > 0 && q0 < nhalo; q0 += kBh * nth) {  // (an empty slab loads nothing)
             T v[kBh];
 #pragma unroll
             for (int u = 0; u < kBh; ++u) {
@@ -883,16 +918,16 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     const int half = (NJ + 1) / 2;
     // (FP64 registers for both colours would spill: FP64 keeps the shared-memory path)
     bool regs = false;
-    if constexpr (sizeof(T) == 4)
+    if constexpr (REGS && sizeof(T) == 4)
         regs = fits && NI <= kShortG * kShortL && half * NK <= 2 * (nth >> 5) * (32 / kShortG);
     if (regs) {
-        if constexpr (sizeof(T) == 4) {
+        if constexpr (REGS && sizeof(T) == 4) {
             if (half * NK <= (nth >> 5) * (32 / kShortG))
                 sweep_short_regs<T, false>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ, at, ab, an, as, su, pr,
-                                           cf, id, qr, ph);
+                                           cf, id, qr, ph, between);
             else
                 sweep_short_regs<T, true>(b, NI, NJ, NK, sm, ncell, &ph(0, 0, 0), HI, HJ, at, ab, an, as, su, pr,
-                                          cf, id, qr, ph);
+                                          cf, id, qr, ph, between);
         }
     } else if (NI <= 48) {
         // Short lines (the usual melt-pool box): a group of G lanes per line, each
@@ -923,7 +958,7 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
                     group_line_shared<T>(at, ab, an, as, su, pr, cf, id, qr, ph, BoxLine{NI, sub, a, e}, jj, kk, act);
                     __syncwarp();
                 }
-                __syncthreads();
+                between(sweep, color);
             }
     } else {
         const int lane = tid & 31, warp = tid >> 5, nwarp = nth >> 5;
@@ -982,7 +1017,7 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
                     }
                     __syncwarp();
                 }
-                __syncthreads();
+                between(sweep, color);
             }
     }
     if (fits) {
@@ -994,29 +1029,129 @@ __device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &
     }
 }
 
-// Phase helpers of the one-CTA kernels.
+// The whole box in one CTA (shared memory when it fits, else in place in global
+// memory), a CTA barrier after every colour pass.
 template <typename T>
-__device__ __forceinline__ void small_bc(const Params &p, const Fields<T> &g, Status *st, const Box &b,
-                                         int ivar, double *red_umax, double *sh)
+__device__ void solve_box_small(const Params &p, const Fields<T> &g, const Box &b, T *phi, T *sm,
+                                int smem_elems, T *scratch)
+{
+    const int NK = b.k1 - b.k0 + 1;
+    const bool fits = slab_elems(b.ni_, b.nj_, NK) <= (long long)smem_elems;
+    auto bar = [](int, int) { __syncthreads(); };
+    solve_box_slab<T, true>(p, g, b, Slab{0, b.nj_}, phi, sm, fits, scratch, bar);
+}
+
+// The box over the CTAs of a cluster, one slab of rows each.  With the slabs in
+// shared memory, after a colour pass each CTA copies the lines of that colour in
+// the rows either side of its slab from the CTAs that own them (distributed
+// shared memory): the next pass, of the other colour, reads exactly those.
+// Without, every CTA works in place in global memory and the cluster barrier
+// orders the passes.  Every pass ends at a cluster barrier, the last one too, so
+// that no CTA leaves while another may still read its shared memory.
+// After each colour pass of a cluster's slabs: the cluster barrier and, with the
+// slabs in shared memory, the copy of the lines of that colour in the rows either
+// side of this CTA's slab from the CTAs that own them (values, not references, so
+// that the line loops keep their registers).
+template <typename T>
+struct ClusterBetween {
+    T *sm, *my_ph;
+    int NI, NJ, NK, HI, nc, j0, k0;
+    Slab sl;
+    bool fits;
+    __device__ int owner(int jg) const
+    {
+        int o = 0;
+        for (int r = 1; r < nc; ++r)
+            if (slab_of(NJ, r, nc).jl0 <= jg) o = r;
+        return o;
+    }
+    __device__ void operator()(int sweep, int color) const
+    {
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        if (!fits || sl.njl == 0 || (sweep == 3 && color == 1)) return;
+        for (int side = 0; side < 2; ++side) {
+            const int jg = side == 0 ? sl.jl0 - 1 : sl.jl0 + sl.njl;  // box row next to the slab
+            if (jg < 0 || jg >= NJ) continue;
+            const int o = owner(jg);
+            const Slab os = slab_of(NJ, o, nc);
+            // phi of o's slab, with its halo, after its nine cell arrays
+            const T *rph = cl.map_shared_rank(sm, (unsigned)o) + 9ll * NI * os.njl * NK;
+            const int rj = jg - os.jl0 + 1, lj = side == 0 ? 0 : sl.njl + 1;  // halo row indices
+            const long long rsk = (long long)HI * (os.njl + 2), lsk = (long long)HI * (sl.njl + 2);
+            const int j = j0 + jg;
+            for (int q = threadIdx.x; q < NI * NK; q += blockDim.x) {
+                const int ii = q % NI, kk = q / NI;
+                if (((j + k0 + kk) & 1) != color) continue;  // a line of the colour just solved
+                my_ph[(ii + 1) + lj * HI + (kk + 1) * lsk] = rph[(ii + 1) + rj * HI + (kk + 1) * rsk];
+            }
+        }
+        __syncthreads();
+    }
+};
+
+// The box over the CTAs of a cluster, one slab of rows each.  With the slabs in
+// shared memory, after a colour pass each CTA copies the lines of that colour in
+// the rows either side of its slab from the CTAs that own them (distributed
+// shared memory): the next pass, of the other colour, reads exactly those.
+// Without, every CTA works in place in global memory and the cluster barrier
+// orders the passes.  Every pass ends at a cluster barrier, the last one too, so
+// that no CTA leaves while another may still read its shared memory.
+template <typename T>
+__device__ void solve_box_cluster(const Params &p, const Fields<T> &g, const Box &b, T *phi, T *sm,
+                                  int smem_elems, T *scratch, int nc, int rank)
+{
+    const int NI = b.ni_, NJ = b.nj_, NK = b.k1 - b.k0 + 1;
+    ClusterBetween<T> bw;
+    bw.sl = slab_of(NJ, rank, nc);
+    // the same decision in every CTA: the largest slab has ceil(NJ / nc) rows
+    bw.fits = slab_elems(NI, (NJ + nc - 1) / nc, NK) <= (long long)smem_elems;
+    bw.sm = sm;
+    bw.my_ph = sm + 9ll * NI * bw.sl.njl * NK;
+    bw.NI = NI; bw.NJ = NJ; bw.NK = NK; bw.HI = NI + 2; bw.nc = nc; bw.j0 = b.j0; bw.k0 = b.k0;
+    solve_box_slab<T, false>(p, g, b, bw.sl, phi, sm, bw.fits, scratch, bw);
+}
+
+// Phase helpers of the one-CTA and cluster kernels.  `t`/`nt`: this thread's
+// index and the thread count over which box items are spread.
+template <typename T>
+__device__ __forceinline__ double box_bc(const Params &p, const Fields<T> &g, Status *st, const Box &b, int ivar,
+                                         int t, int nt)
 {
     int ntop;
     const int nbc = mom_bc_items(p, st, b, ivar, ntop);
     double um = 0.0;
-    for (int q = threadIdx.x; q < nbc; q += blockDim.x) um = maxd(um, mom_bc_item<T>(p, g, st, b, ivar, q, ntop));
+    for (int q = t; q < nbc; q += nt) um = maxd(um, mom_bc_item<T>(p, g, st, b, ivar, q, ntop));
+    return um;
+}
+template <typename T>
+__device__ __forceinline__ void small_bc(const Params &p, const Fields<T> &g, Status *st, const Box &b,
+                                         int ivar, double *red_umax, double *sh)
+{
+    double um = box_bc<T>(p, g, st, b, ivar, threadIdx.x, blockDim.x);
     if (ivar == 1) {
         um = cta_max(um, sh);
         if (threadIdx.x == 0) red_umax[R_UMAX] = um;  // entry 0 of the umax region
     }
 }
 
-// cleanVelocities + applyBCs(1): one CTA.
+// Whether a box is spread over the cluster: it does not fit one CTA's shared
+// memory.  Read from the status block, so the same in every CTA.
+__device__ __forceinline__ bool spread(const Box &b, int smem_elems)
+{
+    return slab_elems(b.ni_, b.nj_, b.k1 - b.k0 + 1) > (long long)smem_elems;
+}
+
+// ---- one CTA (boxes that fit its shared memory; a no-op otherwise) --------------------
+// cleanVelocities + applyBCs(1).
 template <typename T>
-__global__ void __launch_bounds__(kMomThreads, 1) mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax)
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems)
 {
     __shared__ double sh[32];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b)) return;
+    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
     for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
         int i, j, k;
         box_cell(b, q, i, j, k);
@@ -1026,7 +1161,7 @@ __global__ void __launch_bounds__(kMomThreads, 1) mom_small_pre_kernel(Params p,
     small_bc<T>(p, g, st, b, 1, red_umax, sh);
 }
 
-// Line solve of equation ivar (1..3) on the box, then applyBCs(ivar + 1): one CTA.
+// Line solve of equation ivar (1..3) on the box, then applyBCs(ivar + 1).
 template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems, double *red_umax)
@@ -1035,13 +1170,13 @@ mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems
     __shared__ double sh[32];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b)) return;
+    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
     T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : g.wvel;
     solve_box_small<T>(p, g, b, phi, reinterpret_cast<T *>(smraw), smem_elems, scratch);
     small_bc<T>(p, g, st, b, ivar + 1, red_umax, sh);
 }
 
-// Line solve of p', correctPressure and the residual normalisation: one CTA.
+// Line solve of p', correctPressure and the residual normalisation.
 template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb)
@@ -1050,7 +1185,7 @@ mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const d
     __shared__ double scratch_r[40];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b)) return;
+    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
     solve_box_small<T>(p, g, b, g.pp, reinterpret_cast<T *>(smraw), smem_elems, scratch);
     for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
         int i, j, k;
@@ -1067,9 +1202,122 @@ mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const d
     mom_finalize_body(p, st, red, nb, 1, scratch_r);
 }
 
-// Largest box (cells) the small-box path keeps in shared memory, with room
-// for the halo of a thin box.
-template <typename T> int mom_small_capacity(const Inst<T> &I) { return (int)(I.mom_small_smem / sizeof(T) / 12); }
+// ---- one cluster of CTAs (boxes past one CTA's shared memory; a no-op otherwise) ------
+// The same three steps with the box items spread over all threads of the cluster
+// and the cluster barrier where one step reads what another CTA wrote.
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_cluster_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems)
+{
+    __shared__ double sh[32];
+    __shared__ double cmax;
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b) || !spread(b, smem_elems)) return;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int t = rank * blockDim.x + threadIdx.x, nt = nc * blockDim.x;
+    for (int q = t; q < b.n; q += nt) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        clean_cell<T>(p, g, i, j, k);
+    }
+    cl.sync();
+    double um = cta_max(box_bc<T>(p, g, st, b, 1, t, nt), sh);
+    if (threadIdx.x == 0) cmax = um;
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+        double m = cmax;
+        for (int r = 1; r < nc; ++r) m = maxd(m, *cl.map_shared_rank(&cmax, (unsigned)r));
+        red_umax[R_UMAX] = m;
+    }
+    cl.sync();  // every CTA's maximum is read before any CTA leaves
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_cluster_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b) || !spread(b, smem_elems)) return;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : g.wvel;
+    solve_box_cluster<T>(p, g, b, phi, reinterpret_cast<T *>(smraw), smem_elems, scratch, nc, rank);
+    box_bc<T>(p, g, st, b, ivar + 1, rank * blockDim.x + threadIdx.x, nc * blockDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kMomThreads, 1)
+mom_cluster_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double scratch_r[40];
+    Status *st = g.st;
+    Box b;
+    if (!get_box(st, p, b) || !spread(b, smem_elems)) return;
+    cg::cluster_group cl = cg::this_cluster();
+    const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    solve_box_cluster<T>(p, g, b, g.pp, reinterpret_cast<T *>(smraw), smem_elems, scratch, nc, rank);
+    const int t = rank * blockDim.x + threadIdx.x, nt = nc * blockDim.x;
+    cl.sync();  // p' of the whole box is in global memory
+    for (int q = t; q < b.n; q += nt) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_velocity_cell<T>(p, g, i, j, k);
+    }
+    cl.sync();
+    for (int q = t; q < b.n; q += nt) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_pressure_cell<T>(p, g, i, j, k);
+    }
+    if (rank == 0) {
+        __syncthreads();
+        mom_finalize_body(p, st, red, nb, 1, scratch_r);
+    }
+}
+
+// Largest box (cells) the one-CTA / cluster path takes: one CTA's shared memory
+// holds about smem/12 cells of a thin box; a cluster of nc CTAs about nc/2 times
+// as many (slabs of whole rows, uneven by up to one row, each with two halo rows).
+template <typename T> int mom_small_capacity(const Inst<T> &I)
+{
+    const int one = (int)(I.mom_small_smem / sizeof(T) / 12);
+    return I.mom_cluster > 1 ? one * I.mom_cluster / 2 : one;
+}
+
+// Cluster size of the small-box kernels: the largest the device schedules with
+// this shared memory, at most 16.
+template <typename T> static int max_cluster(size_t smem)
+{
+    cudaFuncSetAttribute(mom_cluster_mid_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(mom_cluster_post_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(mom_cluster_pre_kernel<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    int best = 1;
+    for (int nc : {16, 8, 4, 2}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = nc;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(nc);
+        cfg.blockDim = dim3(kMomThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (void *)mom_cluster_mid_kernel<T>, &cfg) == cudaSuccess && n > 0) {
+            best = nc;
+            break;
+        }
+        cudaGetLastError();
+    }
+    return best;
+}
 
 template <typename T> void setup_mom_small(Inst<T> &I)
 {
@@ -1080,7 +1328,29 @@ template <typename T> void setup_mom_small(Inst<T> &I)
     bytes = bytes / 16 * 16;
     cudaFuncSetAttribute(mom_small_mid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     cudaFuncSetAttribute(mom_small_post_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(mom_cluster_mid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    cudaFuncSetAttribute(mom_cluster_post_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     I.mom_small_smem = bytes;
+    I.mom_cluster = max_cluster<T>(bytes);
+}
+
+// A launch of nc CTAs forming one cluster.
+template <typename... K, typename... A>
+static void launch_cluster(void (*kern)(K...), int nc, size_t smem, cudaStream_t s, A... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = nc;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(nc);
+    cfg.blockDim = dim3(kMomThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kern, static_cast<K>(args)...);
 }
 
 // ---------------------------------------------------------------------------
@@ -1092,20 +1362,29 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
     const size_t region = (size_t)nb * R_NSLOTS;
     if (small) {
         // assemblies over a grid sized for the box capacity (one cell a thread),
-        // everything latency-bound in one CTA between them
+        // everything latency-bound in one CTA between them, or in one cluster of
+        // CTAs when the box is larger than one CTA's shared memory
         const int se = (int)(I.mom_small_smem / sizeof(T));
         const int nbs = std::max(1, std::min(nb, (mom_small_capacity<T>(I) + 255) / 256));
         const size_t rs = (size_t)nbs * R_NSLOTS;
         double *red_umax = I.red_mom + 4 * rs;
-        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax);
+        // (each step is one launch on one CTA and one on the cluster; the one whose
+        // case it is not returns at once)
+        const int nc = I.mom_cluster;
+        const size_t sm = I.mom_small_smem;
+        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax, se);
+        if (nc > 1) launch_cluster(mom_cluster_pre_kernel<T>, nc, 0, I.stream, I.p, I.g, red_umax, se);
         for (int ivar = 1; ivar <= 3; ++ivar) {
             mom_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * rs);
-            mom_small_mid_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
-                I.p, I.g, ivar, I.mom_scratch, se, red_umax);
+            mom_small_mid_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, ivar, I.mom_scratch, se, red_umax);
+            if (nc > 1)
+                launch_cluster(mom_cluster_mid_kernel<T>, nc, sm, I.stream, I.p, I.g, ivar, I.mom_scratch, se);
         }
         pp_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * rs);
-        mom_small_post_kernel<T><<<1, kMomThreads, I.mom_small_smem, I.stream>>>(
-            I.p, I.g, I.mom_scratch, se, I.red_mom, nbs);
+        mom_small_post_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, I.mom_scratch, se, I.red_mom, nbs);
+        if (nc > 1)
+            launch_cluster(mom_cluster_post_kernel<T>, nc, sm, I.stream, I.p, I.g, I.mom_scratch, se,
+                           (const double *)I.red_mom, nbs);
         return;
     }
     launch_box_tickets<T>(I);

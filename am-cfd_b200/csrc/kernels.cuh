@@ -98,6 +98,7 @@ struct Inst {
     AsmMaps asm_maps[2];      // by property parity
     T *mom_scratch = nullptr; // one field: line-solve scratch of the small-box momentum path
     size_t mom_small_smem = 0;  // its dynamic shared memory
+    int mom_cluster = 1;        // CTAs of the cluster that takes boxes past one CTA's shared memory
     const T *asm_diff_a = nullptr;  // diff_cur at parity 0
     // updateSolutions inputs of the current step (powder bed)
     double trackindx = 1.0;

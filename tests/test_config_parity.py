@@ -110,6 +110,15 @@ def test_production_path_melt_pool_within_one_cell(name, tmp_path_factory):
     s.close()
 
 
+def _one_cta(r, nk, elem):
+    """Whether the momentum box of report r fits the shared memory of one CTA of
+    the box solve (200 KiB: nine arrays of its cells and phi with a halo)."""
+    ni = r["iend"] - r["istat"] - 1
+    nj = r["jend"] - r["jstat"] + 1
+    nkb = nk - 2 - r["kstat"] + 1
+    return 9 * ni * nj * nkb + (ni + 2) * (nj + 2) * (nkb + 2) <= 204800 // elem
+
+
 def test_small_box_two_lines_per_group_matches_grid_path(tmp_path):
     """The FP32 register sweep of the one-CTA momentum path keeps one line of a
     colour per 8-lane group in registers; with 65 to 128 lines of a colour a group
@@ -121,19 +130,49 @@ def test_small_box_two_lines_per_group_matches_grid_path(tmp_path):
     d = amcfd.Deck(D.config1(steps=20).write(str(tmp_path)))
     a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1, small_box=0)
     b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1, small_box=1)
-    capacity = 4266  # cells of the FP32 one-CTA path (mom_small_capacity)
     two = 0
     for q in range(20):
         ra, rb = a.step(), b.step()
         lines = (rb["jend"] - rb["jstat"] + 1) * (d.dims[2] - 2 - rb["kstat"] + 1)
         per_colour = (lines + 1) // 2
-        if 64 < per_colour <= 128 and 0 < rb["momentum_cells"] <= capacity:
+        if 64 < per_colour <= 128 and 0 < rb["momentum_cells"] and _one_cta(rb, d.dims[2], 4):
             two += 1
             for f in ("temp", "uvel", "vvel", "wvel", "pressure"):
                 x, y = b.get(f), a.get(f)
                 if np.linalg.norm(y) > 0:
                     assert rel_l2(x, y) < 1e-3, (q + 1, f, rel_l2(x, y))
     assert two > 0, "the box never had 65-128 lines of one colour within the small-box capacity"
+    assert b.launches < a.launches
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("prec,steps", [(0, 24), (1, 45)])
+def test_cluster_box_momentum_matches_grid_path(prec, steps, tmp_path):
+    """A melt-pool box larger than one CTA's shared memory is spread over a
+    cluster of CTAs (slabs of rows, the rows next to a slab exchanged through
+    distributed shared memory after every colour pass).  On the config-1 deck the
+    box outgrows one CTA within the first steps (FP64 sooner than FP32); those
+    steps agree with the multi-kernel momentum path to 1e-6 (FP64, with the same
+    outer-iteration counts) / 1e-3 (FP32) relative L2."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.config1(steps=steps).write(str(tmp_path)))
+    a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1, small_box=0)
+    b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1, small_box=1)
+    tol = 1e-6 if prec == 0 else 1e-3
+    spread = 0
+    for q in range(steps):
+        ra, rb = a.step(), b.step()
+        if prec == 0:
+            assert ra["niter"] == rb["niter"], (q + 1, ra["niter"], rb["niter"])
+        if rb["momentum_cells"] > 0 and not _one_cta(rb, d.dims[2], 8 if prec == 0 else 4):
+            spread += 1
+            for f in ("temp", "uvel", "vvel", "wvel", "pressure"):
+                x, y = b.get(f), a.get(f)
+                if np.linalg.norm(y) > 0:
+                    assert rel_l2(x, y) < tol, (q + 1, f, rel_l2(x, y))
+    assert spread > 0, "the box never outgrew one CTA"
     assert b.launches < a.launches
     a.close()
     b.close()
