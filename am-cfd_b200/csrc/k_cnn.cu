@@ -21,8 +21,8 @@
 // set of the layer stays in shared memory.  Tiles are double-buffered: the
 // gather of tile q+1 and the epilogue of tile q overlap the MMAs.  The same
 // kernel computes input gradients (transposed, tap-reversed weights) with the
-// ReLU derivative applied in the epilogue.  Weight gradients are reduced on
-// the CUDA cores (FP32).
+// ReLU derivative applied in the epilogue.  Weight gradients are a third
+// tensor-core contraction, over cells (wgrad_tc_kernel).
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -37,11 +37,9 @@
 namespace amcfd {
 namespace cnn {
 
-constexpr int kThreads = 256;      // weight-gradient kernel
 constexpr int kConvThreads = 160;  // convolution kernel: four epilogue warps + one TMA/MMA warp
 constexpr int kM = 128;  // cells per tile
 constexpr int kR = 136;  // rows per (dk, dj) group: 128 + 2 halo, rounded up to 8
-constexpr int kG = 9;    // (dk, dj) groups
 constexpr int kLayers = 4;
 constexpr int kCin[kLayers] = {16, 32, 32, 32};
 constexpr int kCout[kLayers] = {32, 32, 32, 16};
@@ -364,59 +362,175 @@ __global__ void pack_bwd_kernel(const float *w, __nv_bfloat16 *wp, int cin, int 
     }
 }
 
-// dW[t][cout][cin] = sum over interior cells c of dz[c][cout] * x[c + off(t)][cin],
-// db[cout] = sum of dz[c][cout]; per-CTA partials, reduced in a fixed order.
-template <int CIN, int COUT>
-__global__ void __launch_bounds__(kThreads, 1) wgrad_kernel(const __nv_bfloat16 *x, const __nv_bfloat16 *dz,
-                                                           long long ncell, int ni, int nj, float *part)
+// ---- weight gradients on the tensor cores ----------------------------------------
+// Per layer dW[t][co][ci] = sum over cells c of dz[c][co] x[c + off(t)][ci] (dz is
+// zero on boundary nodes), with off(t) = (dk-1) plane + (dj-1) ni + (di-1) for
+// t = 9 dk + 3 dj + di.  As D[m][n] = sum_k A[m][k] B[n][k] over K = cells: the CTAs
+// of group dk (blockIdx.y) take rows m = (di, co), A[(di, co)][k] = dz[c - di + 1][co],
+// and columns n = (dj, ci), B[(dj, ci)][k] = x[c + (dk-1) plane + (dj-1) ni][ci], for
+// the cells c of their chunks; then D[(di, co)][(dj, ci)] = dW[9 dk + 3 dj + di][co][ci]
+// (the three di taps share the x rows and differ by the shift of dz).  Chunks of 64
+// cells cover c = -1 .. ncell, so every shifted pair is counted once.  M = 128 (rows
+// past 3 COUT are zero), N = 3 CIN, FP32 accumulators in tensor memory across all
+// chunks of the CTA, operands transposed into the K-major no-swizzle layout by the
+// CUDA cores (element (r, k) at (k/8) LBO + (r/8) 128 + (r%8) 16 + (k%8) 2 bytes,
+// LBO = rows x 16), two buffers so that staging chunk q+1 overlaps the MMAs of q.
+constexpr int kWgThreads = 128;
+constexpr int kWgK = 64;  // cells per chunk
+
+template <int CIN, int COUT> struct WgSmem {
+    static constexpr int NB = 3 * CIN;                 // rows of B
+    static constexpr int A_BYTES = (kWgK / 8) * 128 * 16;
+    static constexpr int B_BYTES = (kWgK / 8) * NB * 16;
+    static constexpr size_t BYTES = 2 * (size_t)(A_BYTES + B_BYTES) + 8 * 2 + 16 + 1024;
+    static constexpr uint32_t COLS = NB <= 32 ? 32 : NB <= 64 ? 64 : 128;  // TMEM columns
+};
+
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int lbo)
 {
+    return (uint32_t)((k >> 3) * lbo + ((r >> 3) << 7) + ((r & 7) << 4) + ((k & 7) << 1));
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kWgThreads, 3) wgrad_tc_kernel(const __nv_bfloat16 *x, const __nv_bfloat16 *dz,
+                                                               long long ncell, int ni, int nj, float *part,
+                                                               int *err)
+{
+    using S = WgSmem<CIN, COUT>;
     constexpr int NW = 27 * COUT * CIN;
-    constexpr int PER = (NW + kThreads - 1) / kThreads;
-    constexpr int TC = 32;  // cells per step
-    __shared__ float sx[kG][TC + 2][CIN];
-    __shared__ float sdz[TC][COUT];
+    constexpr int NB = S::NB;
+    constexpr int LBO_A = 128 * 16, LBO_B = NB * 16;
+    extern __shared__ __align__(1024) unsigned char smraw[];
+    unsigned char *base = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    unsigned char *Abuf[2] = {base, base + S::A_BYTES};
+    unsigned char *Bbuf[2] = {base + 2 * S::A_BYTES, base + 2 * S::A_BYTES + S::B_BYTES};
+    uint64_t *done = reinterpret_cast<uint64_t *>(base + 2 * (S::A_BYTES + S::B_BYTES));
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(done + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int dk = blockIdx.y;
     const long long plane = (long long)ni * nj;
-    float acc[PER];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) acc[q] = 0.f;
-    float bacc = 0.f;
-    const long long nsteps = (ncell + TC - 1) / TC;
-    for (long long st = blockIdx.x; st < nsteps; st += gridDim.x) {
-        const long long c0 = st * TC;
-        for (int idx = threadIdx.x; idx < kG * (TC + 2) * CIN; idx += blockDim.x) {
-            const int cc = idx % CIN, rest = idx / CIN, r = rest % (TC + 2), g = rest / (TC + 2);
-            const int dk = g / 3 - 1, dj = g % 3 - 1;
-            const long long s = c0 - 1 + r + dk * plane + (long long)dj * ni;
-            sx[g][r][cc] = (s >= 0 && s < ncell) ? __bfloat162float(x[s * CIN + cc]) : 0.f;
+    const long long xoff = (long long)(dk - 1) * plane;
+    const long long nch = (ncell + 2 + kWgK - 1) / kWgK;  // chunks over c = -1 .. ncell
+    const long long nmy = blockIdx.x < nch ? (nch - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    if (tid == 0) {
+        mbar_init(&done[0]);
+        mbar_init(&done[1]);
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tslot)), "r"(S::COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    // rows 3 COUT .. 127 of A stay zero
+    for (int q = tid; q < 2 * S::A_BYTES / 16; q += kWgThreads)
+        reinterpret_cast<uint4 *>(base)[q] = make_uint4(0u, 0u, 0u, 0u);
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tbase = *tslot;
+    constexpr uint32_t idesc = idesc_bf16<NB>();
+    bool ok = true;
+    for (long long it = 0; it < nmy; ++it) {
+        const int b = (int)(it & 1);
+        if (it >= 2 && !mbar_try(&done[b], (uint32_t)(((it - 2) >> 1) & 1), kSpinLimit)) {
+            ok = false;  // (the loop ends below for every thread: the flag is made uniform)
         }
-        for (int idx = threadIdx.x; idx < TC * COUT; idx += blockDim.x) {
-            const int cc = idx % COUT, r = idx / COUT;
-            const long long c = c0 + r;
-            sdz[r][cc] = (c < ncell) ? __bfloat162float(dz[c * COUT + cc]) : 0.f;
+        if (!__syncthreads_and(ok)) {
+            ok = false;
+            break;
         }
-        __syncthreads();
+        const long long c0 = (it * gridDim.x + blockIdx.x) * kWgK - 1;
+        unsigned char *A = Abuf[b], *Bm = Bbuf[b];
+        // A: dz rows c0-1 .. c0+64, each row to the three di rows it feeds
+        constexpr int GA = COUT / 8, NA = (kWgK + 2) * GA;
+        for (int q = tid; q < NA; q += kWgThreads) {
+            const int r = q / GA, g = q - r * GA;
+            const long long c = c0 - 1 + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (c >= 0 && c < ncell) v = *reinterpret_cast<const uint4 *>(dz + c * COUT + 8 * g);
+            const unsigned short *h = reinterpret_cast<const unsigned short *>(&v);
 #pragma unroll
-        for (int q = 0; q < PER; ++q) {
-            const int o = threadIdx.x + q * kThreads;
-            if (o < NW) {
-                const int ci = o % CIN, rest = o / CIN, co = rest % COUT, t = rest / COUT;
-                const int g = t / 3, di = t % 3;
-                float a = acc[q];
-                for (int r = 0; r < TC; ++r) a = fmaf(sdz[r][co], sx[g][r + di][ci], a);
-                acc[q] = a;
+            for (int di = 0; di < 3; ++di) {
+                const int k = r - 2 + di;
+                if (k < 0 || k >= kWgK) continue;
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    *reinterpret_cast<unsigned short *>(A + kmajor_off(di * COUT + 8 * g + e, k, LBO_A)) = h[e];
             }
         }
-        if (threadIdx.x < COUT)
-            for (int r = 0; r < TC; ++r) bacc += sdz[r][threadIdx.x];
-        __syncthreads();
-    }
-    float *p = part + (size_t)blockIdx.x * (NW + COUT);
+        // B: x rows of the three (dk, dj) row groups
+        constexpr int GB = CIN / 8, NBI = 3 * kWgK * GB;
+        for (int q = tid; q < NBI; q += kWgThreads) {
+            const int g = q % GB, r = q / GB, k = r % kWgK, dj = r / kWgK;
+            const long long c = c0 + k + xoff + (long long)(dj - 1) * ni;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (c >= 0 && c < ncell) v = *reinterpret_cast<const uint4 *>(x + c * CIN + 8 * g);
+            const unsigned short *h = reinterpret_cast<const unsigned short *>(&v);
 #pragma unroll
-    for (int q = 0; q < PER; ++q) {
-        const int o = threadIdx.x + q * kThreads;
-        if (o < NW) p[o] = acc[q];
+            for (int e = 0; e < 8; ++e)
+                *reinterpret_cast<unsigned short *>(Bm + kmajor_off(dj * CIN + 8 * g + e, k, LBO_B)) = h[e];
+        }
+        fence_proxy_async();  // the generic-proxy stores, seen by the tensor cores
+        tc_before_sync();
+        __syncthreads();
+        if (tid == 0) {
+            tc_after_sync();
+#pragma unroll
+            for (int s = 0; s < kWgK / 16; ++s) {
+                const uint64_t a = smem_desc(smem_u32(A) + 2 * s * LBO_A, LBO_A, 128);
+                const uint64_t bd = smem_desc(smem_u32(Bm) + 2 * s * LBO_B, LBO_B, 128);
+                mma_bf16(tbase, a, bd, idesc, (it == 0 && s == 0) ? 0u : 1u);
+            }
+            mma_commit(&done[b]);
+        }
     }
-    if (threadIdx.x < COUT) p[NW + threadIdx.x] = bacc;
+    // the last commit covers every MMA of the CTA
+    if (nmy > 0 && !mbar_try(&done[(int)((nmy - 1) & 1)], (uint32_t)(((nmy - 1) >> 1) & 1), kSpinLimit))
+        ok = false;
+    if (!ok && tid == 0) atomicExch(err, AMCFD_E_TIMEOUT);
+    tc_after_sync();
+    float *pp = part + (size_t)blockIdx.x * (NW + COUT);
+    const int m = 32 * warp + lane;  // accumulator row = TMEM lane
+#pragma unroll
+    for (int n0 = 0; n0 < NB; n0 += 16) {
+        uint32_t r[16];
+        tmem_ld<16>(tbase + ((uint32_t)(32 * warp) << 16) + (uint32_t)n0, r);
+        tmem_wait_ld();
+        if (m < 3 * COUT) {
+            const int di = m / COUT, co = m - di * COUT;
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int n = n0 + e, dj = n / CIN, ci = n - dj * CIN;
+                const int t = 9 * dk + 3 * dj + di;
+                pp[((size_t)t * COUT + co) * CIN + ci] = nmy > 0 ? __uint_as_float(r[e]) : 0.f;
+            }
+        }
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(S::COLS) : "memory");
+}
+
+// db[co] = sum over cells of dz[c][co]: CTA x sums its contiguous range of cells,
+// in a fixed order, into the bias slots of its partial row.
+template <int COUT>
+__global__ void __launch_bounds__(256) bgrad_kernel(const __nv_bfloat16 *dz, long long ncell, float *part, int nw)
+{
+    __shared__ float sh[256];
+    const long long a = ncell * blockIdx.x / gridDim.x, e = ncell * (blockIdx.x + 1) / gridDim.x;
+    const int co = threadIdx.x % COUT, lanes = 256 / COUT;
+    float acc = 0.f;
+    for (long long c = a + threadIdx.x / COUT; c < e; c += lanes) acc += __bfloat162float(dz[c * COUT + co]);
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < COUT) {
+        float s = 0.f;
+        for (int q = 0; q < lanes; ++q) s += sh[q * COUT + threadIdx.x];
+        part[(size_t)blockIdx.x * (nw + COUT) + nw + threadIdx.x] = s;
+    }
 }
 
 __global__ void reduce_parts_kernel(const float *part, int nparts, int n, float *out)
@@ -514,12 +628,28 @@ static int conv(int cin, int cout, ConvArgs a, int grid, cudaStream_t s)
     return 0;
 }
 
-static void wgrad(int cin, int cout, const __nv_bfloat16 *x, const __nv_bfloat16 *dz, long long ncell, int ni,
-                  int nj, float *part, int grid, cudaStream_t s)
+template <int CIN, int COUT> void set_wgrad_smem()
 {
-    if (cin == 16 && cout == 32) wgrad_kernel<16, 32><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
-    else if (cin == 32 && cout == 32) wgrad_kernel<32, 32><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
-    else if (cin == 32 && cout == 16) wgrad_kernel<32, 16><<<grid, kThreads, 0, s>>>(x, dz, ncell, ni, nj, part);
+    cudaFuncSetAttribute(wgrad_tc_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)WgSmem<CIN, COUT>::BYTES);
+}
+
+template <int CIN, int COUT>
+static void launch_wgrad(const __nv_bfloat16 *x, const __nv_bfloat16 *dz, long long ncell, int ni, int nj,
+                         float *part, int grid, int *err, cudaStream_t s)
+{
+    wgrad_tc_kernel<CIN, COUT><<<dim3(grid, 3), kWgThreads, WgSmem<CIN, COUT>::BYTES, s>>>(x, dz, ncell, ni, nj,
+                                                                                          part, err);
+    bgrad_kernel<COUT><<<grid, 256, 0, s>>>(dz, ncell, part, 27 * CIN * COUT);
+}
+
+// Per-CTA partial weight and bias gradients of one layer (grid rows of part).
+static void wgrad(int cin, int cout, const __nv_bfloat16 *x, const __nv_bfloat16 *dz, long long ncell, int ni,
+                  int nj, float *part, int grid, int *err, cudaStream_t s)
+{
+    if (cin == 16 && cout == 32) launch_wgrad<16, 32>(x, dz, ncell, ni, nj, part, grid, err, s);
+    else if (cin == 32 && cout == 32) launch_wgrad<32, 32>(x, dz, ncell, ni, nj, part, grid, err, s);
+    else if (cin == 32 && cout == 16) launch_wgrad<32, 16>(x, dz, ncell, ni, nj, part, grid, err, s);
 }
 
 }  // namespace cnn
@@ -628,6 +758,9 @@ int amcfd_net_create(int device, unsigned long long seed, amcfd_net **out)
     set_conv_smem<32, 32>();
     set_conv_smem<32, 16>();
     set_conv_smem<16, 16>();
+    set_wgrad_smem<16, 32>();
+    set_wgrad_smem<32, 32>();
+    set_wgrad_smem<32, 16>();
     // initialisation: uniform(-a, a), a = sqrt(6 / fan_in) (ReLU layers), the last
     // layer scaled by 0.1 so that the first predictions are near zero; padding 0
     std::vector<float> h(np, 0.f);
@@ -767,7 +900,8 @@ int amcfd_net_backward(amcfd_net *net, const float *target_dev, double *loss)
     int cur = 0;
     for (int l = kLayers - 1; l >= 0; --l) {
         const size_t nw = (size_t)27 * kCin[l] * kCout[l];
-        wgrad(kCin[l], kCout[l], net->act[l], net->grad[cur], n, ni, nj, net->part, net->sm, net->stream);
+        wgrad(kCin[l], kCout[l], net->act[l], net->grad[cur], n, ni, nj, net->part, net->sm, net->errd,
+              net->stream);
         reduce_parts_kernel<<<64, 256, 0, net->stream>>>(net->part, net->sm, (int)(nw + kCout[l]),
                                                           net->g + layer_off(l));
         if (l > 0) {
