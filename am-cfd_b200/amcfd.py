@@ -82,7 +82,8 @@ class AmcfdReport(C.Structure):
 class AmcfdOptions(C.Structure):
     _fields_ = [("device", _I), ("order", _I), ("precision", _I), ("use_graphs", _I),
                 ("check_finite", _I), ("no_small_box", _I), ("host_loop", _I),
-                ("wait_polls", _I), ("reserved", _I * 5)]
+                ("wait_polls", _I), ("autotune", _I), ("asm_kseg", _I), ("sweep_warps", _I),
+                ("reserved", _I * 2)]
 
 
 class AmcfdError(RuntimeError):
@@ -130,6 +131,7 @@ def lib() -> C.CDLL:
             L.amcfd_profile.argtypes = [VP, _I]
             L.amcfd_free_surface.argtypes = [VP, P(AmcfdFreeSurface)]
             L.amcfd_run_steps.argtypes = [VP, _I, P(AmcfdReport), P(_D)]
+            L.amcfd_tuning.argtypes = [VP, P(_I), P(_I), P(_D)]
             L.amcfd_kernel_launches.argtypes = [VP]
             L.amcfd_kernel_launches.restype = C.c_longlong
             L.amcfd_run_batch.argtypes = [P(VP), _I, _I, _I, P(AmcfdReport), P(_I)]
@@ -312,13 +314,15 @@ class Solver:
 
     def __init__(self, deck: Deck, order: int = ORDER_EXACT, precision: int = PREC_FP64,
                  device: int = 0, use_graphs: int = 0, check_finite: int = 1,
-                 small_box: int = 1, host_loop: int = 0, wait_polls: int = 0):
+                 small_box: int = 1, host_loop: int = 0, wait_polls: int = 0, autotune: int = 0,
+                 asm_kseg: int = 0, sweep_warps: int = 0):
         L = lib()
         self.deck = deck  # keeps toolpath storage alive
         opts = AmcfdOptions(device=device, order=order, precision=precision,
                             use_graphs=use_graphs, check_finite=check_finite,
                             no_small_box=0 if small_box else 1, host_loop=host_loop,
-                            wait_polls=wait_polls)
+                            wait_polls=wait_polls, autotune=autotune, asm_kseg=asm_kseg,
+                            sweep_warps=sweep_warps)
         self._h = C.c_void_p()
         rc = L.amcfd_create(C.byref(deck.params), C.byref(opts), C.byref(self._h))
         if rc != 0:
@@ -366,6 +370,15 @@ class Solver:
 
     def profile(self, enable: bool = True):
         self._check(lib().amcfd_profile(self._h, 1 if enable else 0))
+
+    def tuning(self) -> Dict:
+        """Launch shapes in use (amcfd_tuning): assembly planes per CTA, sweep lines
+        per CTA and, after autotuning, the candidates' times in ms."""
+        a, w = _I(), _I()
+        t = (_D * 6)()
+        self._check(lib().amcfd_tuning(self._h, C.byref(a), C.byref(w), t))
+        return {"asm_kseg": a.value, "sweep_warps": w.value,
+                "asm_ms": {4: t[0], 8: t[1], 16: t[2]}, "sweep_ms": {2: t[3], 4: t[4], 8: t[5]}}
 
     @property
     def launches(self) -> int:

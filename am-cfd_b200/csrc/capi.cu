@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -22,8 +23,8 @@
 namespace amcfd {
 template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
 template <typename T> void set_sweep_smem_limit(size_t smem);
-template <typename T> bool set_rounds_smem_limit(const Params &p);
-dim3 energy_assemble_grid(const Params &p);
+template <typename T> int set_rounds_smem_limit(const Params &p);
+dim3 energy_assemble_grid(const Params &p, int kseg);
 template <typename T> int h2t_blocks_per_sm();
 template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
                                              long long rows, int sm_count, cudaStream_t s);
@@ -116,6 +117,8 @@ struct amcfd_ctx {
     cudaGraphExec_t gloop[2] = {};
     bool host_loop = false;        // drive the outer iterations from the host even with graphs
     long long wait_polls = 0;      // budget of the exact-order sweep's line waits (0: default)
+    int autotune = 0, asm_kseg = 0, sweep_warps = 0;  // launch shapes: tuned, or pinned (0: default)
+    double tune_ms[6] = {0};       // the autotuner's measured candidates
     int mom_cluster = 1;           // CTAs of the cluster momentum path (1: none)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
@@ -333,7 +336,7 @@ static int set_active_nk(amcfd_ctx *ctx, Inst<T> &I, int nk)
                                                std::to_string(nk) + " of " + std::to_string(p.nk_alloc) + ")");
     CK(cudaStreamSynchronize(ctx->stream));
     p.nk = nk; p.nkm1 = nk - 1; p.nkm2 = nk - 2;
-    I.asm_grid = energy_assemble_grid(p);
+    I.asm_grid = energy_assemble_grid(p, I.asm_kseg);
     I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
     I.g.npart = I.asm_grid.y * I.asm_grid.z;
     I.max_lines = (p.nj - 2) * (p.nk - 2);
@@ -436,18 +439,27 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     I.order = ctx->order;
     I.nb_las = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 255) / 256));
     I.nb_bc = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 2 * p.nk * (p.ni + p.nj) + 255) / 256));
-    I.asm_grid = energy_assemble_grid(p);
+    I.asm_kseg = ctx->asm_kseg;
+    I.sweep_warps = ctx->sweep_warps > 0 ? ctx->sweep_warps : 4;
+    I.asm_grid = energy_assemble_grid(p, I.asm_kseg);
     I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
-    // the assembly's per-CTA buffers hold the largest grid of any active height
+    // the assembly's per-CTA buffers hold the largest grid of any active height and
+    // of any shape the autotuner may pick
     int nb_asm_max = I.nb_asm, npart_max = I.asm_grid.y * I.asm_grid.z;
-    if (p.powder)
-        for (int nka = ctx->nk_active; nka <= p.nk; nka += std::max(1, q.ncvzlayer)) {
+    for (int nka = ctx->nk_active; nka <= p.nk; nka += std::max(1, q.ncvzlayer)) {
+        if (!p.powder) nka = p.nk;
+        const int cand[4] = {I.asm_kseg, 4, 8, 16};
+        for (int c = 0; c < 4; ++c) {
+            const int seg = cand[c];
+            if (c > 0 && !ctx->autotune) continue;
             Params pa = p;
             pa.nk = nka;
-            const dim3 ga = energy_assemble_grid(pa);
+            const dim3 ga = energy_assemble_grid(pa, seg);
             nb_asm_max = std::max(nb_asm_max, (int)(ga.x * ga.y * ga.z));
             npart_max = std::max(npart_max, (int)(ga.y * ga.z));
         }
+        if (!p.powder) break;
+    }
     I.nb_h2t = std::max(1, std::min(I.sm_count * h2t_blocks_per_sm<T>(), (int)((n3 + 255) / 256)));
     I.nb_mom = I.sm_count * 2;
     I.grid_1d = std::max(1, std::min(I.sm_count * 8, (int)((n3 + 255) / 256)));
@@ -500,8 +512,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         for (float **f : {&d.an, &d.as, &d.ae, &d.aw, &d.at, &d.ab, &d.ap, &d.su, &d.pr, &d.cf, &d.iden,
                           &d.delta})
             if ((rc = alloc3<float>(ctx, f, n3))) return rc;
-        if (!set_rounds_smem_limit<float>(p))
-            return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
+        I.sweep_warps_max = std::min(I.sweep_warps_max, set_rounds_smem_limit<float>(p));
+        if (I.sweep_warps_max < 2) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
         I.dc_on = true;
     }
     I.check_finite = 0;
@@ -509,7 +521,11 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
     I.line_smem = (size_t)I.exact_warps * 8 * p.nip * sizeof(T) + (size_t)I.exact_warps * 8;
     set_sweep_smem_limit<T>(I.line_smem);
-    if (!set_rounds_smem_limit<T>(p)) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
+    I.sweep_warps_max = set_rounds_smem_limit<T>(p);
+    if (I.sweep_warps_max < 2) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
+    if (ctx->sweep_warps > I.sweep_warps_max)
+        return fail(ctx, AMCFD_E_CAPACITY, "sweep_warps beyond what the x-lines leave room for");
+    I.sweep_warps = std::min(I.sweep_warps, I.sweep_warps_max);
     int bps = exact_sweep_blocks_per_sm<T>(I.exact_warps, I.line_smem);
     // A wave of the exact-order sweep holds about 2(nj-2)/3 lines; about three
     // waves of lines in flight keep the dependency chain fed without flooding L2
@@ -1161,8 +1177,88 @@ static void ws_after(amcfd_ctx *ctx, Inst<T> &I)
     ctx->launches += 1;
 }
 
+// ---- autotuner ------------------------------------------------------------------------
+// At creation (opt-in): the energy assembly with 4, 8 and 16 planes per CTA and a
+// factorising plus a plain red-black pass with 2, 4 and 8 lines per CTA, each timed
+// with CUDA events on the context stream (one untimed round, then the minimum of
+// three rounds in rotated order) on this grid; the fastest of each is kept unless
+// the options pin it.  The assembly runs in place (everything it writes is formed
+// again by the first outer iteration); the sweep passes run on a scratch field.
+template <typename T>
+static int autotune(amcfd_ctx *ctx, Inst<T> &I)
+{
+    cudaEvent_t e0 = ctx->ev[14], e1 = ctx->ev[15];
+    const int segs[3] = {4, 8, 16}, warps[3] = {2, 4, 8};
+    float best_asm[3], best_sw[3];
+    for (int c = 0; c < 3; ++c) best_asm[c] = best_sw[c] = INFINITY;
+    auto set_seg = [&](int seg) {
+        I.asm_kseg = seg;
+        I.asm_grid = energy_assemble_grid(I.p, seg);
+        I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
+        I.g.npart = I.asm_grid.y * I.asm_grid.z;
+    };
+    auto sweep_probe = [&](int w) {
+        if constexpr (sizeof(T) == sizeof(double)) {
+            if (I.dc_on) {
+                launch_dc_sweep_probe(I, w);
+                return;
+            }
+        }
+        launch_sweep_probe<T>(I, I.mom_scratch, w);
+    };
+    for (int round = 0; round < 4; ++round)
+        for (int q = 0; q < 3; ++q) {
+            const int c = (q + round) % 3;
+            float ms = 0.f;
+            if (!ctx->asm_kseg) {
+                set_seg(segs[c]);
+                CK(cudaEventRecord(e0, ctx->stream));
+                launch_energy_assemble<T>(I);
+                CK(cudaEventRecord(e1, ctx->stream));
+                CK(cudaEventSynchronize(e1));
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (round > 0) best_asm[c] = std::min(best_asm[c], ms);
+            }
+            if (!ctx->sweep_warps && ctx->order == AMCFD_ORDER_REDBLACK && warps[c] <= I.sweep_warps_max) {
+                CK(cudaEventRecord(e0, ctx->stream));
+                sweep_probe(warps[c]);
+                CK(cudaEventRecord(e1, ctx->stream));
+                CK(cudaEventSynchronize(e1));
+                CK(cudaEventElapsedTime(&ms, e0, e1));
+                if (round > 0) best_sw[c] = std::min(best_sw[c], ms);
+            }
+        }
+    CK(cudaGetLastError());
+    if (!ctx->asm_kseg) {
+        const int c = (int)(std::min_element(best_asm, best_asm + 3) - best_asm);
+        set_seg(segs[c]);
+        ctx->asm_kseg = segs[c];
+        for (int q = 0; q < 3; ++q) ctx->tune_ms[q] = best_asm[q];
+    }
+    if (!ctx->sweep_warps && ctx->order == AMCFD_ORDER_REDBLACK) {
+        const int c = (int)(std::min_element(best_sw, best_sw + 3) - best_sw);
+        I.sweep_warps = warps[c];
+        ctx->sweep_warps = warps[c];
+        for (int q = 0; q < 3; ++q) ctx->tune_ms[3 + q] = best_sw[q];
+    }
+    ctx->launches += 4 * 3 * 3;
+    return 0;
+}
+
 // =========================================================================================
 extern "C" {
+
+int amcfd_tuning(const amcfd_ctx *ctx, int *asm_kseg, int *sweep_warps, double *times)
+{
+    if (!ctx) return AMCFD_E_ARG;
+    const int seg = ctx->precision == AMCFD_PREC_FP64 ? ctx->I64.asm_kseg : ctx->I32.asm_kseg;
+    const int w = ctx->precision == AMCFD_PREC_FP64 ? ctx->I64.sweep_warps : ctx->I32.sweep_warps;
+    if (asm_kseg) *asm_kseg = seg;
+    if (sweep_warps) *sweep_warps = w;
+    if (times)
+        for (int q = 0; q < 6; ++q) times[q] = ctx->tune_ms[q];
+    return 0;
+}
 
 int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ctx **out)
 {
@@ -1194,6 +1290,13 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->host_loop = opts->host_loop != 0;
         if (opts->wait_polls < 0) return fail(ctx, AMCFD_E_ARG, "wait_polls must not be negative");
         ctx->wait_polls = opts->wait_polls;
+        if (opts->asm_kseg != 0 && opts->asm_kseg != 4 && opts->asm_kseg != 8 && opts->asm_kseg != 16)
+            return fail(ctx, AMCFD_E_ARG, "asm_kseg must be 0, 4, 8 or 16");
+        if (opts->sweep_warps != 0 && opts->sweep_warps != 2 && opts->sweep_warps != 4 && opts->sweep_warps != 8)
+            return fail(ctx, AMCFD_E_ARG, "sweep_warps must be 0, 2, 4 or 8");
+        ctx->autotune = opts->autotune != 0;
+        ctx->asm_kseg = opts->asm_kseg;
+        ctx->sweep_warps = opts->sweep_warps;
     }
     if (ctx->order != AMCFD_ORDER_EXACT && ctx->order != AMCFD_ORDER_REDBLACK)
         return fail(ctx, AMCFD_E_ARG, "unknown line-sweep order");
@@ -1267,6 +1370,10 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
     int cf = opts ? opts->check_finite : 0;
     ctx->I64.check_finite = cf;
     ctx->I32.check_finite = cf;
+    if (ctx->autotune) {
+        rc = ctx->precision == AMCFD_PREC_FP64 ? autotune<double>(ctx, ctx->I64) : autotune<float>(ctx, ctx->I32);
+        if (rc) return rc;
+    }
     if (p.steady) laser_coords(ctx);  // main.cpp:105-106
     return 0;
 }

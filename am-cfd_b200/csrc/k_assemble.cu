@@ -20,6 +20,8 @@
 // widths, formed in FP64 in the reference's order.  The arithmetic is the
 // reference's expression by expression; the FP32 build evaluates properties
 // and divisions in FP32.
+#include <algorithm>
+
 #include "kernels.cuh"
 #include "async.cuh"
 
@@ -428,12 +430,16 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
 }
 
 // k-segments: long enough to amortise the two-plane prologue, short enough to
-// give every SM several CTAs (at least 4 x 148 tiles x segments).
-dim3 energy_assemble_grid(const Params &p)
+// give every SM several CTAs (at least 4 x 148 tiles x segments); kseg > 0 takes
+// that segment length instead (4, 8 or 16 planes: the autotuner's candidates).
+dim3 energy_assemble_grid(const Params &p, int kseg)
 {
     const int tiles = ((p.ni + kTX - 1) / kTX) * ((p.nj + kTY - 1) / kTY);
     int seg = kKSEG;
-    while (seg > 4 && tiles * ((p.nk + seg - 1) / seg) < 4 * 148) seg /= 2;
+    if (kseg > 0)
+        seg = std::min(kseg, kKSEG);
+    else
+        while (seg > 4 && tiles * ((p.nk + seg - 1) / seg) < 4 * 148) seg /= 2;
     return dim3((p.ni + kTX - 1) / kTX, (p.nj + kTY - 1) / kTY, (p.nk + seg - 1) / seg);
 }
 

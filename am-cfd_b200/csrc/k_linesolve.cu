@@ -434,7 +434,7 @@ template <typename T>
 __device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d);
 
 template <typename T, bool FACTOR>
-__global__ void __launch_bounds__(128) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
+__global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
                                                               int correct)
 {
     constexpr int V = 16 / (int)sizeof(T);
@@ -842,18 +842,30 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
             for (int color = 0; color < 2; ++color)
                 sweep_rb_kernel<T, true><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
     } else {
-        // whole domain: 4 warps per CTA, one line per warp
+        // whole domain: one line per warp, sweep_warps warps per CTA
+        const int w = I.sweep_warps;
         const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
-        const int grid = std::max(1, (lines + 3) / 4);
-        const size_t rs = rounds_smem<T>(I.p, 4);
+        const int grid = std::max(1, (lines + w - 1) / w);
+        const size_t rs = rounds_smem<T>(I.p, w);
         for (int color = 0; color < 2; ++color)
-            sweep_rb_rounds_kernel<T, true><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color, color == 0);
+            sweep_rb_rounds_kernel<T, true><<<grid, 32 * w, rs, I.stream>>>(I.p, I.g, phi, color, color == 0);
         for (int sweep = 1; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color)
-                sweep_rb_rounds_kernel<T, false><<<grid, 128, rs, I.stream>>>(I.p, I.g, phi, color, 0);
+                sweep_rb_rounds_kernel<T, false><<<grid, 32 * w, rs, I.stream>>>(I.p, I.g, phi, color, 0);
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
+
+// One red-black pass of both kinds (the factorising first pass and a plain one) on
+// `phi` with `warps` warps per CTA: what the autotuner times (phi is a scratch copy).
+template <typename T> void launch_sweep_probe(Inst<T> &I, T *phi, int warps)
+{
+    const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
+    const int grid = std::max(1, (lines + warps - 1) / warps);
+    const size_t rs = rounds_smem<T>(I.p, warps);
+    sweep_rb_rounds_kernel<T, true><<<grid, 32 * warps, rs, I.stream>>>(I.p, I.g, phi, 0, 0);
+    sweep_rb_rounds_kernel<T, false><<<grid, 32 * warps, rs, I.stream>>>(I.p, I.g, phi, 1, 0);
+}
 
 // ---------------------------------------------------------------------------
 // Defect correction of the energy solve (AMCFD_PREC_FP32_DC).  The assembly left
@@ -872,15 +884,34 @@ void launch_dc_sweeps(Inst<double> &I)
     f.pr = d.pr; f.cf = d.cf; f.iden = d.iden;
     f.delphi = I.g.delphi;
     f.st = I.g.st;
+    const int w = I.sweep_warps;
     const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
-    const int grid = std::max(1, (lines + 3) / 4);
-    const size_t rs = rounds_smem<float>(I.p, 4);
+    const int grid = std::max(1, (lines + w - 1) / w);
+    const size_t rs = rounds_smem<float>(I.p, w);
     for (int color = 0; color < 2; ++color)
-        sweep_rb_rounds_kernel<float, true><<<grid, 128, rs, I.stream>>>(I.p, f, d.delta, color,
-                                                                          color == 0 ? 2 : 0);
+        sweep_rb_rounds_kernel<float, true><<<grid, 32 * w, rs, I.stream>>>(I.p, f, d.delta, color,
+                                                                             color == 0 ? 2 : 0);
     for (int sweep = 1; sweep < 4; ++sweep)
         for (int color = 0; color < 2; ++color)
-            sweep_rb_rounds_kernel<float, false><<<grid, 128, rs, I.stream>>>(I.p, f, d.delta, color, 0);
+            sweep_rb_rounds_kernel<float, false><<<grid, 32 * w, rs, I.stream>>>(I.p, f, d.delta, color, 0);
+}
+
+// One factorising and one plain pass of the defect-correction sweeps with `warps`
+// lines per CTA (the autotuner's probe; it overwrites only the correction).
+void launch_dc_sweep_probe(Inst<double> &I, int warps)
+{
+    Fields<float> f;
+    memset(&f, 0, sizeof(f));
+    const DcBuf &d = I.dc;
+    f.an = d.an; f.as = d.as; f.ae = d.ae; f.aw = d.aw; f.at = d.at; f.ab = d.ab; f.ap = d.ap; f.su = d.su;
+    f.pr = d.pr; f.cf = d.cf; f.iden = d.iden;
+    f.delphi = I.g.delphi;
+    f.st = I.g.st;
+    const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
+    const int grid = std::max(1, (lines + warps - 1) / warps);
+    const size_t rs = rounds_smem<float>(I.p, warps);
+    sweep_rb_rounds_kernel<float, true><<<grid, 32 * warps, rs, I.stream>>>(I.p, f, d.delta, 0, 2);
+    sweep_rb_rounds_kernel<float, false><<<grid, 32 * warps, rs, I.stream>>>(I.p, f, d.delta, 1, 0);
 }
 
 // h += delta over the interior (delta is zero elsewhere), 16-byte vectors of
@@ -929,29 +960,35 @@ template <typename T> void set_sweep_smem_limit(size_t smem)
     cudaFuncSetAttribute(sweep_exact_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(sweep_rb_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
-// The whole-domain red-black kernel's buffer (qr and pr of 4 warps); false when it
-// does not fit a CTA.
-template <typename T> bool set_rounds_smem_limit(const Params &p)
+// The whole-domain red-black kernel's buffer (qr and pr of each warp's line): the
+// most warps per CTA (8, 4 or 2) whose buffers fit 200 KiB, with the attribute set
+// for them; 0 when not even 2 fit.
+template <typename T> int set_rounds_smem_limit(const Params &p)
 {
-    const size_t need = rounds_smem<T>(p, 4);
-    if (need > 200 * 1024) return false;
-    return cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)need) == cudaSuccess &&
-           cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)need) == cudaSuccess;
+    for (int w = 8; w >= 2; w /= 2) {
+        const size_t need = rounds_smem<T>(p, w);
+        if (need > 200 * 1024) continue;
+        if (cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)need) == cudaSuccess &&
+            cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)need) == cudaSuccess)
+            return w;
+    }
+    return 0;
 }
 
 #define AMCFD_INST(T)                                                     \
     template void launch_energy_factor<T>(Inst<T> &);                    \
     template void launch_box_factor<T>(Inst<T> &);                       \
     template void launch_energy_sweeps<T>(Inst<T> &);                    \
+    template void launch_sweep_probe<T>(Inst<T> &, T *, int);            \
     template void launch_phi_factor<T>(Inst<T> &, T *);                  \
     template void launch_phi_sweeps<T>(Inst<T> &, T *);                  \
     template void launch_box_sweeps<T>(Inst<T> &, int);                  \
     template void launch_box_tickets<T>(Inst<T> &);                      \
     template int exact_sweep_blocks_per_sm<T>(int, size_t);              \
     template void set_sweep_smem_limit<T>(size_t);                       \
-    template bool set_rounds_smem_limit<T>(const Params &);
+    template int set_rounds_smem_limit<T>(const Params &);
 AMCFD_INST(double)
 AMCFD_INST(float)
 #undef AMCFD_INST

@@ -99,6 +99,10 @@ struct Inst {
     T *mom_scratch = nullptr; // one field: line-solve scratch of the small-box momentum path
     size_t mom_small_smem = 0;  // its dynamic shared memory
     int mom_cluster = 1;        // CTAs of the cluster that takes boxes past one CTA's shared memory
+    // launch shapes picked by the autotuner (or pinned by the options)
+    int asm_kseg = 0;           // planes per CTA of the energy assembly (0: the default rule)
+    int sweep_warps = 4;        // warps (lines) per CTA of the whole-domain red-black sweeps
+    int sweep_warps_max = 4;    // the most whose line buffers fit a CTA's shared memory
     const T *asm_diff_a = nullptr;  // diff_cur at parity 0
     // updateSolutions inputs of the current step (powder bed)
     double trackindx = 1.0;
@@ -122,6 +126,7 @@ template <typename T> void launch_update_solutions(Inst<T> &I);
 // line solvers (k_linesolve.cu)
 template <typename T> void launch_energy_factor(Inst<T> &I);
 template <typename T> void launch_energy_sweeps(Inst<T> &I);
+template <typename T> void launch_sweep_probe(Inst<T> &I, T *phi, int warps);
 template <typename T> void launch_phi_factor(Inst<T> &I, T *phi);   // whole-domain phi
 template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi);
 template <typename T> void launch_box_factor(Inst<T> &I);
@@ -129,6 +134,7 @@ template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
 template <typename T> void launch_box_tickets(Inst<T> &I);
 // defect correction: the energy line sweeps in FP32 on the correction, and h += delta
 void launch_dc_sweeps(Inst<double> &I);
+void launch_dc_sweep_probe(Inst<double> &I, int warps);
 void launch_dc_apply(Inst<double> &I);
 // momentum (k_momentum.cu)
 template <typename T> void launch_momentum(Inst<T> &I, bool small);

@@ -193,6 +193,147 @@ CONFIG_DESC = {
 START_STEP = {"config1": 60, "config0": 20, "config4": 130}
 
 
+SWEEP_DESC = ("process-parameter sweep: 64 single-track instances, grids 60x30x20 .. 240x120x60 cells "
+              "(domain scaled from the 120x60x40 deck), P ~ U[100,400] W, v ~ U[0.5,1.5] m/s, "
+              "r ~ U[40,80] um (seeded), dt=1e-5 s, <=20 outer iterations/step, tolerance 1e-5")
+
+
+def sweep_reference(decks, paths, skip: int, steps: int, cores: int):
+    """The reference solver on the sweep: one process per instance (as the reference
+    runs), OMP_NUM_THREADS=1, `cores` processes at a time; skip + steps steps each,
+    the last `steps` timed; returns the aggregate over instances."""
+    import oracle_py
+    from concurrent.futures import ThreadPoolExecutor
+    exe = oracle_py.REF_DUMP
+    if not os.path.exists(exe):
+        return None, "reference binary oracle/_ref/amcfd_ref_dump not built"
+
+    def one(path):
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        out = subprocess.run([exe, path, "--time", "--steps", str(skip + steps)], env=env,
+                             capture_output=True, text=True, timeout=3600)
+        if out.returncode != 0:
+            raise RuntimeError(out.stderr[-300:])
+        return json.loads(out.stdout.strip().splitlines()[-1])
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        res = list(ex.map(one, paths))
+    wall = time.perf_counter() - t0
+    # every process ran skip + steps steps; the timed share of the wall clock is the
+    # timed steps' share of the summed step times
+    tot = sum(sum(js["step_seconds"]) for js in res)
+    timed = sum(sum(js["step_seconds"][skip:]) for js in res)
+    wall_timed = wall * timed / max(tot, 1e-30)
+    sim_ms = sum(1e3 * d.dt * steps for d in decks)
+    cells_iters = sum(js["interior_cells"] * sum(js["step_iters"][skip:]) for js in res)
+    return {"value": sim_ms / wall_timed, "cell_iters_per_s": cells_iters / wall_timed, "seconds": wall_timed,
+            "processes": cores}, None
+
+
+def sweep_main(args):
+    """The config-2 sweep: every rank solves its longest-processing-time shard of the
+    64 instances; each instance is a context with its own stream and step graph, a
+    pool of host threads keeps them in flight (amcfd_run_batch).  value = simulated
+    ms of all instances / wall s of the slowest rank."""
+    import amcfd_decks as D
+    import amcfd_sweep as SW
+    warmup = max(3, args.warmup)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = physical_cores()
+    tmp = tempfile.mkdtemp(prefix=f"amcfd_sweep{rank}_")
+    decks = D.config2(steps=warmup + args.steps + 1)
+    paths = [dk.write(os.path.join(tmp, dk.name)) for dk in decks]
+    cfg = {"workload": SWEEP_DESC, "deck": "config2", "instances": len(decks),
+           "window": f"steps {warmup + 1}-{warmup + args.steps} of every instance after {warmup} warm-up steps",
+           "timing": "host wall clock around the batch (device synchronised before and after); every "
+                     "instance runs on its own stream"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        r, why = sweep_reference(decks, paths, warmup, args.steps, cores)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}))
+            return
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": r["value"], "unit": METRIC,
+                          "n_gpus": args.gpus, "steps": args.steps, "warmup": warmup,
+                          "ms_per_step": 1e3 * r["seconds"] / args.steps, "higher_is_better": True,
+                          "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic decks",
+                          "config": dict(cfg, solver="reference build (oracle/_ref), one process per instance"),
+                          "cell_iters_per_s": r["cell_iters_per_s"],
+                          "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["processes"],
+                                           "kind": "reference", "sample": cfg["window"]},
+                          "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}))
+        shutil.rmtree(tmp, ignore_errors=True)
+        return
+    import torch
+    import amcfd
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    prec = {"fp32": amcfd.PREC_FP32, "fp32dc": amcfd.PREC_FP32_DC, "fp64": amcfd.PREC_FP64}[args.precision]
+    costs = [SW.instance_cost(amcfd.Deck(p).dims, args.steps) for p in paths]
+    mine = SW.shard(costs, world)[rank]
+    dk = [amcfd.Deck(paths[q]) for q in mine]
+    solvers = [amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, device=local, use_graphs=1)
+               for d in dk]
+    amcfd.run_batch(solvers, warmup)
+    it0 = [s.report.itertot for s in solvers]
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = sum(s.launches for s in solvers)
+    t0 = time.perf_counter()
+    reps, _ = amcfd.run_batch(solvers, args.steps)
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    ck = clocks.stop()
+    launches = sum(s.launches for s in solvers) - l0
+    cells_iters = sum((d.dims[0] - 2) * (d.dims[1] - 2) * (d.dims[2] - 2) * (r["itertot"] - i)
+                      for d, r, i in zip(dk, reps, it0))
+    sim_ms = sum(1e3 * decks[q].dt * args.steps for q in mine)
+    tot = torch.tensor([secs, sim_ms, cells_iters, launches], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        mx = tot[:1].clone()
+        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
+        sm_ = tot[1:].clone()
+        torch.distributed.all_reduce(sm_, op=torch.distributed.ReduceOp.SUM)
+        secs, (sim_ms, cells_iters, launches) = float(mx.item()), sm_.tolist()
+    for s in solvers:
+        s.close()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": sim_ms / secs, "unit": METRIC, "n_gpus": world,
+                          "steps": args.steps, "warmup": warmup, "ms_per_step": 1e3 * secs / args.steps,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                          "dtype": {amcfd.PREC_FP32: "f32", amcfd.PREC_FP32_DC: "f64 (energy line solves f32 "
+                                    "on the correction)", amcfd.PREC_FP64: "f64"}[prec],
+                          "data": "synthetic decks",
+                          "config": dict(cfg, precision=args.precision, order="redblack", graphs=1,
+                                         parallelism=f"instance shards over {world} GPU(s)"),
+                          "cell_iters_per_s": cells_iters / secs, "gpu_launches": int(launches),
+                          "clocks": ck,
+                          "e2e": {"value": sim_ms / secs, "unit": METRIC, "h2d_bytes_per_step": 52 * len(decks),
+                                  "d2h_bytes_per_step": 512 * len(decks),
+                                  "note": "the batch call is the public API; per step every instance copies "
+                                          "its laser block in and its status block out"}}))
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,7 +356,12 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--feature", default="none", choices=sorted(FEATURES),
                     help="solve the deck with one of the optional models switched on")
+    ap.add_argument("--workload", default="track", choices=["track", "sweep"],
+                    help="track: one melt-pool instance per GPU (--config); sweep: the 64-instance "
+                         "process-parameter sweep, sharded over the GPUs")
     args = ap.parse_args()
+    if args.workload == "sweep":
+        return sweep_main(args)
     warmup = max(3, args.warmup)
     start = START_STEP[args.config] if args.start_step is None else max(0, args.start_step)
     skip = start + warmup  # steps before the timed window

@@ -158,7 +158,15 @@ typedef struct amcfd_options {
                             waits for a neighbouring line before the step fails with
                             AMCFD_E_TIMEOUT; 0 = the default 2^24 (about one second).  The
                             reference has no such wait (its sweeps are sequential). */
-    int reserved[5];
+    int autotune;        /* 1: at creation, time the candidate launch shapes of the energy
+                            assembly (planes per CTA) and of the red-black line sweeps (lines
+                            per CTA) on this grid and keep the fastest (amcfd_tuning reports
+                            them); 0: the fixed defaults.  The assembly's shape sets the order
+                            of its FP64 partial sums, so contexts whose results must agree bit
+                            for bit pin it (asm_kseg). */
+    int asm_kseg;        /* planes per CTA of the energy assembly: 4, 8 or 16; 0 = default/tuned */
+    int sweep_warps;     /* lines (warps) per CTA of the red-black sweeps: 2, 4 or 8; 0 = default/tuned */
+    int reserved[2];
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;
@@ -253,6 +261,13 @@ int amcfd_run_steps(amcfd_ctx *ctx, int nsteps, amcfd_step_report *report, doubl
 
 /* Number of kernels the context has launched since creation. */
 long long amcfd_kernel_launches(const amcfd_ctx *ctx);
+
+/* Launch shapes in use (no counterpart in the reference): planes per CTA of the
+ * energy assembly (*asm_kseg, 0 = the default rule) and lines per CTA of the
+ * red-black sweeps (*sweep_warps); with amcfd_options.autotune, the measured times
+ * of the candidates in ms (times[0..2]: assembly with 4, 8, 16 planes; times[3..5]:
+ * a factorising and a plain sweep pass with 2, 4, 8 lines; 0 when not timed). */
+int amcfd_tuning(const amcfd_ctx *ctx, int *asm_kseg, int *sweep_warps, double *times);
 
 /* Parameter sweep over independent instances: runs nsteps time steps of every
  * context in ctxs[0..n), each on its own stream, spread over nthreads host threads
