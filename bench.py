@@ -281,8 +281,8 @@ def sweep_main(args):
     costs = [SW.instance_cost(amcfd.Deck(p).dims, args.steps) for p in paths]
     mine = SW.shard(costs, world)[rank]
     dk = [amcfd.Deck(paths[q]) for q in mine]
-    solvers = [amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, device=local, use_graphs=1)
-               for d in dk]
+    solvers = [amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, device=local, use_graphs=1,
+                            autotune=1) for d in dk]
     amcfd.run_batch(solvers, warmup)
     it0 = [s.report.itertot for s in solvers]
 
@@ -417,9 +417,17 @@ def main():
     ni, nj, nk = d.dims
     ncell = (ni - 2) * (nj - 2) * (nk - 2)
 
+    tune = {}
+
     def solver(p=prec):
-        return amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
-                            host_loop=1 if args.host_loop else 0)
+        # the production path tunes its launch shapes at creation; later solvers of the
+        # same precision are pinned to the first one's choice
+        kw = dict(asm_kseg=tune[p]["asm_kseg"], sweep_warps=tune[p]["sweep_warps"]) if p in tune else \
+            dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
+        sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
+                          host_loop=1 if args.host_loop else 0, **kw)
+        tune.setdefault(p, sv.tuning())
+        return sv
 
     s = solver()
     s.run_steps(skip)
@@ -509,7 +517,8 @@ def main():
                 "iteration_frac": (sum(words[f] * wsize[f] for f in words) * ncell * iters / (ms / 1e3) / 1e9) / peak}
 
     extra = {"momentum_box_cells": {"mean": float(np.mean(boxes)), "min": int(min(boxes)),
-                                    "max": int(max(boxes))}}
+                                    "max": int(max(boxes))},
+             "tuning": tune[prec]}
     if args.feature == "freesurf":
         # one free-surface update (bisection + projection) on a fresh state; the call
         # returns after its kernels and the read-back of the monitor values

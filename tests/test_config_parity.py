@@ -27,11 +27,26 @@ from conftest import rel_l2
 pytestmark = pytest.mark.gpu
 
 SNAP = ("temp", "uvel", "vvel", "wvel", "enthalpy")
+VEL = ("uvel", "vvel", "wvel")
 BOX = ("istat", "iend", "jstat", "jend", "kstat")
 STEPS = {"config0": 4, "config1": 2}
-# production path against the oracle: relative L2 bounds per field (measured
-# values are printed by the test)
-PROD_TOL = {"temp": 1e-3, "enthalpy": 1e-3, "uvel": 0.3, "vvel": 0.3, "wvel": 0.3}
+# production path against the oracle: L2 error relative to the oracle's field
+# (T, h) or to the oracle's whole velocity field (u, v, w: a component that is
+# only starting to move, w in the first steps, has no scale of its own).
+# Measured on B200: T and h <= 1e-5, velocities <= 2e-3.
+PROD_TOL = {"temp": 1e-4, "enthalpy": 1e-4, "uvel": 1e-2, "vvel": 1e-2, "wvel": 1e-2}
+
+
+def _errors(get, fo):
+    """Relative L2 errors of the fields of `get(name)` against the oracle's `fo`;
+    velocity components against the norm of the oracle's velocity field."""
+    vnorm = float(np.sqrt(sum(np.linalg.norm(fo[f]) ** 2 for f in VEL)))
+    out = {}
+    for f in SNAP:
+        d = float(np.linalg.norm(get(f) - fo[f]))
+        ref = vnorm if f in VEL else float(np.linalg.norm(fo[f]))
+        out[f] = d / ref if ref > 0 else d
+    return out
 
 _cache = {}
 
@@ -82,10 +97,10 @@ def test_exact_fp64_matches_oracle(name, tmp_path_factory):
             assert rg[k] == ro[k], (where, k, rg[k], ro[k])
         for k in ("alen", "depth", "width", "tpeak"):
             assert abs(rg[k] - ro[k]) <= 1e-8 * max(abs(ro[k]), 1e-12) + 1e-14, (where, k, rg[k], ro[k])
-        for f in SNAP:
-            err = rel_l2(s.get(f), fo[f])
-            print(f"{where} exact fp64 {f} rel-L2 {err:.3e}")
-            assert err < 1e-8, (where, f, err)
+        errs = _errors(s.get, fo)
+        print(where, "exact fp64", " ".join(f"{f} {e:.3e}" for f, e in errs.items()))
+        for f, e in errs.items():
+            assert e < 1e-8, (where, f, e)
     s.close()
 
 
@@ -99,7 +114,7 @@ def test_production_path_melt_pool_within_one_cell(name, tmp_path_factory):
         rg = s.step()
         where = f"{name} step {q + 1}"
         cell = _one_cell(grid, ro)
-        errs = {f: rel_l2(s.get(f), fo[f]) for f in SNAP}
+        errs = _errors(s.get, fo)
         print(where, "fp32 red-black niter", rg["niter"], "oracle", ro["niter"],
               " ".join(f"{f} {e:.3e}" for f, e in errs.items()),
               " ".join(f"{k} {rg[k]:.6e}/{ro[k]:.6e} (cell {cell[k]:.2e})" for k in cell))

@@ -133,13 +133,16 @@ def test_feature_rows_are_checked(tmp_path):
 def test_option_checks_before_any_device_work(tmp_path):
     """Option combinations the solver does not support fail with AMCFD_E_ARG
     before the context touches a GPU: defect correction outside red-black order,
-    an unknown precision and a negative wait budget."""
+    an unknown precision, a negative wait budget and launch shapes the kernels do
+    not offer."""
     import amcfd
     import amcfd_decks as D
     d = amcfd.Deck(D.small("opts", steps=1).write(str(tmp_path)))
     for kw in (dict(order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP32_DC),
                dict(order=amcfd.ORDER_REDBLACK, precision=7),
-               dict(order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, wait_polls=-5)):
+               dict(order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, wait_polls=-5),
+               dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, asm_kseg=5),
+               dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, sweep_warps=3)):
         opts = amcfd.AmcfdOptions(**kw)
         h = C.c_void_p()
         assert amcfd.lib().amcfd_create(C.byref(d.params), C.byref(opts), C.byref(h)) == -1, kw
