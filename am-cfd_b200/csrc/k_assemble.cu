@@ -17,9 +17,10 @@
 // to one plane apart instead of waiting for the slowest, and no thread waits on
 // a global load.
 // Face areas and volumes are products of per-column (x, y) and per-plane (z)
-// widths, formed in FP64 in the reference's order.  The arithmetic is the
-// reference's expression by expression; the FP32 build evaluates properties
-// and divisions in FP32.
+// widths, formed in FP64 in the reference's order.  The FP64 build's arithmetic
+// is the reference's expression by expression; the FP32 build evaluates
+// properties and divisions in FP32, and it and the defect-correction build form
+// each face's conductance and Peclet number from one reciprocal.
 #include <algorithm>
 
 #include "kernels.cuh"
@@ -52,12 +53,27 @@ constexpr int kAsmWarps = kTX * kTY / 32, kAsmCounters = 4;
 enum { FA_D = 0, FA_H, FA_F, FA_R, FA_W };
 enum { FB_U = 0, FB_V, FB_T, FB_HN, FB_FN };
 
+// A face of the fast builds: conductance d = num / den (den = 1 on a boundary face,
+// else the harmonic-mean denominator) and the pair D A(|F|/D) + max(0, -+F), with
+// one reciprocal r = 1 / (num den): d = num^2 r and |F| / d = |F| den^2 r.
+__device__ __forceinline__ float rcp_fast(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double rcp_fast(double x) { return 1.0 / x; }
+template <typename R>
+__device__ __forceinline__ void face_fast(int sch, R num, R den, R f, R &plus, R &minus)
+{
+    const R r = rcp_fast(num * den);
+    const R d = num * num * r;
+    const R a = d * scheme_fn<R>(sch, fabs(f) * (den * den * r));
+    plus = a + maxd(R(0), -f);
+    minus = a + maxd(R(0), f);
+}
+
 // SCH: the discretisation scheme as a compile-time constant (one instantiation per
 // scheme), so that the six face coefficients carry no untaken scheme branches.
-// DC (FP64 only, defect correction): the coefficients are formed in FP64 exactly
-// as without it, but stored rounded to FP32 in `dco`, and the FP32 `su` slot
-// receives the FP64 defect su + sum a_nb h_nb - ap h of the current enthalpy;
-// the FP64 coefficient arrays are not written.
+// DC (FP64 only, defect correction): the coefficients are formed in FP64 (with
+// the fast builds' one reciprocal per face), stored rounded to FP32 in `dco`, and
+// the FP32 `su` slot receives the FP64 defect su + sum a_nb h_nb - ap h of the
+// current enthalpy; the FP64 coefficient arrays are not written.
 template <typename T, int SCH, bool DC>
 __global__ void __launch_bounds__(256, AsmBox<T>::MINB)
 energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp, DcBuf dco)
@@ -169,6 +185,10 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     // divisions by per-launch constants become multiplications by their reciprocals
     // (the FP64 build keeps the reference's FP64 products and exact divisions)
     constexpr bool kF32 = sizeof(R) == 4;
+    // FAST (FP32 bulk, or FP64 under defect correction; neither is compared bit for
+    // bit with the reference): one reciprocal per face instead of two divisions,
+    // and the divisions by per-launch constants as multiplications
+    constexpr bool FAST = kF32 || DC;
     const R fdx = (R)dx, fdy = (R)dy;
     const R inv_acpl = (R)(1.0 / p.acpl), inv_delt = (R)(1.0 / delt), inv_urfh = (R)(1.0 / p.urfh);
     const R dxp_e = (R)g.dxpwinv[nim1], dxp_w = (R)g.dxpwinv[1];
@@ -197,7 +217,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
             // ---- material properties (every node) ----
             {
                 const R t = t_c, fl = f_c;
-                const R diffl = kF32 ? (thla * t + thlb) * inv_acpl : bdiv(thla * t + thlb, acpl);
+                const R diffl = FAST ? (thla * t + thlb) * inv_acpl : bdiv(thla * t + thlb, acpl);
                 R dn = diffl, rn = denl, vn = visc;
                 if (!(t >= tliq)) {
                     R diffs, rs = dens;
@@ -243,76 +263,118 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 // north face
                 {
                     R fn = Ac[FA_R * FE + BX] * v_n * aik;
-                    R dn;
-                    if (j == njm2) {
-                        dn = dcc * aik * dyp_n;
+                    if constexpr (FAST) {
+                        const bool bnd = j == njm2;
+                        const R num = bnd ? dcc * aik * dyp_n : dcc * d_nn * aik * dyp_p;
+                        const R den = bnd ? R(1) : (R(1) - fy_j) * d_nn + fy_j * dcc;
+                        face_fast<R>(sch, num, den, fn, an, tmp);
                     } else {
-                        R difn = bdiv(dcc * d_nn, (R(1) - fy_j) * d_nn + fy_j * dcc);
-                        dn = difn * aik * dyp_p;
+                        R dn;
+                        if (j == njm2) {
+                            dn = dcc * aik * dyp_n;
+                        } else {
+                            R difn = bdiv(dcc * d_nn, (R(1) - fy_j) * d_nn + fy_j * dcc);
+                            dn = difn * aik * dyp_p;
+                        }
+                        face_coef<R>(sch, dn, fn, an, tmp);
                     }
-                    face_coef<R>(sch, dn, fn, an, tmp);
                 }
                 // south face
                 {
                     R fs = rhc * v_c * aik;
-                    R ds;
-                    if (j == 1) {
-                        ds = dcc * aik * dyp_s;
+                    if constexpr (FAST) {
+                        const bool bnd = j == 1;
+                        const R num = bnd ? dcc * aik * dyp_s : d_s * dcc * aik * dyp_j;
+                        const R den = bnd ? R(1) : (R(1) - fy_m) * dcc + fy_m * d_s;
+                        face_fast<R>(sch, num, den, fs, tmp, as_);
                     } else {
-                        R difs = bdiv(d_s * dcc, (R(1) - fy_m) * dcc + fy_m * d_s);
-                        ds = difs * aik * dyp_j;
+                        R ds;
+                        if (j == 1) {
+                            ds = dcc * aik * dyp_s;
+                        } else {
+                            R difs = bdiv(d_s * dcc, (R(1) - fy_m) * dcc + fy_m * d_s);
+                            ds = difs * aik * dyp_j;
+                        }
+                        face_coef<R>(sch, ds, fs, tmp, as_);
                     }
-                    face_coef<R>(sch, ds, fs, tmp, as_);
                 }
                 // east face
                 {
                     R fe = Ac[FA_R * FE + 1] * u_e * ajk;
-                    R de;
-                    if (i == nim2) {
-                        de = dcc * ajk * dxp_e;
+                    if constexpr (FAST) {
+                        const bool bnd = i == nim2;
+                        const R num = bnd ? dcc * ajk * dxp_e : dcc * d_e * ajk * dxp_p;
+                        const R den = bnd ? R(1) : (R(1) - fx_i) * d_e + fx_i * dcc;
+                        face_fast<R>(sch, num, den, fe, ae, tmp);
                     } else {
-                        R dife = bdiv(dcc * d_e, (R(1) - fx_i) * d_e + fx_i * dcc);
-                        de = dife * ajk * dxp_p;
+                        R de;
+                        if (i == nim2) {
+                            de = dcc * ajk * dxp_e;
+                        } else {
+                            R dife = bdiv(dcc * d_e, (R(1) - fx_i) * d_e + fx_i * dcc);
+                            de = dife * ajk * dxp_p;
+                        }
+                        face_coef<R>(sch, de, fe, ae, tmp);
                     }
-                    face_coef<R>(sch, de, fe, ae, tmp);
                 }
                 // west face
                 {
                     R fw = rhc * u_c * ajk;
-                    R dw;
-                    if (i == 1) {
-                        dw = dcc * ajk * dxp_w;
+                    if constexpr (FAST) {
+                        const bool bnd = i == 1;
+                        const R num = bnd ? dcc * ajk * dxp_w : d_w * dcc * ajk * dxp_i;
+                        const R den = bnd ? R(1) : (R(1) - fx_m) * dcc + fx_m * d_w;
+                        face_fast<R>(sch, num, den, fw, tmp, aw);
                     } else {
-                        R difw = bdiv(d_w * dcc, (R(1) - fx_m) * dcc + fx_m * d_w);
-                        dw = difw * ajk * dxp_i;
+                        R dw;
+                        if (i == 1) {
+                            dw = dcc * ajk * dxp_w;
+                        } else {
+                            R difw = bdiv(d_w * dcc, (R(1) - fx_m) * dcc + fx_m * d_w);
+                            dw = difw * ajk * dxp_i;
+                        }
+                        face_coef<R>(sch, dw, fw, tmp, aw);
                     }
-                    face_coef<R>(sch, dw, fw, tmp, aw);
                 }
                 // top face
                 {
                     R ft = Ap[FA_R * FE] * w_p * aij;
-                    R dt;
-                    if (k == nkm2) {
-                        dt = dcc * aij * dzp_t;
+                    if constexpr (FAST) {
+                        const bool bnd = k == nkm2;
+                        const R num = bnd ? dcc * aij * dzp_t : dcc * d_p * aij * dzp_p;
+                        const R den = bnd ? R(1) : (R(1) - fz_k) * d_p + fz_k * dcc;
+                        face_fast<R>(sch, num, den, ft, at, tmp);
                     } else {
-                        R dift = bdiv(dcc * d_p, (R(1) - fz_k) * d_p + fz_k * dcc);
-                        dt = dift * aij * dzp_p;
+                        R dt;
+                        if (k == nkm2) {
+                            dt = dcc * aij * dzp_t;
+                        } else {
+                            R dift = bdiv(dcc * d_p, (R(1) - fz_k) * d_p + fz_k * dcc);
+                            dt = dift * aij * dzp_p;
+                        }
+                        face_coef<R>(sch, dt, ft, at, tmp);
                     }
-                    face_coef<R>(sch, dt, ft, at, tmp);
                 }
                 // bottom face
                 {
                     R fb = rhc * w_c * aij;
-                    R db;
-                    if (k == 1) {
-                        db = dcc * aij * dzp_b;
+                    if constexpr (FAST) {
+                        const bool bnd = k == 1;
+                        const R num = bnd ? dcc * aij * dzp_b : d_m * dcc * aij * dzp_k;
+                        const R den = bnd ? R(1) : (R(1) - fz_m) * dcc + fz_m * d_m;
+                        face_fast<R>(sch, num, den, fb, tmp, ab);
                     } else {
-                        R difb = bdiv(d_m * dcc, (R(1) - fz_m) * dcc + fz_m * d_m);
-                        db = difb * aij * dzp_k;
+                        R db;
+                        if (k == 1) {
+                            db = dcc * aij * dzp_b;
+                        } else {
+                            R difb = bdiv(d_m * dcc, (R(1) - fz_m) * dcc + fz_m * d_m);
+                            db = difb * aij * dzp_k;
+                        }
+                        face_coef<R>(sch, db, fb, tmp, ab);
                     }
-                    face_coef<R>(sch, db, fb, tmp, ab);
                 }
-                const R densbydt = kF32 ? rhc * inv_delt : bdiv(rhc, (R)delt);
+                const R densbydt = FAST ? rhc * inv_delt : bdiv(rhc, (R)delt);
                 const R apnot = densbydt * vol;
                 R sp = R(0);
                 R su = apnot * Bc[FB_HN * FE];
@@ -330,7 +392,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                     g.sourceinput[c] = srcin;
                 }
                 const R hlatnt = (R)p.hlatnt;
-                const R variable1 = kF32 ? hlatnt * rhc * inv_delt : bdiv(hlatnt * rhc, (R)delt);
+                const R variable1 = FAST ? hlatnt * rhc * inv_delt : bdiv(hlatnt * rhc, (R)delt);
                 const R volht = vol * variable1;
                 const R flc = f_c;
                 su -= volht * (flc - Bc[FB_FN * FE]);
@@ -358,7 +420,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 if (i == nim2) { su += ae * hip; sp -= ae; ae = R(0); }
                 R ap = an + as_ + ae + aw + at + ab + apnot - sp;
                 const R urfh = (R)p.urfh;
-                ap = kF32 ? ap * inv_urfh : bdiv(ap, urfh);
+                ap = FAST ? ap * inv_urfh : bdiv(ap, urfh);
                 su += (R(1) - urfh) * ap * hc;
                 if constexpr (DC) {
                     const double dfc = ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc;

@@ -354,6 +354,9 @@ def main():
                          "host (default: one graph per step, iterations chained on the device)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--profile-window", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop, so that "
+                         "ncu --profile-from-start off captures those launches only")
     ap.add_argument("--feature", default="none", choices=sorted(FEATURES),
                     help="solve the deck with one of the optional models switched on")
     ap.add_argument("--workload", default="track", choices=["track", "sweep"],
@@ -451,7 +454,12 @@ def main():
     clocks.start()
     l0 = s.launches
     it0 = s.report.itertot
+    if args.profile_window:
+        torch.cuda.cudart().cudaProfilerStart()
     rep, ms = s.run_steps(args.steps)
+    if args.profile_window:
+        torch.cuda.synchronize()
+        torch.cuda.cudart().cudaProfilerStop()
     launches = s.launches - l0
     iters = rep["itertot"] - it0
     torch.cuda.synchronize()
