@@ -103,8 +103,9 @@ def evaluate(net: amcfd.Net, deck_path: str, steps: int, precision: int = amcfd.
 # Tensor-core FLOPs per cell of one forward pass (padded channels, as executed):
 # 2 x 27 taps x sum over layers of cin x cout.
 FWD_FLOP_PER_CELL = 2 * 27 * (16 * 32 + 32 * 32 + 32 * 32 + 32 * 16)
-# input-gradient convolutions of layers 3, 2, 1 (tensor cores)
-BWD_TC_FLOP_PER_CELL = 2 * 27 * (16 * 32 + 32 * 32 + 32 * 32)
+# backward on the tensor cores: input-gradient convolutions of layers 3, 2, 1 and
+# the weight-gradient contractions of all four layers (as many FLOPs as the forward)
+BWD_TC_FLOP_PER_CELL = 2 * 27 * (16 * 32 + 32 * 32 + 32 * 32) + FWD_FLOP_PER_CELL
 
 
 def bench_network(dims=(202, 102, 62), reps: int = 10, device: int = 0) -> Dict:
@@ -146,14 +147,16 @@ if __name__ == "__main__":
     ap.add_argument("--bench", action="store_true", help="network throughput on the config-3 grid")
     ap.add_argument("--eval", type=int, default=0, help="train, then evaluate N steps of config 3")
     ap.add_argument("--train-steps", type=int, default=60)
+    ap.add_argument("--train-instances", type=int, default=8,
+                    help="config-2 instances to train on (of the seeded 64; steps x instances pairs)")
     args = ap.parse_args()
     if args.bench:
         print(json.dumps(bench_network()))
     if args.eval:
         tmp = tempfile.mkdtemp(prefix="amcfd_ws_")
-        # training decks: config-2 instances (seeded draws of power, speed,
-        # radius), the smaller half of the size range to keep training short
-        decks = [d for d in D.config2(n=16, steps=args.train_steps + 1)][:8]
+        # training decks: the first config-2 instances of the seeded sweep (draws of
+        # grid size, power, speed, radius)
+        decks = D.config2(n=64, steps=args.train_steps + 1)[:args.train_instances]
         paths = [d.write(os.path.join(tmp, d.name)) for d in decks]
         net = amcfd.Net(seed=3)
         t0 = time.perf_counter()

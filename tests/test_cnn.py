@@ -73,12 +73,15 @@ def test_forward_and_gradients_match_oracle():
     yo, acts = O.forward(params, feat.astype(np.float64), DIMS)
     lo, go = O.backward(params, acts, yo, target.astype(np.float64), DIMS)
     yg = y.cpu().numpy().astype(np.float64)
-    assert np.linalg.norm(yg - yo) <= 2e-2 * np.linalg.norm(yo), np.linalg.norm(yg - yo) / np.linalg.norm(yo)
+    ey = np.linalg.norm(yg - yo) / np.linalg.norm(yo)
+    eg = [[float(np.linalg.norm(g[sl] - go[sl]) / max(np.linalg.norm(go[sl]), 1e-300)) for sl in ls]
+          for ls in O.layer_slices()]
+    print(f"outputs {ey:.2e}, loss {abs(loss - lo) / abs(lo):.2e}, "
+          "gradients (W, b) per layer " + " ".join(f"({a:.2e}, {b:.2e})" for a, b in eg))
+    assert ey <= 2e-2, ey
     assert abs(loss - lo) <= 1e-2 * abs(lo), (loss, lo)
-    for l, (ws, bs) in enumerate(O.layer_slices()):
-        for sl in (ws, bs):
-            a, b = g[sl], go[sl]
-            assert np.linalg.norm(a - b) <= 5e-2 * np.linalg.norm(b) + 1e-12, (l, np.linalg.norm(a - b) / np.linalg.norm(b))
+    for l, (a, b) in enumerate(eg):
+        assert a <= 5e-2 and b <= 5e-2, (l, a, b)
     net.close()
 
 
