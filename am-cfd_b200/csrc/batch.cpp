@@ -14,6 +14,10 @@
 
 #include "amcfd.h"
 
+namespace amcfd {
+int ctx_kind(const amcfd_ctx *ctx);
+}
+
 extern "C" int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nthreads,
                                amcfd_step_report *reports, int *status)
 {
@@ -22,17 +26,28 @@ extern "C" int amcfd_run_batch(amcfd_ctx *const *ctxs, int n, int nsteps, int nt
     for (int q = 0; q < n; ++q)
         if (!ctxs[q]) return AMCFD_E_ARG;
     const int nt = std::min(n, nthreads == 0 ? 64 : nthreads);
-    std::vector<int> st(n, 0);
+    std::vector<int> st(n, 0), done(n, 0);
+    std::vector<amcfd_step_report> rep(n);
+    // The first step of the first context of each kind runs here, alone: it loads
+    // every kernel that kind launches (a kernel's first launch loads its module,
+    // which must not happen while another thread captures a graph).
+    std::vector<int> kinds;
+    for (int q = 0; q < n && nsteps > 0; ++q) {
+        const int k = amcfd::ctx_kind(ctxs[q]);
+        if (std::find(kinds.begin(), kinds.end(), k) != kinds.end()) continue;
+        kinds.push_back(k);
+        st[q] = amcfd_step(ctxs[q], &rep[q]);
+        done[q] = 1;
+    }
     std::atomic<int> next{0};
     auto work = [&]() {
         for (;;) {
             const int q = next.fetch_add(1);
             if (q >= n) return;
-            amcfd_step_report rep{};
-            int rc = 0;
-            for (int s = 0; s < nsteps && rc == 0; ++s) rc = amcfd_step(ctxs[q], &rep);
+            int rc = st[q];
+            for (int s = done[q]; s < nsteps && rc == 0; ++s) rc = amcfd_step(ctxs[q], &rep[q]);
             st[q] = rc;
-            if (reports) reports[q] = rep;
+            if (reports) reports[q] = rep[q];
         }
     };
     std::vector<std::thread> pool;

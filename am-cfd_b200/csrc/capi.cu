@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <initializer_list>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -120,6 +121,7 @@ struct amcfd_ctx {
     int autotune = 0, asm_kseg = 0, sweep_warps = 0;  // launch shapes: tuned, or pinned (0: default)
     double tune_ms[6] = {0};       // the autotuner's measured candidates
     int mom_cluster = 1;           // CTAs of the cluster momentum path (1: none)
+    int mom_cluster_req = 0;       // as requested by the options (0: default)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
@@ -501,6 +503,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
         if ((rc = alloc3<int2>(ctx, &g.tickets_mom, tk.size()))) return rc;
         if ((rc = alloc3<int>(ctx, &g.ntickets_mom, 1))) return rc;
         if ((rc = alloc3<T>(ctx, &I.mom_scratch, n3))) return rc;
+        I.mom_cluster = ctx->mom_cluster_req;
         setup_mom_small<T>(I);
         ctx->mom_cluster = I.mom_cluster;
     }
@@ -859,6 +862,11 @@ static void launch_iteration(amcfd_ctx *ctx, Inst<T> &I, bool capturing)
     if (ev) rec(ctx, 6, capturing);
 }
 
+// Graph captures of all contexts of the process, one at a time: a capture must
+// not overlap anything that loads a kernel module (a first launch of a kernel),
+// which a capture in another thread may do.
+static std::mutex g_capture_mu;
+
 // One outer iteration replayed from a CUDA graph.  Every launch of an iteration
 // has a fixed grid and reads its data-dependent extents (the momentum box, the
 // sweep tickets) from the device status block, so the graph captured on the
@@ -869,6 +877,7 @@ static int launch_iteration_graph(amcfd_ctx *ctx, Inst<T> &I)
     const int par = (const void *)I.g.diff_cur == ctx->diff_a ? 0 : 1;
     cudaGraphExec_t &ge = ctx->gexec[ctx->events ? 1 : 0][par][mom_small<T>(ctx, I) ? 1 : 0];
     if (!ge) {
+        std::lock_guard<std::mutex> lock(g_capture_mu);
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         launch_iteration<T>(ctx, I, true);  // swaps the property buffers
@@ -907,6 +916,7 @@ constexpr int kMaxChain = 64;  // longer maxit: the host drives the loop
 template <typename T>
 static int build_loop_graph(amcfd_ctx *ctx, Inst<T> &I, cudaGraphExec_t &ge)
 {
+    std::lock_guard<std::mutex> lock(g_capture_mu);
     const int maxit = ctx->prm.maxit;
     const int cap = ctx->small_box && ctx->order == AMCFD_ORDER_REDBLACK ? mom_small_capacity<T>(I) : -1;
     const double tol = ctx->prm.nonlintol;
@@ -1294,6 +1304,10 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
             return fail(ctx, AMCFD_E_ARG, "asm_kseg must be 0, 4, 8 or 16");
         if (opts->sweep_warps != 0 && opts->sweep_warps != 2 && opts->sweep_warps != 4 && opts->sweep_warps != 8)
             return fail(ctx, AMCFD_E_ARG, "sweep_warps must be 0, 2, 4 or 8");
+        if (opts->mom_cluster != 0 && opts->mom_cluster != 1 && opts->mom_cluster != 2 && opts->mom_cluster != 4 &&
+            opts->mom_cluster != 8 && opts->mom_cluster != 16)
+            return fail(ctx, AMCFD_E_ARG, "mom_cluster must be 0, 1, 2, 4, 8 or 16");
+        ctx->mom_cluster_req = opts->mom_cluster;
         ctx->autotune = opts->autotune != 0;
         ctx->asm_kseg = opts->asm_kseg;
         ctx->sweep_warps = opts->sweep_warps;
@@ -1472,6 +1486,12 @@ static int field_ptr(amcfd_ctx *ctx, const char *name, void **ptr);
 }
 namespace amcfd {
 void ctx_report(amcfd_ctx *ctx, amcfd_step_report *r) { fill_report(ctx, r); }
+// The kernel set a context launches: its precision, defect correction, order and
+// graph use (contexts of one kind load the same kernels).
+int ctx_kind(const amcfd_ctx *ctx)
+{
+    return ctx->precision + 2 * (ctx->dc ? 1 : 0) + 4 * ctx->order + 8 * (ctx->use_graphs ? 1 : 0);
+}
 double ctx_delt(const amcfd_ctx *ctx) { return ctx->delt; }
 double ctx_outtime(const amcfd_ctx *ctx) { return ctx->outtime; }
 const amcfd_params &ctx_params(const amcfd_ctx *ctx) { return ctx->prm; }

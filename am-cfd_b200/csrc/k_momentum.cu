@@ -1142,16 +1142,17 @@ __device__ __forceinline__ bool spread(const Box &b, int smem_elems)
     return slab_elems(b.ni_, b.nj_, b.k1 - b.k0 + 1) > (long long)smem_elems;
 }
 
-// ---- one CTA (boxes that fit its shared memory; a no-op otherwise) --------------------
+// ---- one CTA (boxes that fit its shared memory, and with `wide` 0 every box; a
+// no-op for the boxes a cluster takes) ---------------------------------------------------
 // cleanVelocities + applyBCs(1).
 template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
-mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems)
+mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems, int wide)
 {
     __shared__ double sh[32];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
+    if (!get_box(st, p, b) || (wide && spread(b, smem_elems))) return;
     for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
         int i, j, k;
         box_cell(b, q, i, j, k);
@@ -1164,13 +1165,13 @@ mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems)
 // Line solve of equation ivar (1..3) on the box, then applyBCs(ivar + 1).
 template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
-mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems, double *red_umax)
+mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems, double *red_umax, int wide)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double sh[32];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
+    if (!get_box(st, p, b) || (wide && spread(b, smem_elems))) return;
     T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : g.wvel;
     solve_box_small<T>(p, g, b, phi, reinterpret_cast<T *>(smraw), smem_elems, scratch);
     small_bc<T>(p, g, st, b, ivar + 1, red_umax, sh);
@@ -1179,13 +1180,13 @@ mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems
 // Line solve of p', correctPressure and the residual normalisation.
 template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
-mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb)
+mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb, int wide)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double scratch_r[40];
     Status *st = g.st;
     Box b;
-    if (!get_box(st, p, b) || spread(b, smem_elems)) return;
+    if (!get_box(st, p, b) || (wide && spread(b, smem_elems))) return;
     solve_box_small<T>(p, g, b, g.pp, reinterpret_cast<T *>(smraw), smem_elems, scratch);
     for (int q = threadIdx.x; q < b.n; q += blockDim.x) {
         int i, j, k;
@@ -1289,6 +1290,9 @@ template <typename T> int mom_small_capacity(const Inst<T> &I)
     return I.mom_cluster > 1 ? one * I.mom_cluster / 2 : one;
 }
 
+// Default cluster size of the box solve (the options may pin another).
+constexpr int kDefaultCluster = 8;
+
 // Cluster size of the small-box kernels: the largest the device schedules with
 // this shared memory, at most 16.
 template <typename T> static int max_cluster(size_t smem)
@@ -1331,7 +1335,8 @@ template <typename T> void setup_mom_small(Inst<T> &I)
     cudaFuncSetAttribute(mom_cluster_mid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     cudaFuncSetAttribute(mom_cluster_post_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     I.mom_small_smem = bytes;
-    I.mom_cluster = max_cluster<T>(bytes);
+    const int most = max_cluster<T>(bytes);
+    I.mom_cluster = I.mom_cluster > 0 ? std::min(I.mom_cluster, most) : std::min(kDefaultCluster, most);
 }
 
 // A launch of nc CTAs forming one cluster.
@@ -1372,16 +1377,19 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
         // case it is not returns at once)
         const int nc = I.mom_cluster;
         const size_t sm = I.mom_small_smem;
-        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax, se);
+        const int wide = nc > 1;
+        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax, se, wide);
         if (nc > 1) launch_cluster(mom_cluster_pre_kernel<T>, nc, 0, I.stream, I.p, I.g, red_umax, se);
         for (int ivar = 1; ivar <= 3; ++ivar) {
             mom_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * rs);
-            mom_small_mid_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, ivar, I.mom_scratch, se, red_umax);
+            mom_small_mid_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, ivar, I.mom_scratch, se, red_umax,
+                                                                      wide);
             if (nc > 1)
                 launch_cluster(mom_cluster_mid_kernel<T>, nc, sm, I.stream, I.p, I.g, ivar, I.mom_scratch, se);
         }
         pp_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * rs);
-        mom_small_post_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, I.mom_scratch, se, I.red_mom, nbs);
+        mom_small_post_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, I.mom_scratch, se, I.red_mom, nbs,
+                                                                   wide);
         if (nc > 1)
             launch_cluster(mom_cluster_post_kernel<T>, nc, sm, I.stream, I.p, I.g, I.mom_scratch, se,
                            (const double *)I.red_mom, nbs);

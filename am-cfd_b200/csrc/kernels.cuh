@@ -98,7 +98,8 @@ struct Inst {
     AsmMaps asm_maps[2];      // by property parity
     T *mom_scratch = nullptr; // one field: line-solve scratch of the small-box momentum path
     size_t mom_small_smem = 0;  // its dynamic shared memory
-    int mom_cluster = 1;        // CTAs of the cluster that takes boxes past one CTA's shared memory
+    int mom_cluster = 0;        // CTAs of the cluster that takes boxes past one CTA's shared memory
+                                // (set by setup_mom_small from the request here: 0 = default)
     // launch shapes picked by the autotuner (or pinned by the options)
     int asm_kseg = 0;           // planes per CTA of the energy assembly (0: the default rule)
     int sweep_warps = 4;        // warps (lines) per CTA of the whole-domain red-black sweeps

@@ -354,6 +354,8 @@ def main():
                          "host (default: one graph per step, iterations chained on the device)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--mom-cluster", type=int, default=0, choices=[0, 1, 2, 4, 8, 16],
+                    help="CTAs of the cluster momentum solve (1: none, 0: the library default)")
     ap.add_argument("--profile-window", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop, so that "
                          "ncu --profile-from-start off captures those launches only")
@@ -428,7 +430,7 @@ def main():
         kw = dict(asm_kseg=tune[p]["asm_kseg"], sweep_warps=tune[p]["sweep_warps"]) if p in tune else \
             dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
         sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
-                          host_loop=1 if args.host_loop else 0, **kw)
+                          host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster, **kw)
         tune.setdefault(p, sv.tuning())
         return sv
 

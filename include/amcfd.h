@@ -166,7 +166,11 @@ typedef struct amcfd_options {
                             for bit pin it (asm_kseg). */
     int asm_kseg;        /* planes per CTA of the energy assembly: 4, 8 or 16; 0 = default/tuned */
     int sweep_warps;     /* lines (warps) per CTA of the red-black sweeps: 2, 4 or 8; 0 = default/tuned */
-    int reserved[2];
+    int mom_cluster;     /* CTAs of the cluster that solves a momentum box larger than one CTA's
+                            shared memory (red-black order): 2, 4, 8 or 16, at most what the
+                            device schedules; 1 = no cluster (such boxes take the multi-kernel
+                            path); 0 = the default */
+    int reserved[1];
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;
@@ -272,7 +276,10 @@ int amcfd_tuning(const amcfd_ctx *ctx, int *asm_kseg, int *sweep_warps, double *
 /* Parameter sweep over independent instances: runs nsteps time steps of every
  * context in ctxs[0..n), each on its own stream, spread over nthreads host threads
  * (0 = one per context, at most 64).  A thread takes the next context in array
- * order and runs all its steps, so pass the contexts largest first.  reports[q]
+ * order and runs all its steps, so pass the contexts largest first.  The first
+ * step of the first context of each kind (precision, order, graph use) runs on the
+ * calling thread before the others start: it loads every kernel that kind
+ * launches, so that no thread loads a kernel while another captures a graph.  reports[q]
  * receives the last step's report of ctxs[q] and status[q] its return code (0, or
  * a negative AMCFD_E_* code; that context's amcfd_last_error says why); either may
  * be NULL.  Returns 0 when every context succeeded, else the first failing code in

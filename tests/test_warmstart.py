@@ -62,6 +62,7 @@ def test_trained_warm_start_saves_outer_iterations(tmp_path):
     assert np.isfinite(losses).all()
     ev = W.evaluate(net, held, 25, precision=amcfd.PREC_FP32, ref_maxit=200)
     s = ev["summary"]
+    print({k: v for k, v in s.items() if not isinstance(v, (list, tuple))})
     assert s["fallback_rate"] < 0.5, s
     assert s["iters_warm"] < s["iters_plain"], s
     assert s["temp_err_warm"] <= max(3.0 * s["temp_err_plain"], 0.03), s
