@@ -954,24 +954,33 @@ template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, sweep_exact_kernel<T, true>, 32 * warps, smem);
     return std::max(1, std::min(nb, nb2));
 }
+// A kernel's dynamic shared-memory limit is one value per process, shared by every
+// context: it is only ever raised, so that a context with a smaller grid never
+// lowers it under what another context's launches need.
+static cudaError_t raise_smem_limit(const void *func, size_t need)
+{
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, func);
+    if (e != cudaSuccess) return e;
+    if ((int)need <= a.maxDynamicSharedSizeBytes) return cudaSuccess;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
 template <typename T> void set_sweep_smem_limit(size_t smem)
 {
-    cudaFuncSetAttribute(sweep_exact_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(sweep_exact_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(sweep_rb_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    raise_smem_limit((const void *)sweep_exact_kernel<T, false>, smem);
+    raise_smem_limit((const void *)sweep_exact_kernel<T, true>, smem);
+    raise_smem_limit((const void *)sweep_rb_kernel<T, true>, smem);
 }
 // The whole-domain red-black kernel's buffer (qr and pr of each warp's line): the
-// most warps per CTA (8, 4 or 2) whose buffers fit 200 KiB, with the attribute set
+// most warps per CTA (8, 4 or 2) whose buffers fit 200 KiB, with the limit raised
 // for them; 0 when not even 2 fit.
 template <typename T> int set_rounds_smem_limit(const Params &p)
 {
     for (int w = 8; w >= 2; w /= 2) {
         const size_t need = rounds_smem<T>(p, w);
         if (need > 200 * 1024) continue;
-        if (cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)need) == cudaSuccess &&
-            cudaFuncSetAttribute(sweep_rb_rounds_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)need) == cudaSuccess)
+        if (raise_smem_limit((const void *)sweep_rb_rounds_kernel<T, false>, need) == cudaSuccess &&
+            raise_smem_limit((const void *)sweep_rb_rounds_kernel<T, true>, need) == cudaSuccess)
             return w;
     }
     return 0;

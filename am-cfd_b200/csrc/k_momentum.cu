@@ -1290,8 +1290,12 @@ template <typename T> int mom_small_capacity(const Inst<T> &I)
     return I.mom_cluster > 1 ? one * I.mom_cluster / 2 : one;
 }
 
-// Default cluster size of the box solve (the options may pin another).
-constexpr int kDefaultCluster = 8;
+// Default cluster size of the box solve (the options may pin another): none.  On
+// the 400 x 200 x 100 deck's steady box (about 5800 cells) the cluster path took
+// 0.246 / 0.256 / 0.299 ms per outer iteration with 4 / 8 / 16 CTAs against 0.211
+// for the multi-kernel path: a cluster launch of the line solve spends its time at
+// the barriers between colour passes (27 % issue active, 51 us a launch).
+constexpr int kDefaultCluster = 1;
 
 // Cluster size of the small-box kernels: the largest the device schedules with
 // this shared memory, at most 16.

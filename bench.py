@@ -52,8 +52,9 @@ WORDS_REDBLACK = {"energy_assemble": 40, "factor": 0, "energy_sweeps": 42, "h2t_
 # FP32 bulk); the line reports them scaled by the cell count.
 # The red-black sweep figure is the average over the 8 launches of an iteration
 # (the first sweep of each colour also forms and stores the factorisation).
-TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 87.1, "energy_sweeps:fp32:redblack": 21.2,
-                    "h2t_meltpool:fp32:redblack": 29.4}
+TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 87.0, "energy_sweeps:fp32:redblack": 21.2,
+                    "h2t_meltpool:fp32:redblack": 29.4, "energy_assemble:fp32dc:redblack": 146.2,
+                    "energy_sweeps:fp32dc:redblack": 21.2}
 
 
 def _peaks():

@@ -169,7 +169,8 @@ typedef struct amcfd_options {
     int mom_cluster;     /* CTAs of the cluster that solves a momentum box larger than one CTA's
                             shared memory (red-black order): 2, 4, 8 or 16, at most what the
                             device schedules; 1 = no cluster (such boxes take the multi-kernel
-                            path); 0 = the default */
+                            path); 0 = the default, 1 (the multi-kernel path measured faster
+                            on the benchmark decks' boxes) */
     int reserved[1];
 } amcfd_options;
 

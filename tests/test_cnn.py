@@ -1,9 +1,11 @@
 """Warm-start network: tensor-core forward and backward passes against the
 FP64 numpy restatement (oracle/cnn_oracle.py) with BF16 operand rounding.
 
-Tolerances: BF16 operands (8-bit mantissa) with FP32 accumulation over 27 x 32
-terms per output: outputs within 2e-2 relative L2, parameter gradients within
-5e-2 relative L2 per layer, the loss within 1e-2 relative.
+Tolerances: the restatement rounds to BF16 at the same points, so what is left
+is FP32 accumulation against FP64 and the BF16 roundings that this flips (an
+activation one BF16 step apart): outputs within 5e-3 relative L2, every
+layer's weight and bias gradients within 5e-3, the loss within 1e-3 (measured on
+B200: outputs 5.9e-4, gradients at most 2.5e-3, loss 4.4e-6).
 """
 import numpy as np
 import pytest
@@ -78,10 +80,10 @@ def test_forward_and_gradients_match_oracle():
           for ls in O.layer_slices()]
     print(f"outputs {ey:.2e}, loss {abs(loss - lo) / abs(lo):.2e}, "
           "gradients (W, b) per layer " + " ".join(f"({a:.2e}, {b:.2e})" for a, b in eg))
-    assert ey <= 2e-2, ey
-    assert abs(loss - lo) <= 1e-2 * abs(lo), (loss, lo)
+    assert ey <= 5e-3, ey
+    assert abs(loss - lo) <= 1e-3 * abs(lo), (loss, lo)
     for l, (a, b) in enumerate(eg):
-        assert a <= 5e-2 and b <= 5e-2, (l, a, b)
+        assert a <= 5e-3 and b <= 5e-3, (l, a, b)
     net.close()
 
 

@@ -142,7 +142,8 @@ def test_option_checks_before_any_device_work(tmp_path):
                dict(order=amcfd.ORDER_REDBLACK, precision=7),
                dict(order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, wait_polls=-5),
                dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, asm_kseg=5),
-               dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, sweep_warps=3)):
+               dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, sweep_warps=3),
+               dict(order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, mom_cluster=3)):
         opts = amcfd.AmcfdOptions(**kw)
         h = C.c_void_p()
         assert amcfd.lib().amcfd_create(C.byref(d.params), C.byref(opts), C.byref(h)) == -1, kw

@@ -247,3 +247,26 @@ def test_small_box_momentum_matches_grid_path(prec, deckdir):
     assert b.launches < a.launches
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec,order", [(0, 0), (1, 1)])
+def test_contexts_of_different_grid_widths_coexist(prec, order, deckdir):
+    """Kernel launch limits are per process, shared by all contexts: creating a
+    context on a narrow grid after one on a wide grid leaves the wide one's line
+    sweeps launchable (the limit is only ever raised), with and without graphs."""
+    import amcfd
+    import amcfd_decks as D
+    wide = amcfd.Deck(D.small("wide", nx=300, ny=14, nz=10, steps=2).write(deckdir + "/wide"))
+    narrow = amcfd.Deck(D.small("narrow", nx=20, ny=12, nz=8, steps=2).write(deckdir + "/narrow"))
+    for graphs in (0, 1):
+        a = amcfd.Solver(wide, order=order, precision=prec, use_graphs=graphs)
+        b = amcfd.Solver(narrow, order=order, precision=prec, use_graphs=graphs)
+        ra = [a.step() for _ in range(2)]
+        b.step()
+        c = amcfd.Solver(wide, order=order, precision=prec, use_graphs=graphs)
+        rc = [c.step() for _ in range(2)]
+        assert [r["niter"] for r in ra] == [r["niter"] for r in rc]
+        for f in FIELDS:
+            assert np.array_equal(a.get(f), c.get(f)), (graphs, f)
+        for s in (a, b, c):
+            s.close()
