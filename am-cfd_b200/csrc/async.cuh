@@ -75,6 +75,13 @@ __device__ __forceinline__ void fence_proxy_async()
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Orders earlier generic-proxy writes of global memory before later async-proxy
+// copies that read them.
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 // 1-D bulk copy global -> shared (both 16-byte aligned, bytes a multiple of 16).
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {

@@ -122,6 +122,8 @@ struct amcfd_ctx {
     double tune_ms[6] = {0};       // the autotuner's measured candidates
     int mom_cluster = 1;           // CTAs of the cluster momentum path (1: none)
     int mom_cluster_req = 0;       // as requested by the options (0: default)
+    int serial_launch = 0;         // 1: no programmatic dependent launch, box solve per pass
+    int box_ctas = 0;              // CTAs of the cooperative box solve (0: what the box needs)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
@@ -439,6 +441,7 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     cudaDeviceGetAttribute(&I.sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
     I.stream = ctx->stream;
     I.order = ctx->order;
+    I.pdl = !ctx->serial_launch;
     I.nb_las = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 255) / 256));
     I.nb_bc = std::max(1, std::min(I.sm_count * 2, (p.ni * p.nj + 2 * p.nk * (p.ni + p.nj) + 255) / 256));
     I.asm_kseg = ctx->asm_kseg;
@@ -524,6 +527,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     // per warp: 8 staged coefficient rows + one mbarrier (k_linesolve.cu)
     I.line_smem = (size_t)I.exact_warps * 8 * p.nip * sizeof(T) + (size_t)I.exact_warps * 8;
     set_sweep_smem_limit<T>(I.line_smem);
+    setup_box_solve<T>(I, !ctx->serial_launch);
+    if (ctx->box_ctas > 0 && I.box_grid > 0) I.box_grid = std::min(ctx->box_ctas, I.box_grid);
     I.sweep_warps_max = set_rounds_smem_limit<T>(p);
     if (I.sweep_warps_max < 2) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
     if (ctx->sweep_warps > I.sweep_warps_max)
@@ -816,7 +821,12 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : sweeps;
     case AMCFD_PHASE_H2T: return ctx->dc ? 2 : 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
-    case AMCFD_PHASE_MOMENTUM: return small ? (ctx->mom_cluster > 1 ? 14 : 9) : 2 + 4 * (3 + sweeps) + 2 + 1;
+    case AMCFD_PHASE_MOMENTUM: {
+        // per equation applyBCs, assembly and the line solve: one cooperative launch,
+        // or the factorisation and the sweeps
+        const bool coop = (ctx->precision == AMCFD_PREC_FP64 ? ctx->I64.box_grid : ctx->I32.box_grid) > 0;
+        return small ? (ctx->mom_cluster > 1 ? 14 : 9) : 2 + 4 * (coop ? 3 : 3 + sweeps) + 2 + 1;
+    }
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;
     case AMCFD_PHASE_SPECIES: return ctx->prm.species ? (ctx->order == AMCFD_ORDER_EXACT ? 4 : 3) + sweeps : 0;
@@ -1308,6 +1318,9 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
             opts->mom_cluster != 8 && opts->mom_cluster != 16)
             return fail(ctx, AMCFD_E_ARG, "mom_cluster must be 0, 1, 2, 4, 8 or 16");
         ctx->mom_cluster_req = opts->mom_cluster;
+        ctx->serial_launch = opts->serial_launch != 0;
+        if (opts->box_ctas < 0) return fail(ctx, AMCFD_E_ARG, "box_ctas must not be negative");
+        ctx->box_ctas = opts->box_ctas;
         ctx->autotune = opts->autotune != 0;
         ctx->asm_kseg = opts->asm_kseg;
         ctx->sweep_warps = opts->sweep_warps;

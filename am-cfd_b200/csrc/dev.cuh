@@ -77,6 +77,8 @@ struct Status {
     int nonfinite;     // a reduction produced NaN/Inf
     unsigned long long seq_energy, done_energy, ticket_energy;
     unsigned long long seq_mom, done_mom, ticket_mom;
+    // grid barrier of the cooperative momentum-box solve: arrivals, generation
+    unsigned gbar_count, gbar_gen;
 };
 
 // Outer-loop control of a step captured as one CUDA graph (a chain of
@@ -271,5 +273,19 @@ __device__ __forceinline__ void ld16(const T *ptr, T (&o)[16 / sizeof(T)])
 
 // Bounded spin budget for every device-side wait (about one second).
 constexpr long long kSpinLimit = 1ll << 24;
+
+// Programmatic dependent launch.  Every kernel of the outer iteration calls this
+// before it touches memory.  Launched with programmatic stream serialisation
+// (launch_k), it waits here until the kernel before it in the stream has
+// completed and that kernel's writes are visible, then releases the launch of
+// the kernel after it, whose CTAs become resident and wait in their own
+// pdl_enter: a launch's latency overlaps the run of the kernel before it instead
+// of following its drain.  Launched without the attribute, both instructions
+// return at once.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 
 }  // namespace amcfd

@@ -78,6 +78,7 @@ template <typename T, int SCH, bool DC>
 __global__ void __launch_bounds__(256, AsmBox<T>::MINB)
 energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant__ AsmMaps mp, DcBuf dco)
 {
+    pdl_enter();
     using R = T;
     using B = AsmBox<T>;
     constexpr int OX = B::OX, BX = B::BX, FE = B::FE;
@@ -549,13 +550,13 @@ template <typename T, bool DC> static void assemble_scheme(Inst<T> &I, const Asm
     const size_t sm = AsmBox<T>::SMEM;
     switch (I.p.scheme) {
     case AMCFD_SCHEME_UPWIND:
-        energy_assemble_kernel<T, 0, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        launch_k(I.pdl, energy_assemble_kernel<T, 0, DC>, I.asm_grid, blk, sm, I.stream, I.p, I.g, I.red_asm, m, I.dc);
         break;
     case AMCFD_SCHEME_POWER_LAW:
-        energy_assemble_kernel<T, 1, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        launch_k(I.pdl, energy_assemble_kernel<T, 1, DC>, I.asm_grid, blk, sm, I.stream, I.p, I.g, I.red_asm, m, I.dc);
         break;
     default:
-        energy_assemble_kernel<T, 2, DC><<<I.asm_grid, blk, sm, I.stream>>>(I.p, I.g, I.red_asm, m, I.dc);
+        launch_k(I.pdl, energy_assemble_kernel<T, 2, DC>, I.asm_grid, blk, sm, I.stream, I.p, I.g, I.red_asm, m, I.dc);
         break;
     }
 }

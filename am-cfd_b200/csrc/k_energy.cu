@@ -13,6 +13,7 @@ namespace amcfd {
 template <typename T>
 __global__ void laser_kernel(Params p, Fields<T> g, double *red)
 {
+    pdl_enter();
     const Status *st = g.st;
     double acc = 0.0;
     const double rb2 = p.alasrb * p.alasrb;
@@ -45,6 +46,7 @@ __global__ void laser_kernel(Params p, Fields<T> g, double *red)
 template <typename T>
 __global__ void energy_bc_kernel(Params p, Fields<T> g, double *red)
 {
+    pdl_enter();
     Status *st = g.st;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         if (p.nheattable > 0) {
@@ -124,6 +126,7 @@ __global__ void energy_bc_kernel(Params p, Fields<T> g, double *red)
 template <typename T>
 __global__ void __launch_bounds__(256) bc_reduce_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     __shared__ double sh[8][33];
     const int i = blockIdx.x * 32 + threadIdx.x, w = blockIdx.y, nip = p.nip;
     double s = 0.0;
@@ -235,6 +238,7 @@ template <typename T>
 __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, int nblk_asm,
                                      int check_finite, int ivar)
 {
+    pdl_enter();
     extern __shared__ double sm[];  // 4 * nip
     const int nip = p.nip, nim2 = p.nim2;
     double *bl = sm, *blp = sm + nip, *blm = sm + 2 * nip, *blc = sm + 3 * nip;
@@ -269,6 +273,7 @@ __global__ void block_correct_kernel(Params p, Fields<T> gd, double *red_asm, in
 template <typename T>
 __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, double *red)
 {
+    pdl_enter();
     const Status *st = g.st;
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
     const int nim1 = p.nim1, njm1 = p.njm1, nkm1 = p.nkm1, nim2 = p.nim2, njm2 = p.njm2,
@@ -511,6 +516,7 @@ template <typename T>
 __global__ void __launch_bounds__(1024) meltpool_kernel(Params p, Fields<T> g, const double *red_h2t,
                                                         int nblk_h2t)
 {
+    pdl_enter();
     Status *st = g.st;
     __shared__ double scratch[40];
     extern __shared__ double colv[];  // 3 * nip doubles + nip ints
@@ -639,6 +645,7 @@ __global__ void converge_kernel(Params p, Fields<T> gd, const double *red_h2t, i
                                 const double *red_mom, int nb_mom, double tol, int check_finite,
                                 LoopCtl lc)
 {
+    pdl_enter();
     __shared__ double scratch[40];
     __shared__ double scr8[8 * 33];
     Status *st = gd.st;
@@ -714,6 +721,7 @@ void launch_loop_init(Status *st, const LoopCtl &lc, cudaStream_t s)
 template <typename T>
 __global__ void update_solutions_kernel(Params p, Fields<T> g, double trackindx, int trackid)
 {
+    pdl_enter();
     const size_t total = (size_t)p.nk * p.nj * p.nip;
     const T ts = (T)p.tsolid;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
@@ -743,17 +751,16 @@ __global__ void update_solutions_kernel(Params p, Fields<T> g, double trackindx,
 // ---------------------------------------------------------------------------
 template <typename T> void launch_laser(Inst<T> &I)
 {
-    laser_kernel<T><<<I.nb_las, 256, 0, I.stream>>>(I.p, I.g, I.red_las);
+    launch_k(I.pdl, laser_kernel<T>, I.nb_las, 256, 0, I.stream, I.p, I.g, I.red_las);
 }
 template <typename T> void launch_energy_bc(Inst<T> &I)
 {
-    energy_bc_kernel<T><<<I.nb_bc, 256, 0, I.stream>>>(I.p, I.g, I.red_bc);
+    launch_k(I.pdl, energy_bc_kernel<T>, I.nb_bc, 256, 0, I.stream, I.p, I.g, I.red_bc);
 }
 template <typename T> void launch_block_correct(Inst<T> &I, int ivar)
 {
-    bc_reduce_kernel<T><<<dim3(I.p.nip / 32, 4), dim3(32, 8), 0, I.stream>>>(I.p, I.g);
-    block_correct_kernel<T><<<1, 1024, 4 * I.p.nip * sizeof(double), I.stream>>>(
-        I.p, I.g, I.red_asm, I.nb_asm, I.check_finite, ivar);
+    launch_k(I.pdl, bc_reduce_kernel<T>, dim3(I.p.nip / 32, 4), dim3(32, 8), 0, I.stream, I.p, I.g);
+    launch_k(I.pdl, block_correct_kernel<T>, 1, 1024, 4 * I.p.nip * sizeof(double), I.stream, I.p, I.g, I.red_asm, I.nb_asm, I.check_finite, ivar);
 }
 // Field read-out: the padded [k][j][nip] array widened to FP64 and packed to
 // the reference's unpadded [k][j][ni] layout (CFDSolverManager.cpp:249), so
@@ -813,22 +820,22 @@ template <typename T> int h2t_blocks_per_sm()
 }
 template <typename T> void launch_h2t(Inst<T> &I)
 {
-    h2t_kernel<T><<<I.nb_h2t, 256, 0, I.stream>>>(I.p, I.g, I.red_h2t);
+    launch_k(I.pdl, h2t_kernel<T>, I.nb_h2t, 256, 0, I.stream, I.p, I.g, I.red_h2t);
 }
 template <typename T> void launch_meltpool(Inst<T> &I)
 {
     size_t smem = 3 * (size_t)I.p.nip * sizeof(double) + (size_t)I.p.nip * sizeof(int);
-    meltpool_kernel<T><<<1, 1024, smem, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t);
+    launch_k(I.pdl, meltpool_kernel<T>, 1, 1024, smem, I.stream, I.p, I.g, I.red_h2t, I.nb_h2t);
 }
 template <typename T> void launch_converge(Inst<T> &I, double tol, const LoopCtl &lc)
 {
-    converge_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_h2t, I.nb_h2t, I.red_bc, I.nb_bc,
+    launch_k(I.pdl, converge_kernel<T>, 1, 1024, 0, I.stream, I.p, I.g, I.red_h2t, I.nb_h2t, I.red_bc, I.nb_bc,
                                                   I.red_las, I.nb_las, I.red_mom, I.nb_mom, tol,
                                                   I.check_finite, lc);
 }
 template <typename T> void launch_update_solutions(Inst<T> &I)
 {
-    update_solutions_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g, I.trackindx, I.trackid);
+    launch_k(I.pdl, update_solutions_kernel<T>, I.grid_1d, 256, 0, I.stream, I.p, I.g, I.trackindx, I.trackid);
 }
 
 #define AMCFD_INST(T)                                        \

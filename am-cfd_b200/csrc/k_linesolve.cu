@@ -38,6 +38,7 @@ namespace amcfd {
 template <typename T, bool BOX>
 __global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g, T *phi)
 {
+    pdl_enter();
     __shared__ T tap[32][33], taw[32][33], tae[32][33], tph[32][33];
     const Status *st = g.st;
     int i0, i1, j0, j1, k0, k1;
@@ -109,7 +110,7 @@ template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) {
 // aligned cell ib <= i0 and is rounded up to whole 16-byte units (never past
 // the padded row, nip being a multiple of 32 cells).
 // ---------------------------------------------------------------------------
-enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N };
+enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N, S_Q = S_N };
 
 template <typename T>
 __device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int ib, int ie, T *sl,
@@ -194,15 +195,18 @@ __device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T 
 
 // One x-line solved by one warp from its staged rows.  `row` is the offset of
 // node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
-// ends; sl holds the line from cell ib on.
+// ends; sl holds the line from cell ib on.  The right-hand side and the forward
+// recurrence go to row `qrow` of sl: the source row S_SU itself (consumed), or
+// the scratch row S_Q of a buffer that keeps the line's rows for later passes.
 template <typename T, bool COHERENT>
 __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
-                                             size_t sj, size_t sk, T *sl, int nmax)
+                                             size_t sj, size_t sk, T *sl, int nmax, int qrow = S_SU)
 {
     const int lane = threadIdx.x & 31;
-    T *sat = sl + S_AT * nmax, *sab = sl + S_AB * nmax, *san = sl + S_AN * nmax,
-      *sas = sl + S_AS * nmax, *se = sl + S_SU * nmax, *sc = sl + S_CF * nmax,
-      *sp = sl + S_PR * nmax, *sid = sl + S_ID * nmax;
+    const T *sat = sl + S_AT * nmax, *sab = sl + S_AB * nmax, *san = sl + S_AN * nmax,
+            *sas = sl + S_AS * nmax, *ssu = sl + S_SU * nmax, *sc = sl + S_CF * nmax,
+            *sp = sl + S_PR * nmax, *sid = sl + S_ID * nmax;
+    T *se = sl + (size_t)qrow * nmax;
     auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
     // right-hand side e_i = d_i / den_i, coalesced neighbour rows; four
     // iterations' neighbour loads are issued before any result is stored
@@ -224,7 +228,7 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
             const int iu = i + 32 * u;
             if (iu < i0 || iu > i1) continue;
             const int s = iu - ib;
-            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + se[s];
+            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + ssu[s];
             se[s] = d * sid[s];
         }
     }
@@ -359,6 +363,7 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
 template <typename T, bool BOX>
 __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 {
+    pdl_enter();
     extern __shared__ unsigned char smraw[];
     const Status *st = g.st;
     if (BOX && !st->momentum_active) return;
@@ -400,6 +405,163 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 }
 
 // ---------------------------------------------------------------------------
+// Barrier over the first n CTAs of a cooperative launch (all co-resident).  The
+// last CTA to arrive resets the count and advances the generation; the others
+// poll the generation at most `limit` times, then record AMCFD_E_TIMEOUT (detail
+// `where`).  Writes of a CTA before the barrier are visible to every CTA after
+// it (CTA barrier, then a GPU-scope fence on either side of the arrival).  False
+// once a device error is raised; a context whose device wait gave up stays
+// failed, so the count left behind by an abandoned barrier is never used again.
+// ---------------------------------------------------------------------------
+__device__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned n, Status *st, long long limit, int where)
+{
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned g0 = *(volatile unsigned *)gen;
+        __threadfence();
+        if (atomicAdd(count, 1u) == n - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicAdd(gen, 1u);
+        } else {
+            long long it = 0;
+            while (*(volatile unsigned *)gen == g0) {
+                if ((it & 63) == 63 && *(volatile int *)&st->error) { ok = 0; break; }
+                if (++it > limit) {
+                    if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        ok_s = ok && *(volatile int *)&st->error == 0;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// ---------------------------------------------------------------------------
+// Momentum-box line solve of one equation in red-black order as one
+// cooperative launch (solveLiquidDomain, CFDSolverManager.cpp:2367-2454): the
+// factorisation of every line, then the four sweeps x two colours with a grid
+// barrier between colour passes.  Same arithmetic, in the same order, as the
+// multi-launch form (factor_kernel<T, true>, then eight sweep_rb_kernel<T, true>
+// launches), so the same bits.  Warp w of the W warps that take part solves
+// lines w, w + W, ... of each colour.  When no warp has more than one line of a
+// colour ("resident"), a warp's two lines stay in its two shared-memory buffers
+// (coefficient rows, factorisation, and a scratch row for the recurrences) for
+// all eight passes, and a pass reads only the neighbouring lines' phi, from L2:
+// other CTAs wrote them.  Otherwise the factorisation goes to pr, cf, iden and
+// every visit stages its line again.  CTAs past the W / warps-per-CTA that the
+// box needs return at once and take no part in the barriers.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) box_rb_solve_kernel(Params p, Fields<T> g, T *phi)
+{
+    pdl_enter();
+    extern __shared__ unsigned char smraw[];
+    Status *st = g.st;
+    if (!st->momentum_active || *(volatile int *)&st->error) return;
+    int i0, i1, j0, j1, k0, k1;
+    box_of<true>(p, st, i0, i1, j0, j1, k0, k1);
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int half = (J + 1) / 2, nl = half * K;  // line slots of a colour
+    const int nact = min((int)gridDim.x, (nl + wpb - 1) / wpb);
+    if ((int)blockIdx.x >= nact) return;
+    const int W = nact * wpb, gw = blockIdx.x * wpb + warp;
+    const bool resident = nl <= W;
+    const int nmax = p.nip;
+    const size_t slot = (size_t)(S_N + 1) * nmax;  // the staged rows and the scratch row
+    T *buf = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * slot;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<T *>(smraw) + (size_t)wpb * 2 * slot) + warp;
+    if (lane == 0) mbar_init(bar);
+    __syncwarp();
+    uint32_t parity = 0;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    int ib, ie;
+    stage_window<T>(i0, i1, ib, ie);
+    const int n = i1 - i0 + 1, o = i0 - ib;
+    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
+    // node (0, j, k) of slot q of colour c; false past the box's last row
+    auto line_row = [&](int c, int q, size_t &row) {
+        const int kk = q / half, r = q - kk * half, k = k0 + kk;
+        const int j = j0 + ((c - k - j0) % 2 + 2) % 2 + 2 * r;
+        row = cidx(0, j, k, nj, nip);
+        return j <= j1;
+    };
+    bool ok = true;
+    // factorisation: factor_kernel's recurrence and guard on |den| (:2438-2439),
+    // one lane over the line's staged ap, aw, ae (held in the iden, cf, pr rows)
+    for (int c = 0; c < 2; ++c)
+        for (int q = gw; q < nl && ok; q += W) {
+            size_t row;
+            if (!line_row(c, q, row)) continue;
+            T *sl = buf + (resident ? c : 0) * slot;
+            if (lane == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(bar, bytes * S_N);
+                const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.aw, g.ae, g.ap};  // S_CF S_PR S_ID <- aw ae ap
+#pragma unroll
+                for (int r = 0; r < S_N; ++r) bulk_load(sl + (size_t)r * nmax, src[r] + row + ib, bytes, bar);
+            }
+            ok = mbar_wait(bar, parity, st, -3);
+            parity ^= 1u;
+            if (!ok) break;
+            T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
+            if (lane == 0) {
+                T prv = T(0);
+                for (int i = 0; i < n; ++i) {
+                    T den = sid[i] - scf[i] * prv;
+                    if (fabs(den) <= T(1e-12)) den += T(kSmall);
+                    const T id = T(1) / den;
+                    const T pv = spr[i] * id;
+                    spr[i] = pv;
+                    scf[i] = scf[i] * id;
+                    sid[i] = id;
+                    prv = pv;
+                }
+            }
+            __syncwarp();
+            if (!resident) {
+                for (int i = lane; i < n; i += 32) {
+                    g.pr[row + i0 + i] = spr[i];
+                    g.cf[row + i0 + i] = scf[i];
+                    g.iden[row + i0 + i] = sid[i];
+                }
+                fence_proxy_async_global();  // before the copies that stage these rows again
+                __syncwarp();
+            }
+        }
+    // the eight colour passes
+    for (int pass = 0; pass < 8; ++pass) {
+        const int c = pass & 1;
+        if (pass > 0 && !grid_barrier(&st->gbar_count, &st->gbar_gen, (unsigned)nact, st, p.wait_polls, -2))
+            return;
+        for (int q = gw; q < nl && ok; q += W) {
+            size_t row;
+            if (!line_row(c, q, row)) continue;
+            T *sl = buf + (resident ? c : 0) * slot;
+            if (!resident) {
+                if (lane == 0) stage_line<T>(g, row, ib, ie, sl, nmax, bar);
+                ok = mbar_wait(bar, parity, st, -3);
+                parity ^= 1u;
+                if (!ok) break;
+                __syncwarp();
+            }
+            solve_staged<T, true>(phi, row, i0, i1, ib, sj, sk, sl, nmax, resident ? S_Q : S_SU);
+            __syncwarp();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Red-black sweep of the whole domain (enthalpy, avgconcentration) in rounds,
 // one warp per line.  In round m lane l holds the 16-byte vector of V cells
 // starting at i = ib + 32 V m + V l (V = 4 in FP32, 2 in FP64; ib = i0 rounded
@@ -437,6 +599,7 @@ template <typename T, bool FACTOR>
 __global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
                                                               int correct)
 {
+    pdl_enter();
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int RC = 32 * V;
     extern __shared__ unsigned char smraw[];
@@ -657,6 +820,7 @@ __device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d)
 template <typename T>
 __global__ void __launch_bounds__(128) factor_rounds_kernel(Params p, Fields<T> g, T *phi)
 {
+    pdl_enter();
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int RC = 32 * V;
     const int i0 = 1, i1 = p.nim2;
@@ -756,6 +920,7 @@ template <typename T> size_t rounds_smem(const Params &p, int warps)
 __global__ void __launch_bounds__(1024) box_tickets_kernel(Params p, int2 *tickets, int *ntickets,
                                                            Status *st)
 {
+    pdl_enter();
     __shared__ int cnt[1024];
     if (!st->momentum_active) return;
     const int J = st->jend - st->jstat + 1, M = p.nkm2 - st->kstat + 1;
@@ -813,14 +978,14 @@ template <typename T> void launch_phi_factor(Inst<T> &I, T *phi)
 {
     if (I.order != AMCFD_ORDER_EXACT) return;
     const int lines = (I.p.nj - 2) * (I.p.nk - 2);
-    factor_rounds_kernel<T><<<std::max(1, (lines + 3) / 4), 128, 0, I.stream>>>(I.p, I.g, phi);
+    launch_k(I.pdl, factor_rounds_kernel<T>, std::max(1, (lines + 3) / 4), 128, 0, I.stream, I.p, I.g, phi);
 }
 template <typename T> void launch_energy_factor(Inst<T> &I) { launch_phi_factor<T>(I, I.g.h); }
 template <typename T> void launch_box_factor(Inst<T> &I)
 {
     // the box is small (a melt pool); one CTA per SM covers up to 4736 lines per pass
     int grid = std::min((I.max_lines + 31) / 32, I.sm_count);
-    factor_kernel<T, true><<<grid, 256, 0, I.stream>>>(I.p, I.g, nullptr);
+    launch_k(I.pdl, factor_kernel<T, true>, grid, 256, 0, I.stream, I.p, I.g, nullptr);
 }
 template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
 {
@@ -840,7 +1005,7 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
         int grid = std::max(1, std::min((I.max_lines / 2 + warps - 1) / warps + 1, I.sm_count));
         for (int sweep = 0; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color)
-                sweep_rb_kernel<T, true><<<grid, 32 * warps, smem, I.stream>>>(I.p, I.g, phi, color);
+                launch_k(I.pdl, sweep_rb_kernel<T, true>, grid, 32 * warps, smem, I.stream, I.p, I.g, phi, color);
     } else {
         // whole domain: one line per warp, sweep_warps warps per CTA
         const int w = I.sweep_warps;
@@ -848,10 +1013,11 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
         const int grid = std::max(1, (lines + w - 1) / w);
         const size_t rs = rounds_smem<T>(I.p, w);
         for (int color = 0; color < 2; ++color)
-            sweep_rb_rounds_kernel<T, true><<<grid, 32 * w, rs, I.stream>>>(I.p, I.g, phi, color, color == 0);
+            launch_k(I.pdl, sweep_rb_rounds_kernel<T, true>, grid, 32 * w, rs, I.stream, I.p, I.g, phi, color,
+                     color == 0);
         for (int sweep = 1; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color)
-                sweep_rb_rounds_kernel<T, false><<<grid, 32 * w, rs, I.stream>>>(I.p, I.g, phi, color, 0);
+                launch_k(I.pdl, sweep_rb_rounds_kernel<T, false>, grid, 32 * w, rs, I.stream, I.p, I.g, phi, color, 0);
     }
 }
 template <typename T> void launch_energy_sweeps(Inst<T> &I) { sweeps<T>(I, I.g.h, false); }
@@ -863,8 +1029,8 @@ template <typename T> void launch_sweep_probe(Inst<T> &I, T *phi, int warps)
     const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
     const int grid = std::max(1, (lines + warps - 1) / warps);
     const size_t rs = rounds_smem<T>(I.p, warps);
-    sweep_rb_rounds_kernel<T, true><<<grid, 32 * warps, rs, I.stream>>>(I.p, I.g, phi, 0, 0);
-    sweep_rb_rounds_kernel<T, false><<<grid, 32 * warps, rs, I.stream>>>(I.p, I.g, phi, 1, 0);
+    launch_k(I.pdl, sweep_rb_rounds_kernel<T, true>, grid, 32 * warps, rs, I.stream, I.p, I.g, phi, 0, 0);
+    launch_k(I.pdl, sweep_rb_rounds_kernel<T, false>, grid, 32 * warps, rs, I.stream, I.p, I.g, phi, 1, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -889,11 +1055,12 @@ void launch_dc_sweeps(Inst<double> &I)
     const int grid = std::max(1, (lines + w - 1) / w);
     const size_t rs = rounds_smem<float>(I.p, w);
     for (int color = 0; color < 2; ++color)
-        sweep_rb_rounds_kernel<float, true><<<grid, 32 * w, rs, I.stream>>>(I.p, f, d.delta, color,
+        launch_k(I.pdl, sweep_rb_rounds_kernel<float, true>, grid, 32 * w, rs, I.stream, I.p, f, d.delta, color,
                                                                              color == 0 ? 2 : 0);
     for (int sweep = 1; sweep < 4; ++sweep)
         for (int color = 0; color < 2; ++color)
-            sweep_rb_rounds_kernel<float, false><<<grid, 32 * w, rs, I.stream>>>(I.p, f, d.delta, color, 0);
+            launch_k(I.pdl, sweep_rb_rounds_kernel<float, false>, grid, 32 * w, rs, I.stream, I.p, f, d.delta, color,
+                     0);
 }
 
 // One factorising and one plain pass of the defect-correction sweeps with `warps`
@@ -910,14 +1077,15 @@ void launch_dc_sweep_probe(Inst<double> &I, int warps)
     const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
     const int grid = std::max(1, (lines + warps - 1) / warps);
     const size_t rs = rounds_smem<float>(I.p, warps);
-    sweep_rb_rounds_kernel<float, true><<<grid, 32 * warps, rs, I.stream>>>(I.p, f, d.delta, 0, 2);
-    sweep_rb_rounds_kernel<float, false><<<grid, 32 * warps, rs, I.stream>>>(I.p, f, d.delta, 1, 0);
+    launch_k(I.pdl, sweep_rb_rounds_kernel<float, true>, grid, 32 * warps, rs, I.stream, I.p, f, d.delta, 0, 2);
+    launch_k(I.pdl, sweep_rb_rounds_kernel<float, false>, grid, 32 * warps, rs, I.stream, I.p, f, d.delta, 1, 0);
 }
 
 // h += delta over the interior (delta is zero elsewhere), 16-byte vectors of
 // delta: four FP32 corrections onto two FP64 vectors of h.
 __global__ void __launch_bounds__(256) dc_apply_kernel(double *h, const float *delta, size_t n4)
 {
+    pdl_enter();
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n4; q += (size_t)gridDim.x * blockDim.x) {
         const float4 d = reinterpret_cast<const float4 *>(delta)[q];
         double2 *hp = reinterpret_cast<double2 *>(h) + 2 * q;
@@ -932,7 +1100,7 @@ void launch_dc_apply(Inst<double> &I)
 {
     // the padded pitch is a multiple of 32, so the array is a whole number of 4-vectors
     const size_t n4 = (size_t)I.p.nk * I.p.nj * I.p.nip / 4;
-    dc_apply_kernel<<<I.grid_1d, 256, 0, I.stream>>>(I.g.h, I.dc.delta, n4);
+    launch_k(I.pdl, dc_apply_kernel, I.grid_1d, 256, 0, I.stream, I.g.h, I.dc.delta, n4);
 }
 template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi) { sweeps<T>(I, phi, false); }
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
@@ -940,9 +1108,53 @@ template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
     T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
     sweeps<T>(I, phi, true);
 }
+static cudaError_t raise_smem_limit(const void *func, size_t need);
+
+// The momentum box's red-black line solve of one equation as one cooperative
+// launch (box_rb_solve_kernel); false when the context has none (exact order, the
+// serial launch form, or x-lines too long for its buffers).
+template <typename T> bool launch_box_solve(Inst<T> &I, int ivar)
+{
+    if (I.order != AMCFD_ORDER_REDBLACK || I.box_grid <= 0) return false;
+    T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.gridDim = dim3(I.box_grid);
+    cfg.blockDim = dim3(32 * I.box_warps);
+    cfg.dynamicSmemBytes = I.box_smem;
+    cfg.stream = I.stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, box_rb_solve_kernel<T>, I.p, I.g, phi);
+    return true;
+}
+// Launch shape of box_rb_solve_kernel: the most warps per CTA (4, 2 or 1) whose
+// buffers (two lines of 8 staged rows and a scratch row each, one mbarrier) fit
+// 200 KiB, and as many CTAs as the box's largest colour needs, at most as many as
+// are resident at once (a cooperative launch).  box_grid 0: none fits.
+template <typename T> void setup_box_solve(Inst<T> &I, bool enable)
+{
+    I.box_grid = 0;
+    if (!enable || I.order != AMCFD_ORDER_REDBLACK) return;
+    for (int w = 4; w >= 1; w /= 2) {
+        const size_t need = (size_t)w * (2 * (S_N + 1) * (size_t)I.p.nip * sizeof(T) + 8);
+        if (need > 200 * 1024) continue;
+        if (raise_smem_limit((const void *)box_rb_solve_kernel<T>, need) != cudaSuccess) return;
+        int bps = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, box_rb_solve_kernel<T>, 32 * w, need);
+        if (bps < 1) return;
+        const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);  // most lines of a colour
+        I.box_warps = w;
+        I.box_smem = need;
+        I.box_grid = std::max(1, std::min((lines + w - 1) / w, bps * I.sm_count));
+        return;
+    }
+}
 template <typename T> void launch_box_tickets(Inst<T> &I)
 {
-    box_tickets_kernel<<<1, 1024, 0, I.stream>>>(I.p, I.g.tickets_mom, I.g.ntickets_mom, I.g.st);
+    launch_k(I.pdl, box_tickets_kernel, 1, 1024, 0, I.stream, I.p, I.g.tickets_mom, I.g.ntickets_mom, I.g.st);
 }
 
 // Occupancy of the persistent sweep (host helper used at context creation).
@@ -995,6 +1207,8 @@ template <typename T> int set_rounds_smem_limit(const Params &p)
     template void launch_phi_sweeps<T>(Inst<T> &, T *);                  \
     template void launch_box_sweeps<T>(Inst<T> &, int);                  \
     template void launch_box_tickets<T>(Inst<T> &);                      \
+    template bool launch_box_solve<T>(Inst<T> &, int);                   \
+    template void setup_box_solve<T>(Inst<T> &, bool);                   \
     template int exact_sweep_blocks_per_sm<T>(int, size_t);              \
     template void set_sweep_smem_limit<T>(size_t);                       \
     template int set_rounds_smem_limit<T>(const Params &);

@@ -53,6 +53,7 @@ __device__ __forceinline__ void clean_cell(const Params &p, const Fields<T> &g, 
 template <typename T>
 __global__ void clean_velocities_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     Box b;
     if (!get_box(g.st, p, b)) return;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
@@ -123,6 +124,7 @@ __device__ __forceinline__ double mom_bc_item(const Params &p, const Fields<T> &
 template <typename T>
 __global__ void mom_bc_kernel(Params p, Fields<T> g, int ivar, double *red_umax)
 {
+    pdl_enter();
     Box b;
     const Status *st = g.st;
     double umax = 0.0;
@@ -354,6 +356,7 @@ __device__ __forceinline__ double mom_assemble_cell(const Params &p, const Field
 template <typename T>
 __global__ void __launch_bounds__(256) mom_assemble_kernel(Params p, Fields<T> g, int ivar, double *red)
 {
+    pdl_enter();
     Box b;
     double sumd = 0.0;
     if (get_box(g.st, p, b)) {
@@ -411,6 +414,7 @@ __device__ __forceinline__ void pp_assemble_cell(const Params &p, const Fields<T
 template <typename T>
 __global__ void __launch_bounds__(256) pp_assemble_kernel(Params p, Fields<T> g, double *red)
 {
+    pdl_enter();
     Box b;
     double resorm = 0.0, denom = 0.0;
     if (get_box(g.st, p, b)) {
@@ -452,6 +456,7 @@ __device__ __forceinline__ void correct_pressure_cell(const Params &p, const Fie
 template <typename T>
 __global__ void correct_velocity_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     Box b;
     if (!get_box(g.st, p, b)) return;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
@@ -463,6 +468,7 @@ __global__ void correct_velocity_kernel(Params p, Fields<T> g)
 template <typename T>
 __global__ void correct_pressure_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     Box b;
     if (!get_box(g.st, p, b)) return;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < b.n; q += gridDim.x * blockDim.x) {
@@ -532,6 +538,7 @@ __device__ void mom_finalize_body(const Params &p, Status *st, const double *red
 template <typename T>
 __global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, int nb)
 {
+    pdl_enter();
     __shared__ double scratch[40];
     Status *st = g.st;
     if (!st->momentum_active) return;
@@ -1149,6 +1156,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_small_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems, int wide)
 {
+    pdl_enter();
     __shared__ double sh[32];
     Status *st = g.st;
     Box b;
@@ -1167,6 +1175,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_small_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems, double *red_umax, int wide)
 {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double sh[32];
     Status *st = g.st;
@@ -1182,6 +1191,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_small_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb, int wide)
 {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double scratch_r[40];
     Status *st = g.st;
@@ -1210,6 +1220,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_cluster_pre_kernel(Params p, Fields<T> g, double *red_umax, int smem_elems)
 {
+    pdl_enter();
     __shared__ double sh[32];
     __shared__ double cmax;
     Status *st = g.st;
@@ -1239,6 +1250,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_cluster_mid_kernel(Params p, Fields<T> g, int ivar, T *scratch, int smem_elems)
 {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     Status *st = g.st;
     Box b;
@@ -1254,6 +1266,7 @@ template <typename T>
 __global__ void __launch_bounds__(kMomThreads, 1)
 mom_cluster_post_kernel(Params p, Fields<T> g, T *scratch, int smem_elems, const double *red, int nb)
 {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double scratch_r[40];
     Status *st = g.st;
@@ -1343,22 +1356,25 @@ template <typename T> void setup_mom_small(Inst<T> &I)
     I.mom_cluster = I.mom_cluster > 0 ? std::min(I.mom_cluster, most) : std::min(kDefaultCluster, most);
 }
 
-// A launch of nc CTAs forming one cluster.
+// A launch of nc CTAs forming one cluster (with `pdl`, also programmatic stream
+// serialisation, as launch_k).
 template <typename... K, typename... A>
-static void launch_cluster(void (*kern)(K...), int nc, size_t smem, cudaStream_t s, A... args)
+static void launch_cluster(bool pdl, void (*kern)(K...), int nc, size_t smem, cudaStream_t s, A... args)
 {
     cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
+    cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
     at[0].val.clusterDim.x = nc;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
     cfg.gridDim = dim3(nc);
     cfg.blockDim = dim3(kMomThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     cfg.attrs = at;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = pdl ? 2 : 1;
     cudaLaunchKernelEx(&cfg, kern, static_cast<K>(args)...);
 }
 
@@ -1382,39 +1398,44 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
         const int nc = I.mom_cluster;
         const size_t sm = I.mom_small_smem;
         const int wide = nc > 1;
-        mom_small_pre_kernel<T><<<1, kMomThreads, 0, I.stream>>>(I.p, I.g, red_umax, se, wide);
-        if (nc > 1) launch_cluster(mom_cluster_pre_kernel<T>, nc, 0, I.stream, I.p, I.g, red_umax, se);
+        launch_k(I.pdl, mom_small_pre_kernel<T>, 1, kMomThreads, 0, I.stream, I.p, I.g, red_umax, se, wide);
+        if (nc > 1) launch_cluster(I.pdl, mom_cluster_pre_kernel<T>, nc, 0, I.stream, I.p, I.g, red_umax, se);
         for (int ivar = 1; ivar <= 3; ++ivar) {
-            mom_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * rs);
-            mom_small_mid_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, ivar, I.mom_scratch, se, red_umax,
-                                                                      wide);
+            launch_k(I.pdl, mom_assemble_kernel<T>, nbs, 256, 0, I.stream, I.p, I.g, ivar,
+                     I.red_mom + (ivar - 1) * rs);
+            launch_k(I.pdl, mom_small_mid_kernel<T>, 1, kMomThreads, sm, I.stream, I.p, I.g, ivar, I.mom_scratch,
+                     se, red_umax, wide);
             if (nc > 1)
-                launch_cluster(mom_cluster_mid_kernel<T>, nc, sm, I.stream, I.p, I.g, ivar, I.mom_scratch, se);
+                launch_cluster(I.pdl, mom_cluster_mid_kernel<T>, nc, sm, I.stream, I.p, I.g, ivar, I.mom_scratch,
+                               se);
         }
-        pp_assemble_kernel<T><<<nbs, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * rs);
-        mom_small_post_kernel<T><<<1, kMomThreads, sm, I.stream>>>(I.p, I.g, I.mom_scratch, se, I.red_mom, nbs,
-                                                                   wide);
+        launch_k(I.pdl, pp_assemble_kernel<T>, nbs, 256, 0, I.stream, I.p, I.g, I.red_mom + 3 * rs);
+        launch_k(I.pdl, mom_small_post_kernel<T>, 1, kMomThreads, sm, I.stream, I.p, I.g, I.mom_scratch, se,
+                 I.red_mom, nbs, wide);
         if (nc > 1)
-            launch_cluster(mom_cluster_post_kernel<T>, nc, sm, I.stream, I.p, I.g, I.mom_scratch, se,
+            launch_cluster(I.pdl, mom_cluster_post_kernel<T>, nc, sm, I.stream, I.p, I.g, I.mom_scratch, se,
                            (const double *)I.red_mom, nbs);
         return;
     }
     launch_box_tickets<T>(I);
-    clean_velocities_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
+    launch_k(I.pdl, clean_velocities_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
     for (int ivar = 1; ivar <= 4; ++ivar) {
-        mom_bc_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + 4 * region);
+        launch_k(I.pdl, mom_bc_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, ivar, I.red_mom + 4 * region);
         if (ivar <= 3)
-            mom_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, ivar, I.red_mom + (ivar - 1) * region);
+            launch_k(I.pdl, mom_assemble_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, ivar,
+                     I.red_mom + (ivar - 1) * region);
         else
-            pp_assemble_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g, I.red_mom + 3 * region);
-        launch_box_factor<T>(I);
-        launch_box_sweeps<T>(I, ivar);
+            launch_k(I.pdl, pp_assemble_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, I.red_mom + 3 * region);
+        if (!launch_box_solve<T>(I, ivar)) {
+            launch_box_factor<T>(I);
+            launch_box_sweeps<T>(I, ivar);
+        }
         if (ivar == 4) {
-            correct_velocity_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
-            correct_pressure_kernel<T><<<nb, 256, 0, I.stream>>>(I.p, I.g);
+            launch_k(I.pdl, correct_velocity_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
+            launch_k(I.pdl, correct_pressure_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
         }
     }
-    mom_finalize_kernel<T><<<1, 1024, 0, I.stream>>>(I.p, I.g, I.red_mom, nb);
+    launch_k(I.pdl, mom_finalize_kernel<T>, 1, 1024, 0, I.stream, I.p, I.g, I.red_mom, nb);
 }
 
 template void launch_momentum<double>(Inst<double> &, bool);

@@ -61,6 +61,7 @@ __device__ __forceinline__ T species_a1(const Params &p, const Fields<T> &g, int
 template <typename T>
 __global__ void __launch_bounds__(256) species_bc_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     const int ni = p.ni, nj = p.nj, nk = p.nk, nip = p.nip;
     const long long fij = (long long)ni * nj, fik = (long long)ni * nk, fjk = (long long)nj * nk;
     const long long total = 2 * (fij + fik + fjk);
@@ -105,6 +106,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSX * kSY)
 species_assemble_kernel(Params p, Fields<T> g, double *red)
 {
+    pdl_enter();
     using R = T;
     __shared__ double sb[4][kSY][kSX + 1];
     const Status *st = g.st;
@@ -208,6 +210,7 @@ species_assemble_kernel(Params p, Fields<T> g, double *red)
 template <typename T>
 __global__ void species_update_kernel(Params p, Fields<T> g)
 {
+    pdl_enter();
     const size_t total = (size_t)p.nk * p.nj * p.nip;
     const T kp = (T)p.kp;
     for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < total;
@@ -228,9 +231,9 @@ template <typename T> void launch_species(Inst<T> &I)
     const Params &p = I.p;
     const long long nb = 2ll * ((long long)p.ni * p.nj + (long long)p.ni * p.nk + (long long)p.nj * p.nk);
     const int grid = (int)std::max(1ll, std::min((long long)I.sm_count * 4, (nb + 255) / 256));
-    species_bc_kernel<T><<<grid, 256, 0, I.stream>>>(I.p, I.g);
+    launch_k(I.pdl, species_bc_kernel<T>, grid, 256, 0, I.stream, I.p, I.g);
     // the energy assembly's grid: its per-CTA partial buffers are reused
-    species_assemble_kernel<T><<<I.asm_grid, dim3(kSX, kSY), 0, I.stream>>>(I.p, I.g, I.red_asm);
+    launch_k(I.pdl, species_assemble_kernel<T>, I.asm_grid, dim3(kSX, kSY), 0, I.stream, I.p, I.g, I.red_asm);
     launch_block_correct<T>(I, 6);
     launch_phi_factor<T>(I, I.g.conc);
     launch_phi_sweeps<T>(I, I.g.conc);
@@ -238,7 +241,7 @@ template <typename T> void launch_species(Inst<T> &I)
 template <typename T> void launch_species_update(Inst<T> &I)
 {
     if (!I.p.species) return;
-    species_update_kernel<T><<<I.grid_1d, 256, 0, I.stream>>>(I.p, I.g);
+    launch_k(I.pdl, species_update_kernel<T>, I.grid_1d, 256, 0, I.stream, I.p, I.g);
 }
 
 template void launch_species<double>(Inst<double> &);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda.h>
 #include <cstdio>
+#include <utility>
 #include "dev.cuh"
 
 namespace amcfd {
@@ -111,7 +112,36 @@ struct Inst {
     // defect correction of the energy line solves (FP64 instances only)
     bool dc_on = false;
     DcBuf dc{};
+    // launches of the outer iteration overlap the end of the kernel before them
+    // (programmatic dependent launch, launch_k)
+    bool pdl = true;
+    // cooperative red-black line solve of the momentum box (box_grid 0: the
+    // multi-launch form): CTAs, warps per CTA, dynamic shared memory
+    int box_grid = 0, box_warps = 4;
+    size_t box_smem = 0;
 };
+
+// Launch of a kernel that begins with pdl_enter().  With `pdl` the launch carries
+// programmatic stream serialisation: it may start while the kernel before it in
+// the stream drains (the kernel's pdl_enter waits for that kernel's completion).
+template <typename... K, typename... A>
+inline void launch_k(bool pdl, void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                     A &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    if (pdl) {
+        at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[0].val.programmaticStreamSerializationAllowed = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+    }
+    cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 // launchers (k_energy.cu)
 template <typename T> void launch_laser(Inst<T> &I);
@@ -132,6 +162,8 @@ template <typename T> void launch_phi_factor(Inst<T> &I, T *phi);   // whole-dom
 template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi);
 template <typename T> void launch_box_factor(Inst<T> &I);
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
+template <typename T> bool launch_box_solve(Inst<T> &I, int ivar);
+template <typename T> void setup_box_solve(Inst<T> &I, bool enable);
 template <typename T> void launch_box_tickets(Inst<T> &I);
 // defect correction: the energy line sweeps in FP32 on the correction, and h += delta
 void launch_dc_sweeps(Inst<double> &I);

@@ -171,6 +171,17 @@ typedef struct amcfd_options {
                             device schedules; 1 = no cluster (such boxes take the multi-kernel
                             path); 0 = the default, 1 (the multi-kernel path measured faster
                             on the benchmark decks' boxes) */
+    int serial_launch;   /* 1: every kernel of an outer iteration is launched only after the
+                            kernel before it has finished; 0: a kernel's launch overlaps the
+                            end of the one before it (programmatic dependent launch: it
+                            still waits for that kernel's completion before it reads
+                            anything, so the results are the same bits); 1 also solves the
+                            momentum box's lines of an equation with a launch per colour pass
+                            instead of one cooperative launch */
+    int box_ctas;        /* CTAs of the cooperative momentum-box line solve (capped at what the
+                            largest box needs and what is resident at once); 0 = that cap
+                            (fewer make each warp take several lines of a colour, restaging
+                            them every pass) */
     int reserved[1];
 } amcfd_options;
 

@@ -177,6 +177,42 @@ def test_graph_replay_bit_identical(prec, order, deckdir):
     b.close()
 
 
+@pytest.mark.parametrize("prec,order,small_box,graphs,box_ctas", [(0, 0, 1, 1, 0), (1, 1, 1, 1, 0), (1, 1, 0, 1, 0),
+                                                                  (0, 1, 0, 0, 0), (2, 1, 1, 1, 0), (1, 1, 0, 1, 1),
+                                                                  (0, 1, 0, 1, 2)])
+def test_overlapped_launches_bit_identical(prec, order, small_box, graphs, box_ctas, deckdir):
+    """Launches that overlap the end of the kernel before them (programmatic
+    dependent launch, the default) and the momentum box's line solve as one
+    cooperative launch with grid barriers between the colour passes give the same
+    bits and iteration counts as the serial form (serial_launch: each launch
+    starts after the one before it has finished, one launch per colour pass):
+    every kernel waits for its predecessor's completion before it reads anything,
+    and the cooperative solve repeats the multi-launch arithmetic.  FP64 exact
+    order, FP32 red-black and FP32 defect correction; the one-CTA and the
+    multi-kernel momentum paths; graphs (the device-driven outer loop) and direct
+    launches; and the cooperative solve on 1 and 2 CTAs (box_ctas), where every
+    warp takes several lines of a colour and stages them again for each pass."""
+    import amcfd
+    import amcfd_decks as D
+    d = amcfd.Deck(D.small("pdl", steps=4, power=350.0, toolpath=True).write(deckdir))
+    kw = dict(order=order, precision=prec, use_graphs=graphs, small_box=small_box)
+    a = amcfd.Solver(d, serial_launch=1, **kw)
+    b = amcfd.Solver(d, serial_launch=0, box_ctas=box_ctas, **kw)
+    saw_box = False
+    for s in range(4):
+        ra, rb = a.step(), b.step()
+        saw_box |= rb["momentum_cells"] > 0
+        ctx = _mismatch_context(s, ra, rb)
+        for k in ("niter", "tpeak", "alen", "depth", "width", "resorh", "resorm", "ratio"):
+            assert ra[k] == rb[k], (k, ctx)
+        for f in FIELDS:
+            x, y = a.get(f), b.get(f)
+            assert np.array_equal(x, y), _field_mismatch(f, x, y, ctx)
+    assert saw_box
+    a.close()
+    b.close()
+
+
 def _mismatch_context(step, ra, rb):
     keys = ("niter", "itertot", "resorh", "resorm", "ratio", "tpeak", "momentum_cells")
     return f"step {step + 1}: direct " + str({k: ra[k] for k in keys}) + " graph " + str({k: rb[k] for k in keys})
