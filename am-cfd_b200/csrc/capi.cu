@@ -822,10 +822,13 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     case AMCFD_PHASE_H2T: return ctx->dc ? 2 : 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
     case AMCFD_PHASE_MOMENTUM: {
-        // per equation applyBCs, assembly and the line solve: one cooperative launch,
-        // or the factorisation and the sweeps
+        // cooperative: cleanVelocities, applyBCs(1), then per equation its assembly and
+        // one launch for the solve and what follows it; otherwise per equation
+        // applyBCs, assembly, factorisation and sweeps, then correctPressure
         const bool coop = (ctx->precision == AMCFD_PREC_FP64 ? ctx->I64.box_grid : ctx->I32.box_grid) > 0;
-        return small ? (ctx->mom_cluster > 1 ? 14 : 9) : 2 + 4 * (coop ? 3 : 3 + sweeps) + 2 + 1;
+        const int tickets = ctx->order == AMCFD_ORDER_EXACT ? 1 : 0;
+        if (small) return ctx->mom_cluster > 1 ? 14 : 9;
+        return coop ? 2 + 4 * 2 : tickets + 1 + 4 * (3 + sweeps) + 2 + 1;
     }
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;

@@ -144,7 +144,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     // per-plane metrics of this segment, converted once for the CTA (the same
     // values every thread would form)
     __shared__ double pl_dz[kKSEG];
-    __shared__ T pl_m[4][kKSEG];  // fracz[k], fracz[k-1], dzpbinv[k], dzpbinv[k+1]
+    __shared__ T pl_m[5][kKSEG];  // fracz[k], fracz[k-1], dzpbinv[k], dzpbinv[k+1], dz
     if (tid < ke - kb) {
         const int k = kb + tid;
         if (k >= 1 && k <= nkm2) {
@@ -153,6 +153,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
             pl_m[1][tid] = (T)g.fracz[k - 1];
             pl_m[2][tid] = (T)g.dzpbinv[k];
             pl_m[3][tid] = (T)g.dzpbinv[k + 1];
+            pl_m[4][tid] = (T)pl_dz[tid];
         }
     }
 
@@ -249,7 +250,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
             if (colint && k >= 1 && k <= nkm2) {
                 const int kl = k - kb;
                 const double dz = pl_dz[kl];
-                const R fdz = (R)dz;
+                const R fdz = pl_m[4][kl];
                 const R aik = kF32 ? fdx * fdz : (R)(dx * dz), ajk = kF32 ? fdy * fdz : (R)(dy * dz);
                 const R vol = kF32 ? aij * fdz : (R)(dx * dy * dz);
                 const R fz_k = pl_m[0][kl], fz_m = pl_m[1][kl];

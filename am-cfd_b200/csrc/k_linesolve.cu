@@ -23,6 +23,7 @@
 #include "kernels.cuh"
 #include "amcfd.h"
 #include "async.cuh"
+#include "linesolve.cuh"
 
 namespace amcfd {
 
@@ -98,154 +99,6 @@ __global__ void __launch_bounds__(256) factor_kernel(Params p, Fields<T> g, T *p
     }
 }
 
-// Load of a value another warp may have just written (bypasses L1).
-template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) { return __ldcg(ptr); }
-
-// ---------------------------------------------------------------------------
-// Per-warp staging of one x-line.  The eight pass-invariant coefficient rows of
-// the line (at ab an as su cf pr iden) are brought into shared memory with
-// TMA bulk copies completing on a per-warp mbarrier; the copies are issued
-// before the exact-order kernel waits on its neighbours, so their latency
-// overlaps the wait.  Rows start 16-byte aligned: the copy starts at the
-// aligned cell ib <= i0 and is rounded up to whole 16-byte units (never past
-// the padded row, nip being a multiple of 32 cells).
-// ---------------------------------------------------------------------------
-enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N, S_Q = S_N };
-
-template <typename T>
-__device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int ib, int ie, T *sl,
-                                           int nmax, uint64_t *bar)
-{
-    // lane 0 only.  Previous generic-proxy use of this shared buffer is ordered
-    // before the asynchronous copies by the proxy fence.
-    fence_proxy_async();
-    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
-    mbar_expect_tx(bar, bytes * S_N);
-    const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.cf, g.pr, g.iden};
-#pragma unroll
-    for (int q = 0; q < S_N; ++q) bulk_load(sl + (size_t)q * nmax, src[q] + row + ib, bytes, bar);
-}
-
-// ---------------------------------------------------------------------------
-// Thomas recurrences of one line by one warp, from shared-memory rows indexed
-// by i - i0: e (right-hand side / den on entry, the solution on exit), cf and
-// pr.  Each lane owns a contiguous chunk; the chunks are chained by warp scans
-// of affine maps (x -> A x + B), forward for qr_i = cf_i qr_{i-1} + e_i and
-// backward for phi_i = pr_i phi_{i+1} + qr_i; then the line is stored.
-template <typename T, bool COHERENT>
-__device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T *se, const T *sc,
-                                          const T *sp)
-{
-    const int lane = threadIdx.x & 31;
-    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
-    const int n = i1 - i0 + 1;
-    const int L = (n + 31) >> 5;
-    const int a = lane * L;
-    const int b = min(a + L, n);
-    T A = T(1), B = T(0);
-    for (int i = a; i < b; ++i) {
-        const T cfi = sc[i];
-        B = cfi * B + se[i];
-        A = cfi * A;
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T A2 = __shfl_up_sync(0xffffffffu, A, o);
-        T B2 = __shfl_up_sync(0xffffffffu, B, o);
-        if (lane >= o) {
-            B = A * B2 + B;
-            A = A * A2;
-        }
-    }
-    T Ae = __shfl_up_sync(0xffffffffu, A, 1);
-    T Be = __shfl_up_sync(0xffffffffu, B, 1);
-    if (lane == 0) { Ae = T(1); Be = T(0); }
-    T q = Ae * ldp(row + i0 - 1) + Be;
-    for (int i = a; i < b; ++i) {
-        q = sc[i] * q + se[i];
-        se[i] = q;
-    }
-    A = T(1);
-    B = T(0);
-    for (int i = b - 1; i >= a; --i) {
-        const T pri = sp[i];
-        B = pri * B + se[i];
-        A = pri * A;
-    }
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        T A2 = __shfl_down_sync(0xffffffffu, A, o);
-        T B2 = __shfl_down_sync(0xffffffffu, B, o);
-        if (lane + o < 32) {
-            B = A * B2 + B;
-            A = A * A2;
-        }
-    }
-    Ae = __shfl_down_sync(0xffffffffu, A, 1);
-    Be = __shfl_down_sync(0xffffffffu, B, 1);
-    if (lane == 31) { Ae = T(1); Be = T(0); }
-    T x = Ae * ldp(row + i1 + 1) + Be;
-    for (int i = b - 1; i >= a; --i) {
-        x = sp[i] * x + se[i];
-        se[i] = x;
-    }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) phi[row + i0 + i] = se[i];
-}
-
-// One x-line solved by one warp from its staged rows.  `row` is the offset of
-// node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
-// ends; sl holds the line from cell ib on.  The right-hand side and the forward
-// recurrence go to row `qrow` of sl: the source row S_SU itself (consumed), or
-// the scratch row S_Q of a buffer that keeps the line's rows for later passes.
-template <typename T, bool COHERENT>
-__device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
-                                             size_t sj, size_t sk, T *sl, int nmax, int qrow = S_SU)
-{
-    const int lane = threadIdx.x & 31;
-    const T *sat = sl + S_AT * nmax, *sab = sl + S_AB * nmax, *san = sl + S_AN * nmax,
-            *sas = sl + S_AS * nmax, *ssu = sl + S_SU * nmax, *sc = sl + S_CF * nmax,
-            *sp = sl + S_PR * nmax, *sid = sl + S_ID * nmax;
-    T *se = sl + (size_t)qrow * nmax;
-    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
-    // right-hand side e_i = d_i / den_i, coalesced neighbour rows; four
-    // iterations' neighbour loads are issued before any result is stored
-    constexpr int U = 4;
-    for (int i = ib + lane; i <= i1; i += 32 * U) {
-        T nt[U], nb[U], nn[U], ns[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int iu = i + 32 * u;
-            const bool ok = iu >= i0 && iu <= i1;
-            const size_t c = row + (ok ? iu : i0);
-            nt[u] = ok ? ldp(c + sk) : T(0);
-            nb[u] = ok ? ldp(c - sk) : T(0);
-            nn[u] = ok ? ldp(c + sj) : T(0);
-            ns[u] = ok ? ldp(c - sj) : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int iu = i + 32 * u;
-            if (iu < i0 || iu > i1) continue;
-            const int s = iu - ib;
-            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + ssu[s];
-            se[s] = d * sid[s];
-        }
-    }
-    __syncwarp();
-    const int o = i0 - ib;
-    scan_line<T, COHERENT>(phi, row, i0, i1, se + o, sc + o, sp + o);
-}
-
-// Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).
-template <typename T>
-__device__ __forceinline__ void stage_window(int i0, int i1, int &ib, int &ie)
-{
-    constexpr int V = 16 / sizeof(T);
-    ib = i0 & ~(V - 1);
-    ie = (i1 + 1 + V - 1) & ~(V - 1);
-}
-
 // Bounded wait until *f >= target (wrap-safe); false after `limit` polls or once
 // another warp has raised an error.
 __device__ bool wait_ge(const int *f, int target, Status *st, int where, long long limit)
@@ -260,17 +113,6 @@ __device__ bool wait_ge(const int *f, int target, Status *st, int where, long lo
             return false;
         }
         __nanosleep(64);
-    }
-}
-
-template <bool BOX>
-__device__ __forceinline__ void box_of(const Params &p, const Status *st, int &i0, int &i1,
-                                       int &j0, int &j1, int &k0, int &k1)
-{
-    if (BOX) {
-        i0 = st->istatp1; i1 = st->iendm1; j0 = st->jstat; j1 = st->jend; k0 = st->kstat; k1 = p.nkm2;
-    } else {
-        i0 = 1; i1 = p.nim2; j0 = 1; j1 = p.njm2; k0 = 1; k1 = p.nkm2;
     }
 }
 
@@ -401,163 +243,6 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
         __syncwarp();
         solve_staged<T, false>(phi, row, i0, i1, ib, sj, sk, sl, nmax);
         __syncwarp();
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Barrier over the first n CTAs of a cooperative launch (all co-resident).  The
-// last CTA to arrive resets the count and advances the generation; the others
-// poll the generation at most `limit` times, then record AMCFD_E_TIMEOUT (detail
-// `where`).  Writes of a CTA before the barrier are visible to every CTA after
-// it (CTA barrier, then a GPU-scope fence on either side of the arrival).  False
-// once a device error is raised; a context whose device wait gave up stays
-// failed, so the count left behind by an abandoned barrier is never used again.
-// ---------------------------------------------------------------------------
-__device__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned n, Status *st, long long limit, int where)
-{
-    __shared__ int ok_s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned g0 = *(volatile unsigned *)gen;
-        __threadfence();
-        if (atomicAdd(count, 1u) == n - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            long long it = 0;
-            while (*(volatile unsigned *)gen == g0) {
-                if ((it & 63) == 63 && *(volatile int *)&st->error) { ok = 0; break; }
-                if (++it > limit) {
-                    if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(32);
-            }
-        }
-        __threadfence();
-        ok_s = ok && *(volatile int *)&st->error == 0;
-    }
-    __syncthreads();
-    return ok_s != 0;
-}
-
-// ---------------------------------------------------------------------------
-// Momentum-box line solve of one equation in red-black order as one
-// cooperative launch (solveLiquidDomain, CFDSolverManager.cpp:2367-2454): the
-// factorisation of every line, then the four sweeps x two colours with a grid
-// barrier between colour passes.  Same arithmetic, in the same order, as the
-// multi-launch form (factor_kernel<T, true>, then eight sweep_rb_kernel<T, true>
-// launches), so the same bits.  Warp w of the W warps that take part solves
-// lines w, w + W, ... of each colour.  When no warp has more than one line of a
-// colour ("resident"), a warp's two lines stay in its two shared-memory buffers
-// (coefficient rows, factorisation, and a scratch row for the recurrences) for
-// all eight passes, and a pass reads only the neighbouring lines' phi, from L2:
-// other CTAs wrote them.  Otherwise the factorisation goes to pr, cf, iden and
-// every visit stages its line again.  CTAs past the W / warps-per-CTA that the
-// box needs return at once and take no part in the barriers.
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(128) box_rb_solve_kernel(Params p, Fields<T> g, T *phi)
-{
-    pdl_enter();
-    extern __shared__ unsigned char smraw[];
-    Status *st = g.st;
-    if (!st->momentum_active || *(volatile int *)&st->error) return;
-    int i0, i1, j0, j1, k0, k1;
-    box_of<true>(p, st, i0, i1, j0, j1, k0, k1);
-    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
-    if (J <= 0 || K <= 0 || i1 < i0) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    const int half = (J + 1) / 2, nl = half * K;  // line slots of a colour
-    const int nact = min((int)gridDim.x, (nl + wpb - 1) / wpb);
-    if ((int)blockIdx.x >= nact) return;
-    const int W = nact * wpb, gw = blockIdx.x * wpb + warp;
-    const bool resident = nl <= W;
-    const int nmax = p.nip;
-    const size_t slot = (size_t)(S_N + 1) * nmax;  // the staged rows and the scratch row
-    T *buf = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * slot;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<T *>(smraw) + (size_t)wpb * 2 * slot) + warp;
-    if (lane == 0) mbar_init(bar);
-    __syncwarp();
-    uint32_t parity = 0;
-    const int nj = p.nj, nip = p.nip;
-    const size_t sj = nip, sk = (size_t)nj * nip;
-    int ib, ie;
-    stage_window<T>(i0, i1, ib, ie);
-    const int n = i1 - i0 + 1, o = i0 - ib;
-    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
-    // node (0, j, k) of slot q of colour c; false past the box's last row
-    auto line_row = [&](int c, int q, size_t &row) {
-        const int kk = q / half, r = q - kk * half, k = k0 + kk;
-        const int j = j0 + ((c - k - j0) % 2 + 2) % 2 + 2 * r;
-        row = cidx(0, j, k, nj, nip);
-        return j <= j1;
-    };
-    bool ok = true;
-    // factorisation: factor_kernel's recurrence and guard on |den| (:2438-2439),
-    // one lane over the line's staged ap, aw, ae (held in the iden, cf, pr rows)
-    for (int c = 0; c < 2; ++c)
-        for (int q = gw; q < nl && ok; q += W) {
-            size_t row;
-            if (!line_row(c, q, row)) continue;
-            T *sl = buf + (resident ? c : 0) * slot;
-            if (lane == 0) {
-                fence_proxy_async();
-                mbar_expect_tx(bar, bytes * S_N);
-                const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.aw, g.ae, g.ap};  // S_CF S_PR S_ID <- aw ae ap
-#pragma unroll
-                for (int r = 0; r < S_N; ++r) bulk_load(sl + (size_t)r * nmax, src[r] + row + ib, bytes, bar);
-            }
-            ok = mbar_wait(bar, parity, st, -3);
-            parity ^= 1u;
-            if (!ok) break;
-            T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
-            if (lane == 0) {
-                T prv = T(0);
-                for (int i = 0; i < n; ++i) {
-                    T den = sid[i] - scf[i] * prv;
-                    if (fabs(den) <= T(1e-12)) den += T(kSmall);
-                    const T id = T(1) / den;
-                    const T pv = spr[i] * id;
-                    spr[i] = pv;
-                    scf[i] = scf[i] * id;
-                    sid[i] = id;
-                    prv = pv;
-                }
-            }
-            __syncwarp();
-            if (!resident) {
-                for (int i = lane; i < n; i += 32) {
-                    g.pr[row + i0 + i] = spr[i];
-                    g.cf[row + i0 + i] = scf[i];
-                    g.iden[row + i0 + i] = sid[i];
-                }
-                fence_proxy_async_global();  // before the copies that stage these rows again
-                __syncwarp();
-            }
-        }
-    // the eight colour passes
-    for (int pass = 0; pass < 8; ++pass) {
-        const int c = pass & 1;
-        if (pass > 0 && !grid_barrier(&st->gbar_count, &st->gbar_gen, (unsigned)nact, st, p.wait_polls, -2))
-            return;
-        for (int q = gw; q < nl && ok; q += W) {
-            size_t row;
-            if (!line_row(c, q, row)) continue;
-            T *sl = buf + (resident ? c : 0) * slot;
-            if (!resident) {
-                if (lane == 0) stage_line<T>(g, row, ib, ie, sl, nmax, bar);
-                ok = mbar_wait(bar, parity, st, -3);
-                parity ^= 1u;
-                if (!ok) break;
-                __syncwarp();
-            }
-            solve_staged<T, true>(phi, row, i0, i1, ib, sj, sk, sl, nmax, resident ? S_Q : S_SU);
-            __syncwarp();
-        }
     }
 }
 
@@ -1108,50 +793,6 @@ template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar)
     T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
     sweeps<T>(I, phi, true);
 }
-static cudaError_t raise_smem_limit(const void *func, size_t need);
-
-// The momentum box's red-black line solve of one equation as one cooperative
-// launch (box_rb_solve_kernel); false when the context has none (exact order, the
-// serial launch form, or x-lines too long for its buffers).
-template <typename T> bool launch_box_solve(Inst<T> &I, int ivar)
-{
-    if (I.order != AMCFD_ORDER_REDBLACK || I.box_grid <= 0) return false;
-    T *phi = ivar == 1 ? I.g.uvel : ivar == 2 ? I.g.vvel : ivar == 3 ? I.g.wvel : I.g.pp;
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeCooperative;
-    at[0].val.cooperative = 1;
-    cfg.gridDim = dim3(I.box_grid);
-    cfg.blockDim = dim3(32 * I.box_warps);
-    cfg.dynamicSmemBytes = I.box_smem;
-    cfg.stream = I.stream;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, box_rb_solve_kernel<T>, I.p, I.g, phi);
-    return true;
-}
-// Launch shape of box_rb_solve_kernel: the most warps per CTA (4, 2 or 1) whose
-// buffers (two lines of 8 staged rows and a scratch row each, one mbarrier) fit
-// 200 KiB, and as many CTAs as the box's largest colour needs, at most as many as
-// are resident at once (a cooperative launch).  box_grid 0: none fits.
-template <typename T> void setup_box_solve(Inst<T> &I, bool enable)
-{
-    I.box_grid = 0;
-    if (!enable || I.order != AMCFD_ORDER_REDBLACK) return;
-    for (int w = 4; w >= 1; w /= 2) {
-        const size_t need = (size_t)w * (2 * (S_N + 1) * (size_t)I.p.nip * sizeof(T) + 8);
-        if (need > 200 * 1024) continue;
-        if (raise_smem_limit((const void *)box_rb_solve_kernel<T>, need) != cudaSuccess) return;
-        int bps = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, box_rb_solve_kernel<T>, 32 * w, need);
-        if (bps < 1) return;
-        const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);  // most lines of a colour
-        I.box_warps = w;
-        I.box_smem = need;
-        I.box_grid = std::max(1, std::min((lines + w - 1) / w, bps * I.sm_count));
-        return;
-    }
-}
 template <typename T> void launch_box_tickets(Inst<T> &I)
 {
     launch_k(I.pdl, box_tickets_kernel, 1, 1024, 0, I.stream, I.p, I.g.tickets_mom, I.g.ntickets_mom, I.g.st);
@@ -1165,17 +806,6 @@ template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem)
     int nb2 = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, sweep_exact_kernel<T, true>, 32 * warps, smem);
     return std::max(1, std::min(nb, nb2));
-}
-// A kernel's dynamic shared-memory limit is one value per process, shared by every
-// context: it is only ever raised, so that a context with a smaller grid never
-// lowers it under what another context's launches need.
-static cudaError_t raise_smem_limit(const void *func, size_t need)
-{
-    cudaFuncAttributes a;
-    cudaError_t e = cudaFuncGetAttributes(&a, func);
-    if (e != cudaSuccess) return e;
-    if ((int)need <= a.maxDynamicSharedSizeBytes) return cudaSuccess;
-    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
 }
 template <typename T> void set_sweep_smem_limit(size_t smem)
 {
@@ -1207,8 +837,6 @@ template <typename T> int set_rounds_smem_limit(const Params &p)
     template void launch_phi_sweeps<T>(Inst<T> &, T *);                  \
     template void launch_box_sweeps<T>(Inst<T> &, int);                  \
     template void launch_box_tickets<T>(Inst<T> &);                      \
-    template bool launch_box_solve<T>(Inst<T> &, int);                   \
-    template void setup_box_solve<T>(Inst<T> &, bool);                   \
     template int exact_sweep_blocks_per_sm<T>(int, size_t);              \
     template void set_sweep_smem_limit<T>(size_t);                       \
     template int set_rounds_smem_limit<T>(const Params &);

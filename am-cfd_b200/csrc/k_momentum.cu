@@ -9,6 +9,7 @@
 #include <cooperative_groups.h>
 
 #include "kernels.cuh"
+#include "linesolve.cuh"
 #include "amcfd.h"
 
 namespace cg = cooperative_groups;
@@ -544,6 +545,182 @@ __global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, in
     if (!st->momentum_active) return;
     mom_finalize_body(p, st, red, nb, nb, scratch);
 }
+
+// ---------------------------------------------------------------------------
+// Momentum-box line solve of equation ivar (1..3: u, v, w; 4: p') in red-black
+// order as one cooperative launch (solveLiquidDomain, CFDSolverManager.cpp:
+// 2367-2454): the factorisation of every line, then the four sweeps x two
+// colours with a grid barrier between colour passes.  Same arithmetic, in the
+// same order, as the multi-launch form (factor_kernel<T, true>, then eight
+// sweep_rb_kernel<T, true> launches), so the same bits.  The launch also does
+// the work that follows the solve in the multi-launch chain: applyBCs(ivar + 1)
+// (its items touch only the next equation's unknown), or for p' correctPressure
+// (velocity correction, grid barrier, pressure update) and the momentum
+// residual normalisation (one CTA, from the partial sums of the assemblies).  Warp w of the W warps that take part solves
+// lines w, w + W, ... of each colour.  When no warp has more than one line of a
+// colour ("resident"), a warp's two lines stay in its two shared-memory buffers
+// (coefficient rows, factorisation, and a scratch row for the recurrences) for
+// all eight passes, and a pass reads only the neighbouring lines' phi, from L2:
+// other CTAs wrote them.  Otherwise the factorisation goes to pr, cf, iden and
+// every visit stages its line again.  CTAs past the W / warps-per-CTA that the
+// box needs return at once and take no part in the barriers.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> g, int ivar, const double *red, int nb)
+{
+    pdl_enter();
+    T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
+    extern __shared__ unsigned char smraw[];
+    Status *st = g.st;
+    if (!st->momentum_active || *(volatile int *)&st->error) return;
+    int i0, i1, j0, j1, k0, k1;
+    box_of<true>(p, st, i0, i1, j0, j1, k0, k1);
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int half = (J + 1) / 2, nl = half * K;  // line slots of a colour
+    const int nact = min((int)gridDim.x, (nl + wpb - 1) / wpb);
+    if ((int)blockIdx.x >= nact) return;
+    const int W = nact * wpb, gw = blockIdx.x * wpb + warp;
+    const bool resident = nl <= W;
+    // the barrier generation at the start of the launch: no CTA can advance it
+    // before every taking part has arrived at the first barrier
+    unsigned gen = *(volatile unsigned *)&st->gbar_gen;
+    const int nmax = p.nip;
+    const size_t slot = (size_t)(S_N + 1) * nmax;  // the staged rows and the scratch row
+    T *buf = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * slot;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(reinterpret_cast<T *>(smraw) + (size_t)wpb * 2 * slot) + warp;
+    if (lane == 0) mbar_init(bar);
+    __syncwarp();
+    uint32_t parity = 0;
+    const int nj = p.nj, nip = p.nip;
+    const size_t sj = nip, sk = (size_t)nj * nip;
+    int ib, ie;
+    stage_window<T>(i0, i1, ib, ie);
+    const int n = i1 - i0 + 1, o = i0 - ib;
+    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
+    // node (0, j, k) of slot q of colour c; false past the box's last row
+    auto line_row = [&](int c, int q, size_t &row) {
+        const int kk = q / half, r = q - kk * half, k = k0 + kk;
+        const int j = j0 + ((c - k - j0) % 2 + 2) % 2 + 2 * r;
+        row = cidx(0, j, k, nj, nip);
+        return j <= j1;
+    };
+    bool ok = true;
+    // staging of a line's rows for the factorisation: ap, aw, ae go to the
+    // iden, cf, pr rows (lane 0; the caller arms the barrier)
+    auto stage_factor_rows = [&](T *sl, size_t row) {
+        const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.aw, g.ae, g.ap};
+#pragma unroll
+        for (int r = 0; r < S_N; ++r) bulk_load(sl + (size_t)r * nmax, src[r] + row + ib, bytes, bar);
+    };
+    // factor_kernel's recurrence and guard on |den| (:2438-2439), in place
+    auto factor_line = [&](T *sl) {
+        T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
+        T prv = T(0);
+        for (int i = 0; i < n; ++i) {
+            T den = sid[i] - scf[i] * prv;
+            if (fabs(den) <= T(1e-12)) den += T(kSmall);
+            const T id = T(1) / den;
+            const T pv = spr[i] * id;
+            spr[i] = pv;
+            scf[i] = scf[i] * id;
+            sid[i] = id;
+            prv = pv;
+        }
+    };
+    if (resident) {
+        // both lines of the warp staged at once, factorised by lanes 0 and 1
+        size_t rows[2];
+        bool has[2];
+        for (int c = 0; c < 2; ++c) has[c] = gw < nl && line_row(c, gw, rows[c]);
+        if (has[0] || has[1]) {
+            if (lane == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(bar, bytes * S_N * ((has[0] ? 1u : 0u) + (has[1] ? 1u : 0u)));
+                for (int c = 0; c < 2; ++c)
+                    if (has[c]) stage_factor_rows(buf + c * slot, rows[c]);
+            }
+            ok = mbar_wait(bar, parity, st, -3);
+            parity ^= 1u;
+            if (ok && ((lane == 0 && has[0]) || (lane == 1 && has[1]))) factor_line(buf + lane * slot);
+            __syncwarp();
+        }
+    }
+    // otherwise one line at a time through buffer 0, the factorisation kept in
+    // pr, cf, iden for the passes to stage again
+    for (int c = 0; c < 2 && !resident; ++c)
+        for (int q = gw; q < nl && ok; q += W) {
+            size_t row;
+            if (!line_row(c, q, row)) continue;
+            T *sl = buf;
+            if (lane == 0) {
+                fence_proxy_async();
+                mbar_expect_tx(bar, bytes * S_N);
+                stage_factor_rows(sl, row);
+            }
+            ok = mbar_wait(bar, parity, st, -3);
+            parity ^= 1u;
+            if (!ok) break;
+            if (lane == 0) factor_line(sl);
+            __syncwarp();
+            const T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
+            for (int i = lane; i < n; i += 32) {
+                g.pr[row + i0 + i] = spr[i];
+                g.cf[row + i0 + i] = scf[i];
+                g.iden[row + i0 + i] = sid[i];
+            }
+            fence_proxy_async_global();  // before the copies that stage these rows again
+            __syncwarp();
+        }
+    // the eight colour passes
+    for (int pass = 0; pass < 8; ++pass) {
+        const int c = pass & 1;
+        if (pass > 0 && !grid_barrier(&st->gbar_count, &st->gbar_gen, ++gen, (unsigned)nact, st, p.wait_polls, -2))
+            return;
+        for (int q = gw; q < nl && ok; q += W) {
+            size_t row;
+            if (!line_row(c, q, row)) continue;
+            T *sl = buf + (resident ? c : 0) * slot;
+            if (!resident) {
+                if (lane == 0) stage_line<T>(g, row, ib, ie, sl, nmax, bar);
+                ok = mbar_wait(bar, parity, st, -3);
+                parity ^= 1u;
+                if (!ok) break;
+                __syncwarp();
+            }
+            solve_staged<T, true>(phi, row, i0, i1, ib, sj, sk, sl, nmax, resident ? S_Q : S_SU);
+            __syncwarp();
+        }
+    }
+    // ---- what follows the solve ----
+    Box b;
+    get_box(st, p, b);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, nt = nact * blockDim.x;
+    if (ivar <= 3) {
+        int ntop;
+        const int nbc = mom_bc_items(p, st, b, ivar + 1, ntop);
+        for (int q = t; q < nbc; q += nt) mom_bc_item<T>(p, g, st, b, ivar + 1, q, ntop);
+        return;
+    }
+    if (!grid_barrier(&st->gbar_count, &st->gbar_gen, ++gen, (unsigned)nact, st, p.wait_polls, -2)) return;
+    for (int q = t; q < b.n; q += nt) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_velocity_cell<T>(p, g, i, j, k);
+    }
+    if (!grid_barrier(&st->gbar_count, &st->gbar_gen, ++gen, (unsigned)nact, st, p.wait_polls, -2)) return;
+    for (int q = t; q < b.n; q += nt) {
+        int i, j, k;
+        box_cell(b, q, i, j, k);
+        correct_pressure_cell<T>(p, g, i, j, k);
+    }
+    if (blockIdx.x == 0) {
+        __shared__ double scratch[40];
+        mom_finalize_body(p, st, red, nb, nb, scratch);
+    }
+}
+
 
 // ---------------------------------------------------------------------------
 // Small melt-pool boxes (red-black line order).  A melt pool spans a few
@@ -1378,6 +1555,47 @@ static void launch_cluster(bool pdl, void (*kern)(K...), int nc, size_t smem, cu
     cudaLaunchKernelEx(&cfg, kern, static_cast<K>(args)...);
 }
 
+// The momentum box's red-black line solve of equation ivar as one cooperative
+// launch (mom_box_solve_kernel).
+template <typename T> static void launch_box_solve(Inst<T> &I, int ivar)
+{
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.gridDim = dim3(I.box_grid);
+    cfg.blockDim = dim3(32 * I.box_warps);
+    cfg.dynamicSmemBytes = I.box_smem;
+    cfg.stream = I.stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, mom_box_solve_kernel<T>, I.p, I.g, ivar, (const double *)I.red_mom, I.nb_mom);
+}
+// Launch shape of mom_box_solve_kernel: the most warps per CTA (4, 2 or 1) whose
+// buffers (two lines of 8 staged rows and a scratch row each, one mbarrier) fit
+// 200 KiB, and as many CTAs as the box's largest colour needs, at most as many as
+// are resident at once (a cooperative launch).  box_grid 0: none fits, or not
+// enabled (exact order; the serial launch form), and the chain keeps the
+// multi-launch line solve.
+template <typename T> void setup_box_solve(Inst<T> &I, bool enable)
+{
+    I.box_grid = 0;
+    if (!enable || I.order != AMCFD_ORDER_REDBLACK) return;
+    for (int w = 4; w >= 1; w /= 2) {
+        const size_t need = (size_t)w * (2 * (S_N + 1) * (size_t)I.p.nip * sizeof(T) + 8);
+        if (need > 200 * 1024) continue;
+        if (raise_smem_limit((const void *)mom_box_solve_kernel<T>, need) != cudaSuccess) return;
+        int bps = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, mom_box_solve_kernel<T>, 32 * w, need);
+        if (bps < 1) return;
+        const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);  // most lines of a colour
+        I.box_warps = w;
+        I.box_smem = need;
+        I.box_grid = std::max(1, std::min((lines + w - 1) / w, bps * I.sm_count));
+        return;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // launcher: the whole momentum chain of one outer iteration
 // ---------------------------------------------------------------------------
@@ -1417,7 +1635,23 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
                            (const double *)I.red_mom, nbs);
         return;
     }
-    launch_box_tickets<T>(I);
+    if (I.box_grid > 0) {
+        // red-black: per equation its assembly and one cooperative launch that
+        // solves it and applies the next equation's boundary conditions (for p',
+        // corrects velocity and pressure and normalises the residuals)
+        launch_k(I.pdl, clean_velocities_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
+        launch_k(I.pdl, mom_bc_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, 1, I.red_mom + 4 * region);
+        for (int ivar = 1; ivar <= 4; ++ivar) {
+            if (ivar <= 3)
+                launch_k(I.pdl, mom_assemble_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, ivar,
+                         I.red_mom + (ivar - 1) * region);
+            else
+                launch_k(I.pdl, pp_assemble_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, I.red_mom + 3 * region);
+            launch_box_solve<T>(I, ivar);
+        }
+        return;
+    }
+    if (I.order == AMCFD_ORDER_EXACT) launch_box_tickets<T>(I);  // the exact-order sweep's visit order
     launch_k(I.pdl, clean_velocities_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
     for (int ivar = 1; ivar <= 4; ++ivar) {
         launch_k(I.pdl, mom_bc_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, ivar, I.red_mom + 4 * region);
@@ -1426,10 +1660,8 @@ template <typename T> void launch_momentum(Inst<T> &I, bool small)
                      I.red_mom + (ivar - 1) * region);
         else
             launch_k(I.pdl, pp_assemble_kernel<T>, nb, 256, 0, I.stream, I.p, I.g, I.red_mom + 3 * region);
-        if (!launch_box_solve<T>(I, ivar)) {
-            launch_box_factor<T>(I);
-            launch_box_sweeps<T>(I, ivar);
-        }
+        launch_box_factor<T>(I);
+        launch_box_sweeps<T>(I, ivar);
         if (ivar == 4) {
             launch_k(I.pdl, correct_velocity_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
             launch_k(I.pdl, correct_pressure_kernel<T>, nb, 256, 0, I.stream, I.p, I.g);
@@ -1444,5 +1676,7 @@ template int mom_small_capacity<double>(const Inst<double> &);
 template int mom_small_capacity<float>(const Inst<float> &);
 template void setup_mom_small<double>(Inst<double> &);
 template void setup_mom_small<float>(Inst<float> &);
+template void setup_box_solve<double>(Inst<double> &, bool);
+template void setup_box_solve<float>(Inst<float> &, bool);
 
 }  // namespace amcfd

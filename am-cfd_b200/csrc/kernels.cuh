@@ -162,7 +162,6 @@ template <typename T> void launch_phi_factor(Inst<T> &I, T *phi);   // whole-dom
 template <typename T> void launch_phi_sweeps(Inst<T> &I, T *phi);
 template <typename T> void launch_box_factor(Inst<T> &I);
 template <typename T> void launch_box_sweeps(Inst<T> &I, int ivar);
-template <typename T> bool launch_box_solve(Inst<T> &I, int ivar);
 template <typename T> void setup_box_solve(Inst<T> &I, bool enable);
 template <typename T> void launch_box_tickets(Inst<T> &I);
 // defect correction: the energy line sweeps in FP32 on the correction, and h += delta

@@ -1,0 +1,228 @@
+// Line-solve primitives shared by the energy sweeps (k_linesolve.cu) and the
+// momentum-box solves (k_momentum.cu): per-warp staging of an x-line's
+// coefficient rows, the warp-scan Thomas recurrences of one line, the box
+// extents, and the grid barrier of the cooperative box solve.
+#pragma once
+#include "kernels.cuh"
+#include "amcfd.h"
+#include "async.cuh"
+
+namespace amcfd {
+
+// Load of a value another warp may have just written (bypasses L1).
+template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) { return __ldcg(ptr); }
+
+// ---------------------------------------------------------------------------
+// Per-warp staging of one x-line.  The eight pass-invariant coefficient rows of
+// the line (at ab an as su cf pr iden) are brought into shared memory with
+// TMA bulk copies completing on a per-warp mbarrier; the copies are issued
+// before the exact-order kernel waits on its neighbours, so their latency
+// overlaps the wait.  Rows start 16-byte aligned: the copy starts at the
+// aligned cell ib <= i0 and is rounded up to whole 16-byte units (never past
+// the padded row, nip being a multiple of 32 cells).
+// ---------------------------------------------------------------------------
+enum { S_AT = 0, S_AB, S_AN, S_AS, S_SU, S_CF, S_PR, S_ID, S_N, S_Q = S_N };
+
+template <typename T>
+__device__ __forceinline__ void stage_line(const Fields<T> &g, size_t row, int ib, int ie, T *sl,
+                                           int nmax, uint64_t *bar)
+{
+    // lane 0 only.  Previous generic-proxy use of this shared buffer is ordered
+    // before the asynchronous copies by the proxy fence.
+    fence_proxy_async();
+    const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
+    mbar_expect_tx(bar, bytes * S_N);
+    const T *src[S_N] = {g.at, g.ab, g.an, g.as, g.su, g.cf, g.pr, g.iden};
+#pragma unroll
+    for (int q = 0; q < S_N; ++q) bulk_load(sl + (size_t)q * nmax, src[q] + row + ib, bytes, bar);
+}
+
+// ---------------------------------------------------------------------------
+// Thomas recurrences of one line by one warp, from shared-memory rows indexed
+// by i - i0: e (right-hand side / den on entry, the solution on exit), cf and
+// pr.  Each lane owns a contiguous chunk; the chunks are chained by warp scans
+// of affine maps (x -> A x + B), forward for qr_i = cf_i qr_{i-1} + e_i and
+// backward for phi_i = pr_i phi_{i+1} + qr_i; then the line is stored.  lo and
+// hi are the fixed end values phi_{i0-1} and phi_{i1+1}.
+template <typename T>
+__device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T *se, const T *sc,
+                                          const T *sp, T lo, T hi)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = i1 - i0 + 1;
+    const int L = (n + 31) >> 5;
+    const int a = lane * L;
+    const int b = min(a + L, n);
+    T A = T(1), B = T(0);
+    for (int i = a; i < b; ++i) {
+        const T cfi = sc[i];
+        B = cfi * B + se[i];
+        A = cfi * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_up_sync(0xffffffffu, A, o);
+        T B2 = __shfl_up_sync(0xffffffffu, B, o);
+        if (lane >= o) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    T Ae = __shfl_up_sync(0xffffffffu, A, 1);
+    T Be = __shfl_up_sync(0xffffffffu, B, 1);
+    if (lane == 0) { Ae = T(1); Be = T(0); }
+    T q = Ae * lo + Be;
+    for (int i = a; i < b; ++i) {
+        q = sc[i] * q + se[i];
+        se[i] = q;
+    }
+    A = T(1);
+    B = T(0);
+    for (int i = b - 1; i >= a; --i) {
+        const T pri = sp[i];
+        B = pri * B + se[i];
+        A = pri * A;
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_down_sync(0xffffffffu, A, o);
+        T B2 = __shfl_down_sync(0xffffffffu, B, o);
+        if (lane + o < 32) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    Ae = __shfl_down_sync(0xffffffffu, A, 1);
+    Be = __shfl_down_sync(0xffffffffu, B, 1);
+    if (lane == 31) { Ae = T(1); Be = T(0); }
+    T x = Ae * hi + Be;
+    for (int i = b - 1; i >= a; --i) {
+        x = sp[i] * x + se[i];
+        se[i] = x;
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) phi[row + i0 + i] = se[i];
+}
+
+// One x-line solved by one warp from its staged rows.  `row` is the offset of
+// node (0, j, k); cells i0..i1 are unknowns, phi[i0-1] and phi[i1+1] the fixed
+// ends; sl holds the line from cell ib on.  The right-hand side and the forward
+// recurrence go to row `qrow` of sl: the source row S_SU itself (consumed), or
+// the scratch row S_Q of a buffer that keeps the line's rows for later passes.
+template <typename T, bool COHERENT>
+__device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1, int ib,
+                                             size_t sj, size_t sk, T *sl, int nmax, int qrow = S_SU)
+{
+    const int lane = threadIdx.x & 31;
+    const T *sat = sl + S_AT * nmax, *sab = sl + S_AB * nmax, *san = sl + S_AN * nmax,
+            *sas = sl + S_AS * nmax, *ssu = sl + S_SU * nmax, *sc = sl + S_CF * nmax,
+            *sp = sl + S_PR * nmax, *sid = sl + S_ID * nmax;
+    T *se = sl + (size_t)qrow * nmax;
+    auto ldp = [&](size_t c) -> T { return COHERENT ? ld_shared_row<T>(phi + c) : phi[c]; };
+    // the line's fixed ends, loaded with the neighbour rows rather than in the
+    // middle of the recurrences
+    const T lo = ldp(row + i0 - 1), hi = ldp(row + i1 + 1);
+    // right-hand side e_i = d_i / den_i, coalesced neighbour rows; four
+    // iterations' neighbour loads are issued before any result is stored
+    constexpr int U = 4;
+    for (int i = ib + lane; i <= i1; i += 32 * U) {
+        T nt[U], nb[U], nn[U], ns[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int iu = i + 32 * u;
+            const bool ok = iu >= i0 && iu <= i1;
+            const size_t c = row + (ok ? iu : i0);
+            nt[u] = ok ? ldp(c + sk) : T(0);
+            nb[u] = ok ? ldp(c - sk) : T(0);
+            nn[u] = ok ? ldp(c + sj) : T(0);
+            ns[u] = ok ? ldp(c - sj) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int iu = i + 32 * u;
+            if (iu < i0 || iu > i1) continue;
+            const int s = iu - ib;
+            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + ssu[s];
+            se[s] = d * sid[s];
+        }
+    }
+    __syncwarp();
+    const int o = i0 - ib;
+    scan_line<T>(phi, row, i0, i1, se + o, sc + o, sp + o, lo, hi);
+}
+
+// Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).
+template <typename T>
+__device__ __forceinline__ void stage_window(int i0, int i1, int &ib, int &ie)
+{
+    constexpr int V = 16 / sizeof(T);
+    ib = i0 & ~(V - 1);
+    ie = (i1 + 1 + V - 1) & ~(V - 1);
+}
+
+template <bool BOX>
+__device__ __forceinline__ void box_of(const Params &p, const Status *st, int &i0, int &i1,
+                                       int &j0, int &j1, int &k0, int &k1)
+{
+    if (BOX) {
+        i0 = st->istatp1; i1 = st->iendm1; j0 = st->jstat; j1 = st->jend; k0 = st->kstat; k1 = p.nkm2;
+    } else {
+        i0 = 1; i1 = p.nim2; j0 = 1; j1 = p.njm2; k0 = 1; k1 = p.nkm2;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Barrier over the first n CTAs of a cooperative launch (all co-resident).  The
+// last CTA to arrive resets the count and publishes generation `target`; the
+// others poll the generation at most `limit` times, then record
+// AMCFD_E_TIMEOUT (detail `where`).  Each CTA counts the generations itself
+// (the value at its start plus the barriers it has passed), so an arrival is
+// one atomic and the wait one poll loop.  Writes of a CTA before the barrier
+// are visible to every CTA after it (CTA barrier, then a GPU-scope fence on
+// either side of the arrival).  False once a device error is raised; a context
+// whose device wait gave up stays failed, so the count left behind by an
+// abandoned barrier is never used again.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned target, unsigned n,
+                                             Status *st, long long limit, int where)
+{
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        if (atomicAdd(count, 1u) == n - 1) {
+            atomicExch(count, 0u);
+            __threadfence();
+            atomicExch(gen, target);
+        } else {
+            long long it = 0;
+            while ((int)(*(volatile unsigned *)gen - target) < 0) {
+                if ((it & 63) == 63 && *(volatile int *)&st->error) { ok = 0; break; }
+                if (++it > limit) {
+                    if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// A kernel's dynamic shared-memory limit is one value per process, shared by every
+// context: it is only ever raised, so that a context with a smaller grid never
+// lowers it under what another context's launches need.
+static inline cudaError_t raise_smem_limit(const void *func, size_t need)
+{
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, func);
+    if (e != cudaSuccess) return e;
+    if ((int)need <= a.maxDynamicSharedSizeBytes) return cudaSuccess;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
+
+}  // namespace amcfd
