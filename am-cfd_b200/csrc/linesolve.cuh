@@ -171,17 +171,41 @@ __device__ __forceinline__ void box_of(const Params &p, const Status *st, int &i
     }
 }
 
+// GPU-scope acquire / release accesses of the grid barrier's words.
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned *p, unsigned v)
+{
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_gpu(unsigned *p, unsigned v)
+{
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // ---------------------------------------------------------------------------
-// Barrier over the first n CTAs of a cooperative launch (all co-resident).  The
-// last CTA to arrive resets the count and publishes generation `target`; the
-// others poll the generation at most `limit` times, then record
-// AMCFD_E_TIMEOUT (detail `where`).  Each CTA counts the generations itself
-// (the value at its start plus the barriers it has passed), so an arrival is
-// one atomic and the wait one poll loop.  Writes of a CTA before the barrier
-// are visible to every CTA after it (CTA barrier, then a GPU-scope fence on
-// either side of the arrival).  False once a device error is raised; a context
-// whose device wait gave up stays failed, so the count left behind by an
-// abandoned barrier is never used again.
+// Barrier over the first n CTAs of a cooperative launch (all co-resident).
+// Thread 0 of each CTA arrives with an acquire-release add on the count; the
+// last to arrive resets the count and publishes generation `target` with a
+// release store; the others poll the generation with acquire loads, at most
+// `limit` times, then record AMCFD_E_TIMEOUT (detail `where`).  Each CTA counts
+// the generations itself (the value at its start plus the barriers it has
+// passed).  Writes of a CTA before the barrier are visible to every CTA after
+// it: the CTA barrier orders them before thread 0's release, the chain of
+// read-modify-writes on the count carries every arrival to the last one, and
+// its release of the generation to every acquire that reads it.  False once a
+// device error is raised; a context whose device wait gave up stays failed, so
+// the count left behind by an abandoned barrier is never used again.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned target, unsigned n,
                                              Status *st, long long limit, int where)
@@ -190,14 +214,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, uns
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        __threadfence();
-        if (atomicAdd(count, 1u) == n - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicExch(gen, target);
+        if (atom_add_acq_rel_gpu(count, 1u) == n - 1) {
+            st_relaxed_gpu(count, 0u);
+            st_release_gpu(gen, target);
         } else {
             long long it = 0;
-            while ((int)(*(volatile unsigned *)gen - target) < 0) {
+            while ((int)(ld_acquire_gpu(gen) - target) < 0) {
                 if ((it & 63) == 63 && *(volatile int *)&st->error) { ok = 0; break; }
                 if (++it > limit) {
                     if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
@@ -206,7 +228,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, uns
                 }
             }
         }
-        __threadfence();
         ok_s = ok;
     }
     __syncthreads();

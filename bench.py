@@ -354,6 +354,8 @@ def main():
                     help="with graphs, one graph per outer iteration and the convergence test on the "
                          "host (default: one graph per step, iterations chained on the device)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-threads", type=int, default=0,
+                    help="OpenMP threads of the reference CPU solver (0: every physical core)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--mom-cluster", type=int, default=0, choices=[0, 1, 2, 4, 8, 16],
                     help="CTAs of the cluster momentum solve (1: none, 0: the library default)")
@@ -374,7 +376,7 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    cores = physical_cores()
+    cores = args.ref_threads if args.ref_threads > 0 else physical_cores()
     window = f"steps {skip + 1}-{skip + args.steps} (after {start} untimed steps and {warmup} warm-up steps)"
     cfg_desc = {"workload": CONFIG_DESC[args.config], "deck": args.config, "window": window,
                 "l2": "working set 1.2-6.4 GB > 126 MB L2 (no flush needed)"}
@@ -397,7 +399,7 @@ def main():
                 "cpu_baseline": {"value": r["value"], "unit": METRIC, "cores": r["threads"],
                                  "kind": "reference", "logical_cpus": os.cpu_count(),
                                  "sample": f"the timed window ({window}) of the same deck, "
-                                           f"OpenMP on {r['threads']} physical cores"},
+                                           f"OpenMP on {r['threads']} of {physical_cores()} physical cores"},
                 "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
