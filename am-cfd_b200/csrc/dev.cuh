@@ -77,8 +77,9 @@ struct Status {
     int nonfinite;     // a reduction produced NaN/Inf
     unsigned long long seq_energy, done_energy, ticket_energy;
     unsigned long long seq_mom, done_mom, ticket_mom;
-    // grid barrier of the cooperative momentum-box solve: arrivals, generation
-    unsigned gbar_count, gbar_gen;
+    // grid barrier of the cooperative momentum-box solve: arrivals, generation;
+    // its line-flag epochs: launch sequence number, CTAs done with the passes
+    unsigned gbar_count, gbar_gen, gflag_seq, gflag_done;
 };
 
 // Outer-loop control of a step captured as one CUDA graph (a chain of

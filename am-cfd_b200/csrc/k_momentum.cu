@@ -546,6 +546,91 @@ __global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, in
     mom_finalize_body(p, st, red, nb, nb, scratch);
 }
 
+// Pass-completion flags of the box's lines (one int per (j, k) line), for the
+// resident passes: a line's flag is base + t + 1 once pass t of it is stored,
+// base = 16 x the launch's sequence number, so every value an earlier launch left
+// is below every target of this one.
+struct LineFlags {
+    int *f;
+    int nj, j0, j1, k0, k1, base;
+};
+__device__ __forceinline__ int ld_acquire_gpu_int(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu_int(int *p, int v)
+{
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+// Before pass t of line (j, k): lanes 0..3 wait (bounded) until the four
+// neighbouring lines in the box, of the other colour, have stored pass t - 1;
+// the warp barrier then orders those acquires before every lane's reads.
+// False (for the whole warp) when a wait gave up or an error is raised.
+__device__ __forceinline__ bool wait_neighbours(const LineFlags &lf, int j, int k, int t, Status *st, long long polls)
+{
+    const int lane = threadIdx.x & 31;
+    int jn = j, kn = k;
+    bool need = false;
+    if (lane == 0) { jn = j - 1; need = jn >= lf.j0; }
+    else if (lane == 1) { jn = j + 1; need = jn <= lf.j1; }
+    else if (lane == 2) { kn = k - 1; need = kn >= lf.k0; }
+    else if (lane == 3) { kn = k + 1; need = kn <= lf.k1; }
+    int good = 1;
+    if (need) {
+        const int *p = lf.f + (size_t)kn * lf.nj + jn;
+        const int target = lf.base + t;
+        long long it = 0;
+        while (ld_acquire_gpu_int(p) - target < 0) {
+            if ((it & 63) == 63 && *(volatile int *)&st->error) { good = 0; break; }
+            if (++it > polls) {
+                if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -4;
+                good = 0;
+                break;
+            }
+        }
+    }
+    const bool all = __all_sync(0xffffffffu, good) != 0;
+    __syncwarp();
+    return all;
+}
+
+// The eight colour passes of a resident warp (one line of each colour, or none)
+// from registers.  No grid barrier: each pass of a line waits only for its four
+// neighbours' previous pass (the lines it reads), and publishes its own
+// completion after its stores (warp barrier, then lane 0's release store), which
+// also tells those neighbours that their next pass may overwrite what it read.
+// Every line has its warp resident (a cooperative launch), and a pass waits only
+// on passes before it, so every wait ends.  False when a wait gave up.
+template <typename T, int L>
+__device__ __forceinline__ bool box_passes_regs(T *phi, const size_t (&rows)[2], const int (&jl)[2], int kl,
+                                                const bool (&has)[2], bool ok, const T *buf, size_t slot,
+                                                int nmax, int o, int n, int i0, size_t sj, size_t sk,
+                                                const LineFlags &lf, Status *st, long long polls)
+{
+    const int lane = threadIdx.x & 31;
+    LineRegs<T, L> r0, r1;
+    if (has[0]) load_line_regs<T, L>(r0, buf, nmax, o, n);
+    if (has[1]) load_line_regs<T, L>(r1, buf + slot, nmax, o, n);
+    for (int sweep = 0; sweep < 4; ++sweep) {
+        const int t0 = 2 * sweep, t1 = t0 + 1;
+        if (has[0]) {
+            if (ok && t0 > 0) ok = wait_neighbours(lf, jl[0], kl, t0, st, polls);
+            if (ok) solve_line_regs<T, L>(phi, rows[0], i0, n, sj, sk, r0);
+            __syncwarp();
+            if (ok && lane == 0) st_release_gpu_int(lf.f + (size_t)kl * lf.nj + jl[0], lf.base + t0 + 1);
+        }
+        if (has[1]) {
+            if (ok) ok = wait_neighbours(lf, jl[1], kl, t1, st, polls);
+            if (ok) solve_line_regs<T, L>(phi, rows[1], i0, n, sj, sk, r1);
+            __syncwarp();
+            if (ok && lane == 0) st_release_gpu_int(lf.f + (size_t)kl * lf.nj + jl[1], lf.base + t1 + 1);
+        }
+    }
+    return ok;
+}
+
 // ---------------------------------------------------------------------------
 // Momentum-box line solve of equation ivar (1..3: u, v, w; 4: p') in red-black
 // order as one cooperative launch (solveLiquidDomain, CFDSolverManager.cpp:
@@ -566,7 +651,8 @@ __global__ void mom_finalize_kernel(Params p, Fields<T> g, const double *red, in
 // box needs return at once and take no part in the barriers.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> g, int ivar, const double *red, int nb)
+__global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> g, int ivar, const double *red, int nb,
+                                                            int *flags)
 {
     pdl_enter();
     T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
@@ -586,6 +672,8 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
     // the barrier generation at the start of the launch: no CTA can advance it
     // before every taking part has arrived at the first barrier
     unsigned gen = *(volatile unsigned *)&st->gbar_gen;
+    // the launch's sequence number (advanced by the last CTA to finish the passes)
+    const unsigned seq = *(volatile unsigned *)&st->gflag_seq;
     const int nmax = p.nip;
     const size_t slot = (size_t)(S_N + 1) * nmax;  // the staged rows and the scratch row
     T *buf = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * slot;
@@ -600,11 +688,16 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
     const int n = i1 - i0 + 1, o = i0 - ib;
     const uint32_t bytes = (uint32_t)((ie - ib) * sizeof(T));
     // node (0, j, k) of slot q of colour c; false past the box's last row
-    auto line_row = [&](int c, int q, size_t &row) {
-        const int kk = q / half, r = q - kk * half, k = k0 + kk;
-        const int j = j0 + ((c - k - j0) % 2 + 2) % 2 + 2 * r;
+    auto line_jk = [&](int c, int q, size_t &row, int &j, int &k) {
+        const int kk = q / half, r = q - kk * half;
+        k = k0 + kk;
+        j = j0 + ((c - k - j0) % 2 + 2) % 2 + 2 * r;
         row = cidx(0, j, k, nj, nip);
         return j <= j1;
+    };
+    auto line_row = [&](int c, int q, size_t &row) {
+        int j, k;
+        return line_jk(c, q, row, j, k);
     };
     bool ok = true;
     // staging of a line's rows for the factorisation: ap, aw, ae go to the
@@ -629,11 +722,13 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
             prv = pv;
         }
     };
+    // resident: the warp's line of each colour (none past the box's rows)
+    size_t rows[2] = {0, 0};
+    bool has[2] = {false, false};
+    int jl[2] = {0, 0}, kl = 0;  // (slot gw of both colours: the same plane)
     if (resident) {
         // both lines of the warp staged at once, factorised by lanes 0 and 1
-        size_t rows[2];
-        bool has[2];
-        for (int c = 0; c < 2; ++c) has[c] = gw < nl && line_row(c, gw, rows[c]);
+        for (int c = 0; c < 2; ++c) has[c] = gw < nl && line_jk(c, gw, rows[c], jl[c], kl);
         if (has[0] || has[1]) {
             if (lane == 0) {
                 fence_proxy_async();
@@ -673,8 +768,16 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
             fence_proxy_async_global();  // before the copies that stage these rows again
             __syncwarp();
         }
-    // the eight colour passes
-    for (int pass = 0; pass < 8; ++pass) {
+    // the eight colour passes: lines of up to 64 cells from registers when every
+    // warp holds its lines, otherwise from the staged buffers
+    if (resident && n <= 64) {
+        const LineFlags lf{flags, nj, j0, j1, k0, k1, (int)(seq * 16u)};
+        ok = n <= 32 ? box_passes_regs<T, 1>(phi, rows, jl, kl, has, ok, buf, slot, nmax, o, n, i0, sj, sk, lf, st,
+                                             p.wait_polls)
+                     : box_passes_regs<T, 2>(phi, rows, jl, kl, has, ok, buf, slot, nmax, o, n, i0, sj, sk, lf, st,
+                                             p.wait_polls);
+    }
+    for (int pass = 0; pass < 8 && !(resident && n <= 64); ++pass) {
         const int c = pass & 1;
         if (pass > 0 && !grid_barrier(&st->gbar_count, &st->gbar_gen, ++gen, (unsigned)nact, st, p.wait_polls, -2))
             return;
@@ -692,6 +795,12 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
             solve_staged<T, true>(phi, row, i0, i1, ib, sj, sk, sl, nmax, resident ? S_Q : S_SU);
             __syncwarp();
         }
+    }
+    // the last CTA through advances the sequence number for the next launch
+    __syncthreads();
+    if (threadIdx.x == 0 && atom_add_acq_rel_gpu(&st->gflag_done, 1u) == (unsigned)nact - 1) {
+        st_relaxed_gpu(&st->gflag_done, 0u);
+        st_release_gpu(&st->gflag_seq, seq + 1u);
     }
     // ---- what follows the solve ----
     Box b;
@@ -1569,7 +1678,8 @@ template <typename T> static void launch_box_solve(Inst<T> &I, int ivar)
     cfg.stream = I.stream;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, mom_box_solve_kernel<T>, I.p, I.g, ivar, (const double *)I.red_mom, I.nb_mom);
+    cudaLaunchKernelEx(&cfg, mom_box_solve_kernel<T>, I.p, I.g, ivar, (const double *)I.red_mom, I.nb_mom,
+                       I.flags_mom);
 }
 // Launch shape of mom_box_solve_kernel: the most warps per CTA (4, 2 or 1) whose
 // buffers (two lines of 8 staged rows and a scratch row each, one mbarrier) fit

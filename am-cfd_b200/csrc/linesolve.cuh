@@ -151,6 +151,117 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
     scan_line<T>(phi, row, i0, i1, se + o, sc + o, sp + o, lo, hi);
 }
 
+// ---------------------------------------------------------------------------
+// A line's coefficient rows and factorisation held in registers across passes:
+// lane l keeps cells a = l L .. a + L - 1 of the line (relative to i0), the
+// chunk that scan_line gives a lane on a line of n cells when L = (n + 31) / 32.
+// ---------------------------------------------------------------------------
+template <typename T, int L>
+struct LineRegs {
+    T at[L], ab[L], an[L], as[L], su[L], cf[L], pr[L], id[L];
+};
+// From a staged buffer (rows as stage_line leaves them, cell i0 at offset o).
+template <typename T, int L>
+__device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, const T *sl, int nmax, int o, int n)
+{
+    const int a = (threadIdx.x & 31) * L;
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        const bool ok = a + v < n;
+        const int s = o + (ok ? a + v : 0);
+        r.at[v] = ok ? sl[S_AT * nmax + s] : T(0);
+        r.ab[v] = ok ? sl[S_AB * nmax + s] : T(0);
+        r.an[v] = ok ? sl[S_AN * nmax + s] : T(0);
+        r.as[v] = ok ? sl[S_AS * nmax + s] : T(0);
+        r.su[v] = ok ? sl[S_SU * nmax + s] : T(0);
+        r.cf[v] = ok ? sl[S_CF * nmax + s] : T(0);
+        r.pr[v] = ok ? sl[S_PR * nmax + s] : T(0);
+        r.id[v] = ok ? sl[S_ID * nmax + s] : T(0);
+    }
+}
+// One pass over a line of n <= 32 L cells from its registers: solve_staged and
+// scan_line with the same expressions on the same per-lane chunks (so the same
+// bits), the right-hand side and both recurrences in registers; only the four
+// neighbouring rows and the two fixed ends are read (through L2: other CTAs
+// write them), and the lane's cells are stored.
+template <typename T, int L>
+__device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int n, size_t sj, size_t sk,
+                                                const LineRegs<T, L> &r)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int a = lane * L;
+    const T lo = ld_shared_row<T>(phi + row + i0 - 1), hi = ld_shared_row<T>(phi + row + i0 + n);
+    T nt[L], nb[L], nn[L], ns[L], e[L];
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        const bool ok = a + v < n;
+        const size_t c = row + i0 + (ok ? a + v : 0);
+        nt[v] = ok ? ld_shared_row<T>(phi + c + sk) : T(0);
+        nb[v] = ok ? ld_shared_row<T>(phi + c - sk) : T(0);
+        nn[v] = ok ? ld_shared_row<T>(phi + c + sj) : T(0);
+        ns[v] = ok ? ld_shared_row<T>(phi + c - sj) : T(0);
+    }
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        const T d = r.at[v] * nt[v] + r.ab[v] * nb[v] + r.an[v] * nn[v] + r.as[v] * ns[v] + r.su[v];
+        e[v] = d * r.id[v];
+    }
+    T A = T(1), B = T(0);
+#pragma unroll
+    for (int v = 0; v < L; ++v)
+        if (a + v < n) {
+            B = r.cf[v] * B + e[v];
+            A = r.cf[v] * A;
+        }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_up_sync(full, A, o);
+        T B2 = __shfl_up_sync(full, B, o);
+        if (lane >= o) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    T Ae = __shfl_up_sync(full, A, 1);
+    T Be = __shfl_up_sync(full, B, 1);
+    if (lane == 0) { Ae = T(1); Be = T(0); }
+    T q = Ae * lo + Be;
+#pragma unroll
+    for (int v = 0; v < L; ++v)
+        if (a + v < n) {
+            q = r.cf[v] * q + e[v];
+            e[v] = q;
+        }
+    A = T(1);
+    B = T(0);
+#pragma unroll
+    for (int v = L - 1; v >= 0; --v)
+        if (a + v < n) {
+            B = r.pr[v] * B + e[v];
+            A = r.pr[v] * A;
+        }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T A2 = __shfl_down_sync(full, A, o);
+        T B2 = __shfl_down_sync(full, B, o);
+        if (lane + o < 32) {
+            B = A * B2 + B;
+            A = A * A2;
+        }
+    }
+    Ae = __shfl_down_sync(full, A, 1);
+    Be = __shfl_down_sync(full, B, 1);
+    if (lane == 31) { Ae = T(1); Be = T(0); }
+    T x = Ae * hi + Be;
+#pragma unroll
+    for (int v = L - 1; v >= 0; --v)
+        if (a + v < n) {
+            x = r.pr[v] * x + e[v];
+            phi[row + i0 + a + v] = x;
+        }
+}
+
 // Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).
 template <typename T>
 __device__ __forceinline__ void stage_window(int i0, int i1, int &ib, int &ie)
