@@ -357,6 +357,10 @@ def main():
     ap.add_argument("--ref-threads", type=int, default=0,
                     help="OpenMP threads of the reference CPU solver (0: every physical core)")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-small-box", action="store_true",
+                    help="momentum boxes of every size on the grid path (no one-CTA path)")
+    ap.add_argument("--serial-launch", action="store_true",
+                    help="no programmatic dependent launch; the box line solve as a launch per colour pass")
     ap.add_argument("--mom-cluster", type=int, default=0, choices=[0, 1, 2, 4, 8, 16],
                     help="CTAs of the cluster momentum solve (1: none, 0: the library default)")
     ap.add_argument("--profile-window", action="store_true",
@@ -433,7 +437,9 @@ def main():
         kw = dict(asm_kseg=tune[p]["asm_kseg"], sweep_warps=tune[p]["sweep_warps"]) if p in tune else \
             dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
         sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
-                          host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster, **kw)
+                          host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster,
+                          small_box=0 if args.no_small_box else 1, serial_launch=1 if args.serial_launch else 0,
+                          **kw)
         tune.setdefault(p, sv.tuning())
         return sv
 
@@ -579,6 +585,8 @@ def main():
                           amcfd.PREC_FP64: "f64"}[prec], "data": "synthetic deck",
                 "config": dict(cfg_desc, precision=args.precision, order=args.order, graphs=args.graphs,
                                outer_loop="host" if args.host_loop or not args.graphs else "device",
+                               momentum=("grid" if args.no_small_box else "one-CTA below its capacity, else grid")
+                               + (", serial launches" if args.serial_launch else ""),
                                parallelism=f"replicas{world}"),
                 "cell_iters_per_s": cips, "outer_iters": iters, "gpu_launches": launches,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,
