@@ -203,6 +203,9 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
     double sumd = 0.0, sumh = 0.0;
     double bl = 0.0, blp = 0.0, blm = 0.0, blc = 0.0;
     const int o = (ty + 1) * BX + tx + OX;  // this thread's cell inside a box
+    // the top face's coefficient as seen from the cell above (its bottom face),
+    // carried from one plane to the next
+    R ab_bottom = R(0);
 
     for (int k = kb; k < ke; ++k) {
         if (ok) ok = mbar_wait(&barA[slotA(k + 1)], parA(k + 1), st, 2);
@@ -258,7 +261,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 const R dcc = d_c, rhc = Ac[FA_R * FE];
                 const R d_e = Ac[FA_D * FE + 1], d_w = Ac[FA_D * FE - 1], d_nn = Ac[FA_D * FE + BX],
                         d_s = Ac[FA_D * FE - BX], d_m = Am[FA_D * FE], d_p = Ap[FA_D * FE];
-                R an, as_, ae, aw, at, ab, tmp;
+                R an, as_, ae, aw, at, ab, tmp, ab_up;
                 const R u_c = Bc[FB_U * FE], u_e = Bc[FB_U * FE + 1];
                 const R v_c = Bc[FB_V * FE], v_n = Bc[FB_V * FE + BX];
                 const R w_c = Ac[FA_W * FE], w_p = Ap[FA_W * FE];
@@ -345,7 +348,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                         const bool bnd = k == nkm2;
                         const R num = bnd ? dcc * aij * dzp_t : dcc * d_p * aij * dzp_p;
                         const R den = bnd ? R(1) : (R(1) - fz_k) * d_p + fz_k * dcc;
-                        face_fast<R>(sch, num, den, ft, at, tmp);
+                        face_fast<R>(sch, num, den, ft, at, ab_up);
                     } else {
                         R dt;
                         if (k == nkm2) {
@@ -354,11 +357,15 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                             R dift = bdiv(dcc * d_p, (R(1) - fz_k) * d_p + fz_k * dcc);
                             dt = dift * aij * dzp_p;
                         }
-                        face_coef<R>(sch, dt, ft, at, tmp);
+                        face_coef<R>(sch, dt, ft, at, ab_up);
                     }
                 }
-                // bottom face
-                {
+                // bottom face: the top face of the plane below, as this thread formed
+                // it there (same operands in the same order, so the same bits), or
+                // formed here on the segment's first plane and on the boundary
+                if (k > kb && k > 1) {
+                    ab = ab_bottom;
+                } else {
                     R fb = rhc * w_c * aij;
                     if constexpr (FAST) {
                         const bool bnd = k == 1;
@@ -376,6 +383,7 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                         face_coef<R>(sch, db, fb, tmp, ab);
                     }
                 }
+                ab_bottom = ab_up;
                 const R densbydt = FAST ? rhc * inv_delt : bdiv(rhc, (R)delt);
                 const R apnot = densbydt * vol;
                 R sp = R(0);

@@ -156,6 +156,9 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
 // lane l keeps cells a = l L .. a + L - 1 of the line (relative to i0), the
 // chunk that scan_line gives a lane on a line of n cells when L = (n + 31) / 32.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <typename T, int L>
 struct LineRegs {
     T at[L], ab[L], an[L], as[L], su[L], cf[L], pr[L], id[L];
@@ -202,10 +205,12 @@ __device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int 
         nn[v] = ok ? ld_shared_row<T>(phi + c + sj) : T(0);
         ns[v] = ok ? ld_shared_row<T>(phi + c - sj) : T(0);
     }
+    // e = d / den rounded on its own, as the staged form rounds it by storing it
+    // (left to the compiler, the product would fuse into the recurrence below)
 #pragma unroll
     for (int v = 0; v < L; ++v) {
         const T d = r.at[v] * nt[v] + r.ab[v] * nb[v] + r.an[v] * nn[v] + r.as[v] * ns[v] + r.su[v];
-        e[v] = d * r.id[v];
+        e[v] = mul_rn(d, r.id[v]);
     }
     T A = T(1), B = T(0);
 #pragma unroll
