@@ -12,6 +12,23 @@ namespace amcfd {
 // Load of a value another warp may have just written (bypasses L1).
 template <typename T> __device__ __forceinline__ T ld_shared_row(const T *ptr) { return __ldcg(ptr); }
 
+// Explicitly rounded operations: the right-hand side of a line's cell is formed
+// by the same sequence of roundings whichever code forms it (left to the
+// compiler, which product fuses into which sum may depend on where the operands
+// come from).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+// e = (at phi_t + ab phi_b + an phi_n + as phi_s + su) / den, with 1/den given
+template <typename T>
+__device__ __forceinline__ T line_rhs(T at, T vt, T ab, T vb, T an, T vn, T as, T vs, T su, T id)
+{
+    return mul_rn(add_rn(fma_rn(as, vs, fma_rn(an, vn, fma_rn(ab, vb, mul_rn(at, vt)))), su), id);
+}
+
 // ---------------------------------------------------------------------------
 // Per-warp staging of one x-line.  The eight pass-invariant coefficient rows of
 // the line (at ab an as su cf pr iden) are brought into shared memory with
@@ -56,48 +73,48 @@ __device__ __forceinline__ void scan_line(T *phi, size_t row, int i0, int i1, T 
     T A = T(1), B = T(0);
     for (int i = a; i < b; ++i) {
         const T cfi = sc[i];
-        B = cfi * B + se[i];
-        A = cfi * A;
+        B = fma_rn(cfi, B, se[i]);
+        A = mul_rn(cfi, A);
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         T A2 = __shfl_up_sync(0xffffffffu, A, o);
         T B2 = __shfl_up_sync(0xffffffffu, B, o);
         if (lane >= o) {
-            B = A * B2 + B;
-            A = A * A2;
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
         }
     }
     T Ae = __shfl_up_sync(0xffffffffu, A, 1);
     T Be = __shfl_up_sync(0xffffffffu, B, 1);
     if (lane == 0) { Ae = T(1); Be = T(0); }
-    T q = Ae * lo + Be;
+    T q = fma_rn(Ae, lo, Be);
     for (int i = a; i < b; ++i) {
-        q = sc[i] * q + se[i];
+        q = fma_rn(sc[i], q, se[i]);
         se[i] = q;
     }
     A = T(1);
     B = T(0);
     for (int i = b - 1; i >= a; --i) {
         const T pri = sp[i];
-        B = pri * B + se[i];
-        A = pri * A;
+        B = fma_rn(pri, B, se[i]);
+        A = mul_rn(pri, A);
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         T A2 = __shfl_down_sync(0xffffffffu, A, o);
         T B2 = __shfl_down_sync(0xffffffffu, B, o);
         if (lane + o < 32) {
-            B = A * B2 + B;
-            A = A * A2;
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
         }
     }
     Ae = __shfl_down_sync(0xffffffffu, A, 1);
     Be = __shfl_down_sync(0xffffffffu, B, 1);
     if (lane == 31) { Ae = T(1); Be = T(0); }
-    T x = Ae * hi + Be;
+    T x = fma_rn(Ae, hi, Be);
     for (int i = b - 1; i >= a; --i) {
-        x = sp[i] * x + se[i];
+        x = fma_rn(sp[i], x, se[i]);
         se[i] = x;
     }
     __syncwarp();
@@ -142,8 +159,7 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
             const int iu = i + 32 * u;
             if (iu < i0 || iu > i1) continue;
             const int s = iu - ib;
-            T d = sat[s] * nt[u] + sab[s] * nb[u] + san[s] * nn[u] + sas[s] * ns[u] + ssu[s];
-            se[s] = d * sid[s];
+            se[s] = line_rhs(sat[s], nt[u], sab[s], nb[u], san[s], nn[u], sas[s], ns[u], ssu[s], sid[s]);
         }
     }
     __syncwarp();
@@ -156,9 +172,6 @@ __device__ __forceinline__ void solve_staged(T *phi, size_t row, int i0, int i1,
 // lane l keeps cells a = l L .. a + L - 1 of the line (relative to i0), the
 // chunk that scan_line gives a lane on a line of n cells when L = (n + 31) / 32.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
-
 template <typename T, int L>
 struct LineRegs {
     T at[L], ab[L], an[L], as[L], su[L], cf[L], pr[L], id[L];
@@ -205,37 +218,33 @@ __device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int 
         nn[v] = ok ? ld_shared_row<T>(phi + c + sj) : T(0);
         ns[v] = ok ? ld_shared_row<T>(phi + c - sj) : T(0);
     }
-    // e = d / den rounded on its own, as the staged form rounds it by storing it
-    // (left to the compiler, the product would fuse into the recurrence below)
 #pragma unroll
-    for (int v = 0; v < L; ++v) {
-        const T d = r.at[v] * nt[v] + r.ab[v] * nb[v] + r.an[v] * nn[v] + r.as[v] * ns[v] + r.su[v];
-        e[v] = mul_rn(d, r.id[v]);
-    }
+    for (int v = 0; v < L; ++v)
+        e[v] = line_rhs(r.at[v], nt[v], r.ab[v], nb[v], r.an[v], nn[v], r.as[v], ns[v], r.su[v], r.id[v]);
     T A = T(1), B = T(0);
 #pragma unroll
     for (int v = 0; v < L; ++v)
         if (a + v < n) {
-            B = r.cf[v] * B + e[v];
-            A = r.cf[v] * A;
+            B = fma_rn(r.cf[v], B, e[v]);
+            A = mul_rn(r.cf[v], A);
         }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         T A2 = __shfl_up_sync(full, A, o);
         T B2 = __shfl_up_sync(full, B, o);
         if (lane >= o) {
-            B = A * B2 + B;
-            A = A * A2;
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
         }
     }
     T Ae = __shfl_up_sync(full, A, 1);
     T Be = __shfl_up_sync(full, B, 1);
     if (lane == 0) { Ae = T(1); Be = T(0); }
-    T q = Ae * lo + Be;
+    T q = fma_rn(Ae, lo, Be);
 #pragma unroll
     for (int v = 0; v < L; ++v)
         if (a + v < n) {
-            q = r.cf[v] * q + e[v];
+            q = fma_rn(r.cf[v], q, e[v]);
             e[v] = q;
         }
     A = T(1);
@@ -243,26 +252,26 @@ __device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int 
 #pragma unroll
     for (int v = L - 1; v >= 0; --v)
         if (a + v < n) {
-            B = r.pr[v] * B + e[v];
-            A = r.pr[v] * A;
+            B = fma_rn(r.pr[v], B, e[v]);
+            A = mul_rn(r.pr[v], A);
         }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         T A2 = __shfl_down_sync(full, A, o);
         T B2 = __shfl_down_sync(full, B, o);
         if (lane + o < 32) {
-            B = A * B2 + B;
-            A = A * A2;
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
         }
     }
     Ae = __shfl_down_sync(full, A, 1);
     Be = __shfl_down_sync(full, B, 1);
     if (lane == 31) { Ae = T(1); Be = T(0); }
-    T x = Ae * hi + Be;
+    T x = fma_rn(Ae, hi, Be);
 #pragma unroll
     for (int v = L - 1; v >= 0; --v)
         if (a + v < n) {
-            x = r.pr[v] * x + e[v];
+            x = fma_rn(r.pr[v], x, e[v]);
             phi[row + i0 + a + v] = x;
         }
 }
