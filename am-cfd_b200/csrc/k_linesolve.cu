@@ -202,6 +202,29 @@ __global__ void sweep_exact_kernel(Params p, Fields<T> g, T *phi, int *flags, co
 // ---------------------------------------------------------------------------
 // Red-black sweep: every line of one (j+k) colour, one warp per line.
 // ---------------------------------------------------------------------------
+// Red-black order, momentum box: the factorisation of every line of the box, one
+// warp per line (factor_line_mem), the same operations as the cooperative box
+// solve forms them with.  The exact order keeps factor_kernel<T, true>, the
+// reference's serial recurrence.
+template <typename T>
+__global__ void __launch_bounds__(256) factor_box_warp_kernel(Params p, Fields<T> g)
+{
+    pdl_enter();
+    const Status *st = g.st;
+    if (!st->momentum_active) return;
+    int i0, i1, j0, j1, k0, k1;
+    box_of<true>(p, st, i0, i1, j0, j1, k0, k1);
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1, n = i1 - i0 + 1;
+    if (J <= 0 || K <= 0 || n <= 0) return;
+    const int wpb = blockDim.x >> 5, warp = threadIdx.x >> 5;
+    for (int l = blockIdx.x * wpb + warp; l < J * K; l += gridDim.x * wpb) {
+        const size_t row = cidx(i0, j0 + l % J, k0 + l / J, p.nj, p.nip);
+        factor_line_mem<T>(
+            n, [&](int i, T &w, T &e, T &pp) { w = g.aw[row + i]; e = g.ae[row + i]; pp = g.ap[row + i]; },
+            [&](int i, T pr, T cf, T id) { g.pr[row + i] = pr; g.cf[row + i] = cf; g.iden[row + i] = id; });
+    }
+}
+
 template <typename T, bool BOX>
 __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 {
@@ -669,6 +692,11 @@ template <typename T> void launch_energy_factor(Inst<T> &I) { launch_phi_factor<
 template <typename T> void launch_box_factor(Inst<T> &I)
 {
     // the box is small (a melt pool); one CTA per SM covers up to 4736 lines per pass
+    if (I.order == AMCFD_ORDER_REDBLACK) {
+        const int grid = std::min((I.max_lines + 7) / 8, 2 * I.sm_count);
+        launch_k(I.pdl, factor_box_warp_kernel<T>, grid, 256, 0, I.stream, I.p, I.g);
+        return;
+    }
     int grid = std::min((I.max_lines + 31) / 32, I.sm_count);
     launch_k(I.pdl, factor_kernel<T, true>, grid, 256, 0, I.stream, I.p, I.g, nullptr);
 }

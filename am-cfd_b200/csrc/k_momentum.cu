@@ -604,15 +604,16 @@ __device__ __forceinline__ bool wait_neighbours(const LineFlags &lf, int j, int 
 // Every line has its warp resident (a cooperative launch), and a pass waits only
 // on passes before it, so every wait ends.  False when a wait gave up.
 template <typename T, int L>
-__device__ __forceinline__ bool box_passes_regs(T *phi, const size_t (&rows)[2], const int (&jl)[2], int kl,
-                                                const bool (&has)[2], bool ok, const T *buf, size_t slot,
-                                                int nmax, int o, int n, int i0, size_t sj, size_t sk,
-                                                const LineFlags &lf, Status *st, long long polls)
+__device__ __forceinline__ bool box_passes_regs(const Fields<T> &g, T *phi, const size_t (&rows)[2],
+                                                const int (&jl)[2], int kl, const bool (&has)[2], int n, int i0,
+                                                size_t sj, size_t sk, const LineFlags &lf, Status *st,
+                                                long long polls)
 {
     const int lane = threadIdx.x & 31;
+    bool ok = true;
     LineRegs<T, L> r0, r1;
-    if (has[0]) load_line_regs<T, L>(r0, buf, nmax, o, n);
-    if (has[1]) load_line_regs<T, L>(r1, buf + slot, nmax, o, n);
+    if (has[0]) load_line_regs<T, L>(r0, g, rows[0] + i0, n);
+    if (has[1]) load_line_regs<T, L>(r1, g, rows[1] + i0, n);
     for (int sweep = 0; sweep < 4; ++sweep) {
         const int t0 = 2 * sweep, t1 = t0 + 1;
         if (has[0]) {
@@ -707,29 +708,25 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
 #pragma unroll
         for (int r = 0; r < S_N; ++r) bulk_load(sl + (size_t)r * nmax, src[r] + row + ib, bytes, bar);
     };
-    // factor_kernel's recurrence and guard on |den| (:2438-2439), in place
-    auto factor_line = [&](T *sl) {
+    // the warp factorisation (factor_line_mem) of a staged line, in place
+    auto factor_staged = [&](T *sl) {
         T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
-        T prv = T(0);
-        for (int i = 0; i < n; ++i) {
-            T den = sid[i] - scf[i] * prv;
-            if (fabs(den) <= T(1e-12)) den += T(kSmall);
-            const T id = T(1) / den;
-            const T pv = spr[i] * id;
-            spr[i] = pv;
-            scf[i] = scf[i] * id;
-            sid[i] = id;
-            prv = pv;
-        }
+        factor_line_mem<T>(
+            n, [&](int i, T &w, T &e, T &pp) { w = scf[i]; e = spr[i]; pp = sid[i]; },
+            [&](int i, T pr, T cf, T id) { spr[i] = pr; scf[i] = cf; sid[i] = id; });
+        __syncwarp();
     };
+    // lines of up to 64 cells of a resident warp live in registers, loaded and
+    // factorised there (box_passes_regs); the rest go through shared memory
+    const bool regs = resident && n <= 64;
     // resident: the warp's line of each colour (none past the box's rows)
     size_t rows[2] = {0, 0};
     bool has[2] = {false, false};
     int jl[2] = {0, 0}, kl = 0;  // (slot gw of both colours: the same plane)
     if (resident) {
-        // both lines of the warp staged at once, factorised by lanes 0 and 1
         for (int c = 0; c < 2; ++c) has[c] = gw < nl && line_jk(c, gw, rows[c], jl[c], kl);
-        if (has[0] || has[1]) {
+        if (!regs && (has[0] || has[1])) {
+            // both lines of the warp staged at once
             if (lane == 0) {
                 fence_proxy_async();
                 mbar_expect_tx(bar, bytes * S_N * ((has[0] ? 1u : 0u) + (has[1] ? 1u : 0u)));
@@ -738,8 +735,8 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
             }
             ok = mbar_wait(bar, parity, st, -3);
             parity ^= 1u;
-            if (ok && ((lane == 0 && has[0]) || (lane == 1 && has[1]))) factor_line(buf + lane * slot);
-            __syncwarp();
+            for (int c = 0; c < 2; ++c)
+                if (ok && has[c]) factor_staged(buf + c * slot);
         }
     }
     // otherwise one line at a time through buffer 0, the factorisation kept in
@@ -757,8 +754,7 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
             ok = mbar_wait(bar, parity, st, -3);
             parity ^= 1u;
             if (!ok) break;
-            if (lane == 0) factor_line(sl);
-            __syncwarp();
+            factor_staged(sl);
             const T *scf = sl + S_CF * nmax + o, *spr = sl + S_PR * nmax + o, *sid = sl + S_ID * nmax + o;
             for (int i = lane; i < n; i += 32) {
                 g.pr[row + i0 + i] = spr[i];
@@ -770,14 +766,12 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
         }
     // the eight colour passes: lines of up to 64 cells from registers when every
     // warp holds its lines, otherwise from the staged buffers
-    if (resident && n <= 64) {
+    if (regs) {
         const LineFlags lf{flags, nj, j0, j1, k0, k1, (int)(seq * 16u)};
-        ok = n <= 32 ? box_passes_regs<T, 1>(phi, rows, jl, kl, has, ok, buf, slot, nmax, o, n, i0, sj, sk, lf, st,
-                                             p.wait_polls)
-                     : box_passes_regs<T, 2>(phi, rows, jl, kl, has, ok, buf, slot, nmax, o, n, i0, sj, sk, lf, st,
-                                             p.wait_polls);
+        ok = n <= 32 ? box_passes_regs<T, 1>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls)
+                     : box_passes_regs<T, 2>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls);
     }
-    for (int pass = 0; pass < 8 && !(resident && n <= 64); ++pass) {
+    for (int pass = 0; pass < 8 && !regs; ++pass) {
         const int c = pass & 1;
         if (pass > 0 && !grid_barrier(&st->gbar_count, &st->gbar_gen, ++gen, (unsigned)nact, st, p.wait_polls, -2))
             return;

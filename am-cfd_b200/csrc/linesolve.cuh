@@ -176,25 +176,6 @@ template <typename T, int L>
 struct LineRegs {
     T at[L], ab[L], an[L], as[L], su[L], cf[L], pr[L], id[L];
 };
-// From a staged buffer (rows as stage_line leaves them, cell i0 at offset o).
-template <typename T, int L>
-__device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, const T *sl, int nmax, int o, int n)
-{
-    const int a = (threadIdx.x & 31) * L;
-#pragma unroll
-    for (int v = 0; v < L; ++v) {
-        const bool ok = a + v < n;
-        const int s = o + (ok ? a + v : 0);
-        r.at[v] = ok ? sl[S_AT * nmax + s] : T(0);
-        r.ab[v] = ok ? sl[S_AB * nmax + s] : T(0);
-        r.an[v] = ok ? sl[S_AN * nmax + s] : T(0);
-        r.as[v] = ok ? sl[S_AS * nmax + s] : T(0);
-        r.su[v] = ok ? sl[S_SU * nmax + s] : T(0);
-        r.cf[v] = ok ? sl[S_CF * nmax + s] : T(0);
-        r.pr[v] = ok ? sl[S_PR * nmax + s] : T(0);
-        r.id[v] = ok ? sl[S_ID * nmax + s] : T(0);
-    }
-}
 // One pass over a line of n <= 32 L cells from its registers: solve_staged and
 // scan_line with the same expressions on the same per-lane chunks (so the same
 // bits), the right-hand side and both recurrences in registers; only the four
@@ -274,6 +255,137 @@ __device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int 
             x = fma_rn(r.pr[v], x, e[v]);
             phi[row + i0 + a + v] = x;
         }
+}
+
+// ---------------------------------------------------------------------------
+// Thomas factorisation of one line by one warp: den_i = ap_i - aw_i pr_{i-1},
+// pr_i = ae_i / den_i, cf_i = aw_i / den_i, iden_i = 1 / den_i from pr = 0
+// before the first cell, with solveLiquidDomain's guard on |den|
+// (CFDSolverManager.cpp:2438-2439).  The pivots follow the projective map
+// x -> ae / (ap - aw x), the matrix [[0, ae], [-aw, ap]] on (x, 1): each lane
+// multiplies the matrices of its chunk of L = (n + 31) / 32 cells (rescaled by
+// powers of two, which is exact), an exclusive warp scan gives it the product of
+// the lanes below, whose map applied to 0 is its entry pivot, and the lane then
+// runs the recurrence over its own cells.  The guard acts in that recurrence, on
+// the cell where it fires and the rest of its lane's chunk; the prefixes of the
+// later lanes do not see it (it fires only on degenerate coefficients).  Every
+// operation is explicitly rounded: the register and the memory forms below give
+// the same bits.
+// ---------------------------------------------------------------------------
+template <typename T>
+struct PMat {
+    T a, b, c, d;  // [[a, b], [c, d]]
+};
+template <typename T>
+__device__ __forceinline__ void pmat_rescale(PMat<T> &m)
+{
+    const T mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
+    if (mx > T(0) && mx < T(INFINITY)) {
+        int e;
+        frexp(mx, &e);
+        const T s = ldexp(T(1), -e);
+        m.a *= s; m.b *= s; m.c *= s; m.d *= s;
+    }
+}
+// m <- [[0, e], [-w, p]] m
+template <typename T>
+__device__ __forceinline__ void pmat_cell(PMat<T> &m, T w, T e, T p)
+{
+    const PMat<T> r{mul_rn(e, m.c), mul_rn(e, m.d), fma_rn(p, m.c, mul_rn(-w, m.a)), fma_rn(p, m.d, mul_rn(-w, m.b))};
+    m = r;
+    pmat_rescale(m);
+}
+// The entry pivot of this lane: the product of the lanes below applied to 0.
+template <typename T>
+__device__ __forceinline__ T pmat_entry(PMat<T> m)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const T ba = __shfl_up_sync(full, m.a, o), bb = __shfl_up_sync(full, m.b, o);
+        const T bc = __shfl_up_sync(full, m.c, o), bd = __shfl_up_sync(full, m.d, o);
+        if (lane >= o) {  // own x lower
+            const PMat<T> r{fma_rn(m.a, ba, mul_rn(m.b, bc)), fma_rn(m.a, bb, mul_rn(m.b, bd)),
+                            fma_rn(m.c, ba, mul_rn(m.d, bc)), fma_rn(m.c, bb, mul_rn(m.d, bd))};
+            m = r;
+            pmat_rescale(m);
+        }
+    }
+    const T eb = __shfl_up_sync(full, m.b, 1), ed = __shfl_up_sync(full, m.d, 1);
+    return lane == 0 ? T(0) : eb / ed;
+}
+// One cell of the recurrence from the previous pivot x (updated to this cell's pr).
+template <typename T>
+__device__ __forceinline__ void factor_cell(T w, T e, T p, T &x, T &pr, T &cf, T &id)
+{
+    T den = fma_rn(-w, x, p);
+    if (fabs(den) <= T(1e-12)) den += T(kSmall);
+    id = T(1) / den;
+    pr = mul_rn(e, id);
+    cf = mul_rn(w, id);
+    x = pr;
+}
+// The warp's line from registers: lane l holds cells l L .. l L + L - 1 (n <= 32 L).
+template <typename T, int L>
+__device__ __forceinline__ void factor_line_regs(int n, const T (&w)[L], const T (&e)[L], const T (&p)[L],
+                                                 T (&pr)[L], T (&cf)[L], T (&id)[L])
+{
+    const int a = (threadIdx.x & 31) * L;
+    PMat<T> m{T(1), T(0), T(0), T(1)};
+#pragma unroll
+    for (int v = 0; v < L; ++v)
+        if (a + v < n) pmat_cell(m, w[v], e[v], p[v]);
+    T x = pmat_entry(m);
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        pr[v] = cf[v] = id[v] = T(0);
+        if (a + v < n) factor_cell(w[v], e[v], p[v], x, pr[v], cf[v], id[v]);
+    }
+}
+// A line's coefficients from global memory (cell i0 of the line at offset c0)
+// and its factorisation (factor_line_regs), into the registers of its warp.
+template <typename T, int L>
+__device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, const Fields<T> &g, size_t c0, int n)
+{
+    const int a = (threadIdx.x & 31) * L;
+    T w[L], e[L], p[L];
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        const bool ok = a + v < n;
+        const size_t c = c0 + (ok ? a + v : 0);
+        r.at[v] = ok ? g.at[c] : T(0);
+        r.ab[v] = ok ? g.ab[c] : T(0);
+        r.an[v] = ok ? g.an[c] : T(0);
+        r.as[v] = ok ? g.as[c] : T(0);
+        r.su[v] = ok ? g.su[c] : T(0);
+        w[v] = ok ? g.aw[c] : T(0);
+        e[v] = ok ? g.ae[c] : T(0);
+        p[v] = ok ? g.ap[c] : T(1);
+    }
+    factor_line_regs<T, L>(n, w, e, p, r.pr, r.cf, r.id);
+}
+
+// The warp's line through accessors: get(i, aw, ae, ap) reads cell i (0-based),
+// put(i, pr, cf, iden) writes it.  The same operations as factor_line_regs.
+template <typename T, class Get, class Put>
+__device__ __forceinline__ void factor_line_mem(int n, Get get, Put put)
+{
+    const int L = (n + 31) >> 5;
+    const int a = min((threadIdx.x & 31) * L, n), b = min(a + L, n);
+    PMat<T> m{T(1), T(0), T(0), T(1)};
+    for (int i = a; i < b; ++i) {
+        T w, e, p;
+        get(i, w, e, p);
+        pmat_cell(m, w, e, p);
+    }
+    T x = pmat_entry(m);
+    for (int i = a; i < b; ++i) {
+        T w, e, p, pr, cf, id;
+        get(i, w, e, p);
+        factor_cell(w, e, p, x, pr, cf, id);
+        put(i, pr, cf, id);
+    }
 }
 
 // Aligned staging window [ib, ie) of cells i0..i1 (16-byte units).
