@@ -529,6 +529,8 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     set_sweep_smem_limit<T>(I.line_smem);
     setup_box_solve<T>(I, !ctx->serial_launch);
     if (ctx->box_ctas > 0 && I.box_grid > 0) I.box_grid = std::min(ctx->box_ctas, I.box_grid);
+    if (sizeof(T) == 4 && I.box_grid > 0)  // the FP32 box solve's tagged exchange of line values
+        if ((rc = alloc3<unsigned long long>(ctx, &I.xchg, n3))) return rc;
     I.sweep_warps_max = set_rounds_smem_limit<T>(p);
     if (I.sweep_warps_max < 2) return fail(ctx, AMCFD_E_CAPACITY, "x-lines too long for the red-black sweep");
     if (ctx->sweep_warps > I.sweep_warps_max)

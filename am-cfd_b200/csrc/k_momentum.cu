@@ -632,6 +632,46 @@ __device__ __forceinline__ bool box_passes_regs(const Fields<T> &g, T *phi, cons
     return ok;
 }
 
+// The eight colour passes of a resident FP32 warp from registers, the lines
+// exchanging values through the tagged copy `xc` (solve_line_tagged): version
+// tb holds the colour-1 lines' values before the first pass, a line's pass t
+// reads version tb + t of its neighbours and writes tb + t + 1.  A line's pass
+// t + 1 on a neighbour waits for this line's version tb + t + 1, which it
+// writes after reading its own inputs, so no value is overwritten before it is
+// read.  False when a wait gave up.
+template <int L>
+__device__ __forceinline__ bool box_passes_tagged(const Fields<float> &g, float *phi, unsigned long long *xc,
+                                                  const size_t (&rows)[2], const int (&jl)[2], int kl,
+                                                  const bool (&has)[2], int n, int i0, int j0, int j1, int k0,
+                                                  int k1, size_t sj, size_t sk, unsigned tb, Status *st,
+                                                  long long polls)
+{
+    const int a = (threadIdx.x & 31) * L;
+    LineRegs<float, L> r0, r1;
+    if (has[0]) load_line_regs<float, L>(r0, g, rows[0] + i0, n);
+    if (has[1]) load_line_regs<float, L>(r1, g, rows[1] + i0, n);
+    if (has[1]) {
+#pragma unroll
+        for (int v = 0; v < L; ++v)
+            if (a + v < n) {
+                const size_t c = rows[1] + i0 + a + v;
+                xc[c] = xtag(phi[c], tb);
+            }
+    }
+    const bool t0 = kl + 1 <= k1, b0 = kl - 1 >= k0;  // (both lines lie in plane kl)
+    bool ok = true;
+    for (int sweep = 0; sweep < 4; ++sweep) {
+        const unsigned t = tb + 2u * (unsigned)sweep;
+        if (ok && has[0])
+            ok = solve_line_tagged<L>(phi, xc, rows[0], i0, n, sj, sk, r0, t0, b0, jl[0] + 1 <= j1, jl[0] - 1 >= j0,
+                                      t, sweep == 3, st, polls);
+        if (ok && has[1])
+            ok = solve_line_tagged<L>(phi, xc, rows[1], i0, n, sj, sk, r1, t0, b0, jl[1] + 1 <= j1, jl[1] - 1 >= j0,
+                                      t + 1u, sweep == 3, st, polls);
+    }
+    return ok;
+}
+
 // ---------------------------------------------------------------------------
 // Momentum-box line solve of equation ivar (1..3: u, v, w; 4: p') in red-black
 // order as one cooperative launch (solveLiquidDomain, CFDSolverManager.cpp:
@@ -653,7 +693,7 @@ __device__ __forceinline__ bool box_passes_regs(const Fields<T> &g, T *phi, cons
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> g, int ivar, const double *red, int nb,
-                                                            int *flags)
+                                                            int *flags, unsigned long long *xchg)
 {
     pdl_enter();
     T *phi = ivar == 1 ? g.uvel : ivar == 2 ? g.vvel : ivar == 3 ? g.wvel : g.pp;
@@ -767,9 +807,19 @@ __global__ void __launch_bounds__(128) mom_box_solve_kernel(Params p, Fields<T> 
     // the eight colour passes: lines of up to 64 cells from registers when every
     // warp holds its lines, otherwise from the staged buffers
     if (regs) {
-        const LineFlags lf{flags, nj, j0, j1, k0, k1, (int)(seq * 16u)};
-        ok = n <= 32 ? box_passes_regs<T, 1>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls)
-                     : box_passes_regs<T, 2>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls);
+        if constexpr (sizeof(T) == 4) {
+            // FP32: values and versions exchanged together
+            const unsigned tb = (seq + 1u) * 16u;
+            ok = n <= 32 ? box_passes_tagged<1>(g, phi, xchg, rows, jl, kl, has, n, i0, j0, j1, k0, k1, sj, sk, tb, st,
+                                                p.wait_polls)
+                         : box_passes_tagged<2>(g, phi, xchg, rows, jl, kl, has, n, i0, j0, j1, k0, k1, sj, sk, tb, st,
+                                                p.wait_polls);
+        } else {
+            // FP64 (a value and its version do not fit one access): completion flags
+            const LineFlags lf{flags, nj, j0, j1, k0, k1, (int)(seq * 16u)};
+            ok = n <= 32 ? box_passes_regs<T, 1>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls)
+                         : box_passes_regs<T, 2>(g, phi, rows, jl, kl, has, n, i0, sj, sk, lf, st, p.wait_polls);
+        }
     }
     for (int pass = 0; pass < 8 && !regs; ++pass) {
         const int c = pass & 1;
@@ -1673,7 +1723,7 @@ template <typename T> static void launch_box_solve(Inst<T> &I, int ivar)
     cfg.attrs = at;
     cfg.numAttrs = 1;
     cudaLaunchKernelEx(&cfg, mom_box_solve_kernel<T>, I.p, I.g, ivar, (const double *)I.red_mom, I.nb_mom,
-                       I.flags_mom);
+                       I.flags_mom, I.xchg);
 }
 // Launch shape of mom_box_solve_kernel: the most warps per CTA (4, 2 or 1) whose
 // buffers (two lines of 8 staged rows and a scratch row each, one mbarrier) fit

@@ -119,6 +119,9 @@ struct Inst {
     // multi-launch form): CTAs, warps per CTA, dynamic shared memory
     int box_grid = 0, box_warps = 4;
     size_t box_smem = 0;
+    // FP32 box lines' values exchanged between passes with a version tag (one
+    // 64-bit word per node of the grid)
+    unsigned long long *xchg = nullptr;
 };
 
 // Launch of a kernel that begins with pdl_enter().  With `pdl` the launch carries

@@ -258,6 +258,133 @@ __device__ __forceinline__ void solve_line_regs(T *phi, size_t row, int i0, int 
 }
 
 // ---------------------------------------------------------------------------
+// One pass over an FP32 line of n <= 32 L cells from its registers, exchanging
+// values with the neighbouring lines through a tagged copy: each cell's entry
+// in `xc` is one 64-bit word, the value's bits low and a version tag high,
+// stored in one access, so a reader sees a whole (value, tag) pair.  The pass
+// reads the four neighbours of each of its cells: from `xc`, waiting (bounded)
+// until the tag is `expect`, where the neighbouring line lies in the box (in_t,
+// in_b, in_n, in_s), else from phi (fixed during the solve); the fixed ends
+// from phi.  It stores its cells to `xc` with tag `expect` + 1 and, on the
+// line's last pass (`last`), to phi.  No fence or flag: a value and its version
+// travel together.  The arithmetic is solve_line_regs's.  False (for the whole
+// warp) when a wait gave up or an error is raised.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long xtag(float v, unsigned tag)
+{
+    return ((unsigned long long)tag << 32) | __float_as_uint(v);
+}
+template <int L>
+__device__ __forceinline__ bool solve_line_tagged(float *phi, unsigned long long *xc, size_t row, int i0, int n,
+                                                  size_t sj, size_t sk, const LineRegs<float, L> &r, bool in_t,
+                                                  bool in_b, bool in_n, bool in_s, unsigned expect, bool last,
+                                                  Status *st, long long polls)
+{
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int a = lane * L;
+    const float lo = ld_shared_row<float>(phi + row + i0 - 1), hi = ld_shared_row<float>(phi + row + i0 + n);
+    const bool in[4] = {in_t, in_b, in_n, in_s};
+    const long long off[4] = {(long long)sk, -(long long)sk, (long long)sj, -(long long)sj};
+    unsigned long long q[4][L];
+    float nv[4][L];
+#pragma unroll
+    for (int d = 0; d < 4; ++d)
+#pragma unroll
+        for (int v = 0; v < L; ++v) {
+            const bool ok = a + v < n;
+            const size_t c = row + i0 + (ok ? a + v : 0) + off[d];
+            q[d][v] = (ok && in[d]) ? __ldcg(xc + c) : xtag(0.f, expect);
+            nv[d][v] = (ok && !in[d]) ? ld_shared_row<float>(phi + c) : 0.f;
+        }
+    int good = 1;
+    for (long long it = 0;; ++it) {
+        bool ready = true;
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+#pragma unroll
+            for (int v = 0; v < L; ++v) ready = ready && (unsigned)(q[d][v] >> 32) == expect;
+        if (ready) break;
+        if ((it & 63) == 63 && *(volatile int *)&st->error) { good = 0; break; }
+        if (it > polls) {
+            if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -5;
+            good = 0;
+            break;
+        }
+#pragma unroll
+        for (int d = 0; d < 4; ++d)
+#pragma unroll
+            for (int v = 0; v < L; ++v)
+                if ((unsigned)(q[d][v] >> 32) != expect) {
+                    const size_t c = row + i0 + a + v + off[d];
+                    q[d][v] = __ldcg(xc + c);
+                }
+    }
+    if (!__all_sync(full, good)) return false;
+    float e[L];
+#pragma unroll
+    for (int v = 0; v < L; ++v) {
+        float w[4];
+#pragma unroll
+        for (int d = 0; d < 4; ++d) w[d] = in[d] ? __uint_as_float((unsigned)q[d][v]) : nv[d][v];
+        e[v] = line_rhs(r.at[v], w[0], r.ab[v], w[1], r.an[v], w[2], r.as[v], w[3], r.su[v], r.id[v]);
+    }
+    float A = 1.f, B = 0.f;
+#pragma unroll
+    for (int v = 0; v < L; ++v)
+        if (a + v < n) {
+            B = fma_rn(r.cf[v], B, e[v]);
+            A = mul_rn(r.cf[v], A);
+        }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float A2 = __shfl_up_sync(full, A, o), B2 = __shfl_up_sync(full, B, o);
+        if (lane >= o) {
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
+        }
+    }
+    float Ae = __shfl_up_sync(full, A, 1), Be = __shfl_up_sync(full, B, 1);
+    if (lane == 0) { Ae = 1.f; Be = 0.f; }
+    float x = fma_rn(Ae, lo, Be);
+#pragma unroll
+    for (int v = 0; v < L; ++v)
+        if (a + v < n) {
+            x = fma_rn(r.cf[v], x, e[v]);
+            e[v] = x;
+        }
+    A = 1.f;
+    B = 0.f;
+#pragma unroll
+    for (int v = L - 1; v >= 0; --v)
+        if (a + v < n) {
+            B = fma_rn(r.pr[v], B, e[v]);
+            A = mul_rn(r.pr[v], A);
+        }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const float A2 = __shfl_down_sync(full, A, o), B2 = __shfl_down_sync(full, B, o);
+        if (lane + o < 32) {
+            B = fma_rn(A, B2, B);
+            A = mul_rn(A, A2);
+        }
+    }
+    Ae = __shfl_down_sync(full, A, 1);
+    Be = __shfl_down_sync(full, B, 1);
+    if (lane == 31) { Ae = 1.f; Be = 0.f; }
+    x = fma_rn(Ae, hi, Be);
+#pragma unroll
+    for (int v = L - 1; v >= 0; --v)
+        if (a + v < n) {
+            x = fma_rn(r.pr[v], x, e[v]);
+            const size_t c = row + i0 + a + v;
+            xc[c] = xtag(x, expect + 1u);
+            if (last) phi[c] = x;
+        }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // Thomas factorisation of one line by one warp: den_i = ap_i - aw_i pr_{i-1},
 // pr_i = ae_i / den_i, cf_i = aw_i / den_i, iden_i = 1 / den_i from pr = 0
 // before the first cell, with solveLiquidDomain's guard on |den|
