@@ -612,8 +612,11 @@ __device__ __forceinline__ bool box_passes_regs(const Fields<T> &g, T *phi, cons
     const int lane = threadIdx.x & 31;
     bool ok = true;
     LineRegs<T, L> r0, r1;
-    if (has[0]) load_line_regs<T, L>(r0, g, rows[0] + i0, n);
-    if (has[1]) load_line_regs<T, L>(r1, g, rows[1] + i0, n);
+    LineFetch<T, L> f0, f1;
+    if (has[0]) load_line_regs<T, L>(r0, f0, g, rows[0] + i0, n);
+    if (has[1]) load_line_regs<T, L>(r1, f1, g, rows[1] + i0, n);
+    if (has[0]) factor_line_regs<T, L>(n, f0.w, f0.e, f0.p, r0.pr, r0.cf, r0.id);
+    if (has[1]) factor_line_regs<T, L>(n, f1.w, f1.e, f1.p, r1.pr, r1.cf, r1.id);
     for (int sweep = 0; sweep < 4; ++sweep) {
         const int t0 = 2 * sweep, t1 = t0 + 1;
         if (has[0]) {
@@ -648,8 +651,11 @@ __device__ __forceinline__ bool box_passes_tagged(const Fields<float> &g, float 
 {
     const int a = (threadIdx.x & 31) * L;
     LineRegs<float, L> r0, r1;
-    if (has[0]) load_line_regs<float, L>(r0, g, rows[0] + i0, n);
-    if (has[1]) load_line_regs<float, L>(r1, g, rows[1] + i0, n);
+    LineFetch<float, L> f0, f1;
+    if (has[0]) load_line_regs<float, L>(r0, f0, g, rows[0] + i0, n);
+    if (has[1]) load_line_regs<float, L>(r1, f1, g, rows[1] + i0, n);
+    if (has[0]) factor_line_regs<float, L>(n, f0.w, f0.e, f0.p, r0.pr, r0.cf, r0.id);
+    if (has[1]) factor_line_regs<float, L>(n, f1.w, f1.e, f1.p, r1.pr, r1.cf, r1.id);
     if (has[1]) {
 #pragma unroll
         for (int v = 0; v < L; ++v)

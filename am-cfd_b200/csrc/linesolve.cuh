@@ -403,14 +403,29 @@ template <typename T>
 struct PMat {
     T a, b, c, d;  // [[a, b], [c, d]]
 };
+// Scale by the power of two that brings the largest entry into [1, 2): the
+// exponent field of the largest magnitude gives it directly (entries that are
+// zero, subnormal, infinite or NaN, or too large for the scale to be normal,
+// are left alone).
+__device__ __forceinline__ float pow2_inverse_scale(float mx, bool &ok)
+{
+    const unsigned eb = (__float_as_uint(mx) >> 23) & 0xffu;
+    ok = eb >= 1u && eb <= 253u;
+    return __uint_as_float((254u - eb) << 23);
+}
+__device__ __forceinline__ double pow2_inverse_scale(double mx, bool &ok)
+{
+    const unsigned long long eb = (unsigned long long)(__double_as_longlong(mx) >> 52) & 0x7ffull;
+    ok = eb >= 1ull && eb <= 2045ull;
+    return __longlong_as_double((long long)((2046ull - eb) << 52));
+}
 template <typename T>
 __device__ __forceinline__ void pmat_rescale(PMat<T> &m)
 {
     const T mx = fmax(fmax(fabs(m.a), fabs(m.b)), fmax(fabs(m.c), fabs(m.d)));
-    if (mx > T(0) && mx < T(INFINITY)) {
-        int e;
-        frexp(mx, &e);
-        const T s = ldexp(T(1), -e);
+    bool ok;
+    const T s = pow2_inverse_scale(mx, ok);
+    if (ok) {
         m.a *= s; m.b *= s; m.c *= s; m.d *= s;
     }
 }
@@ -471,12 +486,21 @@ __device__ __forceinline__ void factor_line_regs(int n, const T (&w)[L], const T
     }
 }
 // A line's coefficients from global memory (cell i0 of the line at offset c0)
-// and its factorisation (factor_line_regs), into the registers of its warp.
+// into the registers of its warp; aw, ae, ap into `f` for the factorisation
+// (factor_line_regs), which the caller runs once the loads of all its lines are
+// in flight.
 template <typename T, int L>
-__device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, const Fields<T> &g, size_t c0, int n)
+struct LineFetch {
+    T w[L], e[L], p[L];
+};
+template <typename T, int L>
+__device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, LineFetch<T, L> &f, const Fields<T> &g,
+                                               size_t c0, int n)
 {
     const int a = (threadIdx.x & 31) * L;
-    T w[L], e[L], p[L];
+    T (&w)[L] = f.w;
+    T (&e)[L] = f.e;
+    T (&p)[L] = f.p;
 #pragma unroll
     for (int v = 0; v < L; ++v) {
         const bool ok = a + v < n;
@@ -490,7 +514,6 @@ __device__ __forceinline__ void load_line_regs(LineRegs<T, L> &r, const Fields<T
         e[v] = ok ? g.ae[c] : T(0);
         p[v] = ok ? g.ap[c] : T(1);
     }
-    factor_line_regs<T, L>(n, w, e, p, r.pr, r.cf, r.id);
 }
 
 // The warp's line through accessors: get(i, aw, ae, ap) reads cell i (0-based),
