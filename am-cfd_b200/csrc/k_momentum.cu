@@ -577,23 +577,20 @@ __device__ __forceinline__ bool wait_neighbours(const LineFlags &lf, int j, int 
     else if (lane == 1) { jn = j + 1; need = jn <= lf.j1; }
     else if (lane == 2) { kn = k - 1; need = kn >= lf.k0; }
     else if (lane == 3) { kn = k + 1; need = kn <= lf.k1; }
-    int good = 1;
-    if (need) {
-        const int *p = lf.f + (size_t)kn * lf.nj + jn;
-        const int target = lf.base + t;
-        long long it = 0;
-        while (ld_acquire_gpu_int(p) - target < 0) {
-            if ((it & 63) == 63 && *(volatile int *)&st->error) { good = 0; break; }
-            if (++it > polls) {
-                if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -4;
-                good = 0;
-                break;
-            }
+    // the whole warp polls together, so that it leaves the loop converged
+    const int *p = lf.f + (size_t)kn * lf.nj + jn;
+    const int target = lf.base + t;
+    for (long long it = 0;; ++it) {
+        const bool ready = !need || ld_acquire_gpu_int(p) - target >= 0;
+        if (__all_sync(0xffffffffu, ready)) break;
+        if ((it & 63) == 63 && __any_sync(0xffffffffu, *(volatile int *)&st->error != 0)) return false;
+        if (it > polls) {
+            if (lane == 0 && atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -4;
+            return false;
         }
     }
-    const bool all = __all_sync(0xffffffffu, good) != 0;
     __syncwarp();
-    return all;
+    return true;
 }
 
 // The eight colour passes of a resident warp (one line of each colour, or none)

@@ -297,19 +297,20 @@ __device__ __forceinline__ bool solve_line_tagged(float *phi, unsigned long long
             q[d][v] = (ok && in[d]) ? __ldcg(xc + c) : xtag(0.f, expect);
             nv[d][v] = (ok && !in[d]) ? ld_shared_row<float>(phi + c) : 0.f;
         }
-    int good = 1;
+    // the whole warp polls together (a lane whose values have arrived waits for
+    // the others in the vote), so that it leaves the loop converged: lanes
+    // leaving one by one would run the scans below in as many divergent groups
     for (long long it = 0;; ++it) {
         bool ready = true;
 #pragma unroll
         for (int d = 0; d < 4; ++d)
 #pragma unroll
             for (int v = 0; v < L; ++v) ready = ready && (unsigned)(q[d][v] >> 32) == expect;
-        if (ready) break;
-        if ((it & 63) == 63 && *(volatile int *)&st->error) { good = 0; break; }
+        if (__all_sync(full, ready)) break;
+        if ((it & 63) == 63 && __any_sync(full, *(volatile int *)&st->error != 0)) return false;
         if (it > polls) {
-            if (atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -5;
-            good = 0;
-            break;
+            if (lane == 0 && atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = -5;
+            return false;
         }
 #pragma unroll
         for (int d = 0; d < 4; ++d)
@@ -320,7 +321,6 @@ __device__ __forceinline__ bool solve_line_tagged(float *phi, unsigned long long
                     q[d][v] = __ldcg(xc + c);
                 }
     }
-    if (!__all_sync(full, good)) return false;
     float e[L];
 #pragma unroll
     for (int v = 0; v < L; ++v) {
@@ -618,6 +618,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, unsigned *gen, uns
         ok_s = ok;
     }
     __syncthreads();
+    __syncwarp();  // thread 0's warp leaves converged
     return ok_s != 0;
 }
 
