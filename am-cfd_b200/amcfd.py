@@ -84,7 +84,7 @@ class AmcfdOptions(C.Structure):
                 ("check_finite", _I), ("no_small_box", _I), ("host_loop", _I),
                 ("wait_polls", _I), ("autotune", _I), ("asm_kseg", _I), ("sweep_warps", _I),
                 ("mom_cluster", _I), ("serial_launch", _I), ("box_ctas", _I),
-                ("reserved", _I * 1)]
+                ("pass_launch", _I)]
 
 
 class AmcfdError(RuntimeError):
@@ -317,7 +317,7 @@ class Solver:
                  device: int = 0, use_graphs: int = 0, check_finite: int = 1,
                  small_box: int = 1, host_loop: int = 0, wait_polls: int = 0, autotune: int = 0,
                  asm_kseg: int = 0, sweep_warps: int = 0, mom_cluster: int = 0, serial_launch: int = 0,
-                 box_ctas: int = 0):
+                 box_ctas: int = 0, pass_launch: int = 0):
         L = lib()
         self.deck = deck  # keeps toolpath storage alive
         opts = AmcfdOptions(device=device, order=order, precision=precision,
@@ -325,7 +325,7 @@ class Solver:
                             no_small_box=0 if small_box else 1, host_loop=host_loop,
                             wait_polls=wait_polls, autotune=autotune, asm_kseg=asm_kseg,
                             sweep_warps=sweep_warps, mom_cluster=mom_cluster,
-                            serial_launch=serial_launch, box_ctas=box_ctas)
+                            serial_launch=serial_launch, box_ctas=box_ctas, pass_launch=pass_launch)
         self._h = C.c_void_p()
         rc = L.amcfd_create(C.byref(deck.params), C.byref(opts), C.byref(self._h))
         if rc != 0:

@@ -25,6 +25,7 @@ namespace amcfd {
 template <typename T> int exact_sweep_blocks_per_sm(int warps, size_t smem);
 template <typename T> void set_sweep_smem_limit(size_t smem);
 template <typename T> int set_rounds_smem_limit(const Params &p);
+template <typename T> int setup_pipe_sweep(const Params &p, int warps, int sm_count, size_t &smem);
 dim3 energy_assemble_grid(const Params &p, int kseg);
 template <typename T> int h2t_blocks_per_sm();
 template <typename T> void launch_pack_field(const T *src, double *dst, int ni, int nip,
@@ -123,6 +124,7 @@ struct amcfd_ctx {
     int mom_cluster = 1;           // CTAs of the cluster momentum path (1: none)
     int mom_cluster_req = 0;       // as requested by the options (0: default)
     int serial_launch = 0;         // 1: no programmatic dependent launch, box solve per pass
+    int pass_launch = 0;           // 1: the whole-domain red-black sweeps take a launch per pass
     int box_ctas = 0;              // CTAs of the cooperative box solve (0: what the box needs)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
     bool small_box = true;         // the one-CTA momentum chain may be used
@@ -536,6 +538,12 @@ static int setup_instance(amcfd_ctx *ctx, Inst<T> &I)
     if (ctx->sweep_warps > I.sweep_warps_max)
         return fail(ctx, AMCFD_E_CAPACITY, "sweep_warps beyond what the x-lines leave room for");
     I.sweep_warps = std::min(I.sweep_warps, I.sweep_warps_max);
+    if (I.order == AMCFD_ORDER_REDBLACK && !ctx->serial_launch && !ctx->pass_launch) {
+        // the eight passes of a whole-domain solve in one pipelined launch (k_linesolve.cu)
+        if ((rc = alloc3<int>(ctx, &I.flags_pipe, (size_t)p.nk * p.nj))) return rc;
+        I.pipe_grid = setup_pipe_sweep<T>(p, I.pipe_warps, I.sm_count, I.pipe_smem);
+        if (I.dc_on) I.pipe_grid_dc = setup_pipe_sweep<float>(p, I.pipe_warps, I.sm_count, I.pipe_smem_dc);
+    }
     int bps = exact_sweep_blocks_per_sm<T>(I.exact_warps, I.line_smem);
     // A wave of the exact-order sweep holds about 2(nj-2)/3 lines; about three
     // waves of lines in flight keep the dependency chain fed without flooding L2
@@ -817,10 +825,14 @@ static int read_status(amcfd_ctx *ctx)
 static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
 {
     const long long sweeps = ctx->order == AMCFD_ORDER_EXACT ? 1 : 8;
+    // whole-domain red-black solves: one pipelined launch, or one per pass
+    const bool fp64 = ctx->precision == AMCFD_PREC_FP64;
+    const long long phi_sweeps = (fp64 ? ctx->I64.pipe_grid : ctx->I32.pipe_grid) > 0 ? 1 : sweeps;
+    const long long energy_sweeps = (ctx->dc ? ctx->I64.pipe_grid_dc > 0 : phi_sweeps == 1) ? 1 : sweeps;
     switch (phase) {
     case AMCFD_PHASE_LASER: return 1;
     case AMCFD_PHASE_ENERGY_ASSEMBLE: return 3;
-    case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : sweeps;
+    case AMCFD_PHASE_ENERGY_SOLVE: return ctx->order == AMCFD_ORDER_EXACT ? 1 + sweeps : energy_sweeps;
     case AMCFD_PHASE_H2T: return ctx->dc ? 2 : 1;
     case AMCFD_PHASE_MELTPOOL: return 1;
     case AMCFD_PHASE_MOMENTUM: {
@@ -834,7 +846,7 @@ static long long phase_launches(const amcfd_ctx *ctx, int phase, bool small)
     }
     case AMCFD_PHASE_CONVERGE: return 1;
     case AMCFD_PHASE_UPDATE: return ctx->prm.species ? 2 : 1;
-    case AMCFD_PHASE_SPECIES: return ctx->prm.species ? (ctx->order == AMCFD_ORDER_EXACT ? 4 : 3) + sweeps : 0;
+    case AMCFD_PHASE_SPECIES: return ctx->prm.species ? (ctx->order == AMCFD_ORDER_EXACT ? 4 : 3) + phi_sweeps : 0;
     default: return 0;
     }
 }
@@ -1105,7 +1117,9 @@ static int outer_loop(amcfd_ctx *ctx, Inst<T> &I)
             cudaEventElapsedTime(&ms, ctx->ev[7], ctx->ev[6]);
             ctx->last_ms[5] += ms;
             ctx->last_ms[8] += 1.0;
-            ctx->last_ms[9] += ctx->order == AMCFD_ORDER_EXACT ? 1.0 : 8.0;
+            ctx->last_ms[9] += ctx->order == AMCFD_ORDER_EXACT
+                                   ? 1.0
+                                   : (double)phase_launches(ctx, AMCFD_PHASE_ENERGY_SOLVE, small);
         }
         if (ctx->st_host->converged) break;
     }
@@ -1324,6 +1338,7 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
             return fail(ctx, AMCFD_E_ARG, "mom_cluster must be 0, 1, 2, 4, 8 or 16");
         ctx->mom_cluster_req = opts->mom_cluster;
         ctx->serial_launch = opts->serial_launch != 0;
+        ctx->pass_launch = opts->pass_launch != 0;
         if (opts->box_ctas < 0) return fail(ctx, AMCFD_E_ARG, "box_ctas must not be negative");
         ctx->box_ctas = opts->box_ctas;
         ctx->autotune = opts->autotune != 0;

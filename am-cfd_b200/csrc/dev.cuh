@@ -80,6 +80,9 @@ struct Status {
     // grid barrier of the cooperative momentum-box solve: arrivals, generation;
     // its line-flag epochs: launch sequence number, CTAs done with the passes
     unsigned gbar_count, gbar_gen, gflag_seq, gflag_done;
+    // pipelined red-black sweep (all passes in one launch): launch sequence number,
+    // CTAs done, next work ticket
+    unsigned long long seq_pipe, done_pipe, ticket_pipe;
 };
 
 // Outer-loop control of a step captured as one CUDA graph (a chain of

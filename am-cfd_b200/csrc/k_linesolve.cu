@@ -303,33 +303,36 @@ __global__ void sweep_rb_kernel(Params p, Fields<T> g, T *phi, int color)
 template <typename T>
 __device__ __forceinline__ void mat_rescale(T &a, T &b, T &c, T &d);
 
-template <typename T, bool FACTOR>
-__global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
-                                                              int correct)
+// 16-byte vector load; CG: through L2 only (rows that other SMs write while the
+// kernel runs: the pipelined sweep's neighbour values and factorisation rows).
+template <bool CG, typename T>
+__device__ __forceinline__ void ld16x(const T *ptr, T (&o)[16 / sizeof(T)])
 {
-    pdl_enter();
+    if constexpr (CG) {
+        const typename Vec16<T>::type v = __ldcg(reinterpret_cast<const typename Vec16<T>::type *>(ptr));
+        memcpy(o, &v, 16);
+    } else {
+        ld16(ptr, o);
+    }
+}
+
+// One pass over the interior x-line (j, k) by the calling warp; sq/spr are the
+// warp's qr/pr buffers (2 R RC elements).  The same operations whichever kernel
+// calls it, so the per-pass launches and the pipelined launch give the same bits.
+template <typename T, bool FACTOR, bool CG>
+__device__ __forceinline__ void rb_line_rounds(const Params &p, const Fields<T> &g, T *phi, int j, int k,
+                                               int correct, T *sq, T *spr)
+{
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int RC = 32 * V;
-    extern __shared__ unsigned char smraw[];
     const int i0 = 1, i1 = p.nim2, j0 = 1, j1 = p.njm2, k0 = 1, k1 = p.nkm2;
-    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
-    if (J <= 0 || K <= 0 || i1 < i0) return;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31;
     const unsigned full = 0xffffffffu;
     const int ib = i0 & ~31;
     const int R = (i1 - ib) / RC + 1;
-    T *sq = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * R * RC;
-    T *spr = sq + (size_t)R * RC;
     const int nj = p.nj, nip = p.nip;
     const size_t sj = nip, sk = (size_t)nj * nip;
-    const int half = (J + 1) / 2;
-    const int nl = half * K;
-    for (int q = blockIdx.x * wpb + warp; q < nl; q += gridDim.x * wpb) {
-        const int kk = q / half, r = q - kk * half;
-        const int k = k0 + kk;
-        const int jpar = ((color - k - j0) % 2 + 2) % 2;  // offset of the first j of this colour
-        const int j = j0 + jpar + 2 * r;
-        if (j > j1) continue;  // warp-uniform
+    {
         const size_t row = cidx(0, j, k, nj, nip);
         T carry = phi[row + i0 - 1];
         T carry_pr = T(0);  // FACTOR: pr at cell i0 - 1
@@ -345,7 +348,8 @@ __global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T
 #pragma unroll
                 for (int v = 0; v < V; ++v) vt[v] = vb[v] = vn[v] = vs[v] = T(0);
             } else {
-                ld16(phi + c + sk, vt); ld16(phi + c - sk, vb); ld16(phi + c + sj, vn); ld16(phi + c - sj, vs);
+                ld16x<CG>(phi + c + sk, vt); ld16x<CG>(phi + c - sk, vb);
+                ld16x<CG>(phi + c + sj, vn); ld16x<CG>(phi + c - sj, vs);
             }
             ld16(g.at + c, wt); ld16(g.ab + c, wb); ld16(g.an + c, wn); ld16(g.as + c, ws);
             ld16(g.su + c, wu);
@@ -414,7 +418,7 @@ __global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T
                         }
                 }
             } else {
-                ld16(g.cf + c, wc); ld16(g.iden + c, wi); ld16(g.pr + c, wp);
+                ld16x<CG>(g.cf + c, wc); ld16x<CG>(g.iden + c, wi); ld16x<CG>(g.pr + c, wp);
             }
             T a[V], e[V];
             T Al = T(1), Bl = T(0);
@@ -502,6 +506,165 @@ __global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T
             next = __shfl_sync(full, A * next + B, 0);
         }
         __syncwarp();
+    }
+}
+
+// One red-black pass: every line of colour `color`, one warp per line.
+template <typename T, bool FACTOR>
+__global__ void __launch_bounds__(256) sweep_rb_rounds_kernel(Params p, Fields<T> g, T *phi, int color,
+                                                              int correct)
+{
+    pdl_enter();
+    constexpr int RC = 32 * (16 / (int)sizeof(T));
+    extern __shared__ unsigned char smraw[];
+    const int i0 = 1, i1 = p.nim2, j0 = 1, j1 = p.njm2, k0 = 1, k1 = p.nkm2;
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    if (J <= 0 || K <= 0 || i1 < i0) return;
+    const int warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int R = (i1 - (i0 & ~31)) / RC + 1;
+    T *sq = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * R * RC;
+    T *spr = sq + (size_t)R * RC;
+    const int half = (J + 1) / 2;
+    const int nl = half * K;
+    for (int q = blockIdx.x * wpb + warp; q < nl; q += gridDim.x * wpb) {
+        const int kk = q / half, r = q - kk * half;
+        const int k = k0 + kk;
+        const int jpar = ((color - k - j0) % 2 + 2) % 2;  // offset of the first j of this colour
+        const int j = j0 + jpar + 2 * r;
+        if (j > j1) continue;  // warp-uniform
+        rb_line_rounds<T, FACTOR, false>(p, g, phi, j, k, correct, sq, spr);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The eight red-black passes of one solve (2 colours x 4 sweeps) in a single
+// launch: a pass starts on a plane as soon as the planes it reads have been
+// through the pass before, instead of after the whole previous launch has
+// drained.
+//
+// Work item (pass q, plane k, line j of colour q&1).  Its inputs are the
+// values of the four neighbouring lines after pass q-1 (and the line's own
+// factorisation, formed in pass q&1); the neighbours' pass q-1 in turn read
+// the values that pass q overwrites.  So an item may run once the four
+// neighbours have finished pass q-1 and the line itself pass q-2 -- exactly
+// the values the per-pass launches give it, hence the same bits.
+//
+// Items are handed out by an atomic ticket in the order of the key
+// s = (k - k0) + D q (D = `stride` planes), then q, then j: every item an
+// item waits for has a smaller key, so the smallest outstanding ticket is
+// always runnable (no co-residency assumption).  An item waits for items
+// D - 1 keys back, so D must exceed the keys in flight (about 3500 warps over
+// 800 items a key on the 400x200x100 deck) for the waits to be short; a
+// window small enough for the later passes to find a plane's rows in L2 (D of
+// 2-4) makes every item wait on the one before it instead, and was measured
+// slower than a launch per pass.
+// Per-line flags hold 16 seq + (last pass finished + 1), seq counting launches;
+// every wait is bounded (wait_polls) and records AMCFD_E_TIMEOUT.
+// ---------------------------------------------------------------------------
+// (pass, plane) pairs with key below s, for K planes: sum over q of clamp(s - 2q, 0, K).
+__device__ __forceinline__ int pipe_pairs_before(int s, int K, int D)
+{
+    int n = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) n += min(max(s - D * q, 0), K);
+    return n;
+}
+
+// A warp waits until, in every lane with a flag, *f >= target (wrap-safe): one
+// vote per poll, so the warp leaves converged; false after `limit` polls (the
+// error is recorded) or once another warp has raised an error.
+__device__ bool warp_wait_ge(const int *f, int target, Status *st, int where, long long limit)
+{
+    const unsigned full = 0xffffffffu;
+    for (long long it = 0;; ++it) {
+        const bool ok = f == nullptr || *(volatile const int *)f - target >= 0;
+        if (__all_sync(full, ok)) return true;
+        if ((it & 63) == 63) {
+            int e = 0;
+            if ((threadIdx.x & 31) == 0) e = *(volatile int *)&st->error;
+            if (__shfl_sync(full, e, 0)) return false;
+        }
+        if (it >= limit) {
+            if ((threadIdx.x & 31) == 0 && atomicCAS(&st->error, 0, AMCFD_E_TIMEOUT) == 0) st->error_where = where;
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 3) sweep_rb_pipe_kernel(Params p, Fields<T> g, T *phi, int correct, int stride,
+                                                               int *flags, unsigned long long *seqp,
+                                                               unsigned long long *donep, unsigned long long *ticketp)
+{
+    pdl_enter();
+    constexpr int RC = 32 * (16 / (int)sizeof(T));
+    extern __shared__ unsigned char smraw[];
+    __shared__ unsigned long long seq_s;
+    Status *st = g.st;
+    if (threadIdx.x == 0) seq_s = *(volatile unsigned long long *)seqp;
+    __syncthreads();
+    const int i0 = 1, i1 = p.nim2, j0 = 1, j1 = p.njm2, k0 = 1, k1 = p.nkm2;
+    const int J = j1 - j0 + 1, K = k1 - k0 + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (J > 0 && K > 0 && i1 >= i0) {
+        const int R = (i1 - (i0 & ~31)) / RC + 1;
+        T *sq = reinterpret_cast<T *>(smraw) + (size_t)warp * 2 * R * RC;
+        T *spr = sq + (size_t)R * RC;
+        const int nj = p.nj;
+        const int half = (J + 1) / 2;
+        const unsigned long long nt = (unsigned long long)half * 8ull * (unsigned long long)K;
+        const int base = (int)(seq_s * 16ull);
+        const long long lim = p.wait_polls;
+        while (true) {
+            unsigned long long tk = 0;
+            if (lane == 0) tk = atomicAdd(ticketp, 1ull);
+            tk = __shfl_sync(0xffffffffu, tk, 0);
+            if (tk >= nt) break;
+            const int idx = (int)(tk / (unsigned)half), r = (int)(tk - (unsigned long long)idx * half);
+            int lo = 0, hi = K - 1 + 7 * stride;  // the key: the largest s with pipe_pairs_before(s) <= idx
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (pipe_pairs_before(mid, K, stride) <= idx) lo = mid;
+                else hi = mid - 1;
+            }
+            const int pass = (lo >= K ? (lo - K + stride) / stride : 0) + (idx - pipe_pairs_before(lo, K, stride));
+            const int k = k0 + lo - stride * pass;
+            const int jpar = (((pass & 1) - k - j0) % 2 + 2) % 2;
+            const int j = j0 + jpar + 2 * r;
+            if (j > j1) continue;  // warp-uniform: this colour has one line fewer in the plane
+            // lane 0: the line itself after pass - 2; lanes 1-4: its neighbours after pass - 1
+            const int *f = nullptr;
+            int target = 0;
+            if (lane == 0 && pass >= 2) f = &flags[k * nj + j], target = base + pass - 1;
+            if (pass >= 1) {
+                if (lane == 1 && j > j0) f = &flags[k * nj + j - 1];
+                if (lane == 2 && j < j1) f = &flags[k * nj + j + 1];
+                if (lane == 3 && k > k0) f = &flags[(k - 1) * nj + j];
+                if (lane == 4 && k < k1) f = &flags[(k + 1) * nj + j];
+                if (lane >= 1 && lane <= 4) target = base + pass;
+            }
+            if (!warp_wait_ge(f, target, st, k * nj + j, lim)) break;
+            __threadfence();
+            if (pass < 2)
+                rb_line_rounds<T, true, true>(p, g, phi, j, k, pass == 0 ? correct : 0, sq, spr);
+            else
+                rb_line_rounds<T, false, true>(p, g, phi, j, k, 0, sq, spr);
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) atomicExch(&flags[k * nj + j], base + pass + 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned long long prev = atomicAdd(donep, 1ull);
+        if (prev == (unsigned long long)gridDim.x - 1) {
+            // last CTA of this launch: reset the counters for the next one
+            atomicExch(donep, 0ull);
+            atomicExch(ticketp, 0ull);
+            __threadfence();
+            atomicAdd(seqp, 1ull);
+        }
     }
 }
 
@@ -719,6 +882,11 @@ template <typename T> static void sweeps(Inst<T> &I, T *phi, bool box)
         for (int sweep = 0; sweep < 4; ++sweep)
             for (int color = 0; color < 2; ++color)
                 launch_k(I.pdl, sweep_rb_kernel<T, true>, grid, 32 * warps, smem, I.stream, I.p, I.g, phi, color);
+    } else if (I.pipe_grid > 0) {
+        // whole domain, the eight passes in one pipelined launch
+        Status *st = I.g.st;
+        launch_k(I.pdl, sweep_rb_pipe_kernel<T>, I.pipe_grid, 32 * I.pipe_warps, I.pipe_smem, I.stream, I.p, I.g, phi,
+                 1, I.pipe_stride, I.flags_pipe, &st->seq_pipe, &st->done_pipe, &st->ticket_pipe);
     } else {
         // whole domain: one line per warp, sweep_warps warps per CTA
         const int w = I.sweep_warps;
@@ -763,6 +931,12 @@ void launch_dc_sweeps(Inst<double> &I)
     f.pr = d.pr; f.cf = d.cf; f.iden = d.iden;
     f.delphi = I.g.delphi;
     f.st = I.g.st;
+    if (I.pipe_grid_dc > 0) {
+        Status *st = I.g.st;
+        launch_k(I.pdl, sweep_rb_pipe_kernel<float>, I.pipe_grid_dc, 32 * I.pipe_warps, I.pipe_smem_dc, I.stream, I.p,
+                 f, d.delta, 2, I.pipe_stride, I.flags_pipe, &st->seq_pipe, &st->done_pipe, &st->ticket_pipe);
+        return;
+    }
     const int w = I.sweep_warps;
     const int lines = ((I.p.nj - 2 + 1) / 2) * (I.p.nk - 2);
     const int grid = std::max(1, (lines + w - 1) / w);
@@ -856,7 +1030,22 @@ template <typename T> int set_rounds_smem_limit(const Params &p)
     return 0;
 }
 
+// Launch shape of the pipelined sweep: `warps` lines per CTA, as many CTAs as are
+// resident at once (the kernel needs none of them to be: its tickets come in
+// dependency order); 0 when a CTA's line buffers do not fit.
+template <typename T> int setup_pipe_sweep(const Params &p, int warps, int sm_count, size_t &smem)
+{
+    smem = rounds_smem<T>(p, warps);
+    if (smem > 200 * 1024 || raise_smem_limit((const void *)sweep_rb_pipe_kernel<T>, smem) != cudaSuccess) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sweep_rb_pipe_kernel<T>, 32 * warps, smem) != cudaSuccess ||
+        nb < 1)
+        return 0;
+    return nb * sm_count;
+}
+
 #define AMCFD_INST(T)                                                     \
+    template int setup_pipe_sweep<T>(const Params &, int, int, size_t &); \
     template void launch_energy_factor<T>(Inst<T> &);                    \
     template void launch_box_factor<T>(Inst<T> &);                       \
     template void launch_energy_sweeps<T>(Inst<T> &);                    \

@@ -122,6 +122,15 @@ struct Inst {
     // FP32 box lines' values exchanged between passes with a version tag (one
     // 64-bit word per node of the grid)
     unsigned long long *xchg = nullptr;
+    // the whole-domain red-black passes of a solve as one pipelined launch
+    // (pipe_grid 0: a launch per pass): CTAs, warps per CTA, planes between the
+    // passes in the work order, dynamic shared memory, per-line pass flags;
+    // pipe_*_dc: the FP32 correction sweeps of defect correction.  Measured on the
+    // 400x200x100 deck (FP32, ms per solve): stride 2: 0.567, 4: 0.386, 6: 0.338,
+    // 8: 0.320, 12-32: 0.312-0.315, 128: 0.317; a launch per pass 0.344
+    int pipe_grid = 0, pipe_warps = 8, pipe_grid_dc = 0, pipe_stride = 16;
+    size_t pipe_smem = 0, pipe_smem_dc = 0;
+    int *flags_pipe = nullptr;
 };
 
 // Launch of a kernel that begins with pdl_enter().  With `pdl` the launch carries

@@ -361,6 +361,8 @@ def main():
                     help="momentum boxes of every size on the grid path (no one-CTA path)")
     ap.add_argument("--serial-launch", action="store_true",
                     help="no programmatic dependent launch; the box line solve as a launch per colour pass")
+    ap.add_argument("--pass-launch", action="store_true",
+                    help="the whole-domain red-black line sweeps as a launch per pass (not pipelined)")
     ap.add_argument("--mom-cluster", type=int, default=0, choices=[0, 1, 2, 4, 8, 16],
                     help="CTAs of the cluster momentum solve (1: none, 0: the library default)")
     ap.add_argument("--profile-window", action="store_true",
@@ -439,7 +441,7 @@ def main():
         sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
                           host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster,
                           small_box=0 if args.no_small_box else 1, serial_launch=1 if args.serial_launch else 0,
-                          **kw)
+                          pass_launch=1 if args.pass_launch else 0, **kw)
         tune.setdefault(p, sv.tuning())
         return sv
 
@@ -587,6 +589,8 @@ def main():
                                outer_loop="host" if args.host_loop or not args.graphs else "device",
                                momentum=("grid" if args.no_small_box else "one-CTA below its capacity, else grid")
                                + (", serial launches" if args.serial_launch else ""),
+                               sweeps="a launch per pass" if args.pass_launch or args.serial_launch
+                               else "the 8 passes of a solve in one pipelined launch",
                                parallelism=f"replicas{world}"),
                 "cell_iters_per_s": cips, "outer_iters": iters, "gpu_launches": launches,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": ck,

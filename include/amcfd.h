@@ -182,7 +182,13 @@ typedef struct amcfd_options {
                             largest box needs and what is resident at once); 0 = that cap
                             (fewer make each warp take several lines of a colour, restaging
                             them every pass) */
-    int reserved[1];
+    int pass_launch;     /* 1: the whole-domain red-black line sweeps (enthalpy, species,
+                            the defect correction) take one launch per colour pass; 0: the
+                            eight passes of a solve run in one launch, pipelined along k so
+                            that later passes find a plane's coefficient rows in L2 (the
+                            same bits: each line still reads its neighbours after exactly
+                            the passes the per-pass order gives it).  serial_launch = 1
+                            implies 1. */
 } amcfd_options;
 
 typedef struct amcfd_deck amcfd_deck;

@@ -172,35 +172,48 @@ def test_cluster_box_momentum_matches_grid_path(prec, steps, tmp_path):
     distributed shared memory after every colour pass).  On the config-1 deck the
     box outgrows one CTA within the first steps (FP64 sooner than FP32); those
     steps agree with the multi-kernel momentum path to 1e-6 relative L2 in FP64
-    (with the same outer-iteration counts).  In FP32 the two paths' roundings
-    differ from the first step on and the difference grows along the track
-    (measured 9e-3 in u after 47 steps, 5.9e-2 and 0.10 in pressure after 60), so
-    FP32 is held to 1e-3 in T, 5e-2 in the velocities against the norm of the
-    whole velocity field and 0.25 in pressure."""
+    (with the same outer-iteration counts).  In FP32 every path's roundings
+    differ from the first step on and the flow field drifts along the track
+    (the outer loop never converges on this deck), so two FP32 paths are not
+    compared with each other: both are compared with the FP64 solve in the same
+    order, and the cluster path must stay as close to it as the default FP32
+    path does: within 3x its error plus 1e-3 (of the velocity norm for the
+    velocities; measured on B200: both about 1e-3 in T after 64 steps)."""
     import amcfd
     import amcfd_decks as D
     d = amcfd.Deck(D.config1(steps=steps).write(str(tmp_path)))
-    a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1, small_box=0)
+    a = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=0, use_graphs=1, small_box=0)
     b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1, small_box=1, mom_cluster=8)
-    spread = 0
+    c = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1) if prec else None
+    spread, worst = 0, {}
     for q in range(steps):
         ra, rb = a.step(), b.step()
+        if c is not None:
+            c.step()
         if prec == 0:
             assert ra["niter"] == rb["niter"], (q + 1, ra["niter"], rb["niter"])
         if rb["momentum_cells"] > 0 and not _one_cta(rb, d.dims[2], 8 if prec == 0 else 4):
             spread += 1
             ya = {f: a.get(f) for f in ("temp", "uvel", "vvel", "wvel", "pressure")}
             vnorm = float(np.sqrt(sum(np.linalg.norm(ya[f]) ** 2 for f in VEL)))
-            for f, y in ya.items():
-                x = b.get(f)
-                if f in VEL:
-                    e, tol = float(np.linalg.norm(x - y)) / vnorm, 1e-6 if prec == 0 else 5e-2
-                else:
-                    e, tol = rel_l2(x, y), 1e-6 if prec == 0 else {"temp": 1e-3, "pressure": 0.25}[f]
-                assert e < tol, (q + 1, f, e)
+
+            def err(s, f):
+                x = s.get(f)
+                return float(np.linalg.norm(x - ya[f])) / (vnorm if f in VEL else np.linalg.norm(ya[f]))
+
+            for f in ya:
+                e = err(b, f)
+                if prec == 0:
+                    assert e < 1e-6, (q + 1, f, e)
+                    continue
+                ec = err(c, f)
+                worst[f] = max(worst.get(f, (0, 0)), (e, ec))
+                assert e < 3 * ec + 1e-3, (q + 1, f, e, ec)
+    print("FP32 error against FP64 (cluster path, default path), worst step:", worst)
     assert spread > 0, "the box never outgrew one CTA"
-    a.close()
-    b.close()
+    for s in (a, b, c):
+        if s is not None:
+            s.close()
 
 
 @pytest.mark.parametrize("prec,box_ctas", [(1, 0), (1, 2), (0, 0)])
@@ -228,5 +241,40 @@ def test_cooperative_box_solve_bit_identical_on_config1(prec, box_ctas, tmp_path
             for f in ("uvel", "vvel", "wvel", "pressure", "temp"):
                 x, y = a.get(f), b.get(f)
                 assert np.array_equal(x, y), (where, f, float(np.abs(x - y).max()))
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("prec,species", [(1, False), (2, False), (0, False), (1, True)])
+def test_pipelined_sweeps_bit_identical(prec, species, tmp_path):
+    """The eight red-black passes of a whole-domain line solve in one pipelined
+    launch (the default) give the same bits as one launch per pass
+    (pass_launch = 1): every line still reads its neighbours after exactly the
+    passes the per-pass order gives it, and the line arithmetic is the same code.
+    Config 1 (100 planes, 200 lines a plane) in FP32 bulk, defect correction (its
+    FP32 correction sweeps) and FP64; and a deck with the species equation, whose
+    concentration solve takes the same launch."""
+    import amcfd
+    import amcfd_decks as D
+    if species:
+        dk = D.small("pipe_sp", nx=40, ny=22, nz=14, steps=4, power=350.0, toolpath=True)
+        dk.species = (1.0, 5e-9, 0.3, 0.7)
+        steps = 4
+    else:
+        dk = D.config1(steps=3)
+        steps = 3
+    d = amcfd.Deck(dk.write(str(tmp_path)))
+    kw = dict(order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1, asm_kseg=16, sweep_warps=4)
+    a = amcfd.Solver(d, pass_launch=1, **kw)
+    b = amcfd.Solver(d, pass_launch=0, **kw)
+    fields = ("temp", "enthalpy", "uvel", "pressure") + (("avgconcentration",) if species else ())
+    for q in range(steps):
+        ra, rb = a.step(), b.step()
+        for k in ("niter", "resorh", "resorm", "tpeak", "alen"):
+            assert ra[k] == rb[k], (q + 1, k, ra[k], rb[k])
+        for f in fields:
+            x, y = a.get(f), b.get(f)
+            assert np.array_equal(x, y), (q + 1, f, int((x != y).sum()), float(np.abs(x - y).max()))
+    assert b.launches < a.launches, (b.launches, a.launches)
     a.close()
     b.close()

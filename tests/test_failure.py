@@ -31,12 +31,14 @@ def _deck(tmp, name, **kw):
     return amcfd.Deck(D.small(name, **kw).write(str(tmp / name)))
 
 
-@pytest.mark.parametrize("graphs", [0, 1])
-def test_line_wait_budget_runs_out_with_timeout(graphs, tmp_path):
+@pytest.mark.parametrize("graphs,order,prec", [(0, 0, 0), (1, 0, 0), (1, 1, 1)])
+def test_line_wait_budget_runs_out_with_timeout(graphs, order, prec, tmp_path):
+    """A line sweep whose waits for neighbouring lines may poll only once fails the
+    step with AMCFD_E_TIMEOUT and returns: the exact-order wavefront (FP64) and
+    the pipelined red-black passes (FP32)."""
     import amcfd
     d = _deck(tmp_path, "wait", steps=2)
-    s = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, use_graphs=graphs,
-                     wait_polls=1)
+    s = amcfd.Solver(d, order=order, precision=prec, use_graphs=graphs, wait_polls=1)
     with pytest.raises(amcfd.AmcfdError) as e:
         s.step()
     assert e.value.code == E_TIMEOUT, str(e.value)
@@ -47,8 +49,8 @@ def test_line_wait_budget_runs_out_with_timeout(graphs, tmp_path):
     assert e.value.code == E_TIMEOUT
     s.close()
     # the process's CUDA context is intact: two fresh solvers agree bit for bit
-    a = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, use_graphs=graphs)
-    b = amcfd.Solver(d, order=amcfd.ORDER_EXACT, precision=amcfd.PREC_FP64, use_graphs=0)
+    a = amcfd.Solver(d, order=order, precision=prec, use_graphs=graphs)
+    b = amcfd.Solver(d, order=order, precision=prec, use_graphs=0)
     for _ in range(2):
         ra, rb = a.step(), b.step()
         assert ra["niter"] == rb["niter"]
