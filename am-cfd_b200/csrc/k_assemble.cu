@@ -440,11 +440,19 @@ energy_assemble_kernel(Params p, Fields<T> g, double *red, const __grid_constant
                 } else {
                     g.an[c] = an; g.as[c] = as_; g.ae[c] = ae; g.aw[c] = aw;
                     g.at[c] = at; g.ab[c] = ab; g.ap[c] = ap; g.su[c] = su;
+                }
+                // neighbour sum of calculateResiduals(5); the FP32 build also takes the
+                // block-correction defect from it (one sum instead of two)
+                const R nbsum = an * hjp + as_ * hjm + ae * hip + aw * him + at * hkp + ab * hkm + su;
+                if constexpr (!DC) {
                     // ---- block-correction sum of the defect (enhanceConvergenceSpeed(5)) ----
-                    blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
+                    if constexpr (kF32)
+                        blc += (double)(nbsum - ap * hc);
+                    else
+                        blc += (double)(ae * hip + aw * him + an * hjp + as_ * hjm + at * hkp + ab * hkm + su - ap * hc);
                 }
                 // ---- residual (calculateResiduals(5)) ----
-                R r = bdiv(an * hjp + as_ * hjm + ae * hip + aw * him + at * hkp + ab * hkm + su, ap) - hc;
+                R r = bdiv(nbsum, ap) - hc;
                 sumd += fabs((double)r);
                 sumh += fabs((double)hc);
                 // ---- block-correction sums (enhanceConvergenceSpeed(5)) ----

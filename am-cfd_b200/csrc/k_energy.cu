@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
     const int js = st->jstart, is0 = st->istart;
     const double ts = p.tsolid;
     const bool steady = p.steady != 0;
+    const bool volsrc = p.volsrc != 0;
     const int lane = threadIdx.x & 31;
     // Work unit: a chunk of 32 V cells of one x-line, V = 16 bytes per element;
     // lane l holds the 16-byte vector of cells base = chunk start + V l (the pitch
@@ -313,7 +314,9 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
         const size_t c0 = (size_t)r * nip + (inrow ? base : 0);
         T hv[V], hn[V], fln[V], rn[V], sv[V];
         ld16(g.h + c0, hv); ld16(g.hnot + c0, hn); ld16(g.fraclnot + c0, fln);
-        ld16(g.rho_nxt + c0, rn); ld16(g.sourceinput + c0, sv);
+        ld16(g.rho_nxt + c0, rn);
+        // the volumetric source input is zero everywhere without a volumetric source
+        if (volsrc) ld16(g.sourceinput + c0, sv);
         const bool rowint = !steady && j >= 1 && j <= njm2 && k >= 1 && k <= nkm2;
         T tout[V], fout[V];
         int cmaxl = INT_MAX, cminl = INT_MIN;  // beam-row length candidates of this lane
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
             const double dh1 = h - (double)hn[v] + ((double)(T)fl - (double)fln[v]) * p.hlatnt;
             const double vol = volume_p(p, g, i, j, k);
             accul += kExact ? vol * (double)rn[v] * dh1 / delt : vol * (double)rn[v] * dh1 * inv_delt;
-            heatvol += (double)sv[v] * vol;
+            if (volsrc) heatvol += (double)sv[v] * vol;
         }
         if (inrow) {
             if (base + V <= ni) {

@@ -50,9 +50,11 @@ WORDS_REDBLACK = {"energy_assemble": 40, "factor": 0, "energy_sweeps": 42, "h2t_
 # DRAM bytes per interior cell per launch (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum, one capture of each kernel on the 400x200x100 deck,
 # FP32 bulk); the line reports them scaled by the cell count.
-# The red-black sweep figure is the average over the 8 launches of an iteration
-# (the first sweep of each colour also forms and stores the factorisation).
+# The red-black sweep family is one pipelined launch of the 8 passes per iteration
+# ("pipe"), or with --pass-launch the average over the 8 per-pass launches (the first
+# sweep of each colour also forms and stores the factorisation).
 TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 87.0, "energy_sweeps:fp32:redblack": 21.2,
+                    "energy_sweeps:fp32:redblack:pipe": 172.9,
                     "h2t_meltpool:fp32:redblack": 29.4, "energy_assemble:fp32dc:redblack": 146.2,
                     "energy_sweeps:fp32dc:redblack": 21.2}
 
@@ -530,7 +532,8 @@ def main():
     avg_ms = prof[fam] / max(nlaunch, 1)
     alg_bytes = words[fam] * ncell * w * piters / max(nlaunch, 1)
     achieved = alg_bytes / (avg_ms / 1e3) / 1e9
-    tr = TRAFFIC_PER_CELL.get(f"{fam}:{args.precision}:{args.order}")
+    pipe = ":pipe" if fam == "energy_sweeps" and args.order == "redblack" and nlaunch <= piters else ""
+    tr = TRAFFIC_PER_CELL.get(f"{fam}:{args.precision}:{args.order}{pipe}")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "kernel": fam,
                 "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_ms,
