@@ -154,8 +154,9 @@ typedef struct amcfd_options {
     int host_loop;       /* 1: with use_graphs, still launch one graph per outer iteration and
                             test convergence on the host (0: one graph per step, the
                             iterations chained on the device) */
-    int wait_polls;      /* polls (about 64 ns each) a warp of the exact-order line sweep
-                            waits for a neighbouring line before the step fails with
+    int wait_polls;      /* polls (about 64 ns each) a warp of a line sweep (the exact-order
+                            wavefront, the pipelined red-black passes, the cooperative
+                            momentum-box solve) waits for a neighbouring line before the step fails with
                             AMCFD_E_TIMEOUT; 0 = the default 2^24 (about one second).  The
                             reference has no such wait (its sweeps are sequential). */
     int autotune;        /* 1: at creation, time the candidate launch shapes of the energy
