@@ -296,9 +296,8 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
     // lane l holds the 16-byte vector of cells base = chunk start + V l (the pitch
     // nip is a multiple of 32, so a vector lies wholly inside or wholly past the
     // padded row).  Chunk indices are 32-bit (the chunk count is bounded at
-    // context creation); a warp steps through the chunks by a fixed stride, so
-    // its row (k, j) and chunk advance by precomputed increments instead of a
-    // division per chunk.
+    // context creation): a 64-bit division per chunk costs more than the
+    // chunk's enthalpy inversions.
     constexpr int V = 16 / (int)sizeof(T);
     constexpr int RC = 32 * V;
     const unsigned cpr = ((unsigned)nip + RC - 1) / RC;  // chunks per row
@@ -307,21 +306,10 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
     const unsigned W = gridDim.x * (blockDim.x >> 5);
     const unsigned w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const double *dxw = g.dxpwinv, *dys = g.dypsinv, *dzb = g.dzpbinv;
-    const unsigned step_r = W / cpr, step_c = W - step_r * cpr;    // rows and chunks per stride
-    const unsigned step_k = step_r / unj, step_j = step_r - step_k * unj;
-    unsigned ch = w0 % cpr, r = w0 / cpr;
-    int k = (int)(r / unj), j = (int)(r - (unsigned)k * unj);
     for (unsigned q = w0; q < nchunks; q += W) {
-        if (q != w0) {  // advance by W chunks
-            ch += step_c;
-            const unsigned carry = ch >= cpr ? 1u : 0u;
-            ch -= carry * cpr;
-            r += step_r + carry;
-            j += (int)(step_j + carry);
-            k += (int)step_k;
-            if (j >= nj) { j -= nj; ++k; }
-        }
-        const int base = (int)ch * RC + V * lane;
+        const unsigned r = q / cpr;
+        const int base = (int)(q - r * cpr) * RC + V * lane;
+        const int k = (int)(r / unj), j = (int)(r - (unsigned)k * unj);
         const bool inrow = base < nip;
         const size_t c0 = (size_t)r * nip + (inrow ? base : 0);
         T hv[V], hn[V], fln[V], rn[V], sv[V];
@@ -330,10 +318,6 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
         // the volumetric source input is zero everywhere without a volumetric source
         if (volsrc) ld16(g.sourceinput + c0, sv);
         const bool rowint = !steady && j >= 1 && j <= njm2 && k >= 1 && k <= nkm2;
-        // rows that hold melt-pool scan candidates: the beam row and the top plane
-        const bool mprow = (j == js && k >= 1 && k <= nkm2) || k == nkm1;
-        // y and z widths of the row's cells (volume_p's operands, in its order)
-        const double dyr = rowint ? g.yv[j + 1] - g.yv[j] : 0.0, dzr = rowint ? g.zw[k + 1] - g.zw[k] : 0.0;
         T tout[V], fout[V];
         int cmaxl = INT_MAX, cminl = INT_MIN;  // beam-row length candidates of this lane
 #pragma unroll
@@ -362,9 +346,9 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
             // are solid, so each atomic is issued only when it can still change the
             // value (candidates only move one way); the beam-row scalars are
             // warp-reduced below.
-            if (mprow && j == js && k >= 1 && k <= nkm2 && tt < ts && k > *(volatile int *)&g.mp_kb[i])
+            if (j == js && k >= 1 && k <= nkm2 && tt < ts && k > *(volatile int *)&g.mp_kb[i])
                 atomicMax(&g.mp_kb[i], k);
-            if (mprow && k == nkm1) {
+            if (k == nkm1) {
                 if (j >= js && j <= njm2 && tt < ts && j < *(volatile int *)&g.mp_jup[i])
                     atomicMin(&g.mp_jup[i], j);
                 if (j >= 1 && j <= js && tt < ts && j > *(volatile int *)&g.mp_jdn[i])
@@ -376,7 +360,7 @@ __global__ void __launch_bounds__(256, 4) h2t_kernel(Params p, Fields<T> g, doub
             }
             if (!rowint || i < 1 || i > nim2) continue;
             const double dh1 = h - (double)hn[v] + ((double)(T)fl - (double)fln[v]) * p.hlatnt;
-            const double vol = ((g.xu[i + 1] - g.xu[i]) * dyr) * dzr;  // volume_p
+            const double vol = volume_p(p, g, i, j, k);
             accul += kExact ? vol * (double)rn[v] * dh1 / delt : vol * (double)rn[v] * dh1 * inv_delt;
             if (volsrc) heatvol += (double)sv[v] * vol;
         }
