@@ -311,18 +311,21 @@ def run_batch(solvers: Sequence["Solver"], nsteps: int, nthreads: int = 0):
 
 
 class Solver:
-    """One melt-pool instance on one GPU (amcfd_create ... amcfd_destroy)."""
+    """One melt-pool instance on one GPU (amcfd_create ... amcfd_destroy).
+
+    small_box: None lets the solver choose the momentum path of a small melt-pool
+    box, 1 forces the one-CTA chain whenever the box fits, 0 never takes it."""
 
     def __init__(self, deck: Deck, order: int = ORDER_EXACT, precision: int = PREC_FP64,
                  device: int = 0, use_graphs: int = 0, check_finite: int = 1,
-                 small_box: int = 1, host_loop: int = 0, wait_polls: int = 0, autotune: int = 0,
+                 small_box: Optional[int] = None, host_loop: int = 0, wait_polls: int = 0, autotune: int = 0,
                  asm_kseg: int = 0, sweep_warps: int = 0, mom_cluster: int = 0, serial_launch: int = 0,
                  box_ctas: int = 0, pass_launch: int = 0):
         L = lib()
         self.deck = deck  # keeps toolpath storage alive
         opts = AmcfdOptions(device=device, order=order, precision=precision,
                             use_graphs=use_graphs, check_finite=check_finite,
-                            no_small_box=0 if small_box else 1, host_loop=host_loop,
+                            no_small_box=0 if small_box is None else (-1 if small_box else 1), host_loop=host_loop,
                             wait_polls=wait_polls, autotune=autotune, asm_kseg=asm_kseg,
                             sweep_warps=sweep_warps, mom_cluster=mom_cluster,
                             serial_launch=serial_launch, box_ctas=box_ctas, pass_launch=pass_launch)

@@ -127,7 +127,7 @@ struct amcfd_ctx {
     int pass_launch = 0;           // 1: the whole-domain red-black sweeps take a launch per pass
     int box_ctas = 0;              // CTAs of the cooperative box solve (0: what the box needs)
     int last_box = -1;             // momentum box cells seen by the last outer iteration
-    bool small_box = true;         // the one-CTA momentum chain may be used
+    int small_mode = 0;            // one-CTA momentum chain: 0 auto, 1 never, -1 whenever the box fits
     const void *diff_a = nullptr;  // the current-property buffer of parity 0
     double *pack = nullptr;        // FP64 read-out staging (ni*nj*nk), made on first use
     // asynchronous read-out: the staging is copied to the host on its own stream
@@ -649,11 +649,21 @@ static void swap_props(Inst<T> &I)
 // The one-CTA momentum chain serves red-black runs whose melt-pool box, as of
 // the last outer iteration, fits its shared memory (it stays correct, only
 // slower, if the box has grown past that since).
+// In the automatic mode the one-CTA chain is taken only where the cooperative box
+// solve is unavailable: on the 400x200x100 deck the cooperative path took 0.099
+// against 0.139 ms an outer iteration for boxes of 1300-2200 cells and 0.100
+// against 0.176 for 2600-3100 cells; on the 120x60x40 deck 0.093 against 0.101
+// (1400-1600 cells) and the same 0.090 for 800-1000 cells.
+template <typename T>
+static bool small_allowed(const amcfd_ctx *ctx, const Inst<T> &I)
+{
+    if (ctx->order != AMCFD_ORDER_REDBLACK || ctx->small_mode == 1) return false;
+    return ctx->small_mode == -1 || I.box_grid == 0;
+}
 template <typename T>
 static bool mom_small(const amcfd_ctx *ctx, const Inst<T> &I)
 {
-    return ctx->small_box && ctx->order == AMCFD_ORDER_REDBLACK && ctx->last_box >= 0 &&
-           ctx->last_box <= mom_small_capacity<T>(I);
+    return small_allowed(ctx, I) && ctx->last_box >= 0 && ctx->last_box <= mom_small_capacity<T>(I);
 }
 
 // The energy line solve: with defect correction the FP32 passes on the correction.
@@ -945,7 +955,7 @@ static int build_loop_graph(amcfd_ctx *ctx, Inst<T> &I, cudaGraphExec_t &ge)
 {
     std::lock_guard<std::mutex> lock(g_capture_mu);
     const int maxit = ctx->prm.maxit;
-    const int cap = ctx->small_box && ctx->order == AMCFD_ORDER_REDBLACK ? mom_small_capacity<T>(I) : -1;
+    const int cap = small_allowed(ctx, I) ? mom_small_capacity<T>(I) : -1;
     const double tol = ctx->prm.nonlintol;
     std::vector<cudaGraph_t> parts;  // captured pieces; child nodes hold copies
     cudaGraph_t top = nullptr;
@@ -1325,7 +1335,9 @@ int amcfd_create(const amcfd_params *params, const amcfd_options *opts, amcfd_ct
         ctx->order = opts->order;
         ctx->precision = opts->precision;
         ctx->use_graphs = opts->use_graphs != 0;
-        ctx->small_box = opts->no_small_box == 0;
+        if (opts->no_small_box < -1 || opts->no_small_box > 1)
+            return fail(ctx, AMCFD_E_ARG, "no_small_box must be -1, 0 or 1");
+        ctx->small_mode = opts->no_small_box;
         ctx->host_loop = opts->host_loop != 0;
         if (opts->wait_polls < 0) return fail(ctx, AMCFD_E_ARG, "wait_polls must not be negative");
         ctx->wait_polls = opts->wait_polls;

@@ -361,6 +361,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--no-small-box", action="store_true",
                     help="momentum boxes of every size on the grid path (no one-CTA path)")
+    ap.add_argument("--small-box", action="store_true",
+                    help="the one-CTA momentum chain whenever the box fits its shared memory")
     ap.add_argument("--serial-launch", action="store_true",
                     help="no programmatic dependent launch; the box line solve as a launch per colour pass")
     ap.add_argument("--pass-launch", action="store_true",
@@ -442,7 +444,7 @@ def main():
             dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
         sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
                           host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster,
-                          small_box=0 if args.no_small_box else 1, serial_launch=1 if args.serial_launch else 0,
+                          small_box=0 if args.no_small_box else (1 if args.small_box else None), serial_launch=1 if args.serial_launch else 0,
                           pass_launch=1 if args.pass_launch else 0, **kw)
         tune.setdefault(p, sv.tuning())
         return sv
@@ -590,7 +592,9 @@ def main():
                           amcfd.PREC_FP64: "f64"}[prec], "data": "synthetic deck",
                 "config": dict(cfg_desc, precision=args.precision, order=args.order, graphs=args.graphs,
                                outer_loop="host" if args.host_loop or not args.graphs else "device",
-                               momentum=("grid" if args.no_small_box else "one-CTA below its capacity, else grid")
+                               momentum=("grid" if args.no_small_box else "one-CTA below its capacity, else grid"
+                                         if args.small_box else "cooperative box solve"
+                                         " (one-CTA chain only where that is unavailable)")
                                + (", serial launches" if args.serial_launch else ""),
                                sweeps="a launch per pass" if args.pass_launch or args.serial_launch
                                else "the 8 passes of a solve in one pipelined launch",

@@ -149,8 +149,11 @@ typedef struct amcfd_options {
     int precision;       /* AMCFD_PREC_* */
     int use_graphs;      /* capture the fixed-shape part of an outer iteration */
     int check_finite;    /* fail with AMCFD_E_NONFINITE when a reduction is not finite */
-    int no_small_box;    /* 1: never run the momentum chain of a small melt-pool box in one
-                            CTA (red-black order only; 0 lets the solver choose) */
+    int no_small_box;    /* the momentum chain of a melt-pool box small enough for one CTA's
+                            shared memory (red-black order only): 0 lets the solver choose (the
+                            cooperative box solve where it is available, which measured as fast
+                            or faster for every box size, else the one-CTA chain); 1 never runs
+                            the one-CTA chain; -1 runs it whenever the box fits */
     int host_loop;       /* 1: with use_graphs, still launch one graph per outer iteration and
                             test convergence on the host (0: one graph per step, the
                             iterations chained on the device) */

@@ -11,8 +11,8 @@ the compiled reference) and through the C ABI:
   line solvers run many 16-byte rounds per line, the assembly many 32 x 8 tiles
   and the TMA boxes span 400-node rows);
 * the production path that bench.py times (FP32 bulk with FP64 reductions,
-  red-black line order, the one-CTA momentum path for small boxes, the whole
-  outer loop of a step as one CUDA graph): melt-pool length, depth and width
+  red-black line order, the cooperative momentum-box solve, the whole outer
+  loop of a step as one CUDA graph): melt-pool length, depth and width
   within one cell of the oracle's (the cell widths of the grid where each is
   measured), and T, u, v, w within the stated relative L2 of the oracle.  The
   red-black order is a different iteration from the reference's sweep, and
@@ -111,8 +111,7 @@ def test_exact_fp64_matches_oracle(name, tmp_path_factory):
 def test_production_path_melt_pool_within_one_cell(name, tmp_path_factory):
     import amcfd
     d, steps, grid = _oracle(name, tmp_path_factory)
-    s = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1,
-                     host_loop=0, small_box=1)
+    s = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=amcfd.PREC_FP32, use_graphs=1, host_loop=0)
     for q, (ro, fo) in enumerate(steps):
         rg = s.step()
         where = f"{name} step {q + 1}"
