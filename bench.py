@@ -54,7 +54,7 @@ WORDS_REDBLACK = {"energy_assemble": 40, "factor": 0, "energy_sweeps": 42, "h2t_
 # ("pipe"), or with --pass-launch the average over the 8 per-pass launches (the first
 # sweep of each colour also forms and stores the factorisation).
 TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 87.0, "energy_sweeps:fp32:redblack": 21.2,
-                    "energy_sweeps:fp32:redblack:pipe": 172.9,
+                    "energy_sweeps:fp32:redblack:pipe": 174.3,
                     "h2t_meltpool:fp32:redblack": 29.4, "energy_assemble:fp32dc:redblack": 146.2,
                     "energy_sweeps:fp32dc:redblack": 21.2}
 
