@@ -133,6 +133,7 @@ def lib() -> C.CDLL:
             L.amcfd_free_surface.argtypes = [VP, P(AmcfdFreeSurface)]
             L.amcfd_run_steps.argtypes = [VP, _I, P(AmcfdReport), P(_D)]
             L.amcfd_tuning.argtypes = [VP, P(_I), P(_I), P(_D)]
+            L.amcfd_pipe_stride.argtypes = [VP, P(_I)]
             L.amcfd_kernel_launches.argtypes = [VP]
             L.amcfd_kernel_launches.restype = C.c_longlong
             L.amcfd_run_batch.argtypes = [P(VP), _I, _I, _I, P(AmcfdReport), P(_I)]
@@ -378,13 +379,18 @@ class Solver:
         self._check(lib().amcfd_profile(self._h, 1 if enable else 0))
 
     def tuning(self) -> Dict:
-        """Launch shapes in use (amcfd_tuning): assembly planes per CTA, sweep lines
-        per CTA and, after autotuning, the candidates' times in ms."""
+        """Launch shapes in use (amcfd_tuning, amcfd_pipe_stride): assembly planes per
+        CTA, lines per CTA of the per-pass sweeps, the planes between passes of the
+        pipelined sweep (0 when not pipelined) and, after autotuning, the
+        candidates' times in ms (sweep_ms keyed by stride when pipelined)."""
         a, w = _I(), _I()
         t = (_D * 6)()
         self._check(lib().amcfd_tuning(self._h, C.byref(a), C.byref(w), t))
-        return {"asm_kseg": a.value, "sweep_warps": w.value,
-                "asm_ms": {4: t[0], 8: t[1], 16: t[2]}, "sweep_ms": {2: t[3], 4: t[4], 8: t[5]}}
+        d = _I()
+        self._check(lib().amcfd_pipe_stride(self._h, C.byref(d)))
+        keys = (8, 16, 32) if d.value else (2, 4, 8)
+        return {"asm_kseg": a.value, "sweep_warps": w.value, "pipe_stride": d.value,
+                "asm_ms": {4: t[0], 8: t[1], 16: t[2]}, "sweep_ms": dict(zip(keys, t[3:6]))}
 
     @property
     def launches(self) -> int:

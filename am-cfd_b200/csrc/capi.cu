@@ -1237,7 +1237,12 @@ template <typename T>
 static int autotune(amcfd_ctx *ctx, Inst<T> &I)
 {
     cudaEvent_t e0 = ctx->ev[14], e1 = ctx->ev[15];
-    const int segs[3] = {4, 8, 16}, warps[3] = {2, 4, 8};
+    const int segs[3] = {4, 8, 16}, warps[3] = {2, 4, 8}, strides[3] = {8, 16, 32};
+    // the line sweeps: with the passes pipelined in one launch, the planes between
+    // passes in its work order; otherwise the lines per CTA of the per-pass launches
+    bool pipe = I.pipe_grid > 0;
+    if constexpr (sizeof(T) == sizeof(double))
+        if (I.dc_on) pipe = I.pipe_grid_dc > 0;
     float best_asm[3], best_sw[3];
     for (int c = 0; c < 3; ++c) best_asm[c] = best_sw[c] = INFINITY;
     auto set_seg = [&](int seg) {
@@ -1246,15 +1251,23 @@ static int autotune(amcfd_ctx *ctx, Inst<T> &I)
         I.nb_asm = I.asm_grid.x * I.asm_grid.y * I.asm_grid.z;
         I.g.npart = I.asm_grid.y * I.asm_grid.z;
     };
-    auto sweep_probe = [&](int w) {
+    auto sweep_probe = [&](int c) {
+        if (pipe) I.pipe_stride = strides[c];
         if constexpr (sizeof(T) == sizeof(double)) {
             if (I.dc_on) {
-                launch_dc_sweep_probe(I, w);
+                if (pipe)
+                    launch_dc_sweeps(I);  // overwrites only the correction
+                else
+                    launch_dc_sweep_probe(I, warps[c]);
                 return;
             }
         }
-        launch_sweep_probe<T>(I, I.mom_scratch, w);
+        if (pipe)
+            launch_phi_sweeps<T>(I, I.mom_scratch);  // a scratch field
+        else
+            launch_sweep_probe<T>(I, I.mom_scratch, warps[c]);
     };
+    const bool tune_sweep = ctx->order == AMCFD_ORDER_REDBLACK && (pipe || !ctx->sweep_warps);
     for (int round = 0; round < 4; ++round)
         for (int q = 0; q < 3; ++q) {
             const int c = (q + round) % 3;
@@ -1268,9 +1281,9 @@ static int autotune(amcfd_ctx *ctx, Inst<T> &I)
                 CK(cudaEventElapsedTime(&ms, e0, e1));
                 if (round > 0) best_asm[c] = std::min(best_asm[c], ms);
             }
-            if (!ctx->sweep_warps && ctx->order == AMCFD_ORDER_REDBLACK && warps[c] <= I.sweep_warps_max) {
+            if (tune_sweep && (pipe || warps[c] <= I.sweep_warps_max)) {
                 CK(cudaEventRecord(e0, ctx->stream));
-                sweep_probe(warps[c]);
+                sweep_probe(c);
                 CK(cudaEventRecord(e1, ctx->stream));
                 CK(cudaEventSynchronize(e1));
                 CK(cudaEventElapsedTime(&ms, e0, e1));
@@ -1284,10 +1297,14 @@ static int autotune(amcfd_ctx *ctx, Inst<T> &I)
         ctx->asm_kseg = segs[c];
         for (int q = 0; q < 3; ++q) ctx->tune_ms[q] = best_asm[q];
     }
-    if (!ctx->sweep_warps && ctx->order == AMCFD_ORDER_REDBLACK) {
+    if (tune_sweep) {
         const int c = (int)(std::min_element(best_sw, best_sw + 3) - best_sw);
-        I.sweep_warps = warps[c];
-        ctx->sweep_warps = warps[c];
+        if (pipe) {
+            I.pipe_stride = strides[c];
+        } else {
+            I.sweep_warps = warps[c];
+            ctx->sweep_warps = warps[c];
+        }
         for (int q = 0; q < 3; ++q) ctx->tune_ms[3 + q] = best_sw[q];
     }
     ctx->launches += 4 * 3 * 3;
@@ -1306,6 +1323,15 @@ int amcfd_tuning(const amcfd_ctx *ctx, int *asm_kseg, int *sweep_warps, double *
     if (sweep_warps) *sweep_warps = w;
     if (times)
         for (int q = 0; q < 6; ++q) times[q] = ctx->tune_ms[q];
+    return 0;
+}
+
+int amcfd_pipe_stride(const amcfd_ctx *ctx, int *stride)
+{
+    if (!ctx || !stride) return AMCFD_E_ARG;
+    const bool fp64 = ctx->precision == AMCFD_PREC_FP64;
+    const int grid = fp64 ? (ctx->dc ? ctx->I64.pipe_grid_dc : ctx->I64.pipe_grid) : ctx->I32.pipe_grid;
+    *stride = grid > 0 ? (fp64 ? ctx->I64.pipe_stride : ctx->I32.pipe_stride) : 0;
     return 0;
 }
 

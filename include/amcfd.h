@@ -292,8 +292,14 @@ long long amcfd_kernel_launches(const amcfd_ctx *ctx);
  * energy assembly (*asm_kseg, 0 = the default rule) and lines per CTA of the
  * red-black sweeps (*sweep_warps); with amcfd_options.autotune, the measured times
  * of the candidates in ms (times[0..2]: assembly with 4, 8, 16 planes; times[3..5]:
- * a factorising and a plain sweep pass with 2, 4, 8 lines; 0 when not timed). */
+ * a factorising and a plain sweep pass with 2, 4, 8 lines, or, when the red-black
+ * passes run as one pipelined launch, that launch with its passes 8, 16, 32 planes
+ * apart in its work order; 0 when not timed). */
 int amcfd_tuning(const amcfd_ctx *ctx, int *asm_kseg, int *sweep_warps, double *times);
+/* The planes between successive passes in the work order of the pipelined red-black
+ * line solve (autotuned among 8, 16, 32; default 16), or 0 when the passes take a
+ * launch each.  No counterpart in the reference (its sweeps are sequential loops). */
+int amcfd_pipe_stride(const amcfd_ctx *ctx, int *stride);
 
 /* Parameter sweep over independent instances: runs nsteps time steps of every
  * context in ctxs[0..n), each on its own stream, spread over nthreads host threads

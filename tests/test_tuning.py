@@ -1,9 +1,11 @@
 """The autotuner: at creation it times the energy assembly with 4, 8 and 16
-planes per CTA and the red-black sweep passes with 2, 4 and 8 lines per CTA on
-the context's own grid, and keeps the fastest.  The launch shape changes no
-arithmetic of the sweeps and only the order of the assembly's FP64 partial
-sums, so a context pinned to the shapes the tuner chose reproduces the tuned
-one bit for bit, and every shape agrees with the default to rounding."""
+planes per CTA and the pipelined red-black line solve with its passes 8, 16
+and 32 planes apart in its work order (the per-pass sweeps, when they run, with
+2, 4 and 8 lines per CTA) on the context's own grid, and keeps the fastest.
+The launch shape changes no arithmetic of the sweeps and only the order of the
+assembly's FP64 partial sums, so a context pinned to the assembly shape the
+tuner chose reproduces the tuned one bit for bit (whatever its sweep stride),
+and every shape agrees with the default to rounding."""
 import numpy as np
 import pytest
 
@@ -24,6 +26,8 @@ def test_tuned_shapes_are_reported_and_reproducible(prec, tmp_path):
     assert t["asm_kseg"] in (4, 8, 16) and t["sweep_warps"] in (2, 4, 8), t
     assert all(v > 0 for v in t["asm_ms"].values()), t
     assert t["asm_ms"][t["asm_kseg"]] == min(t["asm_ms"].values())
+    assert t["pipe_stride"] in (8, 16, 32), t
+    assert t["sweep_ms"][t["pipe_stride"]] == min(t["sweep_ms"].values()) > 0, t
     b = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1,
                      asm_kseg=t["asm_kseg"], sweep_warps=t["sweep_warps"])
     c = amcfd.Solver(d, order=amcfd.ORDER_REDBLACK, precision=prec, use_graphs=1)
