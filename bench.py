@@ -79,6 +79,7 @@ class Clocks:
         self.idx = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def start(self):
         if not shutil.which("nvidia-smi"):
@@ -96,6 +97,8 @@ class Clocks:
             if os.path.getsize(self.path) > 0:
                 break
             time.sleep(0.02)
+        with open(self.path) as f:
+            self.skip = sum(1 for _ in f)  # samples taken before the timed region
 
     def stop(self):
         if not self.proc:
@@ -109,18 +112,21 @@ class Clocks:
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    mx = max(mx, float(parts[2]))
-                except ValueError:
-                    continue
-                for n, v in zip(names, parts[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
+            lines = f.readlines()
+        # the samples taken during the timed region (the first one too when it is the only one)
+        lines = lines[self.skip:] if len(lines) > self.skip else lines
+        for line in lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
         os.unlink(self.path)
         if not sm:
             return None
