@@ -452,12 +452,15 @@ def main():
 
     def solver(p=prec):
         # the production path tunes its launch shapes at creation; later solvers of the
-        # same precision are pinned to the first one's choice
-        kw = dict(asm_kseg=tune[p]["asm_kseg"], sweep_warps=tune[p]["sweep_warps"]) if p in tune else \
-            dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
+        # same precision are pinned to the first one's assembly and sweep shapes (the
+        # pipelined sweep's stride, which changes no bits, is tuned again)
+        kw = dict(autotune=1 if order == amcfd.ORDER_REDBLACK else 0)
+        if p in tune:
+            kw.update(asm_kseg=tune[p]["asm_kseg"], sweep_warps=tune[p]["sweep_warps"])
+        small = 0 if args.no_small_box else (1 if args.small_box else None)
         sv = amcfd.Solver(d, order=order, precision=p, device=dev, use_graphs=args.graphs,
                           host_loop=1 if args.host_loop else 0, mom_cluster=args.mom_cluster,
-                          small_box=0 if args.no_small_box else (1 if args.small_box else None), serial_launch=1 if args.serial_launch else 0,
+                          small_box=small, serial_launch=1 if args.serial_launch else 0,
                           pass_launch=1 if args.pass_launch else 0, **kw)
         tune.setdefault(p, sv.tuning())
         return sv
