@@ -266,6 +266,11 @@ class Net:
         self._check(lib().amcfd_net_get_grads(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), self.nparams))
         return out
 
+    def set_grads(self, g: np.ndarray):
+        """Replace the gradients the next adam() applies (amcfd_net_set_grads)."""
+        a = np.ascontiguousarray(g, dtype=np.float32)
+        self._check(lib().amcfd_net_set_grads(self._h, a.ctypes.data_as(C.POINTER(C.c_float)), self.nparams))
+
     def forward(self, feat_ptr: int, dims, y_ptr: int = 0):
         ni, nj, nk = dims
         self._check(lib().amcfd_net_forward(self._h, feat_ptr, ni, nj, nk, y_ptr or None))

@@ -5,6 +5,11 @@ step the network takes ``updates`` Adam steps on that step's pair (features
 at the start of the step -> realised enthalpy and pressure increments), all on
 the GPU with the tensor-core kernels of k_cnn.cu.
 
+Data-parallel training (``train`` with a process group): each rank solves its
+own share of the decks and, after every backward pass, the ranks' gradients
+are averaged with one all-reduce (NCCL over NVLink for CUDA tensors, or gloo)
+before the Adam step, so every rank keeps the same parameters.
+
 Evaluation (``evaluate``): the same deck is solved twice, plainly and with
 the network's prediction as the starting guess of every step (rejected when
 it raises the step's initial energy residual); the outer-iteration counts,
@@ -33,10 +38,44 @@ def device_view(ptr: int, shape):
     return torch.as_tensor(DeviceArray(ptr, shape), device="cuda")
 
 
+def average_grads(net, group=None) -> None:
+    """Replace the network's gradients by their mean over the ranks of `group`
+    (torch.distributed; the default group when None).  Every rank must call it
+    the same number of times.  The gradients go through a CUDA tensor when the
+    group's backend is NCCL, a CPU tensor otherwise."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    if world == 1:
+        return
+    t = torch.from_numpy(net.grads())
+    if dist.get_backend(group) == "nccl":
+        t = t.cuda()
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    net.set_grads((t / world).cpu().numpy())
+
+
+def shard(deck_paths: Sequence[str], rank: int, world: int) -> List[str]:
+    """This rank's decks (every world-th from `rank`); the deck count must divide
+    evenly, so that every rank runs the same number of updates (all-reduces)."""
+    if len(deck_paths) % world:
+        raise ValueError(f"{len(deck_paths)} decks do not split evenly over {world} ranks")
+    return list(deck_paths[rank::world])
+
+
 def train(net: amcfd.Net, deck_paths: Sequence[str], steps: int, lr: float = 1e-3, updates: int = 4,
-          precision: int = amcfd.PREC_FP32, order: int = amcfd.ORDER_REDBLACK, device: int = 0) -> List[float]:
-    """Online training on every step of every deck; returns the loss history."""
+          precision: int = amcfd.PREC_FP32, order: int = amcfd.ORDER_REDBLACK, device: int = 0,
+          group=None) -> List[float]:
+    """Online training on every step of every deck; returns the loss history.
+
+    With `group` (a torch.distributed process group, or True for the default
+    one) each rank trains on its shard of `deck_paths` and the gradients are
+    averaged over the ranks before every Adam step."""
     losses: List[float] = []
+    if group is not None:
+        import torch.distributed as dist
+        grp = None if group is True else group
+        deck_paths = shard(deck_paths, dist.get_rank(grp), dist.get_world_size(grp))
     for path in deck_paths:
         s = amcfd.Solver(amcfd.Deck(path), order=order, precision=precision, device=device, use_graphs=1)
         s.ws_attach(net, amcfd.WS_RECORD)
@@ -47,6 +86,8 @@ def train(net: amcfd.Net, deck_paths: Sequence[str], steps: int, lr: float = 1e-
             for _ in range(updates):
                 net.forward(feat, (ni, nj, nk))
                 losses.append(net.backward(target))
+                if group is not None:
+                    average_grads(net, None if group is True else group)
                 net.adam(lr)
         s.ws_attach(None, amcfd.WS_OFF)
         s.close()

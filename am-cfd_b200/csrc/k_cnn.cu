@@ -840,6 +840,17 @@ int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n)
     return 0;
 }
 
+// Replaces the gradient buffer (what amcfd_net_adam applies next), e.g. with the
+// average over the ranks of a data-parallel training run.
+int amcfd_net_set_grads(amcfd_net *net, const float *host, size_t n)
+{
+    if (!net || !host || n != nparams()) return AMCFD_E_ARG;
+    NCK(cudaSetDevice(net->device));
+    NCK(cudaStreamSynchronize(net->stream));
+    NCK(cudaMemcpy(net->g, host, n * sizeof(float), cudaMemcpyHostToDevice));
+    return 0;
+}
+
 // Forward pass on device features [ncell][11] (FP32) over an ni x nj x nk node
 // grid; y_dev (may be null) receives the two outputs [ncell][2] (FP32).
 int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev)

@@ -366,6 +366,9 @@ const char *amcfd_net_last_error(const amcfd_net *net);
 int amcfd_net_get_params(amcfd_net *net, float *host, size_t n);
 int amcfd_net_set_params(amcfd_net *net, const float *host, size_t n);
 int amcfd_net_get_grads(amcfd_net *net, float *host, size_t n);
+/* Overwrites the gradients that amcfd_net_adam applies next (data-parallel training
+ * averages them over the ranks in between).  No counterpart in the reference. */
+int amcfd_net_set_grads(amcfd_net *net, const float *host, size_t n);
 /* feat_dev: [ncell][11] FP32; y_dev (nullable): [ncell][2] FP32 */
 int amcfd_net_forward(amcfd_net *net, const float *feat_dev, int ni, int nj, int nk, float *y_dev);
 /* MSE of the last forward pass against target_dev [ncell][2] over interior cells;
