@@ -55,7 +55,7 @@ WORDS_REDBLACK = {"energy_assemble": 40, "factor": 0, "energy_sweeps": 42, "h2t_
 # sweep of each colour also forms and stores the factorisation).
 TRAFFIC_PER_CELL = {"energy_assemble:fp32:redblack": 87.0, "energy_sweeps:fp32:redblack": 21.2,
                     "energy_sweeps:fp32:redblack:pipe": 174.3,
-                    "h2t_meltpool:fp32:redblack": 29.4, "energy_assemble:fp32dc:redblack": 146.2,
+                    "h2t_meltpool:fp32:redblack": 24.2, "energy_assemble:fp32dc:redblack": 146.2,
                     "energy_sweeps:fp32dc:redblack": 21.2}
 
 
@@ -109,30 +109,37 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.f.close()
-        sm, mx, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
             lines = f.readlines()
-        # the samples taken during the timed region (the first one too when it is the only one)
-        lines = lines[self.skip:] if len(lines) > self.skip else lines
-        for line in lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = max(mx, float(parts[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
         os.unlink(self.path)
-        if not sm:
-            return None
-        sm.sort()
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return parse_clock_samples(lines, self.skip)
+
+
+def parse_clock_samples(lines, skip: int = 0):
+    """Summary of nvidia-smi samples (rows of Clocks.Q, no header, no units): the
+    median and maximum SM clock and the throttle reasons seen, over the rows after
+    the first `skip` (those taken before the timed region; all rows when that
+    leaves none); None without a parsable row."""
+    sm, mx, reasons = [], 0.0, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    lines = lines[skip:] if len(lines) > skip else lines
+    for line in lines:
+        parts = [p.strip() for p in line.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            sm.append(float(parts[1]))
+            mx = max(mx, float(parts[2]))
+        except ValueError:
+            continue
+        for n, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    if not sm:
+        return None
+    sm.sort()
+    return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
 
 
 FEATURES = {
