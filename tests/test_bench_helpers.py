@@ -46,3 +46,21 @@ def test_traffic_figures_cover_the_production_families():
     assert 8 * t["energy_sweeps:fp32:redblack"] < 1.1 * t["energy_sweeps:fp32:redblack:pipe"]
     for fam in ("energy_assemble", "h2t_meltpool"):
         assert f"{fam}:fp32:redblack" in t
+
+
+def test_clock_sampler_end_to_end_with_a_stand_in_nvidia_smi(tmp_path, monkeypatch):
+    """Clocks.start/stop around a short region, with a stand-in nvidia-smi on PATH
+    that prints one sample row every 50 ms."""
+    import time
+    b = _bench()
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\nwhile true; do echo '0, 1965, 1965, 700.0, 0x0, Not Active, Not Active, "
+                    "Not Active, Not Active'; sleep 0.05; done\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ.get('PATH', '')}")
+    c = b.Clocks(0)
+    c.start()
+    time.sleep(0.3)
+    out = c.stop()
+    assert out is not None and out["samples"] >= 1, out
+    assert out["sm_mhz"] == 1965.0 and out["reasons"] == []
