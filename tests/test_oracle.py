@@ -94,13 +94,20 @@ def _variants():
     d = D.free_surface_track("v_freesurf", steps=4)
     d.scheme, d.single_track = "upwind", (2e-5,) + d.single_track[1:]
     out.append(d)
+    # the 600 x 300 x 120 benchmark deck's toolpath in miniature: a bidirectional
+    # raster with the beam off during a dwell between tracks, 12 steps (first
+    # track, dwell, start of the second)
+    d = D.small("v_raster", steps=12, power=250.0)
+    d.single_track = None
+    d.toolpath = D.raster_toolpath(0.20e-3, 0.26e-3, 0.18e-3, 60e-6, 2, D._top(d.z_zones), 1.0, 2e-5)
+    out.append(d)
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(8))
+@pytest.mark.parametrize("idx", range(9))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
