@@ -101,13 +101,16 @@ def _variants():
     d.single_track = None
     d.toolpath = D.raster_toolpath(0.20e-3, 0.26e-3, 0.18e-3, 60e-6, 2, D._top(d.z_zones), 1.0, 2e-5)
     out.append(d)
+    # the exponential scheme: the reference divides 0/0 at zero Peclet number, and
+    # the oracle reproduces where the NaNs appear
+    out.append(D.small("v_exponential", steps=2, scheme="exponential_law"))
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(9))
+@pytest.mark.parametrize("idx", range(10))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
