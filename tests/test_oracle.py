@@ -109,13 +109,15 @@ def _variants():
     cells = [sum(z[1] for z in q.x_zones) * sum(z[1] for z in q.y_zones) * sum(z[1] for z in q.z_zones)
              for q in sweep]
     out.append(sweep[cells.index(min(cells))])
+    # the 120 x 60 x 40 benchmark deck itself, its first two steps
+    out.append(D.config0(steps=2))
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(11))
+@pytest.mark.parametrize("idx", range(12))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
