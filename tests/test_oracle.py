@@ -111,13 +111,16 @@ def _variants():
     out.append(sweep[cells.index(min(cells))])
     # the 120 x 60 x 40 benchmark deck itself, its first two steps
     out.append(D.config0(steps=2))
+    # and the 400 x 200 x 100 deck bench.py times, its first step (about 40 s of
+    # single-threaded CPU for the two solvers, an 0.9 GB dump)
+    out.append(D.config1(steps=1))
     return out
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref",
                                                     "amcfd_ref_dump")),
                     reason="reference not built in this checkout (oracle/build_ref.sh)")
-@pytest.mark.parametrize("idx", range(12))
+@pytest.mark.parametrize("idx", range(13))
 def test_oracle_bit_exact_live(idx, tmp_path, oracle_lib):
     import amcfd
     import oracle_py
