@@ -122,7 +122,7 @@ typedef struct amcfd_step_report {
     double beamposx, beamposy, scanvel;
     int istat, iend, jstat, jend, kstat, jstart, powerindicator;
     int momentum_cells;  /* cells of the momentum box solved in the last outer iteration */
-    int fallback;        /* reserved: 1 when a warm-start guess was rejected */
+    int fallback;        /* 1 when the step's warm-start guess was rejected */
     double resorc;       /* species residual (calculateResiduals(6)); 0 without *SOLVE_SPECIES */
     int nk_active;       /* nodes in z of the active domain (grows per powder layer) */
     int trackindx;       /* BoundCondManager::trackindx_ */
